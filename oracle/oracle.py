@@ -1,0 +1,149 @@
+"""ctypes binding of the CPU oracle -- TEST INFRASTRUCTURE.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module.  It wraps oracle/_build/libsf2d_oracle.so (built by
+oracle/Makefile) and feeds it a setup Database.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libsf2d_oracle.so")
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+class OracleDb(ctypes.Structure):
+    _fields_ = [
+        ("nspec", ctypes.c_int), ("nglob", ctypes.c_int),
+        ("ibool", _ip),
+        ("xix", _dp), ("xiz", _dp), ("gammax", _dp), ("gammaz", _dp), ("jacobian", _dp),
+        ("rhostore", _dp), ("kappastore", _dp), ("mustore", _dp), ("rho_vpstore", _dp), ("rho_vsstore", _dp),
+        ("rmass_inverse", _dp),
+        ("hprime", _dp), ("hprimewgll", _dp), ("wxgll", _dp), ("wzgll", _dp),
+        ("nstacey", ctypes.c_int), ("st_iglob", _ip),
+        ("st_nx", _dp), ("st_nz", _dp), ("st_w", _dp), ("st_rvp", _dp), ("st_rvs", _dp),
+        ("nsrc", ctypes.c_int), ("src_ispec", _ip), ("sourcearrays", _dp), ("stf", _dp),
+        ("nstep_total", ctypes.c_int), ("nstage", ctypes.c_int),
+        ("nrec", ctypes.c_int), ("rec_ispec", _ip), ("hxir", _dp), ("hgammar", _dp),
+        ("cosrot", ctypes.c_double), ("sinrot", ctypes.c_double),
+        ("seismotype", ctypes.c_int),
+        ("deltat", ctypes.c_double), ("deltatover2", ctypes.c_double), ("deltatsquareover2", ctypes.c_double),
+        ("ispec_is_anisotropic", _ip),
+        ("c11", _dp), ("c13", _dp), ("c15", _dp), ("c33", _dp), ("c35", _dp), ("c55", _dp),
+    ]
+
+
+def build() -> str:
+    """Compile the oracle library if it is missing or older than its source."""
+    src = os.path.join(HERE, "sf2d_oracle.cpp")
+    if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = ctypes.CDLL(build())
+        _lib.sf2d_oracle_newmark_elastic.restype = ctypes.c_int
+        _lib.sf2d_oracle_newmark_elastic.argtypes = [
+            ctypes.POINTER(OracleDb), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _dp, ctypes.c_int]
+        _lib.sf2d_oracle_max_threads.restype = ctypes.c_int
+    return _lib
+
+
+class Oracle:
+    """Holds converted arrays (kept alive) and runs the oracle time loop."""
+
+    def __init__(self, db, precision: int = 4, seismotype: int = 1, db64=None):
+        """``db`` supplies the FP32 setup; ``db64`` (optional) the FP64 one for precision 8."""
+        self.precision = precision
+        src = db64 if (precision == 8 and db64 is not None) else db
+        self.db = src
+        keep = []
+
+        def d(a):
+            arr = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+            keep.append(arr)
+            return arr.ctypes.data_as(_dp)
+
+        def i(a):
+            arr = np.ascontiguousarray(np.asarray(a, dtype=np.int32))
+            keep.append(arr)
+            return arr.ctypes.data_as(_ip)
+
+        g = src.gll
+        if precision == 8:
+            hprime = g.hprime_dble
+            hprimewgll = g.wgll_dble[:, None] * g.hprime_dble
+            wx = g.wgll_dble
+            dt = float(src.dt)
+            dto2 = 0.5 * dt
+            dt2o2 = 0.5 * dt * dt
+        else:
+            hprime = g.hprime
+            hprimewgll = g.hprimewgll
+            wx = g.wxgll
+            dt = float(src.deltat)
+            dto2 = float(src.deltatover2)
+            dt2o2 = float(src.deltatsquareover2)
+        nstage = src.stf.shape[2] if src.stf.ndim == 3 else 1
+        s = OracleDb()
+        s.nspec, s.nglob = src.nspec, src.nglob
+        s.ibool = i(src.ibool)
+        s.xix, s.xiz, s.gammax, s.gammaz, s.jacobian = (d(src.xix), d(src.xiz), d(src.gammax),
+                                                        d(src.gammaz), d(src.jacobian))
+        s.rhostore, s.kappastore, s.mustore = d(src.rhostore), d(src.kappastore), d(src.mustore)
+        s.rho_vpstore, s.rho_vsstore = d(src.rho_vpstore), d(src.rho_vsstore)
+        s.rmass_inverse = d(src.rmass_inverse_elastic)
+        s.hprime, s.hprimewgll, s.wxgll, s.wzgll = d(hprime), d(hprimewgll), d(wx), d(wx)
+        s.nstacey = len(src.stacey_iglob)
+        s.st_iglob = i(src.stacey_iglob)
+        s.st_nx, s.st_nz, s.st_w = d(src.stacey_nx), d(src.stacey_nz), d(src.stacey_weight)
+        s.st_rvp, s.st_rvs = d(src.stacey_rho_vp), d(src.stacey_rho_vs)
+        s.nsrc = len(src.source_ispec)
+        s.src_ispec = i(src.source_ispec)
+        s.sourcearrays = d(src.sourcearrays)
+        s.stf = d(src.stf)
+        s.nstep_total = src.stf.shape[1] if s.nsrc else 0
+        s.nstage = nstage
+        s.nrec = len(src.rec_ispec)
+        s.rec_ispec = i(src.rec_ispec)
+        s.hxir, s.hgammar = d(src.hxir), d(src.hgammar)
+        s.cosrot, s.sinrot = float(src.cosrot), float(src.sinrot)
+        s.seismotype = seismotype
+        s.deltat, s.deltatover2, s.deltatsquareover2 = dt, dto2, dt2o2
+        self._keep = keep
+        self.s = s
+        dtype = np.float32 if precision == 4 else np.float64
+        self.displ = np.zeros((src.nglob, 2), dtype=dtype)
+        self.veloc = np.zeros((src.nglob, 2), dtype=dtype)
+        self.accel = np.zeros((src.nglob, 2), dtype=dtype)
+        self.it = 0
+
+    def run(self, nstep: int, nthreads: int = 0) -> np.ndarray:
+        """Advance nstep Newmark steps; return seismograms (nrec, nstep, 2) float64."""
+        seis = np.zeros((self.s.nrec, nstep, 2), dtype=np.float64)
+        rc = lib().sf2d_oracle_newmark_elastic(
+            ctypes.byref(self.s), self.precision, self.it, nstep,
+            self.displ.ctypes.data, self.veloc.ctypes.data, self.accel.ctypes.data,
+            seis.ctypes.data_as(_dp), nthreads)
+        if rc != 0:
+            raise RuntimeError(f"oracle failed with status {rc}")
+        self.it += nstep
+        return seis
+
+
+def max_threads() -> int:
+    return int(lib().sf2d_oracle_max_threads())

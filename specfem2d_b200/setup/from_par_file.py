@@ -1,0 +1,102 @@
+"""Build a setup Database from a reference-style DATA/ directory.
+
+Supports the internal-mesher subset used by the hot path: interfaces file,
+isotropic material table with regions, Stacey or free edges, force or
+moment-tensor sources, a receiver line (src/meshfem2D/save_stations_file.f90:
+receivers evenly spaced between (xdeb,zdeb) and (xfin,zfin), written with
+7 decimals), Newmark or LDDRK time scheme.
+"""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+
+from .gll import NGLL
+from .mesh import internal_mesh, read_interfaces_file, spline_construction, value_spline
+from .parfile import material_from_row, read_par_file, read_source_file
+from .solver_setup import Source, build_database
+
+
+def _receivers_from_par(par, top_interface):
+    xs_t, zs_t = top_interface
+    t1 = (zs_t[1] - zs_t[0]) / (xs_t[1] - xs_t[0])
+    tn = (zs_t[-1] - zs_t[-2]) / (xs_t[-1] - xs_t[-2])
+    coefs = spline_construction(xs_t, zs_t, t1, tn)
+    nrec = int(par["nrec"])
+    xdeb, zdeb = float(par["xdeb"]), float(par["zdeb"])
+    xfin, zfin = float(par["xfin"]), float(par["zfin"])
+    out = []
+    for irec in range(1, nrec + 1):
+        if nrec > 1:
+            xr = xdeb + float(irec - 1) * (xfin - xdeb) / float(nrec - 1)
+            zr = zdeb + float(irec - 1) * (zfin - zdeb) / float(nrec - 1)
+        else:
+            xr, zr = xdeb, zdeb
+        if par.get("record_at_surface_same_vertical", False):
+            zr = value_spline(xr, xs_t, zs_t, coefs)
+        out.append((round(xr, 7), round(zr, 7)))
+    return out
+
+
+PAR_KEYS = ("NSTEP", "DT", "time_stepping_scheme", "NGNOD", "xmin", "xmax", "nx", "absorbbottom",
+            "absorbright", "absorbtop", "absorbleft", "STACEY_ABSORBING_CONDITIONS", "USER_T0",
+            "anglerec", "nrec", "xdeb", "zdeb", "xfin", "zfin", "record_at_surface_same_vertical",
+            "seismotype", "materials", "regions", "ATTENUATION_VISCOELASTIC", "PML_BOUNDARY_CONDITIONS")
+
+
+def config_from_data_dir(data_dir: str) -> dict:
+    """Parse Par_file, SOURCE and the interfaces file of a DATA/ directory into a plain dict."""
+    par = read_par_file(os.path.join(data_dir, "Par_file"))
+    srcs = read_source_file(os.path.join(data_dir, "SOURCE"))
+    ifile = str(par["interfacesfile"]).strip()
+    cand = [os.path.join(data_dir, ifile), os.path.join(data_dir, os.path.basename(ifile))]
+    ipath = next(p for p in cand if os.path.exists(p))
+    interfaces, nz_layer = read_interfaces_file(ipath)
+    cfg = {k: par[k] for k in PAR_KEYS if k in par}
+    cfg["sources"] = srcs
+    cfg["interfaces"] = [[list(x), list(z)] for (x, z) in interfaces]
+    cfg["nz_layer"] = list(nz_layer)
+    return cfg
+
+
+def database_from_data_dir(data_dir: str, nstep: int | None = None):
+    """Return (Database, config dict) for the example whose DATA/ is ``data_dir``."""
+    cfg = config_from_data_dir(data_dir)
+    return database_from_config(cfg, nstep), cfg
+
+
+def database_from_config(cfg: dict, nstep: int | None = None):
+    """Build the Database from a parsed example configuration."""
+    par = cfg
+    srcs = cfg["sources"]
+    interfaces = [(list(x), list(z)) for (x, z) in cfg["interfaces"]]
+    nz_layer = list(cfg["nz_layer"])
+    absorb = (bool(par["absorbbottom"]), bool(par["absorbright"]), bool(par["absorbtop"]),
+              bool(par["absorbleft"]))
+    mesh = internal_mesh(float(par["xmin"]), float(par["xmax"]), int(par["nx"]), interfaces, nz_layer,
+                         absorb=absorb, ngnod=int(par["NGNOD"]))
+    mats = {m["index"]: m for m in (material_from_row(r) for r in par["materials"])}
+    rho = np.zeros((mesh.nspec, NGLL, NGLL))
+    vp = np.zeros_like(rho)
+    vs = np.zeros_like(rho)
+    for (ix0, ix1, iz0, iz1, imat) in par["regions"]:
+        m = mats[imat]
+        for iz in range(iz0, iz1 + 1):
+            for ix in range(ix0, ix1 + 1):
+                e = (iz - 1) * mesh.nx + (ix - 1)
+                rho[e], vp[e], vs[e] = m["rho"], m["vp"], m["vs"]
+    sources = []
+    for s in srcs:
+        sources.append(Source(x=float(s["xs"]), z=float(s["zs"]), source_type=int(s["source_type"]),
+                              time_function_type=int(s["time_function_type"]), f0=float(s["f0"]),
+                              tshift=float(s["tshift"]), anglesource_deg=float(s["anglesource"]),
+                              Mxx=float(s["Mxx"]), Mzz=float(s["Mzz"]), Mxz=float(s["Mxz"]),
+                              factor=float(s["factor"])))
+    recs = _receivers_from_par(par, interfaces[-1])
+    n = int(par["NSTEP"]) if nstep is None else nstep
+    db = build_database(mesh, rho, vp, vs, sources, recs, n, float(par["DT"]),
+                        stacey=bool(par["STACEY_ABSORBING_CONDITIONS"]), external_model=False,
+                        time_scheme=int(par["time_stepping_scheme"]), user_t0=float(par["USER_T0"]),
+                        anglerec_deg=float(par["anglerec"]))
+    return db

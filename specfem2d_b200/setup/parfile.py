@@ -1,0 +1,92 @@
+"""Reader for the subset of DATA/Par_file, DATA/SOURCE and DATA/STATIONS on the hot path.
+
+Follows the reference's ``key = value`` convention with ``#`` comments
+(src/shared/param_reader.c:98-160, src/shared/read_parameter_file.F90) and the
+material / region tables that follow ``nbmodels`` and ``nbregions``
+(src/shared/read_material_table.f90, src/meshfem2D/read_regions.f90).
+Fortran literals such as ``2.0d-2`` and ``.true.`` are converted.
+"""
+from __future__ import annotations
+
+import re
+
+
+def _fvalue(tok: str):
+    t = tok.strip()
+    tl = t.lower()
+    if tl in (".true.", "true", "t"):
+        return True
+    if tl in (".false.", "false", "f"):
+        return False
+    try:
+        return int(t)
+    except ValueError:
+        pass
+    try:
+        return float(re.sub(r"[dD]", "e", t))
+    except ValueError:
+        return t
+
+
+def read_par_file(path: str) -> dict:
+    """Return {key: value}, plus ``materials`` (list of token lists) and ``regions``."""
+    out: dict = {"materials": [], "regions": []}
+    with open(path) as f:
+        lines = [ln.split("#", 1)[0].rstrip() for ln in f]
+    lines = [ln for ln in lines if ln.strip()]
+    i = 0
+    while i < len(lines):
+        ln = lines[i]
+        if "=" in ln:
+            key, val = ln.split("=", 1)
+            key = key.strip()
+            out[key] = _fvalue(val)
+            if key == "nbmodels":
+                n = int(out[key])
+                out["materials"] = [lines[i + 1 + k].split() for k in range(n)]
+                i += n
+            elif key == "nbregions":
+                n = int(out[key])
+                out["regions"] = [[int(v) for v in lines[i + 1 + k].split()[:5]] for k in range(n)]
+                i += n
+        i += 1
+    return out
+
+
+def read_source_file(path: str) -> list:
+    """Return a list of dicts, one per source block (read_source_file.f90)."""
+    sources = []
+    cur = None
+    with open(path) as f:
+        for ln in f:
+            s = ln.split("#", 1)[0].strip()
+            if not s or "=" not in s:
+                continue
+            k, v = s.split("=", 1)
+            k = k.strip()
+            if k == "source_surf":
+                cur = {}
+                sources.append(cur)
+            if cur is None:
+                cur = {}
+                sources.append(cur)
+            cur[k] = _fvalue(v)
+    return sources
+
+
+def read_stations(path: str) -> list:
+    """STATIONS lines: station network x z elevation burial."""
+    st = []
+    with open(path) as f:
+        for ln in f:
+            p = ln.split()
+            if len(p) >= 4:
+                st.append((p[0], p[1], float(p[2]), float(p[3])))
+    return st
+
+
+def material_from_row(row) -> dict:
+    """Isotropic material row ``n 1 rho vp vs 0 0 Qkappa Qmu ...`` (read_materials.f90:116-140)."""
+    vals = [_fvalue(v) for v in row]
+    return dict(index=int(vals[0]), kind=int(vals[1]), rho=float(vals[2]), vp=float(vals[3]),
+                vs=float(vals[4]), qkappa=float(vals[7]), qmu=float(vals[8]))

@@ -1,0 +1,68 @@
+"""Generate the golden fixtures in this directory from the reference tree.
+
+Run from the repository root, in a container where the reference is mounted:
+
+    python tests/golden/make_golden.py /root/reference
+
+For each pinned example it writes ``<name>.json`` (the parsed Par_file
+subset, SOURCE and interfaces needed to rebuild the run, plus the source and
+receiver locations the reference printed in REF_SEIS/output.log) and
+``<name>_seis.npz`` (the REF_SEIS seismogram values as float64, with the
+first time sample and the time step of the trace).
+"""
+from __future__ import annotations
+
+import json
+import os
+import re
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from specfem2d_b200.setup.from_par_file import config_from_data_dir  # noqa: E402
+
+EXAMPLES = {
+    # name: (example dir, list of (station, component) traces)
+    "tromp2005_kernel": ("EXAMPLES/Tromp2005_kernel", [("S0001", "BXX"), ("S0001", "BXZ")]),
+    "anisotropic_isotropic_model": ("EXAMPLES/anisotropic_isotropic_model", [("S0001", "BXX"), ("S0001", "BXZ")]),
+}
+
+
+def log_locations(path):
+    """(element, xi, gamma) triples printed by locate_source / locate_receivers."""
+    out = []
+    elem = None
+    with open(path) as f:
+        for ln in f:
+            m = re.search(r"in element\s+(\d+)", ln)
+            if m:
+                elem = int(m.group(1))
+            m = re.search(r"at xi,gamma coordinates =\s+(\S+)\s+(\S+)", ln)
+            if m and elem is not None:
+                out.append([elem, float(m.group(1)), float(m.group(2))])
+                elem = None
+    return out
+
+
+def main(ref_root):
+    for name, (rel, traces) in EXAMPLES.items():
+        ex = os.path.join(ref_root, rel)
+        cfg = config_from_data_dir(os.path.join(ex, "DATA"))
+        cfg["log_locations"] = log_locations(os.path.join(ex, "REF_SEIS", "output.log"))
+        with open(os.path.join(HERE, name + ".json"), "w") as f:
+            json.dump(cfg, f, indent=1, default=str)
+        arrs = {}
+        for st, comp in traces:
+            d = np.loadtxt(os.path.join(ex, "REF_SEIS", f"AA.{st}.{comp}.semd"))
+            arrs[f"{st}_{comp}"] = d[:, 1]
+            arrs["t_first"] = np.array(d[0, 0])
+            arrs["t_step"] = np.array(d[1, 0] - d[0, 0])
+        np.savez_compressed(os.path.join(HERE, name + "_seis.npz"), **arrs)
+        print("wrote", name)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

@@ -1,0 +1,64 @@
+"""Pins the setup + CPU oracle against the reference's own golden seismograms.
+
+EXAMPLES/Tromp2005_kernel (elastic, Stacey on three sides, Newmark, force
+source with a first-derivative-of-Gaussian time function) was run by the
+reference xspecfem2D (FP32) to produce REF_SEIS/AA.S0001.BX?.semd.  The
+fixtures in tests/golden were extracted from it by tests/golden/make_golden.py.
+"""
+import numpy as np
+import pytest
+
+from helpers import load_golden, rel_l2
+from specfem2d_b200.setup.from_par_file import database_from_config
+
+
+@pytest.fixture(scope="module")
+def tromp():
+    cfg, seis = load_golden("tromp2005_kernel")
+    db = database_from_config(cfg)
+    return cfg, seis, db
+
+
+def test_setup_matches_reference_log(tromp):
+    cfg, _, db = tromp
+    # locate_source / locate_receivers printed (1-based element, xi, gamma)
+    (se, sxi, sg), (re_, rxi, rg) = cfg["log_locations"]
+    assert db.source_ispec[0] + 1 == se and db.rec_ispec[0] + 1 == re_
+    assert db.src_xi[0] == pytest.approx(sxi, abs=1e-12) and db.src_gamma[0] == pytest.approx(sg, abs=1e-12)
+    assert db.rec_xi[0] == pytest.approx(rxi, abs=1e-12) and db.rec_gamma[0] == pytest.approx(rg, abs=1e-12)
+    # 80 x 32 quads, NGLL = 5 -> (4*80+1) * (4*32+1) points
+    assert db.nspec == 2560 and db.nglob == 321 * 129
+    assert db.t0 == 8.0
+
+
+def test_oracle_fp32_reproduces_ref_seis(tromp):
+    import oracle
+
+    _, seis, db = tromp
+    o = oracle.Oracle(db, 4)
+    out = o.run(db.nstep)
+    assert rel_l2(out[0, :, 0], seis["S0001_BXX"]) < 1e-5
+    assert rel_l2(out[0, :, 1], seis["S0001_BXZ"]) < 1e-5
+    # trace time axis: t = (it-1) * DT - t0
+    assert float(seis["t_first"]) == pytest.approx(-db.t0)
+    assert float(seis["t_step"]) == pytest.approx(db.dt)
+
+
+def test_oracle_fp64_close_to_fp32(tromp):
+    import oracle
+
+    _, seis, db = tromp
+    o = oracle.Oracle(db, 8)
+    out = o.run(db.nstep)
+    # the FP64 run differs from the FP32 reference output by FP32 rounding only
+    assert rel_l2(out[0, :, 0], seis["S0001_BXX"]) < 1e-4
+    assert rel_l2(out[0, :, 1], seis["S0001_BXZ"]) < 1e-4
+
+
+def test_oracle_thread_count_invariant(tromp):
+    import oracle
+
+    _, _, db = tromp
+    a = oracle.Oracle(db, 4).run(200, nthreads=1)
+    b = oracle.Oracle(db, 4).run(200, nthreads=3)
+    assert np.array_equal(a, b)
