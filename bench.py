@@ -1,0 +1,308 @@
+"""Benchmark of the SPECFEM2D time-marching hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload c2_geometry|c1] [--tile-elems T]
+
+A "step" is one Newmark time step of the whole mesh.  The metric is GLL
+point-updates per second (global points x steps / s).  With N > 1 (torchrun,
+one process per GPU) every rank advances its own replica of the workload (the
+shots of a survey are independent), so scaling is weak and `value` sums all
+ranks' point-updates over the slowest rank's time.
+
+`--impl reference` times the CPU restatement of the reference solver (the
+oracle; the Fortran xspecfem2D cannot be built without a Fortran compiler)
+on all host cores, on the same workload, over a bounded number of steps.
+
+Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import pickle
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CACHE = os.path.join("/tmp", "sf2d_bench_cache")
+
+
+def build_workload(name: str, nstep: int):
+    from specfem2d_b200 import configs
+
+    os.makedirs(CACHE, exist_ok=True)
+    path = os.path.join(CACHE, f"{name}_{nstep}.pkl")
+    if os.path.exists(path):
+        with open(path, "rb") as f:
+            return pickle.load(f)
+    if name == "c2_geometry":
+        db = configs.c2_geometry(nstep=nstep)
+    elif name == "c1":
+        db = configs.c1_homogeneous(nstep=nstep)
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    with open(path + ".tmp", "wb") as f:
+        pickle.dump(db, f, protocol=4)
+    os.replace(path + ".tmp", path)
+    return db
+
+
+WORKLOAD_DESC = {
+    "c2_geometry": ("800x320-element (20 km x 8 km, 4,100,481 GLL points) mesh of the coupled "
+                    "acoustic-elastic configuration, run elastic-only: the 1 km top layer is elastic "
+                    "(vp 2000) and Stacey replaces the 20-element CPML; vp 2000->4500 with depth, "
+                    "vs=vp/1.73, Gardner rho, 5% Gaussian random field (corr. 200 m, seed 2), "
+                    "Ricker 8 Hz force, dt 5e-4, 400 receivers"),
+    "c1": "80x60 homogeneous elastic, Stacey L/R/B, free top, Ricker 10 Hz, 20 receivers",
+}
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "50", "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def time_oracle(db, max_steps: int, target_s: float = 15.0, nthreads: int = 0):
+    """Times the CPU oracle (FP32) on a bounded number of steps; returns (steps, seconds, threads)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # noqa: E402  (CPU baseline leg only)
+
+    o = oracle.Oracle(db, 4)
+    t0 = time.perf_counter()
+    o.run(2, nthreads=nthreads)
+    t_step = (time.perf_counter() - t0) / 2
+    n = int(max(2, min(max_steps, math.ceil(target_s / max(t_step, 1e-6)))))
+    t0 = time.perf_counter()
+    o.run(n, nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    threads = nthreads if nthreads > 0 else oracle.max_threads()
+    return n, dt, threads
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    db = build_workload(args.workload, max(args.steps, 8) + args.warmup + 8)
+    n, dt, threads = time_oracle(db, max_steps=max(args.steps, 2), target_s=args.ref_seconds)
+    value = db.nglob * n / dt
+    line = {
+        "metric": "GLL point-updates/s", "value": value, "unit": "point-updates/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": n, "warmup": 2, "ms_per_step": dt / n * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": {"workload": args.workload, "description": WORKLOAD_DESC[args.workload],
+                                        "nspec": db.nspec, "nglob": db.nglob},
+        "cpu_baseline": {"value": value, "unit": "point-updates/s", "cores": threads, "kind": "port",
+                         "sample": f"{n} Newmark steps of the full {db.nspec}-element mesh "
+                                   "(C++ restatement of the reference CPU solver, FP32)"},
+        "e2e": {"value": value, "unit": "point-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=6000)
+    ap.add_argument("--warmup", type=int, default=100)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2_geometry", choices=sorted(WORKLOAD_DESC))
+    ap.add_argument("--tile-elems", type=int, default=64)
+    ap.add_argument("--ref-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist_mod
+
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = dist_mod
+    from specfem2d_b200.configs import algorithmic_bytes_elastic
+    from specfem2d_b200.runtime import ElasticSolver
+
+    K, W = args.steps, args.warmup
+    db = build_workload(args.workload, K + W + 8)
+    solver = ElasticSolver(db, tile_elems=args.tile_elems)
+    info = solver.layout_info()
+    stream = torch.cuda.ExternalStream(solver.stream_handle())
+
+    # warm-up, then the timed region: K steps queued as CUDA graphs on the solver stream
+    solver.enqueue(W)
+    solver.synchronize(600)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    time.sleep(0.3)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    solver.enqueue(K)
+    ev1.record(stream)
+    solver.synchronize(600)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    chunk = 32
+    launches = 2 * K + K // chunk + (1 if K % chunk else 0)
+
+    # kernel-level timing for the roofline (events around each launch, same stream)
+    nk = min(200, max(20, K // 10))
+    k_ms = solver.time_kernels(nk)
+    tile_ms = k_ms[0]
+    st = info
+    nsh = st["nshared"]
+    n_int = db.nglob - nsh
+    # algorithmic bytes of the element kernel per launch: element data + interior points
+    # (u, v, a read+write, rmass) + shared points touched by tiles (u, v, a read, partial write)
+    n_slots = int(np.asarray(solver_slots(db, args.tile_elems)))
+    tile_bytes = 700 * db.nspec + 56 * n_int + 32 * n_slots
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = tile_bytes / (tile_ms * 1e-3) / 1e9
+    step_bytes = algorithmic_bytes_elastic(db.nspec, db.nglob)
+
+    # end to end through the public API with host buffers
+    e2e_solver = ElasticSolver(db, tile_elems=args.tile_elems)
+    zeros = np.zeros((db.nglob, 2), dtype=np.float32)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    e2e_solver.set_fields(zeros, zeros, zeros)
+    seis = e2e_solver.run(K, seismograms=True)
+    d, _, _ = (e2e_solver.get_fields()[0], None, None)
+    t1 = time.perf_counter()
+    e2e_s = t1 - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    h2d = 3 * db.nglob * 8
+    d2h = seis.nbytes + d.nbytes
+    e2e_solver.close()
+
+    value = db.nglob * K * world / (ms * 1e-3)
+    line = {
+        "metric": "GLL point-updates/s", "value": value, "unit": "point-updates/s",
+        "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "description": WORKLOAD_DESC[args.workload],
+                   "nspec": db.nspec, "nglob": db.nglob, "tile_elems": args.tile_elems,
+                   "ntiles": st["ntiles"], "shared_points": nsh,
+                   "l2": "inputs larger than L2 (fields + element data > 126 MB)",
+                   "parallelism": f"replicas x{world}"},
+        "hbm_gbs_step": step_bytes / (ms / K * 1e-3) / 1e9,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "kernel": "k_elastic_tile", "kernel_ms": tile_ms, "shared_kernel_ms": k_ms[1],
+                     "algorithmic_bytes_per_launch": tile_bytes,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
+        "e2e": {"value": db.nglob * K * world / e2e_s, "unit": "point-updates/s",
+                "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        n, dt, threads = time_oracle(db, max_steps=K, target_s=args.ref_seconds)
+        line["cpu_baseline"] = {"value": db.nglob * n / dt, "unit": "point-updates/s", "cores": threads,
+                                "kind": "port",
+                                "sample": f"{n} Newmark steps of the full mesh, C++ restatement of the "
+                                          "reference CPU solver (FP32), all host threads"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def solver_slots(db, tile_elems):
+    from specfem2d_b200.runtime import tiling_stats
+
+    return tiling_stats(db, tile_elems)["n_slots"]
+
+
+if __name__ == "__main__":
+    main()

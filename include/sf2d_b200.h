@@ -1,0 +1,150 @@
+/*
+ * sf2d_b200 -- B200-native (sm_100a) time-marching hot path of SPECFEM2D.
+ *
+ * Plain C ABI: pointers and sizes only, every call returns an int status
+ * (SF2D_OK = 0, negative on error; sf2d_last_error() gives the message).
+ * Nothing here exits the process.  Arrays use the reference solver layout:
+ * per-element GLL arrays are [ispec][j][i] (the memory order of the
+ * Fortran arrays (i,j,ispec)), global vectors [iglob][component]; indices
+ * are 0-based.
+ *
+ * Correspondence with the reference's Fortran->GPU interface
+ * (src/gpu/specfem2D_gpu_cuda_method_stubs.c lists all of them):
+ *   sf2d_elastic_create   <- prepare_constants_device
+ *                            (src/gpu/prepare_mesh_constants_cuda.cu:83),
+ *                            prepare_fields_elastic_device (:527),
+ *                            prepare_stacey_device (:926), plus the source
+ *                            and receiver arrays of prepare_constants_device
+ *   sf2d_set_fields       <- transfer_fields_el_to_device
+ *                            (src/gpu/transfer_fields_cuda.cu:53)
+ *   sf2d_get_fields       <- transfer_fields_el_from_device (:69)
+ *   sf2d_run              <- one call per time step of, in order,
+ *                            update_displacement_cuda
+ *                            (src/gpu/update_displacement_cuda.cu:52),
+ *                            compute_forces_viscoelastic_cuda
+ *                            (src/gpu/compute_forces_viscoelastic_cuda.cu:327),
+ *                            compute_stacey_viscoelastic_cuda
+ *                            (src/gpu/compute_stacey_viscoelastic_cuda.cu:40),
+ *                            compute_add_sources_el_cuda
+ *                            (src/gpu/compute_add_sources_viscoelastic_cuda.cu:46),
+ *                            kernel_3_a_cuda (src/gpu/update_displacement_cuda.cu:221),
+ *                            compute_seismograms_cuda
+ *                            (src/gpu/write_seismograms_cuda.cu:41),
+ *                            fused into one tile-staged kernel per step
+ *   sf2d_get_norm         <- get_norm_elastic_from_device
+ *                            (src/gpu/check_fields_cuda.cu:358)
+ *   sf2d_destroy          <- prepare_cleanup_device
+ *                            (src/gpu/prepare_mesh_constants_cuda.cu:1139)
+ */
+#ifndef SF2D_B200_H
+#define SF2D_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SF2D_OK 0
+#define SF2D_ERR_INVALID (-1)
+#define SF2D_ERR_CUDA (-2)
+#define SF2D_ERR_OOM (-3)
+#define SF2D_ERR_UNSTABLE (-4)
+
+typedef struct sf2d_solver sf2d_solver;
+
+/* Elastic (isotropic) Newmark problem in reference layout. */
+typedef struct {
+  int nspec, nglob;
+  const int *ibool;                          /* nspec*25, 0-based */
+  const float *xix, *xiz, *gammax, *gammaz;  /* nspec*25 */
+  const float *kappastore, *mustore;         /* nspec*25 */
+  const float *rmass_inverse;                /* nglob*2 */
+  const float *hprime, *hprimewgll;          /* 25: [i2*5+i1] = l'_{i1}(xi_{i2}) (times w_{i2}) */
+  const float *wxgll, *wzgll;                /* 5 */
+  const double *centroid_xz;                 /* nspec*2 element centres for tiling, may be NULL */
+  /* Stacey absorbing points, one entry per (edge, GLL point) in the order the
+   * reference visits them (compute_stacey_elastic.f90:116-980) */
+  int nstacey;
+  const int *st_iglob;
+  const float *st_nx, *st_nz, *st_w, *st_rho_vp, *st_rho_vs;
+  /* sources: element, sourcearrays[isrc][j][i][comp], stf[isrc][it] */
+  int nsrc;
+  const int *src_ispec;
+  const float *sourcearrays;
+  const float *stf;
+  /* receivers: element, Lagrange weights hxir[irec][i], hgammar[irec][j] */
+  int nrec;
+  const int *rec_ispec;
+  const double *hxir, *hgammar;
+  double cosrot, sinrot;
+  int seismotype;                            /* 1 displacement, 2 velocity, 3 acceleration */
+  /* time stepping */
+  int nstep;                                 /* length of stf and of the seismogram buffer */
+  float deltat, deltatover2, deltatsquareover2;
+  int tile_elems;                            /* elements per tile, 0 = default (64) */
+} sf2d_elastic_desc;
+
+/* Builds the tiled device layout and uploads everything (fields start at 0). */
+int sf2d_elastic_create(const sf2d_elastic_desc *desc, sf2d_solver **out);
+
+/* Host <-> device copies of the wavefields, nglob*2 floats each in the
+ * original global numbering.  NULL pointers are skipped (set: zero-filled). */
+int sf2d_set_fields(sf2d_solver *s, const float *displ, const float *veloc, const float *accel);
+int sf2d_get_fields(sf2d_solver *s, float *displ, float *veloc, float *accel);
+
+/* Advances nstep time steps on the device.  When `seismograms` is not NULL
+ * the receiver traces of these steps are copied to it (nrec*nstep*2 doubles,
+ * [irec][it][comp], rotated by cosrot/sinrot) before returning.  Returns
+ * SF2D_ERR_UNSTABLE if a displacement became NaN or exceeded 1e25 (the check
+ * of check_stability.F90:95-98), after finishing the steps. */
+int sf2d_run(sf2d_solver *s, int nstep, double *seismograms);
+
+/* Same without a host sync or copy: the steps are queued on the solver's
+ * stream (CUDA graphs of fixed step chunks).  sf2d_synchronize waits (with a
+ * timeout in seconds, <= 0 meaning none) and returns the stability status. */
+int sf2d_enqueue(sf2d_solver *s, int nstep);
+int sf2d_synchronize(sf2d_solver *s, double timeout_s);
+
+/* Copies receiver traces [it0, it0+nstep) already recorded on the device. */
+int sf2d_copy_seismograms(sf2d_solver *s, int it0, int nstep, double *out);
+
+/* Maximum displacement norm over all points (check_stability.F90). */
+int sf2d_get_norm(sf2d_solver *s, float *max_norm);
+
+/* Steps done since creation. */
+int sf2d_step_index(sf2d_solver *s, int *it);
+
+/* The cudaStream_t the solver launches on (as void*). */
+int sf2d_get_stream(sf2d_solver *s, void **stream);
+
+/* Times `nstep` steps launched one kernel at a time with CUDA events around
+ * each launch; writes the average milliseconds per launch of the element
+ * kernel (ms[0]), the shared-point kernel (ms[1]) and their sum per step
+ * (ms[2]).  The steps advance the wavefield like sf2d_run. */
+int sf2d_time_kernels(sf2d_solver *s, int nstep, float *ms);
+
+/* Layout statistics: [ntiles, nshared points, max local points, max elements
+ * per tile, device bytes, dynamic shared memory per CTA, kernel launches per
+ * step, 0]. */
+int sf2d_layout_info(sf2d_solver *s, long long *info8);
+
+int sf2d_destroy(sf2d_solver *s);
+
+const char *sf2d_last_error(void);
+
+/* Host-only diagnostic, no GPU needed: builds the tiling of a mesh and checks
+ * its invariants (one device id per point, local ibool consistent with
+ * ibool, colours conflict-free, shared-point slots complete and in tile
+ * order).  out8 = [ntiles, nshared, max local points, max elements per tile,
+ * max colours, interior points, partial-sum slots, 0].  Returns 0 when every
+ * invariant holds, a negative code naming the first that fails otherwise.
+ * No reference counterpart (the reference assembles with atomics). */
+int sf2d_tiling_stats(int nspec, int nglob, const int *ibool, const double *centroid_xz, int tile_elems,
+                      long long *out8);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

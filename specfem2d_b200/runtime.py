@@ -1,0 +1,248 @@
+"""Python host binding of libsf2d_b200.so (the sm_100a C ABI in include/sf2d_b200.h).
+
+This is the product's host side: it turns a setup Database into the
+reference-layout descriptor the C ABI takes and drives the device time loop.
+There is no CPU fallback: if the CUDA library is missing or fails, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .build import LIB
+
+_f = ctypes.POINTER(ctypes.c_float)
+_d = ctypes.POINTER(ctypes.c_double)
+_i = ctypes.POINTER(ctypes.c_int)
+
+SF2D_OK = 0
+SF2D_ERR_INVALID = -1
+SF2D_ERR_CUDA = -2
+SF2D_ERR_OOM = -3
+SF2D_ERR_UNSTABLE = -4
+
+
+class SF2DError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"sf2d error {code}: {msg}")
+        self.code = code
+
+
+class UnstableError(SF2DError):
+    pass
+
+
+class ElasticDesc(ctypes.Structure):
+    _fields_ = [
+        ("nspec", ctypes.c_int), ("nglob", ctypes.c_int),
+        ("ibool", _i),
+        ("xix", _f), ("xiz", _f), ("gammax", _f), ("gammaz", _f),
+        ("kappastore", _f), ("mustore", _f),
+        ("rmass_inverse", _f),
+        ("hprime", _f), ("hprimewgll", _f), ("wxgll", _f), ("wzgll", _f),
+        ("centroid_xz", _d),
+        ("nstacey", ctypes.c_int), ("st_iglob", _i),
+        ("st_nx", _f), ("st_nz", _f), ("st_w", _f), ("st_rho_vp", _f), ("st_rho_vs", _f),
+        ("nsrc", ctypes.c_int), ("src_ispec", _i), ("sourcearrays", _f), ("stf", _f),
+        ("nrec", ctypes.c_int), ("rec_ispec", _i), ("hxir", _d), ("hgammar", _d),
+        ("cosrot", ctypes.c_double), ("sinrot", ctypes.c_double), ("seismotype", ctypes.c_int),
+        ("nstep", ctypes.c_int),
+        ("deltat", ctypes.c_float), ("deltatover2", ctypes.c_float), ("deltatsquareover2", ctypes.c_float),
+        ("tile_elems", ctypes.c_int),
+    ]
+
+
+_lib = None
+
+
+def load_library(path: str = LIB):
+    """Load the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"CUDA extension not built: {path} (run python -m specfem2d_b200.build)")
+    lib = ctypes.CDLL(path)
+    vp = ctypes.c_void_p
+    sigs = {
+        "sf2d_elastic_create": [ctypes.POINTER(ElasticDesc), ctypes.POINTER(vp)],
+        "sf2d_set_fields": [vp, _f, _f, _f],
+        "sf2d_get_fields": [vp, _f, _f, _f],
+        "sf2d_run": [vp, ctypes.c_int, _d],
+        "sf2d_enqueue": [vp, ctypes.c_int],
+        "sf2d_synchronize": [vp, ctypes.c_double],
+        "sf2d_copy_seismograms": [vp, ctypes.c_int, ctypes.c_int, _d],
+        "sf2d_get_norm": [vp, _f],
+        "sf2d_step_index": [vp, _i],
+        "sf2d_get_stream": [vp, ctypes.POINTER(vp)],
+        "sf2d_time_kernels": [vp, ctypes.c_int, _f],
+        "sf2d_layout_info": [vp, ctypes.POINTER(ctypes.c_longlong)],
+        "sf2d_destroy": [vp],
+    }
+    for name, args in sigs.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = ctypes.c_int
+    lib.sf2d_tiling_stats.argtypes = [ctypes.c_int, ctypes.c_int, _i, _d, ctypes.c_int,
+                                      ctypes.POINTER(ctypes.c_longlong)]
+    lib.sf2d_tiling_stats.restype = ctypes.c_int
+    lib.sf2d_last_error.restype = ctypes.c_char_p
+    lib.sf2d_last_error.argtypes = []
+    _lib = lib
+    return lib
+
+
+def _check(rc):
+    if rc == SF2D_OK:
+        return
+    msg = load_library().sf2d_last_error().decode(errors="replace")
+    if rc == SF2D_ERR_UNSTABLE:
+        raise UnstableError(rc, msg)
+    raise SF2DError(rc, msg)
+
+
+def element_centroids(db) -> np.ndarray:
+    """Element centres (mean of the four corner GLL points) used to order tiles."""
+    ib = db.ibool
+    c = db.coord[ib[:, [0, 0, 4, 4], [0, 4, 0, 4]]]  # (nspec, 4, 2)
+    return np.ascontiguousarray(c.mean(axis=1))
+
+
+def tiling_stats(db, tile_elems: int = 64):
+    """Host-only tiling check (no GPU): returns the statistics dict or raises."""
+    lib = load_library()
+    ib = np.ascontiguousarray(db.ibool, dtype=np.int32)
+    cen = element_centroids(db)
+    out = (ctypes.c_longlong * 8)()
+    rc = lib.sf2d_tiling_stats(db.nspec, db.nglob, ib.ctypes.data_as(_i), cen.ctypes.data_as(_d),
+                               tile_elems, out)
+    if rc != 0:
+        raise SF2DError(rc, "tiling invariant violated")
+    keys = ["ntiles", "nshared", "max_local", "max_elems", "max_colours", "n_interior", "n_slots", "reserved"]
+    return dict(zip(keys, [int(x) for x in out]))
+
+
+class ElasticSolver:
+    """Device-resident isotropic elastic Newmark solver for one Database."""
+
+    def __init__(self, db, tile_elems: int = 64, seismotype: int = 1):
+        lib = load_library()
+        keep = []
+
+        def f(a):
+            arr = np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+            keep.append(arr)
+            return arr.ctypes.data_as(_f)
+
+        def dd(a):
+            arr = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+            keep.append(arr)
+            return arr.ctypes.data_as(_d)
+
+        def i(a):
+            arr = np.ascontiguousarray(np.asarray(a, dtype=np.int32))
+            keep.append(arr)
+            return arr.ctypes.data_as(_i)
+
+        g = db.gll
+        d = ElasticDesc()
+        d.nspec, d.nglob = db.nspec, db.nglob
+        d.ibool = i(db.ibool)
+        d.xix, d.xiz, d.gammax, d.gammaz = f(db.xix), f(db.xiz), f(db.gammax), f(db.gammaz)
+        d.kappastore, d.mustore = f(db.kappastore), f(db.mustore)
+        d.rmass_inverse = f(db.rmass_inverse_elastic)
+        d.hprime, d.hprimewgll, d.wxgll, d.wzgll = f(g.hprime), f(g.hprimewgll), f(g.wxgll), f(g.wzgll)
+        d.centroid_xz = dd(element_centroids(db))
+        d.nstacey = len(db.stacey_iglob)
+        d.st_iglob = i(db.stacey_iglob)
+        d.st_nx, d.st_nz, d.st_w = f(db.stacey_nx), f(db.stacey_nz), f(db.stacey_weight)
+        d.st_rho_vp, d.st_rho_vs = f(db.stacey_rho_vp), f(db.stacey_rho_vs)
+        d.nsrc = len(db.source_ispec)
+        d.src_ispec = i(db.source_ispec)
+        d.sourcearrays = f(db.sourcearrays)
+        d.stf = f(db.stf[:, :, 0])
+        d.nrec = len(db.rec_ispec)
+        d.rec_ispec = i(db.rec_ispec)
+        d.hxir, d.hgammar = dd(db.hxir), dd(db.hgammar)
+        d.cosrot, d.sinrot = float(db.cosrot), float(db.sinrot)
+        d.seismotype = seismotype
+        d.nstep = db.nstep
+        d.deltat, d.deltatover2, d.deltatsquareover2 = (float(db.deltat), float(db.deltatover2),
+                                                        float(db.deltatsquareover2))
+        d.tile_elems = tile_elems
+        h = ctypes.c_void_p()
+        _check(lib.sf2d_elastic_create(ctypes.byref(d), ctypes.byref(h)))
+        self._h = h
+        self._lib = lib
+        self.nglob = db.nglob
+        self.nrec = d.nrec
+        self.nstep_total = db.nstep
+        del keep
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.sf2d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_fields(self, displ=None, veloc=None, accel=None):
+        arrs = [None if x is None else np.ascontiguousarray(x, dtype=np.float32) for x in (displ, veloc, accel)]
+        ptrs = [None if x is None else x.ctypes.data_as(_f) for x in arrs]
+        _check(self._lib.sf2d_set_fields(self._h, *ptrs))
+
+    def get_fields(self):
+        out = [np.empty((self.nglob, 2), dtype=np.float32) for _ in range(3)]
+        _check(self._lib.sf2d_get_fields(self._h, *[x.ctypes.data_as(_f) for x in out]))
+        return out
+
+    def run(self, nstep: int, seismograms: bool = True):
+        """Advance nstep steps; returns seismograms (nrec, nstep, 2) float64 or None."""
+        seis = np.zeros((self.nrec, nstep, 2), dtype=np.float64) if seismograms else None
+        _check(self._lib.sf2d_run(self._h, nstep, None if seis is None else seis.ctypes.data_as(_d)))
+        return seis
+
+    def enqueue(self, nstep: int):
+        _check(self._lib.sf2d_enqueue(self._h, nstep))
+
+    def synchronize(self, timeout_s: float = 0.0):
+        _check(self._lib.sf2d_synchronize(self._h, float(timeout_s)))
+
+    def copy_seismograms(self, it0: int, nstep: int, out=None):
+        if out is None:
+            out = np.zeros((self.nrec, nstep, 2), dtype=np.float64)
+        _check(self._lib.sf2d_copy_seismograms(self._h, it0, nstep, out.ctypes.data_as(_d)))
+        return out
+
+    def max_norm(self) -> float:
+        v = ctypes.c_float()
+        _check(self._lib.sf2d_get_norm(self._h, ctypes.byref(v)))
+        return float(v.value)
+
+    def step_index(self) -> int:
+        v = ctypes.c_int()
+        _check(self._lib.sf2d_step_index(self._h, ctypes.byref(v)))
+        return int(v.value)
+
+    def stream_handle(self) -> int:
+        v = ctypes.c_void_p()
+        _check(self._lib.sf2d_get_stream(self._h, ctypes.byref(v)))
+        return int(v.value or 0)
+
+    def time_kernels(self, nstep: int):
+        ms = (ctypes.c_float * 3)()
+        _check(self._lib.sf2d_time_kernels(self._h, nstep, ms))
+        return [float(x) for x in ms]
+
+    def layout_info(self):
+        v = (ctypes.c_longlong * 8)()
+        _check(self._lib.sf2d_layout_info(self._h, v))
+        keys = ["ntiles", "nshared", "max_local", "max_elems", "device_bytes", "smem_bytes",
+                "launches_per_step", "reserved"]
+        return dict(zip(keys, [int(x) for x in v]))

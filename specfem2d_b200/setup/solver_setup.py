@@ -253,12 +253,41 @@ def mass_matrix_elastic(ibool, nglob, geo, mat, gll: GLL, stacey_pts, newmark: b
     return np.stack([f32(1.0) / mx, f32(1.0) / mz], axis=1).astype(f32)
 
 
-def _locate(mesh: Mesh, ibool, coord, gll: GLL, x_t: float, z_t: float, iterate: bool = True):
+class _PointLocator:
+    """Nearest-GLL-point search with the reference's tie rule.
+
+    The reference scans (ispec, j, i) in order and keeps the first strict
+    minimum of the squared distance (locate_receivers.F90:150-170).  A k-d
+    tree finds the nearest global points; among the element-local
+    occurrences of all points at that exact distance the first in scan order
+    wins, which is the same answer.
+    """
+
+    def __init__(self, ibool, coord):
+        from scipy.spatial import cKDTree
+
+        self.ibool = ibool
+        self.coord = coord
+        self.tree = cKDTree(coord)
+        flat = ibool.ravel()
+        first = np.full(coord.shape[0], flat.size, dtype=np.int64)
+        np.minimum.at(first, flat, np.arange(flat.size))
+        self.first = first
+
+    def nearest_flat(self, x_t, z_t):
+        k = min(16, self.coord.shape[0])
+        _, idx = self.tree.query([x_t, z_t], k=k)
+        idx = np.atleast_1d(idx)
+        d2 = (x_t - self.coord[idx, 0]) ** 2 + (z_t - self.coord[idx, 1]) ** 2
+        best = idx[d2 == d2.min()]
+        return int(self.first[best].min())
+
+
+def _locate(mesh: Mesh, ibool, coord, gll: GLL, x_t: float, z_t: float, iterate: bool = True, locator=None):
     """Shared body of locate_source / locate_receivers: returns (ispec, xi, gamma, x, z)."""
-    xs = coord[ibool.ravel(), 0]
-    zs = coord[ibool.ravel(), 1]
-    d2 = (x_t - xs) ** 2 + (z_t - zs) ** 2
-    k = int(np.argmin(d2))  # first strict minimum in (ispec, j, i) order
+    if locator is None:
+        locator = _PointLocator(ibool, coord)
+    k = locator.nearest_flat(x_t, z_t)
     ispec0 = k // (NGLL * NGLL)
     ix0 = k % NGLL
     iz0 = (k // NGLL) % NGLL
@@ -362,8 +391,9 @@ def build_database(mesh: Mesh, rho, vp, vs, sources, receivers_xz, nstep: int, d
     t0 = compute_t0(sources, user_t0)
     nstage = 1 if time_scheme == 1 else 6
     src_ispec, src_arr, src_stf, sxi, sgam = [], [], [], [], []
+    locator = _PointLocator(ibool, coord)
     for s in sources:
-        e, xi, gamma, _, _ = _locate(mesh, ibool, coord, gll, s.x, s.z, iterate=True)
+        e, xi, gamma, _, _ = _locate(mesh, ibool, coord, gll, s.x, s.z, iterate=True, locator=locator)
         hx, hpx = lagrange_any(xi, gll.xigll)
         hg, hpg = lagrange_any(gamma, gll.zigll)
         arr = np.zeros((NGLL, NGLL, 2), dtype=f32)
@@ -396,7 +426,7 @@ def build_database(mesh: Mesh, rho, vp, vs, sources, receivers_xz, nstep: int, d
         sgam.append(gamma)
     rec_ispec, rxi, rgam, hxr, hgr, rxx, rzz = [], [], [], [], [], [], []
     for (xr, zr) in receivers_xz:
-        e, xi, gamma, x, z = _locate(mesh, ibool, coord, gll, xr, zr, iterate=True)
+        e, xi, gamma, x, z = _locate(mesh, ibool, coord, gll, xr, zr, iterate=True, locator=locator)
         hx, _ = lagrange_any(xi, gll.xigll)
         hg, _ = lagrange_any(gamma, gll.zigll)
         rec_ispec.append(e); rxi.append(xi); rgam.append(gamma)

@@ -1,0 +1,107 @@
+"""Parity of the sm_100a tile-staged elastic Newmark path against the CPU oracle.
+
+Tolerance: seismograms and wavefields within 1e-5 relative L2 of the FP32
+oracle (the FP32 restatement of the reference CPU solver), as the path's
+contract states for floating point.
+"""
+import numpy as np
+import pytest
+
+from helpers import load_golden, rel_l2
+from specfem2d_b200.setup.from_par_file import database_from_config
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def tromp():
+    cfg, seis = load_golden("tromp2005_kernel")
+    return database_from_config(cfg), seis
+
+
+@pytest.fixture(scope="module")
+def tromp_oracle(tromp):
+    import oracle
+
+    db, _ = tromp
+    o = oracle.Oracle(db, 4)
+    s = o.run(db.nstep)
+    return s, o.displ.copy(), o.veloc.copy(), o.accel.copy()
+
+
+def test_tromp_seismograms_match_oracle_and_golden(tromp, tromp_oracle):
+    from specfem2d_b200.runtime import ElasticSolver
+
+    db, golden = tromp
+    s_or = tromp_oracle[0]
+    sol = ElasticSolver(db)
+    s = sol.run(db.nstep)
+    for c in range(2):
+        assert rel_l2(s[0, :, c], s_or[0, :, c]) < TOL
+    assert rel_l2(s[0, :, 0], golden["S0001_BXX"]) < TOL
+    assert rel_l2(s[0, :, 1], golden["S0001_BXZ"]) < TOL
+    d, v, a = sol.get_fields()
+    assert rel_l2(d, tromp_oracle[1]) < TOL
+    assert rel_l2(v, tromp_oracle[2]) < TOL
+    assert rel_l2(a, tromp_oracle[3]) < 1e-4  # acceleration carries more cancellation
+
+
+@pytest.mark.parametrize("tile_elems", [8, 25, 64, 128])
+def test_tile_size_invariance(tromp, tile_elems):
+    import oracle
+    from specfem2d_b200.runtime import ElasticSolver
+
+    db, _ = tromp
+    o = oracle.Oracle(db, 4)
+    ref = o.run(600)
+    sol = ElasticSolver(db, tile_elems=tile_elems)
+    s = sol.run(600)
+    assert rel_l2(s, ref) < TOL
+    d, _, _ = sol.get_fields()
+    assert rel_l2(d, o.displ) < TOL
+
+
+def test_bitwise_deterministic_and_chunking(tromp):
+    from specfem2d_b200.runtime import ElasticSolver
+
+    db, _ = tromp
+    a = ElasticSolver(db).run(500)
+    sol = ElasticSolver(db)
+    b1 = sol.run(123)
+    b2 = sol.run(377)
+    b = np.concatenate([b1, b2], axis=1)
+    assert np.array_equal(a, b)
+
+
+def test_set_get_fields_roundtrip_and_restart(tromp):
+    import oracle
+    from specfem2d_b200.runtime import ElasticSolver
+
+    db, _ = tromp
+    rng = np.random.default_rng(0)
+    d0 = (rng.standard_normal((db.nglob, 2)) * 1e-6).astype(np.float32)
+    sol = ElasticSolver(db)
+    sol.set_fields(d0, None, None)
+    d, v, a = sol.get_fields()
+    assert np.array_equal(d, d0) and not v.any() and not a.any()
+    # restart from a random displacement: compare with the oracle
+    o = oracle.Oracle(db, 4)
+    o.displ[:] = d0
+    ref = o.run(100)
+    s = sol.run(100)
+    assert rel_l2(s, ref) < TOL
+    d, _, _ = sol.get_fields()
+    assert rel_l2(d, o.displ) < TOL
+
+
+def test_unstable_is_reported(tromp):
+    from specfem2d_b200.runtime import ElasticSolver, UnstableError
+
+    db, _ = tromp
+    sol = ElasticSolver(db)
+    bad = np.zeros((db.nglob, 2), dtype=np.float32)
+    bad[db.nglob // 2] = np.nan
+    sol.set_fields(bad, None, None)
+    with pytest.raises(UnstableError):
+        sol.run(3)
