@@ -59,7 +59,9 @@ typedef struct {
   int nspec, nglob;
   const int *ibool;                          /* nspec*25, 0-based */
   const float *xix, *xiz, *gammax, *gammaz;  /* nspec*25 */
-  const float *kappastore, *mustore;         /* nspec*25 */
+  const float *lambdastore, *mustore;        /* nspec*25: lambda = rho*cp*cp - 2*mu with
+                                                cp = rho_vpstore/rhostore, in FP32
+                                                (compute_forces_viscoelastic.F90:286-294) */
   const float *rmass_inverse;                /* nglob*2 */
   const float *hprime, *hprimewgll;          /* 25: [i2*5+i1] = l'_{i1}(xi_{i2}) (times w_{i2}) */
   const float *wxgll, *wzgll;                /* 5 */

@@ -8,7 +8,8 @@
 //      (compute_stacey_elastic.f90:160-335, compute_add_sources_viscoelastic.f90)
 //      by one thread in reference order;
 //   3. per GLL point: gradient through hprime, Jacobian mapping, isotropic
-//      stress with lambda = kappa - mu, weak-form terms
+//      stress (lambda and mu as compute_forces_viscoelastic.F90:286-294 forms
+//      them), weak-form terms
 //      (compute_forces_viscoelastic.F90:184-675);
 //   4. weighted transpose contraction with hprimewgll (:760-782);
 //   5. assembly into the shared-memory accumulator colour by colour
@@ -41,7 +42,7 @@ struct Params {
   const TileInfo *tiles;
   const uint16_t *lib;
   const float4 *geo;   // xix, xiz, gammax, gammaz per element GLL point (tile slot order)
-  const float2 *mat;   // kappa, mu
+  const float2 *mat;   // lambda, mu (lambda = rho*cp*cp - 2*mu in FP32, as the CPU solver forms it)
   const int *sh_ids;
   float2 *partial;
   const int *shp_off, *shp_slots;
@@ -173,8 +174,8 @@ __global__ void __launch_bounds__(BS) k_elastic_tile(const Params P, int record_
     const float duz_dxl = duz_dxi * xixl + duz_dg * gammaxl;
     const float duz_dzl = duz_dxi * xizl + duz_dg * gammazl;
     const float mul = m2.y;
-    const float lambdal = m2.x - mul;
-    const float lambdaplus2mu = m2.x + mul;
+    const float lambdal = m2.x;
+    const float lambdaplus2mu = lambdal + 2.f * mul;
     const float sxx = lambdaplus2mu * dux_dxl + lambdal * duz_dzl;
     const float szz = lambdaplus2mu * duz_dzl + lambdal * dux_dxl;
     const float sxz = mul * (duz_dxl + dux_dzl);
@@ -390,7 +391,7 @@ extern "C" int sf2d_elastic_create(const sf2d_elastic_desc *d, sf2d_solver **out
   if (!d || !out) return fail(SF2D_ERR_INVALID, "null argument");
   *out = nullptr;
   if (d->nspec <= 0 || d->nglob <= 0 || !d->ibool || !d->xix || !d->xiz || !d->gammax || !d->gammaz ||
-      !d->kappastore || !d->mustore || !d->rmass_inverse || !d->hprime || !d->hprimewgll || !d->wxgll ||
+      !d->lambdastore || !d->mustore || !d->rmass_inverse || !d->hprime || !d->hprimewgll || !d->wxgll ||
       !d->wzgll)
     return fail(SF2D_ERR_INVALID, "missing mesh arrays");
   if (d->nstacey < 0 || d->nsrc < 0 || d->nrec < 0 || d->nstep < 0)
@@ -424,7 +425,7 @@ extern "C" int sf2d_elastic_create(const sf2d_elastic_desc *d, sf2d_solver **out
     const size_t src = static_cast<size_t>(T.elem_order[s]) * NGLL2;
     for (int q = 0; q < NGLL2; ++q) {
       geo[s * NGLL2 + q] = make_float4(d->xix[src + q], d->xiz[src + q], d->gammax[src + q], d->gammaz[src + q]);
-      mat[s * NGLL2 + q] = make_float2(d->kappastore[src + q], d->mustore[src + q]);
+      mat[s * NGLL2 + q] = make_float2(d->lambdastore[src + q], d->mustore[src + q]);
     }
   }
   std::vector<float2> rmass(d->nglob);

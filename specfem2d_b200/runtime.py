@@ -39,7 +39,7 @@ class ElasticDesc(ctypes.Structure):
         ("nspec", ctypes.c_int), ("nglob", ctypes.c_int),
         ("ibool", _i),
         ("xix", _f), ("xiz", _f), ("gammax", _f), ("gammaz", _f),
-        ("kappastore", _f), ("mustore", _f),
+        ("lambdastore", _f), ("mustore", _f),
         ("rmass_inverse", _f),
         ("hprime", _f), ("hprimewgll", _f), ("wxgll", _f), ("wzgll", _f),
         ("centroid_xz", _d),
@@ -103,6 +103,15 @@ def _check(rc):
     raise SF2DError(rc, msg)
 
 
+def lambda_store(db) -> np.ndarray:
+    """lambda per GLL point formed in FP32 exactly as the CPU solver does:
+    cpl = rho_vp / rho, lambda = rho*cpl*cpl - 2*mu (compute_forces_viscoelastic.F90:286-294)."""
+    f32 = np.float32
+    rho = db.rhostore.astype(f32)
+    cpl = (db.rho_vpstore.astype(f32) / rho).astype(f32)
+    return ((rho * cpl).astype(f32) * cpl - f32(2.0) * db.mustore.astype(f32)).astype(f32)
+
+
 def element_centroids(db) -> np.ndarray:
     """Element centres (mean of the four corner GLL points) used to order tiles."""
     ib = db.ibool
@@ -151,7 +160,7 @@ class ElasticSolver:
         d.nspec, d.nglob = db.nspec, db.nglob
         d.ibool = i(db.ibool)
         d.xix, d.xiz, d.gammax, d.gammaz = f(db.xix), f(db.xiz), f(db.gammax), f(db.gammaz)
-        d.kappastore, d.mustore = f(db.kappastore), f(db.mustore)
+        d.lambdastore, d.mustore = f(lambda_store(db)), f(db.mustore)
         d.rmass_inverse = f(db.rmass_inverse_elastic)
         d.hprime, d.hprimewgll, d.wxgll, d.wzgll = f(g.hprime), f(g.hprimewgll), f(g.wxgll), f(g.wzgll)
         d.centroid_xz = dd(element_centroids(db))

