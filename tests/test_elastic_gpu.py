@@ -63,10 +63,11 @@ def test_tile_size_invariance(tromp, tile_elems):
     from specfem2d_b200.runtime import ElasticSolver
 
     db, _ = tromp
+    # the P wave reaches the receiver (100 km away) after about 1250 steps
     o = oracle.Oracle(db, 4)
-    ref = o.run(600)
+    ref = o.run(1500)
     sol = ElasticSolver(db, tile_elems=tile_elems)
-    s = sol.run(600)
+    s = sol.run(1500)
     assert rel_l2(s, ref) < TOL
     d, v, _ = sol.get_fields()
     assert rel_l2(d, o.displ) < TOL
