@@ -165,6 +165,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2_geometry", choices=sorted(WORKLOAD_DESC))
     ap.add_argument("--tile-elems", type=int, default=64)
+    ap.add_argument("--threads", type=int, default=256)
+    ap.add_argument("--autotune", action="store_true", help="pick tile size and threads per CTA first")
     ap.add_argument("--ref-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
@@ -194,7 +196,12 @@ def main():
 
     K, W = args.steps, args.warmup
     db = build_workload(args.workload, K + W + 8)
-    solver = ElasticSolver(db, tile_elems=args.tile_elems)
+    tune = None
+    if args.autotune:
+        from specfem2d_b200.autotune import autotune_elastic
+
+        (args.tile_elems, args.threads), tune = autotune_elastic(db, tiles=(48, 64, 96), threads=(256, 512))
+    solver = ElasticSolver(db, tile_elems=args.tile_elems, threads_per_block=args.threads)
     info = solver.layout_info()
     stream = torch.cuda.ExternalStream(solver.stream_handle())
 
@@ -249,7 +256,7 @@ def main():
     if args.no_e2e:
         e2e_solver = None
     else:
-        e2e_solver = ElasticSolver(db, tile_elems=args.tile_elems)
+        e2e_solver = ElasticSolver(db, tile_elems=args.tile_elems, threads_per_block=args.threads)
     zeros = np.zeros((db.nglob, 2), dtype=np.float32)
     torch.cuda.synchronize()
     if dist:
@@ -277,6 +284,7 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": args.workload, "description": WORKLOAD_DESC[args.workload],
                    "nspec": db.nspec, "nglob": db.nglob, "tile_elems": args.tile_elems,
+                   "threads_per_cta": args.threads, "autotuned": bool(tune),
                    "ntiles": st["ntiles"], "shared_points": nsh,
                    "l2": "inputs larger than L2 (fields + element data > 126 MB)",
                    "parallelism": f"replicas x{world}"},

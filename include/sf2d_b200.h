@@ -86,6 +86,7 @@ typedef struct {
   int nstep;                                 /* length of stf and of the seismogram buffer */
   float deltat, deltatover2, deltatsquareover2;
   int tile_elems;                            /* elements per tile, 0 = default (64) */
+  int threads_per_block;                     /* 128, 256 or 512; 0 = default (256) */
 } sf2d_elastic_desc;
 
 /* Builds the tiled device layout and uploads everything (fields start at 0). */
@@ -128,8 +129,7 @@ int sf2d_get_stream(sf2d_solver *s, void **stream);
 int sf2d_time_kernels(sf2d_solver *s, int nstep, float *ms);
 
 /* Layout statistics: [ntiles, nshared points, max local points, max elements
- * per tile, device bytes, dynamic shared memory per CTA, kernel launches per
- * step, 0]. */
+ * per tile, device bytes, dynamic shared memory per CTA, threads per CTA, 0]. */
 int sf2d_layout_info(sf2d_solver *s, long long *info8);
 
 int sf2d_destroy(sf2d_solver *s);

@@ -84,17 +84,43 @@ __device__ __forceinline__ void record_receiver(const Params &P, int r, int step
   out[1] = -P.sinrot * vx + P.cosrot * vz;
 }
 
-__global__ void __launch_bounds__(BS) k_elastic_tile(const Params P, int record_prev) {
+__device__ __forceinline__ unsigned smem_addr(const void *p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void cp_async8(void *s, const void *g) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_addr(s)), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *s, const void *g) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(s)), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Shared-memory layout of one tile (sizes from the largest tile):
+//   s_geo  float4[max_q]  xix, xiz, gammax, gammaz; overwritten by the weak-form terms
+//   s_mat  float2[max_q]  lambda, mu
+//   s_u, s_v, s_acc float2[max_local]  (old u, v, a -> predicted u, v and the accumulator)
+//   s_h    float[64]      hprime, hprimewgll, wxgll, wzgll
+//   s_lib  uint16[max_q rounded to 8]
+__host__ __device__ inline size_t tile_smem_bytes(int max_q, int max_local) {
+  return static_cast<size_t>(max_q) * (sizeof(float4) + sizeof(float2)) +
+         static_cast<size_t>(max_local) * 3 * sizeof(float2) + 64 * sizeof(float) +
+         static_cast<size_t>((max_q + 7) / 8 * 8) * sizeof(uint16_t);
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_prev) {
   extern __shared__ __align__(16) unsigned char smem[];
   const TileInfo &ti = P.tiles[blockIdx.x];
   const int tid = threadIdx.x;
   const int n_int = ti.n_int;
-  const int nl = n_int + ti.n_sh;
+  const int n_sh = ti.n_sh;
+  const int nl = n_int + n_sh;
   const int nq = ti.nelem * 25;
   const int ebase = ti.elem_base * 25;
-  float4 *s_tmp = reinterpret_cast<float4 *>(smem);
-  float2 *s_con = reinterpret_cast<float2 *>(s_tmp + P.max_q);
-  float2 *s_u = s_con + P.max_q;
+  const int int_begin = ti.int_begin;
+  float4 *s_geo = reinterpret_cast<float4 *>(smem);
+  float2 *s_mat = reinterpret_cast<float2 *>(s_geo + P.max_q);
+  float2 *s_u = s_mat + P.max_q;
   float2 *s_v = s_u + P.max_local;
   float2 *s_acc = s_v + P.max_local;
   float *s_h = reinterpret_cast<float *>(s_acc + P.max_local);
@@ -103,13 +129,38 @@ __global__ void __launch_bounds__(BS) k_elastic_tile(const Params P, int record_
   const int step = *P.d_step;
   // receivers of the previous step read the old fields before any write
   if (record_prev && tid < ti.rec_n) record_receiver(P, ti.rec_off + tid, step - 1);
-  if (tid < 60) s_h[tid] = P.hconst[tid];
 
+  // 1. every load of the tile is issued at once, straight into shared memory
+  {
+    const uint4 *glib = reinterpret_cast<const uint4 *>(P.lib + ti.lib_off);
+    const int nlib16 = (nq + 7) / 8;
+    for (int k = tid; k < nlib16; k += NT) cp_async16(s_lib + 8 * k, glib + k);
+    for (int f = tid; f < nq; f += NT) {
+      cp_async16(s_geo + f, P.geo + ebase + f);
+      cp_async8(s_mat + f, P.mat + ebase + f);
+    }
+    for (int l = tid; l < n_int; l += NT) {
+      const int g = int_begin + l;
+      cp_async8(s_u + l, P.u + g);
+      cp_async8(s_v + l, P.v + g);
+      cp_async8(s_acc + l, P.a + g);
+    }
+    for (int k = tid; k < n_sh; k += NT) {
+      const int g = P.sh_ids[ti.sh_off + k];
+      cp_async8(s_u + n_int + k, P.u + g);
+      cp_async8(s_v + n_int + k, P.v + g);
+      cp_async8(s_acc + n_int + k, P.a + g);
+    }
+    if (tid < 60) s_h[tid] = P.hconst[tid];
+    cp_async_wait_all();
+  }
+  __syncthreads();
+
+  // 2. Newmark predictor in place
   const float dt = P.dt, dto2 = P.dto2, dt2o2 = P.dt2o2;
-  for (int l = tid; l < nl; l += BS) {
-    const int g = l < n_int ? ti.int_begin + l : P.sh_ids[ti.sh_off + l - n_int];
-    float2 u = P.u[g], v = P.v[g];
-    const float2 a = P.a[g];
+  for (int l = tid; l < nl; l += NT) {
+    float2 u = s_u[l], v = s_v[l];
+    const float2 a = s_acc[l];
     u.x = u.x + dt * v.x + dt2o2 * a.x;
     u.y = u.y + dt * v.y + dt2o2 * a.y;
     v.x = v.x + dto2 * a.x;
@@ -118,9 +169,9 @@ __global__ void __launch_bounds__(BS) k_elastic_tile(const Params P, int record_
     s_v[l] = v;
     s_acc[l] = make_float2(0.f, 0.f);
   }
-  for (int k = tid; k < nq; k += BS) s_lib[k] = P.lib[ebase + k];
   __syncthreads();
 
+  // 3. boundary terms and sources in reference order, one thread (overlaps pass 1)
   if (tid == 0) {
     for (int p = ti.st_off; p < ti.st_off + ti.st_n; ++p) {
       const int l = P.st_local[p];
@@ -146,8 +197,8 @@ __global__ void __launch_bounds__(BS) k_elastic_tile(const Params P, int record_
     }
   }
 
-  // element pass 1: gradient, stress, weak-form terms
-  for (int f = tid; f < nq; f += BS) {
+  // 4. element pass 1: gradient, stress, weak-form terms (written over the geometry)
+  for (int f = tid; f < nq; f += NT) {
     const int e = f / 25;
     const int q = f - 25 * e;
     const int j = q / 5;
@@ -165,8 +216,8 @@ __global__ void __launch_bounds__(BS) k_elastic_tile(const Params P, int record_
       dux_dg += c.x * hz;
       duz_dg += c.y * hz;
     }
-    const float4 g4 = P.geo[ebase + f];
-    const float2 m2 = P.mat[ebase + f];
+    const float4 g4 = s_geo[f];
+    const float2 m2 = s_mat[f];
     const float xixl = g4.x, xizl = g4.y, gammaxl = g4.z, gammazl = g4.w;
     const float jacobianl = 1.f / (xixl * gammazl - gammaxl * xizl);
     const float dux_dxl = dux_dxi * xixl + dux_dg * gammaxl;
@@ -179,57 +230,51 @@ __global__ void __launch_bounds__(BS) k_elastic_tile(const Params P, int record_
     const float sxx = lambdaplus2mu * dux_dxl + lambdal * duz_dzl;
     const float szz = lambdaplus2mu * duz_dzl + lambdal * dux_dxl;
     const float sxz = mul * (duz_dxl + dux_dzl);
-    s_tmp[f] = make_float4(jacobianl * (sxx * xixl + sxz * xizl), jacobianl * (sxz * xixl + szz * xizl),
+    s_geo[f] = make_float4(jacobianl * (sxx * xixl + sxz * xizl), jacobianl * (sxz * xixl + szz * xizl),
                            jacobianl * (sxx * gammaxl + sxz * gammazl), jacobianl * (sxz * gammaxl + szz * gammazl));
   }
   __syncthreads();
 
-  // element pass 2: weighted transpose contraction
-  for (int f = tid; f < nq; f += BS) {
-    const int e = f / 25;
-    const int q = f - 25 * e;
-    const int j = q / 5;
-    const int i = q - 5 * j;
-    const float4 *te = s_tmp + 25 * e;
-    float tx1 = 0.f, tz1 = 0.f, tx2 = 0.f, tz2 = 0.f;
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-      const float4 r = te[5 * j + k];
-      const float w1 = s_h[25 + 5 * k + i];
-      tx1 += r.x * w1;
-      tz1 += r.y * w1;
-      const float4 c = te[5 * k + i];
-      const float w2 = s_h[25 + 5 * k + j];
-      tx2 += c.z * w2;
-      tz2 += c.w * w2;
-    }
-    const float wz = s_h[55 + j], wx = s_h[50 + i];
-    s_con[f] = make_float2(wz * tx1 + wx * tx2, wz * tz1 + wx * tz2);
-  }
-  __syncthreads();
-
-  // assembly, one colour at a time
+  // 5. weighted transpose contraction assembled straight into the accumulator,
+  //    one colour at a time (elements of a colour share no point)
   int cb = 0;
   for (int c = 0; c < ti.ncol; ++c) {
     const int ce = ti.col_end[c] * 25;
-    for (int f = cb + tid; f < ce; f += BS) {
+    for (int f = cb + tid; f < ce; f += NT) {
+      const int e = f / 25;
+      const int q = f - 25 * e;
+      const int j = q / 5;
+      const int i = q - 5 * j;
+      const float4 *te = s_geo + 25 * e;
+      float tx1 = 0.f, tz1 = 0.f, tx2 = 0.f, tz2 = 0.f;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        const float4 r = te[5 * j + k];
+        const float w1 = s_h[25 + 5 * k + i];
+        tx1 += r.x * w1;
+        tz1 += r.y * w1;
+        const float4 cc = te[5 * k + i];
+        const float w2 = s_h[25 + 5 * k + j];
+        tx2 += cc.z * w2;
+        tz2 += cc.w * w2;
+      }
+      const float wz = s_h[55 + j], wx = s_h[50 + i];
       const int l = s_lib[f];
-      const float2 w = s_con[f];
       float2 acc = s_acc[l];
-      acc.x -= w.x;
-      acc.y -= w.y;
+      acc.x -= wz * tx1 + wx * tx2;
+      acc.y -= wz * tz1 + wx * tz2;
       s_acc[l] = acc;
     }
     cb = ce;
     __syncthreads();
   }
 
-  // mass matrix, corrector, write-back
+  // 6. mass matrix, corrector, write-back
   bool bad = false;
-  for (int l = tid; l < nl; l += BS) {
+  for (int l = tid; l < nl; l += NT) {
     const float2 acc = s_acc[l];
     if (l < n_int) {
-      const int g = ti.int_begin + l;
+      const int g = int_begin + l;
       const float2 rm = P.rmass[g];
       const float2 a = make_float2(acc.x * rm.x, acc.y * rm.y);
       float2 v = s_v[l];
@@ -341,6 +386,7 @@ struct sf2d_solver {
   int chunk = 32;
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
+  int nt = 256;  // threads per CTA of the tile kernel
 
   template <typename T_>
   int alloc(T_ **p, size_t count) {
@@ -360,9 +406,16 @@ struct sf2d_solver {
     if (count) SF2D_CUDA(cudaMemcpy(*p, host, count * sizeof(T_), cudaMemcpyHostToDevice));
     return SF2D_OK;
   }
+  void launch_tile(bool record_prev) {
+    const int rp = record_prev ? 1 : 0;
+    switch (nt) {
+      case 128: sf2d::k_elastic_tile<128><<<T.ntiles, 128, smem, stream>>>(P, rp); break;
+      case 512: sf2d::k_elastic_tile<512><<<T.ntiles, 512, smem, stream>>>(P, rp); break;
+      default: sf2d::k_elastic_tile<256><<<T.ntiles, 256, smem, stream>>>(P, rp); break;
+    }
+  }
   int launch_step(bool record_prev) {
-    const int ntiles = T.ntiles;
-    sf2d::k_elastic_tile<<<ntiles, sf2d::BS, smem, stream>>>(P, record_prev ? 1 : 0);
+    launch_tile(record_prev);
     const int nb = std::max(1, (P.nshared + sf2d::BS - 1) / sf2d::BS);
     sf2d::k_elastic_shared<<<nb, sf2d::BS, 0, stream>>>(P);
     return SF2D_OK;
@@ -477,7 +530,6 @@ extern "C" int sf2d_elastic_create(const sf2d_elastic_desc *d, sf2d_solver **out
       for (int j = 0; j < 5; ++j) rec_h.push_back(d->hgammar[k * 5 + j]);
     }
     tiles[t].rec_n = static_cast<int>(rec_id.size()) - tiles[t].rec_off;
-    if (tiles[t].rec_n > BS) return fail(SF2D_ERR_INVALID, "more receivers in one tile than threads per CTA");
   }
 
   SF2D_CUDA(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
@@ -556,11 +608,20 @@ extern "C" int sf2d_elastic_create(const sf2d_elastic_desc *d, sf2d_solver **out
     P.hconst[50 + k] = d->wxgll[k];
     P.hconst[55 + k] = d->wzgll[k];
   }
-  S->smem = static_cast<size_t>(P.max_q) * (sizeof(float4) + sizeof(float2)) +
-            static_cast<size_t>(P.max_local) * 3 * sizeof(float2) + 64 * sizeof(float) +
-            static_cast<size_t>(P.max_q) * sizeof(uint16_t);
+  S->smem = tile_smem_bytes(P.max_q, P.max_local);
   if (S->smem > 220 * 1024) return fail(SF2D_ERR_INVALID, "tile too large for shared memory");
-  SF2D_CUDA(cudaFuncSetAttribute(k_elastic_tile, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  S->nt = d->threads_per_block > 0 ? d->threads_per_block : 256;
+  if (S->nt != 128 && S->nt != 256 && S->nt != 512)
+    return fail(SF2D_ERR_INVALID, "threads_per_block must be 128, 256 or 512");
+  if (d->nrec > 0) {
+    for (const TileInfo &t : tiles)
+      if (t.rec_n > S->nt) return fail(SF2D_ERR_INVALID, "more receivers in one tile than threads per CTA");
+  }
+  SF2D_CUDA(cudaFuncSetAttribute(k_elastic_tile<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(S->smem)));
+  SF2D_CUDA(cudaFuncSetAttribute(k_elastic_tile<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(S->smem)));
+  SF2D_CUDA(cudaFuncSetAttribute(k_elastic_tile<512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(S->smem)));
   S->nglob = d->nglob;
   S->nrec = d->nrec;
@@ -705,7 +766,7 @@ extern "C" int sf2d_time_kernels(sf2d_solver *S, int nstep, float *ms) {
   for (auto &e : ev) SF2D_CUDA(cudaEventCreate(&e));
   for (int k = 0; k < nstep; ++k) {
     SF2D_CUDA(cudaEventRecord(ev[3 * k], S->stream));
-    sf2d::k_elastic_tile<<<S->T.ntiles, sf2d::BS, S->smem, S->stream>>>(S->P, k > 0 ? 1 : 0);
+    S->launch_tile(k > 0);
     SF2D_CUDA(cudaEventRecord(ev[3 * k + 1], S->stream));
     const int nb = std::max(1, (S->P.nshared + sf2d::BS - 1) / sf2d::BS);
     sf2d::k_elastic_shared<<<nb, sf2d::BS, 0, S->stream>>>(S->P);
@@ -738,7 +799,7 @@ extern "C" int sf2d_layout_info(sf2d_solver *S, long long *info) {
   info[3] = S->T.max_elems;
   info[4] = static_cast<long long>(S->dev_bytes);
   info[5] = static_cast<long long>(S->smem);
-  info[6] = 2;
+  info[6] = S->nt;
   info[7] = 0;
   return SF2D_OK;
 }

@@ -177,6 +177,8 @@ std::string build_tiling(int nspec, int nglob, const int *ibool, const double *c
     std::iota(idx.begin(), idx.end(), 0);
     std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return colour[a] < colour[b]; });
     ti.elem_base = static_cast<int>(T.elem_order.size());
+    while (T.lib.size() % 8) T.lib.push_back(0);
+    ti.lib_off = static_cast<int>(T.lib.size());
     ti.nelem = static_cast<int>(tel[t].size());
     ti.ncol = 0;
     for (int c = 0; c < MAX_COLOURS; ++c) ti.col_end[c] = 0;
@@ -221,7 +223,7 @@ extern "C" int sf2d_tiling_stats(int nspec, int nglob, const int *ibool, const d
     for (int s = ti.elem_base; s < ti.elem_base + ti.nelem; ++s) {
       const int e = T.elem_order[s];
       for (int q = 0; q < NGLL2; ++q) {
-        const int l = T.lib[static_cast<size_t>(s) * NGLL2 + q];
+        const int l = T.lib[static_cast<size_t>(ti.lib_off) + static_cast<size_t>(s - ti.elem_base) * NGLL2 + q];
         const int g = ibool[static_cast<size_t>(e) * NGLL2 + q];
         const int dev = l < ti.n_int ? ti.int_begin + l : T.sh_ids[ti.sh_off + l - ti.n_int];
         if (T.dev2glob[dev] != g) return -3;
@@ -233,7 +235,7 @@ extern "C" int sf2d_tiling_stats(int nspec, int nglob, const int *ibool, const d
       std::vector<char> mark(ti.n_int + ti.n_sh, 0);
       for (int s = cb; s < ti.col_end[c]; ++s)
         for (int q = 0; q < NGLL2; ++q) {
-          const int l = T.lib[static_cast<size_t>(ti.elem_base + s) * NGLL2 + q];
+          const int l = T.lib[static_cast<size_t>(ti.lib_off) + static_cast<size_t>(s) * NGLL2 + q];
           if (mark[l]) return -4;
           mark[l] = 1;
         }

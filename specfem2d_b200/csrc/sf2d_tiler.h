@@ -33,7 +33,8 @@ struct TileInfo {
   int rec_off, rec_n;  // receivers whose element lies in this tile
   int col_end[MAX_COLOURS];  // exclusive end (element index within tile) of each colour
   int ncol;
-  int pad_[3];
+  int lib_off;     // offset of the tile's local ibool (multiple of 8 entries = 16 bytes)
+  int pad_[2];
 };
 static_assert(sizeof(TileInfo) == 24 * 4, "TileInfo layout");
 
@@ -48,7 +49,7 @@ struct Tiling {
   std::vector<TileInfo> tiles;
   std::vector<int> elem_order;        // slot -> original element id
   std::vector<int> elem_tile;         // original element id -> tile
-  std::vector<uint16_t> lib;          // slot*25 + q -> local point id
+  std::vector<uint16_t> lib;          // lib_off + (slot - elem_base)*25 + q -> local point id
   std::vector<int> dev2glob;          // device id -> original global id
   std::vector<int> glob2dev;          // original global id -> device id
   std::vector<int> sh_ids;            // per tile shared local point -> device id

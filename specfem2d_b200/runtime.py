@@ -50,7 +50,7 @@ class ElasticDesc(ctypes.Structure):
         ("cosrot", ctypes.c_double), ("sinrot", ctypes.c_double), ("seismotype", ctypes.c_int),
         ("nstep", ctypes.c_int),
         ("deltat", ctypes.c_float), ("deltatover2", ctypes.c_float), ("deltatsquareover2", ctypes.c_float),
-        ("tile_elems", ctypes.c_int),
+        ("tile_elems", ctypes.c_int), ("threads_per_block", ctypes.c_int),
     ]
 
 
@@ -136,7 +136,7 @@ def tiling_stats(db, tile_elems: int = 64):
 class ElasticSolver:
     """Device-resident isotropic elastic Newmark solver for one Database."""
 
-    def __init__(self, db, tile_elems: int = 64, seismotype: int = 1):
+    def __init__(self, db, tile_elems: int = 64, seismotype: int = 1, threads_per_block: int = 256):
         lib = load_library()
         keep = []
 
@@ -181,6 +181,7 @@ class ElasticSolver:
         d.deltat, d.deltatover2, d.deltatsquareover2 = (float(db.deltat), float(db.deltatover2),
                                                         float(db.deltatsquareover2))
         d.tile_elems = tile_elems
+        d.threads_per_block = threads_per_block
         h = ctypes.c_void_p()
         _check(lib.sf2d_elastic_create(ctypes.byref(d), ctypes.byref(h)))
         self._h = h
@@ -253,5 +254,5 @@ class ElasticSolver:
         v = (ctypes.c_longlong * 8)()
         _check(self._lib.sf2d_layout_info(self._h, v))
         keys = ["ntiles", "nshared", "max_local", "max_elems", "device_bytes", "smem_bytes",
-                "launches_per_step", "reserved"]
+                "threads_per_block", "reserved"]
         return dict(zip(keys, [int(x) for x in v]))

@@ -57,8 +57,8 @@ def test_tromp_seismograms_match_oracle_and_golden(tromp, tromp_oracle):
     assert rel_l2(a, a64) < 1.5 * rel_l2(tromp_oracle[3], a64)
 
 
-@pytest.mark.parametrize("tile_elems", [8, 25, 64, 128])
-def test_tile_size_invariance(tromp, tile_elems):
+@pytest.mark.parametrize("tile_elems,threads", [(8, 128), (25, 256), (64, 512), (128, 256)])
+def test_tile_size_invariance(tromp, tile_elems, threads):
     import oracle
     from specfem2d_b200.runtime import ElasticSolver
 
@@ -66,7 +66,7 @@ def test_tile_size_invariance(tromp, tile_elems):
     # the P wave reaches the receiver (100 km away) after about 1250 steps
     o = oracle.Oracle(db, 4)
     ref = o.run(1500)
-    sol = ElasticSolver(db, tile_elems=tile_elems)
+    sol = ElasticSolver(db, tile_elems=tile_elems, threads_per_block=threads)
     s = sol.run(1500)
     assert rel_l2(s, ref) < TOL
     d, v, _ = sol.get_fields()
