@@ -95,16 +95,36 @@ __device__ __forceinline__ void cp_async16(void *s, const void *g) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// Shared-memory layout of one tile (sizes from the largest tile):
-//   s_geo  float4[max_q]  xix, xiz, gammax, gammaz; overwritten by the weak-form terms
-//   s_mat  float2[max_q]  lambda, mu
-//   s_u, s_v, s_acc float2[max_local]  (old u, v, a -> predicted u, v and the accumulator)
-//   s_h    float[64]      hprime, hprimewgll, wxgll, wzgll
-//   s_lib  uint16[max_q rounded to 8]
-__host__ __device__ inline size_t tile_smem_bytes(int max_q, int max_local) {
-  return static_cast<size_t>(max_q) * (sizeof(float4) + sizeof(float2)) +
-         static_cast<size_t>(max_local) * 3 * sizeof(float2) + 64 * sizeof(float) +
-         static_cast<size_t>((max_q + 7) / 8 * 8) * sizeof(uint16_t);
+// Shared-memory layout of one tile (sizes from the largest tile); every region
+// starts on a 16-byte boundary, as 16-byte cp.async destinations require:
+//   geo  float4[max_q]  xix, xiz, gammax, gammaz; overwritten by the weak-form terms
+//   mat  float2[max_q]  lambda, mu
+//   u, v, acc float2[max_local]  (old u, v, a -> predicted u, v and the accumulator)
+//   h    float[64]      hprime, hprimewgll, wxgll, wzgll
+//   lib  uint16[max_q rounded up to 8]
+struct TileSmem {
+  size_t geo, mat, u, v, acc, h, lib, total;
+};
+__host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~static_cast<size_t>(15); }
+__host__ __device__ inline TileSmem tile_smem_layout(int max_q, int max_local) {
+  TileSmem L;
+  size_t o = 0;
+  L.geo = o;
+  o = align16(o + static_cast<size_t>(max_q) * sizeof(float4));
+  L.mat = o;
+  o = align16(o + static_cast<size_t>(max_q) * sizeof(float2));
+  L.u = o;
+  o = align16(o + static_cast<size_t>(max_local) * sizeof(float2));
+  L.v = o;
+  o = align16(o + static_cast<size_t>(max_local) * sizeof(float2));
+  L.acc = o;
+  o = align16(o + static_cast<size_t>(max_local) * sizeof(float2));
+  L.h = o;
+  o = align16(o + 64 * sizeof(float));
+  L.lib = o;
+  o = align16(o + static_cast<size_t>((max_q + 7) / 8 * 8) * sizeof(uint16_t));
+  L.total = o;
+  return L;
 }
 
 template <int NT>
@@ -118,13 +138,14 @@ __global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_
   const int nq = ti.nelem * 25;
   const int ebase = ti.elem_base * 25;
   const int int_begin = ti.int_begin;
-  float4 *s_geo = reinterpret_cast<float4 *>(smem);
-  float2 *s_mat = reinterpret_cast<float2 *>(s_geo + P.max_q);
-  float2 *s_u = s_mat + P.max_q;
-  float2 *s_v = s_u + P.max_local;
-  float2 *s_acc = s_v + P.max_local;
-  float *s_h = reinterpret_cast<float *>(s_acc + P.max_local);
-  uint16_t *s_lib = reinterpret_cast<uint16_t *>(s_h + 64);
+  const TileSmem L = tile_smem_layout(P.max_q, P.max_local);
+  float4 *s_geo = reinterpret_cast<float4 *>(smem + L.geo);
+  float2 *s_mat = reinterpret_cast<float2 *>(smem + L.mat);
+  float2 *s_u = reinterpret_cast<float2 *>(smem + L.u);
+  float2 *s_v = reinterpret_cast<float2 *>(smem + L.v);
+  float2 *s_acc = reinterpret_cast<float2 *>(smem + L.acc);
+  float *s_h = reinterpret_cast<float *>(smem + L.h);
+  uint16_t *s_lib = reinterpret_cast<uint16_t *>(smem + L.lib);
 
   const int step = *P.d_step;
   // receivers of the previous step read the old fields before any write
@@ -608,7 +629,7 @@ extern "C" int sf2d_elastic_create(const sf2d_elastic_desc *d, sf2d_solver **out
     P.hconst[50 + k] = d->wxgll[k];
     P.hconst[55 + k] = d->wzgll[k];
   }
-  S->smem = tile_smem_bytes(P.max_q, P.max_local);
+  S->smem = tile_smem_layout(P.max_q, P.max_local).total;
   if (S->smem > 220 * 1024) return fail(SF2D_ERR_INVALID, "tile too large for shared memory");
   S->nt = d->threads_per_block > 0 ? d->threads_per_block : 256;
   if (S->nt != 128 && S->nt != 256 && S->nt != 512)

@@ -191,6 +191,8 @@ std::string build_tiling(int nspec, int nglob, const int *ibool, const double *c
     }
     for (int c = 1; c < ti.ncol; ++c) ti.col_end[c] = std::max(ti.col_end[c], ti.col_end[c - 1]);
   }
+  // the kernel copies each tile's local ibool in 16-byte chunks
+  while (T.lib.size() % 8) T.lib.push_back(0);
   return "";
 }
 
