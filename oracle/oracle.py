@@ -37,13 +37,21 @@ class OracleDb(ctypes.Structure):
         ("deltat", ctypes.c_double), ("deltatover2", ctypes.c_double), ("deltatsquareover2", ctypes.c_double),
         ("ispec_is_anisotropic", _ip),
         ("c11", _dp), ("c13", _dp), ("c15", _dp), ("c33", _dp), ("c35", _dp), ("c55", _dp),
+        ("time_scheme", ctypes.c_int), ("alpha_lddrk", _dp), ("beta_lddrk", _dp),
+        ("att_a1", _dp), ("att_b1", _dp), ("att_a2", _dp), ("att_b2", _dp),
+        ("att_itau1", _dp), ("att_phi1", _dp), ("att_itau2", _dp), ("att_phi2", _dp),
     ]
+
+
+DISPL, VELOC, ACCEL, DISPL_LDDRK, VELOC_LDDRK, E1, E11, E13 = range(8)
 
 
 def build() -> str:
     """Compile the oracle library if it is missing or older than its source."""
     src = os.path.join(HERE, "sf2d_oracle.cpp")
-    if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+    hdr = os.path.join(HERE, "sf2d_oracle.h")
+    if (not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src)
+            or os.path.getmtime(LIB_PATH) < os.path.getmtime(hdr)):
         subprocess.run(["make", "-s", "-C", HERE], check=True)
     return LIB_PATH
 
@@ -55,30 +63,41 @@ def lib():
     global _lib
     if _lib is None:
         _lib = ctypes.CDLL(build())
-        _lib.sf2d_oracle_newmark_elastic.restype = ctypes.c_int
-        _lib.sf2d_oracle_newmark_elastic.argtypes = [
-            ctypes.POINTER(OracleDb), ctypes.c_int, ctypes.c_int, ctypes.c_int,
-            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _dp, ctypes.c_int]
+        _lib.sf2d_oracle_create.restype = ctypes.c_void_p
+        _lib.sf2d_oracle_create.argtypes = [ctypes.POINTER(OracleDb), ctypes.c_int]
+        _lib.sf2d_oracle_run.restype = ctypes.c_int
+        _lib.sf2d_oracle_run.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, ctypes.c_int]
+        for fn in (_lib.sf2d_oracle_get, _lib.sf2d_oracle_set):
+            fn.restype = ctypes.c_int
+            fn.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        _lib.sf2d_oracle_destroy.restype = None
+        _lib.sf2d_oracle_destroy.argtypes = [ctypes.c_void_p]
         _lib.sf2d_oracle_max_threads.restype = ctypes.c_int
     return _lib
 
 
 class Oracle:
-    """Holds converted arrays (kept alive) and runs the oracle time loop."""
+    """Holds converted arrays (kept alive) and an oracle state; runs the CPU time loop."""
 
     def __init__(self, db, precision: int = 4, seismotype: int = 1, db64=None):
         """``db`` supplies the FP32 setup; ``db64`` (optional) the FP64 one for precision 8."""
+        from specfem2d_b200.setup.solver_setup import ALPHA_LDDRK, BETA_LDDRK
+
         self.precision = precision
         src = db64 if (precision == 8 and db64 is not None) else db
         self.db = src
         keep = []
 
         def d(a):
+            if a is None:
+                return None
             arr = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
             keep.append(arr)
             return arr.ctypes.data_as(_dp)
 
         def i(a):
+            if a is None:
+                return None
             arr = np.ascontiguousarray(np.asarray(a, dtype=np.int32))
             keep.append(arr)
             return arr.ctypes.data_as(_ip)
@@ -124,21 +143,64 @@ class Oracle:
         s.cosrot, s.sinrot = float(src.cosrot), float(src.sinrot)
         s.seismotype = seismotype
         s.deltat, s.deltatover2, s.deltatsquareover2 = dt, dto2, dt2o2
+        an = getattr(src, "aniso", None)
+        if an is not None:
+            s.ispec_is_anisotropic = i(an["ispec"])
+            s.c11, s.c13, s.c15 = d(an["c11"]), d(an["c13"]), d(an["c15"])
+            s.c33, s.c35, s.c55 = d(an["c33"]), d(an["c35"]), d(an["c55"])
+        s.time_scheme = int(src.time_scheme)
+        s.alpha_lddrk, s.beta_lddrk = d(ALPHA_LDDRK), d(BETA_LDDRK)
+        at = getattr(src, "atten", None)
+        if at is not None:
+            s.att_a1, s.att_b1, s.att_a2, s.att_b2 = d(at["a1"]), d(at["b1"]), d(at["a2"]), d(at["b2"])
+            s.att_itau1, s.att_phi1 = d(at["itau1"]), d(at["phi1"])
+            s.att_itau2, s.att_phi2 = d(at["itau2"]), d(at["phi2"])
         self._keep = keep
         self.s = s
-        dtype = np.float32 if precision == 4 else np.float64
-        self.displ = np.zeros((src.nglob, 2), dtype=dtype)
-        self.veloc = np.zeros((src.nglob, 2), dtype=dtype)
-        self.accel = np.zeros((src.nglob, 2), dtype=dtype)
+        self.h = lib().sf2d_oracle_create(ctypes.byref(s), precision)
+        if not self.h:
+            raise RuntimeError("oracle creation failed")
+        self.dtype = np.float32 if precision == 4 else np.float64
         self.it = 0
 
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            lib().sf2d_oracle_destroy(h)
+            self.h = None
+
+    def _size(self, which):
+        if which <= VELOC_LDDRK:
+            return (self.s.nglob, 2)
+        return (self.s.nspec, 5, 5, 3)
+
+    def get(self, which):
+        out = np.empty(self._size(which), dtype=self.dtype)
+        if lib().sf2d_oracle_get(self.h, which, out.ctypes.data) != 0:
+            raise RuntimeError(f"oracle field {which} unavailable")
+        return out
+
+    def set(self, which, arr):
+        arr = np.ascontiguousarray(arr, dtype=self.dtype).reshape(self._size(which))
+        if lib().sf2d_oracle_set(self.h, which, arr.ctypes.data) != 0:
+            raise RuntimeError(f"oracle field {which} unavailable")
+
+    @property
+    def displ(self):
+        return self.get(DISPL)
+
+    @property
+    def veloc(self):
+        return self.get(VELOC)
+
+    @property
+    def accel(self):
+        return self.get(ACCEL)
+
     def run(self, nstep: int, nthreads: int = 0) -> np.ndarray:
-        """Advance nstep Newmark steps; return seismograms (nrec, nstep, 2) float64."""
+        """Advance nstep time steps; return seismograms (nrec, nstep, 2) float64."""
         seis = np.zeros((self.s.nrec, nstep, 2), dtype=np.float64)
-        rc = lib().sf2d_oracle_newmark_elastic(
-            ctypes.byref(self.s), self.precision, self.it, nstep,
-            self.displ.ctypes.data, self.veloc.ctypes.data, self.accel.ctypes.data,
-            seis.ctypes.data_as(_dp), nthreads)
+        rc = lib().sf2d_oracle_run(self.h, nstep, seis.ctypes.data_as(_dp), nthreads)
         if rc != 0:
             raise RuntimeError(f"oracle failed with status {rc}")
         self.it += nstep

@@ -2,10 +2,12 @@
 //
 // A restatement of the reference's CPU routines, used only as the checker of
 // the CUDA path and as the timed CPU baseline.  `real` is float for the
-// CUSTOM_REAL=4 build and double for the CUSTOM_REAL=8 build.
+// CUSTOM_REAL=4 build and double for the CUSTOM_REAL=8 build; expressions
+// that the reference evaluates in double inside a CUSTOM_REAL=4 build are
+// evaluated in double here too.
 //
-// Summation order follows the serial reference: within a step, Stacey and
-// source terms are added first (iphase 1 of
+// Summation order follows the serial reference: within a step (or LDDRK
+// stage), Stacey and source terms are added first (iphase 1 of
 // src/specfem2D/compute_forces_viscoelastic_calling_routine.F90:58-100, all
 // elements are "inner" with one process), then element contributions in
 // ascending element order.  Element work is spread over host threads into
@@ -16,6 +18,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <cstring>
 #include <thread>
 #include <vector>
 
@@ -23,6 +26,7 @@ namespace {
 
 constexpr int NGLL = 5;
 constexpr int NGLL2 = 25;
+constexpr int NSLS = 3;
 
 int default_threads() {
   const char *env = std::getenv("SF2D_ORACLE_THREADS");
@@ -50,241 +54,392 @@ void parallel_for(int n, int nt, F &&f) {
 }
 
 template <typename real>
-struct Db {
-  int nspec, nglob;
-  const int *ibool;
-  std::vector<real> xix, xiz, gammax, gammaz, jacobian, rho, kappa, mu, rho_vp, rmass;
-  real hprime[NGLL][NGLL], hprimewgll[NGLL][NGLL], wxgll[NGLL], wzgll[NGLL];
-  std::vector<real> st_nx, st_nz, st_w, st_rvp, st_rvs, srcarr;
-  std::vector<real> c11, c13, c15, c33, c35, c55;
-  const int *aniso;
-  real deltat, deltatover2, deltatsquareover2;
-};
-
-template <typename real>
 std::vector<real> cvt(const double *p, size_t n) {
-  std::vector<real> v(n);
+  std::vector<real> v(p ? n : 0);
   if (p)
     for (size_t k = 0; k < n; ++k) v[k] = static_cast<real>(p[k]);
   return v;
 }
 
-template <typename real>
-void load(const sf2d_oracle_db *d, Db<real> &o) {
-  const size_t nl = static_cast<size_t>(d->nspec) * NGLL2;
-  o.nspec = d->nspec;
-  o.nglob = d->nglob;
-  o.ibool = d->ibool;
-  o.xix = cvt<real>(d->xix, nl);
-  o.xiz = cvt<real>(d->xiz, nl);
-  o.gammax = cvt<real>(d->gammax, nl);
-  o.gammaz = cvt<real>(d->gammaz, nl);
-  o.jacobian = cvt<real>(d->jacobian, nl);
-  o.rho = cvt<real>(d->rhostore, nl);
-  o.kappa = cvt<real>(d->kappastore, nl);
-  o.mu = cvt<real>(d->mustore, nl);
-  o.rho_vp = cvt<real>(d->rho_vpstore, nl);
-  o.rmass = cvt<real>(d->rmass_inverse, static_cast<size_t>(d->nglob) * 2);
-  for (int a = 0; a < NGLL; ++a) {
-    o.wxgll[a] = static_cast<real>(d->wxgll[a]);
-    o.wzgll[a] = static_cast<real>(d->wzgll[a]);
-    for (int b = 0; b < NGLL; ++b) {
-      o.hprime[a][b] = static_cast<real>(d->hprime[a * NGLL + b]);
-      o.hprimewgll[a][b] = static_cast<real>(d->hprimewgll[a * NGLL + b]);
-    }
-  }
-  o.st_nx = cvt<real>(d->st_nx, d->nstacey);
-  o.st_nz = cvt<real>(d->st_nz, d->nstacey);
-  o.st_w = cvt<real>(d->st_w, d->nstacey);
-  o.st_rvp = cvt<real>(d->st_rvp, d->nstacey);
-  o.st_rvs = cvt<real>(d->st_rvs, d->nstacey);
-  o.srcarr = cvt<real>(d->sourcearrays, static_cast<size_t>(d->nsrc) * NGLL2 * 2);
-  o.aniso = d->ispec_is_anisotropic;
-  if (d->ispec_is_anisotropic) {
-    o.c11 = cvt<real>(d->c11, nl);
-    o.c13 = cvt<real>(d->c13, nl);
-    o.c15 = cvt<real>(d->c15, nl);
-    o.c33 = cvt<real>(d->c33, nl);
-    o.c35 = cvt<real>(d->c35, nl);
-    o.c55 = cvt<real>(d->c55, nl);
-  }
-  o.deltat = static_cast<real>(d->deltat);
-  o.deltatover2 = static_cast<real>(d->deltatover2);
-  o.deltatsquareover2 = static_cast<real>(d->deltatsquareover2);
-}
+struct StateBase {
+  virtual ~StateBase() = default;
+  virtual int run(int nstep, double *seis, int nthreads) = 0;
+  virtual int get(int which, void *out) = 0;
+  virtual int set(int which, const void *in) = 0;
+};
 
-// Element internal force -K u for one element (compute_forces_viscoelastic.F90:
-// 184-197 gather, :810-883 mxm_4comp_singleA, :220-234 mapping, :286-357
-// isotropic P-SV stress with lambda = rho*cp^2 - 2 mu, :372-445 anisotropic,
-// :669-675 weak-form terms, :760-782 weighted transpose contraction).
-// Writes the 25x2 contributions (to be subtracted) into `out`.
 template <typename real>
-void element_force(const Db<real> &o, int ispec, const real *displ, real *out) {
-  const size_t off = static_cast<size_t>(ispec) * NGLL2;
-  real ux[NGLL][NGLL], uz[NGLL][NGLL];  // [j][i]
-  for (int j = 0; j < NGLL; ++j)
-    for (int i = 0; i < NGLL; ++i) {
-      const int g = o.ibool[off + j * NGLL + i];
-      ux[j][i] = displ[2 * g];
-      uz[j][i] = displ[2 * g + 1];
+struct State : StateBase {
+  const sf2d_oracle_db d;  // shallow copy of the descriptor (pointers stay with the caller)
+  int nspec, nglob;
+  std::vector<real> xix, xiz, gammax, gammaz, jacobian, rho, mu, rho_vp, rmass;
+  real hprime[NGLL][NGLL], hprimewgll[NGLL][NGLL], wxgll[NGLL], wzgll[NGLL];
+  std::vector<real> st_nx, st_nz, st_w, st_rvp, st_rvs, srcarr;
+  std::vector<real> c11, c13, c15, c33, c35, c55;
+  std::vector<real> a1, b1, a2, b2, phi1, phi2;  // Newmark A/B, LDDRK phi (CUSTOM_REAL)
+  std::vector<double> itau1, itau2;             // LDDRK 1/tau_sigma (read as double)
+  real deltat, deltatover2, deltatsquareover2;
+  real alpha[6], beta[6];
+  bool atten;
+  // state
+  std::vector<real> displ, veloc, accel, displ_l, veloc_l;
+  std::vector<real> e1, e11, e13, e1_l, e11_l, e13_l;      // nspec*25*3
+  std::vector<real> dux_dxl_old, duz_dzl_old, dxz_old;      // nspec*25
+  std::vector<real> contrib;
+  int it = 0;  // steps done
+
+  explicit State(const sf2d_oracle_db *p) : d(*p) {
+    nspec = d.nspec;
+    nglob = d.nglob;
+    const size_t nl = static_cast<size_t>(nspec) * NGLL2;
+    xix = cvt<real>(d.xix, nl);
+    xiz = cvt<real>(d.xiz, nl);
+    gammax = cvt<real>(d.gammax, nl);
+    gammaz = cvt<real>(d.gammaz, nl);
+    jacobian = cvt<real>(d.jacobian, nl);
+    rho = cvt<real>(d.rhostore, nl);
+    mu = cvt<real>(d.mustore, nl);
+    rho_vp = cvt<real>(d.rho_vpstore, nl);
+    rmass = cvt<real>(d.rmass_inverse, static_cast<size_t>(nglob) * 2);
+    for (int a = 0; a < NGLL; ++a) {
+      wxgll[a] = static_cast<real>(d.wxgll[a]);
+      wzgll[a] = static_cast<real>(d.wzgll[a]);
+      for (int b = 0; b < NGLL; ++b) {
+        hprime[a][b] = static_cast<real>(d.hprime[a * NGLL + b]);
+        hprimewgll[a][b] = static_cast<real>(d.hprimewgll[a * NGLL + b]);
+      }
     }
-  real t1x[NGLL][NGLL], t1z[NGLL][NGLL], t2x[NGLL][NGLL], t2z[NGLL][NGLL];
-  const bool is_aniso = o.aniso && o.aniso[ispec];
-  for (int j = 0; j < NGLL; ++j)
-    for (int i = 0; i < NGLL; ++i) {
-      // x1 = dux_dxi(i,j) = sum_k A(1,k,j) * hprime(i,k)
-      const real dux_dxi = ux[j][0] * o.hprime[i][0] + ux[j][1] * o.hprime[i][1] +
-                           ux[j][2] * o.hprime[i][2] + ux[j][3] * o.hprime[i][3] +
-                           ux[j][4] * o.hprime[i][4];
-      const real duz_dxi = uz[j][0] * o.hprime[i][0] + uz[j][1] * o.hprime[i][1] +
-                           uz[j][2] * o.hprime[i][2] + uz[j][3] * o.hprime[i][3] +
-                           uz[j][4] * o.hprime[i][4];
-      const real dux_dgamma = ux[0][i] * o.hprime[j][0] + ux[1][i] * o.hprime[j][1] +
-                              ux[2][i] * o.hprime[j][2] + ux[3][i] * o.hprime[j][3] +
-                              ux[4][i] * o.hprime[j][4];
-      const real duz_dgamma = uz[0][i] * o.hprime[j][0] + uz[1][i] * o.hprime[j][1] +
-                              uz[2][i] * o.hprime[j][2] + uz[3][i] * o.hprime[j][3] +
-                              uz[4][i] * o.hprime[j][4];
-      const size_t p = off + j * NGLL + i;
-      const real xixl = o.xix[p], xizl = o.xiz[p], gammaxl = o.gammax[p], gammazl = o.gammaz[p];
-      const real jacobianl = o.jacobian[p];
-      const real dux_dxl = dux_dxi * xixl + dux_dgamma * gammaxl;
-      const real dux_dzl = dux_dxi * xizl + dux_dgamma * gammazl;
-      const real duz_dxl = duz_dxi * xixl + duz_dgamma * gammaxl;
-      const real duz_dzl = duz_dxi * xizl + duz_dgamma * gammazl;
-      real sigma_xx, sigma_zz, sigma_xz;
-      if (!is_aniso) {
-        const real mul = o.mu[p];
-        const real rhol = o.rho[p];
-        const real cpl = o.rho_vp[p] / rhol;
+    st_nx = cvt<real>(d.st_nx, d.nstacey);
+    st_nz = cvt<real>(d.st_nz, d.nstacey);
+    st_w = cvt<real>(d.st_w, d.nstacey);
+    st_rvp = cvt<real>(d.st_rvp, d.nstacey);
+    st_rvs = cvt<real>(d.st_rvs, d.nstacey);
+    srcarr = cvt<real>(d.sourcearrays, static_cast<size_t>(d.nsrc) * NGLL2 * 2);
+    if (d.ispec_is_anisotropic) {
+      c11 = cvt<real>(d.c11, nl);
+      c13 = cvt<real>(d.c13, nl);
+      c15 = cvt<real>(d.c15, nl);
+      c33 = cvt<real>(d.c33, nl);
+      c35 = cvt<real>(d.c35, nl);
+      c55 = cvt<real>(d.c55, nl);
+    }
+    deltat = static_cast<real>(d.deltat);
+    deltatover2 = static_cast<real>(d.deltatover2);
+    deltatsquareover2 = static_cast<real>(d.deltatsquareover2);
+    for (int s = 0; s < 6; ++s) {
+      alpha[s] = d.alpha_lddrk ? static_cast<real>(d.alpha_lddrk[s]) : real(0);
+      beta[s] = d.beta_lddrk ? static_cast<real>(d.beta_lddrk[s]) : real(0);
+    }
+    atten = d.time_scheme == 1 ? (d.att_a1 != nullptr) : (d.att_itau1 != nullptr);
+    if (atten) {
+      const size_t na = nl * NSLS;
+      if (d.time_scheme == 1) {
+        a1 = cvt<real>(d.att_a1, na);
+        b1 = cvt<real>(d.att_b1, na);
+        a2 = cvt<real>(d.att_a2, na);
+        b2 = cvt<real>(d.att_b2, na);
+      } else {
+        phi1 = cvt<real>(d.att_phi1, na);
+        phi2 = cvt<real>(d.att_phi2, na);
+        itau1.assign(d.att_itau1, d.att_itau1 + na);
+        itau2.assign(d.att_itau2, d.att_itau2 + na);
+      }
+      e1.assign(na, 0);
+      e11.assign(na, 0);
+      e13.assign(na, 0);
+      if (d.time_scheme != 1) {
+        e1_l.assign(na, 0);
+        e11_l.assign(na, 0);
+        e13_l.assign(na, 0);
+      }
+      dux_dxl_old.assign(nl, 0);
+      duz_dzl_old.assign(nl, 0);
+      dxz_old.assign(nl, 0);
+    }
+    const size_t ng = static_cast<size_t>(nglob) * 2;
+    displ.assign(ng, 0);
+    veloc.assign(ng, 0);
+    accel.assign(ng, 0);
+    if (d.time_scheme != 1) {
+      displ_l.assign(ng, 0);
+      veloc_l.assign(ng, 0);
+    }
+    contrib.assign(nl * 2, 0);
+  }
+
+  // Memory-variable update at one GLL point; returns the three sums.
+  // compute_attenuation_viscoelastic.f90:36-236 (Newmark branch :109-146,
+  // LDDRK branch :147-163); stage is 0-based.
+  void attenuation(size_t p, real dux_dxl, real dux_dzl, real duz_dxl, real duz_dzl, int stage, real &e1s,
+                   real &e11s, real &e13s) {
+    const real theta_n = dux_dxl + duz_dzl;
+    real *E1 = &e1[p * NSLS], *E11 = &e11[p * NSLS], *E13 = &e13[p * NSLS];
+    if (d.time_scheme == 1) {
+      const real theta_n1 = dux_dxl_old[p] + duz_dzl_old[p];
+      for (int s = 0; s < NSLS; ++s) {
+        const size_t q = p * NSLS + s;
+        real a = a1[q];
+        E1[s] = a * a * E1[s] + b1[q] * (theta_n + a * theta_n1);
+        a = a2[q];
+        E11[s] = a * a * E11[s] + b2[q] * (dux_dxl - theta_n / real(2) + a * (dux_dxl_old[p] - theta_n1 / real(2)));
+        E13[s] = a * a * E13[s] + b2[q] * (dux_dzl + duz_dxl + a * dxz_old[p]);
+      }
+    } else {
+      const real al = alpha[stage], be = beta[stage];
+      for (int s = 0; s < NSLS; ++s) {
+        const size_t q = p * NSLS + s;
+        const real phinu1 = phi1[q], phinu2 = phi2[q];
+        const double tauinvnu1 = itau1[q], tauinvnu2 = itau2[q];
+        // tauinvnu is double in the reference: the products with it are double
+        e1_l[q] = static_cast<real>(static_cast<double>(al * e1_l[q]) +
+                                    static_cast<double>(deltat) *
+                                        (static_cast<double>(theta_n * phinu1) - static_cast<double>(E1[s]) * tauinvnu1));
+        E1[s] = E1[s] + be * e1_l[q];
+        e11_l[q] = static_cast<real>(static_cast<double>(al * e11_l[q] + deltat * ((dux_dxl - theta_n / real(2)) * phinu2)) -
+                                     static_cast<double>(deltat) * (static_cast<double>(E11[s]) * tauinvnu2));
+        E11[s] = E11[s] + be * e11_l[q];
+        e13_l[q] = static_cast<real>(static_cast<double>(al * e13_l[q] + deltat * ((dux_dzl + duz_dxl) * phinu2)) -
+                                     static_cast<double>(deltat) * (static_cast<double>(E13[s]) * tauinvnu2));
+        E13[s] = E13[s] + be * e13_l[q];
+      }
+    }
+    e1s = E1[0] + E1[1] + E1[2];
+    e11s = E11[0] + E11[1] + E11[2];
+    e13s = E13[0] + E13[1] + E13[2];
+    if (d.time_scheme == 1) {
+      dux_dxl_old[p] = dux_dxl;
+      duz_dzl_old[p] = duz_dzl;
+      dxz_old[p] = dux_dzl + duz_dxl;
+    }
+  }
+
+  // Element internal force -K u for one element (compute_forces_viscoelastic.F90:
+  // 184-197 gather, :810-883 mxm_4comp_singleA, :220-234 mapping, :286-357
+  // isotropic P-SV stress with lambda = rho*cp^2 - 2 mu, :372-445 anisotropic,
+  // :481-503 attenuation, :669-675 weak-form terms, :760-782 weighted transpose
+  // contraction).  Writes the 25x2 contributions (to be subtracted) into `out`.
+  void element_force(int ispec, int stage, real *out) {
+    const size_t off = static_cast<size_t>(ispec) * NGLL2;
+    real ux[NGLL][NGLL], uz[NGLL][NGLL];  // [j][i]
+    for (int j = 0; j < NGLL; ++j)
+      for (int i = 0; i < NGLL; ++i) {
+        const int g = d.ibool[off + j * NGLL + i];
+        ux[j][i] = displ[2 * g];
+        uz[j][i] = displ[2 * g + 1];
+      }
+    real t1x[NGLL][NGLL], t1z[NGLL][NGLL], t2x[NGLL][NGLL], t2z[NGLL][NGLL];
+    const bool is_aniso = d.ispec_is_anisotropic && d.ispec_is_anisotropic[ispec];
+    for (int j = 0; j < NGLL; ++j)
+      for (int i = 0; i < NGLL; ++i) {
+        const real dux_dxi = ux[j][0] * hprime[i][0] + ux[j][1] * hprime[i][1] + ux[j][2] * hprime[i][2] +
+                             ux[j][3] * hprime[i][3] + ux[j][4] * hprime[i][4];
+        const real duz_dxi = uz[j][0] * hprime[i][0] + uz[j][1] * hprime[i][1] + uz[j][2] * hprime[i][2] +
+                             uz[j][3] * hprime[i][3] + uz[j][4] * hprime[i][4];
+        const real dux_dgamma = ux[0][i] * hprime[j][0] + ux[1][i] * hprime[j][1] + ux[2][i] * hprime[j][2] +
+                                ux[3][i] * hprime[j][3] + ux[4][i] * hprime[j][4];
+        const real duz_dgamma = uz[0][i] * hprime[j][0] + uz[1][i] * hprime[j][1] + uz[2][i] * hprime[j][2] +
+                                uz[3][i] * hprime[j][3] + uz[4][i] * hprime[j][4];
+        const size_t p = off + j * NGLL + i;
+        const real xixl = xix[p], xizl = xiz[p], gammaxl = gammax[p], gammazl = gammaz[p];
+        const real jacobianl = jacobian[p];
+        const real dux_dxl = dux_dxi * xixl + dux_dgamma * gammaxl;
+        const real dux_dzl = dux_dxi * xizl + dux_dgamma * gammazl;
+        const real duz_dxl = duz_dxi * xixl + duz_dgamma * gammaxl;
+        const real duz_dzl = duz_dxi * xizl + duz_dgamma * gammazl;
+        const real mul = mu[p];
+        const real rhol = rho[p];
+        const real cpl = rho_vp[p] / rhol;
         const real lambdal = rhol * cpl * cpl - real(2) * mul;
         const real lambdaplus2mu = lambdal + real(2) * mul;
-        sigma_xx = lambdaplus2mu * dux_dxl + lambdal * duz_dzl;
-        sigma_zz = lambdaplus2mu * duz_dzl + lambdal * dux_dxl;
-        sigma_xz = mul * (duz_dxl + dux_dzl);
-      } else {
-        // c_ij are read as double in the reference (compute_forces_viscoelastic.F90:112)
-        const double c11 = o.c11[p], c13 = o.c13[p], c15 = o.c15[p];
-        const double c33 = o.c33[p], c35 = o.c35[p], c55 = o.c55[p];
-        sigma_xx = static_cast<real>(c11 * dux_dxl + c13 * duz_dzl + c15 * (duz_dxl + dux_dzl));
-        sigma_zz = static_cast<real>(c13 * dux_dxl + c33 * duz_dzl + c35 * (duz_dxl + dux_dzl));
-        sigma_xz = static_cast<real>(c15 * dux_dxl + c35 * duz_dzl + c55 * (duz_dxl + dux_dzl));
+        const real lambdalplusmul = lambdal + mul;
+        real sigma_xx, sigma_zz, sigma_xz;
+        if (!is_aniso) {
+          sigma_xx = lambdaplus2mu * dux_dxl + lambdal * duz_dzl;
+          sigma_zz = lambdaplus2mu * duz_dzl + lambdal * dux_dxl;
+          sigma_xz = mul * (duz_dxl + dux_dzl);
+        } else {
+          // c_ij are read as double in the reference (compute_forces_viscoelastic.F90:112)
+          const double C11 = c11[p], C13 = c13[p], C15 = c15[p], C33 = c33[p], C35 = c35[p], C55 = c55[p];
+          sigma_xx = static_cast<real>(C11 * dux_dxl + C13 * duz_dzl + C15 * (duz_dxl + dux_dzl));
+          sigma_zz = static_cast<real>(C13 * dux_dxl + C33 * duz_dzl + C35 * (duz_dxl + dux_dzl));
+          sigma_xz = static_cast<real>(C15 * dux_dxl + C35 * duz_dzl + C55 * (duz_dxl + dux_dzl));
+        }
+        if (atten) {
+          real e1s, e11s, e13s;
+          attenuation(p, dux_dxl, dux_dzl, duz_dxl, duz_dzl, stage, e1s, e11s, e13s);
+          sigma_xx = sigma_xx + lambdalplusmul * e1s + real(2) * mul * e11s;
+          sigma_xz = sigma_xz + mul * e13s;
+          sigma_zz = sigma_zz + lambdalplusmul * e1s - real(2) * mul * e11s;
+        }
+        const real sigma_zx = sigma_xz;
+        t1x[j][i] = jacobianl * (sigma_xx * xixl + sigma_zx * xizl);
+        t1z[j][i] = jacobianl * (sigma_xz * xixl + sigma_zz * xizl);
+        t2x[j][i] = jacobianl * (sigma_xx * gammaxl + sigma_zx * gammazl);
+        t2z[j][i] = jacobianl * (sigma_xz * gammaxl + sigma_zz * gammazl);
       }
-      const real sigma_zx = sigma_xz;
-      t1x[j][i] = jacobianl * (sigma_xx * xixl + sigma_zx * xizl);
-      t1z[j][i] = jacobianl * (sigma_xz * xixl + sigma_zz * xizl);
-      t2x[j][i] = jacobianl * (sigma_xx * gammaxl + sigma_zx * gammazl);
-      t2z[j][i] = jacobianl * (sigma_xz * gammaxl + sigma_zz * gammazl);
-    }
-  for (int j = 0; j < NGLL; ++j)
-    for (int i = 0; i < NGLL; ++i) {
-      real tx1 = 0, tx2 = 0, tz1 = 0, tz2 = 0;
-      for (int k = 0; k < NGLL; ++k) {
-        tx1 = tx1 + t1x[j][k] * o.hprimewgll[k][i];
-        tx2 = tx2 + t2x[k][i] * o.hprimewgll[k][j];
-        tz1 = tz1 + t1z[j][k] * o.hprimewgll[k][i];
-        tz2 = tz2 + t2z[k][i] * o.hprimewgll[k][j];
+    for (int j = 0; j < NGLL; ++j)
+      for (int i = 0; i < NGLL; ++i) {
+        real tx1 = 0, tx2 = 0, tz1 = 0, tz2 = 0;
+        for (int k = 0; k < NGLL; ++k) {
+          tx1 = tx1 + t1x[j][k] * hprimewgll[k][i];
+          tx2 = tx2 + t2x[k][i] * hprimewgll[k][j];
+          tz1 = tz1 + t1z[j][k] * hprimewgll[k][i];
+          tz2 = tz2 + t2z[k][i] * hprimewgll[k][j];
+        }
+        out[2 * (j * NGLL + i)] = wzgll[j] * tx1 + wxgll[i] * tx2;
+        out[2 * (j * NGLL + i) + 1] = wzgll[j] * tz1 + wxgll[i] * tz2;
       }
-      out[2 * (j * NGLL + i)] = o.wzgll[j] * tx1 + o.wxgll[i] * tx2;
-      out[2 * (j * NGLL + i) + 1] = o.wzgll[j] * tz1 + o.wxgll[i] * tz2;
-    }
-}
+  }
 
-template <typename real>
-int run_newmark(const sf2d_oracle_db *d, int it0, int nstep, real *displ, real *veloc, real *accel,
-                double *seis, int nthreads) {
-  Db<real> o;
-  load(d, o);
-  const int nglob = d->nglob;
-  const int nspec = d->nspec;
-  std::vector<real> contrib(static_cast<size_t>(nspec) * NGLL2 * 2);
-  const int nt = nthreads > 0 ? nthreads : default_threads();
-  for (int s = 0; s < nstep; ++s) {
-    const int it = it0 + s;
-    // predictor (update_displacement_Newmark.F90:408-454)
-    for (int g = 0; g < 2 * nglob; ++g) {
-      displ[g] = displ[g] + o.deltat * veloc[g] + o.deltatsquareover2 * accel[g];
-      veloc[g] = veloc[g] + o.deltatover2 * accel[g];
-      accel[g] = 0;
-    }
-    // iphase 1: Stacey (compute_stacey_elastic.f90:160-335) then force sources
-    // (compute_add_sources_viscoelastic.f90:36-101)
-    for (int p = 0; p < d->nstacey; ++p) {
-      const int g = d->st_iglob[p];
+  // accel = Stacey(veloc) + sources(stf[it, stage]) - K displ, in reference order
+  void forces(int stage, int nt) {
+    for (int p = 0; p < d.nstacey; ++p) {
+      const int g = d.st_iglob[p];
       const real vx = veloc[2 * g], vz = veloc[2 * g + 1];
-      const real nx = o.st_nx[p], nz = o.st_nz[p];
+      const real nx = st_nx[p], nz = st_nz[p];
       const real vn = nx * vx + nz * vz;
-      const real tx = o.st_rvp[p] * vn * nx + o.st_rvs[p] * (vx - vn * nx);
-      const real tz = o.st_rvp[p] * vn * nz + o.st_rvs[p] * (vz - vn * nz);
-      accel[2 * g] = accel[2 * g] - tx * o.st_w[p];
-      accel[2 * g + 1] = accel[2 * g + 1] - tz * o.st_w[p];
+      const real tx = st_rvp[p] * vn * nx + st_rvs[p] * (vx - vn * nx);
+      const real tz = st_rvp[p] * vn * nz + st_rvs[p] * (vz - vn * nz);
+      accel[2 * g] = accel[2 * g] - tx * st_w[p];
+      accel[2 * g + 1] = accel[2 * g + 1] - tz * st_w[p];
     }
-    for (int isrc = 0; isrc < d->nsrc; ++isrc) {
-      const real stf = static_cast<real>(d->stf[(static_cast<size_t>(isrc) * d->nstep_total + it) * d->nstage]);
-      const int e = d->src_ispec[isrc];
+    for (int isrc = 0; isrc < d.nsrc; ++isrc) {
+      real stf = 0;
+      if (it < d.nstep_total)
+        stf = static_cast<real>(d.stf[(static_cast<size_t>(isrc) * d.nstep_total + it) * d.nstage + stage]);
+      const int e = d.src_ispec[isrc];
       for (int j = 0; j < NGLL; ++j)
         for (int i = 0; i < NGLL; ++i) {
-          const int g = d->ibool[static_cast<size_t>(e) * NGLL2 + j * NGLL + i];
+          const int g = d.ibool[static_cast<size_t>(e) * NGLL2 + j * NGLL + i];
           const size_t q = (static_cast<size_t>(isrc) * NGLL2 + j * NGLL + i) * 2;
-          accel[2 * g] = accel[2 * g] + o.srcarr[q] * stf;
-          accel[2 * g + 1] = accel[2 * g + 1] + o.srcarr[q + 1] * stf;
+          accel[2 * g] = accel[2 * g] + srcarr[q] * stf;
+          accel[2 * g + 1] = accel[2 * g + 1] + srcarr[q + 1] * stf;
         }
     }
-    // iphase 2: all elements
-    parallel_for(nspec, nspec > 256 ? nt : 1, [&](int b, int e1) {
-      for (int e = b; e < e1; ++e) element_force(o, e, displ, &contrib[static_cast<size_t>(e) * NGLL2 * 2]);
+    parallel_for(nspec, nspec > 256 ? nt : 1, [&](int b, int e1_) {
+      for (int e = b; e < e1_; ++e) element_force(e, stage, &contrib[static_cast<size_t>(e) * NGLL2 * 2]);
     });
     for (int e = 0; e < nspec; ++e) {
       const real *c = &contrib[static_cast<size_t>(e) * NGLL2 * 2];
-      const int *ib = &d->ibool[static_cast<size_t>(e) * NGLL2];
+      const int *ib = &d.ibool[static_cast<size_t>(e) * NGLL2];
       for (int q = 0; q < NGLL2; ++q) {
         const int g = ib[q];
         accel[2 * g] = accel[2 * g] - c[2 * q];
         accel[2 * g + 1] = accel[2 * g + 1] - c[2 * q + 1];
       }
     }
-    // mass matrix and corrector (compute_forces_viscoelastic_calling_routine.F90:181,
-    // update_displacement_Newmark.F90:564-589)
-    for (int g = 0; g < 2 * nglob; ++g) {
-      accel[g] = accel[g] * o.rmass[g];
-      veloc[g] = veloc[g] + o.deltatover2 * accel[g];
-    }
-    // receivers (write_seismograms.F90:150-190, compute_interpolated_dva.f90:34-97)
-    if (seis) {
-      const real *field = d->seismotype == 2 ? veloc : (d->seismotype == 3 ? accel : displ);
-      for (int r = 0; r < d->nrec; ++r) {
-        const int e = d->rec_ispec[r];
-        double vx = 0.0, vz = 0.0;
-        for (int j = 0; j < NGLL; ++j)
-          for (int i = 0; i < NGLL; ++i) {
-            const int g = d->ibool[static_cast<size_t>(e) * NGLL2 + j * NGLL + i];
-            const double h = d->hxir[r * NGLL + i] * d->hgammar[r * NGLL + j];
-            vx = vx + static_cast<double>(field[2 * g]) * h;
-            vz = vz + static_cast<double>(field[2 * g + 1]) * h;
-          }
-        double *out = &seis[(static_cast<size_t>(r) * nstep + s) * 2];
-        out[0] = d->cosrot * vx + d->sinrot * vz;
-        out[1] = -d->sinrot * vx + d->cosrot * vz;
-      }
+  }
+
+  void record(double *seis, int nstep, int s) {
+    if (!seis) return;
+    const std::vector<real> &field = d.seismotype == 2 ? veloc : (d.seismotype == 3 ? accel : displ);
+    for (int r = 0; r < d.nrec; ++r) {
+      const int e = d.rec_ispec[r];
+      double vx = 0.0, vz = 0.0;
+      for (int j = 0; j < NGLL; ++j)
+        for (int i = 0; i < NGLL; ++i) {
+          const int g = d.ibool[static_cast<size_t>(e) * NGLL2 + j * NGLL + i];
+          const double h = d.hxir[r * NGLL + i] * d.hgammar[r * NGLL + j];
+          vx = vx + static_cast<double>(field[2 * g]) * h;
+          vz = vz + static_cast<double>(field[2 * g + 1]) * h;
+        }
+      double *out = &seis[(static_cast<size_t>(r) * nstep + s) * 2];
+      out[0] = d.cosrot * vx + d.sinrot * vz;
+      out[1] = -d.sinrot * vx + d.cosrot * vz;
     }
   }
-  return 0;
-}
+
+  int run(int nstep, double *seis, int nthreads) override {
+    const int nt = nthreads > 0 ? nthreads : default_threads();
+    const size_t ng = static_cast<size_t>(nglob) * 2;
+    for (int s = 0; s < nstep; ++s, ++it) {
+      if (d.time_scheme == 1) {
+        // predictor (update_displacement_Newmark.F90:408-454)
+        for (size_t g = 0; g < ng; ++g) {
+          displ[g] = displ[g] + deltat * veloc[g] + deltatsquareover2 * accel[g];
+          veloc[g] = veloc[g] + deltatover2 * accel[g];
+          accel[g] = 0;
+        }
+        forces(0, nt);
+        // mass matrix and corrector (compute_forces_viscoelastic_calling_routine.F90:181,
+        // update_displacement_Newmark.F90:564-589)
+        for (size_t g = 0; g < ng; ++g) {
+          accel[g] = accel[g] * rmass[g];
+          veloc[g] = veloc[g] + deltatover2 * accel[g];
+        }
+      } else {
+        for (int stage = 0; stage < 6; ++stage) {
+          // iterate_time.F90:167-181 clears accel, then forces and the LDDRK update
+          // (update_displacement_LDDRK.F90:55-79)
+          std::fill(accel.begin(), accel.end(), real(0));
+          forces(stage, nt);
+          const real al = alpha[stage], be = beta[stage];
+          for (size_t g = 0; g < ng; ++g) {
+            accel[g] = accel[g] * rmass[g];
+            veloc_l[g] = al * veloc_l[g] + deltat * accel[g];
+            displ_l[g] = al * displ_l[g] + deltat * veloc[g];
+            veloc[g] = veloc[g] + be * veloc_l[g];
+            displ[g] = displ[g] + be * displ_l[g];
+          }
+        }
+      }
+      // receivers (write_seismograms.F90:150-190, compute_interpolated_dva.f90:34-97)
+      record(seis, nstep, s);
+    }
+    return 0;
+  }
+
+  std::vector<real> *field(int which) {
+    switch (which) {
+      case SF2D_OR_DISPL: return &displ;
+      case SF2D_OR_VELOC: return &veloc;
+      case SF2D_OR_ACCEL: return &accel;
+      case SF2D_OR_DISPL_LDDRK: return &displ_l;
+      case SF2D_OR_VELOC_LDDRK: return &veloc_l;
+      case SF2D_OR_E1: return &e1;
+      case SF2D_OR_E11: return &e11;
+      case SF2D_OR_E13: return &e13;
+      default: return nullptr;
+    }
+  }
+  int get(int which, void *out) override {
+    auto *f = field(which);
+    if (!f || !out) return -1;
+    std::memcpy(out, f->data(), f->size() * sizeof(real));
+    return 0;
+  }
+  int set(int which, const void *in) override {
+    auto *f = field(which);
+    if (!f || !in) return -1;
+    std::memcpy(f->data(), in, f->size() * sizeof(real));
+    return 0;
+  }
+};
 
 }  // namespace
 
-extern "C" int sf2d_oracle_newmark_elastic(const sf2d_oracle_db *db, int precision, int it0, int nstep,
-                                           void *displ, void *veloc, void *accel, double *seis,
-                                           int nthreads) {
-  if (!db || !displ || !veloc || !accel || nstep < 0 || it0 < 0) return -1;
-  if (it0 + nstep > db->nstep_total && db->nsrc > 0) return -2;
-  if (precision == 4)
-    return run_newmark<float>(db, it0, nstep, static_cast<float *>(displ), static_cast<float *>(veloc),
-                              static_cast<float *>(accel), seis, nthreads);
-  if (precision == 8)
-    return run_newmark<double>(db, it0, nstep, static_cast<double *>(displ), static_cast<double *>(veloc),
-                               static_cast<double *>(accel), seis, nthreads);
-  return -3;
+extern "C" void *sf2d_oracle_create(const sf2d_oracle_db *db, int precision) {
+  if (!db || db->nspec <= 0 || db->nglob <= 0 || !db->ibool) return nullptr;
+  if (db->time_scheme != 1 && db->time_scheme != 2) return nullptr;
+  if (db->time_scheme == 2 && (!db->alpha_lddrk || !db->beta_lddrk)) return nullptr;
+  if (precision == 4) return static_cast<StateBase *>(new State<float>(db));
+  if (precision == 8) return static_cast<StateBase *>(new State<double>(db));
+  return nullptr;
 }
+
+extern "C" int sf2d_oracle_run(void *h, int nstep, double *seis, int nthreads) {
+  if (!h || nstep < 0) return -1;
+  return static_cast<StateBase *>(h)->run(nstep, seis, nthreads);
+}
+
+extern "C" int sf2d_oracle_get(void *h, int which, void *out) {
+  return h ? static_cast<StateBase *>(h)->get(which, out) : -1;
+}
+
+extern "C" int sf2d_oracle_set(void *h, int which, const void *in) {
+  return h ? static_cast<StateBase *>(h)->set(which, in) : -1;
+}
+
+extern "C" void sf2d_oracle_destroy(void *h) { delete static_cast<StateBase *>(h); }
 
 extern "C" int sf2d_oracle_max_threads(void) { return default_threads(); }

@@ -9,10 +9,12 @@
  * Parity pin: seismograms of the reference's EXAMPLES/Tromp2005_kernel run
  * (REF_SEIS/AA.S0001.BX?.semd) are reproduced by setup + this oracle (see
  * tests/test_oracle_golden.py).  The reference binary itself cannot be built
- * (no Fortran compiler), so 1e-5-level parity to xspecfem2D is unpinned.
+ * (no Fortran compiler), so parity to xspecfem2D is pinned through its golden
+ * outputs only.
  *
  * All arrays use the solver layout: per-element GLL arrays [ispec][j][i]
- * (25 values per element), global vectors [iglob][component], 0-based ids.
+ * (25 values per element), global vectors [iglob][component], attenuation
+ * arrays [ispec][j][i][i_sls] with N_SLS = 3, 0-based ids.
  */
 #ifndef SF2D_ORACLE_H
 #define SF2D_ORACLE_H
@@ -49,16 +51,39 @@ typedef struct {
   /* anisotropy (may be NULL): per-element flag and c11,c13,c15,c33,c35,c55 */
   const int *ispec_is_anisotropic;
   const double *c11, *c13, *c15, *c33, *c35, *c55;
+  /* time scheme: 1 Newmark, 2 LDDRK (6 stages, coefficients in CUSTOM_REAL) */
+  int time_scheme;
+  const double *alpha_lddrk, *beta_lddrk;                 /* 6 each */
+  /* viscoelastic 3-SLS (may be NULL): Newmark recursive-convolution
+   * coefficients A/B (prepare_attenuation.f90:378-396) and the LDDRK
+   * inverse relaxation times and weights (attenuation_model.f90:114-125).
+   * All zero at a point means no attenuation there. */
+  const double *att_a1, *att_b1, *att_a2, *att_b2;        /* nspec*25*3 */
+  const double *att_itau1, *att_phi1, *att_itau2, *att_phi2;
 } sf2d_oracle_db;
 
-/* Runs `nstep` Newmark steps starting at step index `it0` (0-based) on the
- * fields in/out (displ, veloc, accel: nglob*2 each, caller-owned, same
- * precision as `precision`: 4 -> float, 8 -> double).  Seismograms are
- * written to seis (nrec*nstep*2 doubles, [irec][it][comp]).  nthreads <= 0
- * uses all host threads (or SF2D_ORACLE_THREADS).  Returns 0 on success, <0 on bad arguments. */
-int sf2d_oracle_newmark_elastic(const sf2d_oracle_db *db, int precision, int it0, int nstep,
-                                void *displ, void *veloc, void *accel, double *seis,
-                                int nthreads);
+/* Fields addressed by sf2d_oracle_get/set. */
+enum {
+  SF2D_OR_DISPL = 0, SF2D_OR_VELOC = 1, SF2D_OR_ACCEL = 2,
+  SF2D_OR_DISPL_LDDRK = 3, SF2D_OR_VELOC_LDDRK = 4,
+  SF2D_OR_E1 = 5, SF2D_OR_E11 = 6, SF2D_OR_E13 = 7
+};
+
+/* Creates an oracle state (fields zero).  precision: 4 -> float, 8 -> double.
+ * Returns NULL on bad arguments. */
+void *sf2d_oracle_create(const sf2d_oracle_db *db, int precision);
+
+/* Advances nstep time steps.  seis (may be NULL): nrec*nstep*2 doubles,
+ * [irec][it][comp].  nthreads <= 0 uses all host threads (or
+ * SF2D_ORACLE_THREADS).  Returns 0 on success. */
+int sf2d_oracle_run(void *h, int nstep, double *seis, int nthreads);
+
+/* Copy a field out of / into the state, in the state's precision.  Sizes:
+ * DISPL..VELOC_LDDRK nglob*2, E1..E13 nspec*25*3. */
+int sf2d_oracle_get(void *h, int which, void *out);
+int sf2d_oracle_set(void *h, int which, const void *in);
+
+void sf2d_oracle_destroy(void *h);
 
 /* Number of host threads the oracle uses by default. */
 int sf2d_oracle_max_threads(void);

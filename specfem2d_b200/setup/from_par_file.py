@@ -42,13 +42,14 @@ def _receivers_from_par(par, top_interface):
 PAR_KEYS = ("NSTEP", "DT", "time_stepping_scheme", "NGNOD", "xmin", "xmax", "nx", "absorbbottom",
             "absorbright", "absorbtop", "absorbleft", "STACEY_ABSORBING_CONDITIONS", "USER_T0",
             "anglerec", "nrec", "xdeb", "zdeb", "xfin", "zfin", "record_at_surface_same_vertical",
-            "seismotype", "materials", "regions", "ATTENUATION_VISCOELASTIC", "PML_BOUNDARY_CONDITIONS")
+            "seismotype", "materials", "regions", "ATTENUATION_VISCOELASTIC", "PML_BOUNDARY_CONDITIONS",
+            "ATTENUATION_f0_REFERENCE", "NELEM_PML_THICKNESS")
 
 
-def config_from_data_dir(data_dir: str) -> dict:
+def config_from_data_dir(data_dir: str, par_file: str = "Par_file", source_file: str = "SOURCE") -> dict:
     """Parse Par_file, SOURCE and the interfaces file of a DATA/ directory into a plain dict."""
-    par = read_par_file(os.path.join(data_dir, "Par_file"))
-    srcs = read_source_file(os.path.join(data_dir, "SOURCE"))
+    par = read_par_file(os.path.join(data_dir, par_file))
+    srcs = read_source_file(os.path.join(data_dir, source_file))
     ifile = str(par["interfacesfile"]).strip()
     cand = [os.path.join(data_dir, ifile), os.path.join(data_dir, os.path.basename(ifile))]
     ipath = next(p for p in cand if os.path.exists(p))
@@ -66,8 +67,12 @@ def database_from_data_dir(data_dir: str, nstep: int | None = None):
     return database_from_config(cfg, nstep), cfg
 
 
-def database_from_config(cfg: dict, nstep: int | None = None):
-    """Build the Database from a parsed example configuration."""
+def database_from_config(cfg: dict, nstep: int | None = None, absorbing_as_stacey: bool = False):
+    """Build the Database from a parsed example configuration.
+
+    ``absorbing_as_stacey`` puts Stacey conditions on the absorbing edges of
+    an example that uses CPML (for comparisons on a time window that ends
+    before boundary reflections reach the receivers)."""
     par = cfg
     srcs = cfg["sources"]
     interfaces = [(list(x), list(z)) for (x, z) in cfg["interfaces"]]
@@ -80,12 +85,23 @@ def database_from_config(cfg: dict, nstep: int | None = None):
     rho = np.zeros((mesh.nspec, NGLL, NGLL))
     vp = np.zeros_like(rho)
     vs = np.zeros_like(rho)
+    qk = np.full_like(rho, 9999.0)
+    qm = np.full_like(rho, 9999.0)
+    ckeys = ("c11", "c13", "c15", "c33", "c35", "c55")
+    cstore = {k: np.zeros_like(rho) for k in ckeys}
+    is_aniso = np.zeros(mesh.nspec, dtype=bool)
     for (ix0, ix1, iz0, iz1, imat) in par["regions"]:
         m = mats[imat]
         for iz in range(iz0, iz1 + 1):
             for ix in range(ix0, ix1 + 1):
                 e = (iz - 1) * mesh.nx + (ix - 1)
                 rho[e], vp[e], vs[e] = m["rho"], m["vp"], m["vs"]
+                qk[e], qm[e] = m["qkappa"], m["qmu"]
+                if m["kind"] == 2:
+                    is_aniso[e] = True
+                    for k in ckeys:
+                        cstore[k][e] = m[k]
+    atten = bool(par.get("ATTENUATION_VISCOELASTIC", False))
     sources = []
     for s in srcs:
         sources.append(Source(x=float(s["xs"]), z=float(s["zs"]), source_type=int(s["source_type"]),
@@ -95,8 +111,14 @@ def database_from_config(cfg: dict, nstep: int | None = None):
                               factor=float(s["factor"])))
     recs = _receivers_from_par(par, interfaces[-1])
     n = int(par["NSTEP"]) if nstep is None else nstep
+    stacey = bool(par["STACEY_ABSORBING_CONDITIONS"]) or (
+        absorbing_as_stacey and bool(par.get("PML_BOUNDARY_CONDITIONS", False)))
     db = build_database(mesh, rho, vp, vs, sources, recs, n, float(par["DT"]),
-                        stacey=bool(par["STACEY_ABSORBING_CONDITIONS"]), external_model=False,
+                        stacey=stacey, external_model=False,
                         time_scheme=int(par["time_stepping_scheme"]), user_t0=float(par["USER_T0"]),
-                        anglerec_deg=float(par["anglerec"]))
+                        anglerec_deg=float(par["anglerec"]),
+                        qkappa=qk if atten else None, qmu=qm if atten else None,
+                        attenuation_f0=float(par.get("ATTENUATION_f0_REFERENCE", 1.0)))
+    if is_aniso.any():
+        db.aniso = {"ispec": is_aniso, **{k: v.astype(np.float32) for k, v in cstore.items()}}
     return db

@@ -8,6 +8,7 @@ Fortran literals such as ``2.0d-2`` and ``.true.`` are converted.
 """
 from __future__ import annotations
 
+import math
 import re
 
 
@@ -86,7 +87,21 @@ def read_stations(path: str) -> list:
 
 
 def material_from_row(row) -> dict:
-    """Isotropic material row ``n 1 rho vp vs 0 0 Qkappa Qmu ...`` (read_materials.f90:116-140)."""
+    """Material table row (read_materials.f90:116-215).
+
+    Isotropic ``n 1 rho vp vs 0 0 Qkappa Qmu ...``; anisotropic
+    ``n 2 rho c11 c13 c15 c33 c35 c55 c12 c23 c25 c22 Qkappa Qmu``, whose
+    cp = sqrt(c33/rho) and cs = sqrt(c55/rho) feed the isotropic stores used
+    by the mass matrix and Stacey.
+    """
     vals = [_fvalue(v) for v in row]
-    return dict(index=int(vals[0]), kind=int(vals[1]), rho=float(vals[2]), vp=float(vals[3]),
+    kind = int(vals[1])
+    if kind == 2:
+        rho = float(vals[2])
+        c = [float(v) for v in vals[3:9]]
+        qk = float(vals[13]) if len(vals) > 13 and float(vals[13]) > 0.1 else 9999.0
+        qm = float(vals[14]) if len(vals) > 14 and float(vals[14]) > 0.1 else 9999.0
+        return dict(index=int(vals[0]), kind=2, rho=rho, vp=math.sqrt(c[3] / rho), vs=math.sqrt(c[5] / rho),
+                    qkappa=qk, qmu=qm, c11=c[0], c13=c[1], c15=c[2], c33=c[3], c35=c[4], c55=c[5])
+    return dict(index=int(vals[0]), kind=kind, rho=float(vals[2]), vp=float(vals[3]),
                 vs=float(vals[4]), qkappa=float(vals[7]), qmu=float(vals[8]))

@@ -110,6 +110,11 @@ class Database:
     mesh: Mesh = None
     src_xi: np.ndarray = None
     src_gamma: np.ndarray = None
+    # viscoelastic 3-SLS coefficients per GLL point and SLS (None = elastic):
+    # keys a1, b1, a2, b2 (Newmark), itau1, phi1, itau2, phi2 (LDDRK), each (nspec, 5, 5, 3) f32
+    atten: dict = None
+    # anisotropy (None = isotropic): keys ispec (nspec,) bool, c11 c13 c15 c33 c35 c55 (nspec,5,5) f32
+    aniso: dict = None
 
     @property
     def deltat(self):
@@ -369,7 +374,8 @@ def compute_t0(sources, user_t0: float = 0.0):
 
 def build_database(mesh: Mesh, rho, vp, vs, sources, receivers_xz, nstep: int, dt: float,
                    stacey: bool = True, external_model: bool = True, time_scheme: int = 1,
-                   user_t0: float = 0.0, anglerec_deg: float = 0.0) -> Database:
+                   user_t0: float = 0.0, anglerec_deg: float = 0.0, qkappa=None, qmu=None,
+                   attenuation_f0: float | None = None) -> Database:
     """Run the host setup chain and return a Database.
 
     ``rho, vp, vs`` are per-GLL-point arrays (nspec,5,5) (external model) or
@@ -432,6 +438,15 @@ def build_database(mesh: Mesh, rho, vp, vs, sources, receivers_xz, nstep: int, d
         rec_ispec.append(e); rxi.append(xi); rgam.append(gamma)
         hxr.append(hx); hgr.append(hg); rxx.append(x); rzz.append(z)
     ang = anglerec_deg * PI / 180.0
+    atten = None
+    if qkappa is not None and qmu is not None:
+        from .attenuation import attenuation_arrays
+
+        f0_ref = attenuation_f0
+        if sources and sources[0].time_function_type not in (4, 5):
+            f0_ref = sources[0].f0  # prepare_attenuation.f90:319-321
+        atten = attenuation_arrays(np.broadcast_to(np.asarray(qkappa, dtype=np.float64), shp),
+                                   np.broadcast_to(np.asarray(qmu, dtype=np.float64), shp), f0_ref, dt)
     return Database(
         nspec=mesh.nspec, nglob=nglob, ibool=ibool.astype(np.int32),
         xix=geo["xix"], xiz=geo["xiz"], gammax=geo["gammax"], gammaz=geo["gammaz"],
@@ -447,4 +462,4 @@ def build_database(mesh: Mesh, rho, vp, vs, sources, receivers_xz, nstep: int, d
         rec_x=np.array(rxx), rec_z=np.array(rzz),
         cosrot=math.cos(ang), sinrot=math.sin(ang),
         nstep=nstep, dt=dt, t0=t0, time_scheme=time_scheme, gll=gll, mesh=mesh,
-        src_xi=np.array(sxi), src_gamma=np.array(sgam))
+        src_xi=np.array(sxi), src_gamma=np.array(sgam), atten=atten)

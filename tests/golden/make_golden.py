@@ -25,9 +25,15 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 from specfem2d_b200.setup.from_par_file import config_from_data_dir  # noqa: E402
 
 EXAMPLES = {
-    # name: (example dir, list of (station, component) traces)
-    "tromp2005_kernel": ("EXAMPLES/Tromp2005_kernel", [("S0001", "BXX"), ("S0001", "BXZ")]),
-    "anisotropic_isotropic_model": ("EXAMPLES/anisotropic_isotropic_model", [("S0001", "BXX"), ("S0001", "BXZ")]),
+    # name: (example dir, list of (station, component) traces, Par_file name, SOURCE name)
+    "tromp2005_kernel": ("EXAMPLES/Tromp2005_kernel", [("S0001", "BXX"), ("S0001", "BXZ")], "Par_file", "SOURCE"),
+    "anisotropic_isotropic_model": ("EXAMPLES/anisotropic_isotropic_model", [("S0001", "BXX"), ("S0001", "BXZ")],
+                                    "Par_file", "SOURCE"),
+    # REF_SEIS of this example was made with the "shared_by_four_elements" variant
+    # (its output.log locates the source at x = z = 1000 m)
+    "attenuation_viscoelastic": ("EXAMPLES/attenuation/viscoelastic", [("S0001", "BXX"), ("S0001", "BXZ")],
+                                 "Par_file_attenuation_2D_source_in_point_shared_by_four_elements",
+                                 "SOURCE_attenuation_2D_source_in_point_shared_by_four_elements"),
 }
 
 
@@ -48,9 +54,9 @@ def log_locations(path):
 
 
 def main(ref_root):
-    for name, (rel, traces) in EXAMPLES.items():
+    for name, (rel, traces, par_file, source_file) in EXAMPLES.items():
         ex = os.path.join(ref_root, rel)
-        cfg = config_from_data_dir(os.path.join(ex, "DATA"))
+        cfg = config_from_data_dir(os.path.join(ex, "DATA"), par_file, source_file)
         cfg["log_locations"] = log_locations(os.path.join(ex, "REF_SEIS", "output.log"))
         with open(os.path.join(HERE, name + ".json"), "w") as f:
             json.dump(cfg, f, indent=1, default=str)

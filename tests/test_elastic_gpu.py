@@ -109,7 +109,7 @@ def test_set_get_fields_roundtrip_and_restart(tromp):
     assert np.array_equal(d, d0) and not v.any() and not a.any()
     # restart from a random displacement: compare with the oracle
     o = oracle.Oracle(db, 4)
-    o.displ[:] = d0
+    o.set(oracle.DISPL, d0)
     ref = o.run(100)
     s = sol.run(100)
     assert rel_l2(s, ref) < TOL
