@@ -87,6 +87,19 @@ typedef struct {
   float deltat, deltatover2, deltatsquareover2;
   int tile_elems;                            /* elements per tile, 0 = default (64) */
   int threads_per_block;                     /* 128, 256 or 512; 0 = default (256) */
+  /* time scheme: 1 (or 0) Newmark, 2 LDDRK with 6 stages (update_displacement_LDDRK.F90);
+   * stf holds nstage values per step: stf[isrc][it][stage] */
+  int time_scheme;
+  int nstage;
+  const float *alpha_lddrk, *beta_lddrk;     /* 6 each (ALPHA_LDDRK, BETA_LDDRK) */
+  /* anisotropy (NULL = isotropic): per-element flag, c11 c13 c15 c33 c35 c55 per GLL point */
+  const int *ispec_is_anisotropic;
+  const float *c11, *c13, *c15, *c33, *c35, *c55;
+  /* viscoelastic 3 SLS (NULL = elastic), nspec*25*3 [ispec][j][i][sls]; all zero at a
+   * point = no attenuation there.  Newmark: A/B recursive-convolution coefficients
+   * (prepare_attenuation.f90:378-396); LDDRK: 1/tau_sigma and phi (attenuation_model.f90). */
+  const float *att_a1, *att_b1, *att_a2, *att_b2;
+  const float *att_itau1, *att_phi1, *att_itau2, *att_phi2;
 } sf2d_elastic_desc;
 
 /* Builds the tiled device layout and uploads everything (fields start at 0). */
@@ -124,8 +137,8 @@ int sf2d_get_stream(sf2d_solver *s, void **stream);
 
 /* Times `nstep` steps launched one kernel at a time with CUDA events around
  * each launch; writes the average milliseconds per launch of the element
- * kernel (ms[0]), the shared-point kernel (ms[1]) and their sum per step
- * (ms[2]).  The steps advance the wavefield like sf2d_run. */
+ * kernel (ms[0]), the shared-point kernel (ms[1]) and their sum per time step
+ * (ms[2], all LDDRK stages).  The steps advance the wavefield like sf2d_run. */
 int sf2d_time_kernels(sf2d_solver *s, int nstep, float *ms);
 
 /* Layout statistics: [ntiles, nshared points, max local points, max elements

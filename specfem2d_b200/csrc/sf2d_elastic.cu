@@ -1,24 +1,5 @@
-// Tile-staged fused Newmark step for the isotropic elastic SEM (NGLL = 5).
-//
-// One CTA advances one tile of elements by one time step:
-//   1. predictor u' = u + dt v + dt^2/2 a, v' = v + dt/2 a for every point
-//      the tile touches (update_displacement_Newmark.F90:408-454), staged in
-//      shared memory;
-//   2. Stacey traction on the predicted velocity and the force sources
-//      (compute_stacey_elastic.f90:160-335, compute_add_sources_viscoelastic.f90)
-//      by one thread in reference order;
-//   3. per GLL point: gradient through hprime, Jacobian mapping, isotropic
-//      stress (lambda and mu as compute_forces_viscoelastic.F90:286-294 forms
-//      them), weak-form terms
-//      (compute_forces_viscoelastic.F90:184-675);
-//   4. weighted transpose contraction with hprimewgll (:760-782);
-//   5. assembly into the shared-memory accumulator colour by colour
-//      (no two elements of a colour share a point, so no atomics);
-//   6. interior points: a *= rmass_inverse, v = v' + dt/2 a
-//      (update_displacement_Newmark.F90:564-589) and write-back; shared
-//      points: the tile's partial sum is written to its slot.
-// A second kernel finishes shared points, adding the partial sums in tile
-// order.  Results are bit-identical from run to run.
+// Host runtime and C ABI of the elastic time-marching path (see
+// sf2d_kernels.cuh for the device side and include/sf2d_b200.h for the API).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -32,343 +13,8 @@
 #include <vector>
 
 #include "sf2d_b200.h"
+#include "sf2d_kernels.cuh"
 #include "sf2d_tiler.h"
-
-namespace sf2d {
-
-struct Params {
-  float2 *u, *v, *a;
-  const float2 *rmass;
-  const TileInfo *tiles;
-  const uint16_t *lib;
-  const float4 *geo;   // xix, xiz, gammax, gammaz per element GLL point (tile slot order)
-  const float2 *mat;   // lambda, mu (lambda = rho*cp*cp - 2*mu in FP32, as the CPU solver forms it)
-  const int *sh_ids;
-  float2 *partial;
-  const int *shp_off, *shp_slots;
-  const int *st_local;
-  const float4 *st_nw;    // nx, nz, weight, 0
-  const float2 *st_rho;   // rho*vp, rho*vs
-  const int *src_local, *src_id;
-  const float2 *src_arr;
-  const float *stf;
-  const int *rec_id, *rec_dev;
-  const double *rec_h;    // 10 per receiver: hxir[5], hgammar[5]
-  double *seis;           // [irec][it][2]
-  int *d_step, *d_status;
-  int nstep_stf, nstep_seis, seismotype, nrec;
-  double cosrot, sinrot;
-  float dt, dto2, dt2o2;
-  int shared_begin, nshared;
-  int max_q, max_local;
-  float hconst[60];  // hprime[25], hprimewgll[25], wxgll[5], wzgll[5]
-};
-
-constexpr int BS = 256;
-
-__device__ __forceinline__ void record_receiver(const Params &P, int r, int step) {
-  if (step < 0 || step >= P.nstep_seis) return;
-  const float2 *field = P.seismotype == 2 ? P.v : (P.seismotype == 3 ? P.a : P.u);
-  const int *dev = P.rec_dev + 25 * r;
-  const double *h = P.rec_h + 10 * r;
-  double vx = 0.0, vz = 0.0;
-  for (int j = 0; j < 5; ++j)
-    for (int i = 0; i < 5; ++i) {
-      const float2 f = field[dev[j * 5 + i]];
-      const double hl = h[i] * h[5 + j];
-      vx += static_cast<double>(f.x) * hl;
-      vz += static_cast<double>(f.y) * hl;
-    }
-  double *out = P.seis + (static_cast<size_t>(P.rec_id[r]) * P.nstep_seis + step) * 2;
-  out[0] = P.cosrot * vx + P.sinrot * vz;
-  out[1] = -P.sinrot * vx + P.cosrot * vz;
-}
-
-__device__ __forceinline__ unsigned smem_addr(const void *p) {
-  return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void cp_async8(void *s, const void *g) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_addr(s)), "l"(g) : "memory");
-}
-__device__ __forceinline__ void cp_async16(void *s, const void *g) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(s)), "l"(g) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-
-// Shared-memory layout of one tile (sizes from the largest tile); every region
-// starts on a 16-byte boundary, as 16-byte cp.async destinations require:
-//   geo  float4[max_q]  xix, xiz, gammax, gammaz; overwritten by the weak-form terms
-//   mat  float2[max_q]  lambda, mu
-//   u, v, acc float2[max_local]  (old u, v, a -> predicted u, v and the accumulator)
-//   h    float[64]      hprime, hprimewgll, wxgll, wzgll
-//   lib  uint16[max_q rounded up to 8]
-struct TileSmem {
-  size_t geo, mat, u, v, acc, h, lib, total;
-};
-__host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~static_cast<size_t>(15); }
-__host__ __device__ inline TileSmem tile_smem_layout(int max_q, int max_local) {
-  TileSmem L;
-  size_t o = 0;
-  L.geo = o;
-  o = align16(o + static_cast<size_t>(max_q) * sizeof(float4));
-  L.mat = o;
-  o = align16(o + static_cast<size_t>(max_q) * sizeof(float2));
-  L.u = o;
-  o = align16(o + static_cast<size_t>(max_local) * sizeof(float2));
-  L.v = o;
-  o = align16(o + static_cast<size_t>(max_local) * sizeof(float2));
-  L.acc = o;
-  o = align16(o + static_cast<size_t>(max_local) * sizeof(float2));
-  L.h = o;
-  o = align16(o + 64 * sizeof(float));
-  L.lib = o;
-  o = align16(o + static_cast<size_t>((max_q + 7) / 8 * 8) * sizeof(uint16_t));
-  L.total = o;
-  return L;
-}
-
-template <int NT>
-__global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_prev) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  const TileInfo &ti = P.tiles[blockIdx.x];
-  const int tid = threadIdx.x;
-  const int n_int = ti.n_int;
-  const int n_sh = ti.n_sh;
-  const int nl = n_int + n_sh;
-  const int nq = ti.nelem * 25;
-  const int ebase = ti.elem_base * 25;
-  const int int_begin = ti.int_begin;
-  const TileSmem L = tile_smem_layout(P.max_q, P.max_local);
-  float4 *s_geo = reinterpret_cast<float4 *>(smem + L.geo);
-  float2 *s_mat = reinterpret_cast<float2 *>(smem + L.mat);
-  float2 *s_u = reinterpret_cast<float2 *>(smem + L.u);
-  float2 *s_v = reinterpret_cast<float2 *>(smem + L.v);
-  float2 *s_acc = reinterpret_cast<float2 *>(smem + L.acc);
-  float *s_h = reinterpret_cast<float *>(smem + L.h);
-  uint16_t *s_lib = reinterpret_cast<uint16_t *>(smem + L.lib);
-
-  const int step = *P.d_step;
-  // receivers of the previous step read the old fields before any write
-  if (record_prev && tid < ti.rec_n) record_receiver(P, ti.rec_off + tid, step - 1);
-
-  // 1. every load of the tile is issued at once, straight into shared memory
-  {
-    const uint4 *glib = reinterpret_cast<const uint4 *>(P.lib + ti.lib_off);
-    const int nlib16 = (nq + 7) / 8;
-    for (int k = tid; k < nlib16; k += NT) cp_async16(s_lib + 8 * k, glib + k);
-    for (int f = tid; f < nq; f += NT) {
-      cp_async16(s_geo + f, P.geo + ebase + f);
-      cp_async8(s_mat + f, P.mat + ebase + f);
-    }
-    for (int l = tid; l < n_int; l += NT) {
-      const int g = int_begin + l;
-      cp_async8(s_u + l, P.u + g);
-      cp_async8(s_v + l, P.v + g);
-      cp_async8(s_acc + l, P.a + g);
-    }
-    for (int k = tid; k < n_sh; k += NT) {
-      const int g = P.sh_ids[ti.sh_off + k];
-      cp_async8(s_u + n_int + k, P.u + g);
-      cp_async8(s_v + n_int + k, P.v + g);
-      cp_async8(s_acc + n_int + k, P.a + g);
-    }
-    if (tid < 60) s_h[tid] = P.hconst[tid];
-    cp_async_wait_all();
-  }
-  __syncthreads();
-
-  // 2. Newmark predictor in place
-  const float dt = P.dt, dto2 = P.dto2, dt2o2 = P.dt2o2;
-  for (int l = tid; l < nl; l += NT) {
-    float2 u = s_u[l], v = s_v[l];
-    const float2 a = s_acc[l];
-    u.x = u.x + dt * v.x + dt2o2 * a.x;
-    u.y = u.y + dt * v.y + dt2o2 * a.y;
-    v.x = v.x + dto2 * a.x;
-    v.y = v.y + dto2 * a.y;
-    s_u[l] = u;
-    s_v[l] = v;
-    s_acc[l] = make_float2(0.f, 0.f);
-  }
-  __syncthreads();
-
-  // 3. boundary terms and sources in reference order, one thread (overlaps pass 1)
-  if (tid == 0) {
-    for (int p = ti.st_off; p < ti.st_off + ti.st_n; ++p) {
-      const int l = P.st_local[p];
-      const float4 nw = P.st_nw[p];
-      const float2 rr = P.st_rho[p];
-      const float2 v = s_v[l];
-      const float vn = nw.x * v.x + nw.y * v.y;
-      const float tx = rr.x * vn * nw.x + rr.y * (v.x - vn * nw.x);
-      const float tz = rr.x * vn * nw.y + rr.y * (v.y - vn * nw.y);
-      float2 acc = s_acc[l];
-      acc.x -= tx * nw.z;
-      acc.y -= tz * nw.z;
-      s_acc[l] = acc;
-    }
-    for (int p = ti.src_off; p < ti.src_off + ti.src_n; ++p) {
-      const int l = P.src_local[p];
-      const float f = step < P.nstep_stf ? P.stf[static_cast<size_t>(P.src_id[p]) * P.nstep_stf + step] : 0.f;
-      const float2 sa = P.src_arr[p];
-      float2 acc = s_acc[l];
-      acc.x += sa.x * f;
-      acc.y += sa.y * f;
-      s_acc[l] = acc;
-    }
-  }
-
-  // 4. element pass 1: gradient, stress, weak-form terms (written over the geometry)
-  for (int f = tid; f < nq; f += NT) {
-    const int e = f / 25;
-    const int q = f - 25 * e;
-    const int j = q / 5;
-    const int i = q - 5 * j;
-    const uint16_t *le = s_lib + 25 * e;
-    float dux_dxi = 0.f, duz_dxi = 0.f, dux_dg = 0.f, duz_dg = 0.f;
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-      const float2 r = s_u[le[5 * j + k]];
-      const float hx = s_h[5 * i + k];
-      dux_dxi += r.x * hx;
-      duz_dxi += r.y * hx;
-      const float2 c = s_u[le[5 * k + i]];
-      const float hz = s_h[5 * j + k];
-      dux_dg += c.x * hz;
-      duz_dg += c.y * hz;
-    }
-    const float4 g4 = s_geo[f];
-    const float2 m2 = s_mat[f];
-    const float xixl = g4.x, xizl = g4.y, gammaxl = g4.z, gammazl = g4.w;
-    const float jacobianl = 1.f / (xixl * gammazl - gammaxl * xizl);
-    const float dux_dxl = dux_dxi * xixl + dux_dg * gammaxl;
-    const float dux_dzl = dux_dxi * xizl + dux_dg * gammazl;
-    const float duz_dxl = duz_dxi * xixl + duz_dg * gammaxl;
-    const float duz_dzl = duz_dxi * xizl + duz_dg * gammazl;
-    const float mul = m2.y;
-    const float lambdal = m2.x;
-    const float lambdaplus2mu = lambdal + 2.f * mul;
-    const float sxx = lambdaplus2mu * dux_dxl + lambdal * duz_dzl;
-    const float szz = lambdaplus2mu * duz_dzl + lambdal * dux_dxl;
-    const float sxz = mul * (duz_dxl + dux_dzl);
-    s_geo[f] = make_float4(jacobianl * (sxx * xixl + sxz * xizl), jacobianl * (sxz * xixl + szz * xizl),
-                           jacobianl * (sxx * gammaxl + sxz * gammazl), jacobianl * (sxz * gammaxl + szz * gammazl));
-  }
-  __syncthreads();
-
-  // 5. weighted transpose contraction assembled straight into the accumulator,
-  //    one colour at a time (elements of a colour share no point)
-  int cb = 0;
-  for (int c = 0; c < ti.ncol; ++c) {
-    const int ce = ti.col_end[c] * 25;
-    for (int f = cb + tid; f < ce; f += NT) {
-      const int e = f / 25;
-      const int q = f - 25 * e;
-      const int j = q / 5;
-      const int i = q - 5 * j;
-      const float4 *te = s_geo + 25 * e;
-      float tx1 = 0.f, tz1 = 0.f, tx2 = 0.f, tz2 = 0.f;
-#pragma unroll
-      for (int k = 0; k < 5; ++k) {
-        const float4 r = te[5 * j + k];
-        const float w1 = s_h[25 + 5 * k + i];
-        tx1 += r.x * w1;
-        tz1 += r.y * w1;
-        const float4 cc = te[5 * k + i];
-        const float w2 = s_h[25 + 5 * k + j];
-        tx2 += cc.z * w2;
-        tz2 += cc.w * w2;
-      }
-      const float wz = s_h[55 + j], wx = s_h[50 + i];
-      const int l = s_lib[f];
-      float2 acc = s_acc[l];
-      acc.x -= wz * tx1 + wx * tx2;
-      acc.y -= wz * tz1 + wx * tz2;
-      s_acc[l] = acc;
-    }
-    cb = ce;
-    __syncthreads();
-  }
-
-  // 6. mass matrix, corrector, write-back
-  bool bad = false;
-  for (int l = tid; l < nl; l += NT) {
-    const float2 acc = s_acc[l];
-    if (l < n_int) {
-      const int g = int_begin + l;
-      const float2 rm = P.rmass[g];
-      const float2 a = make_float2(acc.x * rm.x, acc.y * rm.y);
-      float2 v = s_v[l];
-      v.x = v.x + dto2 * a.x;
-      v.y = v.y + dto2 * a.y;
-      const float2 u = s_u[l];
-      P.u[g] = u;
-      P.v[g] = v;
-      P.a[g] = a;
-      bad |= !(fabsf(u.x) < 1e25f && fabsf(u.y) < 1e25f);
-    } else {
-      P.partial[ti.sh_off + l - n_int] = acc;
-    }
-  }
-  if (bad) *P.d_status = 1;
-}
-
-__global__ void __launch_bounds__(BS) k_elastic_shared(const Params P) {
-  const int s = blockIdx.x * BS + threadIdx.x;
-  if (s < P.nshared) {
-    const int g = P.shared_begin + s;
-    float2 u = P.u[g], v = P.v[g];
-    const float2 a0 = P.a[g];
-    u.x = u.x + P.dt * v.x + P.dt2o2 * a0.x;
-    u.y = u.y + P.dt * v.y + P.dt2o2 * a0.y;
-    v.x = v.x + P.dto2 * a0.x;
-    v.y = v.y + P.dto2 * a0.y;
-    float2 acc = make_float2(0.f, 0.f);
-    for (int k = P.shp_off[s]; k < P.shp_off[s + 1]; ++k) {
-      const float2 p = P.partial[P.shp_slots[k]];
-      acc.x += p.x;
-      acc.y += p.y;
-    }
-    const float2 rm = P.rmass[g];
-    const float2 a = make_float2(acc.x * rm.x, acc.y * rm.y);
-    v.x = v.x + P.dto2 * a.x;
-    v.y = v.y + P.dto2 * a.y;
-    P.u[g] = u;
-    P.v[g] = v;
-    P.a[g] = a;
-    if (!(fabsf(u.x) < 1e25f && fabsf(u.y) < 1e25f)) *P.d_status = 1;
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) *P.d_step = *P.d_step + 1;
-}
-
-// records the step before *d_step for every receiver
-__global__ void k_receivers(const Params P) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r < P.nrec) record_receiver(P, r, *P.d_step - 1);
-}
-
-__global__ void k_permute_in(const float2 *src, const int *dev2glob, float2 *dst, int n) {
-  const int d = blockIdx.x * blockDim.x + threadIdx.x;
-  if (d < n) dst[d] = src[dev2glob[d]];
-}
-
-__global__ void k_permute_out(const float2 *src, const int *dev2glob, float2 *dst, int n) {
-  const int d = blockIdx.x * blockDim.x + threadIdx.x;
-  if (d < n) dst[dev2glob[d]] = src[d];
-}
-
-__global__ void k_max_norm(const float2 *u, int n, unsigned int *out) {
-  float m = 0.f;
-  for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < n; d += gridDim.x * blockDim.x) {
-    const float2 x = u[d];
-    const float nn = sqrtf(x.x * x.x + x.y * x.y);
-    m = (nn == nn) ? fmaxf(m, nn) : __int_as_float(0x7f800000);
-  }
-  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
-}
-
-}  // namespace sf2d
 
 // ---------------------------------------------------------------------------
 // host runtime
@@ -391,6 +37,30 @@ int fail(int code, const std::string &msg) {
   } while (0)
 
 }  // namespace
+
+namespace sf2d {
+
+using TileKernel = void (*)(Params, int, int);
+
+template <int NT>
+TileKernel pick_tile_kernel(bool aniso, bool atten, bool lddrk) {
+  if (aniso) {
+    if (atten) return lddrk ? k_elastic_tile<NT, true, true, true> : k_elastic_tile<NT, true, true, false>;
+    return lddrk ? k_elastic_tile<NT, true, false, true> : k_elastic_tile<NT, true, false, false>;
+  }
+  if (atten) return lddrk ? k_elastic_tile<NT, false, true, true> : k_elastic_tile<NT, false, true, false>;
+  return lddrk ? k_elastic_tile<NT, false, false, true> : k_elastic_tile<NT, false, false, false>;
+}
+
+TileKernel pick_tile_kernel(int nt, bool aniso, bool atten, bool lddrk) {
+  switch (nt) {
+    case 128: return pick_tile_kernel<128>(aniso, atten, lddrk);
+    case 512: return pick_tile_kernel<512>(aniso, atten, lddrk);
+    default: return pick_tile_kernel<256>(aniso, atten, lddrk);
+  }
+}
+
+}  // namespace sf2d
 
 struct sf2d_solver {
   sf2d::Params P{};
@@ -427,18 +97,27 @@ struct sf2d_solver {
     if (count) SF2D_CUDA(cudaMemcpy(*p, host, count * sizeof(T_), cudaMemcpyHostToDevice));
     return SF2D_OK;
   }
-  void launch_tile(bool record_prev) {
-    const int rp = record_prev ? 1 : 0;
-    switch (nt) {
-      case 128: sf2d::k_elastic_tile<128><<<T.ntiles, 128, smem, stream>>>(P, rp); break;
-      case 512: sf2d::k_elastic_tile<512><<<T.ntiles, 512, smem, stream>>>(P, rp); break;
-      default: sf2d::k_elastic_tile<256><<<T.ntiles, 256, smem, stream>>>(P, rp); break;
-    }
+  using TileFn = void (*)(sf2d::Params, int, int);
+  TileFn tile_fn = nullptr;
+  bool lddrk = false;
+  int nstage = 1;
+
+  void launch_tile(bool record_prev, int stage) {
+    tile_fn<<<T.ntiles, nt, smem, stream>>>(P, record_prev ? 1 : 0, stage);
+  }
+  void launch_shared(int stage) {
+    const int nb = std::max(1, (P.nshared + sf2d::SHARED_NT - 1) / sf2d::SHARED_NT);
+    const int last = stage == nstage - 1 ? 1 : 0;
+    if (lddrk)
+      sf2d::k_elastic_shared<true><<<nb, sf2d::SHARED_NT, 0, stream>>>(P, stage, last);
+    else
+      sf2d::k_elastic_shared<false><<<nb, sf2d::SHARED_NT, 0, stream>>>(P, stage, last);
   }
   int launch_step(bool record_prev) {
-    launch_tile(record_prev);
-    const int nb = std::max(1, (P.nshared + sf2d::BS - 1) / sf2d::BS);
-    sf2d::k_elastic_shared<<<nb, sf2d::BS, 0, stream>>>(P);
+    for (int st = 0; st < nstage; ++st) {
+      launch_tile(record_prev && st == 0, st);
+      launch_shared(st);
+    }
     return SF2D_OK;
   }
   int launch_receivers() {
@@ -477,6 +156,21 @@ extern "C" int sf2d_elastic_create(const sf2d_elastic_desc *d, sf2d_solver **out
   if (d->nstacey > 0 && (!d->st_iglob || !d->st_nx || !d->st_nz || !d->st_w || !d->st_rho_vp || !d->st_rho_vs))
     return fail(SF2D_ERR_INVALID, "missing Stacey arrays");
   if (d->seismotype < 1 || d->seismotype > 3) return fail(SF2D_ERR_INVALID, "seismotype must be 1, 2 or 3");
+  const int scheme = d->time_scheme == 0 ? 1 : d->time_scheme;
+  if (scheme != 1 && scheme != 2) return fail(SF2D_ERR_INVALID, "time_scheme must be 1 (Newmark) or 2 (LDDRK)");
+  const bool lddrk = scheme == 2;
+  const int nstage = lddrk ? 6 : 1;
+  if (lddrk && (!d->alpha_lddrk || !d->beta_lddrk)) return fail(SF2D_ERR_INVALID, "LDDRK needs alpha/beta");
+  if (d->nsrc > 0 && d->nstage != nstage)
+    return fail(SF2D_ERR_INVALID, "stf must hold one value per time step and stage");
+  const bool aniso = d->ispec_is_anisotropic != nullptr;
+  if (aniso && (!d->c11 || !d->c13 || !d->c15 || !d->c33 || !d->c35 || !d->c55))
+    return fail(SF2D_ERR_INVALID, "missing anisotropic coefficients");
+  const bool atten = lddrk ? (d->att_itau1 != nullptr) : (d->att_a1 != nullptr);
+  if (atten && !lddrk && (!d->att_b1 || !d->att_a2 || !d->att_b2))
+    return fail(SF2D_ERR_INVALID, "missing Newmark attenuation coefficients");
+  if (atten && lddrk && (!d->att_phi1 || !d->att_itau2 || !d->att_phi2))
+    return fail(SF2D_ERR_INVALID, "missing LDDRK attenuation coefficients");
 
   auto *S = new sf2d_solver();
   std::unique_ptr<sf2d_solver> guard(S);
@@ -500,6 +194,39 @@ extern "C" int sf2d_elastic_create(const sf2d_elastic_desc *d, sf2d_solver **out
     for (int q = 0; q < NGLL2; ++q) {
       geo[s * NGLL2 + q] = make_float4(d->xix[src + q], d->xiz[src + q], d->gammax[src + q], d->gammaz[src + q]);
       mat[s * NGLL2 + q] = make_float2(d->lambdastore[src + q], d->mustore[src + q]);
+    }
+  }
+  // anisotropic blocks, in slot order
+  std::vector<int> aniso_idx;
+  std::vector<float4> c4;
+  std::vector<float2> c2;
+  if (aniso) {
+    aniso_idx.assign(d->nspec, -1);
+    int na = 0;
+    for (int s = 0; s < d->nspec; ++s) {
+      const int e = T.elem_order[s];
+      if (!d->ispec_is_anisotropic[e]) continue;
+      aniso_idx[s] = na++;
+      const size_t src = static_cast<size_t>(e) * NGLL2;
+      for (int q = 0; q < NGLL2; ++q) {
+        c4.push_back(make_float4(d->c11[src + q], d->c13[src + q], d->c15[src + q], d->c33[src + q]));
+        c2.push_back(make_float2(d->c35[src + q], d->c55[src + q]));
+      }
+    }
+  }
+  // attenuation coefficients: 3 float4 per element point, slot order
+  std::vector<float4> att_coef;
+  if (atten) {
+    att_coef.resize(nq * 3);
+    const float *k0 = lddrk ? d->att_itau1 : d->att_a1, *k1 = lddrk ? d->att_itau2 : d->att_a2;
+    const float *k2 = lddrk ? d->att_phi1 : d->att_b1, *k3 = lddrk ? d->att_phi2 : d->att_b2;
+    for (int s = 0; s < d->nspec; ++s) {
+      const size_t src = static_cast<size_t>(T.elem_order[s]) * NGLL2;
+      for (int q = 0; q < NGLL2; ++q)
+        for (int l = 0; l < 3; ++l) {
+          const size_t o = (src + q) * 3 + l;
+          att_coef[(static_cast<size_t>(s) * NGLL2 + q) * 3 + l] = make_float4(k0[o], k1[o], k2[o], k3[o]);
+        }
     }
   }
   std::vector<float2> rmass(d->nglob);
@@ -587,11 +314,41 @@ extern "C" int sf2d_elastic_create(const sf2d_elastic_desc *d, sf2d_solver **out
   UP(rec_id, int, rec_id);
   UP(rec_dev, int, rec_dev);
   UP(rec_h, double, rec_h);
+  if (aniso) {
+    UP(aniso_idx, int, aniso_idx);
+    UP(c4, float4, c4);
+    UP(c2, float2, c2);
+  }
+  if (atten) {
+    UP(att_coef, float4, att_coef);
+    float4 *st = nullptr;
+    if ((rc = S->alloc(&st, nq * 3))) return rc;
+    SF2D_CUDA(cudaMemset(st, 0, sizeof(float4) * nq * 3));
+    P.att_state = st;
+    if (lddrk) {
+      float4 *stl = nullptr;
+      if ((rc = S->alloc(&stl, nq * 3))) return rc;
+      SF2D_CUDA(cudaMemset(stl, 0, sizeof(float4) * nq * 3));
+      P.att_state_l = stl;
+    }
+  }
+  if (lddrk) {
+    float2 *ul, *vl;
+    if ((rc = S->alloc(&ul, d->nglob)) || (rc = S->alloc(&vl, d->nglob))) return rc;
+    SF2D_CUDA(cudaMemset(ul, 0, sizeof(float2) * d->nglob));
+    SF2D_CUDA(cudaMemset(vl, 0, sizeof(float2) * d->nglob));
+    P.uL = ul;
+    P.vL = vl;
+    for (int k = 0; k < 6; ++k) {
+      P.alpha[k] = d->alpha_lddrk[k];
+      P.beta[k] = d->beta_lddrk[k];
+    }
+  }
 #undef UP
   float2 *partial;
   if ((rc = S->alloc(&partial, T.sh_ids.size()))) return rc;
   P.partial = partial;
-  std::vector<float> stf(static_cast<size_t>(d->nsrc) * d->nstep);
+  std::vector<float> stf(static_cast<size_t>(d->nsrc) * d->nstep * nstage);
   if (d->nsrc) std::memcpy(stf.data(), d->stf, stf.size() * sizeof(float));
   float *d_stf;
   if ((rc = S->upload(&d_stf, stf.data(), stf.size()))) return rc;
@@ -609,6 +366,7 @@ extern "C" int sf2d_elastic_create(const sf2d_elastic_desc *d, sf2d_solver **out
   if ((rc = S->alloc(&S->d_stage, d->nglob))) return rc;
   if ((rc = S->alloc(&S->d_norm, 1))) return rc;
   P.nstep_stf = d->nstep;
+  P.nstage = nstage;
   P.nstep_seis = d->nstep;
   P.seismotype = d->seismotype;
   P.nrec = d->nrec;
@@ -638,11 +396,10 @@ extern "C" int sf2d_elastic_create(const sf2d_elastic_desc *d, sf2d_solver **out
     for (const TileInfo &t : tiles)
       if (t.rec_n > S->nt) return fail(SF2D_ERR_INVALID, "more receivers in one tile than threads per CTA");
   }
-  SF2D_CUDA(cudaFuncSetAttribute(k_elastic_tile<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(S->smem)));
-  SF2D_CUDA(cudaFuncSetAttribute(k_elastic_tile<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(S->smem)));
-  SF2D_CUDA(cudaFuncSetAttribute(k_elastic_tile<512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  S->tile_fn = pick_tile_kernel(S->nt, aniso, atten, lddrk);
+  S->lddrk = lddrk;
+  S->nstage = nstage;
+  SF2D_CUDA(cudaFuncSetAttribute(S->tile_fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(S->smem)));
   S->nglob = d->nglob;
   S->nrec = d->nrec;
@@ -783,32 +540,35 @@ extern "C" int sf2d_get_stream(sf2d_solver *S, void **stream) {
 
 extern "C" int sf2d_time_kernels(sf2d_solver *S, int nstep, float *ms) {
   if (!S || !ms || nstep <= 0) return fail(SF2D_ERR_INVALID, "bad arguments");
-  std::vector<cudaEvent_t> ev(3 * nstep);
+  const int ns = S->nstage;
+  std::vector<cudaEvent_t> ev(static_cast<size_t>(3) * nstep * ns);
   for (auto &e : ev) SF2D_CUDA(cudaEventCreate(&e));
-  for (int k = 0; k < nstep; ++k) {
-    SF2D_CUDA(cudaEventRecord(ev[3 * k], S->stream));
-    S->launch_tile(k > 0);
-    SF2D_CUDA(cudaEventRecord(ev[3 * k + 1], S->stream));
-    const int nb = std::max(1, (S->P.nshared + sf2d::BS - 1) / sf2d::BS);
-    sf2d::k_elastic_shared<<<nb, sf2d::BS, 0, S->stream>>>(S->P);
-    SF2D_CUDA(cudaEventRecord(ev[3 * k + 2], S->stream));
-  }
+  for (int k = 0; k < nstep; ++k)
+    for (int st = 0; st < ns; ++st) {
+      const size_t b = (static_cast<size_t>(k) * ns + st) * 3;
+      SF2D_CUDA(cudaEventRecord(ev[b], S->stream));
+      S->launch_tile(k > 0 && st == 0, st);
+      SF2D_CUDA(cudaEventRecord(ev[b + 1], S->stream));
+      S->launch_shared(st);
+      SF2D_CUDA(cudaEventRecord(ev[b + 2], S->stream));
+    }
   S->launch_receivers();
   SF2D_CUDA(cudaGetLastError());
   SF2D_CUDA(cudaStreamSynchronize(S->stream));
-  double a = 0, b = 0;
-  for (int k = 0; k < nstep; ++k) {
+  double a = 0, bsum = 0;
+  for (size_t k = 0; k < ev.size(); k += 3) {
     float x = 0, y = 0;
-    cudaEventElapsedTime(&x, ev[3 * k], ev[3 * k + 1]);
-    cudaEventElapsedTime(&y, ev[3 * k + 1], ev[3 * k + 2]);
+    cudaEventElapsedTime(&x, ev[k], ev[k + 1]);
+    cudaEventElapsedTime(&y, ev[k + 1], ev[k + 2]);
     a += x;
-    b += y;
+    bsum += y;
   }
   for (auto &e : ev) cudaEventDestroy(e);
   S->steps_done += nstep;
-  ms[0] = static_cast<float>(a / nstep);
-  ms[1] = static_cast<float>(b / nstep);
-  ms[2] = static_cast<float>((a + b) / nstep);
+  const double nl = static_cast<double>(nstep) * ns;
+  ms[0] = static_cast<float>(a / nl);
+  ms[1] = static_cast<float>(bsum / nl);
+  ms[2] = static_cast<float>((a + bsum) / nstep);
   return SF2D_OK;
 }
 

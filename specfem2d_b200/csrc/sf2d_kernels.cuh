@@ -1,0 +1,495 @@
+// Device side of the tile-staged elastic time step (NGLL = 5).
+//
+// One CTA advances one tile of elements by one Newmark step or one LDDRK
+// stage:
+//   1. cp.async of the tile's local ibool, geometry, material and the fields
+//      of all its points straight into shared memory;
+//   2. Newmark predictor u' = u + dt v + dt^2/2 a, v' = v + dt/2 a
+//      (update_displacement_Newmark.F90:408-454) in shared memory, or a
+//      cleared accumulator for an LDDRK stage (iterate_time.F90:167-181);
+//   3. Stacey traction on the (predicted) velocity and the sources, by one
+//      thread in reference order (compute_stacey_elastic.f90:160-335,
+//      compute_add_sources_viscoelastic.f90:36-101);
+//   4. per GLL point: gradient through hprime, Jacobian mapping, isotropic
+//      (lambda, mu as compute_forces_viscoelastic.F90:286-294 forms them) or
+//      anisotropic stress (:372-445, in double as the reference), 3-SLS
+//      memory variables and their stress correction
+//      (compute_attenuation_viscoelastic.f90:36-236, :481-503), weak-form
+//      terms (:669-675);
+//   5. weighted transpose contraction with hprimewgll (:760-782) assembled
+//      into the shared accumulator colour by colour (no two elements of a
+//      colour share a point: no atomics);
+//   6. interior points: a *= rmass_inverse, then the Newmark corrector
+//      (update_displacement_Newmark.F90:564-589) or the LDDRK update
+//      (update_displacement_LDDRK.F90:55-79), write-back; shared points: the
+//      tile's partial sum goes to its slot.
+// A second kernel finishes shared points, adding the partial sums in tile
+// order.  Results are bit-identical from run to run.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "sf2d_tiler.h"
+
+namespace sf2d {
+
+struct Params {
+  float2 *u, *v, *a;
+  float2 *uL, *vL;  // LDDRK auxiliary fields
+  const float2 *rmass;
+  const TileInfo *tiles;
+  const uint16_t *lib;
+  const float4 *geo;   // xix, xiz, gammax, gammaz per element GLL point (tile slot order)
+  const float2 *mat;   // lambda, mu (lambda = rho*cp*cp - 2*mu in FP32, as the CPU solver forms it)
+  const int *aniso_idx;  // per element slot: index of its anisotropic block, -1 when isotropic
+  const float4 *c4;      // c11, c13, c15, c33 per point of anisotropic elements
+  const float2 *c2;      // c35, c55
+  const float4 *att_coef;  // 3 per element point: Newmark {A1, A2, B1, B2}[sls], LDDRK {1/tau1, 1/tau2, phi1, phi2}[sls]
+  float4 *att_state;       // 3 per element point: {e1[0..2], e11[0]}, {e11[1..2], e13[0..1]}, {e13[2], old strains}
+  float4 *att_state_l;     // LDDRK: e1_LDDRK, e11_LDDRK, e13_LDDRK with the same packing
+  const int *sh_ids;
+  float2 *partial;
+  const int *shp_off, *shp_slots;
+  const int *st_local;
+  const float4 *st_nw;    // nx, nz, weight, 0
+  const float2 *st_rho;   // rho*vp, rho*vs
+  const int *src_local, *src_id;
+  const float2 *src_arr;
+  const float *stf;       // [isrc][it][stage]
+  const int *rec_id, *rec_dev;
+  const double *rec_h;    // 10 per receiver: hxir[5], hgammar[5]
+  double *seis;           // [irec][it][2]
+  int *d_step, *d_status;
+  int nstep_stf, nstage, nstep_seis, seismotype, nrec;
+  double cosrot, sinrot;
+  float dt, dto2, dt2o2;
+  float alpha[6], beta[6];
+  int shared_begin, nshared;
+  int max_q, max_local;
+  float hconst[60];  // hprime[25], hprimewgll[25], wxgll[5], wzgll[5]
+};
+
+constexpr int SHARED_NT = 256;
+
+__device__ __forceinline__ void record_receiver(const Params &P, int r, int step) {
+  if (step < 0 || step >= P.nstep_seis) return;
+  const float2 *field = P.seismotype == 2 ? P.v : (P.seismotype == 3 ? P.a : P.u);
+  const int *dev = P.rec_dev + 25 * r;
+  const double *h = P.rec_h + 10 * r;
+  double vx = 0.0, vz = 0.0;
+  for (int j = 0; j < 5; ++j)
+    for (int i = 0; i < 5; ++i) {
+      const float2 f = field[dev[j * 5 + i]];
+      const double hl = h[i] * h[5 + j];
+      vx += static_cast<double>(f.x) * hl;
+      vz += static_cast<double>(f.y) * hl;
+    }
+  double *out = P.seis + (static_cast<size_t>(P.rec_id[r]) * P.nstep_seis + step) * 2;
+  out[0] = P.cosrot * vx + P.sinrot * vz;
+  out[1] = -P.sinrot * vx + P.cosrot * vz;
+}
+
+__device__ __forceinline__ unsigned smem_addr(const void *p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void cp_async8(void *s, const void *g) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_addr(s)), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *s, const void *g) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(s)), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Shared-memory layout of one tile (sizes from the largest tile); every region
+// starts on a 16-byte boundary, as 16-byte cp.async destinations require:
+//   geo  float4[max_q]  xix, xiz, gammax, gammaz; overwritten by the weak-form terms
+//   mat  float2[max_q]  lambda, mu
+//   u, v, acc float2[max_local]  (old u, v, a -> predicted u, v and the accumulator)
+//   h    float[64]      hprime, hprimewgll, wxgll, wzgll
+//   lib  uint16[max_q rounded up to 8]
+struct TileSmem {
+  size_t geo, mat, u, v, acc, h, lib, total;
+};
+__host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~static_cast<size_t>(15); }
+__host__ __device__ inline TileSmem tile_smem_layout(int max_q, int max_local) {
+  TileSmem L;
+  size_t o = 0;
+  L.geo = o;
+  o = align16(o + static_cast<size_t>(max_q) * sizeof(float4));
+  L.mat = o;
+  o = align16(o + static_cast<size_t>(max_q) * sizeof(float2));
+  L.u = o;
+  o = align16(o + static_cast<size_t>(max_local) * sizeof(float2));
+  L.v = o;
+  o = align16(o + static_cast<size_t>(max_local) * sizeof(float2));
+  L.acc = o;
+  o = align16(o + static_cast<size_t>(max_local) * sizeof(float2));
+  L.h = o;
+  o = align16(o + 64 * sizeof(float));
+  L.lib = o;
+  o = align16(o + static_cast<size_t>((max_q + 7) / 8 * 8) * sizeof(uint16_t));
+  L.total = o;
+  return L;
+}
+
+// Memory-variable update of one element point (Newmark recursive convolution or
+// LDDRK ADE stage); returns the sums of e1, e11, e13 over the SLS.
+template <bool LDDRK>
+__device__ __forceinline__ void attenuation_point(const Params &P, size_t pa, float dux_dxl, float dux_dzl,
+                                                  float duz_dxl, float duz_dzl, int stage, float &e1s,
+                                                  float &e11s, float &e13s) {
+  const float4 c0 = P.att_coef[pa], c1 = P.att_coef[pa + 1], c2 = P.att_coef[pa + 2];
+  float4 s0 = P.att_state[pa], s1 = P.att_state[pa + 1], s2 = P.att_state[pa + 2];
+  float e1[3] = {s0.x, s0.y, s0.z}, e11[3] = {s0.w, s1.x, s1.y}, e13[3] = {s1.z, s1.w, s2.x};
+  const float4 cc[3] = {c0, c1, c2};
+  const float theta_n = dux_dxl + duz_dzl;
+  if (!LDDRK) {
+    const float old_xx = s2.y, old_zz = s2.z, old_xz = s2.w;
+    const float theta_n1 = old_xx + old_zz;
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+      float a = cc[s].x;
+      e1[s] = a * a * e1[s] + cc[s].z * (theta_n + a * theta_n1);
+      a = cc[s].y;
+      e11[s] = a * a * e11[s] + cc[s].w * (dux_dxl - theta_n / 2.f + a * (old_xx - theta_n1 / 2.f));
+      e13[s] = a * a * e13[s] + cc[s].w * (dux_dzl + duz_dxl + a * old_xz);
+    }
+    s2.y = dux_dxl;
+    s2.z = duz_dzl;
+    s2.w = dux_dzl + duz_dxl;
+  } else {
+    float4 l0 = P.att_state_l[pa], l1 = P.att_state_l[pa + 1], l2 = P.att_state_l[pa + 2];
+    float e1l[3] = {l0.x, l0.y, l0.z}, e11l[3] = {l0.w, l1.x, l1.y}, e13l[3] = {l1.z, l1.w, l2.x};
+    const float al = P.alpha[stage], be = P.beta[stage];
+    const double dt = static_cast<double>(P.dt);
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+      const double itau1 = cc[s].x, itau2 = cc[s].y;
+      const float phi1 = cc[s].z, phi2 = cc[s].w;
+      // 1/tau_sigma is a double in the reference: these products are double there too
+      e1l[s] = static_cast<float>(static_cast<double>(al * e1l[s]) +
+                                  dt * (static_cast<double>(theta_n * phi1) - static_cast<double>(e1[s]) * itau1));
+      e1[s] = e1[s] + be * e1l[s];
+      e11l[s] = static_cast<float>(static_cast<double>(al * e11l[s] + P.dt * ((dux_dxl - theta_n / 2.f) * phi2)) -
+                                   dt * (static_cast<double>(e11[s]) * itau2));
+      e11[s] = e11[s] + be * e11l[s];
+      e13l[s] = static_cast<float>(static_cast<double>(al * e13l[s] + P.dt * ((dux_dzl + duz_dxl) * phi2)) -
+                                   dt * (static_cast<double>(e13[s]) * itau2));
+      e13[s] = e13[s] + be * e13l[s];
+    }
+    P.att_state_l[pa] = make_float4(e1l[0], e1l[1], e1l[2], e11l[0]);
+    P.att_state_l[pa + 1] = make_float4(e11l[1], e11l[2], e13l[0], e13l[1]);
+    P.att_state_l[pa + 2] = make_float4(e13l[2], 0.f, 0.f, 0.f);
+  }
+  P.att_state[pa] = make_float4(e1[0], e1[1], e1[2], e11[0]);
+  P.att_state[pa + 1] = make_float4(e11[1], e11[2], e13[0], e13[1]);
+  P.att_state[pa + 2] = make_float4(e13[2], s2.y, s2.z, s2.w);
+  e1s = e1[0] + e1[1] + e1[2];
+  e11s = e11[0] + e11[1] + e11[2];
+  e13s = e13[0] + e13[1] + e13[2];
+}
+
+template <int NT, bool ANISO, bool ATTEN, bool LDDRK>
+__global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_prev, int stage) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const TileInfo &ti = P.tiles[blockIdx.x];
+  const int tid = threadIdx.x;
+  const int n_int = ti.n_int;
+  const int n_sh = ti.n_sh;
+  const int nl = n_int + n_sh;
+  const int nq = ti.nelem * 25;
+  const int ebase = ti.elem_base * 25;
+  const int int_begin = ti.int_begin;
+  const TileSmem L = tile_smem_layout(P.max_q, P.max_local);
+  float4 *s_geo = reinterpret_cast<float4 *>(smem + L.geo);
+  float2 *s_mat = reinterpret_cast<float2 *>(smem + L.mat);
+  float2 *s_u = reinterpret_cast<float2 *>(smem + L.u);
+  float2 *s_v = reinterpret_cast<float2 *>(smem + L.v);
+  float2 *s_acc = reinterpret_cast<float2 *>(smem + L.acc);
+  float *s_h = reinterpret_cast<float *>(smem + L.h);
+  uint16_t *s_lib = reinterpret_cast<uint16_t *>(smem + L.lib);
+
+  const int step = *P.d_step;
+  // receivers of the previous step read the old fields before any write
+  if (record_prev && tid < ti.rec_n) record_receiver(P, ti.rec_off + tid, step - 1);
+
+  // 1. every load of the tile is issued at once, straight into shared memory
+  {
+    const uint4 *glib = reinterpret_cast<const uint4 *>(P.lib + ti.lib_off);
+    const int nlib16 = (nq + 7) / 8;
+    for (int k = tid; k < nlib16; k += NT) cp_async16(s_lib + 8 * k, glib + k);
+    for (int f = tid; f < nq; f += NT) {
+      cp_async16(s_geo + f, P.geo + ebase + f);
+      cp_async8(s_mat + f, P.mat + ebase + f);
+    }
+    for (int l = tid; l < n_int; l += NT) {
+      const int g = int_begin + l;
+      cp_async8(s_u + l, P.u + g);
+      cp_async8(s_v + l, P.v + g);
+      if (!LDDRK) cp_async8(s_acc + l, P.a + g);
+    }
+    for (int k = tid; k < n_sh; k += NT) {
+      const int g = P.sh_ids[ti.sh_off + k];
+      cp_async8(s_u + n_int + k, P.u + g);
+      cp_async8(s_v + n_int + k, P.v + g);
+      if (!LDDRK) cp_async8(s_acc + n_int + k, P.a + g);
+    }
+    if (tid < 60) s_h[tid] = P.hconst[tid];
+    cp_async_wait_all();
+  }
+  __syncthreads();
+
+  // 2. Newmark predictor in place, or a cleared accumulator for an LDDRK stage
+  const float dt = P.dt, dto2 = P.dto2, dt2o2 = P.dt2o2;
+  for (int l = tid; l < nl; l += NT) {
+    if (!LDDRK) {
+      float2 u = s_u[l], v = s_v[l];
+      const float2 a = s_acc[l];
+      u.x = u.x + dt * v.x + dt2o2 * a.x;
+      u.y = u.y + dt * v.y + dt2o2 * a.y;
+      v.x = v.x + dto2 * a.x;
+      v.y = v.y + dto2 * a.y;
+      s_u[l] = u;
+      s_v[l] = v;
+    }
+    s_acc[l] = make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+
+  // 3. boundary terms and sources in reference order, one thread (overlaps pass 1)
+  if (tid == 0) {
+    for (int p = ti.st_off; p < ti.st_off + ti.st_n; ++p) {
+      const int l = P.st_local[p];
+      const float4 nw = P.st_nw[p];
+      const float2 rr = P.st_rho[p];
+      const float2 v = s_v[l];
+      const float vn = nw.x * v.x + nw.y * v.y;
+      const float tx = rr.x * vn * nw.x + rr.y * (v.x - vn * nw.x);
+      const float tz = rr.x * vn * nw.y + rr.y * (v.y - vn * nw.y);
+      float2 acc = s_acc[l];
+      acc.x -= tx * nw.z;
+      acc.y -= tz * nw.z;
+      s_acc[l] = acc;
+    }
+    for (int p = ti.src_off; p < ti.src_off + ti.src_n; ++p) {
+      const int l = P.src_local[p];
+      const float f = step < P.nstep_stf
+                          ? P.stf[(static_cast<size_t>(P.src_id[p]) * P.nstep_stf + step) * P.nstage + stage]
+                          : 0.f;
+      const float2 sa = P.src_arr[p];
+      float2 acc = s_acc[l];
+      acc.x += sa.x * f;
+      acc.y += sa.y * f;
+      s_acc[l] = acc;
+    }
+  }
+
+  // 4. element pass 1: gradient, stress, memory variables, weak-form terms
+  for (int f = tid; f < nq; f += NT) {
+    const int e = f / 25;
+    const int q = f - 25 * e;
+    const int j = q / 5;
+    const int i = q - 5 * j;
+    const uint16_t *le = s_lib + 25 * e;
+    float dux_dxi = 0.f, duz_dxi = 0.f, dux_dg = 0.f, duz_dg = 0.f;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      const float2 r = s_u[le[5 * j + k]];
+      const float hx = s_h[5 * i + k];
+      dux_dxi += r.x * hx;
+      duz_dxi += r.y * hx;
+      const float2 c = s_u[le[5 * k + i]];
+      const float hz = s_h[5 * j + k];
+      dux_dg += c.x * hz;
+      duz_dg += c.y * hz;
+    }
+    const float4 g4 = s_geo[f];
+    const float2 m2 = s_mat[f];
+    const float xixl = g4.x, xizl = g4.y, gammaxl = g4.z, gammazl = g4.w;
+    const float jacobianl = 1.f / (xixl * gammazl - gammaxl * xizl);
+    const float dux_dxl = dux_dxi * xixl + dux_dg * gammaxl;
+    const float dux_dzl = dux_dxi * xizl + dux_dg * gammazl;
+    const float duz_dxl = duz_dxi * xixl + duz_dg * gammaxl;
+    const float duz_dzl = duz_dxi * xizl + duz_dg * gammazl;
+    const float mul = m2.y;
+    const float lambdal = m2.x;
+    const float lambdaplus2mu = lambdal + 2.f * mul;
+    float sxx, szz, sxz;
+    int ai = -1;
+    if (ANISO) ai = P.aniso_idx[ti.elem_base + e];
+    if (ANISO && ai >= 0) {
+      const size_t ap = static_cast<size_t>(ai) * 25 + q;
+      const float4 ca = P.c4[ap];
+      const float2 cb = P.c2[ap];
+      const double c11 = ca.x, c13 = ca.y, c15 = ca.z, c33 = ca.w, c35 = cb.x, c55 = cb.y;
+      const double sh = static_cast<double>(duz_dxl) + static_cast<double>(dux_dzl);
+      sxx = static_cast<float>(c11 * dux_dxl + c13 * duz_dzl + c15 * sh);
+      szz = static_cast<float>(c13 * dux_dxl + c33 * duz_dzl + c35 * sh);
+      sxz = static_cast<float>(c15 * dux_dxl + c35 * duz_dzl + c55 * sh);
+    } else {
+      sxx = lambdaplus2mu * dux_dxl + lambdal * duz_dzl;
+      szz = lambdaplus2mu * duz_dzl + lambdal * dux_dxl;
+      sxz = mul * (duz_dxl + dux_dzl);
+    }
+    if (ATTEN) {
+      float e1s, e11s, e13s;
+      attenuation_point<LDDRK>(P, static_cast<size_t>(ebase + f) * 3, dux_dxl, dux_dzl, duz_dxl, duz_dzl, stage, e1s,
+                               e11s, e13s);
+      const float lambdalplusmul = lambdal + mul;
+      sxx = sxx + lambdalplusmul * e1s + 2.f * mul * e11s;
+      sxz = sxz + mul * e13s;
+      szz = szz + lambdalplusmul * e1s - 2.f * mul * e11s;
+    }
+    s_geo[f] = make_float4(jacobianl * (sxx * xixl + sxz * xizl), jacobianl * (sxz * xixl + szz * xizl),
+                           jacobianl * (sxx * gammaxl + sxz * gammazl), jacobianl * (sxz * gammaxl + szz * gammazl));
+  }
+  __syncthreads();
+
+  // 5. weighted transpose contraction assembled straight into the accumulator,
+  //    one colour at a time (elements of a colour share no point)
+  int cb = 0;
+  for (int c = 0; c < ti.ncol; ++c) {
+    const int ce = ti.col_end[c] * 25;
+    for (int f = cb + tid; f < ce; f += NT) {
+      const int e = f / 25;
+      const int q = f - 25 * e;
+      const int j = q / 5;
+      const int i = q - 5 * j;
+      const float4 *te = s_geo + 25 * e;
+      float tx1 = 0.f, tz1 = 0.f, tx2 = 0.f, tz2 = 0.f;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        const float4 r = te[5 * j + k];
+        const float w1 = s_h[25 + 5 * k + i];
+        tx1 += r.x * w1;
+        tz1 += r.y * w1;
+        const float4 cc = te[5 * k + i];
+        const float w2 = s_h[25 + 5 * k + j];
+        tx2 += cc.z * w2;
+        tz2 += cc.w * w2;
+      }
+      const float wz = s_h[55 + j], wx = s_h[50 + i];
+      const int l = s_lib[f];
+      float2 acc = s_acc[l];
+      acc.x -= wz * tx1 + wx * tx2;
+      acc.y -= wz * tz1 + wx * tz2;
+      s_acc[l] = acc;
+    }
+    cb = ce;
+    __syncthreads();
+  }
+
+  // 6. mass matrix, corrector or LDDRK update, write-back
+  bool bad = false;
+  for (int l = tid; l < nl; l += NT) {
+    const float2 acc = s_acc[l];
+    if (l < n_int) {
+      const int g = int_begin + l;
+      const float2 rm = P.rmass[g];
+      const float2 a = make_float2(acc.x * rm.x, acc.y * rm.y);
+      float2 v = s_v[l];
+      float2 u = s_u[l];
+      if (!LDDRK) {
+        v.x = v.x + dto2 * a.x;
+        v.y = v.y + dto2 * a.y;
+      } else {
+        const float al = P.alpha[stage], be = P.beta[stage];
+        float2 vl = P.vL[g], ul = P.uL[g];
+        vl.x = al * vl.x + dt * a.x;
+        vl.y = al * vl.y + dt * a.y;
+        ul.x = al * ul.x + dt * v.x;
+        ul.y = al * ul.y + dt * v.y;
+        v.x = v.x + be * vl.x;
+        v.y = v.y + be * vl.y;
+        u.x = u.x + be * ul.x;
+        u.y = u.y + be * ul.y;
+        P.vL[g] = vl;
+        P.uL[g] = ul;
+      }
+      P.u[g] = u;
+      P.v[g] = v;
+      P.a[g] = a;
+      bad |= !(fabsf(u.x) < 1e25f && fabsf(u.y) < 1e25f);
+    } else {
+      P.partial[ti.sh_off + l - n_int] = acc;
+    }
+  }
+  if (bad) *P.d_status = 1;
+}
+
+template <bool LDDRK>
+__global__ void __launch_bounds__(SHARED_NT) k_elastic_shared(const Params P, int stage, int last_stage) {
+  const int s = blockIdx.x * SHARED_NT + threadIdx.x;
+  if (s < P.nshared) {
+    const int g = P.shared_begin + s;
+    float2 u = P.u[g], v = P.v[g];
+    if (!LDDRK) {
+      const float2 a0 = P.a[g];
+      u.x = u.x + P.dt * v.x + P.dt2o2 * a0.x;
+      u.y = u.y + P.dt * v.y + P.dt2o2 * a0.y;
+      v.x = v.x + P.dto2 * a0.x;
+      v.y = v.y + P.dto2 * a0.y;
+    }
+    float2 acc = make_float2(0.f, 0.f);
+    for (int k = P.shp_off[s]; k < P.shp_off[s + 1]; ++k) {
+      const float2 p = P.partial[P.shp_slots[k]];
+      acc.x += p.x;
+      acc.y += p.y;
+    }
+    const float2 rm = P.rmass[g];
+    const float2 a = make_float2(acc.x * rm.x, acc.y * rm.y);
+    if (!LDDRK) {
+      v.x = v.x + P.dto2 * a.x;
+      v.y = v.y + P.dto2 * a.y;
+    } else {
+      const float al = P.alpha[stage], be = P.beta[stage];
+      float2 vl = P.vL[g], ul = P.uL[g];
+      vl.x = al * vl.x + P.dt * a.x;
+      vl.y = al * vl.y + P.dt * a.y;
+      ul.x = al * ul.x + P.dt * v.x;
+      ul.y = al * ul.y + P.dt * v.y;
+      v.x = v.x + be * vl.x;
+      v.y = v.y + be * vl.y;
+      u.x = u.x + be * ul.x;
+      u.y = u.y + be * ul.y;
+      P.vL[g] = vl;
+      P.uL[g] = ul;
+    }
+    P.u[g] = u;
+    P.v[g] = v;
+    P.a[g] = a;
+    if (!(fabsf(u.x) < 1e25f && fabsf(u.y) < 1e25f)) *P.d_status = 1;
+  }
+  if (last_stage && blockIdx.x == 0 && threadIdx.x == 0) *P.d_step = *P.d_step + 1;
+}
+
+// records the step before *d_step for every receiver
+__global__ void k_receivers(const Params P) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < P.nrec) record_receiver(P, r, *P.d_step - 1);
+}
+
+__global__ void k_permute_in(const float2 *src, const int *dev2glob, float2 *dst, int n) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d < n) dst[d] = src[dev2glob[d]];
+}
+
+__global__ void k_permute_out(const float2 *src, const int *dev2glob, float2 *dst, int n) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d < n) dst[dev2glob[d]] = src[d];
+}
+
+__global__ void k_max_norm(const float2 *u, int n, unsigned int *out) {
+  float m = 0.f;
+  for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < n; d += gridDim.x * blockDim.x) {
+    const float2 x = u[d];
+    const float nn = sqrtf(x.x * x.x + x.y * x.y);
+    m = (nn == nn) ? fmaxf(m, nn) : __int_as_float(0x7f800000);
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
+}
+
+}  // namespace sf2d

@@ -51,6 +51,12 @@ class ElasticDesc(ctypes.Structure):
         ("nstep", ctypes.c_int),
         ("deltat", ctypes.c_float), ("deltatover2", ctypes.c_float), ("deltatsquareover2", ctypes.c_float),
         ("tile_elems", ctypes.c_int), ("threads_per_block", ctypes.c_int),
+        ("time_scheme", ctypes.c_int), ("nstage", ctypes.c_int),
+        ("alpha_lddrk", _f), ("beta_lddrk", _f),
+        ("ispec_is_anisotropic", _i),
+        ("c11", _f), ("c13", _f), ("c15", _f), ("c33", _f), ("c35", _f), ("c55", _f),
+        ("att_a1", _f), ("att_b1", _f), ("att_a2", _f), ("att_b2", _f),
+        ("att_itau1", _f), ("att_phi1", _f), ("att_itau2", _f), ("att_phi2", _f),
     ]
 
 
@@ -171,7 +177,8 @@ class ElasticSolver:
         d.nsrc = len(db.source_ispec)
         d.src_ispec = i(db.source_ispec)
         d.sourcearrays = f(db.sourcearrays)
-        d.stf = f(db.stf[:, :, 0])
+        d.stf = f(db.stf)
+        d.nstage = int(db.stf.shape[2])
         d.nrec = len(db.rec_ispec)
         d.rec_ispec = i(db.rec_ispec)
         d.hxir, d.hgammar = dd(db.hxir), dd(db.hgammar)
@@ -182,6 +189,22 @@ class ElasticSolver:
                                                         float(db.deltatsquareover2))
         d.tile_elems = tile_elems
         d.threads_per_block = threads_per_block
+        from .setup.solver_setup import ALPHA_LDDRK, BETA_LDDRK
+
+        d.time_scheme = int(db.time_scheme)
+        d.alpha_lddrk, d.beta_lddrk = f(ALPHA_LDDRK), f(BETA_LDDRK)
+        an = getattr(db, "aniso", None)
+        if an is not None:
+            d.ispec_is_anisotropic = i(an["ispec"].astype(np.int32))
+            d.c11, d.c13, d.c15 = f(an["c11"]), f(an["c13"]), f(an["c15"])
+            d.c33, d.c35, d.c55 = f(an["c33"]), f(an["c35"]), f(an["c55"])
+        at = getattr(db, "atten", None)
+        if at is not None:
+            if int(db.time_scheme) == 1:
+                d.att_a1, d.att_b1, d.att_a2, d.att_b2 = f(at["a1"]), f(at["b1"]), f(at["a2"]), f(at["b2"])
+            else:
+                d.att_itau1, d.att_phi1 = f(at["itau1"]), f(at["phi1"])
+                d.att_itau2, d.att_phi2 = f(at["itau2"]), f(at["phi2"])
         h = ctypes.c_void_p()
         _check(lib.sf2d_elastic_create(ctypes.byref(d), ctypes.byref(h)))
         self._h = h

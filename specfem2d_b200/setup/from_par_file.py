@@ -67,7 +67,8 @@ def database_from_data_dir(data_dir: str, nstep: int | None = None):
     return database_from_config(cfg, nstep), cfg
 
 
-def database_from_config(cfg: dict, nstep: int | None = None, absorbing_as_stacey: bool = False):
+def database_from_config(cfg: dict, nstep: int | None = None, absorbing_as_stacey: bool = False,
+                         time_scheme: int | None = None):
     """Build the Database from a parsed example configuration.
 
     ``absorbing_as_stacey`` puts Stacey conditions on the absorbing edges of
@@ -115,7 +116,7 @@ def database_from_config(cfg: dict, nstep: int | None = None, absorbing_as_stace
         absorbing_as_stacey and bool(par.get("PML_BOUNDARY_CONDITIONS", False)))
     db = build_database(mesh, rho, vp, vs, sources, recs, n, float(par["DT"]),
                         stacey=stacey, external_model=False,
-                        time_scheme=int(par["time_stepping_scheme"]), user_t0=float(par["USER_T0"]),
+                        time_scheme=int(time_scheme or par["time_stepping_scheme"]), user_t0=float(par["USER_T0"]),
                         anglerec_deg=float(par["anglerec"]),
                         qkappa=qk if atten else None, qmu=qm if atten else None,
                         attenuation_f0=float(par.get("ATTENUATION_f0_REFERENCE", 1.0)))
