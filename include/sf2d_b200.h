@@ -149,6 +149,28 @@ int sf2d_destroy(sf2d_solver *s);
 
 const char *sf2d_last_error(void);
 
+/* ---- misfit gradient (forward/backward pair) ----
+ * sf2d_fwi_create builds a forward and an adjoint solver for one medium and
+ * source (Newmark only) and reserves checkpoint_every displacement frames plus
+ * one state checkpoint per checkpoint_every steps in device memory.
+ * rhostore/kappastore (nspec*25) are used for the final kernel scaling.
+ * Replaces the reference's SIMULATION_TYPE = 3 path with undo_attenuation
+ * checkpointing (iterate_time_undoatt.F90:35-653, compute_kernels.f90:75-292,
+ * save_adjoint_kernels.f90:79-141). */
+typedef struct sf2d_fwi sf2d_fwi;
+int sf2d_fwi_create(const sf2d_elastic_desc *desc, const float *rhostore, const float *kappastore,
+                    int checkpoint_every, sf2d_fwi **out);
+/* Forward run from rest over desc->nstep steps, saving the checkpoints;
+ * seismograms (may be NULL): nrec*nstep*2 doubles. */
+int sf2d_fwi_forward(sf2d_fwi *f, double *seismograms);
+/* Adjoint sweep with adjoint source adj_src[irec][it][comp] (nrec*nstep*2,
+ * time order; the residual for an L2 waveform misfit).  Writes the scaled
+ * kernels rho_kl, kappa_kl, mu_kl (nspec*25 each, [ispec][j][i]):
+ * rho_kl = -rho dt sum(a_adj . u), kappa_kl = -kappa dt sum(div div),
+ * mu_kl = -2 mu dt sum(eps:eps - 1/3 div div). */
+int sf2d_fwi_backward(sf2d_fwi *f, const float *adj_src, float *rho_kl, float *kappa_kl, float *mu_kl);
+int sf2d_fwi_destroy(sf2d_fwi *f);
+
 /* Host-only diagnostic, no GPU needed: builds the tiling of a mesh and checks
  * its invariants (one device id per point, local ibool consistent with
  * ibool, colours conflict-free, shared-point slots complete and in tile

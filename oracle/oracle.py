@@ -40,10 +40,11 @@ class OracleDb(ctypes.Structure):
         ("time_scheme", ctypes.c_int), ("alpha_lddrk", _dp), ("beta_lddrk", _dp),
         ("att_a1", _dp), ("att_b1", _dp), ("att_a2", _dp), ("att_b2", _dp),
         ("att_itau1", _dp), ("att_phi1", _dp), ("att_itau2", _dp), ("att_phi2", _dp),
+        ("adj_src", _dp),
     ]
 
 
-DISPL, VELOC, ACCEL, DISPL_LDDRK, VELOC_LDDRK, E1, E11, E13 = range(8)
+DISPL, VELOC, ACCEL, DISPL_LDDRK, VELOC_LDDRK, E1, E11, E13, ATT_OLD, RHO_KL, KAPPA_KL, MU_KL = range(12)
 
 
 def build() -> str:
@@ -70,6 +71,10 @@ def lib():
         for fn in (_lib.sf2d_oracle_get, _lib.sf2d_oracle_set):
             fn.restype = ctypes.c_int
             fn.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        _lib.sf2d_oracle_accumulate_kernels.restype = ctypes.c_int
+        _lib.sf2d_oracle_accumulate_kernels.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        _lib.sf2d_oracle_set_step.restype = ctypes.c_int
+        _lib.sf2d_oracle_set_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
         _lib.sf2d_oracle_destroy.restype = None
         _lib.sf2d_oracle_destroy.argtypes = [ctypes.c_void_p]
         _lib.sf2d_oracle_max_threads.restype = ctypes.c_int
@@ -79,7 +84,7 @@ def lib():
 class Oracle:
     """Holds converted arrays (kept alive) and an oracle state; runs the CPU time loop."""
 
-    def __init__(self, db, precision: int = 4, seismotype: int = 1, db64=None):
+    def __init__(self, db, precision: int = 4, seismotype: int = 1, db64=None, adj_src=None):
         """``db`` supplies the FP32 setup; ``db64`` (optional) the FP64 one for precision 8."""
         from specfem2d_b200.setup.solver_setup import ALPHA_LDDRK, BETA_LDDRK
 
@@ -155,6 +160,9 @@ class Oracle:
             s.att_a1, s.att_b1, s.att_a2, s.att_b2 = d(at["a1"]), d(at["b1"]), d(at["a2"]), d(at["b2"])
             s.att_itau1, s.att_phi1 = d(at["itau1"]), d(at["phi1"])
             s.att_itau2, s.att_phi2 = d(at["itau2"]), d(at["phi2"])
+        if adj_src is not None:
+            s.adj_src = d(adj_src)
+            s.nstep_total = int(np.asarray(adj_src).shape[1])
         self._keep = keep
         self.s = s
         self.h = lib().sf2d_oracle_create(ctypes.byref(s), precision)
@@ -172,7 +180,14 @@ class Oracle:
     def _size(self, which):
         if which <= VELOC_LDDRK:
             return (self.s.nglob, 2)
+        if which >= RHO_KL:
+            return (self.s.nspec, 5, 5)
         return (self.s.nspec, 5, 5, 3)
+
+    def accumulate_kernels(self, b_displ):
+        b = np.ascontiguousarray(b_displ, dtype=self.dtype).reshape(self.s.nglob, 2)
+        if lib().sf2d_oracle_accumulate_kernels(self.h, b.ctypes.data) != 0:
+            raise RuntimeError("kernel accumulation failed")
 
     def get(self, which):
         out = np.empty(self._size(which), dtype=self.dtype)
@@ -205,6 +220,65 @@ class Oracle:
             raise RuntimeError(f"oracle failed with status {rc}")
         self.it += nstep
         return seis
+
+
+def checkpoint_fields(o):
+    """Fields that define the state of a Newmark run (for segment checkpointing)."""
+    names = [DISPL, VELOC, ACCEL]
+    if o.db.atten is not None:
+        names += [E1, E11, E13, ATT_OLD]
+    return {k: o.get(k) for k in names}
+
+
+def gradient(db, observed, checkpoint_every=200, precision=4, nthreads=0):
+    """Misfit, synthetics and sensitivity kernels of the L2 waveform misfit
+    chi = 1/2 sum_r sum_it |s - d|^2 dt, with the adjoint source s - d.
+
+    Forward run with a state checkpoint every `checkpoint_every` steps, then,
+    segment by segment in reverse, the forward segment is recomputed from its
+    checkpoint (frames of the displacement kept) and the adjoint field is
+    advanced over it; adjoint step it is paired with forward step
+    NSTEP - it + 1 (src/specfem2D/iterate_time_undoatt.F90:193-601).  Returns
+    (chi, synthetics, rho_kl, kappa_kl, mu_kl) with the kernels scaled as
+    save_adjoint_kernels.f90:134-141 does.
+    """
+    nstep = db.nstep
+    fwd = Oracle(db, precision)
+    ckpts = {}
+    seis = np.zeros((db.rec_ispec.size, nstep, 2))
+    for s0 in range(0, nstep, checkpoint_every):
+        ckpts[s0] = checkpoint_fields(fwd)
+        n = min(checkpoint_every, nstep - s0)
+        seis[:, s0:s0 + n] = fwd.run(n, nthreads)
+    resid = seis - observed
+    dt = float(db.dt)
+    chi = 0.5 * float(np.sum(resid ** 2)) * dt
+    adj = Oracle(db, precision, adj_src=resid)
+    for s0 in sorted(ckpts, reverse=True):
+        n = min(checkpoint_every, nstep - s0)
+        rec = Oracle(db, precision)
+        for k, v in ckpts[s0].items():
+            rec.set(k, v)
+        rec.it = s0
+        _set_step(rec, s0)
+        frames = []
+        for _ in range(n):
+            rec.run(1, nthreads)
+            frames.append(rec.displ)
+        for k in range(n - 1, -1, -1):
+            adj.run(1, nthreads)
+            adj.accumulate_kernels(frames[k])
+    f = np.float32 if precision == 4 else np.float64
+    dtf = f(db.deltat) if precision == 4 else dt
+    rho_kl = (-db.rhostore.astype(f) * dtf) * adj.get(RHO_KL)
+    mu_kl = (-f(2.0) * db.mustore.astype(f) * dtf) * adj.get(MU_KL)
+    kappa_kl = (-db.kappastore.astype(f) * dtf) * adj.get(KAPPA_KL)
+    return chi, seis, rho_kl, kappa_kl, mu_kl
+
+
+def _set_step(o, it):
+    """Moves the state's step counter (source time functions are indexed by it)."""
+    lib().sf2d_oracle_set_step(o.h, it)
 
 
 def max_threads() -> int:

@@ -66,6 +66,8 @@ struct StateBase {
   virtual int run(int nstep, double *seis, int nthreads) = 0;
   virtual int get(int which, void *out) = 0;
   virtual int set(int which, const void *in) = 0;
+  virtual int accumulate(const void *b) = 0;
+  virtual void set_step(int it) = 0;
 };
 
 template <typename real>
@@ -84,7 +86,9 @@ struct State : StateBase {
   // state
   std::vector<real> displ, veloc, accel, displ_l, veloc_l;
   std::vector<real> e1, e11, e13, e1_l, e11_l, e13_l;      // nspec*25*3
-  std::vector<real> dux_dxl_old, duz_dzl_old, dxz_old;      // nspec*25
+  std::vector<real> att_old;                                // nspec*25*3: dux_dxl, duz_dzl, dux_dzl+duz_dxl
+  std::vector<real> rho_kl, kappa_kl, mu_kl;                // nspec*25
+  std::vector<real> adj;                                    // nrec*nstep*2
   std::vector<real> contrib;
   int it = 0;  // steps done
 
@@ -152,9 +156,7 @@ struct State : StateBase {
         e11_l.assign(na, 0);
         e13_l.assign(na, 0);
       }
-      dux_dxl_old.assign(nl, 0);
-      duz_dzl_old.assign(nl, 0);
-      dxz_old.assign(nl, 0);
+      att_old.assign(nl * 3, 0);
     }
     const size_t ng = static_cast<size_t>(nglob) * 2;
     displ.assign(ng, 0);
@@ -165,6 +167,10 @@ struct State : StateBase {
       veloc_l.assign(ng, 0);
     }
     contrib.assign(nl * 2, 0);
+    rho_kl.assign(nl, 0);
+    kappa_kl.assign(nl, 0);
+    mu_kl.assign(nl, 0);
+    if (d.adj_src) adj = cvt<real>(d.adj_src, static_cast<size_t>(d.nrec) * d.nstep_total * 2);
   }
 
   // Memory-variable update at one GLL point; returns the three sums.
@@ -175,14 +181,15 @@ struct State : StateBase {
     const real theta_n = dux_dxl + duz_dzl;
     real *E1 = &e1[p * NSLS], *E11 = &e11[p * NSLS], *E13 = &e13[p * NSLS];
     if (d.time_scheme == 1) {
-      const real theta_n1 = dux_dxl_old[p] + duz_dzl_old[p];
+      real *old = &att_old[p * 3];
+      const real theta_n1 = old[0] + old[1];
       for (int s = 0; s < NSLS; ++s) {
         const size_t q = p * NSLS + s;
         real a = a1[q];
         E1[s] = a * a * E1[s] + b1[q] * (theta_n + a * theta_n1);
         a = a2[q];
-        E11[s] = a * a * E11[s] + b2[q] * (dux_dxl - theta_n / real(2) + a * (dux_dxl_old[p] - theta_n1 / real(2)));
-        E13[s] = a * a * E13[s] + b2[q] * (dux_dzl + duz_dxl + a * dxz_old[p]);
+        E11[s] = a * a * E11[s] + b2[q] * (dux_dxl - theta_n / real(2) + a * (old[0] - theta_n1 / real(2)));
+        E13[s] = a * a * E13[s] + b2[q] * (dux_dzl + duz_dxl + a * old[2]);
       }
     } else {
       const real al = alpha[stage], be = beta[stage];
@@ -207,9 +214,10 @@ struct State : StateBase {
     e11s = E11[0] + E11[1] + E11[2];
     e13s = E13[0] + E13[1] + E13[2];
     if (d.time_scheme == 1) {
-      dux_dxl_old[p] = dux_dxl;
-      duz_dzl_old[p] = duz_dzl;
-      dxz_old[p] = dux_dzl + duz_dxl;
+      real *old = &att_old[p * 3];
+      old[0] = dux_dxl;
+      old[1] = duz_dzl;
+      old[2] = dux_dzl + duz_dxl;
     }
   }
 
@@ -303,7 +311,23 @@ struct State : StateBase {
       accel[2 * g] = accel[2 * g] - tx * st_w[p];
       accel[2 * g + 1] = accel[2 * g + 1] - tz * st_w[p];
     }
-    for (int isrc = 0; isrc < d.nsrc; ++isrc) {
+    if (d.adj_src) {
+      // adjoint sources at the receivers, time-reversed (compute_add_sources_viscoelastic.f90:351-405)
+      const int it_tmp = d.nstep_total - 1 - it;
+      for (int r = 0; r < d.nrec && it_tmp >= 0; ++r) {
+        const int e = d.rec_ispec[r];
+        const real ax = adj[(static_cast<size_t>(r) * d.nstep_total + it_tmp) * 2];
+        const real az = adj[(static_cast<size_t>(r) * d.nstep_total + it_tmp) * 2 + 1];
+        for (int j = 0; j < NGLL; ++j)
+          for (int i = 0; i < NGLL; ++i) {
+            const int g = d.ibool[static_cast<size_t>(e) * NGLL2 + j * NGLL + i];
+            const real h = static_cast<real>(d.hxir[r * NGLL + i]) * static_cast<real>(d.hgammar[r * NGLL + j]);
+            accel[2 * g] = accel[2 * g] + h * ax;
+            accel[2 * g + 1] = accel[2 * g + 1] + h * az;
+          }
+      }
+    }
+    for (int isrc = 0; isrc < d.nsrc && !d.adj_src; ++isrc) {
       real stf = 0;
       if (it < d.nstep_total)
         stf = static_cast<real>(d.stf[(static_cast<size_t>(isrc) * d.nstep_total + it) * d.nstage + stage]);
@@ -339,7 +363,9 @@ struct State : StateBase {
       for (int j = 0; j < NGLL; ++j)
         for (int i = 0; i < NGLL; ++i) {
           const int g = d.ibool[static_cast<size_t>(e) * NGLL2 + j * NGLL + i];
-          const double h = d.hxir[r * NGLL + i] * d.hgammar[r * NGLL + j];
+          // xir_store_loc and gammar_store_loc are CUSTOM_REAL: their product is formed in that precision
+          const double h = static_cast<double>(static_cast<real>(d.hxir[r * NGLL + i]) *
+                                               static_cast<real>(d.hgammar[r * NGLL + j]));
           vx = vx + static_cast<double>(field[2 * g]) * h;
           vz = vz + static_cast<double>(field[2 * g + 1]) * h;
         }
@@ -389,6 +415,57 @@ struct State : StateBase {
     return 0;
   }
 
+  // compute_kernels.f90:75-292 (P-SV): strains of both fields with the mapping
+  // derivatives read as double, kernel integrands accumulated in CUSTOM_REAL
+  void accumulate_kernels(const real *b) {
+    for (int e = 0; e < nspec; ++e) {
+      const size_t off = static_cast<size_t>(e) * NGLL2;
+      for (int j = 0; j < NGLL; ++j)
+        for (int i = 0; i < NGLL; ++i) {
+          real dux_dxi = 0, duz_dxi = 0, dux_dg = 0, duz_dg = 0;
+          real bdux_dxi = 0, bduz_dxi = 0, bdux_dg = 0, bduz_dg = 0;
+          for (int k = 0; k < NGLL; ++k) {
+            const int gr = d.ibool[off + j * NGLL + k], gc = d.ibool[off + k * NGLL + i];
+            dux_dxi = dux_dxi + displ[2 * gr] * hprime[i][k];
+            duz_dxi = duz_dxi + displ[2 * gr + 1] * hprime[i][k];
+            dux_dg = dux_dg + displ[2 * gc] * hprime[j][k];
+            duz_dg = duz_dg + displ[2 * gc + 1] * hprime[j][k];
+            bdux_dxi = bdux_dxi + b[2 * gr] * hprime[i][k];
+            bduz_dxi = bduz_dxi + b[2 * gr + 1] * hprime[i][k];
+            bdux_dg = bdux_dg + b[2 * gc] * hprime[j][k];
+            bduz_dg = bduz_dg + b[2 * gc + 1] * hprime[j][k];
+          }
+          const size_t p = off + j * NGLL + i;
+          const double xixl = xix[p], xizl = xiz[p], gammaxl = gammax[p], gammazl = gammaz[p];
+          const real dux_dxl = static_cast<real>(dux_dxi * xixl + dux_dg * gammaxl);
+          const real dux_dzl = static_cast<real>(dux_dxi * xizl + dux_dg * gammazl);
+          const real duz_dxl = static_cast<real>(duz_dxi * xixl + duz_dg * gammaxl);
+          const real duz_dzl = static_cast<real>(duz_dxi * xizl + duz_dg * gammazl);
+          const real bdux_dxl = static_cast<real>(bdux_dxi * xixl + bdux_dg * gammaxl);
+          const real bdux_dzl = static_cast<real>(bdux_dxi * xizl + bdux_dg * gammazl);
+          const real bduz_dxl = static_cast<real>(bduz_dxi * xixl + bduz_dg * gammaxl);
+          const real bduz_dzl = static_cast<real>(bduz_dxi * xizl + bduz_dg * gammazl);
+          const real dsxx = dux_dxl, dszz = duz_dzl;
+          const real dsxz = static_cast<real>(0.5 * (static_cast<double>(duz_dxl) + static_cast<double>(dux_dzl)));
+          const real bdsxx = bdux_dxl, bdszz = bduz_dzl;
+          const real bdsxz = static_cast<real>(0.5 * (static_cast<double>(bduz_dxl) + static_cast<double>(bdux_dzl)));
+          const real kappa_k = (dsxx + dszz) * (bdsxx + bdszz);
+          const real mu_k = dsxx * bdsxx + dszz * bdszz + real(2) * dsxz * bdsxz - real(1) / real(3) * kappa_k;
+          const int g = d.ibool[p];
+          const real rho_k = accel[2 * g] * b[2 * g] + accel[2 * g + 1] * b[2 * g + 1];
+          rho_kl[p] = rho_kl[p] + rho_k;
+          mu_kl[p] = mu_kl[p] + mu_k;
+          kappa_kl[p] = kappa_kl[p] + kappa_k;
+        }
+    }
+  }
+  void set_step(int step) override { it = step; }
+  int accumulate(const void *b) override {
+    if (!b) return -1;
+    accumulate_kernels(static_cast<const real *>(b));
+    return 0;
+  }
+
   std::vector<real> *field(int which) {
     switch (which) {
       case SF2D_OR_DISPL: return &displ;
@@ -399,6 +476,10 @@ struct State : StateBase {
       case SF2D_OR_E1: return &e1;
       case SF2D_OR_E11: return &e11;
       case SF2D_OR_E13: return &e13;
+      case SF2D_OR_ATT_OLD: return &att_old;
+      case SF2D_OR_RHO_KL: return &rho_kl;
+      case SF2D_OR_KAPPA_KL: return &kappa_kl;
+      case SF2D_OR_MU_KL: return &mu_kl;
       default: return nullptr;
     }
   }
@@ -438,6 +519,16 @@ extern "C" int sf2d_oracle_get(void *h, int which, void *out) {
 
 extern "C" int sf2d_oracle_set(void *h, int which, const void *in) {
   return h ? static_cast<StateBase *>(h)->set(which, in) : -1;
+}
+
+extern "C" int sf2d_oracle_accumulate_kernels(void *h, const void *b_displ) {
+  return h ? static_cast<StateBase *>(h)->accumulate(b_displ) : -1;
+}
+
+extern "C" int sf2d_oracle_set_step(void *h, int it) {
+  if (!h || it < 0) return -1;
+  static_cast<StateBase *>(h)->set_step(it);
+  return 0;
 }
 
 extern "C" void sf2d_oracle_destroy(void *h) { delete static_cast<StateBase *>(h); }

@@ -60,13 +60,20 @@ typedef struct {
    * All zero at a point means no attenuation there. */
   const double *att_a1, *att_b1, *att_a2, *att_b2;        /* nspec*25*3 */
   const double *att_itau1, *att_phi1, *att_itau2, *att_phi2;
+  /* adjoint simulation (SIMULATION_TYPE = 3): when adj_src is not NULL the
+   * force sources are replaced by the adjoint sources at the receivers,
+   * adj_src[irec][it][comp] in time order, injected time-reversed
+   * (compute_add_sources_viscoelastic.f90:351-405) */
+  const double *adj_src;
 } sf2d_oracle_db;
 
 /* Fields addressed by sf2d_oracle_get/set. */
 enum {
   SF2D_OR_DISPL = 0, SF2D_OR_VELOC = 1, SF2D_OR_ACCEL = 2,
   SF2D_OR_DISPL_LDDRK = 3, SF2D_OR_VELOC_LDDRK = 4,
-  SF2D_OR_E1 = 5, SF2D_OR_E11 = 6, SF2D_OR_E13 = 7
+  SF2D_OR_E1 = 5, SF2D_OR_E11 = 6, SF2D_OR_E13 = 7,
+  SF2D_OR_ATT_OLD = 8,                                   /* nspec*25*3: dux_dxl, duz_dzl, dux_dzl+duz_dxl of the last step */
+  SF2D_OR_RHO_KL = 9, SF2D_OR_KAPPA_KL = 10, SF2D_OR_MU_KL = 11  /* nspec*25, unscaled sums */
 };
 
 /* Creates an oracle state (fields zero).  precision: 4 -> float, 8 -> double.
@@ -82,6 +89,14 @@ int sf2d_oracle_run(void *h, int nstep, double *seis, int nthreads);
  * DISPL..VELOC_LDDRK nglob*2, E1..E13 nspec*25*3. */
 int sf2d_oracle_get(void *h, int which, void *out);
 int sf2d_oracle_set(void *h, int which, const void *in);
+
+/* Adds, at every element GLL point, the sensitivity-kernel integrands of the
+ * state's (adjoint) displacement and acceleration against the forward
+ * displacement b_displ (nglob*2, state precision): compute_kernels.f90:75-292. */
+int sf2d_oracle_accumulate_kernels(void *h, const void *b_displ);
+
+/* Sets the number of steps done (the source time functions are indexed by it). */
+int sf2d_oracle_set_step(void *h, int it);
 
 void sf2d_oracle_destroy(void *h);
 

@@ -16,130 +16,22 @@
 #include "sf2d_kernels.cuh"
 #include "sf2d_tiler.h"
 
-// ---------------------------------------------------------------------------
-// host runtime
-// ---------------------------------------------------------------------------
+#include "sf2d_runtime.h"
+
+namespace sf2d {
 namespace {
-
 thread_local std::string g_err;
-
+}  // namespace
 int fail(int code, const std::string &msg) {
   g_err = msg;
   return code;
 }
-
-#define SF2D_CUDA(call)                                                                       \
-  do {                                                                                        \
-    cudaError_t e_ = (call);                                                                  \
-    if (e_ != cudaSuccess)                                                                    \
-      return fail(e_ == cudaErrorMemoryAllocation ? SF2D_ERR_OOM : SF2D_ERR_CUDA,             \
-                  std::string(#call) + ": " + cudaGetErrorString(e_));                        \
-  } while (0)
-
-}  // namespace
-
-namespace sf2d {
-
-using TileKernel = void (*)(Params, int, int);
-
-template <int NT>
-TileKernel pick_tile_kernel(bool aniso, bool atten, bool lddrk) {
-  if (aniso) {
-    if (atten) return lddrk ? k_elastic_tile<NT, true, true, true> : k_elastic_tile<NT, true, true, false>;
-    return lddrk ? k_elastic_tile<NT, true, false, true> : k_elastic_tile<NT, true, false, false>;
-  }
-  if (atten) return lddrk ? k_elastic_tile<NT, false, true, true> : k_elastic_tile<NT, false, true, false>;
-  return lddrk ? k_elastic_tile<NT, false, false, true> : k_elastic_tile<NT, false, false, false>;
-}
-
-TileKernel pick_tile_kernel(int nt, bool aniso, bool atten, bool lddrk) {
-  switch (nt) {
-    case 128: return pick_tile_kernel<128>(aniso, atten, lddrk);
-    case 512: return pick_tile_kernel<512>(aniso, atten, lddrk);
-    default: return pick_tile_kernel<256>(aniso, atten, lddrk);
-  }
-}
-
+const char *last_error() { return g_err.c_str(); }
 }  // namespace sf2d
 
-struct sf2d_solver {
-  sf2d::Params P{};
-  sf2d::Tiling T;
-  std::vector<void *> allocs;
-  int *d_dev2glob = nullptr;
-  float2 *d_stage = nullptr;
-  unsigned int *d_norm = nullptr;
-  cudaStream_t stream = nullptr;
-  size_t smem = 0;
-  size_t dev_bytes = 0;
-  int nglob = 0, nrec = 0, nstep_total = 0;
-  int steps_done = 0;
-  int chunk = 32;
-  cudaGraphExec_t graph = nullptr;
-  int graph_steps = 0;
-  int nt = 256;  // threads per CTA of the tile kernel
+extern "C" const char *sf2d_last_error(void) { return sf2d::last_error(); }
 
-  template <typename T_>
-  int alloc(T_ **p, size_t count) {
-    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T_);
-    cudaError_t e = cudaMalloc(reinterpret_cast<void **>(p), bytes);
-    if (e != cudaSuccess)
-      return fail(e == cudaErrorMemoryAllocation ? SF2D_ERR_OOM : SF2D_ERR_CUDA,
-                  std::string("cudaMalloc: ") + cudaGetErrorString(e));
-    allocs.push_back(*p);
-    dev_bytes += bytes;
-    return SF2D_OK;
-  }
-  template <typename T_>
-  int upload(T_ **p, const T_ *host, size_t count) {
-    int rc = alloc(p, count);
-    if (rc) return rc;
-    if (count) SF2D_CUDA(cudaMemcpy(*p, host, count * sizeof(T_), cudaMemcpyHostToDevice));
-    return SF2D_OK;
-  }
-  using TileFn = void (*)(sf2d::Params, int, int);
-  TileFn tile_fn = nullptr;
-  bool lddrk = false;
-  int nstage = 1;
-
-  void launch_tile(bool record_prev, int stage) {
-    tile_fn<<<T.ntiles, nt, smem, stream>>>(P, record_prev ? 1 : 0, stage);
-  }
-  void launch_shared(int stage) {
-    const int nb = std::max(1, (P.nshared + sf2d::SHARED_NT - 1) / sf2d::SHARED_NT);
-    const int last = stage == nstage - 1 ? 1 : 0;
-    if (lddrk)
-      sf2d::k_elastic_shared<true><<<nb, sf2d::SHARED_NT, 0, stream>>>(P, stage, last);
-    else
-      sf2d::k_elastic_shared<false><<<nb, sf2d::SHARED_NT, 0, stream>>>(P, stage, last);
-  }
-  int launch_step(bool record_prev) {
-    for (int st = 0; st < nstage; ++st) {
-      launch_tile(record_prev && st == 0, st);
-      launch_shared(st);
-    }
-    return SF2D_OK;
-  }
-  int launch_receivers() {
-    if (nrec > 0) sf2d::k_receivers<<<(nrec + 127) / 128, 128, 0, stream>>>(P);
-    return SF2D_OK;
-  }
-  int launch_chunk(int n) {
-    for (int k = 0; k < n; ++k) launch_step(k > 0);
-    launch_receivers();
-    SF2D_CUDA(cudaGetLastError());
-    return SF2D_OK;
-  }
-  ~sf2d_solver() {
-    if (graph) cudaGraphExecDestroy(graph);
-    for (void *p : allocs) cudaFree(p);
-    if (stream) cudaStreamDestroy(stream);
-  }
-};
-
-extern "C" const char *sf2d_last_error(void) { return g_err.c_str(); }
-
-extern "C" int sf2d_elastic_create(const sf2d_elastic_desc *d, sf2d_solver **out) {
+int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solver **out) {
   using namespace sf2d;
   if (!d || !out) return fail(SF2D_ERR_INVALID, "null argument");
   *out = nullptr;
@@ -353,15 +245,34 @@ extern "C" int sf2d_elastic_create(const sf2d_elastic_desc *d, sf2d_solver **out
   float *d_stf;
   if ((rc = S->upload(&d_stf, stf.data(), stf.size()))) return rc;
   P.stf = d_stf;
+  S->d_stf = d_stf;
   double *seis;
   if ((rc = S->alloc(&seis, static_cast<size_t>(d->nrec) * d->nstep * 2))) return rc;
   P.seis = seis;
   if (d->nrec && d->nstep) SF2D_CUDA(cudaMemset(seis, 0, sizeof(double) * d->nrec * d->nstep * 2));
   int *ctr;
-  if ((rc = S->alloc(&ctr, 2))) return rc;
-  SF2D_CUDA(cudaMemset(ctr, 0, 2 * sizeof(int)));
+  if ((rc = S->alloc(&ctr, 8))) return rc;
+  SF2D_CUDA(cudaMemset(ctr, 0, 8 * sizeof(int)));
   P.d_step = ctr;
   P.d_status = ctr + 1;
+  P.d_step_b = ctr + 2;
+  P.frame_base = ctr + 3;
+  P.kern_base = ctr + 4;
+  P.nglob = d->nglob;
+  S->ctr = ctr;
+  S->kern = kern;
+  S->atten = atten;
+  S->nspec = d->nspec;
+  S->nq = nq;
+  if (kern) {
+    float2 *kmu;
+    float *rg;
+    if ((rc = S->alloc(&kmu, nq)) || (rc = S->alloc(&rg, d->nglob))) return rc;
+    SF2D_CUDA(cudaMemset(kmu, 0, sizeof(float2) * nq));
+    SF2D_CUDA(cudaMemset(rg, 0, sizeof(float) * d->nglob));
+    P.kmu_kl = kmu;
+    P.rho_kl_glob = rg;
+  }
   if ((rc = S->upload(&S->d_dev2glob, T.dev2glob.data(), T.dev2glob.size()))) return rc;
   if ((rc = S->alloc(&S->d_stage, d->nglob))) return rc;
   if ((rc = S->alloc(&S->d_norm, 1))) return rc;
@@ -387,7 +298,7 @@ extern "C" int sf2d_elastic_create(const sf2d_elastic_desc *d, sf2d_solver **out
     P.hconst[50 + k] = d->wxgll[k];
     P.hconst[55 + k] = d->wzgll[k];
   }
-  S->smem = tile_smem_layout(P.max_q, P.max_local).total;
+  S->smem = tile_smem_layout(P.max_q, P.max_local, kern).total;
   if (S->smem > 220 * 1024) return fail(SF2D_ERR_INVALID, "tile too large for shared memory");
   S->nt = d->threads_per_block > 0 ? d->threads_per_block : 256;
   if (S->nt != 128 && S->nt != 256 && S->nt != 512)
@@ -396,7 +307,7 @@ extern "C" int sf2d_elastic_create(const sf2d_elastic_desc *d, sf2d_solver **out
     for (const TileInfo &t : tiles)
       if (t.rec_n > S->nt) return fail(SF2D_ERR_INVALID, "more receivers in one tile than threads per CTA");
   }
-  S->tile_fn = pick_tile_kernel(S->nt, aniso, atten, lddrk);
+  S->tile_fn = pick_tile_kernel(S->nt, aniso, atten, lddrk, kern);
   S->lddrk = lddrk;
   S->nstage = nstage;
   SF2D_CUDA(cudaFuncSetAttribute(S->tile_fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -407,6 +318,10 @@ extern "C" int sf2d_elastic_create(const sf2d_elastic_desc *d, sf2d_solver **out
   SF2D_CUDA(cudaStreamSynchronize(S->stream));
   *out = guard.release();
   return SF2D_OK;
+}
+
+extern "C" int sf2d_elastic_create(const sf2d_elastic_desc *d, sf2d_solver **out) {
+  return sf2d_create_solver_internal(d, false, out);
 }
 
 extern "C" int sf2d_set_fields(sf2d_solver *S, const float *displ, const float *veloc, const float *accel) {
@@ -589,5 +504,24 @@ extern "C" int sf2d_destroy(sf2d_solver *S) {
   if (!S) return SF2D_OK;
   cudaStreamSynchronize(S->stream);
   delete S;
+  return SF2D_OK;
+}
+
+int sf2d_reset_solver(sf2d_solver *S) {
+  const sf2d::Params &P = S->P;
+  const size_t ng = static_cast<size_t>(S->nglob);
+  SF2D_CUDA(cudaMemsetAsync(P.u, 0, sizeof(float2) * ng, S->stream));
+  SF2D_CUDA(cudaMemsetAsync(P.v, 0, sizeof(float2) * ng, S->stream));
+  SF2D_CUDA(cudaMemsetAsync(P.a, 0, sizeof(float2) * ng, S->stream));
+  if (P.uL) SF2D_CUDA(cudaMemsetAsync(P.uL, 0, sizeof(float2) * ng, S->stream));
+  if (P.vL) SF2D_CUDA(cudaMemsetAsync(P.vL, 0, sizeof(float2) * ng, S->stream));
+  if (P.att_state) SF2D_CUDA(cudaMemsetAsync(P.att_state, 0, sizeof(float4) * S->nq * 3, S->stream));
+  if (P.att_state_l) SF2D_CUDA(cudaMemsetAsync(P.att_state_l, 0, sizeof(float4) * S->nq * 3, S->stream));
+  if (P.kmu_kl) SF2D_CUDA(cudaMemsetAsync(P.kmu_kl, 0, sizeof(float2) * S->nq, S->stream));
+  if (P.rho_kl_glob) SF2D_CUDA(cudaMemsetAsync(P.rho_kl_glob, 0, sizeof(float) * ng, S->stream));
+  if (S->nrec && S->nstep_total)
+    SF2D_CUDA(cudaMemsetAsync(P.seis, 0, sizeof(double) * S->nrec * S->nstep_total * 2, S->stream));
+  SF2D_CUDA(cudaMemsetAsync(S->ctr, 0, 3 * sizeof(int), S->stream));
+  S->steps_done = 0;
   return SF2D_OK;
 }

@@ -62,6 +62,16 @@ struct Params {
   const double *rec_h;    // 10 per receiver: hxir[5], hgammar[5]
   double *seis;           // [irec][it][2]
   int *d_step, *d_status;
+  int *d_step_b;          // copy of *d_step written by the tile kernel, read by the shared-point kernel
+  // segment recomputation: displacement frames written after every step, frame = step - *frame_base
+  float2 *frames;
+  const int *frame_base;
+  int nframes, nglob;
+  // adjoint sweep with kernel accumulation: forward frame = *kern_base - step
+  const float2 *kframes;
+  const int *kern_base;
+  float2 *kmu_kl;         // per element point (slot order): kappa and mu integrand sums
+  float *rho_kl_glob;     // per device point: rho integrand sum
   int nstep_stf, nstage, nstep_seis, seismotype, nrec;
   double cosrot, sinrot;
   float dt, dto2, dt2o2;
@@ -82,7 +92,8 @@ __device__ __forceinline__ void record_receiver(const Params &P, int r, int step
   for (int j = 0; j < 5; ++j)
     for (int i = 0; i < 5; ++i) {
       const float2 f = field[dev[j * 5 + i]];
-      const double hl = h[i] * h[5 + j];
+      // xir_store_loc and gammar_store_loc are CUSTOM_REAL: the product is formed in FP32
+      const double hl = static_cast<double>(static_cast<float>(h[i]) * static_cast<float>(h[5 + j]));
       vx += static_cast<double>(f.x) * hl;
       vz += static_cast<double>(f.y) * hl;
     }
@@ -110,10 +121,10 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 //   h    float[64]      hprime, hprimewgll, wxgll, wzgll
 //   lib  uint16[max_q rounded up to 8]
 struct TileSmem {
-  size_t geo, mat, u, v, acc, h, lib, total;
+  size_t geo, mat, u, v, acc, h, lib, b, total;
 };
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~static_cast<size_t>(15); }
-__host__ __device__ inline TileSmem tile_smem_layout(int max_q, int max_local) {
+__host__ __device__ inline TileSmem tile_smem_layout(int max_q, int max_local, bool kern = false) {
   TileSmem L;
   size_t o = 0;
   L.geo = o;
@@ -130,6 +141,8 @@ __host__ __device__ inline TileSmem tile_smem_layout(int max_q, int max_local) {
   o = align16(o + 64 * sizeof(float));
   L.lib = o;
   o = align16(o + static_cast<size_t>((max_q + 7) / 8 * 8) * sizeof(uint16_t));
+  L.b = o;
+  if (kern) o = align16(o + static_cast<size_t>(max_local) * sizeof(float2));
   L.total = o;
   return L;
 }
@@ -191,7 +204,28 @@ __device__ __forceinline__ void attenuation_point(const Params &P, size_t pa, fl
   e13s = e13[0] + e13[1] + e13[2];
 }
 
-template <int NT, bool ANISO, bool ATTEN, bool LDDRK>
+// Sensitivity-kernel integrands at one element point (compute_kernels.f90:75-292):
+// strains of the adjoint field (a_*) and of the forward frame (b_*) with the mapping
+// derivatives used in double, as the reference declares them.
+__device__ __forceinline__ void kernel_point(float dux_dxi, float duz_dxi, float dux_dg, float duz_dg, float bdux_dxi,
+                                             float bduz_dxi, float bdux_dg, float bduz_dg, float4 g4, float &kap,
+                                             float &muk) {
+  const double xixl = g4.x, xizl = g4.y, gammaxl = g4.z, gammazl = g4.w;
+  const float dux_dxl = static_cast<float>(dux_dxi * xixl + dux_dg * gammaxl);
+  const float dux_dzl = static_cast<float>(dux_dxi * xizl + dux_dg * gammazl);
+  const float duz_dxl = static_cast<float>(duz_dxi * xixl + duz_dg * gammaxl);
+  const float duz_dzl = static_cast<float>(duz_dxi * xizl + duz_dg * gammazl);
+  const float bdux_dxl = static_cast<float>(bdux_dxi * xixl + bdux_dg * gammaxl);
+  const float bdux_dzl = static_cast<float>(bdux_dxi * xizl + bdux_dg * gammazl);
+  const float bduz_dxl = static_cast<float>(bduz_dxi * xixl + bduz_dg * gammaxl);
+  const float bduz_dzl = static_cast<float>(bduz_dxi * xizl + bduz_dg * gammazl);
+  const float dsxz = static_cast<float>(0.5 * (static_cast<double>(duz_dxl) + static_cast<double>(dux_dzl)));
+  const float bdsxz = static_cast<float>(0.5 * (static_cast<double>(bduz_dxl) + static_cast<double>(bdux_dzl)));
+  kap = (dux_dxl + duz_dzl) * (bdux_dxl + bduz_dzl);
+  muk = dux_dxl * bdux_dxl + duz_dzl * bduz_dzl + 2.f * dsxz * bdsxz - 1.f / 3.f * kap;
+}
+
+template <int NT, bool ANISO, bool ATTEN, bool LDDRK, bool KERN>
 __global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_prev, int stage) {
   extern __shared__ __align__(16) unsigned char smem[];
   const TileInfo &ti = P.tiles[blockIdx.x];
@@ -202,8 +236,9 @@ __global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_
   const int nq = ti.nelem * 25;
   const int ebase = ti.elem_base * 25;
   const int int_begin = ti.int_begin;
-  const TileSmem L = tile_smem_layout(P.max_q, P.max_local);
+  const TileSmem L = tile_smem_layout(P.max_q, P.max_local, KERN);
   float4 *s_geo = reinterpret_cast<float4 *>(smem + L.geo);
+  float2 *s_b = reinterpret_cast<float2 *>(smem + L.b);
   float2 *s_mat = reinterpret_cast<float2 *>(smem + L.mat);
   float2 *s_u = reinterpret_cast<float2 *>(smem + L.u);
   float2 *s_v = reinterpret_cast<float2 *>(smem + L.v);
@@ -212,8 +247,11 @@ __global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_
   uint16_t *s_lib = reinterpret_cast<uint16_t *>(smem + L.lib);
 
   const int step = *P.d_step;
+  if (blockIdx.x == 0 && tid == 0) *P.d_step_b = step;
   // receivers of the previous step read the old fields before any write
   if (record_prev && tid < ti.rec_n) record_receiver(P, ti.rec_off + tid, step - 1);
+  const float2 *kframe = nullptr;
+  if (KERN) kframe = P.kframes + static_cast<size_t>(*P.kern_base - step) * P.nglob;
 
   // 1. every load of the tile is issued at once, straight into shared memory
   {
@@ -229,12 +267,14 @@ __global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_
       cp_async8(s_u + l, P.u + g);
       cp_async8(s_v + l, P.v + g);
       if (!LDDRK) cp_async8(s_acc + l, P.a + g);
+      if (KERN) cp_async8(s_b + l, kframe + g);
     }
     for (int k = tid; k < n_sh; k += NT) {
       const int g = P.sh_ids[ti.sh_off + k];
       cp_async8(s_u + n_int + k, P.u + g);
       cp_async8(s_v + n_int + k, P.v + g);
       if (!LDDRK) cp_async8(s_acc + n_int + k, P.a + g);
+      if (KERN) cp_async8(s_b + n_int + k, kframe + g);
     }
     if (tid < 60) s_h[tid] = P.hconst[tid];
     cp_async_wait_all();
@@ -307,6 +347,27 @@ __global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_
     }
     const float4 g4 = s_geo[f];
     const float2 m2 = s_mat[f];
+    if (KERN) {
+      // kernels of this adjoint step: adjoint displacement u' against the forward frame
+      float bdux_dxi = 0.f, bduz_dxi = 0.f, bdux_dg = 0.f, bduz_dg = 0.f;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        const float2 r = s_b[le[5 * j + k]];
+        const float hx = s_h[5 * i + k];
+        bdux_dxi += r.x * hx;
+        bduz_dxi += r.y * hx;
+        const float2 c = s_b[le[5 * k + i]];
+        const float hz = s_h[5 * j + k];
+        bdux_dg += c.x * hz;
+        bduz_dg += c.y * hz;
+      }
+      float kap, muk;
+      kernel_point(dux_dxi, duz_dxi, dux_dg, duz_dg, bdux_dxi, bduz_dxi, bdux_dg, bduz_dg, g4, kap, muk);
+      float2 km = P.kmu_kl[ebase + f];
+      km.x = km.x + kap;
+      km.y = km.y + muk;
+      P.kmu_kl[ebase + f] = km;
+    }
     const float xixl = g4.x, xizl = g4.y, gammaxl = g4.z, gammazl = g4.w;
     const float jacobianl = 1.f / (xixl * gammazl - gammaxl * xizl);
     const float dux_dxl = dux_dxi * xixl + dux_dg * gammaxl;
@@ -411,6 +472,14 @@ __global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_
       P.u[g] = u;
       P.v[g] = v;
       P.a[g] = a;
+      if (P.frames) {
+        const int fi = step - *P.frame_base;
+        if (fi >= 0 && fi < P.nframes) P.frames[static_cast<size_t>(fi) * P.nglob + g] = u;
+      }
+      if (KERN) {
+        const float2 b = s_b[l];
+        P.rho_kl_glob[g] = P.rho_kl_glob[g] + (a.x * b.x + a.y * b.y);
+      }
       bad |= !(fabsf(u.x) < 1e25f && fabsf(u.y) < 1e25f);
     } else {
       P.partial[ti.sh_off + l - n_int] = acc;
@@ -419,9 +488,10 @@ __global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_
   if (bad) *P.d_status = 1;
 }
 
-template <bool LDDRK>
+template <bool LDDRK, bool KERN>
 __global__ void __launch_bounds__(SHARED_NT) k_elastic_shared(const Params P, int stage, int last_stage) {
   const int s = blockIdx.x * SHARED_NT + threadIdx.x;
+  const int step = *P.d_step_b;
   if (s < P.nshared) {
     const int g = P.shared_begin + s;
     float2 u = P.u[g], v = P.v[g];
@@ -460,28 +530,36 @@ __global__ void __launch_bounds__(SHARED_NT) k_elastic_shared(const Params P, in
     P.u[g] = u;
     P.v[g] = v;
     P.a[g] = a;
+    if (P.frames) {
+      const int fi = step - *P.frame_base;
+      if (fi >= 0 && fi < P.nframes) P.frames[static_cast<size_t>(fi) * P.nglob + g] = u;
+    }
+    if (KERN) {
+      const float2 b = P.kframes[static_cast<size_t>(*P.kern_base - step) * P.nglob + g];
+      P.rho_kl_glob[g] = P.rho_kl_glob[g] + (a.x * b.x + a.y * b.y);
+    }
     if (!(fabsf(u.x) < 1e25f && fabsf(u.y) < 1e25f)) *P.d_status = 1;
   }
-  if (last_stage && blockIdx.x == 0 && threadIdx.x == 0) *P.d_step = *P.d_step + 1;
+  if (last_stage && blockIdx.x == 0 && threadIdx.x == 0) *P.d_step = step + 1;
 }
 
 // records the step before *d_step for every receiver
-__global__ void k_receivers(const Params P) {
+static __global__ void k_receivers(const Params P) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r < P.nrec) record_receiver(P, r, *P.d_step - 1);
 }
 
-__global__ void k_permute_in(const float2 *src, const int *dev2glob, float2 *dst, int n) {
+static __global__ void k_permute_in(const float2 *src, const int *dev2glob, float2 *dst, int n) {
   const int d = blockIdx.x * blockDim.x + threadIdx.x;
   if (d < n) dst[d] = src[dev2glob[d]];
 }
 
-__global__ void k_permute_out(const float2 *src, const int *dev2glob, float2 *dst, int n) {
+static __global__ void k_permute_out(const float2 *src, const int *dev2glob, float2 *dst, int n) {
   const int d = blockIdx.x * blockDim.x + threadIdx.x;
   if (d < n) dst[dev2glob[d]] = src[d];
 }
 
-__global__ void k_max_norm(const float2 *u, int n, unsigned int *out) {
+static __global__ void k_max_norm(const float2 *u, int n, unsigned int *out) {
   float m = 0.f;
   for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < n; d += gridDim.x * blockDim.x) {
     const float2 x = u[d];

@@ -86,6 +86,10 @@ def load_library(path: str = LIB):
         "sf2d_time_kernels": [vp, ctypes.c_int, _f],
         "sf2d_layout_info": [vp, ctypes.POINTER(ctypes.c_longlong)],
         "sf2d_destroy": [vp],
+        "sf2d_fwi_create": [ctypes.POINTER(ElasticDesc), _f, _f, ctypes.c_int, ctypes.POINTER(vp)],
+        "sf2d_fwi_forward": [vp, _d],
+        "sf2d_fwi_backward": [vp, _f, _f, _f, _f],
+        "sf2d_fwi_destroy": [vp],
     }
     for name, args in sigs.items():
         fn = getattr(lib, name)
@@ -139,72 +143,78 @@ def tiling_stats(db, tile_elems: int = 64):
     return dict(zip(keys, [int(x) for x in out]))
 
 
+def build_desc(db, tile_elems: int = 32, seismotype: int = 1, threads_per_block: int = 256):
+    """sf2d_elastic_desc for a setup Database; returns (desc, arrays kept alive)."""
+    keep = []
+
+    def f(a):
+        arr = np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+        keep.append(arr)
+        return arr.ctypes.data_as(_f)
+
+    def dd(a):
+        arr = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+        keep.append(arr)
+        return arr.ctypes.data_as(_d)
+
+    def i(a):
+        arr = np.ascontiguousarray(np.asarray(a, dtype=np.int32))
+        keep.append(arr)
+        return arr.ctypes.data_as(_i)
+
+    g = db.gll
+    d = ElasticDesc()
+    d.nspec, d.nglob = db.nspec, db.nglob
+    d.ibool = i(db.ibool)
+    d.xix, d.xiz, d.gammax, d.gammaz = f(db.xix), f(db.xiz), f(db.gammax), f(db.gammaz)
+    d.lambdastore, d.mustore = f(lambda_store(db)), f(db.mustore)
+    d.rmass_inverse = f(db.rmass_inverse_elastic)
+    d.hprime, d.hprimewgll, d.wxgll, d.wzgll = f(g.hprime), f(g.hprimewgll), f(g.wxgll), f(g.wzgll)
+    d.centroid_xz = dd(element_centroids(db))
+    d.nstacey = len(db.stacey_iglob)
+    d.st_iglob = i(db.stacey_iglob)
+    d.st_nx, d.st_nz, d.st_w = f(db.stacey_nx), f(db.stacey_nz), f(db.stacey_weight)
+    d.st_rho_vp, d.st_rho_vs = f(db.stacey_rho_vp), f(db.stacey_rho_vs)
+    d.nsrc = len(db.source_ispec)
+    d.src_ispec = i(db.source_ispec)
+    d.sourcearrays = f(db.sourcearrays)
+    d.stf = f(db.stf)
+    d.nstage = int(db.stf.shape[2])
+    d.nrec = len(db.rec_ispec)
+    d.rec_ispec = i(db.rec_ispec)
+    d.hxir, d.hgammar = dd(db.hxir), dd(db.hgammar)
+    d.cosrot, d.sinrot = float(db.cosrot), float(db.sinrot)
+    d.seismotype = seismotype
+    d.nstep = db.nstep
+    d.deltat, d.deltatover2, d.deltatsquareover2 = (float(db.deltat), float(db.deltatover2),
+                                                    float(db.deltatsquareover2))
+    d.tile_elems = tile_elems
+    d.threads_per_block = threads_per_block
+    from .setup.solver_setup import ALPHA_LDDRK, BETA_LDDRK
+
+    d.time_scheme = int(db.time_scheme)
+    d.alpha_lddrk, d.beta_lddrk = f(ALPHA_LDDRK), f(BETA_LDDRK)
+    an = getattr(db, "aniso", None)
+    if an is not None:
+        d.ispec_is_anisotropic = i(an["ispec"].astype(np.int32))
+        d.c11, d.c13, d.c15 = f(an["c11"]), f(an["c13"]), f(an["c15"])
+        d.c33, d.c35, d.c55 = f(an["c33"]), f(an["c35"]), f(an["c55"])
+    at = getattr(db, "atten", None)
+    if at is not None:
+        if int(db.time_scheme) == 1:
+            d.att_a1, d.att_b1, d.att_a2, d.att_b2 = f(at["a1"]), f(at["b1"]), f(at["a2"]), f(at["b2"])
+        else:
+            d.att_itau1, d.att_phi1 = f(at["itau1"]), f(at["phi1"])
+            d.att_itau2, d.att_phi2 = f(at["itau2"]), f(at["phi2"])
+    return d, keep
+
+
 class ElasticSolver:
-    """Device-resident isotropic elastic Newmark solver for one Database."""
+    """Device-resident elastic solver (Newmark or LDDRK) for one Database."""
 
-    def __init__(self, db, tile_elems: int = 64, seismotype: int = 1, threads_per_block: int = 256):
+    def __init__(self, db, tile_elems: int = 32, seismotype: int = 1, threads_per_block: int = 256):
         lib = load_library()
-        keep = []
-
-        def f(a):
-            arr = np.ascontiguousarray(np.asarray(a, dtype=np.float32))
-            keep.append(arr)
-            return arr.ctypes.data_as(_f)
-
-        def dd(a):
-            arr = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
-            keep.append(arr)
-            return arr.ctypes.data_as(_d)
-
-        def i(a):
-            arr = np.ascontiguousarray(np.asarray(a, dtype=np.int32))
-            keep.append(arr)
-            return arr.ctypes.data_as(_i)
-
-        g = db.gll
-        d = ElasticDesc()
-        d.nspec, d.nglob = db.nspec, db.nglob
-        d.ibool = i(db.ibool)
-        d.xix, d.xiz, d.gammax, d.gammaz = f(db.xix), f(db.xiz), f(db.gammax), f(db.gammaz)
-        d.lambdastore, d.mustore = f(lambda_store(db)), f(db.mustore)
-        d.rmass_inverse = f(db.rmass_inverse_elastic)
-        d.hprime, d.hprimewgll, d.wxgll, d.wzgll = f(g.hprime), f(g.hprimewgll), f(g.wxgll), f(g.wzgll)
-        d.centroid_xz = dd(element_centroids(db))
-        d.nstacey = len(db.stacey_iglob)
-        d.st_iglob = i(db.stacey_iglob)
-        d.st_nx, d.st_nz, d.st_w = f(db.stacey_nx), f(db.stacey_nz), f(db.stacey_weight)
-        d.st_rho_vp, d.st_rho_vs = f(db.stacey_rho_vp), f(db.stacey_rho_vs)
-        d.nsrc = len(db.source_ispec)
-        d.src_ispec = i(db.source_ispec)
-        d.sourcearrays = f(db.sourcearrays)
-        d.stf = f(db.stf)
-        d.nstage = int(db.stf.shape[2])
-        d.nrec = len(db.rec_ispec)
-        d.rec_ispec = i(db.rec_ispec)
-        d.hxir, d.hgammar = dd(db.hxir), dd(db.hgammar)
-        d.cosrot, d.sinrot = float(db.cosrot), float(db.sinrot)
-        d.seismotype = seismotype
-        d.nstep = db.nstep
-        d.deltat, d.deltatover2, d.deltatsquareover2 = (float(db.deltat), float(db.deltatover2),
-                                                        float(db.deltatsquareover2))
-        d.tile_elems = tile_elems
-        d.threads_per_block = threads_per_block
-        from .setup.solver_setup import ALPHA_LDDRK, BETA_LDDRK
-
-        d.time_scheme = int(db.time_scheme)
-        d.alpha_lddrk, d.beta_lddrk = f(ALPHA_LDDRK), f(BETA_LDDRK)
-        an = getattr(db, "aniso", None)
-        if an is not None:
-            d.ispec_is_anisotropic = i(an["ispec"].astype(np.int32))
-            d.c11, d.c13, d.c15 = f(an["c11"]), f(an["c13"]), f(an["c15"])
-            d.c33, d.c35, d.c55 = f(an["c33"]), f(an["c35"]), f(an["c55"])
-        at = getattr(db, "atten", None)
-        if at is not None:
-            if int(db.time_scheme) == 1:
-                d.att_a1, d.att_b1, d.att_a2, d.att_b2 = f(at["a1"]), f(at["b1"]), f(at["a2"]), f(at["b2"])
-            else:
-                d.att_itau1, d.att_phi1 = f(at["itau1"]), f(at["phi1"])
-                d.att_itau2, d.att_phi2 = f(at["itau2"]), f(at["phi2"])
+        d, keep = build_desc(db, tile_elems, seismotype, threads_per_block)
         h = ctypes.c_void_p()
         _check(lib.sf2d_elastic_create(ctypes.byref(d), ctypes.byref(h)))
         self._h = h
