@@ -2,7 +2,14 @@
 restatement of the reference's SIMULATION_TYPE = 3 kernels, and against finite
 differences through the torch.autograd test binding.
 
-Tolerance: kernels within 1e-4 relative L2 of the FP32 oracle's."""
+Tolerances: synthetics within 1e-5 and the misfit within 1e-4 of the FP32
+oracle.  The kernels integrate products of adjoint and forward strains (and
+the adjoint acceleration) over time; FP32 rounding alone moves the oracle's
+FP32 kernels by 2e-3 (kappa) to 1e-2 (mu) relative L2 away from its FP64
+kernels on this case, so two FP32 implementations that round differently
+cannot agree to 1e-4.  The GPU kernels must be as accurate as the FP32
+oracle's: relative L2 error against the FP64 oracle at most 1.5 times the
+FP32 oracle's own."""
 import numpy as np
 import pytest
 
@@ -20,25 +27,26 @@ def case():
     obs = oracle.Oracle(c.true_db(), 8).run(c.nstep)
     db0 = c.start_db()
     ref = oracle.gradient(db0, obs, checkpoint_every=150, precision=4)
-    return c, obs, db0, ref
+    ref64 = oracle.gradient(db0, obs, checkpoint_every=150, precision=8)
+    return c, obs, db0, ref, ref64
 
 
 def test_gpu_kernels_match_oracle(case):
     from specfem2d_b200.fwi import l2_misfit_gradient
 
-    c, obs, db0, (chi_o, syn_o, rk_o, kk_o, mk_o) = case
-    chi, syn, rk, kk, mk = l2_misfit_gradient(db0, obs, checkpoint_every=150)
+    c, obs, db0, (chi_o, syn_o, *k32), ref64 = case
+    chi, syn, *k = l2_misfit_gradient(db0, obs, checkpoint_every=150)
     assert rel_l2(syn, syn_o) < 1e-5
     assert abs(chi - chi_o) / chi_o < 1e-4
-    assert rel_l2(rk, rk_o) < 1e-4
-    assert rel_l2(kk, kk_o) < 1e-4
-    assert rel_l2(mk, mk_o) < 1e-4
+    for got, o32, o64 in zip(k, k32, ref64[2:]):
+        assert rel_l2(got, o64) < 1.5 * rel_l2(o32, o64)
+        assert rel_l2(got, o32) < 2.0 * rel_l2(o32, o64)
 
 
 def test_gpu_checkpoint_interval_invariance(case):
     from specfem2d_b200.fwi import l2_misfit_gradient
 
-    c, obs, db0, _ = case
+    c, obs, db0, _, _ = case
     a = l2_misfit_gradient(db0, obs, checkpoint_every=50)
     b = l2_misfit_gradient(db0, obs, checkpoint_every=900)
     for x, y in zip(a[2:], b[2:]):
@@ -50,7 +58,7 @@ def test_autograd_binding_matches_finite_differences(case):
 
     from specfem2d_b200.fwi import SeismogramOperator
 
-    c, obs, db0, _ = case
+    c, obs, db0, _, _ = case
     op = SeismogramOperator()
     obs_t = torch.from_numpy(obs)
     dt = float(db0.dt)
@@ -83,7 +91,8 @@ def test_viscoelastic_gradient_matches_oracle():
     obs = oracle.Oracle(c.true_db(), 8).run(c.nstep)
     db0 = c.start_db()
     ref = oracle.gradient(db0, obs, checkpoint_every=100, precision=4)
+    ref64 = oracle.gradient(db0, obs, checkpoint_every=100, precision=8)
     got = l2_misfit_gradient(db0, obs, checkpoint_every=100)
     assert rel_l2(got[1], ref[1]) < 1e-5
-    for a, b in zip(got[2:], ref[2:]):
-        assert rel_l2(a, b) < 1e-4
+    for a, b, b64 in zip(got[2:], ref[2:], ref64[2:]):
+        assert rel_l2(a, b64) < 1.5 * rel_l2(b, b64)
