@@ -48,6 +48,10 @@ def build_workload(name: str, nstep: int):
         db = configs.c2_geometry(nstep=nstep)
     elif name == "c1":
         db = configs.c1_homogeneous(nstep=nstep)
+    elif name == "c3_viscoelastic":
+        db = configs.c3_viscoelastic(nstep=nstep, time_scheme=1)
+    elif name == "c3_viscoelastic_lddrk":
+        db = configs.c3_viscoelastic(nstep=nstep, time_scheme=2)
     else:
         raise SystemExit(f"unknown workload {name}")
     with open(path + ".tmp", "wb") as f:
@@ -63,6 +67,10 @@ WORKLOAD_DESC = {
                     "vs=vp/1.73, Gardner rho, 5% Gaussian random field (corr. 200 m, seed 2), "
                     "Ricker 8 Hz force, dt 5e-4, 400 receivers"),
     "c1": "80x60 homogeneous elastic, Stacey L/R/B, free top, Ricker 10 Hz, 20 receivers",
+    "c3_viscoelastic": ("1600x800-element (40 km x 20 km, 20,489,601 GLL points) viscoelastic model under "
+                        "sinusoidal topography (200 m, 5 km), 3 SLS Qkappa 200 Qmu 60, vp 2500-6000, "
+                        "seeded moment tensor, Ricker 5 Hz, dt 3e-4, Newmark"),
+    "c3_viscoelastic_lddrk": "the same viscoelastic model advanced with the 6-stage LDDRK scheme",
 }
 
 
@@ -191,7 +199,7 @@ def main():
 
         dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         dist = dist_mod
-    from specfem2d_b200.configs import algorithmic_bytes_elastic
+    from specfem2d_b200.configs import algorithmic_bytes_elastic, algorithmic_bytes_viscoelastic
     from specfem2d_b200.runtime import ElasticSolver
 
     K, W = args.steps, args.warmup
@@ -229,7 +237,7 @@ def main():
         ms = float(t.item())
         dist.barrier()
     chunk = 32
-    launches = 2 * K + K // chunk + (1 if K % chunk else 0)
+    launches = 2 * K * (6 if db.time_scheme == 2 else 1) + K // chunk + (1 if K % chunk else 0)
 
     # kernel-level timing for the roofline (events around each launch, same stream)
     nk = min(200, max(20, K // 10))
@@ -241,7 +249,18 @@ def main():
     # algorithmic bytes of the element kernel per launch: element data + interior points
     # (u, v, a read+write, rmass) + shared points touched by tiles (u, v, a read, partial write)
     n_slots = int(np.asarray(solver_slots(db, args.tile_elems)))
-    tile_bytes = 700 * db.nspec + 56 * n_int + 32 * n_slots
+    ns = 6 if db.time_scheme == 2 else 1
+    if db.atten is None:
+        tile_bytes = 700 * db.nspec + 56 * n_int + 32 * n_slots
+        step_bytes = algorithmic_bytes_elastic(db.nspec, db.nglob)
+    elif db.time_scheme == 1:
+        tile_bytes = 700 * db.nspec + 3600 * db.nspec + 56 * n_int + 32 * n_slots
+        step_bytes = algorithmic_bytes_viscoelastic(db.nspec, db.nglob, 1)
+    else:
+        # per stage: element data, memory variables and their LDDRK copies, coefficients,
+        # interior points (u, v, u_L, v_L read+write, a written, rmass read), shared reads + partial
+        tile_bytes = db.nspec * (700 + 25 * 192) + 88 * n_int + 24 * n_slots
+        step_bytes = algorithmic_bytes_viscoelastic(db.nspec, db.nglob, 2)
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -250,7 +269,6 @@ def main():
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = tile_bytes / (tile_ms * 1e-3) / 1e9
-    step_bytes = algorithmic_bytes_elastic(db.nspec, db.nglob)
 
     # end to end through the public API with host buffers
     if args.no_e2e:

@@ -103,3 +103,118 @@ def algorithmic_bytes_elastic(nspec: int, nglob: int) -> int:
     layout: 25 points x (xix, xiz, gammax, gammaz, kappa, mu, ibool) x 4 B per
     element, and u, v, a read + write plus rmass_x, rmass_z read per point."""
     return 700 * nspec + 56 * nglob
+
+
+def c4_gradient(nstep: int = 4000, nrec: int = 200, true_model: bool = False, qmu=None, scale: int = 1,
+                shot_x: float = 12500.0):
+    """Elastic 1000 x 400 quads over 25 km x 10 km.  Background: vp = 2500 m/s
+    + 0.2 /s x depth, vs = vp / 1.73, Gardner rho; the true model adds two
+    +-10 % Gaussian anomalies (radius 1 km, centres drawn with seed 4).  One
+    Ricker 8 Hz vertical force 500 m deep, 200 surface receivers, dt 4e-4
+    (Courant ~0.42 with the smallest GLL spacing), Stacey on three sides."""
+    xmax, zmax = 25000.0, 10000.0
+    nx, nz = 1000 // scale, 400 // scale
+    interfaces = [([0.0, xmax], [0.0, 0.0]), ([0.0, xmax], [zmax, zmax])]
+    mesh = internal_mesh(0.0, xmax, nx, interfaces, [nz], absorb=(True, True, False, True))
+    from .setup.gll import GLL
+
+    x, z = _gll_points(mesh, GLL())
+    depth = zmax - z
+    vp = 2500.0 + 0.2 * depth
+    if true_model:
+        rng = np.random.default_rng(4)
+        for sign in (1.0, -1.0):
+            cx = rng.uniform(6000.0, 19000.0)
+            cz = rng.uniform(3000.0, 7000.0)
+            vp = vp * (1.0 + sign * 0.10 * np.exp(-((x - cx) ** 2 + (z - cz) ** 2) / 1000.0 ** 2))
+    vs = vp / 1.73
+    rho = 310.0 * vp ** 0.25
+    src = Source(x=shot_x, z=zmax - 500.0, source_type=1, time_function_type=1, f0=8.0, anglesource_deg=0.0,
+                 factor=1.0e10)
+    xs = np.linspace(250.0, xmax - 250.0, nrec)
+    recs = [(float(xr), zmax) for xr in xs]
+    q = {}
+    if qmu is not None:
+        q = dict(qkappa=np.full_like(vp, 9999.0), qmu=np.full_like(vp, float(qmu)))
+    return build_database(mesh, rho, vp, vs, [src], recs, nstep, 4.0e-4, stacey=True, external_model=True, **q)
+
+
+def random_layered_model(seed: int, nx: int, nz: int, nstep: int, dx: float = 25.0, dt: float = 4.0e-4,
+                         nrec: int = 20):
+    """A random layered elastic model (3 to 6 flat layers, vp 2000..4500 m/s,
+    vs = vp / 1.73, Gardner rho) of nx x nz quads of dx metres, one Ricker
+    8 Hz force and `nrec` surface receivers."""
+    rng = np.random.default_rng(seed)
+    xmax, zmax = nx * dx, nz * dx
+    interfaces = [([0.0, xmax], [0.0, 0.0]), ([0.0, xmax], [zmax, zmax])]
+    mesh = internal_mesh(0.0, xmax, nx, interfaces, [nz], absorb=(True, True, False, True))
+    from .setup.gll import GLL
+
+    x, z = _gll_points(mesh, GLL())
+    nl = int(rng.integers(3, 7))
+    tops = np.sort(rng.uniform(0.0, zmax, nl - 1))
+    vps = np.sort(rng.uniform(2000.0, 4500.0, nl))[::-1]  # faster at depth
+    layer = np.searchsorted(tops, z)
+    vp = vps[np.clip(layer, 0, nl - 1)]
+    vs = vp / 1.73
+    rho = 310.0 * vp ** 0.25
+    src = Source(x=float(rng.uniform(0.2, 0.8) * xmax), z=zmax - 10.0 * dx, source_type=1,
+                 time_function_type=1, f0=8.0, anglesource_deg=0.0, factor=1.0e10)
+    recs = [(float(xr), zmax) for xr in np.linspace(0.05 * xmax, 0.95 * xmax, nrec)]
+    return build_database(mesh, rho, vp, vs, [src], recs, nstep, dt, stacey=True, external_model=True)
+
+
+def c5_model_sizes(count: int = 48, seed: int = 6, lo=(100, 50), hi=(1200, 500)):
+    """Uneven mesh sizes (nx, nz) drawn with `seed` between lo and hi (aspect 2:1 kept)."""
+    rng = np.random.default_rng(seed)
+    f = rng.uniform(0.0, 1.0, count)
+    nx = (lo[0] + f * (hi[0] - lo[0])).astype(int)
+    nz = np.maximum(lo[1], (nx * (hi[1] / hi[0])).astype(int))
+    return list(zip(nx.tolist(), nz.tolist()))
+
+
+def c3_viscoelastic(nstep: int = 8000, time_scheme: int = 1, scale: int = 1, nrec: int = 100):
+    """1600 x 800 quads over 40 km x 20 km under a sinusoidal surface (amplitude
+    200 m, wavelength 5 km); vp rising smoothly 2500 -> 6000 m/s with depth,
+    vs = vp / 1.73, Gardner rho; 3 SLS with Qkappa 200, Qmu 60; moment-tensor
+    source (Mxx, Mzz, Mxz drawn with seed 3) 2 km deep, Ricker 5 Hz;
+    dt 3e-4 (Courant ~0.42 at 6000 m/s with 25 m elements); Newmark
+    (time_scheme 1) or LDDRK (2)."""
+    import math
+
+    xmax, zmax = 40000.0, 20000.0
+    nx, nz = 1600 // scale, 800 // scale
+    interfaces = [([0.0, xmax], [0.0, 0.0]), ([0.0, xmax], [zmax, zmax])]
+
+    def topo(x):
+        return zmax + 200.0 * math.sin(2.0 * math.pi * x / 5000.0)
+
+    mesh = internal_mesh(0.0, xmax, nx, interfaces, [nz], absorb=(True, True, False, True), topography_fn=topo)
+    from .setup.gll import GLL
+
+    x, z = _gll_points(mesh, GLL())
+    depth = np.clip(zmax - z, 0.0, zmax)
+    vp = 2500.0 + 3500.0 * (depth / zmax) ** 0.8
+    vs = vp / 1.73
+    rho = 310.0 * vp ** 0.25
+    rng = np.random.default_rng(3)
+    mxx, mzz, mxz = rng.uniform(-1.0, 1.0, 3)
+    src = Source(x=20000.0, z=zmax - 2000.0, source_type=2, time_function_type=1, f0=5.0,
+                 Mxx=float(mxx), Mzz=float(mzz), Mxz=float(mxz), factor=1.0e10)
+    xs = np.linspace(500.0, xmax - 500.0, nrec)
+    recs = [(float(xr), topo(float(xr))) for xr in xs]
+    return build_database(mesh, rho, vp, vs, [src], recs, nstep, 3.0e-4, stacey=True, external_model=True,
+                          time_scheme=time_scheme, qkappa=np.full_like(vp, 200.0), qmu=np.full_like(vp, 60.0))
+
+
+def algorithmic_bytes_viscoelastic(nspec: int, nglob: int, time_scheme: int = 1) -> int:
+    """Bytes of one viscoelastic 3-SLS step in the reference layout: the elastic
+    step plus, per element GLL point, e1 e11 e13 (3 SLS) read + write (72 B),
+    the A/B coefficients (48 B) and the three previous strains read + write
+    (24 B) for Newmark; LDDRK does 6 stages, each with the element data, the
+    memory variables and their LDDRK copies read + write (144 B), 1/tau and
+    phi (48 B) per element point and u, v, u_L, v_L read + write, a written
+    and rmass read per global point (88 B)."""
+    if time_scheme == 1:
+        return 700 * nspec + 56 * nglob + 3600 * nspec
+    return 6 * (nspec * (700 + 25 * 192) + nglob * 88)

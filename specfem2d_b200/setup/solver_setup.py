@@ -278,6 +278,16 @@ class _PointLocator:
         first = np.full(coord.shape[0], flat.size, dtype=np.int64)
         np.minimum.at(first, flat, np.arange(flat.size))
         self.first = first
+        # corner point -> elements having it as a corner (CSR), for the candidate search
+        corners = ibool[:, [0, 0, NGLL - 1, NGLL - 1], [0, NGLL - 1, 0, NGLL - 1]].ravel()
+        order = np.argsort(corners, kind="stable")
+        self.corner_elems = (order // 4).astype(np.int64)
+        self.corner_ptr = np.searchsorted(corners[order], np.arange(coord.shape[0] + 1))
+
+    def elements_touching(self, points):
+        """Ascending element ids that have any of `points` as a corner."""
+        parts = [self.corner_elems[self.corner_ptr[g]:self.corner_ptr[g + 1]] for g in points]
+        return np.unique(np.concatenate(parts)) if parts else np.zeros(0, dtype=np.int64)
 
     def nearest_flat(self, x_t, z_t):
         k = min(16, self.coord.shape[0])
@@ -299,9 +309,7 @@ def _locate(mesh: Mesh, ibool, coord, gll: GLL, x_t: float, z_t: float, iterate:
     corners = {int(ibool[ispec0, 0, 0]), int(ibool[ispec0, 0, NGLL - 1]),
                int(ibool[ispec0, NGLL - 1, NGLL - 1]), int(ibool[ispec0, NGLL - 1, 0])}
     cand = [ispec0]
-    cset = np.isin(ibool[:, [0, 0, NGLL - 1, NGLL - 1], [0, NGLL - 1, 0, NGLL - 1]],
-                   np.array(sorted(corners)))
-    for e in np.flatnonzero(cset.any(1)):
+    for e in locator.elements_touching(sorted(corners)):
         if int(e) != ispec0:
             cand.append(int(e))
     best = (HUGEVAL, None)
