@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -310,8 +311,18 @@ int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solv
   S->tile_fn = pick_tile_kernel(S->nt, aniso, atten, lddrk, kern);
   S->lddrk = lddrk;
   S->nstage = nstage;
-  SF2D_CUDA(cudaFuncSetAttribute(S->tile_fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(S->smem)));
+  {
+    // The limit is a property of the kernel, shared by every solver in the
+    // process: only ever raise it, or a later solver with smaller tiles would
+    // make the launches of an earlier one with larger tiles fail.
+    static std::mutex attr_mutex;
+    std::lock_guard<std::mutex> lock(attr_mutex);
+    cudaFuncAttributes fa;
+    SF2D_CUDA(cudaFuncGetAttributes(&fa, S->tile_fn));
+    if (fa.maxDynamicSharedSizeBytes < static_cast<int>(S->smem))
+      SF2D_CUDA(cudaFuncSetAttribute(S->tile_fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(S->smem)));
+  }
   S->nglob = d->nglob;
   S->nrec = d->nrec;
   S->nstep_total = d->nstep;

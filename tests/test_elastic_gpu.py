@@ -127,3 +127,19 @@ def test_unstable_is_reported(tromp):
     sol.set_fields(bad, None, None)
     with pytest.raises(UnstableError):
         sol.run(3)
+
+
+def test_solvers_with_different_tile_sizes_coexist(tromp):
+    """The tile kernel's shared-memory limit is per kernel, not per solver: a
+    solver with small tiles created after one with large tiles must not break
+    the launches of the first."""
+    from specfem2d_b200.runtime import ElasticSolver
+
+    db, _ = tromp
+    big = ElasticSolver(db, tile_elems=128)
+    small = ElasticSolver(db, tile_elems=8)
+    a = big.run(64)
+    b = small.run(64)
+    assert rel_l2(a, b) < TOL
+    big.close()
+    small.close()
