@@ -41,10 +41,17 @@ class OracleDb(ctypes.Structure):
         ("att_a1", _dp), ("att_b1", _dp), ("att_a2", _dp), ("att_b2", _dp),
         ("att_itau1", _dp), ("att_phi1", _dp), ("att_itau2", _dp), ("att_phi2", _dp),
         ("adj_src", _dp),
+        ("ispec_is_acoustic", _ip), ("rmass_inverse_acoustic", _dp),
+        ("nstacey_ac", ctypes.c_int), ("st_ac_iglob", _ip), ("st_ac_w", _dp), ("st_ac_rvp", _dp),
+        ("nfree_ac", ctypes.c_int), ("free_ac_iglob", _ip),
+        ("ncpl_ac", ctypes.c_int), ("cpl_ac_iglob", _ip), ("cpl_ac_nx", _dp), ("cpl_ac_nz", _dp), ("cpl_ac_w", _dp),
+        ("ncpl_el", ctypes.c_int), ("cpl_el_iglob", _ip), ("cpl_el_nx", _dp), ("cpl_el_nz", _dp), ("cpl_el_w", _dp),
+        ("use_trick", ctypes.c_int),
     ]
 
 
 DISPL, VELOC, ACCEL, DISPL_LDDRK, VELOC_LDDRK, E1, E11, E13, ATT_OLD, RHO_KL, KAPPA_KL, MU_KL = range(12)
+POT, POT_DOT, POT_DOT_DOT, POT_LDDRK, POT_DOT_LDDRK = range(12, 17)
 
 
 def build() -> str:
@@ -84,8 +91,9 @@ def lib():
 class Oracle:
     """Holds converted arrays (kept alive) and an oracle state; runs the CPU time loop."""
 
-    def __init__(self, db, precision: int = 4, seismotype: int = 1, db64=None, adj_src=None):
-        """``db`` supplies the FP32 setup; ``db64`` (optional) the FP64 one for precision 8."""
+    def __init__(self, db, precision: int = 4, seismotype: int | None = None, db64=None, adj_src=None):
+        """``db`` supplies the FP32 setup; ``db64`` (optional) the FP64 one for precision 8.
+        ``seismotype`` defaults to the database's."""
         from specfem2d_b200.setup.solver_setup import ALPHA_LDDRK, BETA_LDDRK
 
         self.precision = precision
@@ -146,7 +154,7 @@ class Oracle:
         s.rec_ispec = i(src.rec_ispec)
         s.hxir, s.hgammar = d(src.hxir), d(src.hgammar)
         s.cosrot, s.sinrot = float(src.cosrot), float(src.sinrot)
-        s.seismotype = seismotype
+        s.seismotype = int(getattr(src, "seismotype", 1) if seismotype is None else seismotype)
         s.deltat, s.deltatover2, s.deltatsquareover2 = dt, dto2, dt2o2
         an = getattr(src, "aniso", None)
         if an is not None:
@@ -160,6 +168,21 @@ class Oracle:
             s.att_a1, s.att_b1, s.att_a2, s.att_b2 = d(at["a1"]), d(at["b1"]), d(at["a2"]), d(at["b2"])
             s.att_itau1, s.att_phi1 = d(at["itau1"]), d(at["phi1"])
             s.att_itau2, s.att_phi2 = d(at["itau2"]), d(at["phi2"])
+        ac = getattr(src, "acoustic", None)
+        if ac is not None:
+            s.ispec_is_acoustic = i(ac["ispec"])
+            s.rmass_inverse_acoustic = d(ac["rmass"])
+            s.nstacey_ac = len(ac["st_iglob"])
+            s.st_ac_iglob, s.st_ac_w, s.st_ac_rvp = i(ac["st_iglob"]), d(ac["st_w"]), d(ac["st_rvp"])
+            s.nfree_ac = len(ac["free_iglob"])
+            s.free_ac_iglob = i(ac["free_iglob"])
+            s.ncpl_ac = len(ac["cpl_ac_iglob"])
+            s.cpl_ac_iglob = i(ac["cpl_ac_iglob"])
+            s.cpl_ac_nx, s.cpl_ac_nz, s.cpl_ac_w = d(ac["cpl_ac_nx"]), d(ac["cpl_ac_nz"]), d(ac["cpl_ac_w"])
+            s.ncpl_el = len(ac["cpl_el_iglob"])
+            s.cpl_el_iglob = i(ac["cpl_el_iglob"])
+            s.cpl_el_nx, s.cpl_el_nz, s.cpl_el_w = d(ac["cpl_el_nx"]), d(ac["cpl_el_nz"]), d(ac["cpl_el_w"])
+            s.use_trick = int(bool(ac.get("use_trick", False)))
         if adj_src is not None:
             s.adj_src = d(adj_src)
             s.nstep_total = int(np.asarray(adj_src).shape[1])
@@ -178,6 +201,8 @@ class Oracle:
             self.h = None
 
     def _size(self, which):
+        if which >= POT:
+            return (self.s.nglob,)
         if which <= VELOC_LDDRK:
             return (self.s.nglob, 2)
         if which >= RHO_KL:

@@ -90,7 +90,15 @@ struct State : StateBase {
   std::vector<real> rho_kl, kappa_kl, mu_kl;                // nspec*25
   std::vector<real> adj;                                    // nrec*nstep*2
   std::vector<real> contrib;
+  // acoustic domain
+  bool acoustic = false;
+  std::vector<real> kappa, rmass_ac, st_ac_w, st_ac_rvp;
+  std::vector<real> cpl_ac_nx, cpl_ac_nz, cpl_ac_w, cpl_el_nx, cpl_el_nz, cpl_el_w;
+  std::vector<real> pot, pot_d, pot_dd, pot_l, pot_d_l;     // nglob
+  std::vector<real> contrib_ac;                             // nspec*25
   int it = 0;  // steps done
+
+  bool is_acoustic(int e) const { return acoustic && d.ispec_is_acoustic[e] != 0; }
 
   explicit State(const sf2d_oracle_db *p) : d(*p) {
     nspec = d.nspec;
@@ -171,6 +179,111 @@ struct State : StateBase {
     kappa_kl.assign(nl, 0);
     mu_kl.assign(nl, 0);
     if (d.adj_src) adj = cvt<real>(d.adj_src, static_cast<size_t>(d.nrec) * d.nstep_total * 2);
+    acoustic = d.ispec_is_acoustic != nullptr;
+    if (acoustic) {
+      kappa = cvt<real>(d.kappastore, nl);
+      rmass_ac = cvt<real>(d.rmass_inverse_acoustic, nglob);
+      st_ac_w = cvt<real>(d.st_ac_w, d.nstacey_ac);
+      st_ac_rvp = cvt<real>(d.st_ac_rvp, d.nstacey_ac);
+      cpl_ac_nx = cvt<real>(d.cpl_ac_nx, d.ncpl_ac);
+      cpl_ac_nz = cvt<real>(d.cpl_ac_nz, d.ncpl_ac);
+      cpl_ac_w = cvt<real>(d.cpl_ac_w, d.ncpl_ac);
+      cpl_el_nx = cvt<real>(d.cpl_el_nx, d.ncpl_el);
+      cpl_el_nz = cvt<real>(d.cpl_el_nz, d.ncpl_el);
+      cpl_el_w = cvt<real>(d.cpl_el_w, d.ncpl_el);
+      pot.assign(nglob, 0);
+      pot_d.assign(nglob, 0);
+      pot_dd.assign(nglob, 0);
+      if (d.time_scheme != 1) {
+        pot_l.assign(nglob, 0);
+        pot_d_l.assign(nglob, 0);
+      }
+      contrib_ac.assign(nl, 0);
+    }
+  }
+
+  // Acoustic element force for one element (compute_forces_viscoacoustic.f90:
+  // 105-125 gather, :420-470 mxm_2comp_singleA, :142-152 mapping, :226-238
+  // fac = J / rho weak-form terms, :306-322 weighted transpose contraction).
+  // Writes the 25 sums to be subtracted from chi_dot_dot.
+  void acoustic_element_force(int ispec, real *out) {
+    const size_t off = static_cast<size_t>(ispec) * NGLL2;
+    real pe[NGLL][NGLL];  // [j][i]
+    for (int j = 0; j < NGLL; ++j)
+      for (int i = 0; i < NGLL; ++i) pe[j][i] = pot[d.ibool[off + j * NGLL + i]];
+    real t1[NGLL][NGLL], t2[NGLL][NGLL];
+    for (int j = 0; j < NGLL; ++j)
+      for (int i = 0; i < NGLL; ++i) {
+        const real dxi = pe[j][0] * hprime[i][0] + pe[j][1] * hprime[i][1] + pe[j][2] * hprime[i][2] +
+                         pe[j][3] * hprime[i][3] + pe[j][4] * hprime[i][4];
+        const real dgam = pe[0][i] * hprime[j][0] + pe[1][i] * hprime[j][1] + pe[2][i] * hprime[j][2] +
+                          pe[3][i] * hprime[j][3] + pe[4][i] * hprime[j][4];
+        const size_t p = off + j * NGLL + i;
+        const real xixl = xix[p], xizl = xiz[p], gammaxl = gammax[p], gammazl = gammaz[p];
+        const real dxl = dxi * xixl + dgam * gammaxl;
+        const real dzl = dxi * xizl + dgam * gammazl;
+        const real fac = jacobian[p] / rho[p];
+        t1[j][i] = fac * (xixl * dxl + xizl * dzl);
+        t2[j][i] = fac * (gammaxl * dxl + gammazl * dzl);
+      }
+    for (int j = 0; j < NGLL; ++j)
+      for (int i = 0; i < NGLL; ++i) {
+        real s1 = 0, s2 = 0;
+        for (int k = 0; k < NGLL; ++k) {
+          s1 = s1 + t1[j][k] * hprimewgll[k][i];
+          s2 = s2 + t2[k][i] * hprimewgll[k][j];
+        }
+        out[j * NGLL + i] = wzgll[j] * s1 + wxgll[i] * s2;
+      }
+  }
+
+  void enforce_free_surface() {
+    for (int k = 0; k < d.nfree_ac; ++k) {
+      const int g = d.free_ac_iglob[k];
+      pot[g] = 0;
+      pot_d[g] = 0;
+      pot_dd[g] = 0;
+    }
+  }
+
+  // chi_dd = Stacey(chi_d) + coupling(u) + sources - K chi, in the order of
+  // compute_forces_viscoacoustic_calling_routine.F90:40-233 with one process
+  // (phase 1 holds no element: boundary terms first, then all elements).
+  void acoustic_forces(int stage, int nt) {
+    for (int p = 0; p < d.nstacey_ac; ++p) {
+      const int g = d.st_ac_iglob[p];
+      pot_dd[g] = pot_dd[g] - pot_d[g] * st_ac_w[p] / st_ac_rvp[p];
+    }
+    for (int p = 0; p < d.ncpl_ac; ++p) {
+      const int g = d.cpl_ac_iglob[p];
+      const real displ_n = displ[2 * g] * cpl_ac_nx[p] + displ[2 * g + 1] * cpl_ac_nz[p];
+      pot_dd[g] = pot_dd[g] + cpl_ac_w[p] * displ_n;
+    }
+    for (int isrc = 0; isrc < d.nsrc; ++isrc) {
+      const int e = d.src_ispec[isrc];
+      if (!is_acoustic(e)) continue;
+      real stf = 0;
+      if (it < d.nstep_total)
+        stf = static_cast<real>(d.stf[(static_cast<size_t>(isrc) * d.nstep_total + it) * d.nstage + stage]);
+      // compute_add_sources_acoustic.f90:63-70
+      for (int j = 0; j < NGLL; ++j)
+        for (int i = 0; i < NGLL; ++i) {
+          const size_t p = static_cast<size_t>(e) * NGLL2 + j * NGLL + i;
+          const int g = d.ibool[p];
+          const real sa = srcarr[(static_cast<size_t>(isrc) * NGLL2 + j * NGLL + i) * 2];
+          pot_dd[g] = pot_dd[g] + sa * stf / kappa[p];
+        }
+    }
+    parallel_for(nspec, nspec > 256 ? nt : 1, [&](int b, int e1_) {
+      for (int e = b; e < e1_; ++e)
+        if (is_acoustic(e)) acoustic_element_force(e, &contrib_ac[static_cast<size_t>(e) * NGLL2]);
+    });
+    for (int e = 0; e < nspec; ++e) {
+      if (!is_acoustic(e)) continue;
+      const real *c = &contrib_ac[static_cast<size_t>(e) * NGLL2];
+      const int *ib = &d.ibool[static_cast<size_t>(e) * NGLL2];
+      for (int q = 0; q < NGLL2; ++q) pot_dd[ib[q]] = pot_dd[ib[q]] - c[q];
+    }
   }
 
   // Memory-variable update at one GLL point; returns the three sums.
@@ -311,6 +424,13 @@ struct State : StateBase {
       accel[2 * g] = accel[2 * g] - tx * st_w[p];
       accel[2 * g + 1] = accel[2 * g + 1] - tz * st_w[p];
     }
+    // fluid pressure on the solid (compute_coupling_viscoelastic_ac.f90:80-250)
+    for (int p = 0; p < (acoustic ? d.ncpl_el : 0); ++p) {
+      const int g = d.cpl_el_iglob[p];
+      const real pressure = -pot_dd[g];
+      accel[2 * g] = accel[2 * g] + cpl_el_w[p] * cpl_el_nx[p] * pressure;
+      accel[2 * g + 1] = accel[2 * g + 1] + cpl_el_w[p] * cpl_el_nz[p] * pressure;
+    }
     if (d.adj_src) {
       // adjoint sources at the receivers, time-reversed (compute_add_sources_viscoelastic.f90:351-405)
       const int it_tmp = d.nstep_total - 1 - it;
@@ -332,6 +452,7 @@ struct State : StateBase {
       if (it < d.nstep_total)
         stf = static_cast<real>(d.stf[(static_cast<size_t>(isrc) * d.nstep_total + it) * d.nstage + stage]);
       const int e = d.src_ispec[isrc];
+      if (is_acoustic(e)) continue;
       for (int j = 0; j < NGLL; ++j)
         for (int i = 0; i < NGLL; ++i) {
           const int g = d.ibool[static_cast<size_t>(e) * NGLL2 + j * NGLL + i];
@@ -341,9 +462,11 @@ struct State : StateBase {
         }
     }
     parallel_for(nspec, nspec > 256 ? nt : 1, [&](int b, int e1_) {
-      for (int e = b; e < e1_; ++e) element_force(e, stage, &contrib[static_cast<size_t>(e) * NGLL2 * 2]);
+      for (int e = b; e < e1_; ++e)
+        if (!is_acoustic(e)) element_force(e, stage, &contrib[static_cast<size_t>(e) * NGLL2 * 2]);
     });
     for (int e = 0; e < nspec; ++e) {
+      if (is_acoustic(e)) continue;
       const real *c = &contrib[static_cast<size_t>(e) * NGLL2 * 2];
       const int *ib = &d.ibool[static_cast<size_t>(e) * NGLL2];
       for (int q = 0; q < NGLL2; ++q) {
@@ -354,11 +477,59 @@ struct State : StateBase {
     }
   }
 
+  // Receiver in an acoustic element (write_seismograms.F90:75-150):
+  // seismotype 1-3 interpolate grad(chi)/rho of chi, chi_dot or chi_dot_dot
+  // formed in double (compute_vector_field.f90:143-207) and stored in
+  // CUSTOM_REAL; seismotype 4 interpolates the pressure -chi_dot_dot (or -chi
+  // with USE_TRICK_FOR_BETTER_PRESSURE, compute_pressure.f90:542-572).
+  void record_acoustic(int r, double *out) {
+    const int e = d.rec_ispec[r];
+    const size_t off = static_cast<size_t>(e) * NGLL2;
+    double vx = 0.0, vz = 0.0;
+    if (d.seismotype == 4) {
+      const std::vector<real> &f = d.use_trick ? pot : pot_dd;
+      for (int j = 0; j < NGLL; ++j)
+        for (int i = 0; i < NGLL; ++i) {
+          const double h = static_cast<double>(static_cast<real>(d.hxir[r * NGLL + i]) *
+                                               static_cast<real>(d.hgammar[r * NGLL + j]));
+          const real pr = -f[d.ibool[off + j * NGLL + i]];
+          vx = vx + static_cast<double>(pr) * h;
+        }
+      out[0] = vx;
+      out[1] = 0.0;
+      return;
+    }
+    const std::vector<real> &f = d.seismotype == 2 ? pot_d : (d.seismotype == 3 ? pot_dd : pot);
+    for (int j = 0; j < NGLL; ++j)
+      for (int i = 0; i < NGLL; ++i) {
+        double t1 = 0.0, t2 = 0.0;
+        for (int k = 0; k < NGLL; ++k) {
+          t1 = t1 + static_cast<double>(f[d.ibool[off + j * NGLL + k]]) * static_cast<double>(hprime[i][k]);
+          t2 = t2 + static_cast<double>(f[d.ibool[off + k * NGLL + i]]) * static_cast<double>(hprime[j][k]);
+        }
+        const size_t p = off + j * NGLL + i;
+        const double dchi_dx = t1 * static_cast<double>(xix[p]) + t2 * static_cast<double>(gammax[p]);
+        const double dchi_dz = t1 * static_cast<double>(xiz[p]) + t2 * static_cast<double>(gammaz[p]);
+        const real fx = static_cast<real>(dchi_dx / static_cast<double>(rho[p]));
+        const real fz = static_cast<real>(dchi_dz / static_cast<double>(rho[p]));
+        const double h = static_cast<double>(static_cast<real>(d.hxir[r * NGLL + i]) *
+                                             static_cast<real>(d.hgammar[r * NGLL + j]));
+        vx = vx + static_cast<double>(fx) * h;
+        vz = vz + static_cast<double>(fz) * h;
+      }
+    out[0] = d.cosrot * vx + d.sinrot * vz;
+    out[1] = -d.sinrot * vx + d.cosrot * vz;
+  }
+
   void record(double *seis, int nstep, int s) {
     if (!seis) return;
     const std::vector<real> &field = d.seismotype == 2 ? veloc : (d.seismotype == 3 ? accel : displ);
     for (int r = 0; r < d.nrec; ++r) {
       const int e = d.rec_ispec[r];
+      if (is_acoustic(e)) {
+        record_acoustic(r, &seis[(static_cast<size_t>(r) * nstep + s) * 2]);
+        continue;
+      }
       double vx = 0.0, vz = 0.0;
       for (int j = 0; j < NGLL; ++j)
         for (int i = 0; i < NGLL; ++i) {
@@ -386,6 +557,22 @@ struct State : StateBase {
           veloc[g] = veloc[g] + deltatover2 * accel[g];
           accel[g] = 0;
         }
+        if (acoustic) {
+          // acoustic predictor (update_displacement_Newmark.F90:353-402), then the
+          // whole acoustic step before the elastic one (iterate_time.F90:183-196)
+          for (int g = 0; g < nglob; ++g) {
+            pot[g] = pot[g] + deltat * pot_d[g] + deltatsquareover2 * pot_dd[g];
+            pot_d[g] = pot_d[g] + deltatover2 * pot_dd[g];
+            pot_dd[g] = 0;
+          }
+          enforce_free_surface();
+          acoustic_forces(0, nt);
+          for (int g = 0; g < nglob; ++g) {
+            pot_dd[g] = pot_dd[g] * rmass_ac[g];
+            pot_d[g] = pot_d[g] + deltatover2 * pot_dd[g];  // update_veloc_acoustic_Newmark
+          }
+          enforce_free_surface();
+        }
         forces(0, nt);
         // mass matrix and corrector (compute_forces_viscoelastic_calling_routine.F90:181,
         // update_displacement_Newmark.F90:564-589)
@@ -398,8 +585,22 @@ struct State : StateBase {
           // iterate_time.F90:167-181 clears accel, then forces and the LDDRK update
           // (update_displacement_LDDRK.F90:55-79)
           std::fill(accel.begin(), accel.end(), real(0));
-          forces(stage, nt);
           const real al = alpha[stage], be = beta[stage];
+          if (acoustic) {
+            std::fill(pot_dd.begin(), pot_dd.end(), real(0));
+            enforce_free_surface();
+            acoustic_forces(stage, nt);
+            // update_veloc_acoustic_LDDRK (update_displacement_LDDRK.F90:88-115)
+            for (int g = 0; g < nglob; ++g) {
+              pot_dd[g] = pot_dd[g] * rmass_ac[g];
+              pot_d_l[g] = al * pot_d_l[g] + deltat * pot_dd[g];
+              pot_l[g] = al * pot_l[g] + deltat * pot_d[g];
+              pot_d[g] = pot_d[g] + be * pot_d_l[g];
+              pot[g] = pot[g] + be * pot_l[g];
+            }
+            enforce_free_surface();
+          }
+          forces(stage, nt);
           for (size_t g = 0; g < ng; ++g) {
             accel[g] = accel[g] * rmass[g];
             veloc_l[g] = al * veloc_l[g] + deltat * accel[g];
@@ -480,6 +681,11 @@ struct State : StateBase {
       case SF2D_OR_RHO_KL: return &rho_kl;
       case SF2D_OR_KAPPA_KL: return &kappa_kl;
       case SF2D_OR_MU_KL: return &mu_kl;
+      case SF2D_OR_POT: return &pot;
+      case SF2D_OR_POT_DOT: return &pot_d;
+      case SF2D_OR_POT_DOT_DOT: return &pot_dd;
+      case SF2D_OR_POT_LDDRK: return &pot_l;
+      case SF2D_OR_POT_DOT_LDDRK: return &pot_d_l;
       default: return nullptr;
     }
   }
@@ -503,6 +709,13 @@ extern "C" void *sf2d_oracle_create(const sf2d_oracle_db *db, int precision) {
   if (!db || db->nspec <= 0 || db->nglob <= 0 || !db->ibool) return nullptr;
   if (db->time_scheme != 1 && db->time_scheme != 2) return nullptr;
   if (db->time_scheme == 2 && (!db->alpha_lddrk || !db->beta_lddrk)) return nullptr;
+  if (db->ispec_is_acoustic && (!db->kappastore || !db->rmass_inverse_acoustic || db->adj_src)) return nullptr;
+  if (db->seismotype == 4 && db->nrec > 0) {
+    // pressure is recorded in acoustic elements only
+    if (!db->ispec_is_acoustic) return nullptr;
+    for (int r = 0; r < db->nrec; ++r)
+      if (!db->ispec_is_acoustic[db->rec_ispec[r]]) return nullptr;
+  }
   if (precision == 4) return static_cast<StateBase *>(new State<float>(db));
   if (precision == 8) return static_cast<StateBase *>(new State<double>(db));
   return nullptr;

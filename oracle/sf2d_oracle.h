@@ -65,6 +65,25 @@ typedef struct {
    * adj_src[irec][it][comp] in time order, injected time-reversed
    * (compute_add_sources_viscoelastic.f90:351-405) */
   const double *adj_src;
+  /* acoustic (fluid) domain, potential formulation u = grad(chi)/rho (may be
+   * NULL = no acoustic element): compute_forces_viscoacoustic.f90:34-417,
+   * compute_stacey_acoustic.f90:34-199, enforce_acoustic_free_surface.f90:35-96,
+   * compute_coupling_acoustic_el.f90:36-283 (acoustic side) and
+   * compute_coupling_viscoelastic_ac.f90:36-258 (elastic side) */
+  const int *ispec_is_acoustic;                           /* nspec (kappastore above is used) */
+  const double *rmass_inverse_acoustic;                   /* nglob */
+  int nstacey_ac;                                         /* acoustic absorbing points, reference order */
+  const int *st_ac_iglob;
+  const double *st_ac_w, *st_ac_rvp;                      /* jacobian1D*w, rho*vp */
+  int nfree_ac;                                           /* free-surface points (zeroed) */
+  const int *free_ac_iglob;
+  int ncpl_ac;                                            /* coupling points, acoustic side */
+  const int *cpl_ac_iglob;
+  const double *cpl_ac_nx, *cpl_ac_nz, *cpl_ac_w;
+  int ncpl_el;                                            /* coupling points, elastic side */
+  const int *cpl_el_iglob;
+  const double *cpl_el_nx, *cpl_el_nz, *cpl_el_w;
+  int use_trick;                                          /* USE_TRICK_FOR_BETTER_PRESSURE: p = -chi */
 } sf2d_oracle_db;
 
 /* Fields addressed by sf2d_oracle_get/set. */
@@ -73,7 +92,9 @@ enum {
   SF2D_OR_DISPL_LDDRK = 3, SF2D_OR_VELOC_LDDRK = 4,
   SF2D_OR_E1 = 5, SF2D_OR_E11 = 6, SF2D_OR_E13 = 7,
   SF2D_OR_ATT_OLD = 8,                                   /* nspec*25*3: dux_dxl, duz_dzl, dux_dzl+duz_dxl of the last step */
-  SF2D_OR_RHO_KL = 9, SF2D_OR_KAPPA_KL = 10, SF2D_OR_MU_KL = 11  /* nspec*25, unscaled sums */
+  SF2D_OR_RHO_KL = 9, SF2D_OR_KAPPA_KL = 10, SF2D_OR_MU_KL = 11,  /* nspec*25, unscaled sums */
+  SF2D_OR_POT = 12, SF2D_OR_POT_DOT = 13, SF2D_OR_POT_DOT_DOT = 14, /* nglob: chi, chi_dot, chi_dot_dot */
+  SF2D_OR_POT_LDDRK = 15, SF2D_OR_POT_DOT_LDDRK = 16
 };
 
 /* Creates an oracle state (fields zero).  precision: 4 -> float, 8 -> double.
@@ -81,7 +102,7 @@ enum {
 void *sf2d_oracle_create(const sf2d_oracle_db *db, int precision);
 
 /* Advances nstep time steps.  seis (may be NULL): nrec*nstep*2 doubles,
- * [irec][it][comp].  nthreads <= 0 uses all host threads (or
+ * [irec][it][comp]; seismotype 4 (pressure) fills comp 0 and zeroes comp 1.  nthreads <= 0 uses all host threads (or
  * SF2D_ORACLE_THREADS).  Returns 0 on success. */
 int sf2d_oracle_run(void *h, int nstep, double *seis, int nthreads);
 

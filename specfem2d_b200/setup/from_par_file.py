@@ -19,23 +19,26 @@ from .solver_setup import Source, build_database
 
 
 def _receivers_from_par(par, top_interface):
+    """Receiver lines of all receiver sets, in set order."""
     xs_t, zs_t = top_interface
     t1 = (zs_t[1] - zs_t[0]) / (xs_t[1] - xs_t[0])
     tn = (zs_t[-1] - zs_t[-2]) / (xs_t[-1] - xs_t[-2])
     coefs = spline_construction(xs_t, zs_t, t1, tn)
-    nrec = int(par["nrec"])
-    xdeb, zdeb = float(par["xdeb"]), float(par["zdeb"])
-    xfin, zfin = float(par["xfin"]), float(par["zfin"])
+    sets = par.get("receiver_sets") or [par]
     out = []
-    for irec in range(1, nrec + 1):
-        if nrec > 1:
-            xr = xdeb + float(irec - 1) * (xfin - xdeb) / float(nrec - 1)
-            zr = zdeb + float(irec - 1) * (zfin - zdeb) / float(nrec - 1)
-        else:
-            xr, zr = xdeb, zdeb
-        if par.get("record_at_surface_same_vertical", False):
-            zr = value_spline(xr, xs_t, zs_t, coefs)
-        out.append((round(xr, 7), round(zr, 7)))
+    for rs in sets:
+        nrec = int(rs["nrec"])
+        xdeb, zdeb = float(rs["xdeb"]), float(rs["zdeb"])
+        xfin, zfin = float(rs["xfin"]), float(rs["zfin"])
+        for irec in range(1, nrec + 1):
+            if nrec > 1:
+                xr = xdeb + float(irec - 1) * (xfin - xdeb) / float(nrec - 1)
+                zr = zdeb + float(irec - 1) * (zfin - zdeb) / float(nrec - 1)
+            else:
+                xr, zr = xdeb, zdeb
+            if rs.get("record_at_surface_same_vertical", False):
+                zr = value_spline(xr, xs_t, zs_t, coefs)
+            out.append((round(xr, 7), round(zr, 7)))
     return out
 
 
@@ -43,7 +46,8 @@ PAR_KEYS = ("NSTEP", "DT", "time_stepping_scheme", "NGNOD", "xmin", "xmax", "nx"
             "absorbright", "absorbtop", "absorbleft", "STACEY_ABSORBING_CONDITIONS", "USER_T0",
             "anglerec", "nrec", "xdeb", "zdeb", "xfin", "zfin", "record_at_surface_same_vertical",
             "seismotype", "materials", "regions", "ATTENUATION_VISCOELASTIC", "PML_BOUNDARY_CONDITIONS",
-            "ATTENUATION_f0_REFERENCE", "NELEM_PML_THICKNESS")
+            "ATTENUATION_f0_REFERENCE", "NELEM_PML_THICKNESS", "receiver_sets", "USE_TRICK_FOR_BETTER_PRESSURE",
+            "TOMOGRAPHY_FILE", "MODEL")
 
 
 def config_from_data_dir(data_dir: str, par_file: str = "Par_file", source_file: str = "SOURCE") -> dict:
@@ -68,12 +72,15 @@ def database_from_data_dir(data_dir: str, nstep: int | None = None):
 
 
 def database_from_config(cfg: dict, nstep: int | None = None, absorbing_as_stacey: bool = False,
-                         time_scheme: int | None = None):
+                         time_scheme: int | None = None, tomo=None):
     """Build the Database from a parsed example configuration.
 
     ``absorbing_as_stacey`` puts Stacey conditions on the absorbing edges of
     an example that uses CPML (for comparisons on a time window that ends
-    before boundary reflections reach the receivers)."""
+    before boundary reflections reach the receivers).  ``tomo`` = (x, z, vp,
+    vs, rho) of the TOMOGRAPHY_FILE grid when the material table holds a
+    tomographic material (type -1); the whole model then takes the external
+    route (define_external_model_from_tomo_file.f90:386-470)."""
     par = cfg
     srcs = cfg["sources"]
     interfaces = [(list(x), list(z)) for (x, z) in cfg["interfaces"]]
@@ -102,6 +109,28 @@ def database_from_config(cfg: dict, nstep: int | None = None, absorbing_as_stace
                     is_aniso[e] = True
                     for k in ckeys:
                         cstore[k][e] = m[k]
+    tomo_mats = [k for k, m in mats.items() if m["kind"] == -1]
+    external = False
+    if tomo_mats:
+        if tomo is None:
+            raise ValueError("the material table has a tomographic material: pass tomo=(x, z, vp, vs, rho)")
+        from .tomography import tomo_values
+
+        # table materials enter the external arrays as rho, sqrt((lambda+2mu)/rho), sqrt(mu/rho)
+        for m in mats.values():
+            if m["kind"] == -1:
+                continue
+            lp2m = m["rho"] * m["vp"] * m["vp"]
+            mu = m["rho"] * m["vs"] * m["vs"]
+            m["vp"], m["vs"] = float(np.sqrt(lp2m / m["rho"])), float(np.sqrt(mu / m["rho"]))
+        mat_of = np.zeros(mesh.nspec, dtype=np.int64)
+        for (ix0, ix1, iz0, iz1, imat) in par["regions"]:
+            for iz in range(iz0, iz1 + 1):
+                for ix in range(ix0, ix1 + 1):
+                    e = (iz - 1) * mesh.nx + (ix - 1)
+                    mat_of[e] = imat
+                    vp[e], vs[e] = mats[imat]["vp"], mats[imat]["vs"]
+        external = True
     atten = bool(par.get("ATTENUATION_VISCOELASTIC", False))
     sources = []
     for s in srcs:
@@ -114,8 +143,23 @@ def database_from_config(cfg: dict, nstep: int | None = None, absorbing_as_stace
     n = int(par["NSTEP"]) if nstep is None else nstep
     stacey = bool(par["STACEY_ABSORBING_CONDITIONS"]) or (
         absorbing_as_stacey and bool(par.get("PML_BOUNDARY_CONDITIONS", False)))
+    if tomo_mats:
+        from .gll import GLL
+        from .mesh import createnum_fast, get_global, setup_mesh_coordinates
+
+        # tomographic values are taken at the global coordinates of the GLL points
+        gll = GLL()
+        ib0, nglob = createnum_fast(mesh, gll)
+        ibool = get_global(ib0)
+        coord = setup_mesh_coordinates(mesh, gll, ibool, nglob)["coord"]
+        els = np.flatnonzero(np.isin(mat_of, tomo_mats))
+        r_t, vp_t, vs_t = tomo_values(tuple(np.asarray(a, dtype=np.float64) for a in tomo), coord, ibool, els)
+        rho[els], vp[els], vs[els] = r_t, vp_t, vs_t
+        rho, vp, vs = (a.astype(np.float32).astype(np.float64) for a in (rho, vp, vs))
     db = build_database(mesh, rho, vp, vs, sources, recs, n, float(par["DT"]),
-                        stacey=stacey, external_model=False,
+                        stacey=stacey, external_model=external,
+                        use_trick=bool(par.get("USE_TRICK_FOR_BETTER_PRESSURE", False)),
+                        seismotype=int(par.get("seismotype", 1)),
                         time_scheme=int(time_scheme or par["time_stepping_scheme"]), user_t0=float(par["USER_T0"]),
                         anglerec_deg=float(par["anglerec"]),
                         qkappa=qk if atten else None, qmu=qm if atten else None,

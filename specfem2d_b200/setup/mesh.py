@@ -116,6 +116,7 @@ class Mesh:
     abs_type: np.ndarray = None    # (nabs,) IBOTTOM/IRIGHT/ITOP/ILEFT
     abs_corner: np.ndarray = None  # (nabs, 4) bool codeabs_corner
     free_top: bool = True
+    absorb: tuple = (True, True, False, True)  # (bottom, right, top, left) outer edges absorbing
 
 
 def internal_mesh(xmin, xmax, nx, interfaces, nz_layer, absorb=(True, True, False, True),
@@ -171,6 +172,7 @@ def internal_mesh(xmin, xmax, nx, interfaces, nz_layer, absorb=(True, True, Fals
     mesh = Mesh(nspec=nx * nzt, ngnod=4, knods=knods.astype(np.int64), coorg=coorg, nx=nx, nz=nzt)
     _absorbing_edges(mesh, absorb)
     mesh.free_top = not absorb[2]
+    mesh.absorb = tuple(bool(a) for a in absorb)
     return mesh
 
 

@@ -30,8 +30,12 @@ def _fvalue(tok: str):
 
 
 def read_par_file(path: str) -> dict:
-    """Return {key: value}, plus ``materials`` (list of token lists) and ``regions``."""
-    out: dict = {"materials": [], "regions": []}
+    """Return {key: value}, plus ``materials`` (list of token lists), ``regions``
+    and ``receiver_sets`` (one dict per ``nrec`` block, read_parameter_file.F90
+    reads nreceiversets blocks of nrec, xdeb, zdeb, xfin, zfin,
+    record_at_surface_same_vertical)."""
+    out: dict = {"materials": [], "regions": [], "receiver_sets": []}
+    rec_keys = ("nrec", "xdeb", "zdeb", "xfin", "zfin", "record_at_surface_same_vertical")
     with open(path) as f:
         lines = [ln.split("#", 1)[0].rstrip() for ln in f]
     lines = [ln for ln in lines if ln.strip()]
@@ -42,6 +46,10 @@ def read_par_file(path: str) -> dict:
             key, val = ln.split("=", 1)
             key = key.strip()
             out[key] = _fvalue(val)
+            if key == "nrec":
+                out["receiver_sets"].append({})
+            if key in rec_keys and out["receiver_sets"]:
+                out["receiver_sets"][-1][key] = out[key]
             if key == "nbmodels":
                 n = int(out[key])
                 out["materials"] = [lines[i + 1 + k].split() for k in range(n)]
@@ -96,6 +104,9 @@ def material_from_row(row) -> dict:
     """
     vals = [_fvalue(v) for v in row]
     kind = int(vals[1])
+    if kind == -1:
+        # tomographic material: values come from TOMOGRAPHY_FILE (read_materials.f90:192-205)
+        return dict(index=int(vals[0]), kind=-1, rho=0.0, vp=0.0, vs=0.0, qkappa=9999.0, qmu=9999.0)
     if kind == 2:
         rho = float(vals[2])
         c = [float(v) for v in vals[3:9]]

@@ -115,6 +115,12 @@ class Database:
     atten: dict = None
     # anisotropy (None = isotropic): keys ispec (nspec,) bool, c11 c13 c15 c33 c35 c55 (nspec,5,5) f32
     aniso: dict = None
+    # acoustic domain (None = no fluid element): keys ispec (nspec,) bool, rmass (nglob,) f32,
+    # st_iglob/st_w/st_rvp (acoustic absorbing points), free_iglob (free-surface points),
+    # cpl_ac_* and cpl_el_* (iglob, nx, nz, w per coupling point, acoustic and elastic side),
+    # use_trick (USE_TRICK_FOR_BETTER_PRESSURE)
+    acoustic: dict = None
+    seismotype: int = 1                 # 1 displacement, 2 velocity, 3 acceleration, 4 pressure
 
     @property
     def deltat(self):
@@ -197,12 +203,15 @@ def _edge_points(mesh: Mesh, abs_corner_skip=True):
         yield k, t, pts
 
 
-def stacey_points(mesh: Mesh, geo: dict, mat: dict, ibool, gll: GLL, stacey: bool):
-    """Per absorbing GLL point: iglob, normal, weight, rho*vp, rho*vs in FP32 arithmetic."""
+def stacey_points(mesh: Mesh, geo: dict, mat: dict, ibool, gll: GLL, stacey: bool, elastic=None):
+    """Per absorbing GLL point of an elastic element (all elements when
+    ``elastic`` is None): iglob, normal, weight, rho*vp, rho*vs in FP32 arithmetic."""
     out = {k: [] for k in ("iglob", "nx", "nz", "w", "rvp", "rvs")}
     if stacey and mesh.abs_ispec is not None:
         for k, t, pts in _edge_points(mesh):
             e = int(mesh.abs_ispec[k])
+            if elastic is not None and not elastic[e]:
+                continue
             for (i, j) in pts:
                 jac = geo["jacobian"][e, j, i]
                 if t in (ILEFT, IRIGHT):
@@ -234,12 +243,16 @@ def stacey_points(mesh: Mesh, geo: dict, mat: dict, ibool, gll: GLL, stacey: boo
             np.array(out["rvp"], dtype=f32), np.array(out["rvs"], dtype=f32))
 
 
-def mass_matrix_elastic(ibool, nglob, geo, mat, gll: GLL, stacey_pts, newmark: bool, dt: float):
-    """rmass_inverse_elastic (nglob, 2) f32 (invert_mass_matrix.F90:34-849, elastic)."""
+def mass_matrix_elastic(ibool, nglob, geo, mat, gll: GLL, stacey_pts, newmark: bool, dt: float, elastic=None):
+    """rmass_inverse_elastic (nglob, 2) f32 (invert_mass_matrix.F90:34-849, elastic).
+
+    Only elastic elements contribute (all when ``elastic`` is None); points
+    with no elastic mass get 1 before inversion (invert_mass_matrix.F90:820-822)."""
     wxwz = (gll.wxgll[None, :] * gll.wzgll[:, None]).astype(f32)  # [j][i], CUSTOM_REAL product
-    contrib = (wxwz[None].astype(np.float64) * mat["rhostore"].astype(np.float64)
-               * geo["jacobian"].astype(np.float64))
-    m = _sequential_f32_accumulate(nglob, ibool.ravel(), contrib.ravel())
+    el = np.arange(ibool.shape[0]) if elastic is None else np.flatnonzero(elastic)
+    contrib = (wxwz[None].astype(np.float64) * mat["rhostore"][el].astype(np.float64)
+               * geo["jacobian"][el].astype(np.float64))
+    m = _sequential_f32_accumulate(nglob, ibool[el].ravel(), contrib.ravel())
     mx = m.copy()
     mz = m.copy()
     if newmark and len(stacey_pts[0]):
@@ -255,6 +268,8 @@ def mass_matrix_elastic(ibool, nglob, geo, mat, gll: GLL, stacey_pts, newmark: b
             g = iglob[p]
             mx[g] = f32(mx[g] + f32(tx * ws[p]))
             mz[g] = f32(mz[g] + f32(tz * ws[p]))
+    mx = np.where(mx <= 0, f32(1.0), mx).astype(f32)
+    mz = np.where(mz <= 0, f32(1.0), mz).astype(f32)
     return np.stack([f32(1.0) / mx, f32(1.0) / mz], axis=1).astype(f32)
 
 
@@ -337,8 +352,16 @@ def _locate(mesh: Mesh, ibool, coord, gll: GLL, x_t: float, z_t: float, iterate:
     return best[1]
 
 
-def source_time_function(src: Source, t0: float, dt: float, nstep: int, time_scheme: int):
-    """(nstep, nstage) f32 values of -factor * stf(t) (prepare_source_time_function.f90)."""
+def source_time_function(src: Source, t0: float, dt: float, nstep: int, time_scheme: int,
+                         use_trick: bool = False):
+    """(nstep, nstage) f32 values of -factor * stf(t) (prepare_source_time_function.f90).
+
+    ``use_trick`` (USE_TRICK_FOR_BETTER_PRESSURE) replaces the Ricker by its
+    second derivative, the fourth derivative of the Gaussian
+    (prepare_source_time_function.f90:205-216, comp_source_time_function.f90:128-143),
+    so that -chi rather than -chi_dd is the pressure."""
+    if use_trick and src.time_function_type != 1:
+        raise NotImplementedError("USE_TRICK_FOR_BETTER_PRESSURE is restated for the Ricker only")
     nstage = 1 if time_scheme == 1 else 6
     out = np.zeros((nstep, nstage), dtype=f32)
     a = PI ** 2 * src.f0 ** 2
@@ -349,7 +372,9 @@ def source_time_function(src: Source, t0: float, dt: float, nstep: int, time_sch
             else:
                 timeval = float(it - 1 - 1) * dt + float(C_LDDRK[s]) * dt
             t = timeval - t0 - src.tshift
-            if src.time_function_type == 1:
+            if src.time_function_type == 1 and use_trick:
+                v = -2.0 * a * (3.0 - 12.0 * a * t * t + 4.0 * a ** 2 * t * t * t * t) * math.exp(-a * t * t)
+            elif src.time_function_type == 1:
                 v = (1.0 - 2.0 * a * t ** 2) * math.exp(-a * t ** 2)
             elif src.time_function_type == 2:
                 v = t * math.exp(-a * t ** 2)
@@ -383,13 +408,19 @@ def compute_t0(sources, user_t0: float = 0.0):
 def build_database(mesh: Mesh, rho, vp, vs, sources, receivers_xz, nstep: int, dt: float,
                    stacey: bool = True, external_model: bool = True, time_scheme: int = 1,
                    user_t0: float = 0.0, anglerec_deg: float = 0.0, qkappa=None, qmu=None,
-                   attenuation_f0: float | None = None) -> Database:
+                   attenuation_f0: float | None = None, use_trick: bool = False,
+                   seismotype: int = 1) -> Database:
     """Run the host setup chain and return a Database.
 
     ``rho, vp, vs`` are per-GLL-point arrays (nspec,5,5) (external model) or
     scalars/arrays used through the material-table branch when
-    ``external_model`` is False.
+    ``external_model`` is False.  Elements with vs = 0 are acoustic (fluid);
+    the acoustic domain, its absorbing points, free surface and the
+    fluid-solid coupling go into ``Database.acoustic``.  ``seismotype`` 4
+    records pressure (receivers in acoustic elements).
     """
+    from . import acoustic as ac_setup
+
     gll = GLL()
     ib0, nglob = createnum_fast(mesh, gll)
     ibool = get_global(ib0)
@@ -399,8 +430,26 @@ def build_database(mesh: Mesh, rho, vp, vs, sources, receivers_xz, nstep: int, d
     vp = np.broadcast_to(np.asarray(vp, dtype=np.float64), shp)
     vs = np.broadcast_to(np.asarray(vs, dtype=np.float64), shp)
     mat = material_stores_from_velocity(rho, vp, vs, external_model)
-    spts = stacey_points(mesh, geo, mat, ibool, gll, stacey)
-    rmass = mass_matrix_elastic(ibool, nglob, geo, mat, gll, spts, time_scheme == 1, dt)
+    is_ac = ac_setup.acoustic_element_flags(vs)
+    elastic = None if not is_ac.any() else ~is_ac
+    spts = stacey_points(mesh, geo, mat, ibool, gll, stacey, elastic)
+    rmass = mass_matrix_elastic(ibool, nglob, geo, mat, gll, spts, time_scheme == 1, dt, elastic)
+    acoustic = None
+    if is_ac.any():
+        edges = ac_setup.coupling_edges(ibool, is_ac)
+        cpl_ac, cpl_el = ac_setup.coupling_points(edges, ibool, geo, gll)
+        if stacey:
+            st_ac = ac_setup.stacey_acoustic_points(mesh, geo, mat, ibool, gll, is_ac, edges)
+        else:
+            st_ac = (np.zeros(0, np.int32), np.zeros(0, f32), np.zeros(0, f32))
+        acoustic = dict(
+            ispec=is_ac,
+            rmass=ac_setup.mass_matrix_acoustic(ibool, nglob, geo, mat, gll, is_ac, st_ac, time_scheme == 1, dt),
+            st_iglob=st_ac[0], st_w=st_ac[1], st_rvp=st_ac[2],
+            free_iglob=ac_setup.free_surface_points(mesh, ibool, is_ac),
+            cpl_ac_iglob=cpl_ac[0], cpl_ac_nx=cpl_ac[1], cpl_ac_nz=cpl_ac[2], cpl_ac_w=cpl_ac[3],
+            cpl_el_iglob=cpl_el[0], cpl_el_nx=cpl_el[1], cpl_el_nz=cpl_el[2], cpl_el_w=cpl_el[3],
+            use_trick=bool(use_trick))
     coord = geo["coord"]
     t0 = compute_t0(sources, user_t0)
     nstage = 1 if time_scheme == 1 else 6
@@ -411,7 +460,14 @@ def build_database(mesh: Mesh, rho, vp, vs, sources, receivers_xz, nstep: int, d
         hx, hpx = lagrange_any(xi, gll.xigll)
         hg, hpg = lagrange_any(gamma, gll.zigll)
         arr = np.zeros((NGLL, NGLL, 2), dtype=f32)
-        if s.source_type == 1:
+        if is_ac[e]:
+            # pressure source: sourcearray = hlagrange (setup_sources_receivers.F90:1003-1006)
+            if s.source_type != 1:
+                raise ValueError("a moment-tensor source cannot sit in an acoustic element")
+            for j in range(NGLL):
+                for i in range(NGLL):
+                    arr[j, i, :] = f32(hx[i] * hg[j])
+        elif s.source_type == 1:
             ang = s.anglesource_deg * PI / 180.0
             for j in range(NGLL):
                 for i in range(NGLL):
@@ -435,7 +491,7 @@ def build_database(mesh: Mesh, rho, vp, vs, sources, receivers_xz, nstep: int, d
                     arr[m, k, 1] = f32(s.Mxz * dsx + s.Mzz * dsz)
         src_ispec.append(e)
         src_arr.append(arr)
-        src_stf.append(source_time_function(s, t0, dt, nstep, time_scheme))
+        src_stf.append(source_time_function(s, t0, dt, nstep, time_scheme, use_trick))
         sxi.append(xi)
         sgam.append(gamma)
     rec_ispec, rxi, rgam, hxr, hgr, rxx, rzz = [], [], [], [], [], [], []
@@ -470,4 +526,5 @@ def build_database(mesh: Mesh, rho, vp, vs, sources, receivers_xz, nstep: int, d
         rec_x=np.array(rxx), rec_z=np.array(rzz),
         cosrot=math.cos(ang), sinrot=math.sin(ang),
         nstep=nstep, dt=dt, t0=t0, time_scheme=time_scheme, gll=gll, mesh=mesh,
-        src_xi=np.array(sxi), src_gamma=np.array(sgam), atten=atten)
+        src_xi=np.array(sxi), src_gamma=np.array(sgam), atten=atten, acoustic=acoustic,
+        seismotype=int(seismotype))

@@ -6,9 +6,10 @@ Run from the repository root, in a container where the reference is mounted:
 
 For each pinned example it writes ``<name>.json`` (the parsed Par_file
 subset, SOURCE and interfaces needed to rebuild the run, plus the source and
-receiver locations the reference printed in REF_SEIS/output.log) and
+receiver locations the reference printed in REF_SEIS/output.log),
 ``<name>_seis.npz`` (the REF_SEIS seismogram values as float64, with the
-first time sample and the time step of the trace).
+first time sample and the time step of the trace) and, for a tomographic
+model, ``<name>_tomo.npz`` (the gridded model the example's script writes).
 """
 from __future__ import annotations
 
@@ -34,7 +35,47 @@ EXAMPLES = {
     "attenuation_viscoelastic": ("EXAMPLES/attenuation/viscoelastic", [("S0001", "BXX"), ("S0001", "BXZ")],
                                  "Par_file_attenuation_2D_source_in_point_shared_by_four_elements",
                                  "SOURCE_attenuation_2D_source_in_point_shared_by_four_elements"),
+    # fluid layer (tomographic acoustic model) over an elastic layer: coupling, acoustic Stacey,
+    # acoustic free surface, displacement receivers in both domains
+    "tomographic_ocean_model": ("EXAMPLES/tomographic_ocean_model",
+                                [(f"S{k:04d}", c) for k in (1, 3, 6, 9, 12, 14, 16, 18, 20, 22) for c in ("BXX", "BXZ")],
+                                "Par_file", "SOURCE"),
 }
+
+# examples whose TOMOGRAPHY_FILE is written by a script of the reference
+TOMO_SCRIPTS = {"tomographic_ocean_model": "utils/createTomographyFile.py"}
+
+
+def tomography_grid(ref_root, script):
+    """Run the reference's tomography-file script (its plotting calls go to a
+    stub) in a scratch directory and parse the file it writes."""
+    import tempfile
+    import types
+
+    from specfem2d_b200.setup.tomography import read_tomo_file
+
+    stub = types.ModuleType("matplotlib")
+    stub.pyplot = types.SimpleNamespace(**{k: (lambda *a, **kw: None) for k in
+                                           ("clf", "title", "plot", "savefig", "show", "xlabel", "ylabel")})
+    saved = {k: sys.modules.get(k) for k in ("matplotlib", "matplotlib.pyplot")}
+    sys.modules["matplotlib"], sys.modules["matplotlib.pyplot"] = stub, stub.pyplot
+    cwd, argv = os.getcwd(), sys.argv
+    try:
+        with tempfile.TemporaryDirectory(dir=HERE) as tmp:
+            os.chdir(tmp)
+            path = os.path.join(ref_root, script)
+            sys.argv = [path]
+            code = compile(open(path).read(), path, "exec")
+            exec(code, {"__name__": "__main__"})
+            return read_tomo_file(os.path.join(tmp, "profile.xyz"))
+    finally:
+        os.chdir(cwd)
+        sys.argv = argv
+        for k, v in saved.items():
+            if v is None:
+                sys.modules.pop(k, None)
+            else:
+                sys.modules[k] = v
 
 
 def log_locations(path):
@@ -67,6 +108,9 @@ def main(ref_root):
             arrs["t_first"] = np.array(d[0, 0])
             arrs["t_step"] = np.array(d[1, 0] - d[0, 0])
         np.savez_compressed(os.path.join(HERE, name + "_seis.npz"), **arrs)
+        if name in TOMO_SCRIPTS:
+            x, z, vp, vs, rho = tomography_grid(ref_root, TOMO_SCRIPTS[name])
+            np.savez_compressed(os.path.join(HERE, name + "_tomo.npz"), x=x, z=z, vp=vp, vs=vs, rho=rho)
         print("wrote", name)
 
 

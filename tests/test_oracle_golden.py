@@ -5,6 +5,8 @@ source with a first-derivative-of-Gaussian time function) was run by the
 reference xspecfem2D (FP32) to produce REF_SEIS/AA.S0001.BX?.semd.  The
 fixtures in tests/golden were extracted from it by tests/golden/make_golden.py.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -109,3 +111,67 @@ def test_oracle_lddrk_close_to_newmark():
     t = float(seis["t_first"]) + float(seis["t_step"]) * np.arange(nm.nstep)
     w = t <= 0.4
     assert rel_l2(b[0, w, 0], seis["S0001_BXX"][w]) < 2e-2
+
+
+def _ocean(nstep=None, time_scheme=None):
+    cfg, seis = load_golden("tomographic_ocean_model")
+    t = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                             "tomographic_ocean_model_tomo.npz"))
+    db = database_from_config(cfg, nstep=nstep, time_scheme=time_scheme,
+                              tomo=(t["x"], t["z"], t["vp"], t["vs"], t["rho"]))
+    return cfg, seis, db
+
+
+OCEAN_STATIONS = (1, 3, 6, 9, 12, 14, 16, 18, 20, 22)
+
+
+@pytest.fixture(scope="module")
+def ocean():
+    return _ocean()
+
+
+def test_ocean_setup_matches_reference_log(ocean):
+    """EXAMPLES/tomographic_ocean_model: 40 rows of tomographic water over 20 rows
+    of rock, 80 coupling edges, 80 free-surface elements, 22 receivers."""
+    cfg, _, db = ocean
+    ac = db.acoustic
+    assert int(ac["ispec"].sum()) == 3200 and db.nspec == 4800
+    assert len(ac["cpl_ac_iglob"]) == 80 * 5 and len(ac["free_iglob"]) == 4 * 80 + 1
+    locs = cfg["log_locations"]
+    assert db.source_ispec[0] + 1 == locs[0][0]
+    assert db.src_xi[0] == pytest.approx(locs[0][1], abs=1e-9) and db.src_gamma[0] == pytest.approx(locs[0][2], abs=1e-9)
+    assert len(db.rec_ispec) == 22 == len(locs) - 1
+    for r, (e, xi, g) in enumerate(locs[1:]):
+        assert db.rec_ispec[r] + 1 == e
+        assert db.rec_xi[r] == pytest.approx(xi, abs=1e-9) and db.rec_gamma[r] == pytest.approx(g, abs=1e-9)
+
+
+def test_ocean_oracle_reproduces_ref_seis(ocean):
+    """Coupled fluid-solid run: the FP32 oracle sits as close to the reference's
+    FP32 traces as the FP64 oracle does (the remaining gap is FP32 rounding of
+    both FP32 runs)."""
+    import oracle
+
+    _, seis, db = ocean
+    o32 = oracle.Oracle(db, 4).run(db.nstep)
+    o64 = oracle.Oracle(db, 8).run(db.nstep)
+    got32, got64, ref = [], [], []
+    for k in OCEAN_STATIONS:
+        for c, ci in (("BXX", 0), ("BXZ", 1)):
+            r = seis[f"S{k:04d}_{c}"]
+            assert rel_l2(o32[k - 1, :, ci], r) < 2.0 * rel_l2(o64[k - 1, :, ci], r) + 2e-6
+            got32.append(o32[k - 1, :, ci]); got64.append(o64[k - 1, :, ci]); ref.append(r)
+    assert rel_l2(np.concatenate(got32), np.concatenate(ref)) < 3e-5
+    assert rel_l2(np.concatenate(got64), np.concatenate(ref)) < 3e-5
+
+
+def test_ocean_oracle_lddrk_close_to_newmark():
+    """The acoustic LDDRK update (update_displacement_LDDRK.F90:88-115) with
+    coupling solves the same problem as Newmark."""
+    import oracle
+
+    _, seis, nm = _ocean(nstep=900)
+    _, _, lk = _ocean(nstep=900, time_scheme=2)
+    a = oracle.Oracle(nm, 4).run(nm.nstep)
+    b = oracle.Oracle(lk, 4).run(lk.nstep)
+    assert rel_l2(b, a) < 2e-2
