@@ -181,6 +181,35 @@ int sf2d_fwi_destroy(sf2d_fwi *f);
 int sf2d_tiling_stats(int nspec, int nglob, const int *ibool, const double *centroid_xz, int tile_elems,
                       long long *out8);
 
+/* Largest member count sf2d_member_norms_noalloc accepts (its static scratch). */
+#define SF2D_NOALLOC_MAX_MEMBERS 4096
+
+/* Maximum displacement norm per member of a batch, with no device allocation.
+ * No counterpart in the reference: its get_norm_elastic_from_device
+ * (src/gpu/check_fields_cuda.cu:358) allocates and frees its per-block maxima
+ * on every call and takes one field.  This one serves callers that own all
+ * of their device memory (a host code that plans it before the time loop, or
+ * a pooling allocator that holds the GPU's free memory), where a cudaMalloc
+ * can fail and a cudaFree waits for the whole device.
+ *
+ * d_field: caller-owned device array of (ux, uz) float pairs, 8-byte aligned,
+ * on the current device.  Member m covers the points
+ * [offsets[m], offsets[m+1]); offsets (host, nmembers+1 values) start at
+ * >= 0 and never decrease, and must stay inside the field's allocation
+ * (checked).  max_norm (host, nmembers floats) receives
+ * max sqrt(ux^2 + uz^2) per member, +inf where a NaN occurs, 0 for an empty
+ * member.  1 <= nmembers <= SF2D_NOALLOC_MAX_MEMBERS, else SF2D_ERR_INVALID.
+ * stream: cudaStream_t (NULL = default stream); the call returns after the
+ * stream has finished the reduction.
+ *
+ * Intermediates live in one static device array (49,160 bytes per device).
+ * The first call on each device looks its address up with that device
+ * current, so make that first call before any stream capture.  Calls that
+ * overlap on one device (from several host threads) race on that array:
+ * serialise them. */
+int sf2d_member_norms_noalloc(const float *d_field, const int64_t *offsets, int nmembers, float *max_norm,
+                              void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -90,6 +90,7 @@ def load_library(path: str = LIB):
         "sf2d_fwi_forward": [vp, _d],
         "sf2d_fwi_backward": [vp, _f, _f, _f, _f],
         "sf2d_fwi_destroy": [vp],
+        "sf2d_member_norms_noalloc": [vp, ctypes.POINTER(ctypes.c_int64), ctypes.c_int, _f, vp],
     }
     for name, args in sigs.items():
         fn = getattr(lib, name)
@@ -141,6 +142,20 @@ def tiling_stats(db, tile_elems: int = 64):
         raise SF2DError(rc, "tiling invariant violated")
     keys = ["ntiles", "nshared", "max_local", "max_elems", "max_colours", "n_interior", "n_slots", "reserved"]
     return dict(zip(keys, [int(x) for x in out]))
+
+
+def member_norms_noalloc(field_ptr: int, offsets, stream: int = 0) -> np.ndarray:
+    """Maximum displacement norm per batch member of a caller-owned device
+    field of (ux, uz) float pairs at device address `field_ptr`; member m is
+    points offsets[m]:offsets[m+1].  Allocates no device memory (the library
+    keeps its intermediates in a static device array), for callers whose
+    device memory is all owned by another allocator."""
+    lib = load_library()
+    off = np.ascontiguousarray(offsets, dtype=np.int64)
+    out = np.zeros(max(len(off) - 1, 0), dtype=np.float32)
+    _check(lib.sf2d_member_norms_noalloc(ctypes.c_void_p(field_ptr), off.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                         len(off) - 1, out.ctypes.data_as(_f), ctypes.c_void_p(stream)))
+    return out
 
 
 def build_desc(db, tile_elems: int = 32, seismotype: int = 1, threads_per_block: int = 256):
