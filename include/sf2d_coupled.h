@@ -1,0 +1,105 @@
+/*
+ * sf2d_b200 -- coupled fluid-solid runs (acoustic + elastic domains).
+ * Plain C ABI, same conventions as sf2d_b200.h (int status, 0 = OK).
+ *
+ * A mesh with acoustic (fluid) elements runs as two sub-meshes with their own
+ * compact point numberings: the solid one described by an sf2d_elastic_desc
+ * (only its elements, points, absorbing points, sources and receivers) and
+ * the fluid one by an sf2d_acoustic_desc.  Interface points exist in both;
+ * sf2d_coupling_desc lists them in both numberings.  Correspondence:
+ *   sf2d_coupled_create   <- prepare_fields_acoustic_device
+ *                            (src/gpu/prepare_mesh_constants_cuda.cu:319) with
+ *                            the fluid parts of prepare_constants_device and
+ *                            prepare_stacey_device
+ *   sf2d_coupled_run      <- per step, in order: update_displacement_ac_cuda
+ *                            (src/gpu/update_displacement_cuda.cu:133),
+ *                            acoustic_enforce_free_surf_cuda
+ *                            (src/gpu/enforce_acoustic_free_surface_cuda.cu:46),
+ *                            compute_forces_acoustic_cuda
+ *                            (src/gpu/compute_forces_acoustic_cuda.cu:248),
+ *                            compute_stacey_acoustic_cuda
+ *                            (src/gpu/compute_stacey_acoustic_cuda.cu:40),
+ *                            compute_coupling_ac_el_cuda (src/gpu/compute_coupling_cuda.cu:47),
+ *                            compute_add_sources_ac_cuda
+ *                            (src/gpu/compute_add_sources_viscoacoustic_cuda.cu:46),
+ *                            kernel_3_acoustic_cuda (src/gpu/update_displacement_cuda.cu:322),
+ *                            then the solid step of sf2d_run with
+ *                            compute_coupling_el_ac_cuda (src/gpu/compute_coupling_cuda.cu:125)
+ *                            and compute_seismograms_cuda for both domains
+ *   sf2d_coupled_get_fields / set_fields <- transfer_fields_el_{from,to}_device
+ *                            and transfer_fields_ac_{from,to}_device
+ *                            (src/gpu/transfer_fields_cuda.cu:53,69,223,274)
+ */
+#ifndef SF2D_COUPLED_H
+#define SF2D_COUPLED_H
+
+#include "sf2d_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct sf2d_coupled sf2d_coupled;
+
+typedef struct {
+  int nspec, nglob;                          /* fluid elements and their points (own 0-based numbering) */
+  const int *ibool;                          /* nspec*25 */
+  const float *xix, *xiz, *gammax, *gammaz;  /* nspec*25 */
+  const float *jacobian, *rhostore, *kappastore;  /* nspec*25; J/rho is formed in FP32 */
+  const float *rmass_inverse;                /* nglob: rmass_inverse_acoustic (invert_mass_matrix.F90) */
+  const double *centroid_xz;                 /* nspec*2 element centres for tiling, may be NULL */
+  int nfree;                                 /* free-surface points, zeroed every step */
+  const int *free_iglob;
+  int nstacey;                               /* fluid absorbing points in reference order */
+  const int *st_iglob;
+  const float *st_w, *st_rho_vp;             /* jacobian1D * w, rho * vp */
+  int nsrc;                                  /* pressure sources in fluid elements */
+  const int *src_ispec;
+  const float *sourcearrays;                 /* nsrc*25 hlagrange values [isrc][j][i] */
+  const float *stf;                          /* nsrc*nstep*nstage */
+  int nrec;                                  /* receivers in fluid elements */
+  const int *rec_ispec;
+  const double *hxir, *hgammar;              /* nrec*5 */
+  const int *rec_global;                     /* index of each in the run's receiver list */
+  int tile_elems;                            /* 0 = 32 */
+} sf2d_acoustic_desc;
+
+typedef struct {
+  int nrec_total;                            /* receivers of the run (solid + fluid) */
+  const int *el_rec_global;                  /* index of each solid receiver in that list */
+  int seismotype;                            /* 1-3 displacement/velocity/acceleration, 4 pressure (fluid only) */
+  int use_trick;                             /* USE_TRICK_FOR_BETTER_PRESSURE: pressure = -chi */
+  double cosrot, sinrot;
+  /* fluid side (compute_coupling_acoustic_el.f90): chi_dd[ac] += w * (u_pred[el] . n) */
+  int ncpl_ac;
+  const int *cpl_ac_point, *cpl_ac_el_point; /* fluid point, the same point in the solid numbering */
+  const float *cpl_ac_nx, *cpl_ac_nz, *cpl_ac_w;
+  /* solid side (compute_coupling_viscoelastic_ac.f90): a[el] += w * n * (-chi_dd[ac]) */
+  int ncpl_el;
+  const int *cpl_el_point, *cpl_el_ac_point;
+  const float *cpl_el_nx, *cpl_el_nz, *cpl_el_w;
+} sf2d_coupling_desc;
+
+int sf2d_coupled_create(const sf2d_elastic_desc *solid, const sf2d_acoustic_desc *fluid,
+                        const sf2d_coupling_desc *coupling, sf2d_coupled **out);
+/* Advances nstep steps (fluid then solid per step or LDDRK stage); seismograms
+ * (may be NULL): nrec_total*nstep*2 doubles [irec][it][comp]. */
+int sf2d_coupled_run(sf2d_coupled *c, int nstep, double *seismograms);
+/* Fields in the sub-mesh numberings: displ/veloc/accel solid nglob*2,
+ * chi/chi_dot/chi_dot_dot fluid nglob.  NULL skips (get) or zeroes (set). */
+int sf2d_coupled_get_fields(sf2d_coupled *c, float *displ, float *veloc, float *accel, float *chi,
+                            float *chi_dot, float *chi_dot_dot);
+int sf2d_coupled_set_fields(sf2d_coupled *c, const float *displ, const float *veloc, const float *accel,
+                            const float *chi, const float *chi_dot, const float *chi_dot_dot);
+/* Average ms per launch of the fluid tile, fluid shared-point, solid tile and
+ * solid shared-point kernels (ms[0..3]) and per step (ms[4]); advances nstep steps. */
+int sf2d_coupled_time_kernels(sf2d_coupled *c, int nstep, float *ms);
+/* info[6]: fluid tiles, fluid shared points, max local points, shared bytes per CTA,
+ * fluid interior points, partial-sum slots. */
+int sf2d_coupled_layout_info(sf2d_coupled *c, long long *info);
+int sf2d_coupled_destroy(sf2d_coupled *c);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

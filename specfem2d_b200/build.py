@@ -16,8 +16,8 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIBDIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(LIBDIR, "libsf2d_b200.so")
-SOURCES = ["sf2d_elastic.cu", "sf2d_fwi.cu", "sf2d_noalloc.cu", "sf2d_tiler.cpp"]
-HEADERS = ["sf2d_tiler.h", "sf2d_kernels.cuh", "sf2d_runtime.h"]
+SOURCES = ["sf2d_elastic.cu", "sf2d_fwi.cu", "sf2d_noalloc.cu", "sf2d_coupled.cu", "sf2d_tiler.cpp"]
+HEADERS = ["sf2d_tiler.h", "sf2d_kernels.cuh", "sf2d_runtime.h", "sf2d_acoustic.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall", "-shared", "-cudart", "static",
@@ -28,7 +28,8 @@ def needs_build() -> bool:
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(ROOT, "include", "sf2d_b200.h")]
+    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [
+        os.path.join(ROOT, "include", h) for h in ("sf2d_b200.h", "sf2d_coupled.h")]
     return any(os.path.getmtime(p) > t for p in deps)
 
 

@@ -70,10 +70,56 @@ def c1_homogeneous(nstep: int = 2000, nrec: int = 20):
                           stacey=True, external_model=False)
 
 
+def c2_coupled(nstep: int = 6000, nrec: int = 400, scale: int = 1, rec_depth: float = 50.0,
+               time_scheme: int = 1, use_trick: bool = False, pml_thickness: int = 0):
+    """Coupled fluid-solid model: 20 km x 8 km, 800 x 320 quads (``scale``
+    divides both counts), a 1 km water layer (vp 1500 m/s, rho 1020 kg/m^3,
+    vs 0) over rock with vp rising linearly 2000 -> 4500 m/s from the sea
+    floor to the bottom, vs = vp / 1.73, Gardner rho = 310 vp^0.25, and a 5 %
+    Gaussian random perturbation (correlation 200 m, seed 2) of the rock; free
+    sea surface, absorbing sides and bottom (Stacey, or CPML layers of
+    ``pml_thickness`` elements); pressure source 500 m deep in the water,
+    Ricker 8 Hz; ``nrec`` pressure receivers ``rec_depth`` below the sea
+    surface; dt 5e-4 s (Courant ~0.55 at the fastest rock)."""
+    xmax, zmax = 20000.0, 8000.0
+    nx, nz = 800 // scale, 320 // scale
+    interfaces = [([0.0, xmax], [0.0, 0.0]), ([0.0, xmax], [zmax, zmax])]
+    mesh = internal_mesh(0.0, xmax, nx, interfaces, [nz], absorb=(True, True, False, True))
+    from .setup.gll import GLL
+
+    x, z = _gll_points(mesh, GLL())
+    depth = zmax - z
+    seafloor = 1000.0
+    water = (zmax - z.mean(axis=(1, 2))) < seafloor  # whole elements: the sea floor is an element boundary
+    vp = 2000.0 + 2500.0 * np.clip((depth - seafloor) / (zmax - seafloor), 0.0, 1.0)
+    gx, gz, f = gaussian_random_field(xmax, zmax, 200.0, seed=2)
+    vp = vp * (1.0 + 0.05 * _bilinear(gx, gz, f, x, z))
+    vs = vp / 1.73
+    rho = 310.0 * vp ** 0.25
+    vp[water], vs[water], rho[water] = 1500.0, 0.0, 1020.0
+    src = Source(x=10000.0, z=zmax - 500.0, source_type=1, time_function_type=1, f0=8.0,
+                 anglesource_deg=0.0, factor=1.0e10)
+    xs = np.linspace(100.0, xmax - 100.0, nrec)
+    recs = [(float(xr), zmax - rec_depth) for xr in xs]
+    pml = dict(nelem_thickness=pml_thickness) if pml_thickness > 0 else None
+    return build_database(mesh, rho, vp, vs, [src], recs, nstep, 5.0e-4, stacey=pml is None,
+                          external_model=True, time_scheme=time_scheme, seismotype=4, use_trick=use_trick,
+                          **({"pml": pml} if pml else {}))
+
+
+def algorithmic_bytes_coupled(nspec_el: int, nglob_el: int, nspec_ac: int, nglob_ac: int) -> int:
+    """Bytes of one coupled Newmark step in the reference layout: the solid
+    step over its elements and points plus, per fluid element, 25 points x
+    (xix, xiz, gammax, gammaz, rho, ibool) x 4 B and, per fluid point, chi,
+    chi_dot, chi_dot_dot read + write and rmass read."""
+    return 700 * nspec_el + 56 * nglob_el + 600 * nspec_ac + 28 * nglob_ac
+
+
 def c2_geometry(nstep: int = 6000, nrec: int = 400, elastic_only: bool = True, scale: int = 1):
-    """The 800 x 320 coupled-model geometry (``scale`` divides the element counts)."""
+    """The 800 x 320 model geometry with rock everywhere (``scale`` divides the element counts);
+    ``elastic_only=False`` gives the coupled model of c2_coupled."""
     if not elastic_only:
-        raise NotImplementedError("acoustic layer of the coupled model")
+        return c2_coupled(nstep=nstep, nrec=nrec, scale=scale)
     xmax, zmax = 20000.0, 8000.0
     nx, nz = 800 // scale, 320 // scale
     interfaces = [([0.0, xmax], [0.0, 0.0]), ([0.0, xmax], [zmax, zmax])]

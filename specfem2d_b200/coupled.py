@@ -1,0 +1,257 @@
+"""Coupled fluid-solid runs on the GPU.
+
+A Database with acoustic elements is split into a solid sub-mesh (handed to
+the elastic tile solver unchanged) and a fluid sub-mesh (the acoustic tile
+solver), each with its own compact numbering of the points it touches.  The
+fluid-solid interface points exist in both numberings; the coupling lists
+name them in both.  ``CoupledSolver`` wraps sf2d_coupled_* of the C ABI
+(include/sf2d_coupled.h) and gives fields and seismograms back in the
+Database's global numbering and receiver order.
+"""
+from __future__ import annotations
+
+import copy
+import ctypes
+
+import numpy as np
+
+from .runtime import _check, _d, _f, _i, build_desc, load_library
+
+_vp = ctypes.c_void_p
+
+
+class AcousticDesc(ctypes.Structure):
+    _fields_ = [
+        ("nspec", ctypes.c_int), ("nglob", ctypes.c_int),
+        ("ibool", _i),
+        ("xix", _f), ("xiz", _f), ("gammax", _f), ("gammaz", _f),
+        ("jacobian", _f), ("rhostore", _f), ("kappastore", _f),
+        ("rmass_inverse", _f),
+        ("centroid_xz", _d),
+        ("nfree", ctypes.c_int), ("free_iglob", _i),
+        ("nstacey", ctypes.c_int), ("st_iglob", _i), ("st_w", _f), ("st_rho_vp", _f),
+        ("nsrc", ctypes.c_int), ("src_ispec", _i), ("sourcearrays", _f), ("stf", _f),
+        ("nrec", ctypes.c_int), ("rec_ispec", _i), ("hxir", _d), ("hgammar", _d), ("rec_global", _i),
+        ("tile_elems", ctypes.c_int),
+    ]
+
+
+class CouplingDesc(ctypes.Structure):
+    _fields_ = [
+        ("nrec_total", ctypes.c_int), ("el_rec_global", _i),
+        ("seismotype", ctypes.c_int), ("use_trick", ctypes.c_int),
+        ("cosrot", ctypes.c_double), ("sinrot", ctypes.c_double),
+        ("ncpl_ac", ctypes.c_int), ("cpl_ac_point", _i), ("cpl_ac_el_point", _i),
+        ("cpl_ac_nx", _f), ("cpl_ac_nz", _f), ("cpl_ac_w", _f),
+        ("ncpl_el", ctypes.c_int), ("cpl_el_point", _i), ("cpl_el_ac_point", _i),
+        ("cpl_el_nx", _f), ("cpl_el_nz", _f), ("cpl_el_w", _f),
+    ]
+
+
+def _lib():
+    from .runtime import ElasticDesc
+
+    lib = load_library()
+    if not getattr(lib, "_coupled_sigs", False):
+        lib.sf2d_coupled_create.argtypes = [ctypes.POINTER(ElasticDesc), ctypes.POINTER(AcousticDesc),
+                                            ctypes.POINTER(CouplingDesc), ctypes.POINTER(_vp)]
+        lib.sf2d_coupled_run.argtypes = [_vp, ctypes.c_int, _d]
+        lib.sf2d_coupled_get_fields.argtypes = [_vp, _f, _f, _f, _f, _f, _f]
+        lib.sf2d_coupled_set_fields.argtypes = [_vp, _f, _f, _f, _f, _f, _f]
+        lib.sf2d_coupled_time_kernels.argtypes = [_vp, ctypes.c_int, _f]
+        lib.sf2d_coupled_layout_info.argtypes = [_vp, ctypes.POINTER(ctypes.c_longlong)]
+        lib.sf2d_coupled_destroy.argtypes = [_vp]
+        for n in ("create", "run", "get_fields", "set_fields", "time_kernels", "layout_info", "destroy"):
+            getattr(lib, "sf2d_coupled_" + n).restype = ctypes.c_int
+        lib._coupled_sigs = True
+    return lib
+
+
+def _submesh(db, elems):
+    """Sorted global ids of the points of ``elems``, global -> local map, element map."""
+    pts = np.unique(db.ibool[elems])
+    gmap = np.full(db.nglob, -1, dtype=np.int64)
+    gmap[pts] = np.arange(len(pts))
+    emap = np.full(db.nspec, -1, dtype=np.int64)
+    emap[elems] = np.arange(len(elems))
+    return pts, gmap, emap
+
+
+def split(db):
+    """Return (solid Database, fluid arrays dict, coupling arrays dict, index maps)."""
+    ac = db.acoustic
+    if ac is None:
+        raise ValueError("the Database has no acoustic element")
+    if getattr(db, "pml", None) is not None:
+        raise NotImplementedError("CPML layers are not part of the coupled GPU path")
+    is_ac = np.asarray(ac["ispec"], dtype=bool)
+    el_e, ac_e = np.flatnonzero(~is_ac), np.flatnonzero(is_ac)
+    if len(el_e) == 0:
+        raise ValueError("a fluid-only mesh has no solid part to couple to")
+    gl, gmap, emap = _submesh(db, el_e)
+    ga, amap, eamap = _submesh(db, ac_e)
+    src_ac = is_ac[db.source_ispec]
+    rec_ac = is_ac[db.rec_ispec]
+
+    sub = copy.copy(db)
+    sub.nspec, sub.nglob = len(el_e), len(gl)
+    sub.ibool = gmap[db.ibool[el_e]].astype(np.int32)
+    for k in ("xix", "xiz", "gammax", "gammaz", "jacobian", "rhostore", "kappastore", "mustore",
+              "rho_vpstore", "rho_vsstore"):
+        setattr(sub, k, getattr(db, k)[el_e])
+    sub.coord = db.coord[gl]
+    sub.rmass_inverse_elastic = db.rmass_inverse_elastic[gl]
+    sub.stacey_iglob = gmap[db.stacey_iglob].astype(np.int32)
+    if (sub.stacey_iglob < 0).any():
+        raise ValueError("solid absorbing point outside the solid sub-mesh")
+    sm = ~src_ac
+    sub.source_ispec = emap[db.source_ispec[sm]].astype(np.int32)
+    sub.sourcearrays = db.sourcearrays[sm]
+    sub.stf = db.stf[sm]
+    rm = ~rec_ac
+    sub.rec_ispec = emap[db.rec_ispec[rm]].astype(np.int32)
+    sub.hxir, sub.hgammar = db.hxir[rm], db.hgammar[rm]
+    if db.atten is not None:
+        sub.atten = {k: v[el_e] for k, v in db.atten.items()}
+    if db.aniso is not None:
+        sub.aniso = {k: v[el_e] for k, v in db.aniso.items()}
+    sub.acoustic = None
+    sub.mesh = None
+
+    fluid = dict(
+        nspec=len(ac_e), nglob=len(ga), ibool=amap[db.ibool[ac_e]].astype(np.int32),
+        xix=db.xix[ac_e], xiz=db.xiz[ac_e], gammax=db.gammax[ac_e], gammaz=db.gammaz[ac_e],
+        jacobian=db.jacobian[ac_e], rhostore=db.rhostore[ac_e], kappastore=db.kappastore[ac_e],
+        rmass=ac["rmass"][ga], centroid=db.coord[db.ibool[ac_e][:, [0, 0, 4, 4], [0, 4, 0, 4]]].mean(axis=1),
+        free=amap[ac["free_iglob"]].astype(np.int32),
+        st_iglob=amap[ac["st_iglob"]].astype(np.int32), st_w=ac["st_w"], st_rvp=ac["st_rvp"],
+        src_ispec=eamap[db.source_ispec[src_ac]].astype(np.int32),
+        sourcearrays=db.sourcearrays[src_ac][..., 0].astype(np.float32), stf=db.stf[src_ac],
+        rec_ispec=eamap[db.rec_ispec[rec_ac]].astype(np.int32), hxir=db.hxir[rec_ac], hgammar=db.hgammar[rec_ac],
+        rec_global=np.flatnonzero(rec_ac).astype(np.int32))
+    cpl = dict(
+        el_rec_global=np.flatnonzero(~rec_ac).astype(np.int32),
+        ac_point=amap[ac["cpl_ac_iglob"]].astype(np.int32), ac_el_point=gmap[ac["cpl_ac_iglob"]].astype(np.int32),
+        ac_nx=ac["cpl_ac_nx"], ac_nz=ac["cpl_ac_nz"], ac_w=ac["cpl_ac_w"],
+        el_point=gmap[ac["cpl_el_iglob"]].astype(np.int32), el_ac_point=amap[ac["cpl_el_iglob"]].astype(np.int32),
+        el_nx=ac["cpl_el_nx"], el_nz=ac["cpl_el_nz"], el_w=ac["cpl_el_w"],
+        use_trick=bool(ac.get("use_trick", False)))
+    return sub, fluid, cpl, dict(solid_points=gl, fluid_points=ga)
+
+
+class CoupledSolver:
+    """Device-resident coupled fluid-solid solver for one Database."""
+
+    def __init__(self, db, tile_elems: int = 32, threads_per_block: int = 256):
+        lib = _lib()
+        sub, fl, cp, maps = split(db)
+        seismotype = int(getattr(db, "seismotype", 1))
+        ed, keep = build_desc(sub, tile_elems, 1 if seismotype == 4 else seismotype, threads_per_block)
+
+        def f(a):
+            arr = np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+            keep.append(arr)
+            return arr.ctypes.data_as(_f)
+
+        def dd(a):
+            arr = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+            keep.append(arr)
+            return arr.ctypes.data_as(_d)
+
+        def i(a):
+            arr = np.ascontiguousarray(np.asarray(a, dtype=np.int32))
+            keep.append(arr)
+            return arr.ctypes.data_as(_i)
+
+        a = AcousticDesc()
+        a.nspec, a.nglob = fl["nspec"], fl["nglob"]
+        a.ibool = i(fl["ibool"])
+        a.xix, a.xiz, a.gammax, a.gammaz = f(fl["xix"]), f(fl["xiz"]), f(fl["gammax"]), f(fl["gammaz"])
+        a.jacobian, a.rhostore, a.kappastore = f(fl["jacobian"]), f(fl["rhostore"]), f(fl["kappastore"])
+        a.rmass_inverse = f(fl["rmass"])
+        a.centroid_xz = dd(fl["centroid"])
+        a.nfree, a.free_iglob = len(fl["free"]), i(fl["free"])
+        a.nstacey, a.st_iglob = len(fl["st_iglob"]), i(fl["st_iglob"])
+        a.st_w, a.st_rho_vp = f(fl["st_w"]), f(fl["st_rvp"])
+        a.nsrc, a.src_ispec = len(fl["src_ispec"]), i(fl["src_ispec"])
+        a.sourcearrays, a.stf = f(fl["sourcearrays"]), f(fl["stf"])
+        a.nrec, a.rec_ispec = len(fl["rec_ispec"]), i(fl["rec_ispec"])
+        a.hxir, a.hgammar, a.rec_global = dd(fl["hxir"]), dd(fl["hgammar"]), i(fl["rec_global"])
+        a.tile_elems = tile_elems
+        c = CouplingDesc()
+        c.nrec_total = len(db.rec_ispec)
+        c.el_rec_global = i(cp["el_rec_global"])
+        c.seismotype, c.use_trick = seismotype, int(cp["use_trick"])
+        c.cosrot, c.sinrot = float(db.cosrot), float(db.sinrot)
+        c.ncpl_ac = len(cp["ac_point"])
+        c.cpl_ac_point, c.cpl_ac_el_point = i(cp["ac_point"]), i(cp["ac_el_point"])
+        c.cpl_ac_nx, c.cpl_ac_nz, c.cpl_ac_w = f(cp["ac_nx"]), f(cp["ac_nz"]), f(cp["ac_w"])
+        c.ncpl_el = len(cp["el_point"])
+        c.cpl_el_point, c.cpl_el_ac_point = i(cp["el_point"]), i(cp["el_ac_point"])
+        c.cpl_el_nx, c.cpl_el_nz, c.cpl_el_w = f(cp["el_nx"]), f(cp["el_nz"]), f(cp["el_w"])
+        h = _vp()
+        _check(lib.sf2d_coupled_create(ctypes.byref(ed), ctypes.byref(a), ctypes.byref(c), ctypes.byref(h)))
+        self._h, self._lib = h, lib
+        self.nglob, self.nrec, self.nstep_total = db.nglob, len(db.rec_ispec), db.nstep
+        self.solid_points, self.fluid_points = maps["solid_points"], maps["fluid_points"]
+        self.sub_db = sub
+        self.nspec_fluid, self.nglob_fluid = fl["nspec"], fl["nglob"]
+        del keep
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.sf2d_coupled_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, nstep: int, seismograms: bool = True):
+        """Advance nstep steps; returns seismograms (nrec, nstep, 2) float64 or None."""
+        seis = np.zeros((self.nrec, nstep, 2), dtype=np.float64) if seismograms else None
+        _check(self._lib.sf2d_coupled_run(self._h, nstep, None if seis is None else seis.ctypes.data_as(_d)))
+        return seis
+
+    def get_fields(self):
+        """displ, veloc, accel (nglob, 2) and pot, pot_dot, pot_dot_dot (nglob,) in global numbering."""
+        ns, nf = len(self.solid_points), len(self.fluid_points)
+        sv = [np.empty((ns, 2), dtype=np.float32) for _ in range(3)]
+        fv = [np.empty(nf, dtype=np.float32) for _ in range(3)]
+        _check(self._lib.sf2d_coupled_get_fields(self._h, *[x.ctypes.data_as(_f) for x in sv + fv]))
+        out = {}
+        for k, x in zip(("displ", "veloc", "accel"), sv):
+            g = np.zeros((self.nglob, 2), dtype=np.float32)
+            g[self.solid_points] = x
+            out[k] = g
+        for k, x in zip(("pot", "pot_dot", "pot_dot_dot"), fv):
+            g = np.zeros(self.nglob, dtype=np.float32)
+            g[self.fluid_points] = x
+            out[k] = g
+        return out
+
+    def set_fields(self, **fields):
+        """Set displ/veloc/accel (nglob, 2) and pot/pot_dot/pot_dot_dot (nglob,) (global numbering);
+        missing fields are zeroed."""
+        arrs = []
+        for k in ("displ", "veloc", "accel"):
+            v = fields.get(k)
+            arrs.append(None if v is None else np.ascontiguousarray(np.asarray(v, np.float32)[self.solid_points]))
+        for k in ("pot", "pot_dot", "pot_dot_dot"):
+            v = fields.get(k)
+            arrs.append(None if v is None else np.ascontiguousarray(np.asarray(v, np.float32)[self.fluid_points]))
+        _check(self._lib.sf2d_coupled_set_fields(self._h, *[None if x is None else x.ctypes.data_as(_f) for x in arrs]))
+
+    def time_kernels(self, nstep: int):
+        """Average ms per launch: fluid tile, fluid shared, solid tile, solid shared; and per step."""
+        ms = (ctypes.c_float * 5)()
+        _check(self._lib.sf2d_coupled_time_kernels(self._h, nstep, ms))
+        return [float(x) for x in ms]
+
+    def layout_info(self):
+        info = (ctypes.c_longlong * 6)()
+        _check(self._lib.sf2d_coupled_layout_info(self._h, info))
+        keys = ["ntiles", "nshared", "max_local", "smem", "n_interior", "n_slots"]
+        return dict(zip(keys, [int(x) for x in info]))

@@ -1,0 +1,517 @@
+// Host runtime and C ABI of the coupled fluid-solid time step: a fluid
+// (acoustic) tile solver and the solid (elastic) tile solver advanced
+// together, fluid first, on one stream (iterate_time.F90:183-196).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "sf2d_acoustic.cuh"
+#include "sf2d_b200.h"
+#include "sf2d_coupled.h"
+#include "sf2d_kernels.cuh"
+#include "sf2d_runtime.h"
+#include "sf2d_tiler.h"
+
+namespace {
+
+using sf2d::AcParams;
+using sf2d::NGLL2;
+using sf2d::TileInfo;
+using sf2d::Tiling;
+
+__global__ void k_gather_f(const float *src, const int *dev2glob, float *dst, int n) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d < n) dst[d] = src[dev2glob[d]];
+}
+__global__ void k_scatter_f(const float *src, const int *dev2glob, float *dst, int n) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d < n) dst[dev2glob[d]] = src[d];
+}
+
+using AcTileFn = void (*)(AcParams, int, int);
+
+AcTileFn pick_ac_tile(int nt, bool lddrk) {
+  switch (nt) {
+    case 128: return lddrk ? sf2d::k_acoustic_tile<128, true> : sf2d::k_acoustic_tile<128, false>;
+    case 512: return lddrk ? sf2d::k_acoustic_tile<512, true> : sf2d::k_acoustic_tile<512, false>;
+    default: return lddrk ? sf2d::k_acoustic_tile<256, true> : sf2d::k_acoustic_tile<256, false>;
+  }
+}
+
+}  // namespace
+
+struct sf2d_coupled {
+  sf2d_solver *el = nullptr;  // solid sub-solver (owns the stream)
+  AcParams A{};
+  Tiling T;
+  std::vector<void *> allocs;
+  int *d_dev2glob = nullptr;
+  float *d_stage = nullptr;
+  int *ctr = nullptr;
+  double *seis = nullptr;
+  AcTileFn tile_fn = nullptr;
+  size_t smem = 0;
+  int nt = 256, nstage = 1, nglob = 0, nrec_total = 0, nstep = 0, steps_done = 0;
+  bool lddrk = false;
+  int chunk = 32;
+  cudaGraphExec_t graph = nullptr;
+  int graph_steps = 0;
+
+  template <typename T_>
+  int alloc(T_ **p, size_t count) {
+    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T_);
+    cudaError_t e = cudaMalloc(reinterpret_cast<void **>(p), bytes);
+    if (e != cudaSuccess)
+      return sf2d::fail(e == cudaErrorMemoryAllocation ? SF2D_ERR_OOM : SF2D_ERR_CUDA,
+                        std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    allocs.push_back(*p);
+    return SF2D_OK;
+  }
+  template <typename T_>
+  int upload(T_ **p, const T_ *host, size_t count) {
+    int rc = alloc(p, count);
+    if (rc) return rc;
+    if (count) SF2D_CUDA(cudaMemcpy(*p, host, count * sizeof(T_), cudaMemcpyHostToDevice));
+    return SF2D_OK;
+  }
+  template <typename T_>
+  int upload_const(const T_ **p, const std::vector<T_> &v) {
+    T_ *q = nullptr;
+    int rc = upload(&q, v.data(), v.size());
+    *p = q;
+    return rc;
+  }
+
+  void launch_ac_tile(bool record_prev, int stage) {
+    tile_fn<<<T.ntiles, nt, smem, el->stream>>>(A, record_prev ? 1 : 0, stage);
+  }
+  void launch_ac_shared(int stage) {
+    const int nb = std::max(1, (A.nshared + sf2d::SHARED_NT - 1) / sf2d::SHARED_NT);
+    const int last = stage == nstage - 1 ? 1 : 0;
+    if (lddrk)
+      sf2d::k_acoustic_shared<true><<<nb, sf2d::SHARED_NT, 0, el->stream>>>(A, stage, last);
+    else
+      sf2d::k_acoustic_shared<false><<<nb, sf2d::SHARED_NT, 0, el->stream>>>(A, stage, last);
+  }
+  void launch_step(bool record_prev) {
+    for (int st = 0; st < nstage; ++st) {
+      launch_ac_tile(record_prev && st == 0, st);
+      launch_ac_shared(st);
+      el->launch_tile(record_prev && st == 0, st);
+      el->launch_shared(st);
+    }
+  }
+  int launch_chunk(int n) {
+    for (int k = 0; k < n; ++k) launch_step(k > 0);
+    el->launch_receivers();
+    if (A.nrec > 0) sf2d::k_acoustic_receivers<<<(A.nrec + 127) / 128, 128, 0, el->stream>>>(A);
+    SF2D_CUDA(cudaGetLastError());
+    return SF2D_OK;
+  }
+  ~sf2d_coupled() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (el) sf2d_destroy(el);
+    for (void *p : allocs) cudaFree(p);
+  }
+};
+
+extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acoustic_desc *ad,
+                                   const sf2d_coupling_desc *cp, sf2d_coupled **out) {
+  using namespace sf2d;
+  if (!eld || !ad || !cp || !out) return fail(SF2D_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (ad->nspec <= 0 || ad->nglob <= 0 || !ad->ibool || !ad->xix || !ad->xiz || !ad->gammax || !ad->gammaz ||
+      !ad->jacobian || !ad->rhostore || !ad->kappastore || !ad->rmass_inverse)
+    return fail(SF2D_ERR_INVALID, "missing fluid mesh arrays");
+  if (ad->nfree < 0 || ad->nstacey < 0 || ad->nsrc < 0 || ad->nrec < 0 || cp->ncpl_ac < 0 || cp->ncpl_el < 0)
+    return fail(SF2D_ERR_INVALID, "negative count");
+  if (cp->nrec_total != eld->nrec + ad->nrec) return fail(SF2D_ERR_INVALID, "receiver counts do not add up");
+  if (cp->seismotype < 1 || cp->seismotype > 4) return fail(SF2D_ERR_INVALID, "seismotype must be 1 to 4");
+  if (cp->seismotype == 4 && eld->nrec > 0)
+    return fail(SF2D_ERR_INVALID, "pressure receivers must lie in fluid elements");
+  for (int k = 0; k < ad->nrec; ++k)
+    if (!ad->rec_global || ad->rec_global[k] < 0 || ad->rec_global[k] >= cp->nrec_total)
+      return fail(SF2D_ERR_INVALID, "fluid receiver index out of range");
+  for (int k = 0; k < eld->nrec; ++k)
+    if (!cp->el_rec_global || cp->el_rec_global[k] < 0 || cp->el_rec_global[k] >= cp->nrec_total)
+      return fail(SF2D_ERR_INVALID, "solid receiver index out of range");
+  for (long long k = 0; k < static_cast<long long>(ad->nspec) * NGLL2; ++k)
+    if (ad->ibool[k] < 0 || ad->ibool[k] >= ad->nglob) return fail(SF2D_ERR_INVALID, "fluid ibool out of range");
+  for (int k = 0; k < cp->ncpl_ac; ++k)
+    if (cp->cpl_ac_point[k] < 0 || cp->cpl_ac_point[k] >= ad->nglob || cp->cpl_ac_el_point[k] < 0 ||
+        cp->cpl_ac_el_point[k] >= eld->nglob)
+      return fail(SF2D_ERR_INVALID, "coupling point out of range");
+  for (int k = 0; k < cp->ncpl_el; ++k)
+    if (cp->cpl_el_point[k] < 0 || cp->cpl_el_point[k] >= eld->nglob || cp->cpl_el_ac_point[k] < 0 ||
+        cp->cpl_el_ac_point[k] >= ad->nglob)
+      return fail(SF2D_ERR_INVALID, "coupling point out of range");
+  for (int k = 0; k < ad->nstacey; ++k)
+    if (ad->st_iglob[k] < 0 || ad->st_iglob[k] >= ad->nglob) return fail(SF2D_ERR_INVALID, "fluid Stacey point out of range");
+  for (int k = 0; k < ad->nfree; ++k)
+    if (ad->free_iglob[k] < 0 || ad->free_iglob[k] >= ad->nglob) return fail(SF2D_ERR_INVALID, "free-surface point out of range");
+  for (int k = 0; k < ad->nsrc; ++k)
+    if (ad->src_ispec[k] < 0 || ad->src_ispec[k] >= ad->nspec) return fail(SF2D_ERR_INVALID, "fluid source element out of range");
+  for (int k = 0; k < ad->nrec; ++k)
+    if (ad->rec_ispec[k] < 0 || ad->rec_ispec[k] >= ad->nspec) return fail(SF2D_ERR_INVALID, "fluid receiver element out of range");
+
+  auto *C = new sf2d_coupled();
+  std::unique_ptr<sf2d_coupled> guard(C);
+  // the solid sub-solver; its receivers are renumbered into the run's list below
+  sf2d_elastic_desc e2 = *eld;
+  if (e2.seismotype == 4 || e2.seismotype == 0) e2.seismotype = 1;
+  if (int rc = sf2d_create_solver_internal(&e2, false, &C->el)) return rc;
+  sf2d_solver *S = C->el;
+  C->lddrk = S->lddrk;
+  C->nstage = S->nstage;
+  C->nstep = eld->nstep;
+  C->nrec_total = cp->nrec_total;
+  C->nt = S->nt;
+  int rc = 0;
+
+  // ---- fluid tiling and per-slot data
+  const int te = ad->tile_elems > 0 ? ad->tile_elems : 32;
+  std::string err = build_tiling(ad->nspec, ad->nglob, ad->ibool, ad->centroid_xz, te, C->T);
+  if (!err.empty()) return fail(SF2D_ERR_INVALID, "fluid tiling: " + err);
+  const Tiling &T = C->T;
+  const size_t nq = static_cast<size_t>(ad->nspec) * NGLL2;
+  std::vector<float4> geo(nq);
+  std::vector<float> fac(nq);
+  for (int s = 0; s < ad->nspec; ++s) {
+    const size_t src = static_cast<size_t>(T.elem_order[s]) * NGLL2;
+    for (int q = 0; q < NGLL2; ++q) {
+      geo[s * NGLL2 + q] = make_float4(ad->xix[src + q], ad->xiz[src + q], ad->gammax[src + q], ad->gammaz[src + q]);
+      fac[s * NGLL2 + q] = ad->jacobian[src + q] / ad->rhostore[src + q];  // deriv(6) = J / rho in FP32
+    }
+  }
+  std::vector<float> rmass(ad->nglob);
+  std::vector<uint8_t> fmask(ad->nglob, 0);
+  for (int g = 0; g < ad->nglob; ++g) rmass[g] = ad->rmass_inverse[T.dev2glob[g]];
+  for (int k = 0; k < ad->nfree; ++k) fmask[T.glob2dev[ad->free_iglob[k]]] = 1;
+  // a boundary or coupling point goes to the tile of the first element holding it
+  std::vector<int> glob_tile(ad->nglob, -1);
+  for (int e = 0; e < ad->nspec; ++e)
+    for (int q = 0; q < NGLL2; ++q) {
+      const int g = ad->ibool[static_cast<size_t>(e) * NGLL2 + q];
+      if (glob_tile[g] < 0) glob_tile[g] = T.elem_tile[e];
+    }
+  std::vector<TileInfo> tiles = T.tiles;
+  std::vector<std::vector<int>> st_t(T.ntiles), cpl_t(T.ntiles), src_t(T.ntiles), rec_t(T.ntiles);
+  for (int k = 0; k < ad->nstacey; ++k) st_t[glob_tile[ad->st_iglob[k]]].push_back(k);
+  for (int k = 0; k < cp->ncpl_ac; ++k) cpl_t[glob_tile[cp->cpl_ac_point[k]]].push_back(k);
+  for (int k = 0; k < ad->nsrc; ++k) src_t[T.elem_tile[ad->src_ispec[k]]].push_back(k);
+  for (int k = 0; k < ad->nrec; ++k) rec_t[T.elem_tile[ad->rec_ispec[k]]].push_back(k);
+  std::vector<int> st_local, cpl_local, cpl_src, src_local, src_id, rec_id, rec_dev;
+  std::vector<float2> st_wr, src_sk;
+  std::vector<float4> cpl_nw, rec_geo;
+  std::vector<float> rec_rho;
+  std::vector<double> rec_h;
+  for (int t = 0; t < T.ntiles; ++t) {
+    tiles[t].st_off = static_cast<int>(st_local.size());
+    for (int k : st_t[t]) {
+      st_local.push_back(T.local_id(t, ad->st_iglob[k]));
+      st_wr.push_back(make_float2(ad->st_w[k], ad->st_rho_vp[k]));
+    }
+    tiles[t].st_n = static_cast<int>(st_local.size()) - tiles[t].st_off;
+    tiles[t].cpl_off = static_cast<int>(cpl_local.size());
+    for (int k : cpl_t[t]) {
+      cpl_local.push_back(T.local_id(t, cp->cpl_ac_point[k]));
+      cpl_src.push_back(S->T.glob2dev[cp->cpl_ac_el_point[k]]);
+      cpl_nw.push_back(make_float4(cp->cpl_ac_nx[k], cp->cpl_ac_nz[k], cp->cpl_ac_w[k], 0.f));
+    }
+    tiles[t].cpl_n = static_cast<int>(cpl_local.size()) - tiles[t].cpl_off;
+    tiles[t].src_off = static_cast<int>(src_local.size());
+    for (int k : src_t[t])
+      for (int q = 0; q < NGLL2; ++q) {
+        const size_t p = static_cast<size_t>(ad->src_ispec[k]) * NGLL2 + q;
+        src_local.push_back(T.local_id(t, ad->ibool[p]));
+        src_id.push_back(k);
+        src_sk.push_back(make_float2(ad->sourcearrays[static_cast<size_t>(k) * NGLL2 + q], ad->kappastore[p]));
+      }
+    tiles[t].src_n = static_cast<int>(src_local.size()) - tiles[t].src_off;
+    tiles[t].rec_off = static_cast<int>(rec_id.size());
+    for (int k : rec_t[t]) {
+      rec_id.push_back(ad->rec_global[k]);
+      for (int q = 0; q < NGLL2; ++q) {
+        const size_t p = static_cast<size_t>(ad->rec_ispec[k]) * NGLL2 + q;
+        rec_dev.push_back(T.glob2dev[ad->ibool[p]]);
+        rec_geo.push_back(make_float4(ad->xix[p], ad->xiz[p], ad->gammax[p], ad->gammaz[p]));
+        rec_rho.push_back(ad->rhostore[p]);
+      }
+      for (int i = 0; i < 5; ++i) rec_h.push_back(ad->hxir[k * 5 + i]);
+      for (int j = 0; j < 5; ++j) rec_h.push_back(ad->hgammar[k * 5 + j]);
+    }
+    tiles[t].rec_n = static_cast<int>(rec_id.size()) - tiles[t].rec_off;
+  }
+  for (const TileInfo &t : tiles)
+    if (t.rec_n > S->nt) return fail(SF2D_ERR_INVALID, "more fluid receivers in one tile than threads per CTA");
+
+  AcParams &A = C->A;
+  C->nglob = ad->nglob;
+  float *p, *pd, *pdd;
+  if ((rc = C->alloc(&p, ad->nglob)) || (rc = C->alloc(&pd, ad->nglob)) || (rc = C->alloc(&pdd, ad->nglob))) return rc;
+  SF2D_CUDA(cudaMemset(p, 0, sizeof(float) * ad->nglob));
+  SF2D_CUDA(cudaMemset(pd, 0, sizeof(float) * ad->nglob));
+  SF2D_CUDA(cudaMemset(pdd, 0, sizeof(float) * ad->nglob));
+  A.p = p;
+  A.pd = pd;
+  A.pdd = pdd;
+  if (C->lddrk) {
+    float *pl, *pdl;
+    if ((rc = C->alloc(&pl, ad->nglob)) || (rc = C->alloc(&pdl, ad->nglob))) return rc;
+    SF2D_CUDA(cudaMemset(pl, 0, sizeof(float) * ad->nglob));
+    SF2D_CUDA(cudaMemset(pdl, 0, sizeof(float) * ad->nglob));
+    A.pL = pl;
+    A.pdL = pdl;
+    for (int k = 0; k < 6; ++k) {
+      A.alpha[k] = S->P.alpha[k];
+      A.beta[k] = S->P.beta[k];
+    }
+  }
+  if ((rc = C->upload_const(&A.rmass, rmass)) || (rc = C->upload_const(&A.free_mask, fmask)) ||
+      (rc = C->upload_const(&A.tiles, tiles)) || (rc = C->upload_const(&A.lib, T.lib)) ||
+      (rc = C->upload_const(&A.geo, geo)) || (rc = C->upload_const(&A.fac, fac)) ||
+      (rc = C->upload_const(&A.sh_ids, T.sh_ids)) || (rc = C->upload_const(&A.shp_off, T.shp_off)) ||
+      (rc = C->upload_const(&A.shp_slots, T.shp_slots)) || (rc = C->upload_const(&A.st_local, st_local)) ||
+      (rc = C->upload_const(&A.st_wr, st_wr)) || (rc = C->upload_const(&A.cpl_local, cpl_local)) ||
+      (rc = C->upload_const(&A.cpl_src, cpl_src)) || (rc = C->upload_const(&A.cpl_nw, cpl_nw)) ||
+      (rc = C->upload_const(&A.src_local, src_local)) || (rc = C->upload_const(&A.src_id, src_id)) ||
+      (rc = C->upload_const(&A.src_sk, src_sk)) || (rc = C->upload_const(&A.rec_id, rec_id)) ||
+      (rc = C->upload_const(&A.rec_dev, rec_dev)) || (rc = C->upload_const(&A.rec_h, rec_h)) ||
+      (rc = C->upload_const(&A.rec_geo, rec_geo)) || (rc = C->upload_const(&A.rec_rho, rec_rho)))
+    return rc;
+  float *partial;
+  if ((rc = C->alloc(&partial, T.sh_ids.size()))) return rc;
+  A.partial = partial;
+  std::vector<float> stf(static_cast<size_t>(ad->nsrc) * eld->nstep * C->nstage);
+  if (ad->nsrc) {
+    if (!ad->stf || !ad->sourcearrays) return fail(SF2D_ERR_INVALID, "missing fluid source arrays");
+    std::memcpy(stf.data(), ad->stf, stf.size() * sizeof(float));
+  }
+  if ((rc = C->upload_const(&A.stf, stf))) return rc;
+  const size_t nseis = static_cast<size_t>(cp->nrec_total) * eld->nstep * 2;
+  if ((rc = C->alloc(&C->seis, nseis))) return rc;
+  SF2D_CUDA(cudaMemset(C->seis, 0, sizeof(double) * std::max<size_t>(1, nseis)));
+  A.seis = C->seis;
+  if ((rc = C->alloc(&C->ctr, 4))) return rc;
+  SF2D_CUDA(cudaMemset(C->ctr, 0, 4 * sizeof(int)));
+  A.d_step = C->ctr;
+  A.d_step_b = C->ctr + 1;
+  A.d_status = C->ctr + 2;
+  A.u_el = S->P.u;
+  A.v_el = S->P.v;
+  A.a_el = S->P.a;
+  A.nstep_stf = eld->nstep;
+  A.nstage = C->nstage;
+  A.nstep_seis = eld->nstep;
+  A.seismotype = cp->seismotype;
+  A.use_trick = cp->use_trick;
+  A.nrec = ad->nrec;
+  A.cosrot = cp->cosrot;
+  A.sinrot = cp->sinrot;
+  A.dt = eld->deltat;
+  A.dto2 = eld->deltatover2;
+  A.dt2o2 = eld->deltatsquareover2;
+  A.shared_begin = T.shared_begin;
+  A.nshared = T.nshared;
+  A.max_q = T.max_elems * NGLL2;
+  A.max_local = T.max_local;
+  for (int k = 0; k < 60; ++k) A.hconst[k] = S->P.hconst[k];
+  if ((rc = C->upload(&C->d_dev2glob, T.dev2glob.data(), T.dev2glob.size()))) return rc;
+  if ((rc = C->alloc(&C->d_stage, ad->nglob))) return rc;
+  C->smem = ac_smem_layout(A.max_q, A.max_local).total;
+  if (C->smem > 220 * 1024) return fail(SF2D_ERR_INVALID, "fluid tile too large for shared memory");
+  C->tile_fn = pick_ac_tile(C->nt, C->lddrk);
+  {
+    // the limit belongs to the kernel: only ever raise it (see the solid solver)
+    static std::mutex attr_mutex;
+    std::lock_guard<std::mutex> lock(attr_mutex);
+    cudaFuncAttributes fa;
+    SF2D_CUDA(cudaFuncGetAttributes(&fa, C->tile_fn));
+    if (fa.maxDynamicSharedSizeBytes < static_cast<int>(C->smem))
+      SF2D_CUDA(cudaFuncSetAttribute(C->tile_fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(C->smem)));
+  }
+
+  // ---- solid side: receivers into the run's list, coupling entries per tile
+  if (S->nrec > 0) {
+    std::vector<int> ids(S->nrec);
+    SF2D_CUDA(cudaMemcpy(ids.data(), S->P.rec_id, sizeof(int) * S->nrec, cudaMemcpyDeviceToHost));
+    for (int &k : ids) k = cp->el_rec_global[k];
+    SF2D_CUDA(cudaMemcpy(const_cast<int *>(S->P.rec_id), ids.data(), sizeof(int) * S->nrec, cudaMemcpyHostToDevice));
+  }
+  S->P.seis = C->seis;
+  {
+    std::vector<TileInfo> et(S->T.ntiles);
+    SF2D_CUDA(cudaMemcpy(et.data(), S->P.tiles, sizeof(TileInfo) * et.size(), cudaMemcpyDeviceToHost));
+    std::vector<int> eg_tile(eld->nglob, -1);
+    for (int e = 0; e < eld->nspec; ++e)
+      for (int q = 0; q < NGLL2; ++q) {
+        const int g = eld->ibool[static_cast<size_t>(e) * NGLL2 + q];
+        if (eg_tile[g] < 0) eg_tile[g] = S->T.elem_tile[e];
+      }
+    std::vector<std::vector<int>> by_t(S->T.ntiles);
+    for (int k = 0; k < cp->ncpl_el; ++k) by_t[eg_tile[cp->cpl_el_point[k]]].push_back(k);
+    std::vector<int> e_local, e_src;
+    std::vector<float4> e_nw;
+    for (int t = 0; t < S->T.ntiles; ++t) {
+      et[t].cpl_off = static_cast<int>(e_local.size());
+      for (int k : by_t[t]) {
+        e_local.push_back(S->T.local_id(t, cp->cpl_el_point[k]));
+        e_src.push_back(T.glob2dev[cp->cpl_el_ac_point[k]]);
+        e_nw.push_back(make_float4(cp->cpl_el_nx[k], cp->cpl_el_nz[k], cp->cpl_el_w[k], 0.f));
+      }
+      et[t].cpl_n = static_cast<int>(e_local.size()) - et[t].cpl_off;
+    }
+    SF2D_CUDA(cudaMemcpy(const_cast<TileInfo *>(S->P.tiles), et.data(), sizeof(TileInfo) * et.size(),
+                         cudaMemcpyHostToDevice));
+    if ((rc = C->upload_const(&S->P.cpl_local, e_local)) || (rc = C->upload_const(&S->P.cpl_src, e_src)) ||
+        (rc = C->upload_const(&S->P.cpl_nw, e_nw)))
+      return rc;
+    S->P.pdd_ac = A.pdd;
+  }
+  SF2D_CUDA(cudaDeviceSynchronize());
+  *out = guard.release();
+  return SF2D_OK;
+}
+
+extern "C" int sf2d_coupled_run(sf2d_coupled *C, int nstep, double *seismograms) {
+  using namespace sf2d;
+  if (!C || nstep < 0) return fail(SF2D_ERR_INVALID, "bad arguments");
+  const int it0 = C->steps_done;
+  if (seismograms && it0 + nstep > C->nstep) return fail(SF2D_ERR_INVALID, "run exceeds the seismogram buffer length");
+  sf2d_solver *S = C->el;
+  const int K = C->chunk;
+  int done = 0;
+  if (nstep >= K) {
+    if (!C->graph || C->graph_steps != K) {
+      if (C->graph) cudaGraphExecDestroy(C->graph);
+      C->graph = nullptr;
+      cudaGraph_t g;
+      SF2D_CUDA(cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal));
+      C->launch_chunk(K);
+      SF2D_CUDA(cudaStreamEndCapture(S->stream, &g));
+      cudaError_t e = cudaGraphInstantiate(&C->graph, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return fail(SF2D_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+      C->graph_steps = K;
+    }
+    for (; done + K <= nstep; done += K) SF2D_CUDA(cudaGraphLaunch(C->graph, S->stream));
+  }
+  if (done < nstep)
+    if (int rc = C->launch_chunk(nstep - done)) return rc;
+  C->steps_done += nstep;
+  S->steps_done += nstep;
+  SF2D_CUDA(cudaStreamSynchronize(S->stream));
+  int status[2] = {0, 0};
+  SF2D_CUDA(cudaMemcpy(&status[0], S->P.d_status, sizeof(int), cudaMemcpyDeviceToHost));
+  SF2D_CUDA(cudaMemcpy(&status[1], C->A.d_status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (status[0] || status[1]) return fail(SF2D_ERR_UNSTABLE, "wavefield blew up (NaN or |field| > 1e25)");
+  if (seismograms && C->nrec_total && nstep) {
+    SF2D_CUDA(cudaMemcpy2D(seismograms, sizeof(double) * 2 * nstep, C->seis + static_cast<size_t>(it0) * 2,
+                           sizeof(double) * 2 * C->nstep, sizeof(double) * 2 * nstep, C->nrec_total,
+                           cudaMemcpyDeviceToHost));
+  }
+  return SF2D_OK;
+}
+
+extern "C" int sf2d_coupled_get_fields(sf2d_coupled *C, float *displ, float *veloc, float *accel, float *pot,
+                                       float *pot_dot, float *pot_dot_dot) {
+  using namespace sf2d;
+  if (!C) return fail(SF2D_ERR_INVALID, "null solver");
+  if (int rc = sf2d_get_fields(C->el, displ, veloc, accel)) return rc;
+  const float *src[3] = {C->A.p, C->A.pd, C->A.pdd};
+  float *dst[3] = {pot, pot_dot, pot_dot_dot};
+  const int n = C->nglob;
+  cudaStream_t s = C->el->stream;
+  for (int k = 0; k < 3; ++k) {
+    if (!dst[k]) continue;
+    k_scatter_f<<<(n + 255) / 256, 256, 0, s>>>(src[k], C->d_dev2glob, C->d_stage, n);
+    SF2D_CUDA(cudaGetLastError());
+    SF2D_CUDA(cudaMemcpyAsync(dst[k], C->d_stage, sizeof(float) * n, cudaMemcpyDeviceToHost, s));
+    SF2D_CUDA(cudaStreamSynchronize(s));
+  }
+  return SF2D_OK;
+}
+
+extern "C" int sf2d_coupled_set_fields(sf2d_coupled *C, const float *displ, const float *veloc, const float *accel,
+                                       const float *pot, const float *pot_dot, const float *pot_dot_dot) {
+  using namespace sf2d;
+  if (!C) return fail(SF2D_ERR_INVALID, "null solver");
+  if (int rc = sf2d_set_fields(C->el, displ, veloc, accel)) return rc;
+  float *dst[3] = {C->A.p, C->A.pd, C->A.pdd};
+  const float *src[3] = {pot, pot_dot, pot_dot_dot};
+  const int n = C->nglob;
+  cudaStream_t s = C->el->stream;
+  for (int k = 0; k < 3; ++k) {
+    if (!src[k]) {
+      SF2D_CUDA(cudaMemsetAsync(dst[k], 0, sizeof(float) * n, s));
+      continue;
+    }
+    SF2D_CUDA(cudaMemcpyAsync(C->d_stage, src[k], sizeof(float) * n, cudaMemcpyHostToDevice, s));
+    k_gather_f<<<(n + 255) / 256, 256, 0, s>>>(C->d_stage, C->d_dev2glob, dst[k], n);
+    SF2D_CUDA(cudaGetLastError());
+  }
+  SF2D_CUDA(cudaStreamSynchronize(s));
+  return SF2D_OK;
+}
+
+extern "C" int sf2d_coupled_time_kernels(sf2d_coupled *C, int nstep, float *ms) {
+  using namespace sf2d;
+  if (!C || nstep <= 0 || !ms) return fail(SF2D_ERR_INVALID, "bad arguments");
+  sf2d_solver *S = C->el;
+  cudaEvent_t ev[5];
+  for (auto &e : ev) SF2D_CUDA(cudaEventCreate(&e));
+  double acc[4] = {0, 0, 0, 0};
+  for (int k = 0; k < nstep; ++k)
+    for (int st = 0; st < C->nstage; ++st) {
+      const bool rp = k > 0 && st == 0;
+      SF2D_CUDA(cudaEventRecord(ev[0], S->stream));
+      C->launch_ac_tile(rp, st);
+      SF2D_CUDA(cudaEventRecord(ev[1], S->stream));
+      C->launch_ac_shared(st);
+      SF2D_CUDA(cudaEventRecord(ev[2], S->stream));
+      S->launch_tile(rp, st);
+      SF2D_CUDA(cudaEventRecord(ev[3], S->stream));
+      S->launch_shared(st);
+      SF2D_CUDA(cudaEventRecord(ev[4], S->stream));
+      SF2D_CUDA(cudaEventSynchronize(ev[4]));
+      for (int q = 0; q < 4; ++q) {
+        float t = 0.f;
+        SF2D_CUDA(cudaEventElapsedTime(&t, ev[q], ev[q + 1]));
+        acc[q] += t;
+      }
+    }
+  SF2D_CUDA(cudaGetLastError());
+  C->el->launch_receivers();
+  if (C->A.nrec > 0) sf2d::k_acoustic_receivers<<<(C->A.nrec + 127) / 128, 128, 0, S->stream>>>(C->A);
+  SF2D_CUDA(cudaStreamSynchronize(S->stream));
+  C->steps_done += nstep;
+  S->steps_done += nstep;
+  for (auto &e : ev) cudaEventDestroy(e);
+  const double launches = static_cast<double>(nstep) * C->nstage;
+  for (int q = 0; q < 4; ++q) ms[q] = static_cast<float>(acc[q] / launches);
+  ms[4] = static_cast<float>((acc[0] + acc[1] + acc[2] + acc[3]) / nstep);
+  return SF2D_OK;
+}
+
+extern "C" int sf2d_coupled_layout_info(sf2d_coupled *C, long long *info) {
+  using namespace sf2d;
+  if (!C || !info) return fail(SF2D_ERR_INVALID, "bad arguments");
+  info[0] = C->T.ntiles;
+  info[1] = C->T.nshared;
+  info[2] = C->A.max_local;
+  info[3] = static_cast<long long>(C->smem);
+  info[4] = C->T.nglob - C->T.nshared;
+  info[5] = static_cast<long long>(C->T.sh_ids.size());
+  return SF2D_OK;
+}
+
+extern "C" int sf2d_coupled_destroy(sf2d_coupled *C) {
+  delete C;
+  return SF2D_OK;
+}

@@ -72,6 +72,10 @@ struct Params {
   const int *kern_base;
   float2 *kmu_kl;         // per element point (slot order): kappa and mu integrand sums
   float *rho_kl_glob;     // per device point: rho integrand sum
+  // fluid-solid coupling (solid side): tile-local point, fluid device point, (nx, nz, w, 0)
+  const int *cpl_local, *cpl_src;
+  const float4 *cpl_nw;
+  const float *pdd_ac;    // chi_dot_dot of the fluid, fluid device order
   int nstep_stf, nstage, nstep_seis, seismotype, nrec;
   double cosrot, sinrot;
   float dt, dto2, dt2o2;
@@ -82,6 +86,17 @@ struct Params {
 };
 
 constexpr int SHARED_NT = 256;
+
+// Newmark predictor u + dt v + dt^2/2 a and v + dt/2 a in the reference's
+// operation order with every product and sum rounded (no contraction), so
+// that every kernel that forms the predicted field of a point (the tile and
+// shared-point kernels, and the fluid side of the coupling, which needs the
+// solid's predicted displacement before the solid kernels run) gets the
+// same bits (update_displacement_Newmark.F90:353-454).
+__device__ __forceinline__ float newmark_displ(float u, float v, float a, float dt, float dt2o2) {
+  return __fadd_rn(__fadd_rn(u, __fmul_rn(dt, v)), __fmul_rn(dt2o2, a));
+}
+__device__ __forceinline__ float newmark_veloc(float v, float a, float dto2) { return __fadd_rn(v, __fmul_rn(dto2, a)); }
 
 __device__ __forceinline__ void record_receiver(const Params &P, int r, int step) {
   if (step < 0 || step >= P.nstep_seis) return;
@@ -287,10 +302,10 @@ __global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_
     if (!LDDRK) {
       float2 u = s_u[l], v = s_v[l];
       const float2 a = s_acc[l];
-      u.x = u.x + dt * v.x + dt2o2 * a.x;
-      u.y = u.y + dt * v.y + dt2o2 * a.y;
-      v.x = v.x + dto2 * a.x;
-      v.y = v.y + dto2 * a.y;
+      u.x = newmark_displ(u.x, v.x, a.x, dt, dt2o2);
+      u.y = newmark_displ(u.y, v.y, a.y, dt, dt2o2);
+      v.x = newmark_veloc(v.x, a.x, dto2);
+      v.y = newmark_veloc(v.y, a.y, dto2);
       s_u[l] = u;
       s_v[l] = v;
     }
@@ -311,6 +326,17 @@ __global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_
       float2 acc = s_acc[l];
       acc.x -= tx * nw.z;
       acc.y -= tz * nw.z;
+      s_acc[l] = acc;
+    }
+    // pressure of the fluid on the solid, -chi_dot_dot of this step
+    // (compute_coupling_viscoelastic_ac.f90:80-250)
+    for (int p = ti.cpl_off; p < ti.cpl_off + ti.cpl_n; ++p) {
+      const int l = P.cpl_local[p];
+      const float4 nw = P.cpl_nw[p];
+      const float pressure = -P.pdd_ac[P.cpl_src[p]];
+      float2 acc = s_acc[l];
+      acc.x += nw.z * nw.x * pressure;
+      acc.y += nw.z * nw.y * pressure;
       s_acc[l] = acc;
     }
     for (int p = ti.src_off; p < ti.src_off + ti.src_n; ++p) {
@@ -497,10 +523,10 @@ __global__ void __launch_bounds__(SHARED_NT) k_elastic_shared(const Params P, in
     float2 u = P.u[g], v = P.v[g];
     if (!LDDRK) {
       const float2 a0 = P.a[g];
-      u.x = u.x + P.dt * v.x + P.dt2o2 * a0.x;
-      u.y = u.y + P.dt * v.y + P.dt2o2 * a0.y;
-      v.x = v.x + P.dto2 * a0.x;
-      v.y = v.y + P.dto2 * a0.y;
+      u.x = newmark_displ(u.x, v.x, a0.x, P.dt, P.dt2o2);
+      u.y = newmark_displ(u.y, v.y, a0.y, P.dt, P.dt2o2);
+      v.x = newmark_veloc(v.x, a0.x, P.dto2);
+      v.y = newmark_veloc(v.y, a0.y, P.dto2);
     }
     float2 acc = make_float2(0.f, 0.f);
     for (int k = P.shp_off[s]; k < P.shp_off[s + 1]; ++k) {

@@ -34,7 +34,7 @@ struct TileInfo {
   int col_end[MAX_COLOURS];  // exclusive end (element index within tile) of each colour
   int ncol;
   int lib_off;     // offset of the tile's local ibool (multiple of 8 entries = 16 bytes)
-  int pad_[2];
+  int cpl_off, cpl_n;  // fluid-solid coupling entries of this tile (none outside a coupled run)
 };
 static_assert(sizeof(TileInfo) == 24 * 4, "TileInfo layout");
 

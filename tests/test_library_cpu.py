@@ -37,3 +37,21 @@ def test_tiling_invariants(tile_elems):
     assert st["ntiles"] == -(-db.nspec // tile_elems)
     assert st["n_interior"] + st["nshared"] == db.nglob
     assert st["max_colours"] <= 8
+
+
+def test_coupled_split_keeps_every_interface_point():
+    """The fluid/solid split used by the coupled GPU path: both sub-meshes hold
+    every coupling point, solid absorbing points stay in the solid mesh, and
+    receivers are partitioned between the domains."""
+    from specfem2d_b200 import configs
+    from specfem2d_b200.coupled import split
+
+    db = configs.c2_coupled(nstep=10, nrec=8, scale=16)
+    sub, fl, cp, maps = split(db)
+    assert sub.nspec + fl["nspec"] == db.nspec
+    assert (cp["ac_point"] >= 0).all() and (cp["ac_el_point"] >= 0).all()
+    assert (cp["el_point"] >= 0).all() and (cp["el_ac_point"] >= 0).all()
+    g = db.acoustic["cpl_ac_iglob"]
+    assert (maps["fluid_points"][cp["ac_point"]] == g).all() and (maps["solid_points"][cp["ac_el_point"]] == g).all()
+    assert len(fl["rec_global"]) + len(cp["el_rec_global"]) == len(db.rec_ispec)
+    assert sub.ibool.max() == sub.nglob - 1 and fl["ibool"].max() == fl["nglob"] - 1
