@@ -47,6 +47,12 @@ class OracleDb(ctypes.Structure):
         ("ncpl_ac", ctypes.c_int), ("cpl_ac_iglob", _ip), ("cpl_ac_nx", _dp), ("cpl_ac_nz", _dp), ("cpl_ac_w", _dp),
         ("ncpl_el", ctypes.c_int), ("cpl_el_iglob", _ip), ("cpl_el_nx", _dp), ("cpl_el_nz", _dp), ("cpl_el_w", _dp),
         ("use_trick", ctypes.c_int),
+        ("pml_region", _ip),
+        ("pml_K_x", _dp), ("pml_K_z", _dp), ("pml_d_x", _dp), ("pml_d_z", _dp), ("pml_alpha_x", _dp),
+        ("pml_alpha_z", _dp),
+        ("npml_bnd_el", ctypes.c_int), ("npml_bnd_ac", ctypes.c_int), ("pml_bnd_el", _ip), ("pml_bnd_ac", _ip),
+        ("cpl_ac_elpt", _ip), ("cpl_el_acpt", _ip),
+        ("DT", ctypes.c_double),
     ]
 
 
@@ -183,6 +189,17 @@ class Oracle:
             s.cpl_el_iglob = i(ac["cpl_el_iglob"])
             s.cpl_el_nx, s.cpl_el_nz, s.cpl_el_w = d(ac["cpl_el_nx"]), d(ac["cpl_el_nz"]), d(ac["cpl_el_w"])
             s.use_trick = int(bool(ac.get("use_trick", False)))
+            if "cpl_ac_elpt" in ac:
+                s.cpl_ac_elpt, s.cpl_el_acpt = i(ac["cpl_ac_elpt"]), i(ac["cpl_el_acpt"])
+        s.DT = float(src.dt)
+        pm = getattr(src, "pml", None)
+        if pm is not None:
+            s.pml_region = i(pm["region"])
+            s.pml_K_x, s.pml_K_z = d(pm["K_x"]), d(pm["K_z"])
+            s.pml_d_x, s.pml_d_z = d(pm["d_x"]), d(pm["d_z"])
+            s.pml_alpha_x, s.pml_alpha_z = d(pm["alpha_x"]), d(pm["alpha_z"])
+            s.npml_bnd_el, s.pml_bnd_el = len(pm["bnd_el"]), i(pm["bnd_el"])
+            s.npml_bnd_ac, s.pml_bnd_ac = len(pm["bnd_ac"]), i(pm["bnd_ac"])
         if adj_src is not None:
             s.adj_src = d(adj_src)
             s.nstep_total = int(np.asarray(adj_src).shape[1])

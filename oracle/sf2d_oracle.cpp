@@ -61,6 +61,87 @@ std::vector<real> cvt(const double *p, size_t n) {
   return v;
 }
 
+constexpr int CPML_X_ONLY = 1, CPML_Z_ONLY = 2, CPML_XZ = 3;
+
+// compute_coef_convolution (pml_compute.f90:34-86)
+void coef_convolution(double bb, double DT, double &c0, double &c1, double &c2) {
+  const double temp = std::exp(-0.5 * bb * DT);
+  c0 = temp * temp;
+  if (std::fabs(bb) > 1e-5) {
+    c1 = (1.0 - temp) / bb;
+    c2 = c1 * temp;
+  } else {
+    c1 = 0.5 * DT;
+    c2 = c1;
+  }
+}
+
+struct PmlCoef {
+  double A0, A1, A2, A3, A4, bb1, bb2, c0_1, c1_1, c2_1, c0_2, c1_2, c2_2;
+};
+
+// lik_parameter_computation (pml_compute.f90:90-169): coefficients of the
+// memory variables of one strain component; index_ik 13 or 31 swaps the roles
+// of the X-only and Z-only regions.
+PmlCoef lik_parameters(double DT, double kx, double bx, double ax, double kz, double bz, double az, int region,
+                       int index_ik) {
+  const int xo = index_ik == 13 ? CPML_X_ONLY : CPML_Z_ONLY;
+  const int zo = index_ik == 13 ? CPML_Z_ONLY : CPML_X_ONLY;
+  PmlCoef L{};
+  if (region == CPML_XZ) {
+    L.A0 = kx / kz;
+    const double gx = (ax * bz + ax * ax + 2.0 * bx * az - 2.0 * ax * (bx + az)) / (bz - ax);
+    const double gz = (ax * bz + bz * bz + 2.0 * bx * az - 2.0 * bz * (bx + az)) / (ax - bz);
+    L.A1 = L.A0 / 2.0 * (gx - ax);
+    L.A2 = L.A0 / 2.0 * (gz - bz);
+  } else if (region == xo) {
+    L.A0 = kx;
+    L.A1 = -(L.A0 * (ax - bx));
+    L.A2 = 0.0;
+  } else if (region == zo) {
+    L.A0 = 1.0 / kz;
+    L.A1 = 0.0;
+    L.A2 = -(L.A0 * (bz - az));
+  }
+  L.bb1 = ax;
+  coef_convolution(L.bb1, DT, L.c0_1, L.c1_1, L.c2_1);
+  L.bb2 = bz;
+  coef_convolution(L.bb2, DT, L.c0_2, L.c1_2, L.c2_2);
+  return L;
+}
+
+// l_parameter_computation (pml_compute.f90:284-359): coefficients of the
+// acceleration contribution and of the field memory variables.
+PmlCoef l_parameters(double DT, double kx, double bx, double ax, double kz, double bz, double az, int region) {
+  PmlCoef L{};
+  if (region == CPML_XZ) {
+    L.A0 = kx * kz;
+    const double gx = (ax * az + ax * ax + 2.0 * bx * bz - 2.0 * ax * (bx + bz)) / (az - ax);
+    const double gz = (ax * az + az * az + 2.0 * bx * bz - 2.0 * az * (bx + bz)) / (ax - az);
+    L.A1 = L.A0 / 2.0 * (gx - ax + gz - az);
+    L.A2 = L.A0 / 2.0 * (ax * ax - gx * ax + az * az - gz * az);
+    L.A3 = L.A0 / 2.0 * (ax * ax) * (gx - ax);
+    L.A4 = L.A0 / 2.0 * (az * az) * (gz - az);
+  } else if (region == CPML_X_ONLY) {
+    L.A0 = kx;
+    L.A1 = L.A0 * (bx - ax);
+    L.A2 = -(L.A0 * ax * (bx - ax));
+    L.A3 = L.A0 * (ax * ax) * (bx - ax);
+    L.A4 = 0.0;
+  } else if (region == CPML_Z_ONLY) {
+    L.A0 = kz;
+    L.A1 = L.A0 * (bz - az);
+    L.A2 = -(L.A0 * az * (bz - az));
+    L.A3 = 0.0;
+    L.A4 = L.A0 * (az * az) * (bz - az);
+  }
+  L.bb1 = ax;
+  coef_convolution(L.bb1, DT, L.c0_1, L.c1_1, L.c2_1);
+  L.bb2 = az;
+  coef_convolution(L.bb2, DT, L.c0_2, L.c1_2, L.c2_2);
+  return L;
+}
+
 struct StateBase {
   virtual ~StateBase() = default;
   virtual int run(int nstep, double *seis, int nthreads) = 0;
@@ -96,9 +177,39 @@ struct State : StateBase {
   std::vector<real> cpl_ac_nx, cpl_ac_nz, cpl_ac_w, cpl_el_nx, cpl_el_nz, cpl_el_w;
   std::vector<real> pot, pot_d, pot_dd, pot_l, pot_d_l;     // nglob
   std::vector<real> contrib_ac;                             // nspec*25
+  // CPML
+  bool pml = false;
+  std::vector<real> rm_el, rm_el_l;       // nspec*25*8: dux_dx, dux_dx', duz_dx, duz_dx' (zx), dux_dz.., duz_dz.. (xz)
+  std::vector<real> rm_displ, rm_displ_l; // nspec*25*4: (bb1, x), (bb1, z), (bb2, x), (bb2, z)
+  std::vector<real> rm_ac, rm_ac_l;       // nspec*25*4: dchi_dx (2, zx), dchi_dz (2, xz)
+  std::vector<real> rm_pot, rm_pot_l;     // nspec*25*2
+  std::vector<real> rm_fsb, rm_fsb_l;     // 2 per fluid-side coupling entry
+  std::vector<real> rm_sfb, rm_sfb_l;     // 1 per solid-side coupling entry
+  std::vector<real> displ_old, pot_old;
+  std::vector<real> contrib_pml, contrib_ac_pml;
   int it = 0;  // steps done
 
   bool is_acoustic(int e) const { return acoustic && d.ispec_is_acoustic[e] != 0; }
+  int pml_region(int e) const { return pml ? d.pml_region[e] : 0; }
+  void pml_params(size_t p, double &kx, double &bx, double &ax, double &kz, double &bz, double &az) const {
+    kx = d.pml_K_x[p];
+    kz = d.pml_K_z[p];
+    ax = d.pml_alpha_x[p];
+    az = d.pml_alpha_z[p];
+    bx = ax + d.pml_d_x[p] / kx;
+    bz = az + d.pml_d_z[p] / kz;
+  }
+  // Newmark memory-variable update r = c0 r + c1 f + c2 f_old, or the LDDRK
+  // stage r_L = alpha r_L + dt (-bb r + f), r += beta r_L; coefficients in double
+  void rm_update(real &r, real &rl, double c0, double c1, double c2, double bb, real f, real fold, int stage) {
+    if (d.time_scheme == 1) {
+      r = static_cast<real>(c0 * static_cast<double>(r) + c1 * static_cast<double>(f) + c2 * static_cast<double>(fold));
+    } else {
+      rl = static_cast<real>(static_cast<double>(alpha[stage] * rl) +
+                             static_cast<double>(deltat) * (-bb * static_cast<double>(r) + static_cast<double>(f)));
+      r = r + beta[stage] * rl;
+    }
+  }
 
   explicit State(const sf2d_oracle_db *p) : d(*p) {
     nspec = d.nspec;
@@ -200,13 +311,60 @@ struct State : StateBase {
       }
       contrib_ac.assign(nl, 0);
     }
+    pml = d.pml_region != nullptr;
+    if (pml) {
+      rm_el.assign(nl * 8, 0);
+      rm_displ.assign(nl * 4, 0);
+      displ_old.assign(static_cast<size_t>(nglob) * 2, 0);
+      contrib_pml.assign(nl * 2, 0);
+      if (d.time_scheme != 1) {
+        rm_el_l.assign(nl * 8, 0);
+        rm_displ_l.assign(nl * 4, 0);
+      }
+      if (acoustic) {
+        rm_ac.assign(nl * 4, 0);
+        rm_pot.assign(nl * 2, 0);
+        pot_old.assign(nglob, 0);
+        contrib_ac_pml.assign(nl, 0);
+        rm_fsb.assign(static_cast<size_t>(d.ncpl_ac) * 2, 0);
+        rm_sfb.assign(d.ncpl_el, 0);
+        if (d.time_scheme != 1) {
+          rm_ac_l.assign(nl * 4, 0);
+          rm_pot_l.assign(nl * 2, 0);
+          rm_fsb_l.assign(static_cast<size_t>(d.ncpl_ac) * 2, 0);
+          rm_sfb_l.assign(d.ncpl_el, 0);
+        }
+      }
+    }
+  }
+
+  // Zeroes the outer PML edge points (pml_boundary_elastic/_acoustic, pml_compute.f90:502-574)
+  void pml_boundary_elastic() {
+    for (int k = 0; k < (pml ? d.npml_bnd_el : 0); ++k) {
+      const int g = d.pml_bnd_el[k];
+      for (int c = 0; c < 2; ++c) {
+        displ_old[2 * g + c] = 0;
+        displ[2 * g + c] = 0;
+        veloc[2 * g + c] = 0;
+        accel[2 * g + c] = 0;
+      }
+    }
+  }
+  void pml_boundary_acoustic() {
+    for (int k = 0; k < (pml ? d.npml_bnd_ac : 0); ++k) {
+      const int g = d.pml_bnd_ac[k];
+      pot_old[g] = 0;
+      pot[g] = 0;
+      pot_d[g] = 0;
+      pot_dd[g] = 0;
+    }
   }
 
   // Acoustic element force for one element (compute_forces_viscoacoustic.f90:
   // 105-125 gather, :420-470 mxm_2comp_singleA, :142-152 mapping, :226-238
   // fac = J / rho weak-form terms, :306-322 weighted transpose contraction).
   // Writes the 25 sums to be subtracted from chi_dot_dot.
-  void acoustic_element_force(int ispec, real *out) {
+  void acoustic_element_force(int ispec, int stage_, real *out, real *pml_out) {
     const size_t off = static_cast<size_t>(ispec) * NGLL2;
     real pe[NGLL][NGLL];  // [j][i]
     for (int j = 0; j < NGLL; ++j)
@@ -220,8 +378,46 @@ struct State : StateBase {
                           pe[3][i] * hprime[j][3] + pe[4][i] * hprime[j][4];
         const size_t p = off + j * NGLL + i;
         const real xixl = xix[p], xizl = xiz[p], gammaxl = gammax[p], gammazl = gammaz[p];
-        const real dxl = dxi * xixl + dgam * gammaxl;
-        const real dzl = dxi * xizl + dgam * gammazl;
+        real dxl = dxi * xixl + dgam * gammaxl;
+        real dzl = dxi * xizl + dgam * gammazl;
+        const int region = pml_region(ispec);
+        if (region > 0) {
+          // pml_compute_memory_variables_acoustic (pml_compute_memory_variables.f90:42-224)
+          real dxi_o = 0, dgam_o = 0;
+          if (d.time_scheme == 1)
+            for (int k = 0; k < NGLL; ++k) {
+              dxi_o = dxi_o + pot_old[d.ibool[off + j * NGLL + k]] * hprime[i][k];
+              dgam_o = dgam_o + pot_old[d.ibool[off + k * NGLL + i]] * hprime[j][k];
+            }
+          const real dxl_o = dxi_o * xixl + dgam_o * gammaxl, dzl_o = dxi_o * xizl + dgam_o * gammazl;
+          double kx, bx, ax, kz, bz, az;
+          pml_params(p, kx, bx, ax, kz, bz, az);
+          const PmlCoef zx = lik_parameters(d.DT, kz, bz, az, kx, bx, ax, region, 31);
+          const PmlCoef xz = lik_parameters(d.DT, kx, bx, ax, kz, bz, az, region, 13);
+          real *r = &rm_ac[p * 4];
+          real dummy[4] = {0, 0, 0, 0};
+          real *rl = d.time_scheme == 1 ? dummy : &rm_ac_l[p * 4];
+          rm_update(r[0], rl[0], zx.c0_1, zx.c1_1, zx.c2_1, zx.bb1, dxl, dxl_o, stage_);
+          rm_update(r[1], rl[1], zx.c0_2, zx.c1_2, zx.c2_2, zx.bb2, dxl, dxl_o, stage_);
+          rm_update(r[2], rl[2], xz.c0_1, xz.c1_1, xz.c2_1, xz.bb1, dzl, dzl_o, stage_);
+          rm_update(r[3], rl[3], xz.c0_2, xz.c1_2, xz.c2_2, xz.bb2, dzl, dzl_o, stage_);
+          const real pdx = dxl, pdz = dzl;
+          dxl = static_cast<real>(zx.A0 * pdx + zx.A1 * r[0] + zx.A2 * r[1]);
+          dzl = static_cast<real>(xz.A0 * pdz + xz.A1 * r[2] + xz.A2 * r[3]);
+          // pml_compute_accel_contribution_acoustic (pml_compute_accel_contribution.f90:42-180)
+          const int g = d.ibool[p];
+          const real fac2 = jacobian[p] / kappa[p];
+          const PmlCoef L = l_parameters(d.DT, kx, bx, ax, kz, bz, az, region);
+          real *rp = &rm_pot[p * 2];
+          real dummy2[2] = {0, 0};
+          real *rpl = d.time_scheme == 1 ? dummy2 : &rm_pot_l[p * 2];
+          const real po = d.time_scheme == 1 ? pot_old[g] : real(0);
+          rm_update(rp[0], rpl[0], L.c0_1, L.c1_1, L.c2_1, L.bb1, pot[g], po, stage_);
+          rm_update(rp[1], rpl[1], L.c0_2, L.c1_2, L.c2_2, L.bb2, pot[g], po, stage_);
+          const real wwf = wxgll[i] * wzgll[j] * fac2;
+          pml_out[j * NGLL + i] = static_cast<real>(static_cast<double>(wwf) *
+                                                    (L.A1 * pot_d[g] + L.A2 * pot[g] + L.A3 * rp[0] + L.A4 * rp[1]));
+        }
         const real fac = jacobian[p] / rho[p];
         t1[j][i] = fac * (xixl * dxl + xizl * dzl);
         t2[j][i] = fac * (gammaxl * dxl + gammazl * dzl);
@@ -250,13 +446,33 @@ struct State : StateBase {
   // compute_forces_viscoacoustic_calling_routine.F90:40-233 with one process
   // (phase 1 holds no element: boundary terms first, then all elements).
   void acoustic_forces(int stage, int nt) {
+    pml_boundary_acoustic();
     for (int p = 0; p < d.nstacey_ac; ++p) {
       const int g = d.st_ac_iglob[p];
       pot_dd[g] = pot_dd[g] - pot_d[g] * st_ac_w[p] / st_ac_rvp[p];
     }
     for (int p = 0; p < d.ncpl_ac; ++p) {
       const int g = d.cpl_ac_iglob[p];
-      const real displ_n = displ[2 * g] * cpl_ac_nx[p] + displ[2 * g + 1] * cpl_ac_nz[p];
+      real ux = displ[2 * g], uz = displ[2 * g + 1];
+      if (pml && d.pml_region[d.cpl_ac_elpt[p] / NGLL2] > 0) {
+        // solid element in a PML layer (compute_coupling_acoustic_el.f90:78-140)
+        const size_t q = d.cpl_ac_elpt[p];
+        const int region = d.pml_region[q / NGLL2];
+        double kx, bx, ax, kz, bz, az;
+        pml_params(q, kx, bx, ax, kz, bz, az);
+        const PmlCoef L = region == CPML_X_ONLY ? lik_parameters(d.DT, kx, bx, ax, kz, bz, az, region, 13)
+                                                : lik_parameters(d.DT, kz, bz, az, kx, bx, ax, region, 31);
+        real *rf = &rm_fsb[p * 2];
+        real dummy[2] = {0, 0};
+        real *rfl = d.time_scheme == 1 ? dummy : &rm_fsb_l[p * 2];
+        const real ox = d.time_scheme == 1 ? displ_old[2 * g] : real(0);
+        const real oz = d.time_scheme == 1 ? displ_old[2 * g + 1] : real(0);
+        rm_update(rf[0], rfl[0], L.c0_1, L.c1_1, L.c2_1, L.bb1, ux, ox, stage);
+        rm_update(rf[1], rfl[1], L.c0_1, L.c1_1, L.c2_1, L.bb1, uz, oz, stage);
+        ux = static_cast<real>(L.A0 * displ[2 * g] + L.A1 * rf[0]);
+        uz = static_cast<real>(L.A0 * displ[2 * g + 1] + L.A1 * rf[1]);
+      }
+      const real displ_n = ux * cpl_ac_nx[p] + uz * cpl_ac_nz[p];
       pot_dd[g] = pot_dd[g] + cpl_ac_w[p] * displ_n;
     }
     for (int isrc = 0; isrc < d.nsrc; ++isrc) {
@@ -276,14 +492,21 @@ struct State : StateBase {
     }
     parallel_for(nspec, nspec > 256 ? nt : 1, [&](int b, int e1_) {
       for (int e = b; e < e1_; ++e)
-        if (is_acoustic(e)) acoustic_element_force(e, &contrib_ac[static_cast<size_t>(e) * NGLL2]);
+        if (is_acoustic(e))
+          acoustic_element_force(e, stage, &contrib_ac[static_cast<size_t>(e) * NGLL2],
+                                 pml ? &contrib_ac_pml[static_cast<size_t>(e) * NGLL2] : nullptr);
     });
     for (int e = 0; e < nspec; ++e) {
       if (!is_acoustic(e)) continue;
       const real *c = &contrib_ac[static_cast<size_t>(e) * NGLL2];
       const int *ib = &d.ibool[static_cast<size_t>(e) * NGLL2];
       for (int q = 0; q < NGLL2; ++q) pot_dd[ib[q]] = pot_dd[ib[q]] - c[q];
+      if (pml_region(e) > 0) {
+        const real *cp = &contrib_ac_pml[static_cast<size_t>(e) * NGLL2];
+        for (int q = 0; q < NGLL2; ++q) pot_dd[ib[q]] = pot_dd[ib[q]] - cp[q];
+      }
     }
+    pml_boundary_acoustic();
   }
 
   // Memory-variable update at one GLL point; returns the three sums.
@@ -339,7 +562,7 @@ struct State : StateBase {
   // isotropic P-SV stress with lambda = rho*cp^2 - 2 mu, :372-445 anisotropic,
   // :481-503 attenuation, :669-675 weak-form terms, :760-782 weighted transpose
   // contraction).  Writes the 25x2 contributions (to be subtracted) into `out`.
-  void element_force(int ispec, int stage, real *out) {
+  void element_force(int ispec, int stage, real *out, real *pml_out) {
     const size_t off = static_cast<size_t>(ispec) * NGLL2;
     real ux[NGLL][NGLL], uz[NGLL][NGLL];  // [j][i]
     for (int j = 0; j < NGLL; ++j)
@@ -363,27 +586,89 @@ struct State : StateBase {
         const size_t p = off + j * NGLL + i;
         const real xixl = xix[p], xizl = xiz[p], gammaxl = gammax[p], gammazl = gammaz[p];
         const real jacobianl = jacobian[p];
-        const real dux_dxl = dux_dxi * xixl + dux_dgamma * gammaxl;
-        const real dux_dzl = dux_dxi * xizl + dux_dgamma * gammazl;
-        const real duz_dxl = duz_dxi * xixl + duz_dgamma * gammaxl;
-        const real duz_dzl = duz_dxi * xizl + duz_dgamma * gammazl;
+        real dux_dxl = dux_dxi * xixl + dux_dgamma * gammaxl;
+        real dux_dzl = dux_dxi * xizl + dux_dgamma * gammazl;
+        real duz_dxl = duz_dxi * xixl + duz_dgamma * gammaxl;
+        real duz_dzl = duz_dxi * xizl + duz_dgamma * gammazl;
+        // unmodified strains, kept for the PML stress (compute_forces_viscoelastic.F90:600-610)
+        const real p_dux_dxl = dux_dxl, p_dux_dzl = dux_dzl, p_duz_dxl = duz_dxl, p_duz_dzl = duz_dzl;
+        const int region = pml_region(ispec);
+        if (region > 0) {
+          // pml_compute_memory_variables_elastic (pml_compute_memory_variables.f90:230-540)
+          real dxi_ox = 0, dxi_oz = 0, dg_ox = 0, dg_oz = 0;
+          if (d.time_scheme == 1)
+            for (int k = 0; k < NGLL; ++k) {
+              const int gr = d.ibool[off + j * NGLL + k], gc = d.ibool[off + k * NGLL + i];
+              dxi_ox = dxi_ox + displ_old[2 * gr] * hprime[i][k];
+              dxi_oz = dxi_oz + displ_old[2 * gr + 1] * hprime[i][k];
+              dg_ox = dg_ox + displ_old[2 * gc] * hprime[j][k];
+              dg_oz = dg_oz + displ_old[2 * gc + 1] * hprime[j][k];
+            }
+          const real o_dux_dxl = dxi_ox * xixl + dg_ox * gammaxl, o_dux_dzl = dxi_ox * xizl + dg_ox * gammazl;
+          const real o_duz_dxl = dxi_oz * xixl + dg_oz * gammaxl, o_duz_dzl = dxi_oz * xizl + dg_oz * gammazl;
+          double kx, bx, ax, kz, bz, az;
+          pml_params(p, kx, bx, ax, kz, bz, az);
+          const PmlCoef zx = lik_parameters(d.DT, kz, bz, az, kx, bx, ax, region, 31);
+          const PmlCoef xz = lik_parameters(d.DT, kx, bx, ax, kz, bz, az, region, 13);
+          real *r = &rm_el[p * 8];
+          real dummy[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+          real *rl = d.time_scheme == 1 ? dummy : &rm_el_l[p * 8];
+          rm_update(r[0], rl[0], zx.c0_1, zx.c1_1, zx.c2_1, zx.bb1, p_dux_dxl, o_dux_dxl, stage);
+          rm_update(r[1], rl[1], zx.c0_2, zx.c1_2, zx.c2_2, zx.bb2, p_dux_dxl, o_dux_dxl, stage);
+          rm_update(r[2], rl[2], zx.c0_1, zx.c1_1, zx.c2_1, zx.bb1, p_duz_dxl, o_duz_dxl, stage);
+          rm_update(r[3], rl[3], zx.c0_2, zx.c1_2, zx.c2_2, zx.bb2, p_duz_dxl, o_duz_dxl, stage);
+          rm_update(r[4], rl[4], xz.c0_1, xz.c1_1, xz.c2_1, xz.bb1, p_dux_dzl, o_dux_dzl, stage);
+          rm_update(r[5], rl[5], xz.c0_2, xz.c1_2, xz.c2_2, xz.bb2, p_dux_dzl, o_dux_dzl, stage);
+          rm_update(r[6], rl[6], xz.c0_1, xz.c1_1, xz.c2_1, xz.bb1, p_duz_dzl, o_duz_dzl, stage);
+          rm_update(r[7], rl[7], xz.c0_2, xz.c1_2, xz.c2_2, xz.bb2, p_duz_dzl, o_duz_dzl, stage);
+          dux_dxl = static_cast<real>(zx.A0 * p_dux_dxl + zx.A1 * r[0] + zx.A2 * r[1]);
+          duz_dxl = static_cast<real>(zx.A0 * p_duz_dxl + zx.A1 * r[2] + zx.A2 * r[3]);
+          dux_dzl = static_cast<real>(xz.A0 * p_dux_dzl + xz.A1 * r[4] + xz.A2 * r[5]);
+          duz_dzl = static_cast<real>(xz.A0 * p_duz_dzl + xz.A1 * r[6] + xz.A2 * r[7]);
+          // pml_compute_accel_contribution_elastic (pml_compute_accel_contribution.f90:187-333)
+          const int g = d.ibool[p];
+          const real fac = rho[p] * jacobianl;
+          const PmlCoef L = l_parameters(d.DT, kx, bx, ax, kz, bz, az, region);
+          real *rd = &rm_displ[p * 4];
+          real dummy2[4] = {0, 0, 0, 0};
+          real *rdl = d.time_scheme == 1 ? dummy2 : &rm_displ_l[p * 4];
+          const real ox = d.time_scheme == 1 ? displ_old[2 * g] : real(0);
+          const real oz = d.time_scheme == 1 ? displ_old[2 * g + 1] : real(0);
+          rm_update(rd[0], rdl[0], L.c0_1, L.c1_1, L.c2_1, L.bb1, ux[j][i], ox, stage);
+          rm_update(rd[1], rdl[1], L.c0_1, L.c1_1, L.c2_1, L.bb1, uz[j][i], oz, stage);
+          rm_update(rd[2], rdl[2], L.c0_2, L.c1_2, L.c2_2, L.bb2, ux[j][i], ox, stage);
+          rm_update(rd[3], rdl[3], L.c0_2, L.c1_2, L.c2_2, L.bb2, uz[j][i], oz, stage);
+          const double wwf = static_cast<double>(wxgll[i] * wzgll[j] * fac);
+          pml_out[2 * (j * NGLL + i)] = static_cast<real>(
+              wwf * (L.A1 * veloc[2 * g] + L.A2 * ux[j][i] + L.A3 * rd[0] + L.A4 * rd[2]));
+          pml_out[2 * (j * NGLL + i) + 1] = static_cast<real>(
+              wwf * (L.A1 * veloc[2 * g + 1] + L.A2 * uz[j][i] + L.A3 * rd[1] + L.A4 * rd[3]));
+        }
         const real mul = mu[p];
         const real rhol = rho[p];
         const real cpl = rho_vp[p] / rhol;
         const real lambdal = rhol * cpl * cpl - real(2) * mul;
         const real lambdaplus2mu = lambdal + real(2) * mul;
         const real lambdalplusmul = lambdal + mul;
-        real sigma_xx, sigma_zz, sigma_xz;
-        if (!is_aniso) {
+        real sigma_xx, sigma_zz, sigma_xz, sigma_zx;
+        if (region > 0) {
+          // PML stress: modified strains on the diagonal pairs, not symmetric
+          sigma_xx = lambdaplus2mu * dux_dxl + lambdal * p_duz_dzl;
+          sigma_zz = lambdaplus2mu * duz_dzl + lambdal * p_dux_dxl;
+          sigma_zx = mul * (p_duz_dxl + dux_dzl);
+          sigma_xz = mul * (p_dux_dzl + duz_dxl);
+        } else if (!is_aniso) {
           sigma_xx = lambdaplus2mu * dux_dxl + lambdal * duz_dzl;
           sigma_zz = lambdaplus2mu * duz_dzl + lambdal * dux_dxl;
           sigma_xz = mul * (duz_dxl + dux_dzl);
+          sigma_zx = sigma_xz;
         } else {
           // c_ij are read as double in the reference (compute_forces_viscoelastic.F90:112)
           const double C11 = c11[p], C13 = c13[p], C15 = c15[p], C33 = c33[p], C35 = c35[p], C55 = c55[p];
           sigma_xx = static_cast<real>(C11 * dux_dxl + C13 * duz_dzl + C15 * (duz_dxl + dux_dzl));
           sigma_zz = static_cast<real>(C13 * dux_dxl + C33 * duz_dzl + C35 * (duz_dxl + dux_dzl));
           sigma_xz = static_cast<real>(C15 * dux_dxl + C35 * duz_dzl + C55 * (duz_dxl + dux_dzl));
+          sigma_zx = sigma_xz;
         }
         if (atten) {
           real e1s, e11s, e13s;
@@ -391,8 +676,8 @@ struct State : StateBase {
           sigma_xx = sigma_xx + lambdalplusmul * e1s + real(2) * mul * e11s;
           sigma_xz = sigma_xz + mul * e13s;
           sigma_zz = sigma_zz + lambdalplusmul * e1s - real(2) * mul * e11s;
+          sigma_zx = sigma_xz;
         }
-        const real sigma_zx = sigma_xz;
         t1x[j][i] = jacobianl * (sigma_xx * xixl + sigma_zx * xizl);
         t1z[j][i] = jacobianl * (sigma_xz * xixl + sigma_zz * xizl);
         t2x[j][i] = jacobianl * (sigma_xx * gammaxl + sigma_zx * gammazl);
@@ -424,10 +709,23 @@ struct State : StateBase {
       accel[2 * g] = accel[2 * g] - tx * st_w[p];
       accel[2 * g + 1] = accel[2 * g + 1] - tz * st_w[p];
     }
+    pml_boundary_elastic();
     // fluid pressure on the solid (compute_coupling_viscoelastic_ac.f90:80-250)
     for (int p = 0; p < (acoustic ? d.ncpl_el : 0); ++p) {
       const int g = d.cpl_el_iglob[p];
-      const real pressure = -pot_dd[g];
+      real pressure = -pot_dd[g];
+      if (pml && d.pml_region[d.cpl_el_acpt[p] / NGLL2] > 0) {
+        // fluid element in a PML layer (:100-150)
+        const size_t q = d.cpl_el_acpt[p];
+        double kx, bx, ax, kz, bz, az;
+        pml_params(q, kx, bx, ax, kz, bz, az);
+        const PmlCoef L = l_parameters(d.DT, kx, bx, ax, kz, bz, az, d.pml_region[q / NGLL2]);
+        real dummy = 0;
+        real &rl = d.time_scheme == 1 ? dummy : rm_sfb_l[p];
+        rm_update(rm_sfb[p], rl, L.c0_1, L.c1_1, L.c2_1, L.bb1, pot[g], d.time_scheme == 1 ? pot_old[g] : real(0),
+                  stage);
+        pressure = static_cast<real>(-(L.A0 * pot_dd[g] + L.A1 * pot_d[g] + L.A2 * pot[g] + L.A3 * rm_sfb[p]));
+      }
       accel[2 * g] = accel[2 * g] + cpl_el_w[p] * cpl_el_nx[p] * pressure;
       accel[2 * g + 1] = accel[2 * g + 1] + cpl_el_w[p] * cpl_el_nz[p] * pressure;
     }
@@ -463,7 +761,9 @@ struct State : StateBase {
     }
     parallel_for(nspec, nspec > 256 ? nt : 1, [&](int b, int e1_) {
       for (int e = b; e < e1_; ++e)
-        if (!is_acoustic(e)) element_force(e, stage, &contrib[static_cast<size_t>(e) * NGLL2 * 2]);
+        if (!is_acoustic(e))
+          element_force(e, stage, &contrib[static_cast<size_t>(e) * NGLL2 * 2],
+                        pml ? &contrib_pml[static_cast<size_t>(e) * NGLL2 * 2] : nullptr);
     });
     for (int e = 0; e < nspec; ++e) {
       if (is_acoustic(e)) continue;
@@ -473,6 +773,15 @@ struct State : StateBase {
         const int g = ib[q];
         accel[2 * g] = accel[2 * g] - c[2 * q];
         accel[2 * g + 1] = accel[2 * g + 1] - c[2 * q + 1];
+      }
+      if (pml_region(e) > 0) {
+        // the element's PML contribution after its weak-form terms (compute_forces_viscoelastic.F90:785-797)
+        const real *cp = &contrib_pml[static_cast<size_t>(e) * NGLL2 * 2];
+        for (int q = 0; q < NGLL2; ++q) {
+          const int g = ib[q];
+          accel[2 * g] = accel[2 * g] - cp[2 * q];
+          accel[2 * g + 1] = accel[2 * g + 1] - cp[2 * q + 1];
+        }
       }
     }
   }
@@ -551,6 +860,15 @@ struct State : StateBase {
     const size_t ng = static_cast<size_t>(nglob) * 2;
     for (int s = 0; s < nstep; ++s, ++it) {
       if (d.time_scheme == 1) {
+        if (pml) {
+          // mid-step fields of the CPML convolutions (update_displacement_Newmark.F90:374-380, 429-433)
+          const double h = static_cast<double>(deltatsquareover2) / 2.0;
+          for (size_t g = 0; g < ng; ++g)
+            displ_old[g] = static_cast<real>(static_cast<double>(displ[g]) + h * static_cast<double>(accel[g]));
+          if (acoustic)
+            for (int g = 0; g < nglob; ++g)
+              pot_old[g] = static_cast<real>(static_cast<double>(pot[g]) + h * static_cast<double>(pot_dd[g]));
+        }
         // predictor (update_displacement_Newmark.F90:408-454)
         for (size_t g = 0; g < ng; ++g) {
           displ[g] = displ[g] + deltat * veloc[g] + deltatsquareover2 * accel[g];
@@ -710,6 +1028,18 @@ extern "C" void *sf2d_oracle_create(const sf2d_oracle_db *db, int precision) {
   if (db->time_scheme != 1 && db->time_scheme != 2) return nullptr;
   if (db->time_scheme == 2 && (!db->alpha_lddrk || !db->beta_lddrk)) return nullptr;
   if (db->ispec_is_acoustic && (!db->kappastore || !db->rmass_inverse_acoustic || db->adj_src)) return nullptr;
+  if (db->pml_region) {
+    // CPML is restated for isotropic, non-attenuating elements of a forward run
+    if (!db->pml_K_x || !db->pml_K_z || !db->pml_d_x || !db->pml_d_z || !db->pml_alpha_x || !db->pml_alpha_z ||
+        db->adj_src || db->DT <= 0.0)
+      return nullptr;
+    for (int e = 0; e < db->nspec; ++e) {
+      if (db->pml_region[e] <= 0) continue;
+      if (db->ispec_is_anisotropic && db->ispec_is_anisotropic[e]) return nullptr;
+      if ((db->att_a1 || db->att_itau1) && !(db->ispec_is_acoustic && db->ispec_is_acoustic[e])) return nullptr;
+    }
+    if (db->ispec_is_acoustic && (!db->cpl_ac_elpt || !db->cpl_el_acpt)) return nullptr;
+  }
   if (db->seismotype == 4 && db->nrec > 0) {
     // pressure is recorded in acoustic elements only
     if (!db->ispec_is_acoustic) return nullptr;

@@ -84,6 +84,15 @@ typedef struct {
   const int *cpl_el_iglob;
   const double *cpl_el_nx, *cpl_el_nz, *cpl_el_w;
   int use_trick;                                          /* USE_TRICK_FOR_BETTER_PRESSURE: p = -chi */
+  /* CPML layers (pml_region NULL = none): pml_compute_memory_variables.f90,
+   * pml_compute_accel_contribution.f90, pml_compute.f90 (l/lik parameters,
+   * convolution coefficients, outer-edge zeroing) */
+  const int *pml_region;                                  /* nspec: 0 none, 1 X only, 2 Z only, 3 XZ */
+  const double *pml_K_x, *pml_K_z, *pml_d_x, *pml_d_z, *pml_alpha_x, *pml_alpha_z;  /* nspec*25 */
+  int npml_bnd_el, npml_bnd_ac;                           /* outer PML edge points zeroed every step */
+  const int *pml_bnd_el, *pml_bnd_ac;
+  const int *cpl_ac_elpt, *cpl_el_acpt;                   /* other-domain element point per coupling entry */
+  double DT;                                              /* time step in double (PML coefficients) */
 } sf2d_oracle_db;
 
 /* Fields addressed by sf2d_oracle_get/set. */

@@ -108,9 +108,12 @@ def coupling_points(edges, ibool, geo, gll):
     elastic side (compute_coupling_viscoelastic_ac.f90): a[g] += (w n) * (-chi_dd[g])
     Both read and write the same global point (one numbering for both
     domains); the normal is the acoustic element's outward normal.
+    The fifth entry of each list is the element GLL point (ispec*25 + j*5 + i)
+    of the other domain's element at that point, whose CPML profile the
+    coupling uses when that element lies in a PML layer.
     """
-    ac = {k: [] for k in ("iglob", "nx", "nz", "w")}
-    el = {k: [] for k in ("iglob", "nx", "nz", "w")}
+    ac = {k: [] for k in ("iglob", "nx", "nz", "w", "pt")}
+    el = {k: [] for k in ("iglob", "nx", "nz", "w", "pt")}
     for (ea, edge_a, ee, edge_e) in edges:
         for p in range(NGLL):
             ie, je = _ivalue_inverse(p, edge_e)
@@ -119,7 +122,7 @@ def coupling_points(edges, ibool, geo, gll):
             if int(ibool[ee, je, ie]) != g:
                 raise ValueError("fluid/solid coupling points do not match")
             nx, nz, w = _edge_normal(geo, ea, ia, ja, edge_a, gll)
-            for k, v in zip(("iglob", "nx", "nz", "w"), (g, nx, nz, w)):
+            for k, v in zip(("iglob", "nx", "nz", "w", "pt"), (g, nx, nz, w, ee * 25 + je * NGLL + ie)):
                 ac[k].append(v)
         for p in range(NGLL):
             ia, ja = _ivalue_inverse(p, edge_a)
@@ -128,12 +131,12 @@ def coupling_points(edges, ibool, geo, gll):
             if int(ibool[ea, ja, ia]) != g:
                 raise ValueError("fluid/solid coupling points do not match")
             nx, nz, w = _edge_normal(geo, ea, ia, ja, edge_a, gll)
-            for k, v in zip(("iglob", "nx", "nz", "w"), (g, nx, nz, w)):
+            for k, v in zip(("iglob", "nx", "nz", "w", "pt"), (g, nx, nz, w, ea * 25 + ja * NGLL + ia)):
                 el[k].append(v)
 
     def pack(d):
         return (np.array(d["iglob"], dtype=np.int32), np.array(d["nx"], dtype=f32),
-                np.array(d["nz"], dtype=f32), np.array(d["w"], dtype=f32))
+                np.array(d["nz"], dtype=f32), np.array(d["w"], dtype=f32), np.array(d["pt"], dtype=np.int64))
 
     return pack(ac), pack(el)
 
@@ -184,7 +187,7 @@ def stacey_acoustic_points(mesh, geo, mat, ibool, gll, is_acoustic, edges):
     return np.array(g_l, dtype=np.int32), np.array(w_l, dtype=f32), np.array(r_l, dtype=f32)
 
 
-def mass_matrix_acoustic(ibool, nglob, geo, mat, gll, is_acoustic, st_ac, newmark: bool, dt: float):
+def mass_matrix_acoustic(ibool, nglob, geo, mat, gll, is_acoustic, st_ac, newmark: bool, dt: float, pml=None):
     """rmass_inverse_acoustic (nglob,) f32: sum of w_i w_j J / kappa over acoustic
     elements, plus dt/2 * weight / (rho vp) at Newmark absorbing points; zero
     sums become 1 before inversion (invert_mass_matrix.F90:374-430, 700-790, 828-844)."""
@@ -194,7 +197,16 @@ def mass_matrix_acoustic(ibool, nglob, geo, mat, gll, is_acoustic, st_ac, newmar
     el = np.flatnonzero(is_acoustic)
     contrib = (wxwz[None].astype(f32) * geo["jacobian"][el].astype(f32)).astype(f32)
     contrib = (contrib / mat["kappastore"][el].astype(f32)).astype(f32)
-    m = _sequential_f32_accumulate(nglob, ibool[el].ravel().astype(np.int64), contrib.ravel().astype(np.float64))
+    if pml is not None:
+        from .pml import mass_entries
+
+        # PML elements: w w / kappa J in that order, times K (and d dt/2), invert_mass_matrix.F90:264-372
+        base = ((wxwz[None] / mat["kappastore"][el].astype(f32)).astype(f32) * geo["jacobian"][el].astype(f32)).astype(f32)
+        base = base[pml["region"][el] > 0]
+        idx, val = mass_entries(ibool, el, contrib, base, pml, newmark, float(f32(0.5 * float(f32(dt)))))
+        m = _sequential_f32_accumulate(nglob, idx.astype(np.int64), val)
+    else:
+        m = _sequential_f32_accumulate(nglob, ibool[el].ravel().astype(np.int64), contrib.ravel().astype(np.float64))
     if newmark and len(st_ac[0]):
         dto2 = f32(0.5 * float(f32(dt)))
         g, w, rvp = st_ac

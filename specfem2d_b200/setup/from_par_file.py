@@ -47,7 +47,8 @@ PAR_KEYS = ("NSTEP", "DT", "time_stepping_scheme", "NGNOD", "xmin", "xmax", "nx"
             "anglerec", "nrec", "xdeb", "zdeb", "xfin", "zfin", "record_at_surface_same_vertical",
             "seismotype", "materials", "regions", "ATTENUATION_VISCOELASTIC", "PML_BOUNDARY_CONDITIONS",
             "ATTENUATION_f0_REFERENCE", "NELEM_PML_THICKNESS", "receiver_sets", "USE_TRICK_FOR_BETTER_PRESSURE",
-            "TOMOGRAPHY_FILE", "MODEL")
+            "TOMOGRAPHY_FILE", "MODEL", "K_MIN_PML", "K_MAX_PML", "damping_change_factor_acoustic",
+            "damping_change_factor_elastic", "ROTATE_PML_ACTIVATE", "PML_PARAMETER_ADJUSTMENT")
 
 
 def config_from_data_dir(data_dir: str, par_file: str = "Par_file", source_file: str = "SOURCE") -> dict:
@@ -156,7 +157,15 @@ def database_from_config(cfg: dict, nstep: int | None = None, absorbing_as_stace
         r_t, vp_t, vs_t = tomo_values(tuple(np.asarray(a, dtype=np.float64) for a in tomo), coord, ibool, els)
         rho[els], vp[els], vs[els] = r_t, vp_t, vs_t
         rho, vp, vs = (a.astype(np.float32).astype(np.float64) for a in (rho, vp, vs))
-    db = build_database(mesh, rho, vp, vs, sources, recs, n, float(par["DT"]),
+    pml = None
+    if bool(par.get("PML_BOUNDARY_CONDITIONS", False)) and not absorbing_as_stacey:
+        if par.get("ROTATE_PML_ACTIVATE", False) or par.get("PML_PARAMETER_ADJUSTMENT", False):
+            raise NotImplementedError("rotated PML and PML parameter adjustment")
+        pml = dict(nelem_thickness=int(par["NELEM_PML_THICKNESS"]), k_min=float(par.get("K_MIN_PML", 1.0)),
+                   k_max=float(par.get("K_MAX_PML", 1.0)),
+                   damping_acoustic=float(par.get("damping_change_factor_acoustic", 0.5)),
+                   damping_elastic=float(par.get("damping_change_factor_elastic", 1.0)))
+    db = build_database(mesh, rho, vp, vs, sources, recs, n, float(par["DT"]), pml=pml,
                         stacey=stacey, external_model=external,
                         use_trick=bool(par.get("USE_TRICK_FOR_BETTER_PRESSURE", False)),
                         seismotype=int(par.get("seismotype", 1)),

@@ -121,6 +121,9 @@ class Database:
     # use_trick (USE_TRICK_FOR_BETTER_PRESSURE)
     acoustic: dict = None
     seismotype: int = 1                 # 1 displacement, 2 velocity, 3 acceleration, 4 pressure
+    # CPML layers (None = none): keys region (nspec,) int (0 outside, 1 X, 2 Z, 3 XZ),
+    # K_x K_z d_x d_z alpha_x alpha_z (nspec,5,5) float64, bnd_ac/bnd_el outer-edge points, dt
+    pml: dict = None
 
     @property
     def deltat(self):
@@ -243,16 +246,26 @@ def stacey_points(mesh: Mesh, geo: dict, mat: dict, ibool, gll: GLL, stacey: boo
             np.array(out["rvp"], dtype=f32), np.array(out["rvs"], dtype=f32))
 
 
-def mass_matrix_elastic(ibool, nglob, geo, mat, gll: GLL, stacey_pts, newmark: bool, dt: float, elastic=None):
+def mass_matrix_elastic(ibool, nglob, geo, mat, gll: GLL, stacey_pts, newmark: bool, dt: float, elastic=None,
+                        pml=None):
     """rmass_inverse_elastic (nglob, 2) f32 (invert_mass_matrix.F90:34-849, elastic).
 
     Only elastic elements contribute (all when ``elastic`` is None); points
-    with no elastic mass get 1 before inversion (invert_mass_matrix.F90:820-822)."""
+    with no elastic mass get 1 before inversion (invert_mass_matrix.F90:820-822).
+    PML elements (``pml`` dict of setup.pml) carry their K and d dt/2 factors."""
     wxwz = (gll.wxgll[None, :] * gll.wzgll[:, None]).astype(f32)  # [j][i], CUSTOM_REAL product
     el = np.arange(ibool.shape[0]) if elastic is None else np.flatnonzero(elastic)
     contrib = (wxwz[None].astype(np.float64) * mat["rhostore"][el].astype(np.float64)
                * geo["jacobian"][el].astype(np.float64))
-    m = _sequential_f32_accumulate(nglob, ibool[el].ravel(), contrib.ravel())
+    if pml is not None:
+        from .pml import mass_entries
+
+        base = ((wxwz[None] * mat["rhostore"][el].astype(f32)).astype(f32) * geo["jacobian"][el].astype(f32)).astype(f32)
+        base = base[pml["region"][el] > 0]
+        idx, val = mass_entries(ibool, el, contrib, base, pml, newmark, float(f32(0.5 * float(f32(dt)))))
+        m = _sequential_f32_accumulate(nglob, idx, val)
+    else:
+        m = _sequential_f32_accumulate(nglob, ibool[el].ravel(), contrib.ravel())
     mx = m.copy()
     mz = m.copy()
     if newmark and len(stacey_pts[0]):
@@ -356,12 +369,13 @@ def source_time_function(src: Source, t0: float, dt: float, nstep: int, time_sch
                          use_trick: bool = False):
     """(nstep, nstage) f32 values of -factor * stf(t) (prepare_source_time_function.f90).
 
-    ``use_trick`` (USE_TRICK_FOR_BETTER_PRESSURE) replaces the Ricker by its
-    second derivative, the fourth derivative of the Gaussian
-    (prepare_source_time_function.f90:205-216, comp_source_time_function.f90:128-143),
+    ``use_trick`` (USE_TRICK_FOR_BETTER_PRESSURE) replaces each time function
+    by its second derivative (the Ricker by the fourth derivative of the
+    Gaussian, the first derivative by the third, the Gaussian by the second;
+    prepare_source_time_function.f90:205-262, comp_source_time_function.f90:90-143),
     so that -chi rather than -chi_dd is the pressure."""
-    if use_trick and src.time_function_type != 1:
-        raise NotImplementedError("USE_TRICK_FOR_BETTER_PRESSURE is restated for the Ricker only")
+    if use_trick and src.time_function_type not in (1, 2, 3):
+        raise NotImplementedError("USE_TRICK_FOR_BETTER_PRESSURE is restated for the Ricker and Gaussian families")
     nstage = 1 if time_scheme == 1 else 6
     out = np.zeros((nstep, nstage), dtype=f32)
     a = PI ** 2 * src.f0 ** 2
@@ -374,8 +388,11 @@ def source_time_function(src: Source, t0: float, dt: float, nstep: int, time_sch
             t = timeval - t0 - src.tshift
             if src.time_function_type == 1 and use_trick:
                 v = -2.0 * a * (3.0 - 12.0 * a * t * t + 4.0 * a ** 2 * t * t * t * t) * math.exp(-a * t * t)
-            elif src.time_function_type == 1:
+            elif src.time_function_type == 1 or (src.time_function_type == 3 and use_trick):
+                # Ricker; with the trick also the second derivative of the Gaussian (case 3)
                 v = (1.0 - 2.0 * a * t ** 2) * math.exp(-a * t ** 2)
+            elif src.time_function_type == 2 and use_trick:
+                v = 2.0 * a * t * math.exp(-a * t ** 2) * (-3.0 + 2.0 * a * t ** 2)
             elif src.time_function_type == 2:
                 v = t * math.exp(-a * t ** 2)
             elif src.time_function_type == 3:
@@ -409,7 +426,7 @@ def build_database(mesh: Mesh, rho, vp, vs, sources, receivers_xz, nstep: int, d
                    stacey: bool = True, external_model: bool = True, time_scheme: int = 1,
                    user_t0: float = 0.0, anglerec_deg: float = 0.0, qkappa=None, qmu=None,
                    attenuation_f0: float | None = None, use_trick: bool = False,
-                   seismotype: int = 1) -> Database:
+                   seismotype: int = 1, pml: dict | None = None) -> Database:
     """Run the host setup chain and return a Database.
 
     ``rho, vp, vs`` are per-GLL-point arrays (nspec,5,5) (external model) or
@@ -417,7 +434,10 @@ def build_database(mesh: Mesh, rho, vp, vs, sources, receivers_xz, nstep: int, d
     ``external_model`` is False.  Elements with vs = 0 are acoustic (fluid);
     the acoustic domain, its absorbing points, free surface and the
     fluid-solid coupling go into ``Database.acoustic``.  ``seismotype`` 4
-    records pressure (receivers in acoustic elements).
+    records pressure (receivers in acoustic elements).  ``pml`` (keys
+    nelem_thickness, and optionally k_min, k_max, damping_acoustic,
+    damping_elastic) puts CPML layers on the absorbing sides instead of
+    Stacey conditions; the profiles go into ``Database.pml``.
     """
     from . import acoustic as ac_setup
 
@@ -432,8 +452,21 @@ def build_database(mesh: Mesh, rho, vp, vs, sources, receivers_xz, nstep: int, d
     mat = material_stores_from_velocity(rho, vp, vs, external_model)
     is_ac = ac_setup.acoustic_element_flags(vs)
     elastic = None if not is_ac.any() else ~is_ac
+    pml_db = None
+    if pml is not None:
+        from . import pml as pml_setup
+
+        if stacey:
+            raise ValueError("CPML and Stacey conditions are exclusive")
+        is_pml, region, _ = pml_setup.pml_elements(mesh, ibool, int(pml["nelem_thickness"]))
+        coefs = pml_setup.pml_coefficients(
+            ibool, geo["coord"], is_pml, region, mat["rho_vpstore"], mat["rhostore"], is_ac,
+            max(s_.f0 for s_ in sources), pml.get("k_min", 1.0), pml.get("k_max", 1.0),
+            pml.get("damping_acoustic", 0.5), pml.get("damping_elastic", 1.0))
+        bnd_ac, bnd_el = pml_setup.pml_boundary_points(mesh, ibool, is_pml, is_ac)
+        pml_db = dict(region=region, bnd_ac=bnd_ac, bnd_el=bnd_el, dt=float(dt), **coefs)
     spts = stacey_points(mesh, geo, mat, ibool, gll, stacey, elastic)
-    rmass = mass_matrix_elastic(ibool, nglob, geo, mat, gll, spts, time_scheme == 1, dt, elastic)
+    rmass = mass_matrix_elastic(ibool, nglob, geo, mat, gll, spts, time_scheme == 1, dt, elastic, pml_db)
     acoustic = None
     if is_ac.any():
         edges = ac_setup.coupling_edges(ibool, is_ac)
@@ -444,11 +477,13 @@ def build_database(mesh: Mesh, rho, vp, vs, sources, receivers_xz, nstep: int, d
             st_ac = (np.zeros(0, np.int32), np.zeros(0, f32), np.zeros(0, f32))
         acoustic = dict(
             ispec=is_ac,
-            rmass=ac_setup.mass_matrix_acoustic(ibool, nglob, geo, mat, gll, is_ac, st_ac, time_scheme == 1, dt),
+            rmass=ac_setup.mass_matrix_acoustic(ibool, nglob, geo, mat, gll, is_ac, st_ac, time_scheme == 1, dt,
+                                                pml_db),
             st_iglob=st_ac[0], st_w=st_ac[1], st_rvp=st_ac[2],
             free_iglob=ac_setup.free_surface_points(mesh, ibool, is_ac),
             cpl_ac_iglob=cpl_ac[0], cpl_ac_nx=cpl_ac[1], cpl_ac_nz=cpl_ac[2], cpl_ac_w=cpl_ac[3],
             cpl_el_iglob=cpl_el[0], cpl_el_nx=cpl_el[1], cpl_el_nz=cpl_el[2], cpl_el_w=cpl_el[3],
+            cpl_ac_elpt=cpl_ac[4], cpl_el_acpt=cpl_el[4],
             use_trick=bool(use_trick))
     coord = geo["coord"]
     t0 = compute_t0(sources, user_t0)
@@ -527,4 +562,4 @@ def build_database(mesh: Mesh, rho, vp, vs, sources, receivers_xz, nstep: int, d
         cosrot=math.cos(ang), sinrot=math.sin(ang),
         nstep=nstep, dt=dt, t0=t0, time_scheme=time_scheme, gll=gll, mesh=mesh,
         src_xi=np.array(sxi), src_gamma=np.array(sgam), atten=atten, acoustic=acoustic,
-        seismotype=int(seismotype))
+        seismotype=int(seismotype), pml=pml_db)

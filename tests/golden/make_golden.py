@@ -42,6 +42,15 @@ EXAMPLES = {
                                 "Par_file", "SOURCE"),
 }
 
+EXAMPLES["semi_infinite_homogeneous"] = (
+    # elastic half space with CPML layers (3 elements) on all four sides
+    "EXAMPLES/semi_infinite_homogeneous", [("S0001", "BXX"), ("S0001", "BXZ")], "Par_file", "SOURCE")
+
+EXAMPLES["pressure_source_acoustic"] = (
+    # fluid only, CPML on all sides, Gaussian pressure source with USE_TRICK_FOR_BETTER_PRESSURE
+    "EXAMPLES/check_absolute_amplitude_of_pressure_source_seismograms_acoustic", [("S0001", "PRE")],
+    "../REF_SEIS/Par_file", "../REF_SEIS/SOURCE")
+
 # examples whose TOMOGRAPHY_FILE is written by a script of the reference
 TOMO_SCRIPTS = {"tomographic_ocean_model": "utils/createTomographyFile.py"}
 
@@ -103,7 +112,8 @@ def main(ref_root):
             json.dump(cfg, f, indent=1, default=str)
         arrs = {}
         for st, comp in traces:
-            d = np.loadtxt(os.path.join(ex, "REF_SEIS", f"AA.{st}.{comp}.semd"))
+            ext = "semp" if comp == "PRE" else "semd"
+            d = np.loadtxt(os.path.join(ex, "REF_SEIS", f"AA.{st}.{comp}.{ext}"))
             arrs[f"{st}_{comp}"] = d[:, 1]
             arrs["t_first"] = np.array(d[0, 0])
             arrs["t_step"] = np.array(d[1, 0] - d[0, 0])

@@ -175,3 +175,48 @@ def test_ocean_oracle_lddrk_close_to_newmark():
     a = oracle.Oracle(nm, 4).run(nm.nstep)
     b = oracle.Oracle(lk, 4).run(lk.nstep)
     assert rel_l2(b, a) < 2e-2
+
+
+def test_cpml_elastic_example_matches_ref_seis():
+    """EXAMPLES/semi_infinite_homogeneous: CPML layers of 3 elements on all four
+    sides of an elastic square (564 PML elements, as the reference reports)."""
+    import oracle
+
+    cfg, seis = load_golden("semi_infinite_homogeneous")
+    db = database_from_config(cfg)
+    assert int((db.pml["region"] > 0).sum()) == 564 and len(db.stacey_iglob) == 0
+    (se, sxi, sg), (re_, rxi, rg) = cfg["log_locations"]
+    assert db.source_ispec[0] + 1 == se and db.rec_ispec[0] + 1 == re_
+    out = oracle.Oracle(db, 4).run(db.nstep)
+    assert rel_l2(out[0, :, 0], seis["S0001_BXX"]) < 1e-5
+    assert rel_l2(out[0, :, 1], seis["S0001_BXZ"]) < 1e-5
+
+
+def test_cpml_acoustic_pressure_example_matches_ref_seis():
+    """EXAMPLES/check_absolute_amplitude_of_pressure_source_seismograms_acoustic:
+    fluid only, CPML on all sides (492 PML elements), Gaussian pressure source
+    with USE_TRICK_FOR_BETTER_PRESSURE, one pressure receiver."""
+    import oracle
+
+    cfg, seis = load_golden("pressure_source_acoustic")
+    db = database_from_config(cfg)
+    assert int((db.pml["region"] > 0).sum()) == 492 and db.seismotype == 4
+    out = oracle.Oracle(db, 4).run(db.nstep)
+    assert rel_l2(out[0, :, 0], seis["S0001_PRE"]) < 1e-5
+    assert float(seis["t_first"]) == pytest.approx(-db.t0)
+
+
+def test_cpml_coupled_absorbs_like_stacey_before_reflections():
+    """The coupled model with CPML instead of Stacey (the PML terms of both
+    coupling directions are active where the sea floor crosses the side
+    layers): the pressure traces agree until boundary waves return."""
+    import oracle
+    from specfem2d_b200 import configs
+
+    st = configs.c2_coupled(nstep=700, nrec=9, scale=16)
+    pm = configs.c2_coupled(nstep=700, nrec=9, scale=16, pml_thickness=3)
+    assert (pm.pml["region"][pm.acoustic["ispec"]] > 0).any()
+    a = oracle.Oracle(st, 4).run(st.nstep)
+    b = oracle.Oracle(pm, 4).run(pm.nstep)
+    w = slice(0, 500)  # direct and sea-floor waves only
+    assert rel_l2(b[:, w], a[:, w]) < 5e-3
