@@ -1,7 +1,7 @@
 """Benchmark of the SPECFEM2D time-marching hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c2_geometry|c1] [--tile-elems T]
+                    [--workload c2_coupled|c2_geometry|c1|...] [--tile-elems T]
 
 A "step" is one Newmark time step of the whole mesh.  The metric is GLL
 point-updates per second (global points x steps / s).  With N > 1 (torchrun,
@@ -44,7 +44,11 @@ def build_workload(name: str, nstep: int):
     if os.path.exists(path):
         with open(path, "rb") as f:
             return pickle.load(f)
-    if name == "c2_geometry":
+    if name == "c2_coupled":
+        db = configs.c2_coupled(nstep=nstep, pml_thickness=20)
+    elif name == "c2_coupled_stacey":
+        db = configs.c2_coupled(nstep=nstep)
+    elif name == "c2_geometry":
         db = configs.c2_geometry(nstep=nstep)
     elif name == "c1":
         db = configs.c1_homogeneous(nstep=nstep)
@@ -61,6 +65,13 @@ def build_workload(name: str, nstep: int):
 
 
 WORKLOAD_DESC = {
+    "c2_coupled": ("800x320-element (20 km x 8 km, 4,100,481 GLL points) coupled fluid-solid model: 1 km "
+                   "water layer (vp 1500, rho 1020, 32,000 acoustic elements) over rock with vp 2000->4500 "
+                   "with depth, vs=vp/1.73, Gardner rho, 5% Gaussian random field (corr. 200 m, seed 2); "
+                   "20-element CPML on the sides and bottom (28,000 layer elements, 1,600 of them fluid); "
+                   "pressure source 500 m deep, Ricker 8 Hz, dt 5e-4, 400 pressure receivers"),
+    "c2_coupled_stacey": ("the c2_coupled model with Stacey conditions on the sides and bottom instead of "
+                          "the CPML layers"),
     "c2_geometry": ("800x320-element (20 km x 8 km, 4,100,481 GLL points) mesh of the coupled "
                     "acoustic-elastic configuration, run elastic-only: the 1 km top layer is elastic "
                     "(vp 2000) and Stacey replaces the 20-element CPML; vp 2000->4500 with depth, "
@@ -171,8 +182,8 @@ def main():
     ap.add_argument("--steps", type=int, default=6000)
     ap.add_argument("--warmup", type=int, default=100)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2_geometry", choices=sorted(WORKLOAD_DESC))
-    ap.add_argument("--tile-elems", type=int, default=64)
+    ap.add_argument("--workload", default="c2_coupled", choices=sorted(WORKLOAD_DESC))
+    ap.add_argument("--tile-elems", type=int, default=32)
     ap.add_argument("--threads", type=int, default=256)
     ap.add_argument("--autotune", action="store_true", help="pick tile size and threads per CTA first")
     ap.add_argument("--ref-seconds", type=float, default=15.0)
@@ -199,18 +210,26 @@ def main():
 
         dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         dist = dist_mod
-    from specfem2d_b200.configs import algorithmic_bytes_elastic, algorithmic_bytes_viscoelastic
+    from specfem2d_b200.configs import (algorithmic_bytes_coupled, algorithmic_bytes_elastic,
+                                        algorithmic_bytes_viscoelastic)
+    from specfem2d_b200.coupled import CoupledSolver
     from specfem2d_b200.runtime import ElasticSolver
 
     K, W = args.steps, args.warmup
     db = build_workload(args.workload, K + W + 8)
+    coupled = db.acoustic is not None
     tune = None
-    if args.autotune:
+    if args.autotune and not coupled:
         from specfem2d_b200.autotune import autotune_elastic
 
         (args.tile_elems, args.threads), tune = autotune_elastic(db, tiles=(48, 64, 96), threads=(256, 512))
-    solver = ElasticSolver(db, tile_elems=args.tile_elems, threads_per_block=args.threads)
-    info = solver.layout_info()
+
+    def make_solver():
+        cls = CoupledSolver if coupled else ElasticSolver
+        return cls(db, tile_elems=args.tile_elems, threads_per_block=args.threads)
+
+    solver = make_solver()
+    el_db = solver.sub_db if coupled else db   # the solid part the element-kernel roofline refers to
     stream = torch.cuda.ExternalStream(solver.stream_handle())
 
     # warm-up, then the timed region: K steps queued as CUDA graphs on the solver stream
@@ -236,22 +255,27 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
         dist.barrier()
-    chunk = 32
-    launches = 2 * K * (6 if db.time_scheme == 2 else 1) + K // chunk + (1 if K % chunk else 0)
+    # per step (stage): a tile launch per tile group (with and without CPML) and a shared-point
+    # kernel per domain, and the CPML coupling-entry kernels; receiver kernels per chunk
+    launches = solver.launch_count(K)
 
     # kernel-level timing for the roofline (events around each launch, same stream)
     nk = min(200, max(20, K // 10))
     k_ms = solver.time_kernels(nk)
-    tile_ms = k_ms[0]
-    st = info
+    tile_ms = k_ms[2] if coupled else k_ms[0]
+    shared_ms = k_ms[3] if coupled else k_ms[1]
+    st = solver.solid_layout_info() if coupled else solver.layout_info()
     nsh = st["nshared"]
-    n_int = db.nglob - nsh
-    # algorithmic bytes of the element kernel per launch: element data + interior points
+    n_int = el_db.nglob - nsh
+    # algorithmic bytes of the (solid) element kernel per launch: element data + interior points
     # (u, v, a read+write, rmass) + shared points touched by tiles (u, v, a read, partial write)
-    n_slots = int(np.asarray(solver_slots(db, args.tile_elems)))
-    ns = 6 if db.time_scheme == 2 else 1
+    n_slots = st["n_slots"]
+    pm = getattr(db, "pml", None)
+    npml_el = int((el_db.pml["region"] > 0).sum()) if getattr(el_db, "pml", None) is not None else 0
+    npml_ac = int((pm["region"] > 0).sum()) - npml_el if pm is not None else 0
     if db.atten is None:
-        tile_bytes = 700 * db.nspec + 56 * n_int + 32 * n_slots
+        # + per CPML element point: damping profiles (48 B), rho J (4 B), memory variables read + write (96 B)
+        tile_bytes = 700 * el_db.nspec + 56 * n_int + 32 * n_slots + 25 * 148 * npml_el
         step_bytes = algorithmic_bytes_elastic(db.nspec, db.nglob)
     elif db.time_scheme == 1:
         tile_bytes = 700 * db.nspec + 3600 * db.nspec + 56 * n_int + 32 * n_slots
@@ -261,6 +285,9 @@ def main():
         # interior points (u, v, u_L, v_L read+write, a written, rmass read), shared reads + partial
         tile_bytes = db.nspec * (700 + 25 * 192) + 88 * n_int + 24 * n_slots
         step_bytes = algorithmic_bytes_viscoelastic(db.nspec, db.nglob, 2)
+    if coupled:
+        step_bytes = algorithmic_bytes_coupled(el_db.nspec, el_db.nglob, solver.nspec_fluid, solver.nglob_fluid,
+                                               npml_el, npml_ac)
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -274,7 +301,7 @@ def main():
     if args.no_e2e:
         e2e_solver = None
     else:
-        e2e_solver = ElasticSolver(db, tile_elems=args.tile_elems, threads_per_block=args.threads)
+        e2e_solver = make_solver()
     zeros = np.zeros((db.nglob, 2), dtype=np.float32)
     torch.cuda.synchronize()
     if dist:
@@ -282,13 +309,22 @@ def main():
     e2e_s, h2d, d2h = float("nan"), 0, 0
     if e2e_solver is not None:
         t0 = time.perf_counter()
-        e2e_solver.set_fields(zeros, zeros, zeros)
-        seis = e2e_solver.run(K, seismograms=True)
-        d = e2e_solver.get_fields()[0]
+        if coupled:
+            z1 = np.zeros(db.nglob, dtype=np.float32)
+            e2e_solver.set_fields(displ=zeros, veloc=zeros, accel=zeros, pot=z1, pot_dot=z1, pot_dot_dot=z1)
+            seis = e2e_solver.run(K, seismograms=True)
+            d = e2e_solver.get_fields()["pot"]
+            h2d = 3 * len(e2e_solver.solid_points) * 8 + 3 * len(e2e_solver.fluid_points) * 4
+            d2h = seis.nbytes + h2d       # get_fields reads back the same six fields
+        else:
+            e2e_solver.set_fields(zeros, zeros, zeros)
+            seis = e2e_solver.run(K, seismograms=True)
+            d = e2e_solver.get_fields()[0]
+            h2d = 3 * db.nglob * 8
+            d2h = seis.nbytes + h2d
         t1 = time.perf_counter()
         e2e_s = t1 - t0
-        h2d = 3 * db.nglob * 8
-        d2h = seis.nbytes + d.nbytes
+        del d
         e2e_solver.close()
     if dist:
         t = torch.tensor([e2e_s], device="cuda")
@@ -304,12 +340,15 @@ def main():
                    "nspec": db.nspec, "nglob": db.nglob, "tile_elems": args.tile_elems,
                    "threads_per_cta": args.threads, "autotuned": bool(tune),
                    "ntiles": st["ntiles"], "shared_points": nsh,
+                   "nspec_fluid": solver.nspec_fluid if coupled else 0,
+                   "cpml_elements": {"solid": npml_el, "fluid": npml_ac},
                    "l2": "inputs larger than L2 (fields + element data > 126 MB)",
                    "parallelism": f"replicas x{world}"},
         "hbm_gbs_step": step_bytes / (ms / K * 1e-3) / 1e9,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": None,
-                     "kernel": "k_elastic_tile", "kernel_ms": tile_ms, "shared_kernel_ms": k_ms[1],
+                     "kernel": "k_elastic_tile", "kernel_ms": tile_ms, "shared_kernel_ms": shared_ms,
+                     "fluid_kernels_ms": k_ms[:2] if coupled else None, "step_kernels_ms": k_ms[-1],
                      "algorithmic_bytes_per_launch": tile_bytes,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
         "e2e": {"value": db.nglob * K * world / e2e_s, "unit": "point-updates/s",
@@ -321,19 +360,13 @@ def main():
         n, dt, threads = time_oracle(db, max_steps=K, target_s=args.ref_seconds)
         line["cpu_baseline"] = {"value": db.nglob * n / dt, "unit": "point-updates/s", "cores": threads,
                                 "kind": "port",
-                                "sample": f"{n} Newmark steps of the full mesh, C++ restatement of the "
+                                "sample": f"{n} time steps of the full mesh, C++ restatement of the "
                                           "reference CPU solver (FP32), all host threads"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     solver.close()
     if dist:
         dist.destroy_process_group()
-
-
-def solver_slots(db, tile_elems):
-    from specfem2d_b200.runtime import tiling_stats
-
-    return tiling_stats(db, tile_elems)["n_slots"]
 
 
 if __name__ == "__main__":

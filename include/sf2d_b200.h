@@ -100,6 +100,20 @@ typedef struct {
    * (prepare_attenuation.f90:378-396); LDDRK: 1/tau_sigma and phi (attenuation_model.f90). */
   const float *att_a1, *att_b1, *att_a2, *att_b2;
   const float *att_itau1, *att_phi1, *att_itau2, *att_phi2;
+  /* CPML absorbing layer (pml_region NULL = none), the arrays of prepare_pml.f90 /
+   * pml_init.F90: region per element, 0 outside the layer, 1 CPML_X_ONLY, 2 CPML_Z_ONLY,
+   * 3 CPML_XZ; damping profiles K, d, alpha per element GLL point (nspec*25, read in
+   * the layer); rho and the Jacobian per element GLL point (nspec*25) for the layer's
+   * acceleration terms; the points of the layer's outer edge, zeroed every step
+   * (pml_boundary_elastic, pml_compute.f90:545-574); DT in double for the
+   * convolution coefficients.  Isotropic, non-attenuating forward runs only, and
+   * not together with Stacey conditions (read_parameter_file.F90:1495). */
+  const int *pml_region;
+  const double *pml_K_x, *pml_K_z, *pml_d_x, *pml_d_z, *pml_alpha_x, *pml_alpha_z;
+  const float *rhostore, *jacobian;
+  int npml_edge;
+  const int *pml_edge_iglob;
+  double pml_dt;
 } sf2d_elastic_desc;
 
 /* Builds the tiled device layout and uploads everything (fields start at 0). */
@@ -142,8 +156,13 @@ int sf2d_get_stream(sf2d_solver *s, void **stream);
 int sf2d_time_kernels(sf2d_solver *s, int nstep, float *ms);
 
 /* Layout statistics: [ntiles, nshared points, max local points, max elements
- * per tile, device bytes, dynamic shared memory per CTA, threads per CTA, 0]. */
+ * per tile, device bytes, dynamic shared memory per CTA, threads per CTA,
+ * partial-sum slots]. */
 int sf2d_layout_info(sf2d_solver *s, long long *info8);
+
+/* Kernel launches that sf2d_enqueue(s, nstep) issues (all stages, receiver
+ * kernels included), for launch accounting. */
+int sf2d_launch_count(sf2d_solver *s, int nstep, long long *launches);
 
 int sf2d_destroy(sf2d_solver *s);
 

@@ -62,6 +62,13 @@ typedef struct {
   const double *hxir, *hgammar;              /* nrec*5 */
   const int *rec_global;                     /* index of each in the run's receiver list */
   int tile_elems;                            /* 0 = 32 */
+  /* CPML layer in the fluid (pml_region NULL = none), as in sf2d_elastic_desc;
+   * edge points: pml_boundary_acoustic (pml_compute.f90:502-541) */
+  const int *pml_region;
+  const double *pml_K_x, *pml_K_z, *pml_d_x, *pml_d_z, *pml_alpha_x, *pml_alpha_z;
+  int npml_edge;
+  const int *pml_edge_iglob;
+  double pml_dt;
 } sf2d_acoustic_desc;
 
 typedef struct {
@@ -78,6 +85,12 @@ typedef struct {
   int ncpl_el;
   const int *cpl_el_point, *cpl_el_ac_point;
   const float *cpl_el_nx, *cpl_el_nz, *cpl_el_w;
+  /* with CPML layers: the element GLL point (ispec*25 + j*5 + i, sub-mesh numbering)
+   * of the solid element behind each fluid-side entry and of the fluid element behind
+   * each solid-side entry; an entry whose element lies in a layer adds the layer's
+   * memory terms (compute_coupling_acoustic_el.f90:78-140,
+   * compute_coupling_viscoelastic_ac.f90:105-150) */
+  const int *cpl_ac_el_elpt, *cpl_el_ac_elpt;
 } sf2d_coupling_desc;
 
 int sf2d_coupled_create(const sf2d_elastic_desc *solid, const sf2d_acoustic_desc *fluid,
@@ -85,6 +98,12 @@ int sf2d_coupled_create(const sf2d_elastic_desc *solid, const sf2d_acoustic_desc
 /* Advances nstep steps (fluid then solid per step or LDDRK stage); seismograms
  * (may be NULL): nrec_total*nstep*2 doubles [irec][it][comp]. */
 int sf2d_coupled_run(sf2d_coupled *c, int nstep, double *seismograms);
+/* The same steps queued without a host wait (CUDA graphs of fixed step
+ * chunks on the solver's stream); sf2d_coupled_synchronize waits for them and
+ * returns the stability status; sf2d_coupled_get_stream gives the stream. */
+int sf2d_coupled_enqueue(sf2d_coupled *c, int nstep);
+int sf2d_coupled_synchronize(sf2d_coupled *c);
+int sf2d_coupled_get_stream(sf2d_coupled *c, void **stream);
 /* Fields in the sub-mesh numberings: displ/veloc/accel solid nglob*2,
  * chi/chi_dot/chi_dot_dot fluid nglob.  NULL skips (get) or zeroes (set). */
 int sf2d_coupled_get_fields(sf2d_coupled *c, float *displ, float *veloc, float *accel, float *chi,
@@ -97,6 +116,10 @@ int sf2d_coupled_time_kernels(sf2d_coupled *c, int nstep, float *ms);
 /* info[6]: fluid tiles, fluid shared points, max local points, shared bytes per CTA,
  * fluid interior points, partial-sum slots. */
 int sf2d_coupled_layout_info(sf2d_coupled *c, long long *info);
+/* sf2d_layout_info of the solid sub-solver. */
+int sf2d_coupled_solid_layout_info(sf2d_coupled *c, long long *info8);
+/* Kernel launches that sf2d_coupled_enqueue(c, nstep) issues. */
+int sf2d_coupled_launch_count(sf2d_coupled *c, int nstep, long long *launches);
 int sf2d_coupled_destroy(sf2d_coupled *c);
 
 #ifdef __cplusplus

@@ -107,12 +107,18 @@ def c2_coupled(nstep: int = 6000, nrec: int = 400, scale: int = 1, rec_depth: fl
                           **({"pml": pml} if pml else {}))
 
 
-def algorithmic_bytes_coupled(nspec_el: int, nglob_el: int, nspec_ac: int, nglob_ac: int) -> int:
+def algorithmic_bytes_coupled(nspec_el: int, nglob_el: int, nspec_ac: int, nglob_ac: int,
+                              npml_el: int = 0, npml_ac: int = 0) -> int:
     """Bytes of one coupled Newmark step in the reference layout: the solid
     step over its elements and points plus, per fluid element, 25 points x
     (xix, xiz, gammax, gammaz, rho, ibool) x 4 B and, per fluid point, chi,
-    chi_dot, chi_dot_dot read + write and rmass read."""
-    return 700 * nspec_el + 56 * nglob_el + 600 * nspec_ac + 28 * nglob_ac
+    chi_dot, chi_dot_dot read + write and rmass read.  Each CPML element adds,
+    per GLL point, its six damping profiles (K, d, alpha in x and z, 48 B in
+    double) and rho J or J / kappa (4 B), and its memory variables read +
+    write: 12 floats in the solid (strain 8, displacement 4: 96 B), 6 in the
+    fluid (48 B)."""
+    return (700 * nspec_el + 56 * nglob_el + 600 * nspec_ac + 28 * nglob_ac
+            + 25 * (48 + 4 + 96) * npml_el + 25 * (48 + 4 + 48) * npml_ac)
 
 
 def c2_geometry(nstep: int = 6000, nrec: int = 400, elastic_only: bool = True, scale: int = 1):

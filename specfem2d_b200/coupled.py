@@ -33,6 +33,10 @@ class AcousticDesc(ctypes.Structure):
         ("nsrc", ctypes.c_int), ("src_ispec", _i), ("sourcearrays", _f), ("stf", _f),
         ("nrec", ctypes.c_int), ("rec_ispec", _i), ("hxir", _d), ("hgammar", _d), ("rec_global", _i),
         ("tile_elems", ctypes.c_int),
+        ("pml_region", _i),
+        ("pml_K_x", _d), ("pml_K_z", _d), ("pml_d_x", _d), ("pml_d_z", _d), ("pml_alpha_x", _d), ("pml_alpha_z", _d),
+        ("npml_edge", ctypes.c_int), ("pml_edge_iglob", _i),
+        ("pml_dt", ctypes.c_double),
     ]
 
 
@@ -45,6 +49,7 @@ class CouplingDesc(ctypes.Structure):
         ("cpl_ac_nx", _f), ("cpl_ac_nz", _f), ("cpl_ac_w", _f),
         ("ncpl_el", ctypes.c_int), ("cpl_el_point", _i), ("cpl_el_ac_point", _i),
         ("cpl_el_nx", _f), ("cpl_el_nz", _f), ("cpl_el_w", _f),
+        ("cpl_ac_el_elpt", _i), ("cpl_el_ac_elpt", _i),
     ]
 
 
@@ -61,7 +66,13 @@ def _lib():
         lib.sf2d_coupled_time_kernels.argtypes = [_vp, ctypes.c_int, _f]
         lib.sf2d_coupled_layout_info.argtypes = [_vp, ctypes.POINTER(ctypes.c_longlong)]
         lib.sf2d_coupled_destroy.argtypes = [_vp]
-        for n in ("create", "run", "get_fields", "set_fields", "time_kernels", "layout_info", "destroy"):
+        lib.sf2d_coupled_enqueue.argtypes = [_vp, ctypes.c_int]
+        lib.sf2d_coupled_synchronize.argtypes = [_vp]
+        lib.sf2d_coupled_get_stream.argtypes = [_vp, ctypes.POINTER(_vp)]
+        lib.sf2d_coupled_solid_layout_info.argtypes = [_vp, ctypes.POINTER(ctypes.c_longlong)]
+        lib.sf2d_coupled_launch_count.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]
+        for n in ("create", "run", "get_fields", "set_fields", "time_kernels", "layout_info", "destroy",
+                  "enqueue", "synchronize", "get_stream", "solid_layout_info", "launch_count"):
             getattr(lib, "sf2d_coupled_" + n).restype = ctypes.c_int
         lib._coupled_sigs = True
     return lib
@@ -82,8 +93,7 @@ def split(db):
     ac = db.acoustic
     if ac is None:
         raise ValueError("the Database has no acoustic element")
-    if getattr(db, "pml", None) is not None:
-        raise NotImplementedError("CPML layers are not part of the coupled GPU path")
+    pm = getattr(db, "pml", None)
     is_ac = np.asarray(ac["ispec"], dtype=bool)
     el_e, ac_e = np.flatnonzero(~is_ac), np.flatnonzero(is_ac)
     if len(el_e) == 0:
@@ -117,6 +127,11 @@ def split(db):
         sub.aniso = {k: v[el_e] for k, v in db.aniso.items()}
     sub.acoustic = None
     sub.mesh = None
+    pml_keys = ("K_x", "K_z", "d_x", "d_z", "alpha_x", "alpha_z")
+    if pm is not None:
+        bnd_el = gmap[np.asarray(pm["bnd_el"], dtype=np.int64)]
+        sub.pml = dict(region=np.asarray(pm["region"])[el_e], bnd_el=bnd_el[bnd_el >= 0].astype(np.int32),
+                       bnd_ac=np.zeros(0, np.int32), dt=pm["dt"], **{k: pm[k][el_e] for k in pml_keys})
 
     fluid = dict(
         nspec=len(ac_e), nglob=len(ga), ibool=amap[db.ibool[ac_e]].astype(np.int32),
@@ -128,14 +143,26 @@ def split(db):
         src_ispec=eamap[db.source_ispec[src_ac]].astype(np.int32),
         sourcearrays=db.sourcearrays[src_ac][..., 0].astype(np.float32), stf=db.stf[src_ac],
         rec_ispec=eamap[db.rec_ispec[rec_ac]].astype(np.int32), hxir=db.hxir[rec_ac], hgammar=db.hgammar[rec_ac],
-        rec_global=np.flatnonzero(rec_ac).astype(np.int32))
+        rec_global=np.flatnonzero(rec_ac).astype(np.int32), pml=None)
+    if pm is not None:
+        bnd_ac = amap[np.asarray(pm["bnd_ac"], dtype=np.int64)]
+        fluid["pml"] = dict(region=np.asarray(pm["region"])[ac_e], bnd=bnd_ac[bnd_ac >= 0].astype(np.int32),
+                            dt=pm["dt"], **{k: pm[k][ac_e] for k in pml_keys})
     cpl = dict(
         el_rec_global=np.flatnonzero(~rec_ac).astype(np.int32),
         ac_point=amap[ac["cpl_ac_iglob"]].astype(np.int32), ac_el_point=gmap[ac["cpl_ac_iglob"]].astype(np.int32),
         ac_nx=ac["cpl_ac_nx"], ac_nz=ac["cpl_ac_nz"], ac_w=ac["cpl_ac_w"],
         el_point=gmap[ac["cpl_el_iglob"]].astype(np.int32), el_ac_point=amap[ac["cpl_el_iglob"]].astype(np.int32),
         el_nx=ac["cpl_el_nx"], el_nz=ac["cpl_el_nz"], el_w=ac["cpl_el_w"],
-        use_trick=bool(ac.get("use_trick", False)))
+        use_trick=bool(ac.get("use_trick", False)), ac_el_elpt=None, el_ac_elpt=None)
+    if "cpl_ac_elpt" in ac:
+        # element GLL points behind each entry, in the sub-mesh element numberings
+        q = np.asarray(ac["cpl_ac_elpt"], dtype=np.int64)
+        cpl["ac_el_elpt"] = (emap[q // 25] * 25 + q % 25).astype(np.int32)
+        q = np.asarray(ac["cpl_el_acpt"], dtype=np.int64)
+        cpl["el_ac_elpt"] = (eamap[q // 25] * 25 + q % 25).astype(np.int32)
+        if (cpl["ac_el_elpt"] < 0).any() or (cpl["el_ac_elpt"] < 0).any():
+            raise ValueError("coupling entry behind an element of the wrong domain")
     return sub, fluid, cpl, dict(solid_points=gl, fluid_points=ga)
 
 
@@ -178,6 +205,14 @@ class CoupledSolver:
         a.nrec, a.rec_ispec = len(fl["rec_ispec"]), i(fl["rec_ispec"])
         a.hxir, a.hgammar, a.rec_global = dd(fl["hxir"]), dd(fl["hgammar"]), i(fl["rec_global"])
         a.tile_elems = tile_elems
+        fp = fl["pml"]
+        if fp is not None:
+            a.pml_region = i(fp["region"])
+            a.pml_K_x, a.pml_K_z = dd(fp["K_x"]), dd(fp["K_z"])
+            a.pml_d_x, a.pml_d_z = dd(fp["d_x"]), dd(fp["d_z"])
+            a.pml_alpha_x, a.pml_alpha_z = dd(fp["alpha_x"]), dd(fp["alpha_z"])
+            a.npml_edge, a.pml_edge_iglob = len(fp["bnd"]), i(fp["bnd"])
+            a.pml_dt = float(fp["dt"])
         c = CouplingDesc()
         c.nrec_total = len(db.rec_ispec)
         c.el_rec_global = i(cp["el_rec_global"])
@@ -189,6 +224,8 @@ class CoupledSolver:
         c.ncpl_el = len(cp["el_point"])
         c.cpl_el_point, c.cpl_el_ac_point = i(cp["el_point"]), i(cp["el_ac_point"])
         c.cpl_el_nx, c.cpl_el_nz, c.cpl_el_w = f(cp["el_nx"]), f(cp["el_nz"]), f(cp["el_w"])
+        if cp["ac_el_elpt"] is not None:
+            c.cpl_ac_el_elpt, c.cpl_el_ac_elpt = i(cp["ac_el_elpt"]), i(cp["el_ac_elpt"])
         h = _vp()
         _check(lib.sf2d_coupled_create(ctypes.byref(ed), ctypes.byref(a), ctypes.byref(c), ctypes.byref(h)))
         self._h, self._lib = h, lib
@@ -214,6 +251,17 @@ class CoupledSolver:
         seis = np.zeros((self.nrec, nstep, 2), dtype=np.float64) if seismograms else None
         _check(self._lib.sf2d_coupled_run(self._h, nstep, None if seis is None else seis.ctypes.data_as(_d)))
         return seis
+
+    def enqueue(self, nstep: int):
+        _check(self._lib.sf2d_coupled_enqueue(self._h, nstep))
+
+    def synchronize(self, timeout_s: float = 0.0):
+        _check(self._lib.sf2d_coupled_synchronize(self._h))
+
+    def stream_handle(self) -> int:
+        v = _vp()
+        _check(self._lib.sf2d_coupled_get_stream(self._h, ctypes.byref(v)))
+        return int(v.value or 0)
 
     def get_fields(self):
         """displ, veloc, accel (nglob, 2) and pot, pot_dot, pot_dot_dot (nglob,) in global numbering."""
@@ -251,7 +299,22 @@ class CoupledSolver:
         return [float(x) for x in ms]
 
     def layout_info(self):
+        """Layout of the fluid tiling."""
         info = (ctypes.c_longlong * 6)()
         _check(self._lib.sf2d_coupled_layout_info(self._h, info))
         keys = ["ntiles", "nshared", "max_local", "smem", "n_interior", "n_slots"]
         return dict(zip(keys, [int(x) for x in info]))
+
+    def solid_layout_info(self):
+        """Layout of the solid tiling (keys of ElasticSolver.layout_info)."""
+        v = (ctypes.c_longlong * 8)()
+        _check(self._lib.sf2d_coupled_solid_layout_info(self._h, v))
+        keys = ["ntiles", "nshared", "max_local", "max_elems", "device_bytes", "smem_bytes",
+                "threads_per_block", "n_slots"]
+        return dict(zip(keys, [int(x) for x in v]))
+
+    def launch_count(self, nstep: int) -> int:
+        """Kernel launches that enqueue(nstep) issues."""
+        n = ctypes.c_longlong()
+        _check(self._lib.sf2d_coupled_launch_count(self._h, nstep, ctypes.byref(n)))
+        return int(n.value)

@@ -72,13 +72,30 @@ struct AcParams {
   int shared_begin, nshared;
   int max_q, max_local;
   float hconst[60];           // hprime[25], hprimewgll[25], wxgll[5], wzgll[5]
+  // CPML: elements of slots >= pml_slot0 lie in the layer (see Params)
+  int pml_slot0;
+  const int *pml_region;
+  const double2 *pml_coef;    // 3 per PML point: (K_x, K_z), (alpha_x, alpha_z), (beta_x, beta_z)
+  const float *pml_jk;        // jacobian / kappa per PML point
+  float2 *pml_rm;             // 3 per PML point: dchi_dx memory (1, 2), dchi_dz memory (1, 2), chi memory (1, 2)
+  float2 *pml_rm_l;           // LDDRK copies
+  float *pold;                // mid-step chi of this step for the solid's coupling terms (Newmark + CPML)
+  double DT, h_old;
+  // fluid-side coupling entries whose solid element lies in a CPML layer have
+  // cpl_src = ~k: the displacement they see is formed before this kernel (k_cpl_pml_fluid)
+  const float2 *cpl_pml_u;    // per layer entry k: the displacement to apply
 };
 
-// Shared-memory regions of one fluid tile, 16-byte aligned.
+// free_mask bits: free surface, outer edge of a CPML layer; both zero chi,
+// chi_dot and chi_dot_dot before and after the forces
+constexpr uint8_t AC_FREE = 1, AC_EDGE = 2;
+
+// Shared-memory regions of one fluid tile, 16-byte aligned (pold and pml only
+// in CPML tiles).
 struct AcSmem {
-  size_t geo, fac, p, pd, acc, h, lib, total;
+  size_t geo, fac, p, pd, acc, h, lib, pold, pml, total;
 };
-__host__ __device__ inline AcSmem ac_smem_layout(int max_q, int max_local) {
+__host__ __device__ inline AcSmem ac_smem_layout(int max_q, int max_local, bool pml = false) {
   AcSmem L;
   size_t o = 0;
   L.geo = o;
@@ -95,6 +112,10 @@ __host__ __device__ inline AcSmem ac_smem_layout(int max_q, int max_local) {
   o = align16(o + 64 * sizeof(float));
   L.lib = o;
   o = align16(o + static_cast<size_t>((max_q + 7) / 8 * 8) * sizeof(uint16_t));
+  L.pold = o;
+  if (pml) o = align16(o + static_cast<size_t>(max_local) * sizeof(float));
+  L.pml = o;
+  if (pml) o = align16(o + static_cast<size_t>(max_q) * sizeof(float));
   L.total = o;
   return L;
 }
@@ -145,10 +166,14 @@ __device__ __forceinline__ void record_receiver_ac(const AcParams &A, int r, int
   out[1] = -A.sinrot * vx + A.cosrot * vz;
 }
 
-template <int NT, bool LDDRK>
-__global__ void __launch_bounds__(NT) k_acoustic_tile(const AcParams A, int record_prev, int stage) {
+// PML: the tiles of a CPML layer: mid-step chi + dt^2/4 chi_dot_dot, the
+// gradient and potential memory variables, the modified gradient and the
+// extra terms (pml_compute_memory_variables.f90:42-224,
+// pml_compute_accel_contribution.f90:42-180).  Tiles [tile0, tile0 + gridDim.x).
+template <int NT, bool LDDRK, bool PML = false>
+__global__ void __launch_bounds__(NT) k_acoustic_tile(const AcParams A, int record_prev, int stage, int tile0) {
   extern __shared__ __align__(16) unsigned char smem[];
-  const TileInfo &ti = A.tiles[blockIdx.x];
+  const TileInfo &ti = A.tiles[tile0 + blockIdx.x];
   const int tid = threadIdx.x;
   const int n_int = ti.n_int;
   const int n_sh = ti.n_sh;
@@ -156,8 +181,10 @@ __global__ void __launch_bounds__(NT) k_acoustic_tile(const AcParams A, int reco
   const int nq = ti.nelem * 25;
   const int ebase = ti.elem_base * 25;
   const int int_begin = ti.int_begin;
-  const AcSmem L = ac_smem_layout(A.max_q, A.max_local);
+  const AcSmem L = ac_smem_layout(A.max_q, A.max_local, PML);
   float4 *s_geo = reinterpret_cast<float4 *>(smem + L.geo);
+  float *s_pold = reinterpret_cast<float *>(smem + L.pold);
+  float *s_pml = reinterpret_cast<float *>(smem + L.pml);
   float *s_fac = reinterpret_cast<float *>(smem + L.fac);
   float *s_p = reinterpret_cast<float *>(smem + L.p);
   float *s_pd = reinterpret_cast<float *>(smem + L.pd);
@@ -200,12 +227,17 @@ __global__ void __launch_bounds__(NT) k_acoustic_tile(const AcParams A, int reco
   for (int l = tid; l < nl; l += NT) {
     const int g = l < n_int ? int_begin + l : A.sh_ids[ti.sh_off + l - n_int];
     float p = s_p[l], pd = s_pd[l];
+    const uint8_t m = A.free_mask[g];
     if (!LDDRK) {
       const float pdd = s_acc[l];
+      // mid-step potential (update_displacement_Newmark.F90:374-380), zero on the layer's edge
+      if (PML)
+        s_pold[l] = (m & AC_EDGE) ? 0.f
+                                  : static_cast<float>(static_cast<double>(p) + A.h_old * static_cast<double>(pdd));
       p = newmark_displ(p, pd, pdd, dt, dt2o2);
       pd = newmark_veloc(pd, pdd, dto2);
     }
-    if (A.free_mask[g]) {
+    if (m) {
       p = 0.f;
       pd = 0.f;
     }
@@ -224,13 +256,19 @@ __global__ void __launch_bounds__(NT) k_acoustic_tile(const AcParams A, int reco
     }
     for (int q = ti.cpl_off; q < ti.cpl_off + ti.cpl_n; ++q) {
       const int l = A.cpl_local[q];
+      // a negative source names the CPML entry ~src (its displacement formed by k_cpl_pml_fluid)
       const int ge = A.cpl_src[q];
       const float4 nw = A.cpl_nw[q];
-      float2 u = A.u_el[ge];
-      if (!LDDRK) {
-        const float2 v = A.v_el[ge], a = A.a_el[ge];
-        u.x = newmark_displ(u.x, v.x, a.x, dt, dt2o2);
-        u.y = newmark_displ(u.y, v.y, a.y, dt, dt2o2);
+      float2 u;
+      if (ge >= 0) {
+        u = A.u_el[ge];
+        if (!LDDRK) {
+          const float2 v = A.v_el[ge], a = A.a_el[ge];
+          u.x = newmark_displ(u.x, v.x, a.x, dt, dt2o2);
+          u.y = newmark_displ(u.y, v.y, a.y, dt, dt2o2);
+        }
+      } else {
+        u = A.cpl_pml_u[~ge];
       }
       const float displ_n = u.x * nw.x + u.y * nw.y;
       s_acc[l] = s_acc[l] + nw.z * displ_n;
@@ -259,8 +297,60 @@ __global__ void __launch_bounds__(NT) k_acoustic_tile(const AcParams A, int reco
       dgam += s_p[le[5 * k + i]] * s_h[5 * j + k];
     }
     const float4 g4 = s_geo[f];
-    const float dxl = dxi * g4.x + dgam * g4.z;
-    const float dzl = dxi * g4.y + dgam * g4.w;
+    float dxl = dxi * g4.x + dgam * g4.z;
+    float dzl = dxi * g4.y + dgam * g4.w;
+    if (PML) {
+      const int ps = ebase + f - 25 * A.pml_slot0;
+      const int region = A.pml_region[ti.elem_base + e - A.pml_slot0];
+      const PmlPoint c = pml_point(A.pml_coef, ps);
+      float dxl_o = 0.f, dzl_o = 0.f;
+      if (!LDDRK) {
+        float oxi = 0.f, og = 0.f;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+          oxi += s_pold[le[5 * j + k]] * s_h[5 * i + k];
+          og += s_pold[le[5 * k + i]] * s_h[5 * j + k];
+        }
+        dxl_o = oxi * g4.x + og * g4.z;
+        dzl_o = oxi * g4.y + og * g4.w;
+      }
+      const PmlConv cax = pml_conv(c.ax, A.DT), caz = pml_conv(c.az, A.DT);
+      const PmlConv cbx = pml_conv(c.bx, A.DT), cbz = pml_conv(c.bz, A.DT);
+      const PmlLik zx = pml_lik(c.kz, c.bz, c.az, c.kx, c.bx, c.ax, region, false);  // poles alpha_z, beta_x
+      const PmlLik xz = pml_lik(c.kx, c.bx, c.ax, c.kz, c.bz, c.az, region, true);   // poles alpha_x, beta_z
+      float2 rx = A.pml_rm[3 * ps], rz = A.pml_rm[3 * ps + 1], rp = A.pml_rm[3 * ps + 2];
+      float2 lx = make_float2(0.f, 0.f), lz = lx, lp = lx;
+      if (LDDRK) {
+        lx = A.pml_rm_l[3 * ps];
+        lz = A.pml_rm_l[3 * ps + 1];
+        lp = A.pml_rm_l[3 * ps + 2];
+      }
+      const float al = A.alpha[stage], be = A.beta[stage];
+      pml_update<LDDRK>(rx.x, lx.x, caz, c.az, dxl, dxl_o, al, be, dt);
+      pml_update<LDDRK>(rx.y, lx.y, cbx, c.bx, dxl, dxl_o, al, be, dt);
+      pml_update<LDDRK>(rz.x, lz.x, cax, c.ax, dzl, dzl_o, al, be, dt);
+      pml_update<LDDRK>(rz.y, lz.y, cbz, c.bz, dzl, dzl_o, al, be, dt);
+      dxl = static_cast<float>(zx.A0 * dxl + zx.A1 * rx.x + zx.A2 * rx.y);
+      dzl = static_cast<float>(xz.A0 * dzl + xz.A1 * rz.x + xz.A2 * rz.y);
+      // the layer's terms at this point (pml_compute_accel_contribution.f90:42-180)
+      const PmlL Lc = pml_l(c.kx, c.bx, c.ax, c.kz, c.bz, c.az, region);  // poles alpha_x, alpha_z
+      const int lq = le[q];
+      const float pq = s_p[lq], pdq = s_pd[lq];
+      const float po = LDDRK ? 0.f : s_pold[lq];
+      pml_update<LDDRK>(rp.x, lp.x, cax, c.ax, pq, po, al, be, dt);
+      pml_update<LDDRK>(rp.y, lp.y, caz, c.az, pq, po, al, be, dt);
+      const float wwf = s_h[50 + i] * s_h[55 + j] * A.pml_jk[ps];
+      s_pml[f] = static_cast<float>(static_cast<double>(wwf) *
+                                    (Lc.A1 * pdq + Lc.A2 * pq + Lc.A3 * rp.x + Lc.A4 * rp.y));
+      A.pml_rm[3 * ps] = rx;
+      A.pml_rm[3 * ps + 1] = rz;
+      A.pml_rm[3 * ps + 2] = rp;
+      if (LDDRK) {
+        A.pml_rm_l[3 * ps] = lx;
+        A.pml_rm_l[3 * ps + 1] = lz;
+        A.pml_rm_l[3 * ps + 2] = lp;
+      }
+    }
     const float fac = s_fac[f];
     s_geo[f] = make_float4(fac * (g4.x * dxl + g4.y * dzl), fac * (g4.z * dxl + g4.w * dzl), 0.f, 0.f);
   }
@@ -283,7 +373,9 @@ __global__ void __launch_bounds__(NT) k_acoustic_tile(const AcParams A, int reco
         s2 += te[5 * k + i].y * s_h[25 + 5 * k + j];
       }
       const int l = s_lib[f];
-      s_acc[l] = s_acc[l] - (s_h[55 + j] * s1 + s_h[50 + i] * s2);
+      float acc = s_acc[l] - (s_h[55 + j] * s1 + s_h[50 + i] * s2);
+      if (PML) acc = acc - s_pml[f];
+      s_acc[l] = acc;
     }
     cb = ce;
     __syncthreads();
@@ -317,6 +409,7 @@ __global__ void __launch_bounds__(NT) k_acoustic_tile(const AcParams A, int reco
       A.p[g] = p;
       A.pd[g] = pd;
       A.pdd[g] = pdd;
+      if (PML && !LDDRK && A.pold) A.pold[g] = s_pold[l];
       bad |= !(fabsf(p) < 1e25f);
     } else {
       A.partial[ti.sh_off + l - n_int] = acc;
@@ -332,12 +425,16 @@ __global__ void __launch_bounds__(SHARED_NT) k_acoustic_shared(const AcParams A,
   if (s < A.nshared) {
     const int g = A.shared_begin + s;
     float p = A.p[g], pd = A.pd[g];
+    const uint8_t m = A.free_mask[g];
     if (!LDDRK) {
       const float pdd0 = A.pdd[g];
+      if (A.pold)
+        A.pold[g] = (m & AC_EDGE) ? 0.f
+                                  : static_cast<float>(static_cast<double>(p) + A.h_old * static_cast<double>(pdd0));
       p = newmark_displ(p, pd, pdd0, A.dt, A.dt2o2);
       pd = newmark_veloc(pd, pdd0, A.dto2);
     }
-    const bool fs = A.free_mask[g] != 0;
+    const bool fs = m != 0;
     if (fs) {
       p = 0.f;
       pd = 0.f;
@@ -368,6 +465,73 @@ __global__ void __launch_bounds__(SHARED_NT) k_acoustic_shared(const AcParams A,
     if (!(fabsf(p) < 1e25f)) *A.d_status = 1;
   }
   if (last_stage && blockIdx.x == 0 && threadIdx.x == 0) *A.d_step = step + 1;
+}
+
+// Coupling entries next to a CPML layer, one thread per entry, once per step
+// or LDDRK stage.  Both memory variables advance here, so the tile kernels
+// only read the result.
+struct CplPml {
+  int n;              // layer entries
+  const int *point;   // fluid side: solid device point; solid side: fluid device point
+  const double *coef; // fluid side 6 per entry: A0, A1, c0, c1, c2, bb; solid side 8: A0..A3, c0, c1, c2, bb
+  float *rm, *rm_l;   // fluid side 2 per entry (x, z), solid side 1
+  float *out;         // fluid side float2 displacement, solid side pressure
+};
+
+// Fluid side (compute_coupling_acoustic_el.f90:111-160): the solid's predicted
+// displacement u as A0 u + A1 r, r the memory variable of u driven by the
+// mid-step displacement u0 + dt^2/4 a0 (Newmark), for a solid element in a layer.
+template <bool LDDRK>
+__global__ void k_cpl_pml_fluid(const CplPml C, const float2 *u_el, const float2 *v_el, const float2 *a_el, float dt,
+                                float dt2o2, double h_old, float al, float be) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= C.n) return;
+  const int ge = C.point[k];
+  const float2 u0 = u_el[ge];
+  float2 u = u0, uo = make_float2(0.f, 0.f);
+  if (!LDDRK) {
+    const float2 v = v_el[ge], a0 = a_el[ge];
+    u.x = newmark_displ(u0.x, v.x, a0.x, dt, dt2o2);
+    u.y = newmark_displ(u0.y, v.y, a0.y, dt, dt2o2);
+    uo = make_float2(static_cast<float>(static_cast<double>(u0.x) + h_old * static_cast<double>(a0.x)),
+                     static_cast<float>(static_cast<double>(u0.y) + h_old * static_cast<double>(a0.y)));
+  }
+  const double *c = C.coef + 6 * k;
+  const PmlConv cv{c[2], c[3], c[4]};
+  float2 rf = make_float2(C.rm[2 * k], C.rm[2 * k + 1]);
+  float2 rfl = LDDRK ? make_float2(C.rm_l[2 * k], C.rm_l[2 * k + 1]) : make_float2(0.f, 0.f);
+  pml_update<LDDRK>(rf.x, rfl.x, cv, c[5], u.x, uo.x, al, be, dt);
+  pml_update<LDDRK>(rf.y, rfl.y, cv, c[5], u.y, uo.y, al, be, dt);
+  C.rm[2 * k] = rf.x;
+  C.rm[2 * k + 1] = rf.y;
+  if (LDDRK) {
+    C.rm_l[2 * k] = rfl.x;
+    C.rm_l[2 * k + 1] = rfl.y;
+  }
+  C.out[2 * k] = static_cast<float>(c[0] * static_cast<double>(u.x) + c[1] * static_cast<double>(rf.x));
+  C.out[2 * k + 1] = static_cast<float>(c[0] * static_cast<double>(u.y) + c[1] * static_cast<double>(rf.y));
+}
+
+// Solid side (compute_coupling_viscoelastic_ac.f90:105-150): the pressure
+// -(A0 chi_dd + A1 chi_d + A2 chi + A3 r) of a fluid element in a layer, r the
+// memory variable of chi driven by the mid-step chi (Newmark); runs after the
+// fluid step, before the solid tile kernel.
+template <bool LDDRK>
+__global__ void k_cpl_pml_solid(const CplPml C, const float *p, const float *pd, const float *pdd, const float *pold,
+                                float dt, float al, float be) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= C.n) return;
+  const int ga = C.point[k];
+  const double *c = C.coef + 8 * k;
+  const PmlConv cv{c[4], c[5], c[6]};
+  float r = C.rm[k];
+  float rl = LDDRK ? C.rm_l[k] : 0.f;
+  const float pot = p[ga];
+  pml_update<LDDRK>(r, rl, cv, c[7], pot, LDDRK ? 0.f : pold[ga], al, be, dt);
+  C.rm[k] = r;
+  if (LDDRK) C.rm_l[k] = rl;
+  C.out[k] = static_cast<float>(-(c[0] * static_cast<double>(pdd[ga]) + c[1] * static_cast<double>(pd[ga]) +
+                                  c[2] * static_cast<double>(pot) + c[3] * static_cast<double>(r)));
 }
 
 // records the step before *d_step for every fluid receiver

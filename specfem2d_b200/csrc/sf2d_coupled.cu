@@ -33,14 +33,31 @@ __global__ void k_scatter_f(const float *src, const int *dev2glob, float *dst, i
   if (d < n) dst[dev2glob[d]] = src[d];
 }
 
-using AcTileFn = void (*)(AcParams, int, int);
+using AcTileFn = void (*)(AcParams, int, int, int);
 
+template <bool PML>
 AcTileFn pick_ac_tile(int nt, bool lddrk) {
   switch (nt) {
-    case 128: return lddrk ? sf2d::k_acoustic_tile<128, true> : sf2d::k_acoustic_tile<128, false>;
-    case 512: return lddrk ? sf2d::k_acoustic_tile<512, true> : sf2d::k_acoustic_tile<512, false>;
-    default: return lddrk ? sf2d::k_acoustic_tile<256, true> : sf2d::k_acoustic_tile<256, false>;
+    case 128: return lddrk ? sf2d::k_acoustic_tile<128, true, PML> : sf2d::k_acoustic_tile<128, false, PML>;
+    case 512: return lddrk ? sf2d::k_acoustic_tile<512, true, PML> : sf2d::k_acoustic_tile<512, false, PML>;
+    default: return lddrk ? sf2d::k_acoustic_tile<256, true, PML> : sf2d::k_acoustic_tile<256, false, PML>;
   }
+}
+
+// Damping data of one element GLL point p of a descriptor's CPML arrays.
+struct PmlAt {
+  double kx, kz, ax, az, bx, bz;
+};
+template <typename Desc>
+PmlAt pml_at(const Desc *d, size_t p) {
+  PmlAt c;
+  c.kx = d->pml_K_x[p];
+  c.kz = d->pml_K_z[p];
+  c.ax = d->pml_alpha_x[p];
+  c.az = d->pml_alpha_z[p];
+  c.bx = c.ax + d->pml_d_x[p] / c.kx;
+  c.bz = c.az + d->pml_d_z[p] / c.kz;
+  return c;
 }
 
 }  // namespace
@@ -54,9 +71,14 @@ struct sf2d_coupled {
   float *d_stage = nullptr;
   int *ctr = nullptr;
   double *seis = nullptr;
+  sf2d::CplPml cpl_fluid{}, cpl_solid{};  // coupling entries next to a CPML layer
   AcTileFn tile_fn = nullptr;
+  AcTileFn pml_fn = nullptr;  // tiles [pml_tile0, ntiles) hold the fluid CPML layer
+  int pml_tile0 = 0;
+  size_t pml_smem = 0;
   size_t smem = 0;
   int nt = 256, nstage = 1, nglob = 0, nrec_total = 0, nstep = 0, steps_done = 0;
+  size_t npml_q = 0;  // GLL points of the fluid CPML elements
   bool lddrk = false;
   int chunk = 32;
   cudaGraphExec_t graph = nullptr;
@@ -79,6 +101,22 @@ struct sf2d_coupled {
     if (count) SF2D_CUDA(cudaMemcpy(*p, host, count * sizeof(T_), cudaMemcpyHostToDevice));
     return SF2D_OK;
   }
+  // device arrays of one side's CPML coupling entries; `per` memory variables
+  // and outputs per entry
+  int upload_cpl(sf2d::CplPml &c, const std::vector<int> &pt, const std::vector<double> &coef, int per) {
+    int rc = 0;
+    c.n = static_cast<int>(pt.size());
+    if ((rc = upload_const(&c.point, pt)) || (rc = upload_const(&c.coef, coef))) return rc;
+    const size_t n = std::max<size_t>(1, pt.size() * per);
+    if ((rc = alloc(&c.rm, n)) || (rc = alloc(&c.out, n))) return rc;
+    SF2D_CUDA(cudaMemset(c.rm, 0, sizeof(float) * n));
+    SF2D_CUDA(cudaMemset(c.out, 0, sizeof(float) * n));
+    if (lddrk) {
+      if ((rc = alloc(&c.rm_l, n))) return rc;
+      SF2D_CUDA(cudaMemset(c.rm_l, 0, sizeof(float) * n));
+    }
+    return SF2D_OK;
+  }
   template <typename T_>
   int upload_const(const T_ **p, const std::vector<T_> &v) {
     T_ *q = nullptr;
@@ -88,7 +126,10 @@ struct sf2d_coupled {
   }
 
   void launch_ac_tile(bool record_prev, int stage) {
-    tile_fn<<<T.ntiles, nt, smem, el->stream>>>(A, record_prev ? 1 : 0, stage);
+    if (pml_tile0 > 0) tile_fn<<<pml_tile0, nt, smem, el->stream>>>(A, record_prev ? 1 : 0, stage, 0);
+    if (pml_tile0 < T.ntiles)
+      (pml_fn ? pml_fn : tile_fn)<<<T.ntiles - pml_tile0, nt, pml_fn ? pml_smem : smem, el->stream>>>(
+          A, record_prev ? 1 : 0, stage, pml_tile0);
   }
   void launch_ac_shared(int stage) {
     const int nb = std::max(1, (A.nshared + sf2d::SHARED_NT - 1) / sf2d::SHARED_NT);
@@ -98,10 +139,32 @@ struct sf2d_coupled {
     else
       sf2d::k_acoustic_shared<false><<<nb, sf2d::SHARED_NT, 0, el->stream>>>(A, stage, last);
   }
+  void launch_cpl_fluid(int stage) {
+    if (cpl_fluid.n == 0) return;
+    const int nb = (cpl_fluid.n + 127) / 128;
+    const sf2d::Params &P = el->P;
+    if (lddrk)
+      sf2d::k_cpl_pml_fluid<true><<<nb, 128, 0, el->stream>>>(cpl_fluid, P.u, P.v, P.a, P.dt, P.dt2o2, A.h_old,
+                                                              A.alpha[stage], A.beta[stage]);
+    else
+      sf2d::k_cpl_pml_fluid<false><<<nb, 128, 0, el->stream>>>(cpl_fluid, P.u, P.v, P.a, P.dt, P.dt2o2, A.h_old,
+                                                               0.f, 0.f);
+  }
+  void launch_cpl_solid(int stage) {
+    if (cpl_solid.n == 0) return;
+    const int nb = (cpl_solid.n + 127) / 128;
+    if (lddrk)
+      sf2d::k_cpl_pml_solid<true><<<nb, 128, 0, el->stream>>>(cpl_solid, A.p, A.pd, A.pdd, A.pold, A.dt,
+                                                              A.alpha[stage], A.beta[stage]);
+    else
+      sf2d::k_cpl_pml_solid<false><<<nb, 128, 0, el->stream>>>(cpl_solid, A.p, A.pd, A.pdd, A.pold, A.dt, 0.f, 0.f);
+  }
   void launch_step(bool record_prev) {
     for (int st = 0; st < nstage; ++st) {
+      launch_cpl_fluid(st);
       launch_ac_tile(record_prev && st == 0, st);
       launch_ac_shared(st);
+      launch_cpl_solid(st);
       el->launch_tile(record_prev && st == 0, st);
       el->launch_shared(st);
     }
@@ -158,6 +221,34 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
     if (ad->src_ispec[k] < 0 || ad->src_ispec[k] >= ad->nspec) return fail(SF2D_ERR_INVALID, "fluid source element out of range");
   for (int k = 0; k < ad->nrec; ++k)
     if (ad->rec_ispec[k] < 0 || ad->rec_ispec[k] >= ad->nspec) return fail(SF2D_ERR_INVALID, "fluid receiver element out of range");
+  const bool pml_ac = ad->pml_region != nullptr, pml_el = eld->pml_region != nullptr;
+  std::vector<int> group;
+  if (pml_ac) {
+    if (!ad->pml_K_x || !ad->pml_K_z || !ad->pml_d_x || !ad->pml_d_z || !ad->pml_alpha_x || !ad->pml_alpha_z ||
+        !(ad->pml_dt > 0.0))
+      return fail(SF2D_ERR_INVALID, "missing fluid CPML arrays");
+    if (ad->nstacey > 0) return fail(SF2D_ERR_INVALID, "CPML layers and Stacey conditions exclude each other");
+    if (ad->npml_edge < 0 || (ad->npml_edge > 0 && !ad->pml_edge_iglob))
+      return fail(SF2D_ERR_INVALID, "bad fluid CPML edge list");
+    for (int k = 0; k < ad->npml_edge; ++k)
+      if (ad->pml_edge_iglob[k] < 0 || ad->pml_edge_iglob[k] >= ad->nglob)
+        return fail(SF2D_ERR_INVALID, "fluid CPML edge point out of range");
+    group.assign(ad->nspec, 0);
+    for (int e = 0; e < ad->nspec; ++e) {
+      if (ad->pml_region[e] < 0 || ad->pml_region[e] > 3) return fail(SF2D_ERR_INVALID, "CPML region must be 0 to 3");
+      group[e] = ad->pml_region[e] > 0 ? 1 : 0;
+    }
+  }
+  if (pml_ac || pml_el) {
+    if ((cp->ncpl_ac > 0 && !cp->cpl_ac_el_elpt) || (cp->ncpl_el > 0 && !cp->cpl_el_ac_elpt))
+      return fail(SF2D_ERR_INVALID, "coupling entries need their element points with CPML layers");
+    for (int k = 0; k < cp->ncpl_ac; ++k)
+      if (cp->cpl_ac_el_elpt[k] < 0 || cp->cpl_ac_el_elpt[k] >= eld->nspec * NGLL2)
+        return fail(SF2D_ERR_INVALID, "coupling element point out of range");
+    for (int k = 0; k < cp->ncpl_el; ++k)
+      if (cp->cpl_el_ac_elpt[k] < 0 || cp->cpl_el_ac_elpt[k] >= ad->nspec * NGLL2)
+        return fail(SF2D_ERR_INVALID, "coupling element point out of range");
+  }
 
   auto *C = new sf2d_coupled();
   std::unique_ptr<sf2d_coupled> guard(C);
@@ -175,9 +266,12 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
 
   // ---- fluid tiling and per-slot data
   const int te = ad->tile_elems > 0 ? ad->tile_elems : 32;
-  std::string err = build_tiling(ad->nspec, ad->nglob, ad->ibool, ad->centroid_xz, te, C->T);
+  std::string err = build_tiling(ad->nspec, ad->nglob, ad->ibool, ad->centroid_xz, te, C->T,
+                                 pml_ac ? group.data() : nullptr, pml_ac ? 2 : 1);
   if (!err.empty()) return fail(SF2D_ERR_INVALID, "fluid tiling: " + err);
   const Tiling &T = C->T;
+  C->pml_tile0 = pml_ac ? T.group_tile_begin[1] : T.ntiles;
+  const int pml_slot0 = C->pml_tile0 < T.ntiles ? T.tiles[C->pml_tile0].elem_base : ad->nspec;
   const size_t nq = static_cast<size_t>(ad->nspec) * NGLL2;
   std::vector<float4> geo(nq);
   std::vector<float> fac(nq);
@@ -191,7 +285,26 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
   std::vector<float> rmass(ad->nglob);
   std::vector<uint8_t> fmask(ad->nglob, 0);
   for (int g = 0; g < ad->nglob; ++g) rmass[g] = ad->rmass_inverse[T.dev2glob[g]];
-  for (int k = 0; k < ad->nfree; ++k) fmask[T.glob2dev[ad->free_iglob[k]]] = 1;
+  for (int k = 0; k < ad->nfree; ++k) fmask[T.glob2dev[ad->free_iglob[k]]] |= AC_FREE;
+  std::vector<int> pml_region_s;
+  std::vector<double2> pml_coef;
+  std::vector<float> pml_jk;
+  if (pml_ac) {
+    for (int k = 0; k < ad->npml_edge; ++k) fmask[T.glob2dev[ad->pml_edge_iglob[k]]] |= AC_EDGE;
+    for (int s = pml_slot0; s < ad->nspec; ++s) {
+      const int e = T.elem_order[s];
+      pml_region_s.push_back(ad->pml_region[e]);
+      for (int q = 0; q < NGLL2; ++q) {
+        const size_t p = static_cast<size_t>(e) * NGLL2 + q;
+        const PmlAt c = pml_at(ad, p);
+        pml_coef.push_back(make_double2(c.kx, c.kz));
+        pml_coef.push_back(make_double2(c.ax, c.az));
+        pml_coef.push_back(make_double2(c.bx, c.bz));
+        pml_jk.push_back(ad->jacobian[p] / ad->kappastore[p]);  // fac = J / kappa in FP32
+      }
+    }
+  }
+  const size_t npml_q = static_cast<size_t>(ad->nspec - pml_slot0) * NGLL2;
   // a boundary or coupling point goes to the tile of the first element holding it
   std::vector<int> glob_tile(ad->nglob, -1);
   for (int e = 0; e < ad->nspec; ++e)
@@ -205,7 +318,8 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
   for (int k = 0; k < cp->ncpl_ac; ++k) cpl_t[glob_tile[cp->cpl_ac_point[k]]].push_back(k);
   for (int k = 0; k < ad->nsrc; ++k) src_t[T.elem_tile[ad->src_ispec[k]]].push_back(k);
   for (int k = 0; k < ad->nrec; ++k) rec_t[T.elem_tile[ad->rec_ispec[k]]].push_back(k);
-  std::vector<int> st_local, cpl_local, cpl_src, src_local, src_id, rec_id, rec_dev;
+  std::vector<int> st_local, cpl_local, cpl_src, cpl_pml_pt, src_local, src_id, rec_id, rec_dev;
+  std::vector<double> cpl_pml_coef;
   std::vector<float2> st_wr, src_sk;
   std::vector<float4> cpl_nw, rec_geo;
   std::vector<float> rec_rho;
@@ -222,6 +336,22 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
       cpl_local.push_back(T.local_id(t, cp->cpl_ac_point[k]));
       cpl_src.push_back(S->T.glob2dev[cp->cpl_ac_el_point[k]]);
       cpl_nw.push_back(make_float4(cp->cpl_ac_nx[k], cp->cpl_ac_nz[k], cp->cpl_ac_w[k], 0.f));
+      const int q = pml_el ? cp->cpl_ac_el_elpt[k] : -1;
+      const int region = q >= 0 ? eld->pml_region[q / NGLL2] : 0;
+      if (region <= 0) continue;
+      // solid element in the layer: strain coefficients of lik_parameter_computation,
+      // 13 form for X-only, 31 form for Z-only (compute_coupling_acoustic_el.f90:113-134)
+      if (region == CPML_XZ)
+        return fail(SF2D_ERR_INVALID, "a fluid-solid boundary in a CPML corner region is not supported");
+      const PmlAt c = pml_at(eld, static_cast<size_t>(q));
+      const bool x_only = region == CPML_X_ONLY;
+      const PmlLik L = x_only ? pml_lik(c.kx, c.bx, c.ax, c.kz, c.bz, c.az, region, true)
+                              : pml_lik(c.kz, c.bz, c.az, c.kx, c.bx, c.ax, region, false);
+      const double bb = x_only ? c.ax : c.az;
+      const PmlConv cv = pml_conv(bb, eld->pml_dt);
+      cpl_pml_pt.push_back(cpl_src.back());
+      cpl_src.back() = ~static_cast<int>(cpl_pml_pt.size() - 1);
+      for (double x : {L.A0, L.A1, cv.c0, cv.c1, cv.c2, bb}) cpl_pml_coef.push_back(x);
     }
     tiles[t].cpl_n = static_cast<int>(cpl_local.size()) - tiles[t].cpl_off;
     tiles[t].src_off = static_cast<int>(src_local.size());
@@ -284,6 +414,29 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
       (rc = C->upload_const(&A.rec_dev, rec_dev)) || (rc = C->upload_const(&A.rec_h, rec_h)) ||
       (rc = C->upload_const(&A.rec_geo, rec_geo)) || (rc = C->upload_const(&A.rec_rho, rec_rho)))
     return rc;
+  if (pml_ac || pml_el) {
+    if ((rc = C->upload_cpl(C->cpl_fluid, cpl_pml_pt, cpl_pml_coef, 2))) return rc;
+    A.cpl_pml_u = reinterpret_cast<const float2 *>(C->cpl_fluid.out);
+  }
+  if (pml_ac) {
+    if ((rc = C->upload_const(&A.pml_region, pml_region_s)) || (rc = C->upload_const(&A.pml_coef, pml_coef)) ||
+        (rc = C->upload_const(&A.pml_jk, pml_jk)))
+      return rc;
+    for (int l = 0; l < (C->lddrk ? 2 : 1); ++l) {
+      float2 *r = nullptr;
+      if ((rc = C->alloc(&r, npml_q * 3))) return rc;
+      SF2D_CUDA(cudaMemset(r, 0, sizeof(float2) * std::max<size_t>(1, npml_q * 3)));
+      (l ? A.pml_rm_l : A.pml_rm) = r;
+    }
+    if (!C->lddrk) {
+      if ((rc = C->alloc(&A.pold, ad->nglob))) return rc;
+      SF2D_CUDA(cudaMemset(A.pold, 0, sizeof(float) * ad->nglob));
+    }
+    A.pml_slot0 = pml_slot0;
+    A.DT = ad->pml_dt;
+    C->npml_q = npml_q;
+  }
+  A.h_old = static_cast<double>(eld->deltatsquareover2) / 2.0;
   float *partial;
   if ((rc = C->alloc(&partial, T.sh_ids.size()))) return rc;
   A.partial = partial;
@@ -325,16 +478,25 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
   if ((rc = C->alloc(&C->d_stage, ad->nglob))) return rc;
   C->smem = ac_smem_layout(A.max_q, A.max_local).total;
   if (C->smem > 220 * 1024) return fail(SF2D_ERR_INVALID, "fluid tile too large for shared memory");
-  C->tile_fn = pick_ac_tile(C->nt, C->lddrk);
+  C->tile_fn = pick_ac_tile<false>(C->nt, C->lddrk);
+  if (pml_ac) {
+    C->pml_fn = pick_ac_tile<true>(C->nt, C->lddrk);
+    C->pml_smem = ac_smem_layout(A.max_q, A.max_local, true).total;
+    if (C->pml_smem > 220 * 1024) return fail(SF2D_ERR_INVALID, "fluid tile too large for shared memory");
+  }
   {
     // the limit belongs to the kernel: only ever raise it (see the solid solver)
     static std::mutex attr_mutex;
     std::lock_guard<std::mutex> lock(attr_mutex);
-    cudaFuncAttributes fa;
-    SF2D_CUDA(cudaFuncGetAttributes(&fa, C->tile_fn));
-    if (fa.maxDynamicSharedSizeBytes < static_cast<int>(C->smem))
-      SF2D_CUDA(cudaFuncSetAttribute(C->tile_fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(C->smem)));
+    const std::pair<AcTileFn, size_t> fns[2] = {{C->tile_fn, C->smem}, {C->pml_fn, C->pml_smem}};
+    for (const auto &fs : fns) {
+      if (!fs.first) continue;
+      cudaFuncAttributes fa;
+      SF2D_CUDA(cudaFuncGetAttributes(&fa, fs.first));
+      if (fa.maxDynamicSharedSizeBytes < static_cast<int>(fs.second))
+        SF2D_CUDA(cudaFuncSetAttribute(fs.first, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(fs.second)));
+    }
   }
 
   // ---- solid side: receivers into the run's list, coupling entries per tile
@@ -356,16 +518,34 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
       }
     std::vector<std::vector<int>> by_t(S->T.ntiles);
     for (int k = 0; k < cp->ncpl_el; ++k) by_t[eg_tile[cp->cpl_el_point[k]]].push_back(k);
-    std::vector<int> e_local, e_src;
+    std::vector<int> e_local, e_src, e_pt;
     std::vector<float4> e_nw;
+    std::vector<double> e_coef;
     for (int t = 0; t < S->T.ntiles; ++t) {
       et[t].cpl_off = static_cast<int>(e_local.size());
       for (int k : by_t[t]) {
         e_local.push_back(S->T.local_id(t, cp->cpl_el_point[k]));
         e_src.push_back(T.glob2dev[cp->cpl_el_ac_point[k]]);
         e_nw.push_back(make_float4(cp->cpl_el_nx[k], cp->cpl_el_nz[k], cp->cpl_el_w[k], 0.f));
+        const int q = pml_ac ? cp->cpl_el_ac_elpt[k] : -1;
+        const int region = q >= 0 ? ad->pml_region[q / NGLL2] : 0;
+        if (region <= 0) continue;
+        // fluid element in the layer: coefficients of l_parameter_computation
+        // (compute_coupling_viscoelastic_ac.f90:105-123), pole alpha_x
+        const PmlAt c = pml_at(ad, static_cast<size_t>(q));
+        const PmlL L = pml_l(c.kx, c.bx, c.ax, c.kz, c.bz, c.az, region);
+        const PmlConv cv = pml_conv(c.ax, ad->pml_dt);
+        e_pt.push_back(e_src.back());
+        e_src.back() = ~static_cast<int>(e_pt.size() - 1);
+        for (double x : {L.A0, L.A1, L.A2, L.A3, cv.c0, cv.c1, cv.c2, c.ax}) e_coef.push_back(x);
       }
       et[t].cpl_n = static_cast<int>(e_local.size()) - et[t].cpl_off;
+    }
+    if (pml_ac || pml_el) {
+      if ((rc = C->upload_cpl(C->cpl_solid, e_pt, e_coef, 1))) return rc;
+      S->P.cpl_pml_p = C->cpl_solid.out;
+      if (C->cpl_solid.n > 0 && !C->lddrk && !A.pold)
+        return fail(SF2D_ERR_INVALID, "CPML coupling entries without a fluid CPML layer");
     }
     SF2D_CUDA(cudaMemcpy(const_cast<TileInfo *>(S->P.tiles), et.data(), sizeof(TileInfo) * et.size(),
                          cudaMemcpyHostToDevice));
@@ -379,11 +559,9 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
   return SF2D_OK;
 }
 
-extern "C" int sf2d_coupled_run(sf2d_coupled *C, int nstep, double *seismograms) {
+extern "C" int sf2d_coupled_enqueue(sf2d_coupled *C, int nstep) {
   using namespace sf2d;
   if (!C || nstep < 0) return fail(SF2D_ERR_INVALID, "bad arguments");
-  const int it0 = C->steps_done;
-  if (seismograms && it0 + nstep > C->nstep) return fail(SF2D_ERR_INVALID, "run exceeds the seismogram buffer length");
   sf2d_solver *S = C->el;
   const int K = C->chunk;
   int done = 0;
@@ -406,11 +584,28 @@ extern "C" int sf2d_coupled_run(sf2d_coupled *C, int nstep, double *seismograms)
     if (int rc = C->launch_chunk(nstep - done)) return rc;
   C->steps_done += nstep;
   S->steps_done += nstep;
+  return SF2D_OK;
+}
+
+extern "C" int sf2d_coupled_synchronize(sf2d_coupled *C) {
+  using namespace sf2d;
+  if (!C) return fail(SF2D_ERR_INVALID, "null solver");
+  sf2d_solver *S = C->el;
   SF2D_CUDA(cudaStreamSynchronize(S->stream));
   int status[2] = {0, 0};
   SF2D_CUDA(cudaMemcpy(&status[0], S->P.d_status, sizeof(int), cudaMemcpyDeviceToHost));
   SF2D_CUDA(cudaMemcpy(&status[1], C->A.d_status, sizeof(int), cudaMemcpyDeviceToHost));
   if (status[0] || status[1]) return fail(SF2D_ERR_UNSTABLE, "wavefield blew up (NaN or |field| > 1e25)");
+  return SF2D_OK;
+}
+
+extern "C" int sf2d_coupled_run(sf2d_coupled *C, int nstep, double *seismograms) {
+  using namespace sf2d;
+  if (!C || nstep < 0) return fail(SF2D_ERR_INVALID, "bad arguments");
+  const int it0 = C->steps_done;
+  if (seismograms && it0 + nstep > C->nstep) return fail(SF2D_ERR_INVALID, "run exceeds the seismogram buffer length");
+  if (int rc = sf2d_coupled_enqueue(C, nstep)) return rc;
+  if (int rc = sf2d_coupled_synchronize(C)) return rc;
   if (seismograms && C->nrec_total && nstep) {
     SF2D_CUDA(cudaMemcpy2D(seismograms, sizeof(double) * 2 * nstep, C->seis + static_cast<size_t>(it0) * 2,
                            sizeof(double) * 2 * C->nstep, sizeof(double) * 2 * nstep, C->nrec_total,
@@ -471,10 +666,12 @@ extern "C" int sf2d_coupled_time_kernels(sf2d_coupled *C, int nstep, float *ms) 
     for (int st = 0; st < C->nstage; ++st) {
       const bool rp = k > 0 && st == 0;
       SF2D_CUDA(cudaEventRecord(ev[0], S->stream));
+      C->launch_cpl_fluid(st);
       C->launch_ac_tile(rp, st);
       SF2D_CUDA(cudaEventRecord(ev[1], S->stream));
       C->launch_ac_shared(st);
       SF2D_CUDA(cudaEventRecord(ev[2], S->stream));
+      C->launch_cpl_solid(st);
       S->launch_tile(rp, st);
       SF2D_CUDA(cudaEventRecord(ev[3], S->stream));
       S->launch_shared(st);
@@ -508,6 +705,30 @@ extern "C" int sf2d_coupled_layout_info(sf2d_coupled *C, long long *info) {
   info[3] = static_cast<long long>(C->smem);
   info[4] = C->T.nglob - C->T.nshared;
   info[5] = static_cast<long long>(C->T.sh_ids.size());
+  return SF2D_OK;
+}
+
+extern "C" int sf2d_coupled_solid_layout_info(sf2d_coupled *C, long long *info8) {
+  using namespace sf2d;
+  if (!C) return fail(SF2D_ERR_INVALID, "null solver");
+  return sf2d_layout_info(C->el, info8);
+}
+
+extern "C" int sf2d_coupled_launch_count(sf2d_coupled *C, int nstep, long long *launches) {
+  using namespace sf2d;
+  if (!C || !launches || nstep < 0) return fail(SF2D_ERR_INVALID, "bad arguments");
+  const sf2d_solver *S = C->el;
+  const long long per_stage = (C->cpl_fluid.n > 0) + (C->pml_tile0 > 0) + (C->pml_tile0 < C->T.ntiles) + 1 +
+                              (C->cpl_solid.n > 0) + (S->pml_tile0 > 0) + (S->pml_tile0 < S->T.ntiles) + 1;
+  const long long chunks = nstep / C->chunk + (nstep % C->chunk ? 1 : 0);
+  *launches = per_stage * C->nstage * nstep + ((S->nrec > 0) + (C->A.nrec > 0)) * chunks;
+  return SF2D_OK;
+}
+
+extern "C" int sf2d_coupled_get_stream(sf2d_coupled *C, void **stream) {
+  using namespace sf2d;
+  if (!C || !stream) return fail(SF2D_ERR_INVALID, "bad arguments");
+  *stream = static_cast<void *>(C->el->stream);
   return SF2D_OK;
 }
 

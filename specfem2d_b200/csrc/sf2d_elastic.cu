@@ -64,11 +64,34 @@ int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solv
     return fail(SF2D_ERR_INVALID, "missing Newmark attenuation coefficients");
   if (atten && lddrk && (!d->att_phi1 || !d->att_itau2 || !d->att_phi2))
     return fail(SF2D_ERR_INVALID, "missing LDDRK attenuation coefficients");
+  const bool pml = d->pml_region != nullptr;
+  std::vector<int> group;
+  if (pml) {
+    if (!d->pml_K_x || !d->pml_K_z || !d->pml_d_x || !d->pml_d_z || !d->pml_alpha_x || !d->pml_alpha_z ||
+        !d->rhostore || !d->jacobian || !(d->pml_dt > 0.0))
+      return fail(SF2D_ERR_INVALID, "missing CPML arrays");
+    if (kern) return fail(SF2D_ERR_INVALID, "CPML layers are not part of the adjoint sweep");
+    if (d->nstacey > 0) return fail(SF2D_ERR_INVALID, "CPML layers and Stacey conditions exclude each other");
+    if (atten) return fail(SF2D_ERR_INVALID, "CPML layers need a non-attenuating medium");
+    if (d->npml_edge < 0 || (d->npml_edge > 0 && !d->pml_edge_iglob))
+      return fail(SF2D_ERR_INVALID, "bad CPML edge list");
+    for (int k = 0; k < d->npml_edge; ++k)
+      if (d->pml_edge_iglob[k] < 0 || d->pml_edge_iglob[k] >= d->nglob)
+        return fail(SF2D_ERR_INVALID, "CPML edge point out of range");
+    group.assign(d->nspec, 0);
+    for (int e = 0; e < d->nspec; ++e) {
+      const int r = d->pml_region[e];
+      if (r < 0 || r > 3) return fail(SF2D_ERR_INVALID, "CPML region must be 0 to 3");
+      if (r > 0 && aniso && d->ispec_is_anisotropic[e]) return fail(SF2D_ERR_INVALID, "anisotropic element in a CPML layer");
+      group[e] = r > 0 ? 1 : 0;
+    }
+  }
 
   auto *S = new sf2d_solver();
   std::unique_ptr<sf2d_solver> guard(S);
   const int te = d->tile_elems > 0 ? d->tile_elems : 64;
-  std::string err = build_tiling(d->nspec, d->nglob, d->ibool, d->centroid_xz, te, S->T);
+  std::string err = build_tiling(d->nspec, d->nglob, d->ibool, d->centroid_xz, te, S->T,
+                                 pml ? group.data() : nullptr, pml ? 2 : 1);
   if (!err.empty()) return fail(SF2D_ERR_INVALID, "tiling: " + err);
   const Tiling &T = S->T;
   for (int k = 0; k < d->nsrc; ++k)
@@ -172,6 +195,40 @@ int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solv
     }
     tiles[t].rec_n = static_cast<int>(rec_id.size()) - tiles[t].rec_off;
   }
+  // CPML layer: element slots [pml_slot0, nspec) (the last tiles), per-point
+  // damping data, the outer edge as per-tile local lists and a shared-point mask
+  S->pml_tile0 = pml ? T.group_tile_begin[1] : T.ntiles;
+  const int pml_slot0 = S->pml_tile0 < T.ntiles ? T.tiles[S->pml_tile0].elem_base : d->nspec;
+  std::vector<int> pml_region_s, edge_local;
+  std::vector<double2> pml_coef;
+  std::vector<float> pml_rhoj;
+  std::vector<uint8_t> sh_edge;
+  if (pml) {
+    for (int s = pml_slot0; s < d->nspec; ++s) {
+      const int e = T.elem_order[s];
+      pml_region_s.push_back(d->pml_region[e]);
+      for (int q = 0; q < NGLL2; ++q) {
+        const size_t p = static_cast<size_t>(e) * NGLL2 + q;
+        const double kx = d->pml_K_x[p], kz = d->pml_K_z[p], ax = d->pml_alpha_x[p], az = d->pml_alpha_z[p];
+        // beta = alpha + d / K (pml_compute_memory_variables.f90:164-165)
+        pml_coef.push_back(make_double2(kx, kz));
+        pml_coef.push_back(make_double2(ax, az));
+        pml_coef.push_back(make_double2(ax + d->pml_d_x[p] / kx, az + d->pml_d_z[p] / kz));
+        pml_rhoj.push_back(d->rhostore[p] * d->jacobian[p]);
+      }
+    }
+    std::vector<uint8_t> on_edge(d->nglob, 0);
+    for (int k = 0; k < d->npml_edge; ++k) on_edge[d->pml_edge_iglob[k]] = 1;
+    for (int t = 0; t < T.ntiles; ++t) {
+      tiles[t].edge_off = static_cast<int>(edge_local.size());
+      for (const auto &gl : T.tile_glob_local[t])
+        if (on_edge[gl.first]) edge_local.push_back(gl.second);
+      tiles[t].edge_n = static_cast<int>(edge_local.size()) - tiles[t].edge_off;
+    }
+    sh_edge.assign(std::max(T.nshared, 1), 0);
+    for (int s = 0; s < T.nshared; ++s) sh_edge[s] = on_edge[T.dev2glob[T.shared_begin + s]];
+  }
+  S->npml_q = static_cast<size_t>(d->nspec - pml_slot0) * NGLL2;
 
   SF2D_CUDA(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
   Params &P = S->P;
@@ -236,6 +293,26 @@ int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solv
       P.alpha[k] = d->alpha_lddrk[k];
       P.beta[k] = d->beta_lddrk[k];
     }
+  }
+  if (pml) {
+    UP(pml_region, int, pml_region_s);
+    UP(pml_coef, double2, pml_coef);
+    UP(pml_rhoj, float, pml_rhoj);
+    UP(edge_local, int, edge_local);
+    UP(sh_edge, uint8_t, sh_edge);
+    float4 *rm = nullptr;
+    if ((rc = S->alloc(&rm, S->npml_q * 3))) return rc;
+    SF2D_CUDA(cudaMemset(rm, 0, sizeof(float4) * std::max<size_t>(1, S->npml_q * 3)));
+    P.pml_rm = rm;
+    if (lddrk) {
+      float4 *rml = nullptr;
+      if ((rc = S->alloc(&rml, S->npml_q * 3))) return rc;
+      SF2D_CUDA(cudaMemset(rml, 0, sizeof(float4) * std::max<size_t>(1, S->npml_q * 3)));
+      P.pml_rm_l = rml;
+    }
+    P.pml_slot0 = pml_slot0;
+    P.DT = d->pml_dt;
+    P.h_old = static_cast<double>(d->deltatsquareover2) / 2.0;
   }
 #undef UP
   float2 *partial;
@@ -309,6 +386,11 @@ int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solv
       if (t.rec_n > S->nt) return fail(SF2D_ERR_INVALID, "more receivers in one tile than threads per CTA");
   }
   S->tile_fn = pick_tile_kernel(S->nt, aniso, atten, lddrk, kern);
+  if (pml) {
+    S->pml_fn = pick_pml_kernel(S->nt, lddrk);
+    S->pml_smem = tile_smem_layout(P.max_q, P.max_local, false, true).total;
+    if (S->pml_smem > 220 * 1024) return fail(SF2D_ERR_INVALID, "tile too large for shared memory");
+  }
   S->lddrk = lddrk;
   S->nstage = nstage;
   {
@@ -317,11 +399,15 @@ int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solv
     // make the launches of an earlier one with larger tiles fail.
     static std::mutex attr_mutex;
     std::lock_guard<std::mutex> lock(attr_mutex);
-    cudaFuncAttributes fa;
-    SF2D_CUDA(cudaFuncGetAttributes(&fa, S->tile_fn));
-    if (fa.maxDynamicSharedSizeBytes < static_cast<int>(S->smem))
-      SF2D_CUDA(cudaFuncSetAttribute(S->tile_fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(S->smem)));
+    const std::pair<TileKernel, size_t> fns[2] = {{S->tile_fn, S->smem}, {S->pml_fn, S->pml_smem}};
+    for (const auto &fs : fns) {
+      if (!fs.first) continue;
+      cudaFuncAttributes fa;
+      SF2D_CUDA(cudaFuncGetAttributes(&fa, fs.first));
+      if (fa.maxDynamicSharedSizeBytes < static_cast<int>(fs.second))
+        SF2D_CUDA(cudaFuncSetAttribute(fs.first, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(fs.second)));
+    }
   }
   S->nglob = d->nglob;
   S->nrec = d->nrec;
@@ -507,7 +593,15 @@ extern "C" int sf2d_layout_info(sf2d_solver *S, long long *info) {
   info[4] = static_cast<long long>(S->dev_bytes);
   info[5] = static_cast<long long>(S->smem);
   info[6] = S->nt;
-  info[7] = 0;
+  info[7] = static_cast<long long>(S->T.sh_ids.size());
+  return SF2D_OK;
+}
+
+extern "C" int sf2d_launch_count(sf2d_solver *S, int nstep, long long *launches) {
+  if (!S || !launches || nstep < 0) return fail(SF2D_ERR_INVALID, "bad arguments");
+  const long long per_stage = (S->pml_tile0 > 0) + (S->pml_tile0 < S->T.ntiles) + 1;
+  const long long chunks = nstep / S->chunk + (nstep % S->chunk ? 1 : 0);
+  *launches = per_stage * S->nstage * nstep + (S->nrec > 0 ? chunks : 0);
   return SF2D_OK;
 }
 
@@ -530,6 +624,8 @@ int sf2d_reset_solver(sf2d_solver *S) {
   if (P.att_state_l) SF2D_CUDA(cudaMemsetAsync(P.att_state_l, 0, sizeof(float4) * S->nq * 3, S->stream));
   if (P.kmu_kl) SF2D_CUDA(cudaMemsetAsync(P.kmu_kl, 0, sizeof(float2) * S->nq, S->stream));
   if (P.rho_kl_glob) SF2D_CUDA(cudaMemsetAsync(P.rho_kl_glob, 0, sizeof(float) * ng, S->stream));
+  if (P.pml_rm) SF2D_CUDA(cudaMemsetAsync(P.pml_rm, 0, sizeof(float4) * S->npml_q * 3, S->stream));
+  if (P.pml_rm_l) SF2D_CUDA(cudaMemsetAsync(P.pml_rm_l, 0, sizeof(float4) * S->npml_q * 3, S->stream));
   if (S->nrec && S->nstep_total)
     SF2D_CUDA(cudaMemsetAsync(P.seis, 0, sizeof(double) * S->nrec * S->nstep_total * 2, S->stream));
   SF2D_CUDA(cudaMemsetAsync(S->ctr, 0, 3 * sizeof(int), S->stream));

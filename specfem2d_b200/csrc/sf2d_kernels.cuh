@@ -31,6 +31,7 @@
 
 #include <cstdint>
 
+#include "sf2d_pml.cuh"
 #include "sf2d_tiler.h"
 
 namespace sf2d {
@@ -76,6 +77,21 @@ struct Params {
   const int *cpl_local, *cpl_src;
   const float4 *cpl_nw;
   const float *pdd_ac;    // chi_dot_dot of the fluid, fluid device order
+  // CPML: elements of slots >= pml_slot0 lie in the layer, "PML points" are
+  // their GLL points in slot order (index (slot - pml_slot0) * 25 + q)
+  int pml_slot0;
+  const int *pml_region;  // per PML element: CPML_X_ONLY, CPML_Z_ONLY or CPML_XZ
+  const double2 *pml_coef;  // 3 per PML point: (K_x, K_z), (alpha_x, alpha_z), (beta_x, beta_z)
+  const float *pml_rhoj;  // rho * jacobian per PML point
+  float4 *pml_rm;         // 3 per PML point: strain memory zx (dux_dx 1,2, duz_dx 1,2), xz (dux_dz, duz_dz),
+                          // displacement memory (x 1, z 1, x 2, z 2)
+  float4 *pml_rm_l;       // LDDRK copies
+  const int *edge_local;  // per tile (edge_off, edge_n): local points on the layer's outer edge
+  const uint8_t *sh_edge; // per shared point: 1 on the outer edge
+  double DT, h_old;       // DT, and deltatsquareover2 / 2 for the mid-step field
+  // solid-side coupling entries whose fluid element lies in a CPML layer have
+  // cpl_src = ~k: their pressure is formed before this kernel (k_cpl_pml_solid)
+  const float *cpl_pml_p; // per layer entry k: the pressure to apply
   int nstep_stf, nstage, nstep_seis, seismotype, nrec;
   double cosrot, sinrot;
   float dt, dto2, dt2o2;
@@ -135,11 +151,14 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 //   u, v, acc float2[max_local]  (old u, v, a -> predicted u, v and the accumulator)
 //   h    float[64]      hprime, hprimewgll, wxgll, wzgll
 //   lib  uint16[max_q rounded up to 8]
+//   b    float2[max_local]  forward frame (adjoint sweep with kernels)
+//   uold float2[max_local], pml float2[max_q]  mid-step displacement and the
+//        layer's acceleration terms (CPML tiles)
 struct TileSmem {
-  size_t geo, mat, u, v, acc, h, lib, b, total;
+  size_t geo, mat, u, v, acc, h, lib, b, uold, pml, total;
 };
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~static_cast<size_t>(15); }
-__host__ __device__ inline TileSmem tile_smem_layout(int max_q, int max_local, bool kern = false) {
+__host__ __device__ inline TileSmem tile_smem_layout(int max_q, int max_local, bool kern = false, bool pml = false) {
   TileSmem L;
   size_t o = 0;
   L.geo = o;
@@ -158,6 +177,10 @@ __host__ __device__ inline TileSmem tile_smem_layout(int max_q, int max_local, b
   o = align16(o + static_cast<size_t>((max_q + 7) / 8 * 8) * sizeof(uint16_t));
   L.b = o;
   if (kern) o = align16(o + static_cast<size_t>(max_local) * sizeof(float2));
+  L.uold = o;
+  if (pml) o = align16(o + static_cast<size_t>(max_local) * sizeof(float2));
+  L.pml = o;
+  if (pml) o = align16(o + static_cast<size_t>(max_q) * sizeof(float2));
   L.total = o;
   return L;
 }
@@ -240,10 +263,16 @@ __device__ __forceinline__ void kernel_point(float dux_dxi, float duz_dxi, float
   muk = dux_dxl * bdux_dxl + duz_dzl * bduz_dzl + 2.f * dsxz * bdsxz - 1.f / 3.f * kap;
 }
 
-template <int NT, bool ANISO, bool ATTEN, bool LDDRK, bool KERN>
-__global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_prev, int stage) {
+// PML: the tiles of a CPML layer (isotropic, no attenuation, no kernels):
+// mid-step displacement u + dt^2/4 a of the tile's points, the layer's strain
+// and displacement memory variables, the modified non-symmetric stress and
+// the extra acceleration terms (pml_compute_memory_variables.f90:230-540,
+// pml_compute_accel_contribution.f90:187-333, compute_forces_viscoelastic.F90:600-675, 785-797).
+// Tiles [tile0, tile0 + gridDim.x) are advanced.
+template <int NT, bool ANISO, bool ATTEN, bool LDDRK, bool KERN, bool PML = false>
+__global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_prev, int stage, int tile0) {
   extern __shared__ __align__(16) unsigned char smem[];
-  const TileInfo &ti = P.tiles[blockIdx.x];
+  const TileInfo &ti = P.tiles[tile0 + blockIdx.x];
   const int tid = threadIdx.x;
   const int n_int = ti.n_int;
   const int n_sh = ti.n_sh;
@@ -251,8 +280,10 @@ __global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_
   const int nq = ti.nelem * 25;
   const int ebase = ti.elem_base * 25;
   const int int_begin = ti.int_begin;
-  const TileSmem L = tile_smem_layout(P.max_q, P.max_local, KERN);
+  const TileSmem L = tile_smem_layout(P.max_q, P.max_local, KERN, PML);
   float4 *s_geo = reinterpret_cast<float4 *>(smem + L.geo);
+  float2 *s_uold = reinterpret_cast<float2 *>(smem + L.uold);
+  float2 *s_pml = reinterpret_cast<float2 *>(smem + L.pml);
   float2 *s_b = reinterpret_cast<float2 *>(smem + L.b);
   float2 *s_mat = reinterpret_cast<float2 *>(smem + L.mat);
   float2 *s_u = reinterpret_cast<float2 *>(smem + L.u);
@@ -302,6 +333,10 @@ __global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_
     if (!LDDRK) {
       float2 u = s_u[l], v = s_v[l];
       const float2 a = s_acc[l];
+      // mid-step displacement of the layer's convolutions (update_displacement_Newmark.F90:374-380)
+      if (PML)
+        s_uold[l] = make_float2(static_cast<float>(static_cast<double>(u.x) + P.h_old * static_cast<double>(a.x)),
+                                static_cast<float>(static_cast<double>(u.y) + P.h_old * static_cast<double>(a.y)));
       u.x = newmark_displ(u.x, v.x, a.x, dt, dt2o2);
       u.y = newmark_displ(u.y, v.y, a.y, dt, dt2o2);
       v.x = newmark_veloc(v.x, a.x, dto2);
@@ -312,6 +347,19 @@ __global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_
     s_acc[l] = make_float2(0.f, 0.f);
   }
   __syncthreads();
+  // outer edge of a CPML layer: displacement, velocity, mid-step displacement
+  // and acceleration zeroed before the forces (pml_boundary_elastic,
+  // pml_compute.f90:545-574); the layer excludes Stacey terms, so the order
+  // against them does not matter
+  if (ti.edge_n > 0) {
+    for (int k = tid; k < ti.edge_n; k += NT) {
+      const int l = P.edge_local[ti.edge_off + k];
+      s_u[l] = make_float2(0.f, 0.f);
+      s_v[l] = make_float2(0.f, 0.f);
+      if (PML && !LDDRK) s_uold[l] = make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+  }
 
   // 3. boundary terms and sources in reference order, one thread (overlaps pass 1)
   if (tid == 0) {
@@ -333,7 +381,9 @@ __global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_
     for (int p = ti.cpl_off; p < ti.cpl_off + ti.cpl_n; ++p) {
       const int l = P.cpl_local[p];
       const float4 nw = P.cpl_nw[p];
-      const float pressure = -P.pdd_ac[P.cpl_src[p]];
+      // a negative source names the CPML entry ~src (its pressure formed by k_cpl_pml_solid)
+      const int ga = P.cpl_src[p];
+      const float pressure = ga >= 0 ? -P.pdd_ac[ga] : P.cpl_pml_p[~ga];
       float2 acc = s_acc[l];
       acc.x += nw.z * nw.x * pressure;
       acc.y += nw.z * nw.y * pressure;
@@ -403,6 +453,84 @@ __global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_
     const float mul = m2.y;
     const float lambdal = m2.x;
     const float lambdaplus2mu = lambdal + 2.f * mul;
+    if (PML) {
+      const int ps = ebase + f - 25 * P.pml_slot0;
+      const int region = P.pml_region[ti.elem_base + e - P.pml_slot0];
+      const PmlPoint c = pml_point(P.pml_coef, ps);
+      // strains of the mid-step displacement
+      float o_dux_dxl = 0.f, o_dux_dzl = 0.f, o_duz_dxl = 0.f, o_duz_dzl = 0.f;
+      if (!LDDRK) {
+        float ox_xi = 0.f, oz_xi = 0.f, ox_g = 0.f, oz_g = 0.f;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+          const float2 r = s_uold[le[5 * j + k]];
+          const float hx = s_h[5 * i + k];
+          ox_xi += r.x * hx;
+          oz_xi += r.y * hx;
+          const float2 cc = s_uold[le[5 * k + i]];
+          const float hz = s_h[5 * j + k];
+          ox_g += cc.x * hz;
+          oz_g += cc.y * hz;
+        }
+        o_dux_dxl = ox_xi * xixl + ox_g * gammaxl;
+        o_dux_dzl = ox_xi * xizl + ox_g * gammazl;
+        o_duz_dxl = oz_xi * xixl + oz_g * gammaxl;
+        o_duz_dzl = oz_xi * xizl + oz_g * gammazl;
+      }
+      const PmlConv cax = pml_conv(c.ax, P.DT), caz = pml_conv(c.az, P.DT);
+      const PmlConv cbx = pml_conv(c.bx, P.DT), cbz = pml_conv(c.bz, P.DT);
+      const PmlLik zx = pml_lik(c.kz, c.bz, c.az, c.kx, c.bx, c.ax, region, false);  // poles alpha_z, beta_x
+      const PmlLik xz = pml_lik(c.kx, c.bx, c.ax, c.kz, c.bz, c.az, region, true);   // poles alpha_x, beta_z
+      float4 r0 = P.pml_rm[3 * ps], r1 = P.pml_rm[3 * ps + 1], rd = P.pml_rm[3 * ps + 2];
+      float4 l0 = make_float4(0.f, 0.f, 0.f, 0.f), l1 = l0, ld = l0;
+      if (LDDRK) {
+        l0 = P.pml_rm_l[3 * ps];
+        l1 = P.pml_rm_l[3 * ps + 1];
+        ld = P.pml_rm_l[3 * ps + 2];
+      }
+      const float al = P.alpha[stage], be = P.beta[stage];
+      pml_update<LDDRK>(r0.x, l0.x, caz, c.az, dux_dxl, o_dux_dxl, al, be, dt);
+      pml_update<LDDRK>(r0.y, l0.y, cbx, c.bx, dux_dxl, o_dux_dxl, al, be, dt);
+      pml_update<LDDRK>(r0.z, l0.z, caz, c.az, duz_dxl, o_duz_dxl, al, be, dt);
+      pml_update<LDDRK>(r0.w, l0.w, cbx, c.bx, duz_dxl, o_duz_dxl, al, be, dt);
+      pml_update<LDDRK>(r1.x, l1.x, cax, c.ax, dux_dzl, o_dux_dzl, al, be, dt);
+      pml_update<LDDRK>(r1.y, l1.y, cbz, c.bz, dux_dzl, o_dux_dzl, al, be, dt);
+      pml_update<LDDRK>(r1.z, l1.z, cax, c.ax, duz_dzl, o_duz_dzl, al, be, dt);
+      pml_update<LDDRK>(r1.w, l1.w, cbz, c.bz, duz_dzl, o_duz_dzl, al, be, dt);
+      const float m_dux_dxl = static_cast<float>(zx.A0 * dux_dxl + zx.A1 * r0.x + zx.A2 * r0.y);
+      const float m_duz_dxl = static_cast<float>(zx.A0 * duz_dxl + zx.A1 * r0.z + zx.A2 * r0.w);
+      const float m_dux_dzl = static_cast<float>(xz.A0 * dux_dzl + xz.A1 * r1.x + xz.A2 * r1.y);
+      const float m_duz_dzl = static_cast<float>(xz.A0 * duz_dzl + xz.A1 * r1.z + xz.A2 * r1.w);
+      // the layer's acceleration terms at this point (pml_compute_accel_contribution.f90:187-333)
+      const PmlL Lc = pml_l(c.kx, c.bx, c.ax, c.kz, c.bz, c.az, region);  // poles alpha_x, alpha_z
+      const int lq = le[q];
+      const float2 uq = s_u[lq], vq = s_v[lq];
+      const float2 uo = LDDRK ? make_float2(0.f, 0.f) : s_uold[lq];
+      pml_update<LDDRK>(rd.x, ld.x, cax, c.ax, uq.x, uo.x, al, be, dt);
+      pml_update<LDDRK>(rd.y, ld.y, cax, c.ax, uq.y, uo.y, al, be, dt);
+      pml_update<LDDRK>(rd.z, ld.z, caz, c.az, uq.x, uo.x, al, be, dt);
+      pml_update<LDDRK>(rd.w, ld.w, caz, c.az, uq.y, uo.y, al, be, dt);
+      const double wwf = static_cast<double>(s_h[50 + i] * s_h[55 + j] * P.pml_rhoj[ps]);
+      s_pml[f] = make_float2(
+          static_cast<float>(wwf * (Lc.A1 * vq.x + Lc.A2 * uq.x + Lc.A3 * rd.x + Lc.A4 * rd.z)),
+          static_cast<float>(wwf * (Lc.A1 * vq.y + Lc.A2 * uq.y + Lc.A3 * rd.y + Lc.A4 * rd.w)));
+      P.pml_rm[3 * ps] = r0;
+      P.pml_rm[3 * ps + 1] = r1;
+      P.pml_rm[3 * ps + 2] = rd;
+      if (LDDRK) {
+        P.pml_rm_l[3 * ps] = l0;
+        P.pml_rm_l[3 * ps + 1] = l1;
+        P.pml_rm_l[3 * ps + 2] = ld;
+      }
+      // modified strains on the diagonal pairs: the stress is not symmetric
+      const float sxx = lambdaplus2mu * m_dux_dxl + lambdal * duz_dzl;
+      const float szz = lambdaplus2mu * m_duz_dzl + lambdal * dux_dxl;
+      const float szx = mul * (duz_dxl + m_dux_dzl);
+      const float sxz = mul * (dux_dzl + m_duz_dxl);
+      s_geo[f] = make_float4(jacobianl * (sxx * xixl + szx * xizl), jacobianl * (sxz * xixl + szz * xizl),
+                             jacobianl * (sxx * gammaxl + szx * gammazl), jacobianl * (sxz * gammaxl + szz * gammazl));
+      continue;
+    }
     float sxx, szz, sxz;
     int ai = -1;
     if (ANISO) ai = P.aniso_idx[ti.elem_base + e];
@@ -462,6 +590,12 @@ __global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_
       float2 acc = s_acc[l];
       acc.x -= wz * tx1 + wx * tx2;
       acc.y -= wz * tz1 + wx * tz2;
+      if (PML) {
+        // the layer's terms after the element's weak-form terms (compute_forces_viscoelastic.F90:785-797)
+        const float2 pm = s_pml[f];
+        acc.x -= pm.x;
+        acc.y -= pm.y;
+      }
       s_acc[l] = acc;
     }
     cb = ce;
@@ -527,6 +661,10 @@ __global__ void __launch_bounds__(SHARED_NT) k_elastic_shared(const Params P, in
       u.y = newmark_displ(u.y, v.y, a0.y, P.dt, P.dt2o2);
       v.x = newmark_veloc(v.x, a0.x, P.dto2);
       v.y = newmark_veloc(v.y, a0.y, P.dto2);
+    }
+    if (P.sh_edge && P.sh_edge[s]) {  // outer edge of a CPML layer
+      u = make_float2(0.f, 0.f);
+      v = make_float2(0.f, 0.f);
     }
     float2 acc = make_float2(0.f, 0.f);
     for (int k = P.shp_off[s]; k < P.shp_off[s + 1]; ++k) {

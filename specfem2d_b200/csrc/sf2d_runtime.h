@@ -29,7 +29,7 @@ using sf2d::fail;
 
 namespace sf2d {
 
-using TileKernel = void (*)(Params, int, int);
+using TileKernel = void (*)(Params, int, int, int);
 
 template <int NT, bool KERN>
 TileKernel pick_tile_kernel(bool aniso, bool atten, bool lddrk) {
@@ -39,6 +39,15 @@ TileKernel pick_tile_kernel(bool aniso, bool atten, bool lddrk) {
   }
   if (atten) return lddrk ? k_elastic_tile<NT, false, true, true, KERN> : k_elastic_tile<NT, false, true, false, KERN>;
   return lddrk ? k_elastic_tile<NT, false, false, true, KERN> : k_elastic_tile<NT, false, false, false, KERN>;
+}
+
+// the kernel of a CPML layer's tiles (isotropic, no attenuation, forward)
+inline TileKernel pick_pml_kernel(int nt, bool lddrk) {
+  switch (nt) {
+    case 128: return lddrk ? k_elastic_tile<128, false, false, true, false, true> : k_elastic_tile<128, false, false, false, false, true>;
+    case 512: return lddrk ? k_elastic_tile<512, false, false, true, false, true> : k_elastic_tile<512, false, false, false, false, true>;
+    default: return lddrk ? k_elastic_tile<256, false, false, true, false, true> : k_elastic_tile<256, false, false, false, false, true>;
+  }
 }
 
 inline TileKernel pick_tile_kernel(int nt, bool aniso, bool atten, bool lddrk, bool kern) {
@@ -86,8 +95,12 @@ struct sf2d_solver {
     if (count) SF2D_CUDA(cudaMemcpy(*p, host, count * sizeof(T_), cudaMemcpyHostToDevice));
     return SF2D_OK;
   }
-  using TileFn = void (*)(sf2d::Params, int, int);
+  using TileFn = void (*)(sf2d::Params, int, int, int);
   TileFn tile_fn = nullptr;
+  TileFn pml_fn = nullptr;   // tiles [pml_tile0, ntiles) hold the CPML layer's elements
+  int pml_tile0 = 0;
+  size_t pml_smem = 0;
+  size_t npml_q = 0;         // GLL points of the layer's elements
   bool lddrk = false;
   bool kern = false;
   bool atten = false;
@@ -98,7 +111,10 @@ struct sf2d_solver {
   size_t nq = 0;
 
   void launch_tile(bool record_prev, int stage) {
-    tile_fn<<<T.ntiles, nt, smem, stream>>>(P, record_prev ? 1 : 0, stage);
+    if (pml_tile0 > 0) tile_fn<<<pml_tile0, nt, smem, stream>>>(P, record_prev ? 1 : 0, stage, 0);
+    if (pml_tile0 < T.ntiles)
+      (pml_fn ? pml_fn : tile_fn)<<<T.ntiles - pml_tile0, nt, pml_fn ? pml_smem : smem, stream>>>(
+          P, record_prev ? 1 : 0, stage, pml_tile0);
   }
   void launch_shared(int stage) {
     const int nb = std::max(1, (P.nshared + sf2d::SHARED_NT - 1) / sf2d::SHARED_NT);

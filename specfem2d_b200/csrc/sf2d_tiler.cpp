@@ -28,11 +28,16 @@ int Tiling::local_id(int tile, int glob) const {
 }
 
 std::string build_tiling(int nspec, int nglob, const int *ibool, const double *centroid_xz,
-                         int tile_elems, Tiling &T) {
+                         int tile_elems, Tiling &T, const int *elem_group, int ngroups) {
   if (nspec <= 0 || nglob <= 0 || !ibool) return "empty mesh";
   if (tile_elems < 1 || tile_elems > 256) return "tile_elems must be in [1, 256]";
+  if (ngroups < 1 || ngroups > 8) return "ngroups must be in [1, 8]";
   for (long long k = 0; k < static_cast<long long>(nspec) * NGLL2; ++k)
     if (ibool[k] < 0 || ibool[k] >= nglob) return "ibool entry out of range";
+  if (elem_group)
+    for (int e = 0; e < nspec; ++e)
+      if (elem_group[e] < 0 || elem_group[e] >= ngroups) return "element group out of range";
+  auto group = [&](int e) { return elem_group ? elem_group[e] : 0; };
 
   // 1. element order along a Morton curve of the centroids (uniform scale)
   std::vector<int> order(nspec);
@@ -54,22 +59,29 @@ std::string build_tiling(int nspec, int nglob, const int *ibool, const double *c
     }
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return code[a] < code[b]; });
   }
+  if (elem_group) std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return group(a) < group(b); });
 
-  // 2. chunk into tiles, elements ascending inside each tile
-  const int ntiles = (nspec + tile_elems - 1) / tile_elems;
+  // 2. chunk each group into tiles, elements ascending inside each tile
   T = Tiling();
+  std::vector<std::vector<int>> tel;
+  T.group_tile_begin.assign(ngroups + 1, 0);
+  for (int b = 0; b < nspec;) {
+    int e = b + 1;
+    while (e < nspec && e - b < tile_elems && group(order[e]) == group(order[b])) ++e;
+    tel.emplace_back(order.begin() + b, order.begin() + e);
+    std::sort(tel.back().begin(), tel.back().end());
+    T.group_tile_begin[group(order[b]) + 1] = static_cast<int>(tel.size());
+    b = e;
+  }
+  for (int k = 1; k <= ngroups; ++k) T.group_tile_begin[k] = std::max(T.group_tile_begin[k], T.group_tile_begin[k - 1]);
+  const int ntiles = static_cast<int>(tel.size());
   T.ntiles = ntiles;
   T.nglob = nglob;
   T.nelem = nspec;
   T.tiles.assign(ntiles, TileInfo{});
   T.elem_tile.assign(nspec, -1);
-  std::vector<std::vector<int>> tel(ntiles);
-  for (int t = 0; t < ntiles; ++t) {
-    const int b = t * tile_elems, e = std::min(nspec, b + tile_elems);
-    tel[t].assign(order.begin() + b, order.begin() + e);
-    std::sort(tel[t].begin(), tel[t].end());
+  for (int t = 0; t < ntiles; ++t)
     for (int x : tel[t]) T.elem_tile[x] = t;
-  }
 
   // 3. how many tiles touch each point
   std::vector<int> last(nglob, -1), touch(nglob, 0);

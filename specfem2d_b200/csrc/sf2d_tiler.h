@@ -35,8 +35,10 @@ struct TileInfo {
   int ncol;
   int lib_off;     // offset of the tile's local ibool (multiple of 8 entries = 16 bytes)
   int cpl_off, cpl_n;  // fluid-solid coupling entries of this tile (none outside a coupled run)
+  int edge_off, edge_n;  // local points on the outer edge of a CPML layer, zeroed every step
+  int pad_[2];
 };
-static_assert(sizeof(TileInfo) == 24 * 4, "TileInfo layout");
+static_assert(sizeof(TileInfo) == 28 * 4, "TileInfo layout");
 
 struct Tiling {
   int ntiles = 0;
@@ -58,13 +60,18 @@ struct Tiling {
   // global point id -> (tile, local id) lookup used when attaching boundary terms
   int local_id(int tile, int glob) const;
   std::vector<std::vector<std::pair<int, int>>> tile_glob_local;  // per tile sorted (glob, local)
+  // tiles of element group k are [group_tile_begin[k], group_tile_begin[k+1])
+  std::vector<int> group_tile_begin;
 };
 
 // Builds the tiling.  `ibool` is nspec*25 0-based ids in [ispec][j][i]
 // order; `centroid_xz` (nspec*2, may be null) orders elements along a Morton
 // curve so tiles are compact; without it elements keep their input order.
+// `elem_group` (nspec values in [0, ngroups), may be null) keeps elements of
+// different groups in different tiles, group 0 first: the elements of a CPML
+// layer get tiles (and a kernel variant) of their own.
 // Returns an empty string on success, else an error message.
 std::string build_tiling(int nspec, int nglob, const int *ibool, const double *centroid_xz,
-                         int tile_elems, Tiling &out);
+                         int tile_elems, Tiling &out, const int *elem_group = nullptr, int ngroups = 1);
 
 }  // namespace sf2d

@@ -57,6 +57,11 @@ class ElasticDesc(ctypes.Structure):
         ("c11", _f), ("c13", _f), ("c15", _f), ("c33", _f), ("c35", _f), ("c55", _f),
         ("att_a1", _f), ("att_b1", _f), ("att_a2", _f), ("att_b2", _f),
         ("att_itau1", _f), ("att_phi1", _f), ("att_itau2", _f), ("att_phi2", _f),
+        ("pml_region", _i),
+        ("pml_K_x", _d), ("pml_K_z", _d), ("pml_d_x", _d), ("pml_d_z", _d), ("pml_alpha_x", _d), ("pml_alpha_z", _d),
+        ("rhostore", _f), ("jacobian", _f),
+        ("npml_edge", ctypes.c_int), ("pml_edge_iglob", _i),
+        ("pml_dt", ctypes.c_double),
     ]
 
 
@@ -85,6 +90,7 @@ def load_library(path: str = LIB):
         "sf2d_get_stream": [vp, ctypes.POINTER(vp)],
         "sf2d_time_kernels": [vp, ctypes.c_int, _f],
         "sf2d_layout_info": [vp, ctypes.POINTER(ctypes.c_longlong)],
+        "sf2d_launch_count": [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)],
         "sf2d_destroy": [vp],
         "sf2d_fwi_create": [ctypes.POINTER(ElasticDesc), _f, _f, ctypes.c_int, ctypes.POINTER(vp)],
         "sf2d_fwi_forward": [vp, _d],
@@ -221,6 +227,15 @@ def build_desc(db, tile_elems: int = 32, seismotype: int = 1, threads_per_block:
         else:
             d.att_itau1, d.att_phi1 = f(at["itau1"]), f(at["phi1"])
             d.att_itau2, d.att_phi2 = f(at["itau2"]), f(at["phi2"])
+    pm = getattr(db, "pml", None)
+    if pm is not None:
+        d.pml_region = i(pm["region"])
+        d.pml_K_x, d.pml_K_z = dd(pm["K_x"]), dd(pm["K_z"])
+        d.pml_d_x, d.pml_d_z = dd(pm["d_x"]), dd(pm["d_z"])
+        d.pml_alpha_x, d.pml_alpha_z = dd(pm["alpha_x"]), dd(pm["alpha_z"])
+        d.rhostore, d.jacobian = f(db.rhostore), f(db.jacobian)
+        d.npml_edge, d.pml_edge_iglob = len(pm["bnd_el"]), i(pm["bnd_el"])
+        d.pml_dt = float(pm["dt"])
     return d, keep
 
 
@@ -302,5 +317,11 @@ class ElasticSolver:
         v = (ctypes.c_longlong * 8)()
         _check(self._lib.sf2d_layout_info(self._h, v))
         keys = ["ntiles", "nshared", "max_local", "max_elems", "device_bytes", "smem_bytes",
-                "threads_per_block", "reserved"]
+                "threads_per_block", "n_slots"]
         return dict(zip(keys, [int(x) for x in v]))
+
+    def launch_count(self, nstep: int) -> int:
+        """Kernel launches that enqueue(nstep) issues."""
+        n = ctypes.c_longlong()
+        _check(self._lib.sf2d_launch_count(self._h, nstep, ctypes.byref(n)))
+        return int(n.value)
