@@ -156,6 +156,32 @@ def time_oracle(db, max_steps: int, target_s: float = 15.0, nthreads: int = 0):
     return n, dt, threads
 
 
+def run_reference_fwi(args, rank):
+    """The CPU restatement's gradient (forward, checkpointed reverse sweep) on
+    the smallest model of the FWI workload, per shot."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # noqa: E402  (reference arm only)
+
+    models = fwi_members(args.models, args.fwi_steps)
+    db = min(models, key=lambda m: m.nspec)
+    t0 = time.perf_counter()
+    oracle.gradient(db, np.zeros((len(db.rec_ispec), db.nstep, 2)), checkpoint_every=100, precision=4)
+    dt = time.perf_counter() - t0
+    threads = oracle.max_threads()
+    line = {"metric": "s per FWI gradient per shot", "value": dt, "unit": "s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.fwi_steps, "warmup": 0, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "description": FWI_WORKLOADS[args.workload],
+                       "sample_nspec": db.nspec},
+            "cpu_baseline": {"value": dt, "unit": "s", "cores": threads, "kind": "port",
+                             "sample": f"one gradient of the smallest model ({db.nspec} elements, "
+                                       f"{db.nstep} steps), C++ restatement of the reference CPU solver"},
+            "e2e": {"value": dt, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
@@ -176,13 +202,98 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+FWI_WORKLOADS = {
+    "c5_fwi_models": ("misfit gradients of independent random-layered elastic models with uneven meshes "
+                      "(sizes drawn with seed 6 between 100x50 and 1200x500 elements, 3-6 layers, vp 2000-4500, "
+                      "one Ricker 8 Hz force, 20 surface receivers, dt 4e-4, Stacey on three sides); "
+                      "L2 misfit against zero data (adjoint source = the synthetics), checkpoint every 100 steps; "
+                      "batched = all models packed into one mesh and one launch per step, plain = one "
+                      "model per run"),
+}
+
+
+def fwi_members(n_models: int, nstep: int):
+    from specfem2d_b200 import configs
+
+    os.makedirs(CACHE, exist_ok=True)
+    path = os.path.join(CACHE, f"c5_models_{n_models}_{nstep}.pkl")
+    if os.path.exists(path):
+        with open(path, "rb") as f:
+            return pickle.load(f)
+    sizes = configs.c5_model_sizes()[:n_models]
+    models = [configs.random_layered_model(seed=100 + k, nx=nx, nz=nz, nstep=nstep) for k, (nx, nz) in
+              enumerate(sizes)]
+    with open(path, "wb") as f:
+        pickle.dump(models, f)
+    return models
+
+
+def run_fwi(args, rank, world):
+    """Seconds per misfit gradient per model: plain (one model per run) and
+    batched (all models in one packed mesh), both through sf2d_fwi_* with the
+    traces and kernels copied to the host."""
+    import torch
+
+    from specfem2d_b200 import batch
+    from specfem2d_b200.fwi import FWIGradient
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    models = fwi_members(args.models, args.fwi_steps)
+    every = 100
+    nq = sum(m.nspec for m in models)
+
+    def one(db):
+        g = FWIGradient(db, every, tile_elems=args.tile_elems, threads_per_block=args.threads)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        seis = g.forward()
+        kern = g.backward(seis)
+        t1 = time.perf_counter()
+        g.close()
+        return t1 - t0, kern
+
+    # warm-up on the smallest member (module load, graph instantiation)
+    one(min(models, key=lambda m: m.nspec))
+    plain_s, plain_k = 0.0, []
+    for m in models:
+        t, k = one(m)
+        plain_s += t
+        plain_k.append(k)
+    packed, idx = batch.pack(models)
+    batched_s, bk = one(packed)
+    # gradient agreement: packed kernels against the per-model ones
+    num = den = 0.0
+    for c in range(3):
+        for m, part in enumerate(batch.split_elements(bk[c], idx)):
+            ref = plain_k[m][c].astype(np.float64)
+            num += float(np.sum((part.astype(np.float64) - ref) ** 2))
+            den += float(np.sum(ref ** 2))
+    n = len(models)
+    line = {
+        "metric": "s per FWI gradient per shot", "value": batched_s / n, "unit": "s", "n_gpus": world,
+        "steps": args.fwi_steps, "warmup": 1, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "description": FWI_WORKLOADS[args.workload], "models": n,
+                   "nspec_total": nq, "nglob_total": int(packed.nglob), "checkpoint_every": every,
+                   "tile_elems": args.tile_elems, "threads_per_cta": args.threads},
+        "plain_s_per_shot": plain_s / n, "batched_s_per_shot": batched_s / n,
+        "speedup_batched_vs_plain": plain_s / batched_s,
+        "gradient_rel_l2_batched_vs_plain": (num / den) ** 0.5 if den > 0 else 0.0,
+        "point_updates_per_s_batched": 3.0 * packed.nglob * args.fwi_steps / batched_s,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=6000)
     ap.add_argument("--warmup", type=int, default=100)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2_coupled", choices=sorted(WORKLOAD_DESC))
+    ap.add_argument("--workload", default="c2_coupled", choices=sorted(WORKLOAD_DESC) + sorted(FWI_WORKLOADS))
+    ap.add_argument("--models", type=int, default=12, help="models of the FWI workload")
+    ap.add_argument("--fwi-steps", type=int, default=1000, help="time steps of each FWI model")
     ap.add_argument("--tile-elems", type=int, default=32)
     ap.add_argument("--threads", type=int, default=256)
     ap.add_argument("--autotune", action="store_true", help="pick tile size and threads per CTA first")
@@ -195,6 +306,12 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
 
+    if args.workload in FWI_WORKLOADS:
+        if args.impl == "reference":
+            run_reference_fwi(args, rank)
+        else:
+            run_fwi(args, rank, world)
+        return
     if args.impl == "reference":
         run_reference(args, rank)
         return

@@ -86,7 +86,8 @@ typedef struct {
   int nstep;                                 /* length of stf and of the seismogram buffer */
   float deltat, deltatover2, deltatsquareover2;
   int tile_elems;                            /* elements per tile, 0 = default (64) */
-  int threads_per_block;                     /* 128, 256 or 512; 0 = default (256) */
+  int threads_per_block;                     /* 128, 250, 256 or 512; 0 = default (256); 250 keeps
+                                                each thread on one GLL position of every element */
   /* time scheme: 1 (or 0) Newmark, 2 LDDRK with 6 stages (update_displacement_LDDRK.F90);
    * stf holds nstage values per step: stf[isrc][it][stage] */
   int time_scheme;

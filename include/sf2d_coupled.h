@@ -93,6 +93,11 @@ typedef struct {
   const int *cpl_ac_el_elpt, *cpl_el_ac_elpt;
 } sf2d_coupling_desc;
 
+/* A solid description with nspec = 0 makes a fluid-only run (no coupling entries,
+ * solid sources or solid receivers): only its time-stepping members (nstep,
+ * deltat, deltatover2, deltatsquareover2, time_scheme, nstage, alpha_lddrk,
+ * beta_lddrk, threads_per_block) and GLL arrays (hprime, hprimewgll, wxgll,
+ * wzgll) are read. */
 int sf2d_coupled_create(const sf2d_elastic_desc *solid, const sf2d_acoustic_desc *fluid,
                         const sf2d_coupling_desc *coupling, sf2d_coupled **out);
 /* Advances nstep steps (fluid then solid per step or LDDRK stage); seismograms

@@ -15,7 +15,7 @@ import ctypes
 
 import numpy as np
 
-from .runtime import _check, _d, _f, _i, build_desc, load_library
+from .runtime import _check, _d, _f, _i, build_desc, load_library, time_desc
 
 _vp = ctypes.c_void_p
 
@@ -88,6 +88,30 @@ def _submesh(db, elems):
     return pts, gmap, emap
 
 
+def _fluid_arrays(db, ac_e, src_ac, rec_ac, pml_keys):
+    """The fluid sub-mesh of the acoustic elements ac_e: its arrays (compact
+    point numbering), its global points, and the point and element maps."""
+    ac = db.acoustic
+    pm = getattr(db, "pml", None)
+    ga, amap, eamap = _submesh(db, ac_e)
+    fluid = dict(
+        nspec=len(ac_e), nglob=len(ga), ibool=amap[db.ibool[ac_e]].astype(np.int32),
+        xix=db.xix[ac_e], xiz=db.xiz[ac_e], gammax=db.gammax[ac_e], gammaz=db.gammaz[ac_e],
+        jacobian=db.jacobian[ac_e], rhostore=db.rhostore[ac_e], kappastore=db.kappastore[ac_e],
+        rmass=ac["rmass"][ga], centroid=db.coord[db.ibool[ac_e][:, [0, 0, 4, 4], [0, 4, 0, 4]]].mean(axis=1),
+        free=amap[ac["free_iglob"]].astype(np.int32),
+        st_iglob=amap[ac["st_iglob"]].astype(np.int32), st_w=ac["st_w"], st_rvp=ac["st_rvp"],
+        src_ispec=eamap[db.source_ispec[src_ac]].astype(np.int32),
+        sourcearrays=db.sourcearrays[src_ac][..., 0].astype(np.float32), stf=db.stf[src_ac],
+        rec_ispec=eamap[db.rec_ispec[rec_ac]].astype(np.int32), hxir=db.hxir[rec_ac], hgammar=db.hgammar[rec_ac],
+        rec_global=np.flatnonzero(rec_ac).astype(np.int32), pml=None)
+    if pm is not None:
+        bnd_ac = amap[np.asarray(pm["bnd_ac"], dtype=np.int64)]
+        fluid["pml"] = dict(region=np.asarray(pm["region"])[ac_e], bnd=bnd_ac[bnd_ac >= 0].astype(np.int32),
+                            dt=pm["dt"], **{k: pm[k][ac_e] for k in pml_keys})
+    return fluid, ga, amap, eamap
+
+
 def split(db):
     """Return (solid Database, fluid arrays dict, coupling arrays dict, index maps)."""
     ac = db.acoustic
@@ -96,12 +120,18 @@ def split(db):
     pm = getattr(db, "pml", None)
     is_ac = np.asarray(ac["ispec"], dtype=bool)
     el_e, ac_e = np.flatnonzero(~is_ac), np.flatnonzero(is_ac)
-    if len(el_e) == 0:
-        raise ValueError("a fluid-only mesh has no solid part to couple to")
-    gl, gmap, emap = _submesh(db, el_e)
-    ga, amap, eamap = _submesh(db, ac_e)
     src_ac = is_ac[db.source_ispec]
     rec_ac = is_ac[db.rec_ispec]
+    pml_keys = ("K_x", "K_z", "d_x", "d_z", "alpha_x", "alpha_z")
+    fluid, ga, amap, eamap = _fluid_arrays(db, ac_e, src_ac, rec_ac, pml_keys)
+    if len(el_e) == 0:
+        # fluid-only mesh: no solid sub-mesh, no coupling
+        e, ef = np.zeros(0, np.int32), np.zeros(0, np.float32)
+        cpl = dict(el_rec_global=e, ac_point=e, ac_el_point=e, ac_nx=ef, ac_nz=ef, ac_w=ef, el_point=e,
+                   el_ac_point=e, el_nx=ef, el_nz=ef, el_w=ef, use_trick=bool(ac.get("use_trick", False)),
+                   ac_el_elpt=None, el_ac_elpt=None)
+        return None, fluid, cpl, dict(solid_points=np.zeros(0, np.int64), fluid_points=ga)
+    gl, gmap, emap = _submesh(db, el_e)
 
     sub = copy.copy(db)
     sub.nspec, sub.nglob = len(el_e), len(gl)
@@ -127,27 +157,11 @@ def split(db):
         sub.aniso = {k: v[el_e] for k, v in db.aniso.items()}
     sub.acoustic = None
     sub.mesh = None
-    pml_keys = ("K_x", "K_z", "d_x", "d_z", "alpha_x", "alpha_z")
     if pm is not None:
         bnd_el = gmap[np.asarray(pm["bnd_el"], dtype=np.int64)]
         sub.pml = dict(region=np.asarray(pm["region"])[el_e], bnd_el=bnd_el[bnd_el >= 0].astype(np.int32),
                        bnd_ac=np.zeros(0, np.int32), dt=pm["dt"], **{k: pm[k][el_e] for k in pml_keys})
 
-    fluid = dict(
-        nspec=len(ac_e), nglob=len(ga), ibool=amap[db.ibool[ac_e]].astype(np.int32),
-        xix=db.xix[ac_e], xiz=db.xiz[ac_e], gammax=db.gammax[ac_e], gammaz=db.gammaz[ac_e],
-        jacobian=db.jacobian[ac_e], rhostore=db.rhostore[ac_e], kappastore=db.kappastore[ac_e],
-        rmass=ac["rmass"][ga], centroid=db.coord[db.ibool[ac_e][:, [0, 0, 4, 4], [0, 4, 0, 4]]].mean(axis=1),
-        free=amap[ac["free_iglob"]].astype(np.int32),
-        st_iglob=amap[ac["st_iglob"]].astype(np.int32), st_w=ac["st_w"], st_rvp=ac["st_rvp"],
-        src_ispec=eamap[db.source_ispec[src_ac]].astype(np.int32),
-        sourcearrays=db.sourcearrays[src_ac][..., 0].astype(np.float32), stf=db.stf[src_ac],
-        rec_ispec=eamap[db.rec_ispec[rec_ac]].astype(np.int32), hxir=db.hxir[rec_ac], hgammar=db.hgammar[rec_ac],
-        rec_global=np.flatnonzero(rec_ac).astype(np.int32), pml=None)
-    if pm is not None:
-        bnd_ac = amap[np.asarray(pm["bnd_ac"], dtype=np.int64)]
-        fluid["pml"] = dict(region=np.asarray(pm["region"])[ac_e], bnd=bnd_ac[bnd_ac >= 0].astype(np.int32),
-                            dt=pm["dt"], **{k: pm[k][ac_e] for k in pml_keys})
     cpl = dict(
         el_rec_global=np.flatnonzero(~rec_ac).astype(np.int32),
         ac_point=amap[ac["cpl_ac_iglob"]].astype(np.int32), ac_el_point=gmap[ac["cpl_ac_iglob"]].astype(np.int32),
@@ -173,7 +187,10 @@ class CoupledSolver:
         lib = _lib()
         sub, fl, cp, maps = split(db)
         seismotype = int(getattr(db, "seismotype", 1))
-        ed, keep = build_desc(sub, tile_elems, 1 if seismotype == 4 else seismotype, threads_per_block)
+        if sub is not None:
+            ed, keep = build_desc(sub, tile_elems, 1 if seismotype == 4 else seismotype, threads_per_block)
+        else:  # fluid-only mesh
+            ed, keep = time_desc(db, tile_elems, threads_per_block)
 
         def f(a):
             arr = np.ascontiguousarray(np.asarray(a, dtype=np.float32))

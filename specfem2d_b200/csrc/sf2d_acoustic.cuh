@@ -5,20 +5,23 @@
 // It uses the same tiling as the solid (sf2d_tiler.h) over the fluid
 // elements, with its own device numbering of the fluid points.  One CTA per
 // tile and time step (or LDDRK stage):
-//   1. cp.async of local ibool, geometry, J/rho and chi, chi_dot,
-//      chi_dot_dot of the tile's points into shared memory;
+//   1. cp.async of local ibool and chi, chi_dot, chi_dot_dot of the tile's
+//      points into shared memory (geometry and J/rho are read from global
+//      memory where they are used);
 //   2. Newmark predictor (update_displacement_Newmark.F90:353-402) or a
 //      cleared accumulator (LDDRK), free-surface points zeroed
 //      (enforce_acoustic_free_surface.f90:35-96);
-//   3. one thread, in reference order: Stacey chi_dd -= chi_d w / (rho vp)
+//   3. one thread per receiving point, in the reference's order at that
+//      point: Stacey chi_dd -= chi_d w / (rho vp)
 //      (compute_stacey_acoustic.f90:78-180), the solid's normal displacement
 //      chi_dd += w (u . n) (compute_coupling_acoustic_el.f90:60-283, with the
 //      solid's predicted displacement formed here from its u, v, a), the
 //      pressure sources chi_dd += s stf / kappa (compute_add_sources_acoustic.f90:49-75);
-//   4. per GLL point: gradient through hprime, mapping, J/rho weak-form terms
-//      (compute_forces_viscoacoustic.f90:105-238);
-//   5. weighted transpose contraction with hprimewgll assembled colour by
-//      colour (:306-322);
+//   4. derivative lines through hprime (one thread per element row or
+//      column), per GLL point the mapping and J/rho weak-form terms
+//      (compute_forces_viscoacoustic.f90:105-238), weighted transpose lines
+//      with hprimewgll (:306-322);
+//   5. assembly colour by colour;
 //   6. interior points: chi_dd *= rmass_inverse, corrector or LDDRK update
 //      (update_displacement_Newmark.F90:631-662, update_displacement_LDDRK.F90:88-115),
 //      free-surface zeroing, write-back; shared points: partial sums.
@@ -48,6 +51,8 @@ struct AcParams {
   const int *sh_ids;
   float *partial;
   const int *shp_off, *shp_slots;
+  const int4 *bgroups;        // per tile (grp_off, grp_n): point, first idx, Stacey | coupling << 8, sources
+  const int *bnd_idx;         // entries of each group
   const int *st_local;
   const float2 *st_wr;        // Stacey weight (jacobian1D * w), rho * vp
   // coupling (fluid side): tile-local point, solid device point, (nx, nz, w, 0)
@@ -74,8 +79,8 @@ struct AcParams {
   float hconst[60];           // hprime[25], hprimewgll[25], wxgll[5], wzgll[5]
   // CPML: elements of slots >= pml_slot0 lie in the layer (see Params)
   int pml_slot0;
-  const int *pml_region;
-  const double2 *pml_coef;    // 3 per PML point: (K_x, K_z), (alpha_x, alpha_z), (beta_x, beta_z)
+  const PmlSet *pml_sets;     // coefficient sets of the layer
+  const int *pml_set_idx;     // per PML point: its set
   const float *pml_jk;        // jacobian / kappa per PML point
   float2 *pml_rm;             // 3 per PML point: dchi_dx memory (1, 2), dchi_dz memory (1, 2), chi memory (1, 2)
   float2 *pml_rm_l;           // LDDRK copies
@@ -86,6 +91,35 @@ struct AcParams {
   const float2 *cpl_pml_u;    // per layer entry k: the displacement to apply
 };
 
+// Scalar line helpers of the fluid kernel (as line_derivs / line_weighted of
+// the solid kernel): out[m] = sum_k f_k hprime[m][k]; in place
+// t[m] = sum_k t_k hprimewgll[k][m]; constant-bank coefficients.
+__device__ __forceinline__ void line_derivs_ac(const AcParams &A, const float *fld, const uint16_t *le, int st,
+                                               float *out) {
+  float in[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) in[k] = fld[le[st * k]];
+#pragma unroll
+  for (int m = 0; m < 5; ++m) {
+    float d = 0.f;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) d += in[k] * A.hconst[5 * m + k];
+    out[st * m] = d;
+  }
+}
+__device__ __forceinline__ void line_weighted_ac(const AcParams &A, float *buf, int st) {
+  float in[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) in[k] = buf[st * k];
+#pragma unroll
+  for (int m = 0; m < 5; ++m) {
+    float d = 0.f;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) d += in[k] * A.hconst[25 + 5 * k + m];
+    buf[st * m] = d;
+  }
+}
+
 // free_mask bits: free surface, outer edge of a CPML layer; both zero chi,
 // chi_dot and chi_dot_dot before and after the forces
 constexpr uint8_t AC_FREE = 1, AC_EDGE = 2;
@@ -93,15 +127,11 @@ constexpr uint8_t AC_FREE = 1, AC_EDGE = 2;
 // Shared-memory regions of one fluid tile, 16-byte aligned (pold and pml only
 // in CPML tiles).
 struct AcSmem {
-  size_t geo, fac, p, pd, acc, h, lib, pold, pml, total;
+  size_t p, pd, acc, h, lib, d1, d2, pold, od1, od2, pml, total;
 };
 __host__ __device__ inline AcSmem ac_smem_layout(int max_q, int max_local, bool pml = false) {
   AcSmem L;
   size_t o = 0;
-  L.geo = o;
-  o = align16(o + static_cast<size_t>(max_q) * sizeof(float4));
-  L.fac = o;
-  o = align16(o + static_cast<size_t>(max_q) * sizeof(float));
   L.p = o;
   o = align16(o + static_cast<size_t>(max_local) * sizeof(float));
   L.pd = o;
@@ -112,10 +142,19 @@ __host__ __device__ inline AcSmem ac_smem_layout(int max_q, int max_local, bool 
   o = align16(o + 64 * sizeof(float));
   L.lib = o;
   o = align16(o + static_cast<size_t>((max_q + 7) / 8 * 8) * sizeof(uint16_t));
+  const size_t qb = align16(static_cast<size_t>(max_q) * sizeof(float));
+  L.d1 = o;
+  o += qb;
+  L.d2 = o;
+  o += qb;
   L.pold = o;
   if (pml) o = align16(o + static_cast<size_t>(max_local) * sizeof(float));
+  L.od1 = o;
+  if (pml) o += qb;
+  L.od2 = o;
+  if (pml) o += qb;
   L.pml = o;
-  if (pml) o = align16(o + static_cast<size_t>(max_q) * sizeof(float));
+  if (pml) o += qb;
   L.total = o;
   return L;
 }
@@ -182,10 +221,12 @@ __global__ void __launch_bounds__(NT) k_acoustic_tile(const AcParams A, int reco
   const int ebase = ti.elem_base * 25;
   const int int_begin = ti.int_begin;
   const AcSmem L = ac_smem_layout(A.max_q, A.max_local, PML);
-  float4 *s_geo = reinterpret_cast<float4 *>(smem + L.geo);
   float *s_pold = reinterpret_cast<float *>(smem + L.pold);
   float *s_pml = reinterpret_cast<float *>(smem + L.pml);
-  float *s_fac = reinterpret_cast<float *>(smem + L.fac);
+  float *s_d1 = reinterpret_cast<float *>(smem + L.d1);
+  float *s_d2 = reinterpret_cast<float *>(smem + L.d2);
+  float *s_od1 = reinterpret_cast<float *>(smem + L.od1);
+  float *s_od2 = reinterpret_cast<float *>(smem + L.od2);
   float *s_p = reinterpret_cast<float *>(smem + L.p);
   float *s_pd = reinterpret_cast<float *>(smem + L.pd);
   float *s_acc = reinterpret_cast<float *>(smem + L.acc);
@@ -201,10 +242,6 @@ __global__ void __launch_bounds__(NT) k_acoustic_tile(const AcParams A, int reco
     const uint4 *glib = reinterpret_cast<const uint4 *>(A.lib + ti.lib_off);
     const int nlib16 = (nq + 7) / 8;
     for (int k = tid; k < nlib16; k += NT) cp_async16(s_lib + 8 * k, glib + k);
-    for (int f = tid; f < nq; f += NT) {
-      cp_async16(s_geo + f, A.geo + ebase + f);
-      cp_async4(s_fac + f, A.fac + ebase + f);
-    }
     for (int l = tid; l < n_int; l += NT) {
       const int g = int_begin + l;
       cp_async4(s_p + l, A.p + g);
@@ -247,16 +284,23 @@ __global__ void __launch_bounds__(NT) k_acoustic_tile(const AcParams A, int reco
   }
   __syncthreads();
 
-  // 3. boundary terms, coupling and sources in reference order, one thread
-  if (tid == 0) {
-    for (int q = ti.st_off; q < ti.st_off + ti.st_n; ++q) {
-      const int l = A.st_local[q];
-      const float2 wr = A.st_wr[q];
-      s_acc[l] = s_acc[l] - s_pd[l] * wr.x / wr.y;
+  // 3. boundary terms, coupling and sources: one thread per receiving point,
+  //    in the reference's order at that point
+  for (int gi = tid; gi < ti.grp_n; gi += NT) {
+    const int4 g = A.bgroups[ti.grp_off + gi];
+    const int l = g.x;
+    const int *ix = A.bnd_idx + g.y;
+    float acc = s_acc[l];
+    const int nst = g.z & 255, ncp = g.z >> 8;
+    for (int k = 0; k < nst; ++k) {
+      const float2 wr = A.st_wr[ix[k]];
+      acc = acc - s_pd[l] * wr.x / wr.y;
     }
-    for (int q = ti.cpl_off; q < ti.cpl_off + ti.cpl_n; ++q) {
-      const int l = A.cpl_local[q];
-      // a negative source names the CPML entry ~src (its displacement formed by k_cpl_pml_fluid)
+    ix += nst;
+    // the solid's normal displacement; a negative source names the CPML entry
+    // ~src, whose displacement k_cpl_pml_fluid formed
+    for (int k = 0; k < ncp; ++k) {
+      const int q = ix[k];
       const int ge = A.cpl_src[q];
       const float4 nw = A.cpl_nw[q];
       float2 u;
@@ -271,53 +315,59 @@ __global__ void __launch_bounds__(NT) k_acoustic_tile(const AcParams A, int reco
         u = A.cpl_pml_u[~ge];
       }
       const float displ_n = u.x * nw.x + u.y * nw.y;
-      s_acc[l] = s_acc[l] + nw.z * displ_n;
+      acc = acc + nw.z * displ_n;
     }
-    for (int q = ti.src_off; q < ti.src_off + ti.src_n; ++q) {
-      const int l = A.src_local[q];
+    ix += ncp;
+    for (int k = 0; k < g.w; ++k) {
+      const int q = ix[k];
       const float f = step < A.nstep_stf
                           ? A.stf[(static_cast<size_t>(A.src_id[q]) * A.nstep_stf + step) * A.nstage + stage]
                           : 0.f;
       const float2 sk = A.src_sk[q];
-      s_acc[l] = s_acc[l] + sk.x * f / sk.y;
+      acc = acc + sk.x * f / sk.y;
     }
+    s_acc[l] = acc;
   }
 
-  // 4. element pass 1: gradient of chi and the J/rho weak-form terms
+  // 4a. derivative lines: one thread per element row (xi) or column (gamma),
+  //     hprime from the kernel's constant bank (see the solid kernel)
+  const int nlines = 10 * ti.nelem;
+  for (int t = tid; t < nlines; t += NT) {
+    const int e = t / 10, r = t - 10 * e;
+    const int a0 = r < 5 ? 5 * r : r - 5;
+    const int st = r < 5 ? 1 : 5;
+    const uint16_t *le = s_lib + 25 * e + a0;
+    const int o = 25 * e + a0;
+    line_derivs_ac(A, s_p, le, st, (r < 5 ? s_d1 : s_d2) + o);
+    if (PML && !LDDRK) line_derivs_ac(A, s_pold, le, st, (r < 5 ? s_od1 : s_od2) + o);
+  }
+  __syncthreads();
+
+  // 4b. per GLL point: mapping and the J/rho weak-form terms (t1, t2 overwrite
+  //     the derivatives), the layer's memory variables in CPML tiles
+  constexpr bool FIXQ = NT % 25 == 0;  // every thread keeps one GLL position
+  const int q0 = tid % 25, j0 = q0 / 5, i0 = q0 - 5 * j0;
   for (int f = tid; f < nq; f += NT) {
     const int e = f / 25;
-    const int q = f - 25 * e;
-    const int j = q / 5;
-    const int i = q - 5 * j;
+    const int q = FIXQ ? q0 : f - 25 * e;
+    const int j = FIXQ ? j0 : q / 5;
+    const int i = FIXQ ? i0 : q - 5 * j;
     const uint16_t *le = s_lib + 25 * e;
-    float dxi = 0.f, dgam = 0.f;
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-      dxi += s_p[le[5 * j + k]] * s_h[5 * i + k];
-      dgam += s_p[le[5 * k + i]] * s_h[5 * j + k];
-    }
-    const float4 g4 = s_geo[f];
+    const float dxi = s_d1[f], dgam = s_d2[f];
+    const float4 g4 = __ldg(A.geo + ebase + f);  // geometry from global memory, as in the solid kernel
     float dxl = dxi * g4.x + dgam * g4.z;
     float dzl = dxi * g4.y + dgam * g4.w;
     if (PML) {
       const int ps = ebase + f - 25 * A.pml_slot0;
-      const int region = A.pml_region[ti.elem_base + e - A.pml_slot0];
-      const PmlPoint c = pml_point(A.pml_coef, ps);
+      const PmlSet &c = A.pml_sets[A.pml_set_idx[ps]];
       float dxl_o = 0.f, dzl_o = 0.f;
       if (!LDDRK) {
-        float oxi = 0.f, og = 0.f;
-#pragma unroll
-        for (int k = 0; k < 5; ++k) {
-          oxi += s_pold[le[5 * j + k]] * s_h[5 * i + k];
-          og += s_pold[le[5 * k + i]] * s_h[5 * j + k];
-        }
+        const float oxi = s_od1[f], og = s_od2[f];
         dxl_o = oxi * g4.x + og * g4.z;
         dzl_o = oxi * g4.y + og * g4.w;
       }
-      const PmlConv cax = pml_conv(c.ax, A.DT), caz = pml_conv(c.az, A.DT);
-      const PmlConv cbx = pml_conv(c.bx, A.DT), cbz = pml_conv(c.bz, A.DT);
-      const PmlLik zx = pml_lik(c.kz, c.bz, c.az, c.kx, c.bx, c.ax, region, false);  // poles alpha_z, beta_x
-      const PmlLik xz = pml_lik(c.kx, c.bx, c.ax, c.kz, c.bz, c.az, region, true);   // poles alpha_x, beta_z
+      const PmlConv &cax = c.cax, &caz = c.caz, &cbx = c.cbx, &cbz = c.cbz;
+      const PmlLik &zx = c.zx, &xz = c.xz;  // poles (alpha_z, beta_x) and (alpha_x, beta_z)
       float2 rx = A.pml_rm[3 * ps], rz = A.pml_rm[3 * ps + 1], rp = A.pml_rm[3 * ps + 2];
       float2 lx = make_float2(0.f, 0.f), lz = lx, lp = lx;
       if (LDDRK) {
@@ -333,7 +383,7 @@ __global__ void __launch_bounds__(NT) k_acoustic_tile(const AcParams A, int reco
       dxl = static_cast<float>(zx.A0 * dxl + zx.A1 * rx.x + zx.A2 * rx.y);
       dzl = static_cast<float>(xz.A0 * dzl + xz.A1 * rz.x + xz.A2 * rz.y);
       // the layer's terms at this point (pml_compute_accel_contribution.f90:42-180)
-      const PmlL Lc = pml_l(c.kx, c.bx, c.ax, c.kz, c.bz, c.az, region);  // poles alpha_x, alpha_z
+      const PmlL &Lc = c.l;  // poles alpha_x, alpha_z
       const int lq = le[q];
       const float pq = s_p[lq], pdq = s_pd[lq];
       const float po = LDDRK ? 0.f : s_pold[lq];
@@ -351,29 +401,31 @@ __global__ void __launch_bounds__(NT) k_acoustic_tile(const AcParams A, int reco
         A.pml_rm_l[3 * ps + 2] = lp;
       }
     }
-    const float fac = s_fac[f];
-    s_geo[f] = make_float4(fac * (g4.x * dxl + g4.y * dzl), fac * (g4.z * dxl + g4.w * dzl), 0.f, 0.f);
+    const float fac = __ldg(A.fac + ebase + f);
+    s_d1[f] = fac * (g4.x * dxl + g4.y * dzl);
+    s_d2[f] = fac * (g4.z * dxl + g4.w * dzl);
   }
   __syncthreads();
 
-  // 5. weighted transpose contraction, colour by colour
+  // 4c. weighted transpose lines, in place
+  for (int t = tid; t < nlines; t += NT) {
+    const int e = t / 10, r = t - 10 * e;
+    const int a0 = r < 5 ? 5 * r : r - 5;
+    line_weighted_ac(A, (r < 5 ? s_d1 : s_d2) + 25 * e + a0, r < 5 ? 1 : 5);
+  }
+  __syncthreads();
+
+  // 5. assembly, colour by colour: chi_dd -= wz * row term + wx * column term
   int cb = 0;
   for (int c = 0; c < ti.ncol; ++c) {
     const int ce = ti.col_end[c] * 25;
-    for (int f = cb + tid; f < ce; f += NT) {
+    for (int f = cb + tid; f < ce; f += NT) {  // cb is a multiple of 25: FIXQ positions hold
       const int e = f / 25;
-      const int q = f - 25 * e;
-      const int j = q / 5;
-      const int i = q - 5 * j;
-      const float4 *te = s_geo + 25 * e;
-      float s1 = 0.f, s2 = 0.f;
-#pragma unroll
-      for (int k = 0; k < 5; ++k) {
-        s1 += te[5 * j + k].x * s_h[25 + 5 * k + i];
-        s2 += te[5 * k + i].y * s_h[25 + 5 * k + j];
-      }
+      const int q = FIXQ ? q0 : f - 25 * e;
+      const int j = FIXQ ? j0 : q / 5;
+      const int i = FIXQ ? i0 : q - 5 * j;
       const int l = s_lib[f];
-      float acc = s_acc[l] - (s_h[55 + j] * s1 + s_h[50 + i] * s2);
+      float acc = s_acc[l] - (s_h[55 + j] * s_d1[f] + s_h[50 + i] * s_d2[f]);
       if (PML) acc = acc - s_pml[f];
       s_acc[l] = acc;
     }

@@ -39,6 +39,7 @@ template <bool PML>
 AcTileFn pick_ac_tile(int nt, bool lddrk) {
   switch (nt) {
     case 128: return lddrk ? sf2d::k_acoustic_tile<128, true, PML> : sf2d::k_acoustic_tile<128, false, PML>;
+    case 250: return lddrk ? sf2d::k_acoustic_tile<250, true, PML> : sf2d::k_acoustic_tile<250, false, PML>;
     case 512: return lddrk ? sf2d::k_acoustic_tile<512, true, PML> : sf2d::k_acoustic_tile<512, false, PML>;
     default: return lddrk ? sf2d::k_acoustic_tile<256, true, PML> : sf2d::k_acoustic_tile<256, false, PML>;
   }
@@ -63,7 +64,9 @@ PmlAt pml_at(const Desc *d, size_t p) {
 }  // namespace
 
 struct sf2d_coupled {
-  sf2d_solver *el = nullptr;  // solid sub-solver (owns the stream)
+  sf2d_solver *el = nullptr;  // solid sub-solver (owns the stream); none for a fluid-only mesh
+  cudaStream_t own_stream = nullptr;  // the stream of a fluid-only run
+  cudaStream_t stream() const { return el ? el->stream : own_stream; }
   AcParams A{};
   Tiling T;
   std::vector<void *> allocs;
@@ -125,19 +128,32 @@ struct sf2d_coupled {
     return rc;
   }
 
+  // the fluid's CPML tiles beside the others, as the solid's (sf2d_solver::launch_tile)
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   void launch_ac_tile(bool record_prev, int stage) {
-    if (pml_tile0 > 0) tile_fn<<<pml_tile0, nt, smem, el->stream>>>(A, record_prev ? 1 : 0, stage, 0);
+    const int rp = record_prev ? 1 : 0;
+    cudaStream_t s = stream();
+    if (side) {
+      cudaEventRecord(ev_fork, s);
+      cudaStreamWaitEvent(side, ev_fork, 0);
+      pml_fn<<<T.ntiles - pml_tile0, nt, pml_smem, side>>>(A, rp, stage, pml_tile0);
+      cudaEventRecord(ev_join, side);
+      tile_fn<<<pml_tile0, nt, smem, s>>>(A, rp, stage, 0);
+      cudaStreamWaitEvent(s, ev_join, 0);
+      return;
+    }
+    if (pml_tile0 > 0) tile_fn<<<pml_tile0, nt, smem, s>>>(A, rp, stage, 0);
     if (pml_tile0 < T.ntiles)
-      (pml_fn ? pml_fn : tile_fn)<<<T.ntiles - pml_tile0, nt, pml_fn ? pml_smem : smem, el->stream>>>(
-          A, record_prev ? 1 : 0, stage, pml_tile0);
+      (pml_fn ? pml_fn : tile_fn)<<<T.ntiles - pml_tile0, nt, pml_fn ? pml_smem : smem, s>>>(A, rp, stage, pml_tile0);
   }
   void launch_ac_shared(int stage) {
     const int nb = std::max(1, (A.nshared + sf2d::SHARED_NT - 1) / sf2d::SHARED_NT);
     const int last = stage == nstage - 1 ? 1 : 0;
     if (lddrk)
-      sf2d::k_acoustic_shared<true><<<nb, sf2d::SHARED_NT, 0, el->stream>>>(A, stage, last);
+      sf2d::k_acoustic_shared<true><<<nb, sf2d::SHARED_NT, 0, stream()>>>(A, stage, last);
     else
-      sf2d::k_acoustic_shared<false><<<nb, sf2d::SHARED_NT, 0, el->stream>>>(A, stage, last);
+      sf2d::k_acoustic_shared<false><<<nb, sf2d::SHARED_NT, 0, stream()>>>(A, stage, last);
   }
   void launch_cpl_fluid(int stage) {
     if (cpl_fluid.n == 0) return;
@@ -154,10 +170,10 @@ struct sf2d_coupled {
     if (cpl_solid.n == 0) return;
     const int nb = (cpl_solid.n + 127) / 128;
     if (lddrk)
-      sf2d::k_cpl_pml_solid<true><<<nb, 128, 0, el->stream>>>(cpl_solid, A.p, A.pd, A.pdd, A.pold, A.dt,
+      sf2d::k_cpl_pml_solid<true><<<nb, 128, 0, stream()>>>(cpl_solid, A.p, A.pd, A.pdd, A.pold, A.dt,
                                                               A.alpha[stage], A.beta[stage]);
     else
-      sf2d::k_cpl_pml_solid<false><<<nb, 128, 0, el->stream>>>(cpl_solid, A.p, A.pd, A.pdd, A.pold, A.dt, 0.f, 0.f);
+      sf2d::k_cpl_pml_solid<false><<<nb, 128, 0, stream()>>>(cpl_solid, A.p, A.pd, A.pdd, A.pold, A.dt, 0.f, 0.f);
   }
   void launch_step(bool record_prev) {
     for (int st = 0; st < nstage; ++st) {
@@ -165,14 +181,16 @@ struct sf2d_coupled {
       launch_ac_tile(record_prev && st == 0, st);
       launch_ac_shared(st);
       launch_cpl_solid(st);
-      el->launch_tile(record_prev && st == 0, st);
-      el->launch_shared(st);
+      if (el) {
+        el->launch_tile(record_prev && st == 0, st);
+        el->launch_shared(st);
+      }
     }
   }
   int launch_chunk(int n) {
     for (int k = 0; k < n; ++k) launch_step(k > 0);
-    el->launch_receivers();
-    if (A.nrec > 0) sf2d::k_acoustic_receivers<<<(A.nrec + 127) / 128, 128, 0, el->stream>>>(A);
+    if (el) el->launch_receivers();
+    if (A.nrec > 0) sf2d::k_acoustic_receivers<<<(A.nrec + 127) / 128, 128, 0, stream()>>>(A);
     SF2D_CUDA(cudaGetLastError());
     return SF2D_OK;
   }
@@ -180,6 +198,10 @@ struct sf2d_coupled {
     if (graph) cudaGraphExecDestroy(graph);
     if (el) sf2d_destroy(el);
     for (void *p : allocs) cudaFree(p);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (side) cudaStreamDestroy(side);
+    if (own_stream) cudaStreamDestroy(own_stream);
   }
 };
 
@@ -252,16 +274,37 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
 
   auto *C = new sf2d_coupled();
   std::unique_ptr<sf2d_coupled> guard(C);
-  // the solid sub-solver; its receivers are renumbered into the run's list below
-  sf2d_elastic_desc e2 = *eld;
-  if (e2.seismotype == 4 || e2.seismotype == 0) e2.seismotype = 1;
-  if (int rc = sf2d_create_solver_internal(&e2, false, &C->el)) return rc;
-  sf2d_solver *S = C->el;
-  C->lddrk = S->lddrk;
-  C->nstage = S->nstage;
+  // the solid sub-solver; its receivers are renumbered into the run's list below.
+  // A solid description with nspec = 0 makes a fluid-only run: only its time
+  // stepping members (nstep, deltat..., time_scheme, nstage, alpha/beta_lddrk,
+  // threads_per_block) and the GLL arrays (hprime, hprimewgll, wxgll, wzgll) are read.
+  const bool fluid_only = eld->nspec == 0;
+  sf2d_solver *S = nullptr;
+  const int scheme = eld->time_scheme == 0 ? 1 : eld->time_scheme;
+  if (fluid_only) {
+    if (cp->ncpl_ac > 0 || cp->ncpl_el > 0 || eld->nrec > 0 || eld->nsrc > 0)
+      return fail(SF2D_ERR_INVALID, "a fluid-only run has no coupling, solid source or solid receiver");
+    if (!eld->hprime || !eld->hprimewgll || !eld->wxgll || !eld->wzgll) return fail(SF2D_ERR_INVALID, "missing GLL arrays");
+    if (scheme != 1 && scheme != 2) return fail(SF2D_ERR_INVALID, "time_scheme must be 1 (Newmark) or 2 (LDDRK)");
+    if (scheme == 2 && (!eld->alpha_lddrk || !eld->beta_lddrk)) return fail(SF2D_ERR_INVALID, "LDDRK needs alpha/beta");
+    C->lddrk = scheme == 2;
+    C->nstage = C->lddrk ? 6 : 1;
+    C->nt = eld->threads_per_block > 0 ? eld->threads_per_block : 256;
+    if (C->nt != 128 && C->nt != 250 && C->nt != 256 && C->nt != 512)
+      return fail(SF2D_ERR_INVALID, "threads_per_block must be 128, 250, 256 or 512");
+    SF2D_CUDA(cudaStreamCreateWithFlags(&C->own_stream, cudaStreamNonBlocking));
+  } else {
+    sf2d_elastic_desc e2 = *eld;
+    if (e2.seismotype == 4 || e2.seismotype == 0) e2.seismotype = 1;
+    if (int rc = sf2d_create_solver_internal(&e2, false, &C->el)) return rc;
+    S = C->el;
+    C->lddrk = S->lddrk;
+    C->nstage = S->nstage;
+    C->nt = S->nt;
+  }
+  if (ad->nsrc > 0 && eld->nstage != C->nstage) return fail(SF2D_ERR_INVALID, "stf must hold one value per step and stage");
   C->nstep = eld->nstep;
   C->nrec_total = cp->nrec_total;
-  C->nt = S->nt;
   int rc = 0;
 
   // ---- fluid tiling and per-slot data
@@ -286,23 +329,17 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
   std::vector<uint8_t> fmask(ad->nglob, 0);
   for (int g = 0; g < ad->nglob; ++g) rmass[g] = ad->rmass_inverse[T.dev2glob[g]];
   for (int k = 0; k < ad->nfree; ++k) fmask[T.glob2dev[ad->free_iglob[k]]] |= AC_FREE;
-  std::vector<int> pml_region_s;
-  std::vector<double2> pml_coef;
+  std::vector<int> pml_set_idx;
+  std::vector<PmlSet> pml_sets;
   std::vector<float> pml_jk;
   if (pml_ac) {
     for (int k = 0; k < ad->npml_edge; ++k) fmask[T.glob2dev[ad->pml_edge_iglob[k]]] |= AC_EDGE;
-    for (int s = pml_slot0; s < ad->nspec; ++s) {
-      const int e = T.elem_order[s];
-      pml_region_s.push_back(ad->pml_region[e]);
+    pml_build_sets(ad, T.elem_order, pml_slot0, ad->nspec - pml_slot0, ad->pml_dt, pml_sets, pml_set_idx);
+    for (int s = pml_slot0; s < ad->nspec; ++s)
       for (int q = 0; q < NGLL2; ++q) {
-        const size_t p = static_cast<size_t>(e) * NGLL2 + q;
-        const PmlAt c = pml_at(ad, p);
-        pml_coef.push_back(make_double2(c.kx, c.kz));
-        pml_coef.push_back(make_double2(c.ax, c.az));
-        pml_coef.push_back(make_double2(c.bx, c.bz));
+        const size_t p = static_cast<size_t>(T.elem_order[s]) * NGLL2 + q;
         pml_jk.push_back(ad->jacobian[p] / ad->kappastore[p]);  // fac = J / kappa in FP32
       }
-    }
   }
   const size_t npml_q = static_cast<size_t>(ad->nspec - pml_slot0) * NGLL2;
   // a boundary or coupling point goes to the tile of the first element holding it
@@ -334,7 +371,7 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
     tiles[t].cpl_off = static_cast<int>(cpl_local.size());
     for (int k : cpl_t[t]) {
       cpl_local.push_back(T.local_id(t, cp->cpl_ac_point[k]));
-      cpl_src.push_back(S->T.glob2dev[cp->cpl_ac_el_point[k]]);
+      cpl_src.push_back(S->T.glob2dev[cp->cpl_ac_el_point[k]]);  // entries exist only with a solid
       cpl_nw.push_back(make_float4(cp->cpl_ac_nx[k], cp->cpl_ac_nz[k], cp->cpl_ac_w[k], 0.f));
       const int q = pml_el ? cp->cpl_ac_el_elpt[k] : -1;
       const int region = q >= 0 ? eld->pml_region[q / NGLL2] : 0;
@@ -378,7 +415,11 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
     tiles[t].rec_n = static_cast<int>(rec_id.size()) - tiles[t].rec_off;
   }
   for (const TileInfo &t : tiles)
-    if (t.rec_n > S->nt) return fail(SF2D_ERR_INVALID, "more fluid receivers in one tile than threads per CTA");
+    if (t.rec_n > C->nt) return fail(SF2D_ERR_INVALID, "more fluid receivers in one tile than threads per CTA");
+  std::vector<int4> bgroups;
+  std::vector<int> bnd_idx;
+  err = build_boundary_groups(tiles, st_local, cpl_local, src_local, bgroups, bnd_idx);
+  if (!err.empty()) return fail(SF2D_ERR_INVALID, err);
 
   AcParams &A = C->A;
   C->nglob = ad->nglob;
@@ -398,12 +439,13 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
     A.pL = pl;
     A.pdL = pdl;
     for (int k = 0; k < 6; ++k) {
-      A.alpha[k] = S->P.alpha[k];
-      A.beta[k] = S->P.beta[k];
+      A.alpha[k] = eld->alpha_lddrk[k];
+      A.beta[k] = eld->beta_lddrk[k];
     }
   }
   if ((rc = C->upload_const(&A.rmass, rmass)) || (rc = C->upload_const(&A.free_mask, fmask)) ||
       (rc = C->upload_const(&A.tiles, tiles)) || (rc = C->upload_const(&A.lib, T.lib)) ||
+      (rc = C->upload_const(&A.bgroups, bgroups)) || (rc = C->upload_const(&A.bnd_idx, bnd_idx)) ||
       (rc = C->upload_const(&A.geo, geo)) || (rc = C->upload_const(&A.fac, fac)) ||
       (rc = C->upload_const(&A.sh_ids, T.sh_ids)) || (rc = C->upload_const(&A.shp_off, T.shp_off)) ||
       (rc = C->upload_const(&A.shp_slots, T.shp_slots)) || (rc = C->upload_const(&A.st_local, st_local)) ||
@@ -419,7 +461,7 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
     A.cpl_pml_u = reinterpret_cast<const float2 *>(C->cpl_fluid.out);
   }
   if (pml_ac) {
-    if ((rc = C->upload_const(&A.pml_region, pml_region_s)) || (rc = C->upload_const(&A.pml_coef, pml_coef)) ||
+    if ((rc = C->upload_const(&A.pml_sets, pml_sets)) || (rc = C->upload_const(&A.pml_set_idx, pml_set_idx)) ||
         (rc = C->upload_const(&A.pml_jk, pml_jk)))
       return rc;
     for (int l = 0; l < (C->lddrk ? 2 : 1); ++l) {
@@ -455,9 +497,11 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
   A.d_step = C->ctr;
   A.d_step_b = C->ctr + 1;
   A.d_status = C->ctr + 2;
-  A.u_el = S->P.u;
-  A.v_el = S->P.v;
-  A.a_el = S->P.a;
+  if (S) {
+    A.u_el = S->P.u;
+    A.v_el = S->P.v;
+    A.a_el = S->P.a;
+  }
   A.nstep_stf = eld->nstep;
   A.nstage = C->nstage;
   A.nstep_seis = eld->nstep;
@@ -473,7 +517,14 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
   A.nshared = T.nshared;
   A.max_q = T.max_elems * NGLL2;
   A.max_local = T.max_local;
-  for (int k = 0; k < 60; ++k) A.hconst[k] = S->P.hconst[k];
+  for (int k = 0; k < 25; ++k) {
+    A.hconst[k] = eld->hprime[k];
+    A.hconst[25 + k] = eld->hprimewgll[k];
+  }
+  for (int k = 0; k < 5; ++k) {
+    A.hconst[50 + k] = eld->wxgll[k];
+    A.hconst[55 + k] = eld->wzgll[k];
+  }
   if ((rc = C->upload(&C->d_dev2glob, T.dev2glob.data(), T.dev2glob.size()))) return rc;
   if ((rc = C->alloc(&C->d_stage, ad->nglob))) return rc;
   C->smem = ac_smem_layout(A.max_q, A.max_local).total;
@@ -483,6 +534,11 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
     C->pml_fn = pick_ac_tile<true>(C->nt, C->lddrk);
     C->pml_smem = ac_smem_layout(A.max_q, A.max_local, true).total;
     if (C->pml_smem > 220 * 1024) return fail(SF2D_ERR_INVALID, "fluid tile too large for shared memory");
+    if (C->pml_tile0 > 0 && C->pml_tile0 < T.ntiles) {
+      SF2D_CUDA(cudaStreamCreateWithFlags(&C->side, cudaStreamNonBlocking));
+      SF2D_CUDA(cudaEventCreateWithFlags(&C->ev_fork, cudaEventDisableTiming));
+      SF2D_CUDA(cudaEventCreateWithFlags(&C->ev_join, cudaEventDisableTiming));
+    }
   }
   {
     // the limit belongs to the kernel: only ever raise it (see the solid solver)
@@ -500,6 +556,11 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
   }
 
   // ---- solid side: receivers into the run's list, coupling entries per tile
+  if (fluid_only) {
+    SF2D_CUDA(cudaDeviceSynchronize());
+    *out = guard.release();
+    return SF2D_OK;
+  }
   if (S->nrec > 0) {
     std::vector<int> ids(S->nrec);
     SF2D_CUDA(cudaMemcpy(ids.data(), S->P.rec_id, sizeof(int) * S->nrec, cudaMemcpyDeviceToHost));
@@ -547,6 +608,12 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
       if (C->cpl_solid.n > 0 && !C->lddrk && !A.pold)
         return fail(SF2D_ERR_INVALID, "CPML coupling entries without a fluid CPML layer");
     }
+    // the solid's boundary terms regrouped with the coupling entries
+    std::vector<int4> eg;
+    std::vector<int> ei;
+    err = build_boundary_groups(et, S->h_st_local, e_local, S->h_src_local, eg, ei);
+    if (!err.empty()) return fail(SF2D_ERR_INVALID, err);
+    if ((rc = C->upload_const(&S->P.bgroups, eg)) || (rc = C->upload_const(&S->P.bnd_idx, ei))) return rc;
     SF2D_CUDA(cudaMemcpy(const_cast<TileInfo *>(S->P.tiles), et.data(), sizeof(TileInfo) * et.size(),
                          cudaMemcpyHostToDevice));
     if ((rc = C->upload_const(&S->P.cpl_local, e_local)) || (rc = C->upload_const(&S->P.cpl_src, e_src)) ||
@@ -563,6 +630,7 @@ extern "C" int sf2d_coupled_enqueue(sf2d_coupled *C, int nstep) {
   using namespace sf2d;
   if (!C || nstep < 0) return fail(SF2D_ERR_INVALID, "bad arguments");
   sf2d_solver *S = C->el;
+  cudaStream_t st = C->stream();
   const int K = C->chunk;
   int done = 0;
   if (nstep >= K) {
@@ -570,20 +638,20 @@ extern "C" int sf2d_coupled_enqueue(sf2d_coupled *C, int nstep) {
       if (C->graph) cudaGraphExecDestroy(C->graph);
       C->graph = nullptr;
       cudaGraph_t g;
-      SF2D_CUDA(cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal));
+      SF2D_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
       C->launch_chunk(K);
-      SF2D_CUDA(cudaStreamEndCapture(S->stream, &g));
+      SF2D_CUDA(cudaStreamEndCapture(st, &g));
       cudaError_t e = cudaGraphInstantiate(&C->graph, g, 0);
       cudaGraphDestroy(g);
       if (e != cudaSuccess) return fail(SF2D_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
       C->graph_steps = K;
     }
-    for (; done + K <= nstep; done += K) SF2D_CUDA(cudaGraphLaunch(C->graph, S->stream));
+    for (; done + K <= nstep; done += K) SF2D_CUDA(cudaGraphLaunch(C->graph, st));
   }
   if (done < nstep)
     if (int rc = C->launch_chunk(nstep - done)) return rc;
   C->steps_done += nstep;
-  S->steps_done += nstep;
+  if (S) S->steps_done += nstep;
   return SF2D_OK;
 }
 
@@ -591,9 +659,9 @@ extern "C" int sf2d_coupled_synchronize(sf2d_coupled *C) {
   using namespace sf2d;
   if (!C) return fail(SF2D_ERR_INVALID, "null solver");
   sf2d_solver *S = C->el;
-  SF2D_CUDA(cudaStreamSynchronize(S->stream));
+  SF2D_CUDA(cudaStreamSynchronize(C->stream()));
   int status[2] = {0, 0};
-  SF2D_CUDA(cudaMemcpy(&status[0], S->P.d_status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (S) SF2D_CUDA(cudaMemcpy(&status[0], S->P.d_status, sizeof(int), cudaMemcpyDeviceToHost));
   SF2D_CUDA(cudaMemcpy(&status[1], C->A.d_status, sizeof(int), cudaMemcpyDeviceToHost));
   if (status[0] || status[1]) return fail(SF2D_ERR_UNSTABLE, "wavefield blew up (NaN or |field| > 1e25)");
   return SF2D_OK;
@@ -618,11 +686,12 @@ extern "C" int sf2d_coupled_get_fields(sf2d_coupled *C, float *displ, float *vel
                                        float *pot_dot, float *pot_dot_dot) {
   using namespace sf2d;
   if (!C) return fail(SF2D_ERR_INVALID, "null solver");
-  if (int rc = sf2d_get_fields(C->el, displ, veloc, accel)) return rc;
+  if (C->el)
+    if (int rc = sf2d_get_fields(C->el, displ, veloc, accel)) return rc;
   const float *src[3] = {C->A.p, C->A.pd, C->A.pdd};
   float *dst[3] = {pot, pot_dot, pot_dot_dot};
   const int n = C->nglob;
-  cudaStream_t s = C->el->stream;
+  cudaStream_t s = C->stream();
   for (int k = 0; k < 3; ++k) {
     if (!dst[k]) continue;
     k_scatter_f<<<(n + 255) / 256, 256, 0, s>>>(src[k], C->d_dev2glob, C->d_stage, n);
@@ -637,11 +706,12 @@ extern "C" int sf2d_coupled_set_fields(sf2d_coupled *C, const float *displ, cons
                                        const float *pot, const float *pot_dot, const float *pot_dot_dot) {
   using namespace sf2d;
   if (!C) return fail(SF2D_ERR_INVALID, "null solver");
-  if (int rc = sf2d_set_fields(C->el, displ, veloc, accel)) return rc;
+  if (C->el)
+    if (int rc = sf2d_set_fields(C->el, displ, veloc, accel)) return rc;
   float *dst[3] = {C->A.p, C->A.pd, C->A.pdd};
   const float *src[3] = {pot, pot_dot, pot_dot_dot};
   const int n = C->nglob;
-  cudaStream_t s = C->el->stream;
+  cudaStream_t s = C->stream();
   for (int k = 0; k < 3; ++k) {
     if (!src[k]) {
       SF2D_CUDA(cudaMemsetAsync(dst[k], 0, sizeof(float) * n, s));
@@ -659,23 +729,24 @@ extern "C" int sf2d_coupled_time_kernels(sf2d_coupled *C, int nstep, float *ms) 
   using namespace sf2d;
   if (!C || nstep <= 0 || !ms) return fail(SF2D_ERR_INVALID, "bad arguments");
   sf2d_solver *S = C->el;
+  cudaStream_t str = C->stream();
   cudaEvent_t ev[5];
   for (auto &e : ev) SF2D_CUDA(cudaEventCreate(&e));
   double acc[4] = {0, 0, 0, 0};
   for (int k = 0; k < nstep; ++k)
     for (int st = 0; st < C->nstage; ++st) {
       const bool rp = k > 0 && st == 0;
-      SF2D_CUDA(cudaEventRecord(ev[0], S->stream));
+      SF2D_CUDA(cudaEventRecord(ev[0], str));
       C->launch_cpl_fluid(st);
       C->launch_ac_tile(rp, st);
-      SF2D_CUDA(cudaEventRecord(ev[1], S->stream));
+      SF2D_CUDA(cudaEventRecord(ev[1], str));
       C->launch_ac_shared(st);
-      SF2D_CUDA(cudaEventRecord(ev[2], S->stream));
+      SF2D_CUDA(cudaEventRecord(ev[2], str));
       C->launch_cpl_solid(st);
-      S->launch_tile(rp, st);
-      SF2D_CUDA(cudaEventRecord(ev[3], S->stream));
-      S->launch_shared(st);
-      SF2D_CUDA(cudaEventRecord(ev[4], S->stream));
+      if (S) S->launch_tile(rp, st);
+      SF2D_CUDA(cudaEventRecord(ev[3], str));
+      if (S) S->launch_shared(st);
+      SF2D_CUDA(cudaEventRecord(ev[4], str));
       SF2D_CUDA(cudaEventSynchronize(ev[4]));
       for (int q = 0; q < 4; ++q) {
         float t = 0.f;
@@ -684,11 +755,11 @@ extern "C" int sf2d_coupled_time_kernels(sf2d_coupled *C, int nstep, float *ms) 
       }
     }
   SF2D_CUDA(cudaGetLastError());
-  C->el->launch_receivers();
-  if (C->A.nrec > 0) sf2d::k_acoustic_receivers<<<(C->A.nrec + 127) / 128, 128, 0, S->stream>>>(C->A);
-  SF2D_CUDA(cudaStreamSynchronize(S->stream));
+  if (S) S->launch_receivers();
+  if (C->A.nrec > 0) sf2d::k_acoustic_receivers<<<(C->A.nrec + 127) / 128, 128, 0, str>>>(C->A);
+  SF2D_CUDA(cudaStreamSynchronize(str));
   C->steps_done += nstep;
-  S->steps_done += nstep;
+  if (S) S->steps_done += nstep;
   for (auto &e : ev) cudaEventDestroy(e);
   const double launches = static_cast<double>(nstep) * C->nstage;
   for (int q = 0; q < 4; ++q) ms[q] = static_cast<float>(acc[q] / launches);
@@ -711,6 +782,7 @@ extern "C" int sf2d_coupled_layout_info(sf2d_coupled *C, long long *info) {
 extern "C" int sf2d_coupled_solid_layout_info(sf2d_coupled *C, long long *info8) {
   using namespace sf2d;
   if (!C) return fail(SF2D_ERR_INVALID, "null solver");
+  if (!C->el) return fail(SF2D_ERR_INVALID, "a fluid-only run has no solid layout");
   return sf2d_layout_info(C->el, info8);
 }
 
@@ -718,17 +790,18 @@ extern "C" int sf2d_coupled_launch_count(sf2d_coupled *C, int nstep, long long *
   using namespace sf2d;
   if (!C || !launches || nstep < 0) return fail(SF2D_ERR_INVALID, "bad arguments");
   const sf2d_solver *S = C->el;
-  const long long per_stage = (C->cpl_fluid.n > 0) + (C->pml_tile0 > 0) + (C->pml_tile0 < C->T.ntiles) + 1 +
-                              (C->cpl_solid.n > 0) + (S->pml_tile0 > 0) + (S->pml_tile0 < S->T.ntiles) + 1;
+  long long per_stage = (C->cpl_fluid.n > 0) + (C->pml_tile0 > 0) + (C->pml_tile0 < C->T.ntiles) + 1 +
+                        (C->cpl_solid.n > 0);
+  if (S) per_stage += (S->pml_tile0 > 0) + (S->pml_tile0 < S->T.ntiles) + 1;
   const long long chunks = nstep / C->chunk + (nstep % C->chunk ? 1 : 0);
-  *launches = per_stage * C->nstage * nstep + ((S->nrec > 0) + (C->A.nrec > 0)) * chunks;
+  *launches = per_stage * C->nstage * nstep + ((S && S->nrec > 0) + (C->A.nrec > 0)) * chunks;
   return SF2D_OK;
 }
 
 extern "C" int sf2d_coupled_get_stream(sf2d_coupled *C, void **stream) {
   using namespace sf2d;
   if (!C || !stream) return fail(SF2D_ERR_INVALID, "bad arguments");
-  *stream = static_cast<void *>(C->el->stream);
+  *stream = static_cast<void *>(C->stream());
   return SF2D_OK;
 }
 

@@ -199,24 +199,17 @@ int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solv
   // damping data, the outer edge as per-tile local lists and a shared-point mask
   S->pml_tile0 = pml ? T.group_tile_begin[1] : T.ntiles;
   const int pml_slot0 = S->pml_tile0 < T.ntiles ? T.tiles[S->pml_tile0].elem_base : d->nspec;
-  std::vector<int> pml_region_s, edge_local;
-  std::vector<double2> pml_coef;
+  std::vector<int> pml_set_idx, edge_local;
+  std::vector<PmlSet> pml_sets;
   std::vector<float> pml_rhoj;
   std::vector<uint8_t> sh_edge;
   if (pml) {
-    for (int s = pml_slot0; s < d->nspec; ++s) {
-      const int e = T.elem_order[s];
-      pml_region_s.push_back(d->pml_region[e]);
+    pml_build_sets(d, T.elem_order, pml_slot0, d->nspec - pml_slot0, d->pml_dt, pml_sets, pml_set_idx);
+    for (int s = pml_slot0; s < d->nspec; ++s)
       for (int q = 0; q < NGLL2; ++q) {
-        const size_t p = static_cast<size_t>(e) * NGLL2 + q;
-        const double kx = d->pml_K_x[p], kz = d->pml_K_z[p], ax = d->pml_alpha_x[p], az = d->pml_alpha_z[p];
-        // beta = alpha + d / K (pml_compute_memory_variables.f90:164-165)
-        pml_coef.push_back(make_double2(kx, kz));
-        pml_coef.push_back(make_double2(ax, az));
-        pml_coef.push_back(make_double2(ax + d->pml_d_x[p] / kx, az + d->pml_d_z[p] / kz));
+        const size_t p = static_cast<size_t>(T.elem_order[s]) * NGLL2 + q;
         pml_rhoj.push_back(d->rhostore[p] * d->jacobian[p]);
       }
-    }
     std::vector<uint8_t> on_edge(d->nglob, 0);
     for (int k = 0; k < d->npml_edge; ++k) on_edge[d->pml_edge_iglob[k]] = 1;
     for (int t = 0; t < T.ntiles; ++t) {
@@ -229,6 +222,12 @@ int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solv
     for (int s = 0; s < T.nshared; ++s) sh_edge[s] = on_edge[T.dev2glob[T.shared_begin + s]];
   }
   S->npml_q = static_cast<size_t>(d->nspec - pml_slot0) * NGLL2;
+  std::vector<int4> bgroups;
+  std::vector<int> bnd_idx;
+  err = build_boundary_groups(tiles, st_local, {}, src_local, bgroups, bnd_idx);
+  if (!err.empty()) return fail(SF2D_ERR_INVALID, err);
+  S->h_st_local = st_local;
+  S->h_src_local = src_local;
 
   SF2D_CUDA(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
   Params &P = S->P;
@@ -255,6 +254,8 @@ int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solv
   UP(sh_ids, int, T.sh_ids);
   UP(shp_off, int, T.shp_off);
   UP(shp_slots, int, T.shp_slots);
+  UP(bgroups, int4, bgroups);
+  UP(bnd_idx, int, bnd_idx);
   UP(st_local, int, st_local);
   UP(st_nw, float4, st_nw);
   UP(st_rho, float2, st_rho);
@@ -295,8 +296,8 @@ int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solv
     }
   }
   if (pml) {
-    UP(pml_region, int, pml_region_s);
-    UP(pml_coef, double2, pml_coef);
+    UP(pml_sets, PmlSet, pml_sets);
+    UP(pml_set_idx, int, pml_set_idx);
     UP(pml_rhoj, float, pml_rhoj);
     UP(edge_local, int, edge_local);
     UP(sh_edge, uint8_t, sh_edge);
@@ -379,8 +380,8 @@ int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solv
   S->smem = tile_smem_layout(P.max_q, P.max_local, kern).total;
   if (S->smem > 220 * 1024) return fail(SF2D_ERR_INVALID, "tile too large for shared memory");
   S->nt = d->threads_per_block > 0 ? d->threads_per_block : 256;
-  if (S->nt != 128 && S->nt != 256 && S->nt != 512)
-    return fail(SF2D_ERR_INVALID, "threads_per_block must be 128, 256 or 512");
+  if (S->nt != 128 && S->nt != 250 && S->nt != 256 && S->nt != 512)
+    return fail(SF2D_ERR_INVALID, "threads_per_block must be 128, 250, 256 or 512");
   if (d->nrec > 0) {
     for (const TileInfo &t : tiles)
       if (t.rec_n > S->nt) return fail(SF2D_ERR_INVALID, "more receivers in one tile than threads per CTA");
@@ -393,6 +394,7 @@ int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solv
   }
   S->lddrk = lddrk;
   S->nstage = nstage;
+  if ((rc = S->make_side_stream())) return rc;
   {
     // The limit is a property of the kernel, shared by every solver in the
     // process: only ever raise it, or a later solver with smaller tiles would

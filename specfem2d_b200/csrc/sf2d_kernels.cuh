@@ -2,23 +2,26 @@
 //
 // One CTA advances one tile of elements by one Newmark step or one LDDRK
 // stage:
-//   1. cp.async of the tile's local ibool, geometry, material and the fields
-//      of all its points straight into shared memory;
+//   1. cp.async of the tile's local ibool and the fields of all its points
+//      straight into shared memory (geometry and material are read from
+//      global memory where they are used);
 //   2. Newmark predictor u' = u + dt v + dt^2/2 a, v' = v + dt/2 a
 //      (update_displacement_Newmark.F90:408-454) in shared memory, or a
 //      cleared accumulator for an LDDRK stage (iterate_time.F90:167-181);
-//   3. Stacey traction on the (predicted) velocity and the sources, by one
-//      thread in reference order (compute_stacey_elastic.f90:160-335,
+//   3. Stacey traction on the (predicted) velocity, fluid pressure and
+//      sources, one thread per receiving point in the reference's order at
+//      that point (compute_stacey_elastic.f90:160-335,
 //      compute_add_sources_viscoelastic.f90:36-101);
-//   4. per GLL point: gradient through hprime, Jacobian mapping, isotropic
-//      (lambda, mu as compute_forces_viscoelastic.F90:286-294 forms them) or
-//      anisotropic stress (:372-445, in double as the reference), 3-SLS
-//      memory variables and their stress correction
-//      (compute_attenuation_viscoelastic.f90:36-236, :481-503), weak-form
-//      terms (:669-675);
-//   5. weighted transpose contraction with hprimewgll (:760-782) assembled
-//      into the shared accumulator colour by colour (no two elements of a
-//      colour share a point: no atomics);
+//   4. derivative lines (one thread per element row or column: the 5x5
+//      contraction with hprime, mxm_4comp_singleA :810-883), then per GLL
+//      point the Jacobian mapping, isotropic (lambda, mu as
+//      compute_forces_viscoelastic.F90:286-294 forms them) or anisotropic
+//      stress (:372-445, in double as the reference), 3-SLS memory variables
+//      and their stress correction (compute_attenuation_viscoelastic.f90:36-236,
+//      :481-503), weak-form terms (:669-675), then the weighted transpose
+//      lines with hprimewgll (:760-782);
+//   5. assembly into the shared accumulator colour by colour (no two elements
+//      of a colour share a point: no atomics);
 //   6. interior points: a *= rmass_inverse, then the Newmark corrector
 //      (update_displacement_Newmark.F90:564-589) or the LDDRK update
 //      (update_displacement_LDDRK.F90:55-79), write-back; shared points: the
@@ -53,6 +56,8 @@ struct Params {
   const int *sh_ids;
   float2 *partial;
   const int *shp_off, *shp_slots;
+  const int4 *bgroups;    // per tile (grp_off, grp_n): point, first idx, Stacey | coupling << 8, sources
+  const int *bnd_idx;     // entries of each group
   const int *st_local;
   const float4 *st_nw;    // nx, nz, weight, 0
   const float2 *st_rho;   // rho*vp, rho*vs
@@ -80,8 +85,8 @@ struct Params {
   // CPML: elements of slots >= pml_slot0 lie in the layer, "PML points" are
   // their GLL points in slot order (index (slot - pml_slot0) * 25 + q)
   int pml_slot0;
-  const int *pml_region;  // per PML element: CPML_X_ONLY, CPML_Z_ONLY or CPML_XZ
-  const double2 *pml_coef;  // 3 per PML point: (K_x, K_z), (alpha_x, alpha_z), (beta_x, beta_z)
+  const PmlSet *pml_sets;  // coefficient sets of the layer
+  const int *pml_set_idx;  // per PML point: its set
   const float *pml_rhoj;  // rho * jacobian per PML point
   float4 *pml_rm;         // 3 per PML point: strain memory zx (dux_dx 1,2, duz_dx 1,2), xz (dux_dz, duz_dz),
                           // displacement memory (x 1, z 1, x 2, z 2)
@@ -146,25 +151,22 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // Shared-memory layout of one tile (sizes from the largest tile); every region
 // starts on a 16-byte boundary, as 16-byte cp.async destinations require:
-//   geo  float4[max_q]  xix, xiz, gammax, gammaz; overwritten by the weak-form terms
-//   mat  float2[max_q]  lambda, mu
 //   u, v, acc float2[max_local]  (old u, v, a -> predicted u, v and the accumulator)
 //   h    float[64]      hprime, hprimewgll, wxgll, wzgll
 //   lib  uint16[max_q rounded up to 8]
-//   b    float2[max_local]  forward frame (adjoint sweep with kernels)
-//   uold float2[max_local], pml float2[max_q]  mid-step displacement and the
-//        layer's acceleration terms (CPML tiles)
+//   d1, d2 float2[max_q]  xi / gamma derivatives, then the weak-form terms t1, t2,
+//        then their weighted transposes
+//   b    float2[max_local], bd1, bd2 float2[max_q]  forward frame and its
+//        derivatives (adjoint sweep with kernels)
+//   uold float2[max_local], od1, od2, pml float2[max_q]  mid-step displacement,
+//        its derivatives and the layer's acceleration terms (CPML tiles)
 struct TileSmem {
-  size_t geo, mat, u, v, acc, h, lib, b, uold, pml, total;
+  size_t u, v, acc, h, lib, d1, d2, b, bd1, bd2, uold, od1, od2, pml, total;
 };
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~static_cast<size_t>(15); }
 __host__ __device__ inline TileSmem tile_smem_layout(int max_q, int max_local, bool kern = false, bool pml = false) {
   TileSmem L;
   size_t o = 0;
-  L.geo = o;
-  o = align16(o + static_cast<size_t>(max_q) * sizeof(float4));
-  L.mat = o;
-  o = align16(o + static_cast<size_t>(max_q) * sizeof(float2));
   L.u = o;
   o = align16(o + static_cast<size_t>(max_local) * sizeof(float2));
   L.v = o;
@@ -175,12 +177,26 @@ __host__ __device__ inline TileSmem tile_smem_layout(int max_q, int max_local, b
   o = align16(o + 64 * sizeof(float));
   L.lib = o;
   o = align16(o + static_cast<size_t>((max_q + 7) / 8 * 8) * sizeof(uint16_t));
+  const size_t qb = align16(static_cast<size_t>(max_q) * sizeof(float2));
+  const size_t lb = align16(static_cast<size_t>(max_local) * sizeof(float2));
+  L.d1 = o;
+  o += qb;
+  L.d2 = o;
+  o += qb;
   L.b = o;
-  if (kern) o = align16(o + static_cast<size_t>(max_local) * sizeof(float2));
+  if (kern) o += lb;
+  L.bd1 = o;
+  if (kern) o += qb;
+  L.bd2 = o;
+  if (kern) o += qb;
   L.uold = o;
-  if (pml) o = align16(o + static_cast<size_t>(max_local) * sizeof(float2));
+  if (pml) o += lb;
+  L.od1 = o;
+  if (pml) o += qb;
+  L.od2 = o;
+  if (pml) o += qb;
   L.pml = o;
-  if (pml) o = align16(o + static_cast<size_t>(max_q) * sizeof(float2));
+  if (pml) o += qb;
   L.total = o;
   return L;
 }
@@ -263,6 +279,47 @@ __device__ __forceinline__ void kernel_point(float dux_dxi, float duz_dxi, float
   muk = dux_dxl * bdux_dxl + duz_dzl * bduz_dzl + 2.f * dsxz * bdsxz - 1.f / 3.f * kap;
 }
 
+// Derivatives along one element line of 5 GLL points (stride st in the
+// element's [j][i] order, first local index at le[0]): out[m] = sum_k f_k
+// hprime[m][k] with hprime from the kernel parameters (compile-time indices
+// after unrolling: constant-bank operands).  Same operation order as a
+// point-by-point sum, so the results are the same.
+__device__ __forceinline__ void line_derivs(const Params &P, const float2 *fld, const uint16_t *le, int st,
+                                            float2 *out) {
+  float2 in[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) in[k] = fld[le[st * k]];
+#pragma unroll
+  for (int m = 0; m < 5; ++m) {
+    float2 d = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      const float h = P.hconst[5 * m + k];
+      d.x += in[k].x * h;
+      d.y += in[k].y * h;
+    }
+    out[st * m] = d;
+  }
+}
+
+// Weighted transpose along one line, in place: out[m] = sum_k t_k hprimewgll[k][m].
+__device__ __forceinline__ void line_weighted(const Params &P, float2 *buf, int st) {
+  float2 in[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) in[k] = buf[st * k];
+#pragma unroll
+  for (int m = 0; m < 5; ++m) {
+    float2 d = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      const float w = P.hconst[25 + 5 * k + m];
+      d.x += in[k].x * w;
+      d.y += in[k].y * w;
+    }
+    buf[st * m] = d;
+  }
+}
+
 // PML: the tiles of a CPML layer (isotropic, no attenuation, no kernels):
 // mid-step displacement u + dt^2/4 a of the tile's points, the layer's strain
 // and displacement memory variables, the modified non-symmetric stress and
@@ -281,11 +338,15 @@ __global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_
   const int ebase = ti.elem_base * 25;
   const int int_begin = ti.int_begin;
   const TileSmem L = tile_smem_layout(P.max_q, P.max_local, KERN, PML);
-  float4 *s_geo = reinterpret_cast<float4 *>(smem + L.geo);
   float2 *s_uold = reinterpret_cast<float2 *>(smem + L.uold);
   float2 *s_pml = reinterpret_cast<float2 *>(smem + L.pml);
+  float2 *s_d1 = reinterpret_cast<float2 *>(smem + L.d1);
+  float2 *s_d2 = reinterpret_cast<float2 *>(smem + L.d2);
+  float2 *s_bd1 = reinterpret_cast<float2 *>(smem + L.bd1);
+  float2 *s_bd2 = reinterpret_cast<float2 *>(smem + L.bd2);
+  float2 *s_od1 = reinterpret_cast<float2 *>(smem + L.od1);
+  float2 *s_od2 = reinterpret_cast<float2 *>(smem + L.od2);
   float2 *s_b = reinterpret_cast<float2 *>(smem + L.b);
-  float2 *s_mat = reinterpret_cast<float2 *>(smem + L.mat);
   float2 *s_u = reinterpret_cast<float2 *>(smem + L.u);
   float2 *s_v = reinterpret_cast<float2 *>(smem + L.v);
   float2 *s_acc = reinterpret_cast<float2 *>(smem + L.acc);
@@ -304,10 +365,6 @@ __global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_
     const uint4 *glib = reinterpret_cast<const uint4 *>(P.lib + ti.lib_off);
     const int nlib16 = (nq + 7) / 8;
     for (int k = tid; k < nlib16; k += NT) cp_async16(s_lib + 8 * k, glib + k);
-    for (int f = tid; f < nq; f += NT) {
-      cp_async16(s_geo + f, P.geo + ebase + f);
-      cp_async8(s_mat + f, P.mat + ebase + f);
-    }
     for (int l = tid; l < n_int; l += NT) {
       const int g = int_begin + l;
       cp_async8(s_u + l, P.u + g);
@@ -361,84 +418,92 @@ __global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_
     __syncthreads();
   }
 
-  // 3. boundary terms and sources in reference order, one thread (overlaps pass 1)
-  if (tid == 0) {
-    for (int p = ti.st_off; p < ti.st_off + ti.st_n; ++p) {
-      const int l = P.st_local[p];
+  // 3. boundary terms, coupling and sources: one thread per receiving point,
+  //    in the reference's order at that point (overlaps pass 1, which does not
+  //    touch the accumulator)
+  for (int gi = tid; gi < ti.grp_n; gi += NT) {
+    const int4 g = P.bgroups[ti.grp_off + gi];
+    const int l = g.x;
+    const int *ix = P.bnd_idx + g.y;
+    float2 acc = s_acc[l];
+    const float2 v = s_v[l];
+    const int nst = g.z & 255, ncp = g.z >> 8;
+    // Stacey traction on the predicted velocity (compute_stacey_elastic.f90:160-335)
+    for (int k = 0; k < nst; ++k) {
+      const int p = ix[k];
       const float4 nw = P.st_nw[p];
       const float2 rr = P.st_rho[p];
-      const float2 v = s_v[l];
       const float vn = nw.x * v.x + nw.y * v.y;
       const float tx = rr.x * vn * nw.x + rr.y * (v.x - vn * nw.x);
       const float tz = rr.x * vn * nw.y + rr.y * (v.y - vn * nw.y);
-      float2 acc = s_acc[l];
       acc.x -= tx * nw.z;
       acc.y -= tz * nw.z;
-      s_acc[l] = acc;
     }
+    ix += nst;
     // pressure of the fluid on the solid, -chi_dot_dot of this step
-    // (compute_coupling_viscoelastic_ac.f90:80-250)
-    for (int p = ti.cpl_off; p < ti.cpl_off + ti.cpl_n; ++p) {
-      const int l = P.cpl_local[p];
+    // (compute_coupling_viscoelastic_ac.f90:80-250); a negative source names
+    // the CPML entry ~src, whose pressure k_cpl_pml_solid formed
+    for (int k = 0; k < ncp; ++k) {
+      const int p = ix[k];
       const float4 nw = P.cpl_nw[p];
-      // a negative source names the CPML entry ~src (its pressure formed by k_cpl_pml_solid)
       const int ga = P.cpl_src[p];
       const float pressure = ga >= 0 ? -P.pdd_ac[ga] : P.cpl_pml_p[~ga];
-      float2 acc = s_acc[l];
       acc.x += nw.z * nw.x * pressure;
       acc.y += nw.z * nw.y * pressure;
-      s_acc[l] = acc;
     }
-    for (int p = ti.src_off; p < ti.src_off + ti.src_n; ++p) {
-      const int l = P.src_local[p];
+    ix += ncp;
+    // sources (compute_add_sources_viscoelastic.f90:36-101)
+    for (int k = 0; k < g.w; ++k) {
+      const int p = ix[k];
       const float f = step < P.nstep_stf
                           ? P.stf[(static_cast<size_t>(P.src_id[p]) * P.nstep_stf + step) * P.nstage + stage]
                           : 0.f;
       const float2 sa = P.src_arr[p];
-      float2 acc = s_acc[l];
       acc.x += sa.x * f;
       acc.y += sa.y * f;
-      s_acc[l] = acc;
     }
+    s_acc[l] = acc;
   }
 
-  // 4. element pass 1: gradient, stress, memory variables, weak-form terms
+  // 4a. derivative lines: one thread per element row (xi) or column (gamma)
+  //     forms the 5 derivatives along it; the loops are fully unrolled, so
+  //     hprime comes straight from the kernel's constant bank, and each point's
+  //     field is read twice per element instead of ten times
+  const int nlines = 10 * ti.nelem;
+  for (int t = tid; t < nlines; t += NT) {
+    const int e = t / 10, r = t - 10 * e;
+    const int a0 = r < 5 ? 5 * r : r - 5;  // first point: (j = r, 0) of a row, (0, i = r - 5) of a column
+    const int st = r < 5 ? 1 : 5;          // stride along the line
+    const uint16_t *le = s_lib + 25 * e + a0;
+    const int o = 25 * e + a0;
+    float2 *d = r < 5 ? s_d1 : s_d2;
+    line_derivs(P, s_u, le, st, d + o);
+    if (KERN) line_derivs(P, s_b, le, st, (r < 5 ? s_bd1 : s_bd2) + o);
+    if (PML && !LDDRK) line_derivs(P, s_uold, le, st, (r < 5 ? s_od1 : s_od2) + o);
+  }
+  __syncthreads();
+
+  // 4b. per GLL point: mapping, stress, memory variables, weak-form terms
+  //     (t1 = J (sigma . xi_x), t2 = J (sigma . gamma_x) overwrite the derivatives)
+  constexpr bool FIXQ = NT % 25 == 0;  // every thread keeps one GLL position
+  const int q0 = tid % 25, j0 = q0 / 5, i0 = q0 - 5 * j0;
   for (int f = tid; f < nq; f += NT) {
     const int e = f / 25;
-    const int q = f - 25 * e;
-    const int j = q / 5;
-    const int i = q - 5 * j;
+    const int q = FIXQ ? q0 : f - 25 * e;
+    const int j = FIXQ ? j0 : q / 5;
+    const int i = FIXQ ? i0 : q - 5 * j;
     const uint16_t *le = s_lib + 25 * e;
-    float dux_dxi = 0.f, duz_dxi = 0.f, dux_dg = 0.f, duz_dg = 0.f;
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-      const float2 r = s_u[le[5 * j + k]];
-      const float hx = s_h[5 * i + k];
-      dux_dxi += r.x * hx;
-      duz_dxi += r.y * hx;
-      const float2 c = s_u[le[5 * k + i]];
-      const float hz = s_h[5 * j + k];
-      dux_dg += c.x * hz;
-      duz_dg += c.y * hz;
-    }
-    const float4 g4 = s_geo[f];
-    const float2 m2 = s_mat[f];
+    // geometry and material straight from global memory (coalesced in f): not
+    // staging them keeps the tile's shared memory small and more tiles resident
+    const float4 g4 = __ldg(P.geo + ebase + f);
+    const float2 m2 = __ldg(P.mat + ebase + f);
+    const float2 d1 = s_d1[f], d2 = s_d2[f];
+    const float dux_dxi = d1.x, duz_dxi = d1.y, dux_dg = d2.x, duz_dg = d2.y;
     if (KERN) {
       // kernels of this adjoint step: adjoint displacement u' against the forward frame
-      float bdux_dxi = 0.f, bduz_dxi = 0.f, bdux_dg = 0.f, bduz_dg = 0.f;
-#pragma unroll
-      for (int k = 0; k < 5; ++k) {
-        const float2 r = s_b[le[5 * j + k]];
-        const float hx = s_h[5 * i + k];
-        bdux_dxi += r.x * hx;
-        bduz_dxi += r.y * hx;
-        const float2 c = s_b[le[5 * k + i]];
-        const float hz = s_h[5 * j + k];
-        bdux_dg += c.x * hz;
-        bduz_dg += c.y * hz;
-      }
+      const float2 b1 = s_bd1[f], b2 = s_bd2[f];
       float kap, muk;
-      kernel_point(dux_dxi, duz_dxi, dux_dg, duz_dg, bdux_dxi, bduz_dxi, bdux_dg, bduz_dg, g4, kap, muk);
+      kernel_point(dux_dxi, duz_dxi, dux_dg, duz_dg, b1.x, b1.y, b2.x, b2.y, g4, kap, muk);
       float2 km = P.kmu_kl[ebase + f];
       km.x = km.x + kap;
       km.y = km.y + muk;
@@ -455,32 +520,19 @@ __global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_
     const float lambdaplus2mu = lambdal + 2.f * mul;
     if (PML) {
       const int ps = ebase + f - 25 * P.pml_slot0;
-      const int region = P.pml_region[ti.elem_base + e - P.pml_slot0];
-      const PmlPoint c = pml_point(P.pml_coef, ps);
+      const PmlSet &c = P.pml_sets[P.pml_set_idx[ps]];
       // strains of the mid-step displacement
       float o_dux_dxl = 0.f, o_dux_dzl = 0.f, o_duz_dxl = 0.f, o_duz_dzl = 0.f;
       if (!LDDRK) {
-        float ox_xi = 0.f, oz_xi = 0.f, ox_g = 0.f, oz_g = 0.f;
-#pragma unroll
-        for (int k = 0; k < 5; ++k) {
-          const float2 r = s_uold[le[5 * j + k]];
-          const float hx = s_h[5 * i + k];
-          ox_xi += r.x * hx;
-          oz_xi += r.y * hx;
-          const float2 cc = s_uold[le[5 * k + i]];
-          const float hz = s_h[5 * j + k];
-          ox_g += cc.x * hz;
-          oz_g += cc.y * hz;
-        }
+        const float2 od1 = s_od1[f], od2 = s_od2[f];
+        const float ox_xi = od1.x, oz_xi = od1.y, ox_g = od2.x, oz_g = od2.y;
         o_dux_dxl = ox_xi * xixl + ox_g * gammaxl;
         o_dux_dzl = ox_xi * xizl + ox_g * gammazl;
         o_duz_dxl = oz_xi * xixl + oz_g * gammaxl;
         o_duz_dzl = oz_xi * xizl + oz_g * gammazl;
       }
-      const PmlConv cax = pml_conv(c.ax, P.DT), caz = pml_conv(c.az, P.DT);
-      const PmlConv cbx = pml_conv(c.bx, P.DT), cbz = pml_conv(c.bz, P.DT);
-      const PmlLik zx = pml_lik(c.kz, c.bz, c.az, c.kx, c.bx, c.ax, region, false);  // poles alpha_z, beta_x
-      const PmlLik xz = pml_lik(c.kx, c.bx, c.ax, c.kz, c.bz, c.az, region, true);   // poles alpha_x, beta_z
+      const PmlConv &cax = c.cax, &caz = c.caz, &cbx = c.cbx, &cbz = c.cbz;
+      const PmlLik &zx = c.zx, &xz = c.xz;  // poles (alpha_z, beta_x) and (alpha_x, beta_z)
       float4 r0 = P.pml_rm[3 * ps], r1 = P.pml_rm[3 * ps + 1], rd = P.pml_rm[3 * ps + 2];
       float4 l0 = make_float4(0.f, 0.f, 0.f, 0.f), l1 = l0, ld = l0;
       if (LDDRK) {
@@ -502,7 +554,7 @@ __global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_
       const float m_dux_dzl = static_cast<float>(xz.A0 * dux_dzl + xz.A1 * r1.x + xz.A2 * r1.y);
       const float m_duz_dzl = static_cast<float>(xz.A0 * duz_dzl + xz.A1 * r1.z + xz.A2 * r1.w);
       // the layer's acceleration terms at this point (pml_compute_accel_contribution.f90:187-333)
-      const PmlL Lc = pml_l(c.kx, c.bx, c.ax, c.kz, c.bz, c.az, region);  // poles alpha_x, alpha_z
+      const PmlL &Lc = c.l;  // poles alpha_x, alpha_z
       const int lq = le[q];
       const float2 uq = s_u[lq], vq = s_v[lq];
       const float2 uo = LDDRK ? make_float2(0.f, 0.f) : s_uold[lq];
@@ -527,8 +579,8 @@ __global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_
       const float szz = lambdaplus2mu * m_duz_dzl + lambdal * dux_dxl;
       const float szx = mul * (duz_dxl + m_dux_dzl);
       const float sxz = mul * (dux_dzl + m_duz_dxl);
-      s_geo[f] = make_float4(jacobianl * (sxx * xixl + szx * xizl), jacobianl * (sxz * xixl + szz * xizl),
-                             jacobianl * (sxx * gammaxl + szx * gammazl), jacobianl * (sxz * gammaxl + szz * gammazl));
+      s_d1[f] = make_float2(jacobianl * (sxx * xixl + szx * xizl), jacobianl * (sxz * xixl + szz * xizl));
+      s_d2[f] = make_float2(jacobianl * (sxx * gammaxl + szx * gammazl), jacobianl * (sxz * gammaxl + szz * gammazl));
       continue;
     }
     float sxx, szz, sxz;
@@ -557,39 +609,38 @@ __global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_
       sxz = sxz + mul * e13s;
       szz = szz + lambdalplusmul * e1s - 2.f * mul * e11s;
     }
-    s_geo[f] = make_float4(jacobianl * (sxx * xixl + sxz * xizl), jacobianl * (sxz * xixl + szz * xizl),
-                           jacobianl * (sxx * gammaxl + sxz * gammazl), jacobianl * (sxz * gammaxl + szz * gammazl));
+    s_d1[f] = make_float2(jacobianl * (sxx * xixl + sxz * xizl), jacobianl * (sxz * xixl + szz * xizl));
+    s_d2[f] = make_float2(jacobianl * (sxx * gammaxl + sxz * gammazl), jacobianl * (sxz * gammaxl + szz * gammazl));
   }
   __syncthreads();
 
-  // 5. weighted transpose contraction assembled straight into the accumulator,
-  //    one colour at a time (elements of a colour share no point)
+
+  // 4c. weighted transpose lines: rows contract t1 with hprimewgll, columns t2,
+  //     in place
+  for (int t = tid; t < nlines; t += NT) {
+    const int e = t / 10, r = t - 10 * e;
+    const int a0 = r < 5 ? 5 * r : r - 5;
+    const int st = r < 5 ? 1 : 5;
+    line_weighted(P, (r < 5 ? s_d1 : s_d2) + 25 * e + a0, st);
+  }
+  __syncthreads();
+
+  // 5. assembly into the accumulator, one colour at a time (elements of a
+  //    colour share no point): a -= wz * row term + wx * column term
   int cb = 0;
   for (int c = 0; c < ti.ncol; ++c) {
     const int ce = ti.col_end[c] * 25;
-    for (int f = cb + tid; f < ce; f += NT) {
+    for (int f = cb + tid; f < ce; f += NT) {  // cb is a multiple of 25: FIXQ positions hold
       const int e = f / 25;
-      const int q = f - 25 * e;
-      const int j = q / 5;
-      const int i = q - 5 * j;
-      const float4 *te = s_geo + 25 * e;
-      float tx1 = 0.f, tz1 = 0.f, tx2 = 0.f, tz2 = 0.f;
-#pragma unroll
-      for (int k = 0; k < 5; ++k) {
-        const float4 r = te[5 * j + k];
-        const float w1 = s_h[25 + 5 * k + i];
-        tx1 += r.x * w1;
-        tz1 += r.y * w1;
-        const float4 cc = te[5 * k + i];
-        const float w2 = s_h[25 + 5 * k + j];
-        tx2 += cc.z * w2;
-        tz2 += cc.w * w2;
-      }
+      const int q = FIXQ ? q0 : f - 25 * e;
+      const int j = FIXQ ? j0 : q / 5;
+      const int i = FIXQ ? i0 : q - 5 * j;
+      const float2 rt = s_d1[f], ct = s_d2[f];
       const float wz = s_h[55 + j], wx = s_h[50 + i];
       const int l = s_lib[f];
       float2 acc = s_acc[l];
-      acc.x -= wz * tx1 + wx * tx2;
-      acc.y -= wz * tz1 + wx * tz2;
+      acc.x -= wz * rt.x + wx * ct.x;
+      acc.y -= wz * rt.y + wx * ct.y;
       if (PML) {
         // the layer's terms after the element's weak-form terms (compute_forces_viscoelastic.F90:785-797)
         const float2 pm = s_pml[f];

@@ -8,7 +8,12 @@
 
 #include <cuda_runtime.h>
 
+#include <array>
 #include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <vector>
 
 namespace sf2d {
 
@@ -111,14 +116,69 @@ __device__ __forceinline__ void pml_update(float &r, float &rl, const PmlConv &c
   }
 }
 
-// Per-point damping data as the tile kernels read it: (K_x, K_z),
-// (alpha_x, alpha_z), (beta_x, beta_z).
-struct PmlPoint {
-  double kx, kz, ax, az, bx, bz;
+// Every coefficient one GLL point of a layer element needs, formed once on
+// the host from its region and (K, alpha, beta) in x and z: the strain
+// coefficients of the 31 form (zx, poles alpha_z, beta_x) and of the 13 form
+// (xz, poles alpha_x, beta_z), the field coefficients (poles alpha_x,
+// alpha_z) and the convolution weights of the four poles.  Points with equal
+// damping data share one set, so a layer along a straight edge needs a few
+// hundred sets and each point carries only the index of its set.
+struct alignas(16) PmlSet {
+  PmlLik zx, xz;
+  PmlL l;
+  PmlConv cax, caz, cbx, cbz;
+  double ax, az, bx, bz;  // the poles (LDDRK stages)
 };
-__device__ __forceinline__ PmlPoint pml_point(const double2 *coef, int ps) {
-  const double2 k = coef[3 * ps], a = coef[3 * ps + 1], b = coef[3 * ps + 2];
-  return PmlPoint{k.x, k.y, a.x, a.y, b.x, b.y};
+inline PmlSet pml_set(double kx, double kz, double ax, double az, double bx, double bz, int region, double DT) {
+  PmlSet s;
+  s.zx = pml_lik(kz, bz, az, kx, bx, ax, region, false);
+  s.xz = pml_lik(kx, bx, ax, kz, bz, az, region, true);
+  s.l = pml_l(kx, bx, ax, kz, bz, az, region);
+  s.cax = pml_conv(ax, DT);
+  s.caz = pml_conv(az, DT);
+  s.cbx = pml_conv(bx, DT);
+  s.cbz = pml_conv(bz, DT);
+  s.ax = ax;
+  s.az = az;
+  s.bx = bx;
+  s.bz = bz;
+  return s;
+}
+
+// The coefficient sets of the layer elements in slots [slot0, slot0 + nslots)
+// (slot -> element through elem_order), deduplicated on the exact bits of
+// (region, K_x, K_z, d_x, d_z, alpha_x, alpha_z); idx gets one set index per
+// GLL point in slot order.  Desc carries the per-point arrays pml_K_x ...
+// pml_alpha_z (double, [ispec][j][i]) and pml_region per element.
+template <typename Desc>
+void pml_build_sets(const Desc *d, const std::vector<int> &elem_order, int slot0, int nslots, double DT,
+                    std::vector<PmlSet> &sets, std::vector<int> &idx) {
+  std::map<std::array<uint64_t, 7>, int> seen;
+  auto bits = [](double x) {
+    uint64_t b;
+    std::memcpy(&b, &x, sizeof(b));
+    return b;
+  };
+  sets.clear();
+  idx.clear();
+  for (int s = slot0; s < slot0 + nslots; ++s) {
+    const int e = elem_order[s];
+    const int region = d->pml_region[e];
+    for (int q = 0; q < 25; ++q) {
+      const size_t p = static_cast<size_t>(e) * 25 + q;
+      const double kx = d->pml_K_x[p], kz = d->pml_K_z[p], dx = d->pml_d_x[p], dz = d->pml_d_z[p];
+      const double ax = d->pml_alpha_x[p], az = d->pml_alpha_z[p];
+      const std::array<uint64_t, 7> key{static_cast<uint64_t>(region), bits(kx), bits(kz), bits(dx), bits(dz),
+                                        bits(ax), bits(az)};
+      auto it = seen.find(key);
+      if (it == seen.end()) {
+        // beta = alpha + d / K (pml_compute_memory_variables.f90:164-165)
+        sets.push_back(pml_set(kx, kz, ax, az, ax + dx / kx, az + dz / kz, region, DT));
+        it = seen.emplace(key, static_cast<int>(sets.size()) - 1).first;
+      }
+      idx.push_back(it->second);
+    }
+  }
 }
 
 }  // namespace sf2d

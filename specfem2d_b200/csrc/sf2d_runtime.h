@@ -45,6 +45,7 @@ TileKernel pick_tile_kernel(bool aniso, bool atten, bool lddrk) {
 inline TileKernel pick_pml_kernel(int nt, bool lddrk) {
   switch (nt) {
     case 128: return lddrk ? k_elastic_tile<128, false, false, true, false, true> : k_elastic_tile<128, false, false, false, false, true>;
+    case 250: return lddrk ? k_elastic_tile<250, false, false, true, false, true> : k_elastic_tile<250, false, false, false, false, true>;
     case 512: return lddrk ? k_elastic_tile<512, false, false, true, false, true> : k_elastic_tile<512, false, false, false, false, true>;
     default: return lddrk ? k_elastic_tile<256, false, false, true, false, true> : k_elastic_tile<256, false, false, false, false, true>;
   }
@@ -53,9 +54,56 @@ inline TileKernel pick_pml_kernel(int nt, bool lddrk) {
 inline TileKernel pick_tile_kernel(int nt, bool aniso, bool atten, bool lddrk, bool kern) {
   switch (nt) {
     case 128: return kern ? pick_tile_kernel<128, true>(aniso, atten, lddrk) : pick_tile_kernel<128, false>(aniso, atten, lddrk);
+    case 250: return kern ? pick_tile_kernel<250, true>(aniso, atten, lddrk) : pick_tile_kernel<250, false>(aniso, atten, lddrk);
     case 512: return kern ? pick_tile_kernel<512, true>(aniso, atten, lddrk) : pick_tile_kernel<512, false>(aniso, atten, lddrk);
     default: return kern ? pick_tile_kernel<256, true>(aniso, atten, lddrk) : pick_tile_kernel<256, false>(aniso, atten, lddrk);
   }
+}
+
+// Boundary terms of each tile grouped by receiving point, so that one thread
+// per point applies them (in parallel over points, in the reference's order at
+// each point: Stacey, coupling, sources).  groups: one int4 per point (local
+// point, first index into idx, Stacey count | coupling count << 8, source
+// count); idx: the point's entries of each type in their list order.  The
+// *_local vectors give each entry's tile-local point; tiles' st/cpl/src
+// ranges index them.  Sets grp_off / grp_n of every tile.
+inline std::string build_boundary_groups(std::vector<TileInfo> &tiles, const std::vector<int> &st_local,
+                                         const std::vector<int> &cpl_local, const std::vector<int> &src_local,
+                                         std::vector<int4> &groups, std::vector<int> &idx) {
+  groups.clear();
+  idx.clear();
+  std::vector<std::vector<int>> st, cp, sr;
+  std::vector<int> pts;
+  for (TileInfo &t : tiles) {
+    t.grp_off = static_cast<int>(groups.size());
+    pts.clear();
+    auto add = [&](std::vector<std::vector<int>> &lists, int l, int k) {
+      if (static_cast<int>(st.size()) <= l) {
+        st.resize(l + 1);
+        cp.resize(l + 1);
+        sr.resize(l + 1);
+      }
+      if (st[l].empty() && cp[l].empty() && sr[l].empty()) pts.push_back(l);
+      lists[l].push_back(k);
+    };
+    for (int k = t.st_off; k < t.st_off + t.st_n; ++k) add(st, st_local[k], k);
+    for (int k = t.cpl_off; k < t.cpl_off + t.cpl_n; ++k) add(cp, cpl_local[k], k);
+    for (int k = t.src_off; k < t.src_off + t.src_n; ++k) add(sr, src_local[k], k);
+    std::sort(pts.begin(), pts.end());
+    for (int l : pts) {
+      if (st[l].size() > 255 || cp[l].size() > 255) return "more than 255 boundary entries at one point";
+      groups.push_back(make_int4(l, static_cast<int>(idx.size()),
+                                 static_cast<int>(st[l].size() | (cp[l].size() << 8)), static_cast<int>(sr[l].size())));
+      for (int k : st[l]) idx.push_back(k);
+      for (int k : cp[l]) idx.push_back(k);
+      for (int k : sr[l]) idx.push_back(k);
+      st[l].clear();
+      cp[l].clear();
+      sr[l].clear();
+    }
+    t.grp_n = static_cast<int>(groups.size()) - t.grp_off;
+  }
+  return "";
 }
 
 }  // namespace sf2d
@@ -109,12 +157,37 @@ struct sf2d_solver {
   int *ctr = nullptr;  // device ints: step, status, step shadow, frame base, kernel frame base
   float *d_stf = nullptr;
   size_t nq = 0;
+  // tile-local point of every Stacey and source entry, kept to regroup the
+  // boundary terms when coupling entries are added
+  std::vector<int> h_st_local, h_src_local;
 
+  // With both tile groups present, the CPML tiles run on a side stream beside
+  // the other tiles (the two write disjoint points and slots), joined before
+  // the shared-point kernel: their longer latency hides behind the bulk.
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  int make_side_stream() {
+    if (side || !(pml_tile0 > 0 && pml_tile0 < T.ntiles)) return SF2D_OK;
+    SF2D_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    SF2D_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    SF2D_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+    return SF2D_OK;
+  }
   void launch_tile(bool record_prev, int stage) {
-    if (pml_tile0 > 0) tile_fn<<<pml_tile0, nt, smem, stream>>>(P, record_prev ? 1 : 0, stage, 0);
+    const int rp = record_prev ? 1 : 0;
+    if (side) {
+      cudaEventRecord(ev_fork, stream);
+      cudaStreamWaitEvent(side, ev_fork, 0);
+      pml_fn<<<T.ntiles - pml_tile0, nt, pml_smem, side>>>(P, rp, stage, pml_tile0);
+      cudaEventRecord(ev_join, side);
+      tile_fn<<<pml_tile0, nt, smem, stream>>>(P, rp, stage, 0);
+      cudaStreamWaitEvent(stream, ev_join, 0);
+      return;
+    }
+    if (pml_tile0 > 0) tile_fn<<<pml_tile0, nt, smem, stream>>>(P, rp, stage, 0);
     if (pml_tile0 < T.ntiles)
-      (pml_fn ? pml_fn : tile_fn)<<<T.ntiles - pml_tile0, nt, pml_fn ? pml_smem : smem, stream>>>(
-          P, record_prev ? 1 : 0, stage, pml_tile0);
+      (pml_fn ? pml_fn : tile_fn)<<<T.ntiles - pml_tile0, nt, pml_fn ? pml_smem : smem, stream>>>(P, rp, stage,
+                                                                                                   pml_tile0);
   }
   void launch_shared(int stage) {
     const int nb = std::max(1, (P.nshared + sf2d::SHARED_NT - 1) / sf2d::SHARED_NT);
@@ -146,6 +219,9 @@ struct sf2d_solver {
   ~sf2d_solver() {
     if (graph) cudaGraphExecDestroy(graph);
     for (void *p : allocs) cudaFree(p);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (side) cudaStreamDestroy(side);
     if (stream) cudaStreamDestroy(stream);
   }
 };

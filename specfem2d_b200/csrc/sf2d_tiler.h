@@ -36,7 +36,7 @@ struct TileInfo {
   int lib_off;     // offset of the tile's local ibool (multiple of 8 entries = 16 bytes)
   int cpl_off, cpl_n;  // fluid-solid coupling entries of this tile (none outside a coupled run)
   int edge_off, edge_n;  // local points on the outer edge of a CPML layer, zeroed every step
-  int pad_[2];
+  int grp_off, grp_n;    // points that receive boundary, coupling or source terms (one thread each)
 };
 static_assert(sizeof(TileInfo) == 28 * 4, "TileInfo layout");
 

@@ -239,6 +239,32 @@ def build_desc(db, tile_elems: int = 32, seismotype: int = 1, threads_per_block:
     return d, keep
 
 
+def time_desc(db, tile_elems: int = 32, threads_per_block: int = 256):
+    """sf2d_elastic_desc with no element: the time stepping and GLL members of
+    `db` only (the solid side of a fluid-only coupled run)."""
+    keep = []
+
+    def f(a):
+        arr = np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+        keep.append(arr)
+        return arr.ctypes.data_as(_f)
+
+    from .setup.solver_setup import ALPHA_LDDRK, BETA_LDDRK
+
+    g = db.gll
+    d = ElasticDesc()
+    d.hprime, d.hprimewgll, d.wxgll, d.wzgll = f(g.hprime), f(g.hprimewgll), f(g.wxgll), f(g.wzgll)
+    d.nstep = db.nstep
+    d.deltat, d.deltatover2, d.deltatsquareover2 = (float(db.deltat), float(db.deltatover2),
+                                                    float(db.deltatsquareover2))
+    d.tile_elems, d.threads_per_block = tile_elems, threads_per_block
+    d.time_scheme = int(db.time_scheme)
+    d.nstage = int(db.stf.shape[2])
+    d.alpha_lddrk, d.beta_lddrk = f(ALPHA_LDDRK), f(BETA_LDDRK)
+    d.seismotype = 1
+    return d, keep
+
+
 class ElasticSolver:
     """Device-resident elastic solver (Newmark or LDDRK) for one Database."""
 

@@ -70,7 +70,7 @@ def oracle_1500(tromp):
     return ref, o.displ.copy(), o.veloc.copy(), o64.veloc.copy()
 
 
-@pytest.mark.parametrize("tile_elems,threads", [(8, 128), (25, 256), (64, 512), (128, 256)])
+@pytest.mark.parametrize("tile_elems,threads", [(8, 128), (25, 256), (64, 512), (128, 256), (32, 250), (10, 250)])
 def test_tile_size_invariance(tromp, oracle_1500, tile_elems, threads):
     from specfem2d_b200.runtime import ElasticSolver
 

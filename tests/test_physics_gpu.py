@@ -26,21 +26,22 @@ def _compare(db, nstep, **solver_kw):
     return s, ref, d, o.displ
 
 
-def test_anisotropic_gpu_matches_oracle_and_golden():
+@pytest.mark.parametrize("threads", [256, 250])
+def test_anisotropic_gpu_matches_oracle_and_golden(threads):
     cfg, golden = load_golden("anisotropic_isotropic_model")
     db = database_from_config(cfg)
-    s, ref, d, d_or = _compare(db, db.nstep)
+    s, ref, d, d_or = _compare(db, db.nstep, threads_per_block=threads)
     assert rel_l2(s, ref) < TOL
     assert rel_l2(d, d_or) < TOL
     assert rel_l2(s[0, :, 0], golden["S0001_BXX"]) < TOL
     assert rel_l2(s[0, :, 1], golden["S0001_BXZ"]) < TOL
 
 
-@pytest.mark.parametrize("tile_elems", [16, 64])
-def test_viscoelastic_newmark_gpu_matches_oracle_and_golden(tile_elems):
+@pytest.mark.parametrize("tile_elems,threads", [(16, 256), (64, 256), (32, 250)])
+def test_viscoelastic_newmark_gpu_matches_oracle_and_golden(tile_elems, threads):
     cfg, golden = load_golden("attenuation_viscoelastic")
     db = database_from_config(cfg, absorbing_as_stacey=True)
-    s, ref, d, d_or = _compare(db, db.nstep, tile_elems=tile_elems)
+    s, ref, d, d_or = _compare(db, db.nstep, tile_elems=tile_elems, threads_per_block=threads)
     assert rel_l2(s, ref) < TOL
     assert rel_l2(d, d_or) < TOL
     t = float(golden["t_first"]) + float(golden["t_step"]) * np.arange(db.nstep)
@@ -57,10 +58,11 @@ def test_lddrk_elastic_gpu_matches_oracle():
     assert rel_l2(d, d_or) < TOL
 
 
-def test_lddrk_viscoelastic_gpu_matches_oracle():
+@pytest.mark.parametrize("threads", [256, 250])
+def test_lddrk_viscoelastic_gpu_matches_oracle(threads):
     cfg, _ = load_golden("attenuation_viscoelastic")
     db = database_from_config(cfg, absorbing_as_stacey=True, time_scheme=2)
-    s, ref, d, d_or = _compare(db, db.nstep, tile_elems=32)
+    s, ref, d, d_or = _compare(db, db.nstep, tile_elems=32, threads_per_block=threads)
     assert rel_l2(s, ref) < TOL
     assert rel_l2(d, d_or) < TOL
 

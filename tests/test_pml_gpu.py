@@ -54,6 +54,26 @@ def test_semi_infinite_cpml_fields_and_layer_absorbs():
     assert _close(u_gpu, o32.displ, o64.displ, 2.0)
 
 
+def test_fluid_only_cpml_pressure_matches_oracle_and_ref_seis():
+    """EXAMPLES/check_absolute_amplitude_of_pressure_source_seismograms_acoustic:
+    a fluid-only mesh (no solid sub-solver) with CPML on all sides (492 layer
+    elements), a Gaussian pressure source with USE_TRICK_FOR_BETTER_PRESSURE
+    and one pressure receiver."""
+    import oracle
+    from specfem2d_b200.coupled import CoupledSolver
+
+    cfg, seis = load_golden("pressure_source_acoustic")
+    db = database_from_config(cfg)
+    assert int((db.pml["region"] > 0).sum()) == 492 and db.seismotype == 4
+    s = CoupledSolver(db)
+    gpu = s.run(db.nstep)
+    o32 = oracle.Oracle(db, 4).run(db.nstep)
+    o64 = oracle.Oracle(db, 8).run(db.nstep)
+    assert _close(gpu, o32, o64, 2.0)
+    assert rel_l2(gpu[0, :, 0], seis["S0001_PRE"]) < 1e-5
+    assert s.launch_count(64) > 0
+
+
 @pytest.fixture(scope="module")
 def c2_pml():
     db = configs.c2_coupled(nstep=1200, nrec=24, scale=8, pml_thickness=3)
@@ -77,6 +97,19 @@ def test_coupled_cpml_pressure_and_fields(c2_pml):
     assert _close(gpu, r32, r64)
     assert _close(f["displ"], o32.displ, o64.displ, 2.0)
     assert _close(f["pot"], o32.get(oracle.POT), o64.get(oracle.POT), 2.0)
+
+
+def test_coupled_cpml_250_threads(c2_pml):
+    """250-thread CTAs (one GLL position per thread, hprime rows in
+    registers) in both domains' tile kernels, with and without the layer."""
+    import oracle
+    from specfem2d_b200.coupled import CoupledSolver
+
+    db = c2_pml
+    gpu = CoupledSolver(db, threads_per_block=250).run(600)
+    r32 = oracle.Oracle(db, 4).run(600)
+    r64 = oracle.Oracle(db, 8).run(600)
+    assert _close(gpu, r32, r64)
 
 
 def test_coupled_cpml_lddrk(c2_pml):
