@@ -164,20 +164,26 @@ def run_reference_fwi(args, rank):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle  # noqa: E402  (reference arm only)
 
-    models = fwi_members(args.models, args.fwi_steps)
+    models = fwi_members(args.models, args.fwi_steps, args.fwi_set)
     db = min(models, key=lambda m: m.nspec)
     t0 = time.perf_counter()
     oracle.gradient(db, np.zeros((len(db.rec_ispec), db.nstep, 2)), checkpoint_every=100, precision=4)
-    dt = time.perf_counter() - t0
+    t_sample = time.perf_counter() - t0
+    # per shot of the workload: the sample's time scaled by the mean point count
+    scale = float(np.mean([m.nglob for m in models])) / float(db.nglob)
+    dt = t_sample * scale
     threads = oracle.max_threads()
     line = {"metric": "s per FWI gradient per shot", "value": dt, "unit": "s", "impl": "reference",
             "n_gpus": args.gpus, "steps": args.fwi_steps, "warmup": 0, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": args.workload, "description": FWI_WORKLOADS[args.workload],
-                       "sample_nspec": db.nspec},
+                       "model_set": args.fwi_set, "models": len(models), "sample_nspec": db.nspec,
+                       "sample_seconds": t_sample},
             "cpu_baseline": {"value": dt, "unit": "s", "cores": threads, "kind": "port",
                              "sample": f"one gradient of the smallest model ({db.nspec} elements, "
-                                       f"{db.nstep} steps), C++ restatement of the reference CPU solver"},
+                                       f"{db.nstep} steps, {t_sample:.1f} s) scaled by the mean point count "
+                                       f"of the {len(models)} models (x{scale:.2f}); C++ restatement of the "
+                                       "reference CPU solver"},
             "e2e": {"value": dt, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -212,17 +218,20 @@ FWI_WORKLOADS = {
 }
 
 
-def fwi_members(n_models: int, nstep: int):
+def fwi_members(n_models: int, nstep: int, which: str = "first"):
+    """The first n_models of the 48 seeded model sizes, or the n_models smallest."""
     from specfem2d_b200 import configs
 
     os.makedirs(CACHE, exist_ok=True)
-    path = os.path.join(CACHE, f"c5_models_{n_models}_{nstep}.pkl")
+    path = os.path.join(CACHE, f"c5_models_{which}_{n_models}_{nstep}.pkl")
     if os.path.exists(path):
         with open(path, "rb") as f:
             return pickle.load(f)
-    sizes = configs.c5_model_sizes()[:n_models]
-    models = [configs.random_layered_model(seed=100 + k, nx=nx, nz=nz, nstep=nstep) for k, (nx, nz) in
-              enumerate(sizes)]
+    sizes = list(enumerate(configs.c5_model_sizes()))
+    if which == "smallest":
+        sizes = sorted(sizes, key=lambda kv: kv[1][0] * kv[1][1])
+    sizes = sizes[:n_models]
+    models = [configs.random_layered_model(seed=100 + k, nx=nx, nz=nz, nstep=nstep) for k, (nx, nz) in sizes]
     with open(path, "wb") as f:
         pickle.dump(models, f)
     return models
@@ -238,7 +247,7 @@ def run_fwi(args, rank, world):
     from specfem2d_b200.fwi import FWIGradient
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    models = fwi_members(args.models, args.fwi_steps)
+    models = fwi_members(args.models, args.fwi_steps, args.fwi_set)
     every = 100
     nq = sum(m.nspec for m in models)
 
@@ -274,6 +283,7 @@ def run_fwi(args, rank, world):
         "steps": args.fwi_steps, "warmup": 1, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": args.workload, "description": FWI_WORKLOADS[args.workload], "models": n,
+                   "model_set": args.fwi_set, "sizes": [[int(m.nspec), int(m.nglob)] for m in models],
                    "nspec_total": nq, "nglob_total": int(packed.nglob), "checkpoint_every": every,
                    "tile_elems": args.tile_elems, "threads_per_cta": args.threads},
         "plain_s_per_shot": plain_s / n, "batched_s_per_shot": batched_s / n,
@@ -294,8 +304,12 @@ def main():
     ap.add_argument("--workload", default="c2_coupled", choices=sorted(WORKLOAD_DESC) + sorted(FWI_WORKLOADS))
     ap.add_argument("--models", type=int, default=12, help="models of the FWI workload")
     ap.add_argument("--fwi-steps", type=int, default=1000, help="time steps of each FWI model")
+    ap.add_argument("--fwi-set", default="first", choices=["first", "smallest"],
+                    help="the first --models of the 48 seeded sizes, or the smallest")
     ap.add_argument("--tile-elems", type=int, default=32)
     ap.add_argument("--threads", type=int, default=256)
+    ap.add_argument("--fluid-tile-elems", type=int, default=0, help="fluid tiles (coupled runs); 0 = --tile-elems")
+    ap.add_argument("--fluid-threads", type=int, default=0, help="fluid CTA threads; 0 = --threads")
     ap.add_argument("--autotune", action="store_true", help="pick tile size and threads per CTA first")
     ap.add_argument("--ref-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -342,8 +356,10 @@ def main():
         (args.tile_elems, args.threads), tune = autotune_elastic(db, tiles=(48, 64, 96), threads=(256, 512))
 
     def make_solver():
-        cls = CoupledSolver if coupled else ElasticSolver
-        return cls(db, tile_elems=args.tile_elems, threads_per_block=args.threads)
+        if coupled:
+            return CoupledSolver(db, tile_elems=args.tile_elems, threads_per_block=args.threads,
+                                 fluid_tile_elems=args.fluid_tile_elems, fluid_threads_per_block=args.fluid_threads)
+        return ElasticSolver(db, tile_elems=args.tile_elems, threads_per_block=args.threads)
 
     solver = make_solver()
     el_db = solver.sub_db if coupled else db   # the solid part the element-kernel roofline refers to
@@ -455,6 +471,8 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": args.workload, "description": WORKLOAD_DESC[args.workload],
                    "nspec": db.nspec, "nglob": db.nglob, "tile_elems": args.tile_elems,
+                   "fluid_tile_elems": args.fluid_tile_elems or args.tile_elems,
+                   "fluid_threads_per_cta": args.fluid_threads or args.threads,
                    "threads_per_cta": args.threads, "autotuned": bool(tune),
                    "ntiles": st["ntiles"], "shared_points": nsh,
                    "nspec_fluid": solver.nspec_fluid if coupled else 0,

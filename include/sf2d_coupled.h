@@ -69,6 +69,7 @@ typedef struct {
   int npml_edge;
   const int *pml_edge_iglob;
   double pml_dt;
+  int threads_per_block;                     /* fluid tile kernel: 128, 250, 256 or 512; 0 = the solid's */
 } sf2d_acoustic_desc;
 
 typedef struct {

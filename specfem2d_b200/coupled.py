@@ -37,6 +37,7 @@ class AcousticDesc(ctypes.Structure):
         ("pml_K_x", _d), ("pml_K_z", _d), ("pml_d_x", _d), ("pml_d_z", _d), ("pml_alpha_x", _d), ("pml_alpha_z", _d),
         ("npml_edge", ctypes.c_int), ("pml_edge_iglob", _i),
         ("pml_dt", ctypes.c_double),
+        ("threads_per_block", ctypes.c_int),
     ]
 
 
@@ -183,7 +184,9 @@ def split(db):
 class CoupledSolver:
     """Device-resident coupled fluid-solid solver for one Database."""
 
-    def __init__(self, db, tile_elems: int = 32, threads_per_block: int = 256):
+    def __init__(self, db, tile_elems: int = 32, threads_per_block: int = 256, fluid_tile_elems: int = 0,
+                 fluid_threads_per_block: int = 0):
+        """Tile sizes and threads per CTA of the solid; the fluid's default to the same."""
         lib = _lib()
         sub, fl, cp, maps = split(db)
         seismotype = int(getattr(db, "seismotype", 1))
@@ -221,7 +224,8 @@ class CoupledSolver:
         a.sourcearrays, a.stf = f(fl["sourcearrays"]), f(fl["stf"])
         a.nrec, a.rec_ispec = len(fl["rec_ispec"]), i(fl["rec_ispec"])
         a.hxir, a.hgammar, a.rec_global = dd(fl["hxir"]), dd(fl["hgammar"]), i(fl["rec_global"])
-        a.tile_elems = tile_elems
+        a.tile_elems = fluid_tile_elems or tile_elems
+        a.threads_per_block = fluid_threads_per_block
         fp = fl["pml"]
         if fp is not None:
             a.pml_region = i(fp["region"])

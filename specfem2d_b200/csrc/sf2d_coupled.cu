@@ -303,6 +303,11 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
     C->nt = S->nt;
   }
   if (ad->nsrc > 0 && eld->nstage != C->nstage) return fail(SF2D_ERR_INVALID, "stf must hold one value per step and stage");
+  if (ad->threads_per_block > 0) {
+    C->nt = ad->threads_per_block;
+    if (C->nt != 128 && C->nt != 250 && C->nt != 256 && C->nt != 512)
+      return fail(SF2D_ERR_INVALID, "threads_per_block must be 128, 250, 256 or 512");
+  }
   C->nstep = eld->nstep;
   C->nrec_total = cp->nrec_total;
   int rc = 0;

@@ -326,8 +326,19 @@ __device__ __forceinline__ void line_weighted(const Params &P, float2 *buf, int 
 // the extra acceleration terms (pml_compute_memory_variables.f90:230-540,
 // pml_compute_accel_contribution.f90:187-333, compute_forces_viscoelastic.F90:600-675, 785-797).
 // Tiles [tile0, tile0 + gridDim.x) are advanced.
+// Resident threads per SM the variants ask for: 1536 for the plain ones (6
+// CTAs of 256, at most 40 registers; with the geometry read from global memory
+// the tile's shared memory allows it, and the extra warps hide the loads'
+// latency), 768 for the anisotropic, attenuating, kernel and CPML ones (at
+// most 80 registers; left unbounded the compiler takes over 130 and one CTA
+// fits an SM).
+template <int NT, bool ANISO, bool ATTEN, bool KERN, bool PML>
+constexpr int tile_min_blocks() {
+  return (ANISO || ATTEN || KERN || PML) ? 768 / NT : 1536 / NT;
+}
 template <int NT, bool ANISO, bool ATTEN, bool LDDRK, bool KERN, bool PML = false>
-__global__ void __launch_bounds__(NT) k_elastic_tile(const Params P, int record_prev, int stage, int tile0) {
+__global__ void __launch_bounds__(NT, tile_min_blocks<NT, ANISO, ATTEN, KERN, PML>())
+    k_elastic_tile(const Params P, int record_prev, int stage, int tile0) {
   extern __shared__ __align__(16) unsigned char smem[];
   const TileInfo &ti = P.tiles[tile0 + blockIdx.x];
   const int tid = threadIdx.x;
