@@ -101,12 +101,18 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "50", "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                 "-lms", "100", "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
                 text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except OSError:
             self.proc = None
+            return
+        # nvidia-smi's start-up (NVML initialisation) must not overlap the timed
+        # region: wait for its first two samples
+        t0 = time.time()
+        while len(self.lines) < 2 and time.time() - t0 < 15.0 and self.proc.poll() is None:
+            time.sleep(0.02)
 
     def _read(self):
         for ln in self.proc.stdout:
@@ -365,7 +371,9 @@ def main():
     el_db = solver.sub_db if coupled else db   # the solid part the element-kernel roofline refers to
     stream = torch.cuda.ExternalStream(solver.stream_handle())
 
-    # warm-up, then the timed region: K steps queued as CUDA graphs on the solver stream
+    # graph built and uploaded outside the timed region, warm-up, then the timed
+    # region: K steps queued as CUDA graphs on the solver stream
+    solver.prepare()
     solver.enqueue(W)
     solver.synchronize(600)
     if dist:

@@ -136,6 +136,9 @@ int sf2d_run(sf2d_solver *s, int nstep, double *seismograms);
  * stream (CUDA graphs of fixed step chunks).  sf2d_synchronize waits (with a
  * timeout in seconds, <= 0 meaning none) and returns the stability status. */
 int sf2d_enqueue(sf2d_solver *s, int nstep);
+/* Builds and uploads the CUDA graph of one step chunk now (capture runs
+ * nothing), so that a later sf2d_enqueue starts without that host work. */
+int sf2d_prepare(sf2d_solver *s);
 int sf2d_synchronize(sf2d_solver *s, double timeout_s);
 
 /* Copies receiver traces [it0, it0+nstep) already recorded on the device. */

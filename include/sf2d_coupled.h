@@ -108,6 +108,7 @@ int sf2d_coupled_run(sf2d_coupled *c, int nstep, double *seismograms);
  * chunks on the solver's stream); sf2d_coupled_synchronize waits for them and
  * returns the stability status; sf2d_coupled_get_stream gives the stream. */
 int sf2d_coupled_enqueue(sf2d_coupled *c, int nstep);
+int sf2d_coupled_prepare(sf2d_coupled *c);  /* as sf2d_prepare */
 int sf2d_coupled_synchronize(sf2d_coupled *c);
 int sf2d_coupled_get_stream(sf2d_coupled *c, void **stream);
 /* Fields in the sub-mesh numberings: displ/veloc/accel solid nglob*2,

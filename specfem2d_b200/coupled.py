@@ -68,12 +68,13 @@ def _lib():
         lib.sf2d_coupled_layout_info.argtypes = [_vp, ctypes.POINTER(ctypes.c_longlong)]
         lib.sf2d_coupled_destroy.argtypes = [_vp]
         lib.sf2d_coupled_enqueue.argtypes = [_vp, ctypes.c_int]
+        lib.sf2d_coupled_prepare.argtypes = [_vp]
         lib.sf2d_coupled_synchronize.argtypes = [_vp]
         lib.sf2d_coupled_get_stream.argtypes = [_vp, ctypes.POINTER(_vp)]
         lib.sf2d_coupled_solid_layout_info.argtypes = [_vp, ctypes.POINTER(ctypes.c_longlong)]
         lib.sf2d_coupled_launch_count.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]
         for n in ("create", "run", "get_fields", "set_fields", "time_kernels", "layout_info", "destroy",
-                  "enqueue", "synchronize", "get_stream", "solid_layout_info", "launch_count"):
+                  "enqueue", "synchronize", "get_stream", "solid_layout_info", "launch_count", "prepare"):
             getattr(lib, "sf2d_coupled_" + n).restype = ctypes.c_int
         lib._coupled_sigs = True
     return lib
@@ -275,6 +276,10 @@ class CoupledSolver:
 
     def enqueue(self, nstep: int):
         _check(self._lib.sf2d_coupled_enqueue(self._h, nstep))
+
+    def prepare(self):
+        """Build the step-chunk graph ahead of the first enqueue (runs nothing)."""
+        _check(self._lib.sf2d_coupled_prepare(self._h))
 
     def synchronize(self, timeout_s: float = 0.0):
         _check(self._lib.sf2d_coupled_synchronize(self._h))

@@ -50,7 +50,7 @@ struct AcParams {
   const float *fac;           // jacobian / rho formed in FP32
   const int *sh_ids;
   float *partial;
-  const int *shp_off, *shp_slots;
+  const int *shp_off, *slot_pos;  // point-major partial sums, as in the solid kernels
   const int4 *bgroups;        // per tile (grp_off, grp_n): point, first idx, Stacey | coupling << 8, sources
   const int *bnd_idx;         // entries of each group
   const int *st_local;
@@ -329,6 +329,14 @@ __global__ void __launch_bounds__(NT) k_acoustic_tile(const AcParams A, int reco
     s_acc[l] = acc;
   }
 
+  // the first point's geometry and J/rho are requested now (see the solid kernel)
+  float4 g_next = make_float4(0.f, 0.f, 0.f, 0.f);
+  float fac_next = 0.f;
+  if (tid < nq) {
+    g_next = __ldg(A.geo + ebase + tid);
+    fac_next = __ldg(A.fac + ebase + tid);
+  }
+
   // 4a. derivative lines: one thread per element row (xi) or column (gamma),
   //     hprime from the kernel's constant bank (see the solid kernel)
   const int nlines = 10 * ti.nelem;
@@ -354,7 +362,13 @@ __global__ void __launch_bounds__(NT) k_acoustic_tile(const AcParams A, int reco
     const int i = FIXQ ? i0 : q - 5 * j;
     const uint16_t *le = s_lib + 25 * e;
     const float dxi = s_d1[f], dgam = s_d2[f];
-    const float4 g4 = __ldg(A.geo + ebase + f);  // geometry from global memory, as in the solid kernel
+    // geometry from global memory, the next point's requested before this one is computed
+    const float4 g4 = g_next;
+    const float fac = fac_next;
+    if (f + NT < nq) {
+      g_next = __ldg(A.geo + ebase + f + NT);
+      fac_next = __ldg(A.fac + ebase + f + NT);
+    }
     float dxl = dxi * g4.x + dgam * g4.z;
     float dzl = dxi * g4.y + dgam * g4.w;
     if (PML) {
@@ -401,7 +415,6 @@ __global__ void __launch_bounds__(NT) k_acoustic_tile(const AcParams A, int reco
         A.pml_rm_l[3 * ps + 2] = lp;
       }
     }
-    const float fac = __ldg(A.fac + ebase + f);
     s_d1[f] = fac * (g4.x * dxl + g4.y * dzl);
     s_d2[f] = fac * (g4.z * dxl + g4.w * dzl);
   }
@@ -433,13 +446,32 @@ __global__ void __launch_bounds__(NT) k_acoustic_tile(const AcParams A, int reco
     __syncthreads();
   }
 
-  // 6. mass, corrector or LDDRK update, free surface, write-back
+  // 6. mass, corrector or LDDRK update, free surface, write-back (each
+  //    point's rmass, mask or slot requested one iteration ahead)
   bool bad = false;
+  float rm_next = 0.f;
+  uint8_t fm_next = 0;
+  int sp_next = 0;
+  if (tid < n_int) {
+    rm_next = A.rmass[int_begin + tid];
+    fm_next = A.free_mask[int_begin + tid];
+  } else if (tid < nl) {
+    sp_next = A.slot_pos[ti.sh_off + tid - n_int];
+  }
   for (int l = tid; l < nl; l += NT) {
     const float acc = s_acc[l];
+    const float rm = rm_next;
+    const uint8_t fm = fm_next;
+    const int sp = sp_next;
+    if (l + NT < n_int) {
+      rm_next = A.rmass[int_begin + l + NT];
+      fm_next = A.free_mask[int_begin + l + NT];
+    } else if (l + NT < nl) {
+      sp_next = A.slot_pos[ti.sh_off + l + NT - n_int];
+    }
     if (l < n_int) {
       const int g = int_begin + l;
-      float pdd = acc * A.rmass[g];
+      float pdd = acc * rm;
       float pd = s_pd[l], p = s_p[l];
       if (!LDDRK) {
         pd = newmark_veloc(pd, pdd, dto2);
@@ -453,7 +485,7 @@ __global__ void __launch_bounds__(NT) k_acoustic_tile(const AcParams A, int reco
         A.pdL[g] = pdl;
         A.pL[g] = pl;
       }
-      if (A.free_mask[g]) {
+      if (fm) {
         p = 0.f;
         pd = 0.f;
         pdd = 0.f;
@@ -464,7 +496,7 @@ __global__ void __launch_bounds__(NT) k_acoustic_tile(const AcParams A, int reco
       if (PML && !LDDRK && A.pold) A.pold[g] = s_pold[l];
       bad |= !(fabsf(p) < 1e25f);
     } else {
-      A.partial[ti.sh_off + l - n_int] = acc;
+      A.partial[sp] = acc;
     }
   }
   if (bad) *A.d_status = 1;
@@ -492,7 +524,7 @@ __global__ void __launch_bounds__(SHARED_NT) k_acoustic_shared(const AcParams A,
       pd = 0.f;
     }
     float acc = 0.f;
-    for (int k = A.shp_off[s]; k < A.shp_off[s + 1]; ++k) acc += A.partial[A.shp_slots[k]];
+    for (int k = A.shp_off[s]; k < A.shp_off[s + 1]; ++k) acc += A.partial[k];
     float pdd = acc * A.rmass[g];
     if (!LDDRK) {
       pd = newmark_veloc(pd, pdd, A.dto2);

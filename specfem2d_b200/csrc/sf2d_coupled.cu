@@ -421,6 +421,8 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
   }
   for (const TileInfo &t : tiles)
     if (t.rec_n > C->nt) return fail(SF2D_ERR_INVALID, "more fluid receivers in one tile than threads per CTA");
+  std::vector<int> slot_pos(T.shp_slots.size());
+  for (size_t k = 0; k < T.shp_slots.size(); ++k) slot_pos[T.shp_slots[k]] = static_cast<int>(k);
   std::vector<int4> bgroups;
   std::vector<int> bnd_idx;
   err = build_boundary_groups(tiles, st_local, cpl_local, src_local, bgroups, bnd_idx);
@@ -453,7 +455,7 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
       (rc = C->upload_const(&A.bgroups, bgroups)) || (rc = C->upload_const(&A.bnd_idx, bnd_idx)) ||
       (rc = C->upload_const(&A.geo, geo)) || (rc = C->upload_const(&A.fac, fac)) ||
       (rc = C->upload_const(&A.sh_ids, T.sh_ids)) || (rc = C->upload_const(&A.shp_off, T.shp_off)) ||
-      (rc = C->upload_const(&A.shp_slots, T.shp_slots)) || (rc = C->upload_const(&A.st_local, st_local)) ||
+      (rc = C->upload_const(&A.slot_pos, slot_pos)) || (rc = C->upload_const(&A.st_local, st_local)) ||
       (rc = C->upload_const(&A.st_wr, st_wr)) || (rc = C->upload_const(&A.cpl_local, cpl_local)) ||
       (rc = C->upload_const(&A.cpl_src, cpl_src)) || (rc = C->upload_const(&A.cpl_nw, cpl_nw)) ||
       (rc = C->upload_const(&A.src_local, src_local)) || (rc = C->upload_const(&A.src_id, src_id)) ||
@@ -631,6 +633,27 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
   return SF2D_OK;
 }
 
+extern "C" int sf2d_coupled_prepare(sf2d_coupled *C) {
+  using namespace sf2d;
+  if (!C) return fail(SF2D_ERR_INVALID, "null solver");
+  const int K = C->chunk;
+  if (C->graph && C->graph_steps == K) return SF2D_OK;
+  if (C->graph) cudaGraphExecDestroy(C->graph);
+  C->graph = nullptr;
+  cudaStream_t st = C->stream();
+  cudaGraph_t g;
+  SF2D_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  C->launch_chunk(K);
+  SF2D_CUDA(cudaStreamEndCapture(st, &g));
+  cudaError_t e = cudaGraphInstantiate(&C->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(SF2D_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+  SF2D_CUDA(cudaGraphUpload(C->graph, st));
+  SF2D_CUDA(cudaStreamSynchronize(st));
+  C->graph_steps = K;
+  return SF2D_OK;
+}
+
 extern "C" int sf2d_coupled_enqueue(sf2d_coupled *C, int nstep) {
   using namespace sf2d;
   if (!C || nstep < 0) return fail(SF2D_ERR_INVALID, "bad arguments");
@@ -639,18 +662,7 @@ extern "C" int sf2d_coupled_enqueue(sf2d_coupled *C, int nstep) {
   const int K = C->chunk;
   int done = 0;
   if (nstep >= K) {
-    if (!C->graph || C->graph_steps != K) {
-      if (C->graph) cudaGraphExecDestroy(C->graph);
-      C->graph = nullptr;
-      cudaGraph_t g;
-      SF2D_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-      C->launch_chunk(K);
-      SF2D_CUDA(cudaStreamEndCapture(st, &g));
-      cudaError_t e = cudaGraphInstantiate(&C->graph, g, 0);
-      cudaGraphDestroy(g);
-      if (e != cudaSuccess) return fail(SF2D_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
-      C->graph_steps = K;
-    }
+    if (int rc = sf2d_coupled_prepare(C)) return rc;
     for (; done + K <= nstep; done += K) SF2D_CUDA(cudaGraphLaunch(C->graph, st));
   }
   if (done < nstep)

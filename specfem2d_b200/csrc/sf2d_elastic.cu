@@ -253,7 +253,11 @@ int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solv
   UP(mat, float2, mat);
   UP(sh_ids, int, T.sh_ids);
   UP(shp_off, int, T.shp_off);
-  UP(shp_slots, int, T.shp_slots);
+  {
+    std::vector<int> slot_pos(T.shp_slots.size());
+    for (size_t k = 0; k < T.shp_slots.size(); ++k) slot_pos[T.shp_slots[k]] = static_cast<int>(k);
+    UP(slot_pos, int, slot_pos);
+  }
   UP(bgroups, int4, bgroups);
   UP(bnd_idx, int, bnd_idx);
   UP(st_local, int, st_local);
@@ -456,23 +460,32 @@ extern "C" int sf2d_get_fields(sf2d_solver *S, float *displ, float *veloc, float
   return SF2D_OK;
 }
 
+extern "C" int sf2d_prepare(sf2d_solver *S) {
+  if (!S) return fail(SF2D_ERR_INVALID, "null solver");
+  const int K = S->chunk;
+  if (S->graph && S->graph_steps == K) return SF2D_OK;
+  if (S->graph) cudaGraphExecDestroy(S->graph);
+  S->graph = nullptr;
+  // capture records the chunk's launches without running them
+  cudaGraph_t g;
+  SF2D_CUDA(cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal));
+  S->launch_chunk(K);
+  SF2D_CUDA(cudaStreamEndCapture(S->stream, &g));
+  cudaError_t e = cudaGraphInstantiate(&S->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(SF2D_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+  SF2D_CUDA(cudaGraphUpload(S->graph, S->stream));
+  SF2D_CUDA(cudaStreamSynchronize(S->stream));
+  S->graph_steps = K;
+  return SF2D_OK;
+}
+
 extern "C" int sf2d_enqueue(sf2d_solver *S, int nstep) {
   if (!S || nstep < 0) return fail(SF2D_ERR_INVALID, "bad arguments");
   const int K = S->chunk;
   int done = 0;
   if (nstep >= K) {
-    if (!S->graph || S->graph_steps != K) {
-      if (S->graph) cudaGraphExecDestroy(S->graph);
-      S->graph = nullptr;
-      cudaGraph_t g;
-      SF2D_CUDA(cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal));
-      S->launch_chunk(K);
-      SF2D_CUDA(cudaStreamEndCapture(S->stream, &g));
-      cudaError_t e = cudaGraphInstantiate(&S->graph, g, 0);
-      cudaGraphDestroy(g);
-      if (e != cudaSuccess) return fail(SF2D_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
-      S->graph_steps = K;
-    }
+    if (int rc = sf2d_prepare(S)) return rc;
     for (; done + K <= nstep; done += K) SF2D_CUDA(cudaGraphLaunch(S->graph, S->stream));
   }
   if (done < nstep) {

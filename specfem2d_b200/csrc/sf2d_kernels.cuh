@@ -55,7 +55,10 @@ struct Params {
   float4 *att_state_l;     // LDDRK: e1_LDDRK, e11_LDDRK, e13_LDDRK with the same packing
   const int *sh_ids;
   float2 *partial;
-  const int *shp_off, *shp_slots;
+  // shared-point partial sums, point-major: the slots of shared point s are
+  // [shp_off[s], shp_off[s+1]) in tile order; slot_pos maps a tile's shared
+  // local point (sh_off + k) to its slot
+  const int *shp_off, *slot_pos;
   const int4 *bgroups;    // per tile (grp_off, grp_n): point, first idx, Stacey | coupling << 8, sources
   const int *bnd_idx;     // entries of each group
   const int *st_local;
@@ -476,6 +479,15 @@ __global__ void __launch_bounds__(NT, tile_min_blocks<NT, ANISO, ATTEN, KERN, PM
     s_acc[l] = acc;
   }
 
+  // the first point's geometry and material are requested now, so that their
+  // latency passes during the derivative lines (software pipelining of 4b)
+  float4 g_next = make_float4(0.f, 0.f, 0.f, 0.f);
+  float2 m_next = make_float2(0.f, 0.f);
+  if (tid < nq) {
+    g_next = __ldg(P.geo + ebase + tid);
+    m_next = __ldg(P.mat + ebase + tid);
+  }
+
   // 4a. derivative lines: one thread per element row (xi) or column (gamma)
   //     forms the 5 derivatives along it; the loops are fully unrolled, so
   //     hprime comes straight from the kernel's constant bank, and each point's
@@ -505,9 +517,14 @@ __global__ void __launch_bounds__(NT, tile_min_blocks<NT, ANISO, ATTEN, KERN, PM
     const int i = FIXQ ? i0 : q - 5 * j;
     const uint16_t *le = s_lib + 25 * e;
     // geometry and material straight from global memory (coalesced in f): not
-    // staging them keeps the tile's shared memory small and more tiles resident
-    const float4 g4 = __ldg(P.geo + ebase + f);
-    const float2 m2 = __ldg(P.mat + ebase + f);
+    // staging them keeps the tile's shared memory small and more tiles resident;
+    // the next point's are requested before this one is computed
+    const float4 g4 = g_next;
+    const float2 m2 = m_next;
+    if (f + NT < nq) {
+      g_next = __ldg(P.geo + ebase + f + NT);
+      m_next = __ldg(P.mat + ebase + f + NT);
+    }
     const float2 d1 = s_d1[f], d2 = s_d2[f];
     const float dux_dxi = d1.x, duz_dxi = d1.y, dux_dg = d2.x, duz_dg = d2.y;
     if (KERN) {
@@ -636,6 +653,14 @@ __global__ void __launch_bounds__(NT, tile_min_blocks<NT, ANISO, ATTEN, KERN, PM
   }
   __syncthreads();
 
+  // step-6 operands of the thread's first point, requested before the assembly
+  float2 rm_next = make_float2(0.f, 0.f);
+  int sp_next = 0;
+  if (tid < n_int)
+    rm_next = P.rmass[int_begin + tid];
+  else if (tid < nl)
+    sp_next = P.slot_pos[ti.sh_off + tid - n_int];
+
   // 5. assembly into the accumulator, one colour at a time (elements of a
   //    colour share no point): a -= wz * row term + wx * column term
   int cb = 0;
@@ -668,9 +693,14 @@ __global__ void __launch_bounds__(NT, tile_min_blocks<NT, ANISO, ATTEN, KERN, PM
   bool bad = false;
   for (int l = tid; l < nl; l += NT) {
     const float2 acc = s_acc[l];
+    const float2 rm = rm_next;
+    const int sp = sp_next;
+    if (l + NT < n_int)
+      rm_next = P.rmass[int_begin + l + NT];
+    else if (l + NT < nl)
+      sp_next = P.slot_pos[ti.sh_off + l + NT - n_int];
     if (l < n_int) {
       const int g = int_begin + l;
-      const float2 rm = P.rmass[g];
       const float2 a = make_float2(acc.x * rm.x, acc.y * rm.y);
       float2 v = s_v[l];
       float2 u = s_u[l];
@@ -704,7 +734,7 @@ __global__ void __launch_bounds__(NT, tile_min_blocks<NT, ANISO, ATTEN, KERN, PM
       }
       bad |= !(fabsf(u.x) < 1e25f && fabsf(u.y) < 1e25f);
     } else {
-      P.partial[ti.sh_off + l - n_int] = acc;
+      P.partial[sp] = acc;
     }
   }
   if (bad) *P.d_status = 1;
@@ -730,7 +760,7 @@ __global__ void __launch_bounds__(SHARED_NT) k_elastic_shared(const Params P, in
     }
     float2 acc = make_float2(0.f, 0.f);
     for (int k = P.shp_off[s]; k < P.shp_off[s + 1]; ++k) {
-      const float2 p = P.partial[P.shp_slots[k]];
+      const float2 p = P.partial[k];
       acc.x += p.x;
       acc.y += p.y;
     }

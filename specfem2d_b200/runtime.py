@@ -83,6 +83,7 @@ def load_library(path: str = LIB):
         "sf2d_get_fields": [vp, _f, _f, _f],
         "sf2d_run": [vp, ctypes.c_int, _d],
         "sf2d_enqueue": [vp, ctypes.c_int],
+        "sf2d_prepare": [vp],
         "sf2d_synchronize": [vp, ctypes.c_double],
         "sf2d_copy_seismograms": [vp, ctypes.c_int, ctypes.c_int, _d],
         "sf2d_get_norm": [vp, _f],
@@ -309,6 +310,10 @@ class ElasticSolver:
 
     def enqueue(self, nstep: int):
         _check(self._lib.sf2d_enqueue(self._h, nstep))
+
+    def prepare(self):
+        """Build the step-chunk graph ahead of the first enqueue (runs nothing)."""
+        _check(self._lib.sf2d_prepare(self._h))
 
     def synchronize(self, timeout_s: float = 0.0):
         _check(self._lib.sf2d_synchronize(self._h, float(timeout_s)))
