@@ -252,10 +252,20 @@ def run_fwi(args, rank, world):
     from specfem2d_b200 import batch
     from specfem2d_b200.fwi import FWIGradient
 
+    from specfem2d_b200.distributed import max_over_ranks, shard, sum_over_ranks
+
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    models = fwi_members(args.models, args.fwi_steps, args.fwi_set)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    all_models = fwi_members(args.models, args.fwi_steps, args.fwi_set)
+    # models are independent: each rank takes a share of nearly equal size
+    models = [all_models[k] for k in shard([m.nspec for m in all_models], rank, world)]
     every = 100
-    nq = sum(m.nspec for m in models)
+    nq = sum(m.nspec for m in all_models)
 
     def one(db):
         g = FWIGradient(db, every, tile_elems=args.tile_elems, threads_per_block=args.threads)
@@ -267,38 +277,51 @@ def run_fwi(args, rank, world):
         g.close()
         return t1 - t0, kern
 
-    # warm-up on the smallest member (module load, graph instantiation)
-    one(min(models, key=lambda m: m.nspec))
-    plain_s, plain_k = 0.0, []
-    for m in models:
-        t, k = one(m)
-        plain_s += t
-        plain_k.append(k)
-    packed, idx = batch.pack(models)
-    batched_s, bk = one(packed)
-    # gradient agreement: packed kernels against the per-model ones
-    num = den = 0.0
-    for c in range(3):
-        for m, part in enumerate(batch.split_elements(bk[c], idx)):
-            ref = plain_k[m][c].astype(np.float64)
-            num += float(np.sum((part.astype(np.float64) - ref) ** 2))
-            den += float(np.sum(ref ** 2))
-    n = len(models)
+    plain_s = batched_s = num = den = 0.0
+    local_nglob = 0
+    if models:
+        # warm-up on the smallest member (module load, graph instantiation)
+        one(min(models, key=lambda m: m.nspec))
+        plain_k = []
+        for m in models:
+            t, k = one(m)
+            plain_s += t
+            plain_k.append(k)
+        packed, idx = batch.pack(models)
+        local_nglob = packed.nglob
+        batched_s, bk = one(packed)
+        # gradient agreement: packed kernels against the per-model ones
+        for c in range(3):
+            for m, part in enumerate(batch.split_elements(bk[c], idx)):
+                ref = plain_k[m][c].astype(np.float64)
+                num += float(np.sum((part.astype(np.float64) - ref) ** 2))
+                den += float(np.sum(ref ** 2))
+    # the job takes as long as its slowest rank
+    plain_s = max_over_ranks(plain_s, device="cuda")
+    batched_s = max_over_ranks(batched_s, device="cuda")
+    num, den = (float(x) for x in sum_over_ranks(np.array([num, den]), device="cuda"))
+    n = len(all_models)
+    packed_nglob = int(sum_over_ranks(np.array([float(local_nglob)]), device="cuda")[0])
     line = {
         "metric": "s per FWI gradient per shot", "value": batched_s / n, "unit": "s", "n_gpus": world,
-        "steps": args.fwi_steps, "warmup": 1, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "steps": args.fwi_steps, "warmup": 1, "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": args.workload, "description": FWI_WORKLOADS[args.workload], "models": n,
-                   "model_set": args.fwi_set, "sizes": [[int(m.nspec), int(m.nglob)] for m in models],
-                   "nspec_total": nq, "nglob_total": int(packed.nglob), "checkpoint_every": every,
+                   "model_set": args.fwi_set, "sizes": [[int(m.nspec), int(m.nglob)] for m in all_models],
+                   "nspec_total": nq, "nglob_total": packed_nglob, "checkpoint_every": every,
+                   "parallelism": f"models sharded over {world} GPU(s)",
                    "tile_elems": args.tile_elems, "threads_per_cta": args.threads},
         "plain_s_per_shot": plain_s / n, "batched_s_per_shot": batched_s / n,
         "speedup_batched_vs_plain": plain_s / batched_s,
         "gradient_rel_l2_batched_vs_plain": (num / den) ** 0.5 if den > 0 else 0.0,
-        "point_updates_per_s_batched": 3.0 * packed.nglob * args.fwi_steps / batched_s,
+        "point_updates_per_s_batched": 3.0 * packed_nglob * args.fwi_steps / batched_s,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
 
 
 def main():
@@ -350,6 +373,7 @@ def main():
     from specfem2d_b200.configs import (algorithmic_bytes_coupled, algorithmic_bytes_elastic,
                                         algorithmic_bytes_viscoelastic)
     from specfem2d_b200.coupled import CoupledSolver
+    from specfem2d_b200.distributed import job_throughput, max_over_ranks
     from specfem2d_b200.runtime import ElasticSolver
 
     K, W = args.steps, args.warmup
@@ -390,11 +414,8 @@ def main():
     solver.synchronize(600)
     torch.cuda.synchronize()
     clk = clocks.stop()
-    ms = ev0.elapsed_time(ev1)
+    ms = max_over_ranks(ev0.elapsed_time(ev1), device="cuda")  # the job lasts as long as its slowest rank
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
     # per step (stage): a tile launch per tile group (with and without CPML) and a shared-point
     # kernel per domain, and the CPML coupling-entry kernels; receiver kernels per chunk
@@ -467,12 +488,9 @@ def main():
         e2e_s = t1 - t0
         del d
         e2e_solver.close()
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, device="cuda")
 
-    value = db.nglob * K * world / (ms * 1e-3)
+    value = job_throughput(db.nglob * K, ms * 1e-3, world, device="cuda")
     line = {
         "metric": "GLL point-updates/s", "value": value, "unit": "point-updates/s",
         "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True,
