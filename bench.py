@@ -170,25 +170,33 @@ def run_reference_fwi(args, rank):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle  # noqa: E402  (reference arm only)
 
-    models = fwi_members(args.models, args.fwi_steps, args.fwi_set)
-    db = min(models, key=lambda m: m.nspec)
+    if args.workload == "c4_fwi_shots":
+        from specfem2d_b200 import configs
+
+        # one shot of the same model at 1/8 of the element count per direction (bounded CPU sample)
+        db = configs.c4_gradient(nstep=args.fwi_steps, scale=8)
+        nglobs = [(4 * 1000 + 1) * (4 * 400 + 1)] * args.models
+    else:
+        models = fwi_members(args.models, args.fwi_steps, args.fwi_set)
+        db = min(models, key=lambda m: m.nspec)
+        nglobs = [m.nglob for m in models]
     t0 = time.perf_counter()
     oracle.gradient(db, np.zeros((len(db.rec_ispec), db.nstep, 2)), checkpoint_every=100, precision=4)
     t_sample = time.perf_counter() - t0
     # per shot of the workload: the sample's time scaled by the mean point count
-    scale = float(np.mean([m.nglob for m in models])) / float(db.nglob)
+    scale = float(np.mean(nglobs)) / float(db.nglob)
     dt = t_sample * scale
     threads = oracle.max_threads()
     line = {"metric": "s per FWI gradient per shot", "value": dt, "unit": "s", "impl": "reference",
             "n_gpus": args.gpus, "steps": args.fwi_steps, "warmup": 0, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": args.workload, "description": FWI_WORKLOADS[args.workload],
-                       "model_set": args.fwi_set, "models": len(models), "sample_nspec": db.nspec,
+                       "model_set": args.fwi_set, "models": len(nglobs), "sample_nspec": db.nspec,
                        "sample_seconds": t_sample},
             "cpu_baseline": {"value": dt, "unit": "s", "cores": threads, "kind": "port",
-                             "sample": f"one gradient of the smallest model ({db.nspec} elements, "
+                             "sample": f"one gradient of a {db.nspec}-element model ("
                                        f"{db.nstep} steps, {t_sample:.1f} s) scaled by the mean point count "
-                                       f"of the {len(models)} models (x{scale:.2f}); C++ restatement of the "
+                                       f"of the {len(nglobs)} members (x{scale:.2f}); C++ restatement of the "
                                        "reference CPU solver"},
             "e2e": {"value": dt, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -215,6 +223,13 @@ def run_reference(args, rank):
 
 
 FWI_WORKLOADS = {
+    "c4_fwi_shots": ("misfit gradients of shots on the 1000x400-element (25 km x 10 km, 6,405,601 GLL points) "
+                     "elastic model (vp 2500 m/s + 0.2 /s x depth, vs = vp/1.73, Gardner rho); Ricker 8 Hz "
+                     "force 500 m deep at seeded surface positions (seed 5), 200 receivers, dt 4e-4, L2 misfit "
+                     "against zero data (adjoint source = the synthetics: within 4000 steps no reflection "
+                     "from the true model's anomalies, 3-7 km deep, reaches the receivers, so true-model data "
+                     "would leave only rounding in the residual), checkpoint every 100 steps; batched = the "
+                     "shots packed into meshes of --batch shots, plain = one shot per run"),
     "c5_fwi_models": ("misfit gradients of independent random-layered elastic models with uneven meshes "
                       "(sizes drawn with seed 6 between 100x50 and 1200x500 elements, 3-6 layers, vp 2000-4500, "
                       "one Ricker 8 Hz force, 20 surface receivers, dt 4e-4, Stacey on three sides); "
@@ -222,6 +237,25 @@ FWI_WORKLOADS = {
                       "batched = all models packed into one mesh and one launch per step, plain = one "
                       "model per run"),
 }
+
+
+def c4_shots(n_shots: int, nstep: int):
+    """Shots of the C4 gradient workload on the starting model."""
+    from specfem2d_b200 import batch, configs
+
+    os.makedirs(CACHE, exist_ok=True)
+    path = os.path.join(CACHE, f"c4_shots_{n_shots}_{nstep}.pkl")
+    if os.path.exists(path):
+        with open(path, "rb") as f:
+            return pickle.load(f)
+    xs = np.sort(np.random.default_rng(5).uniform(1000.0, 24000.0, n_shots))
+    start = configs.c4_gradient(nstep=nstep)
+    out = batch.shots_on_model(start, [(float(x), 9500.0) for x in xs])
+    for d in out:
+        d.mesh = None  # not needed past the source location
+    with open(path, "wb") as f:
+        pickle.dump(out, f)
+    return out
 
 
 def fwi_members(n_models: int, nstep: int, which: str = "first"):
@@ -261,18 +295,23 @@ def run_fwi(args, rank, world):
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    all_models = fwi_members(args.models, args.fwi_steps, args.fwi_set)
-    # models are independent: each rank takes a share of nearly equal size
-    models = [all_models[k] for k in shard([m.nspec for m in all_models], rank, world)]
+    if args.workload == "c4_fwi_shots":
+        all_models = c4_shots(args.models, args.fwi_steps)
+    else:
+        all_models = fwi_members(args.models, args.fwi_steps, args.fwi_set)
+    # shots and models are independent: each rank takes a share of nearly equal size
+    mine = shard([m.nspec for m in all_models], rank, world)
+    models = [all_models[k] for k in mine]
+    observed = [np.zeros((len(m.rec_ispec), args.fwi_steps, 2)) for m in models]
     every = 100
     nq = sum(m.nspec for m in all_models)
 
-    def one(db):
+    def one(db, obs):
         g = FWIGradient(db, every, tile_elems=args.tile_elems, threads_per_block=args.threads)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         seis = g.forward()
-        kern = g.backward(seis)
+        kern = g.backward(seis - obs)
         t1 = time.perf_counter()
         g.close()
         return t1 - t0, kern
@@ -281,18 +320,28 @@ def run_fwi(args, rank, world):
     local_nglob = 0
     if models:
         # warm-up on the smallest member (module load, graph instantiation)
-        one(min(models, key=lambda m: m.nspec))
+        w = min(range(len(models)), key=lambda k: models[k].nspec)
+        one(models[w], observed[w])
         plain_k = []
-        for m in models:
-            t, k = one(m)
+        for m, obs in zip(models, observed):
+            t, k = one(m, obs)
             plain_s += t
             plain_k.append(k)
-        packed, idx = batch.pack(models)
-        local_nglob = packed.nglob
-        batched_s, bk = one(packed)
+        # batched: the members packed into meshes of at most --batch members
+        # (device memory: checkpoint frames grow with the packed mesh)
+        bsize = args.batch if args.batch > 0 else len(models)
+        bk = [[], [], []]
+        for b0 in range(0, len(models), bsize):
+            grp = models[b0:b0 + bsize]
+            packed, idx = batch.pack(grp)
+            local_nglob += packed.nglob
+            t, kk = one(packed, np.concatenate(observed[b0:b0 + bsize], axis=0))
+            batched_s += t
+            for c in range(3):
+                bk[c].extend(batch.split_elements(kk[c], idx))
         # gradient agreement: packed kernels against the per-model ones
         for c in range(3):
-            for m, part in enumerate(batch.split_elements(bk[c], idx)):
+            for m, part in enumerate(bk[c]):
                 ref = plain_k[m][c].astype(np.float64)
                 num += float(np.sum((part.astype(np.float64) - ref) ** 2))
                 den += float(np.sum(ref ** 2))
@@ -335,6 +384,7 @@ def main():
     ap.add_argument("--fwi-steps", type=int, default=1000, help="time steps of each FWI model")
     ap.add_argument("--fwi-set", default="first", choices=["first", "smallest"],
                     help="the first --models of the 48 seeded sizes, or the smallest")
+    ap.add_argument("--batch", type=int, default=0, help="members per packed mesh in the FWI workloads (0 = all)")
     ap.add_argument("--tile-elems", type=int, default=32)
     ap.add_argument("--threads", type=int, default=256)
     ap.add_argument("--fluid-tile-elems", type=int, default=0, help="fluid tiles (coupled runs); 0 = --tile-elems")

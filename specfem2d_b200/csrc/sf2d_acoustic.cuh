@@ -210,7 +210,8 @@ __device__ __forceinline__ void record_receiver_ac(const AcParams &A, int r, int
 // extra terms (pml_compute_memory_variables.f90:42-224,
 // pml_compute_accel_contribution.f90:42-180).  Tiles [tile0, tile0 + gridDim.x).
 template <int NT, bool LDDRK, bool PML = false>
-__global__ void __launch_bounds__(NT) k_acoustic_tile(const AcParams A, int record_prev, int stage, int tile0) {
+__global__ void __launch_bounds__(NT, PML ? 768 / NT : 1536 / NT)
+    k_acoustic_tile(const AcParams A, int record_prev, int stage, int tile0) {
   extern __shared__ __align__(16) unsigned char smem[];
   const TileInfo &ti = A.tiles[tile0 + blockIdx.x];
   const int tid = threadIdx.x;
@@ -235,7 +236,9 @@ __global__ void __launch_bounds__(NT) k_acoustic_tile(const AcParams A, int reco
 
   const int step = *A.d_step;
   if (blockIdx.x == 0 && tid == 0) *A.d_step_b = step;
-  if (record_prev && tid < ti.rec_n) record_receiver_ac(A, ti.rec_off + tid, step - 1);
+  // fluid receivers are recorded by k_acoustic_receivers after each step: their
+  // double-precision gradient would hold registers through the whole tile
+  (void)record_prev;
 
   // 1. loads
   {
@@ -618,7 +621,8 @@ __global__ void k_cpl_pml_solid(const CplPml C, const float *p, const float *pd,
                                   c[2] * static_cast<double>(pot) + c[3] * static_cast<double>(r)));
 }
 
-// records the step before *d_step for every fluid receiver
+// records the step before *d_step for every fluid receiver (launched after the
+// last stage of every step)
 static __global__ void k_acoustic_receivers(const AcParams A) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r < A.nrec) record_receiver_ac(A, r, *A.d_step - 1);

@@ -175,11 +175,35 @@ struct sf2d_coupled {
     else
       sf2d::k_cpl_pml_solid<false><<<nb, 128, 0, stream()>>>(cpl_solid, A.p, A.pd, A.pdd, A.pold, A.dt, 0.f, 0.f);
   }
+  // fluid receivers of the step just finished; on the side stream when there is
+  // one (they only read fluid fields, which the solid kernels do not touch),
+  // joined before the next fluid tile kernel
+  cudaEvent_t ev_rec = nullptr, ev_rec_done = nullptr;
+  bool rec_pending = false;
+  void launch_ac_receivers() {
+    if (A.nrec <= 0) return;
+    const int nb = (A.nrec + 127) / 128;
+    if (side) {
+      cudaEventRecord(ev_rec, stream());
+      cudaStreamWaitEvent(side, ev_rec, 0);
+      sf2d::k_acoustic_receivers<<<nb, 128, 0, side>>>(A);
+      cudaEventRecord(ev_rec_done, side);
+      rec_pending = true;
+    } else {
+      sf2d::k_acoustic_receivers<<<nb, 128, 0, stream()>>>(A);
+    }
+  }
+  void join_ac_receivers() {
+    if (rec_pending) cudaStreamWaitEvent(stream(), ev_rec_done, 0);
+    rec_pending = false;
+  }
   void launch_step(bool record_prev) {
     for (int st = 0; st < nstage; ++st) {
       launch_cpl_fluid(st);
+      join_ac_receivers();
       launch_ac_tile(record_prev && st == 0, st);
       launch_ac_shared(st);
+      if (st == nstage - 1) launch_ac_receivers();
       launch_cpl_solid(st);
       if (el) {
         el->launch_tile(record_prev && st == 0, st);
@@ -189,8 +213,8 @@ struct sf2d_coupled {
   }
   int launch_chunk(int n) {
     for (int k = 0; k < n; ++k) launch_step(k > 0);
+    join_ac_receivers();
     if (el) el->launch_receivers();
-    if (A.nrec > 0) sf2d::k_acoustic_receivers<<<(A.nrec + 127) / 128, 128, 0, stream()>>>(A);
     SF2D_CUDA(cudaGetLastError());
     return SF2D_OK;
   }
@@ -200,6 +224,8 @@ struct sf2d_coupled {
     for (void *p : allocs) cudaFree(p);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
+    if (ev_rec) cudaEventDestroy(ev_rec);
+    if (ev_rec_done) cudaEventDestroy(ev_rec_done);
     if (side) cudaStreamDestroy(side);
     if (own_stream) cudaStreamDestroy(own_stream);
   }
@@ -545,6 +571,8 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
       SF2D_CUDA(cudaStreamCreateWithFlags(&C->side, cudaStreamNonBlocking));
       SF2D_CUDA(cudaEventCreateWithFlags(&C->ev_fork, cudaEventDisableTiming));
       SF2D_CUDA(cudaEventCreateWithFlags(&C->ev_join, cudaEventDisableTiming));
+      SF2D_CUDA(cudaEventCreateWithFlags(&C->ev_rec, cudaEventDisableTiming));
+      SF2D_CUDA(cudaEventCreateWithFlags(&C->ev_rec_done, cudaEventDisableTiming));
     }
   }
   {
@@ -758,6 +786,8 @@ extern "C" int sf2d_coupled_time_kernels(sf2d_coupled *C, int nstep, float *ms) 
       C->launch_ac_tile(rp, st);
       SF2D_CUDA(cudaEventRecord(ev[1], str));
       C->launch_ac_shared(st);
+      if (st == C->nstage - 1 && C->A.nrec > 0)  // the step's fluid receivers, on the timed stream
+        sf2d::k_acoustic_receivers<<<(C->A.nrec + 127) / 128, 128, 0, str>>>(C->A);
       SF2D_CUDA(cudaEventRecord(ev[2], str));
       C->launch_cpl_solid(st);
       if (S) S->launch_tile(rp, st);
@@ -773,7 +803,6 @@ extern "C" int sf2d_coupled_time_kernels(sf2d_coupled *C, int nstep, float *ms) 
     }
   SF2D_CUDA(cudaGetLastError());
   if (S) S->launch_receivers();
-  if (C->A.nrec > 0) sf2d::k_acoustic_receivers<<<(C->A.nrec + 127) / 128, 128, 0, str>>>(C->A);
   SF2D_CUDA(cudaStreamSynchronize(str));
   C->steps_done += nstep;
   if (S) S->steps_done += nstep;
@@ -811,7 +840,7 @@ extern "C" int sf2d_coupled_launch_count(sf2d_coupled *C, int nstep, long long *
                         (C->cpl_solid.n > 0);
   if (S) per_stage += (S->pml_tile0 > 0) + (S->pml_tile0 < S->T.ntiles) + 1;
   const long long chunks = nstep / C->chunk + (nstep % C->chunk ? 1 : 0);
-  *launches = per_stage * C->nstage * nstep + ((S && S->nrec > 0) + (C->A.nrec > 0)) * chunks;
+  *launches = per_stage * C->nstage * nstep + (C->A.nrec > 0 ? nstep : 0) + (S && S->nrec > 0 ? chunks : 0);
   return SF2D_OK;
 }
 
