@@ -51,6 +51,7 @@ struct AcParams {
   const int *sh_ids;
   float *partial;
   const int *shp_off, *slot_pos;  // point-major partial sums, as in the solid kernels
+  const int *edge_local;      // per tile (edge_off, edge_n): local point | free_mask bits << 16
   const int4 *bgroups;        // per tile (grp_off, grp_n): point, first idx, Stacey | coupling << 8, sources
   const int *bnd_idx;         // entries of each group
   const int *st_local;
@@ -127,7 +128,7 @@ constexpr uint8_t AC_FREE = 1, AC_EDGE = 2;
 // Shared-memory regions of one fluid tile, 16-byte aligned (pold and pml only
 // in CPML tiles).
 struct AcSmem {
-  size_t p, pd, acc, h, lib, d1, d2, pold, od1, od2, pml, total;
+  size_t p, pd, acc, h, lib, mask, d1, d2, pold, od1, od2, pml, total;
 };
 __host__ __device__ inline AcSmem ac_smem_layout(int max_q, int max_local, bool pml = false) {
   AcSmem L;
@@ -142,6 +143,8 @@ __host__ __device__ inline AcSmem ac_smem_layout(int max_q, int max_local, bool 
   o = align16(o + 64 * sizeof(float));
   L.lib = o;
   o = align16(o + static_cast<size_t>((max_q + 7) / 8 * 8) * sizeof(uint16_t));
+  L.mask = o;  // uint8 per local point: free surface / layer edge bits
+  o = align16(o + static_cast<size_t>(max_local));
   const size_t qb = align16(static_cast<size_t>(max_q) * sizeof(float));
   L.d1 = o;
   o += qb;
@@ -225,6 +228,7 @@ __global__ void __launch_bounds__(NT, PML ? 768 / NT : 1536 / NT)
   float *s_pold = reinterpret_cast<float *>(smem + L.pold);
   float *s_pml = reinterpret_cast<float *>(smem + L.pml);
   float *s_d1 = reinterpret_cast<float *>(smem + L.d1);
+  uint8_t *s_mask = reinterpret_cast<uint8_t *>(smem + L.mask);
   float *s_d2 = reinterpret_cast<float *>(smem + L.d2);
   float *s_od1 = reinterpret_cast<float *>(smem + L.od1);
   float *s_od2 = reinterpret_cast<float *>(smem + L.od2);
@@ -262,30 +266,37 @@ __global__ void __launch_bounds__(NT, PML ? 768 / NT : 1536 / NT)
   }
   __syncthreads();
 
-  // 2. predictor (or cleared accumulator), free surface
+  // 2. predictor (or cleared accumulator); then the tile's free-surface and
+  //    layer-edge points (a per-tile list: no per-point mask loads) are zeroed
+  //    and flagged for step 6
   const float dt = A.dt, dto2 = A.dto2, dt2o2 = A.dt2o2;
   for (int l = tid; l < nl; l += NT) {
-    const int g = l < n_int ? int_begin + l : A.sh_ids[ti.sh_off + l - n_int];
     float p = s_p[l], pd = s_pd[l];
-    const uint8_t m = A.free_mask[g];
     if (!LDDRK) {
       const float pdd = s_acc[l];
-      // mid-step potential (update_displacement_Newmark.F90:374-380), zero on the layer's edge
-      if (PML)
-        s_pold[l] = (m & AC_EDGE) ? 0.f
-                                  : static_cast<float>(static_cast<double>(p) + A.h_old * static_cast<double>(pdd));
+      // mid-step potential (update_displacement_Newmark.F90:374-380)
+      if (PML) s_pold[l] = static_cast<float>(static_cast<double>(p) + A.h_old * static_cast<double>(pdd));
       p = newmark_displ(p, pd, pdd, dt, dt2o2);
       pd = newmark_veloc(pd, pdd, dto2);
-    }
-    if (m) {
-      p = 0.f;
-      pd = 0.f;
     }
     s_p[l] = p;
     s_pd[l] = pd;
     s_acc[l] = 0.f;
+    s_mask[l] = 0;
   }
   __syncthreads();
+  if (ti.edge_n > 0) {
+    for (int k = tid; k < ti.edge_n; k += NT) {
+      const int v = A.edge_local[ti.edge_off + k];
+      const int l = v & 0xFFFF;
+      const uint8_t m = static_cast<uint8_t>(v >> 16);
+      s_p[l] = 0.f;
+      s_pd[l] = 0.f;
+      if (PML && !LDDRK && (m & AC_EDGE)) s_pold[l] = 0.f;  // the layer's edge (pml_boundary_acoustic)
+      s_mask[l] = m;
+    }
+    __syncthreads();
+  }
 
   // 3. boundary terms, coupling and sources: one thread per receiving point,
   //    in the reference's order at that point
@@ -343,8 +354,10 @@ __global__ void __launch_bounds__(NT, PML ? 768 / NT : 1536 / NT)
   // 4a. derivative lines: one thread per element row (xi) or column (gamma),
   //     hprime from the kernel's constant bank (see the solid kernel)
   const int nlines = 10 * ti.nelem;
-  for (int t = tid; t < nlines; t += NT) {
-    const int e = t / 10, r = t - 10 * e;
+  for (int t = tid, el = tid / 10; t < nlines; t += NT, el += NT / 10) {
+    // with NT a multiple of 10 every thread keeps one line position r
+    const int e = NT % 10 == 0 ? el : t / 10;
+    const int r = NT % 10 == 0 ? tid % 10 : t - 10 * e;
     const int a0 = r < 5 ? 5 * r : r - 5;
     const int st = r < 5 ? 1 : 5;
     const uint16_t *le = s_lib + 25 * e + a0;
@@ -358,8 +371,8 @@ __global__ void __launch_bounds__(NT, PML ? 768 / NT : 1536 / NT)
   //     the derivatives), the layer's memory variables in CPML tiles
   constexpr bool FIXQ = NT % 25 == 0;  // every thread keeps one GLL position
   const int q0 = tid % 25, j0 = q0 / 5, i0 = q0 - 5 * j0;
-  for (int f = tid; f < nq; f += NT) {
-    const int e = f / 25;
+  for (int f = tid, ef = tid / 25; f < nq; f += NT, ef += NT / 25) {
+    const int e = FIXQ ? ef : f / 25;
     const int q = FIXQ ? q0 : f - 25 * e;
     const int j = FIXQ ? j0 : q / 5;
     const int i = FIXQ ? i0 : q - 5 * j;
@@ -424,8 +437,10 @@ __global__ void __launch_bounds__(NT, PML ? 768 / NT : 1536 / NT)
   __syncthreads();
 
   // 4c. weighted transpose lines, in place
-  for (int t = tid; t < nlines; t += NT) {
-    const int e = t / 10, r = t - 10 * e;
+  for (int t = tid, el = tid / 10; t < nlines; t += NT, el += NT / 10) {
+    // with NT a multiple of 10 every thread keeps one line position r
+    const int e = NT % 10 == 0 ? el : t / 10;
+    const int r = NT % 10 == 0 ? tid % 10 : t - 10 * e;
     const int a0 = r < 5 ? 5 * r : r - 5;
     line_weighted_ac(A, (r < 5 ? s_d1 : s_d2) + 25 * e + a0, r < 5 ? 1 : 5);
   }
@@ -435,8 +450,8 @@ __global__ void __launch_bounds__(NT, PML ? 768 / NT : 1536 / NT)
   int cb = 0;
   for (int c = 0; c < ti.ncol; ++c) {
     const int ce = ti.col_end[c] * 25;
-    for (int f = cb + tid; f < ce; f += NT) {  // cb is a multiple of 25: FIXQ positions hold
-      const int e = f / 25;
+    for (int f = cb + tid, ef = (cb + tid) / 25; f < ce; f += NT, ef += NT / 25) {  // cb: a multiple of 25
+      const int e = FIXQ ? ef : f / 25;
       const int q = FIXQ ? q0 : f - 25 * e;
       const int j = FIXQ ? j0 : q / 5;
       const int i = FIXQ ? i0 : q - 5 * j;
@@ -453,22 +468,18 @@ __global__ void __launch_bounds__(NT, PML ? 768 / NT : 1536 / NT)
   //    point's rmass, mask or slot requested one iteration ahead)
   bool bad = false;
   float rm_next = 0.f;
-  uint8_t fm_next = 0;
   int sp_next = 0;
-  if (tid < n_int) {
+  if (tid < n_int)
     rm_next = A.rmass[int_begin + tid];
-    fm_next = A.free_mask[int_begin + tid];
-  } else if (tid < nl) {
+  else if (tid < nl)
     sp_next = A.slot_pos[ti.sh_off + tid - n_int];
-  }
   for (int l = tid; l < nl; l += NT) {
     const float acc = s_acc[l];
     const float rm = rm_next;
-    const uint8_t fm = fm_next;
+    const uint8_t fm = s_mask[l];
     const int sp = sp_next;
     if (l + NT < n_int) {
       rm_next = A.rmass[int_begin + l + NT];
-      fm_next = A.free_mask[int_begin + l + NT];
     } else if (l + NT < nl) {
       sp_next = A.slot_pos[ti.sh_off + l + NT - n_int];
     }

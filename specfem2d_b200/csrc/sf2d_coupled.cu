@@ -340,8 +340,11 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
 
   // ---- fluid tiling and per-slot data
   const int te = ad->tile_elems > 0 ? ad->tile_elems : 32;
+  // the fluid layer's tiles are a quarter of the size: there are few of them
+  // (one wave), so the shorter per-tile latency sets the layer kernel's time
+  const int group_te[2] = {te, std::max(4, te / 4)};
   std::string err = build_tiling(ad->nspec, ad->nglob, ad->ibool, ad->centroid_xz, te, C->T,
-                                 pml_ac ? group.data() : nullptr, pml_ac ? 2 : 1);
+                                 pml_ac ? group.data() : nullptr, pml_ac ? 2 : 1, pml_ac ? group_te : nullptr);
   if (!err.empty()) return fail(SF2D_ERR_INVALID, "fluid tiling: " + err);
   const Tiling &T = C->T;
   C->pml_tile0 = pml_ac ? T.group_tile_begin[1] : T.ntiles;
@@ -449,6 +452,16 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
     if (t.rec_n > C->nt) return fail(SF2D_ERR_INVALID, "more fluid receivers in one tile than threads per CTA");
   std::vector<int> slot_pos(T.shp_slots.size());
   for (size_t k = 0; k < T.shp_slots.size(); ++k) slot_pos[T.shp_slots[k]] = static_cast<int>(k);
+  // per tile: the local points on the free surface or a layer's outer edge, with their bits
+  std::vector<int> edge_local;
+  for (int t = 0; t < T.ntiles; ++t) {
+    tiles[t].edge_off = static_cast<int>(edge_local.size());
+    for (const auto &gl : T.tile_glob_local[t]) {
+      const uint8_t m = fmask[T.glob2dev[gl.first]];
+      if (m) edge_local.push_back(gl.second | (static_cast<int>(m) << 16));
+    }
+    tiles[t].edge_n = static_cast<int>(edge_local.size()) - tiles[t].edge_off;
+  }
   std::vector<int4> bgroups;
   std::vector<int> bnd_idx;
   err = build_boundary_groups(tiles, st_local, cpl_local, src_local, bgroups, bnd_idx);
@@ -482,6 +495,7 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
       (rc = C->upload_const(&A.geo, geo)) || (rc = C->upload_const(&A.fac, fac)) ||
       (rc = C->upload_const(&A.sh_ids, T.sh_ids)) || (rc = C->upload_const(&A.shp_off, T.shp_off)) ||
       (rc = C->upload_const(&A.slot_pos, slot_pos)) || (rc = C->upload_const(&A.st_local, st_local)) ||
+      (rc = C->upload_const(&A.edge_local, edge_local)) ||
       (rc = C->upload_const(&A.st_wr, st_wr)) || (rc = C->upload_const(&A.cpl_local, cpl_local)) ||
       (rc = C->upload_const(&A.cpl_src, cpl_src)) || (rc = C->upload_const(&A.cpl_nw, cpl_nw)) ||
       (rc = C->upload_const(&A.src_local, src_local)) || (rc = C->upload_const(&A.src_id, src_id)) ||

@@ -493,8 +493,10 @@ __global__ void __launch_bounds__(NT, tile_min_blocks<NT, ANISO, ATTEN, KERN, PM
   //     hprime comes straight from the kernel's constant bank, and each point's
   //     field is read twice per element instead of ten times
   const int nlines = 10 * ti.nelem;
-  for (int t = tid; t < nlines; t += NT) {
-    const int e = t / 10, r = t - 10 * e;
+  for (int t = tid, el = tid / 10; t < nlines; t += NT, el += NT / 10) {
+    // with NT a multiple of 10 every thread keeps one line position r
+    const int e = NT % 10 == 0 ? el : t / 10;
+    const int r = NT % 10 == 0 ? tid % 10 : t - 10 * e;
     const int a0 = r < 5 ? 5 * r : r - 5;  // first point: (j = r, 0) of a row, (0, i = r - 5) of a column
     const int st = r < 5 ? 1 : 5;          // stride along the line
     const uint16_t *le = s_lib + 25 * e + a0;
@@ -510,8 +512,8 @@ __global__ void __launch_bounds__(NT, tile_min_blocks<NT, ANISO, ATTEN, KERN, PM
   //     (t1 = J (sigma . xi_x), t2 = J (sigma . gamma_x) overwrite the derivatives)
   constexpr bool FIXQ = NT % 25 == 0;  // every thread keeps one GLL position
   const int q0 = tid % 25, j0 = q0 / 5, i0 = q0 - 5 * j0;
-  for (int f = tid; f < nq; f += NT) {
-    const int e = f / 25;
+  for (int f = tid, ef = tid / 25; f < nq; f += NT, ef += NT / 25) {
+    const int e = FIXQ ? ef : f / 25;
     const int q = FIXQ ? q0 : f - 25 * e;
     const int j = FIXQ ? j0 : q / 5;
     const int i = FIXQ ? i0 : q - 5 * j;
@@ -645,8 +647,10 @@ __global__ void __launch_bounds__(NT, tile_min_blocks<NT, ANISO, ATTEN, KERN, PM
 
   // 4c. weighted transpose lines: rows contract t1 with hprimewgll, columns t2,
   //     in place
-  for (int t = tid; t < nlines; t += NT) {
-    const int e = t / 10, r = t - 10 * e;
+  for (int t = tid, el = tid / 10; t < nlines; t += NT, el += NT / 10) {
+    // with NT a multiple of 10 every thread keeps one line position r
+    const int e = NT % 10 == 0 ? el : t / 10;
+    const int r = NT % 10 == 0 ? tid % 10 : t - 10 * e;
     const int a0 = r < 5 ? 5 * r : r - 5;
     const int st = r < 5 ? 1 : 5;
     line_weighted(P, (r < 5 ? s_d1 : s_d2) + 25 * e + a0, st);
@@ -666,8 +670,8 @@ __global__ void __launch_bounds__(NT, tile_min_blocks<NT, ANISO, ATTEN, KERN, PM
   int cb = 0;
   for (int c = 0; c < ti.ncol; ++c) {
     const int ce = ti.col_end[c] * 25;
-    for (int f = cb + tid; f < ce; f += NT) {  // cb is a multiple of 25: FIXQ positions hold
-      const int e = f / 25;
+    for (int f = cb + tid, ef = (cb + tid) / 25; f < ce; f += NT, ef += NT / 25) {  // cb: a multiple of 25
+      const int e = FIXQ ? ef : f / 25;
       const int q = FIXQ ? q0 : f - 25 * e;
       const int j = FIXQ ? j0 : q / 5;
       const int i = FIXQ ? i0 : q - 5 * j;

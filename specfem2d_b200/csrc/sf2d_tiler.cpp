@@ -28,10 +28,14 @@ int Tiling::local_id(int tile, int glob) const {
 }
 
 std::string build_tiling(int nspec, int nglob, const int *ibool, const double *centroid_xz,
-                         int tile_elems, Tiling &T, const int *elem_group, int ngroups) {
+                         int tile_elems, Tiling &T, const int *elem_group, int ngroups,
+                         const int *group_tile_elems) {
   if (nspec <= 0 || nglob <= 0 || !ibool) return "empty mesh";
   if (tile_elems < 1 || tile_elems > 256) return "tile_elems must be in [1, 256]";
   if (ngroups < 1 || ngroups > 8) return "ngroups must be in [1, 8]";
+  if (group_tile_elems)
+    for (int k = 0; k < ngroups; ++k)
+      if (group_tile_elems[k] < 1 || group_tile_elems[k] > 256) return "tile_elems must be in [1, 256]";
   for (long long k = 0; k < static_cast<long long>(nspec) * NGLL2; ++k)
     if (ibool[k] < 0 || ibool[k] >= nglob) return "ibool entry out of range";
   if (elem_group)
@@ -67,7 +71,8 @@ std::string build_tiling(int nspec, int nglob, const int *ibool, const double *c
   T.group_tile_begin.assign(ngroups + 1, 0);
   for (int b = 0; b < nspec;) {
     int e = b + 1;
-    while (e < nspec && e - b < tile_elems && group(order[e]) == group(order[b])) ++e;
+    const int te = group_tile_elems ? group_tile_elems[group(order[b])] : tile_elems;
+    while (e < nspec && e - b < te && group(order[e]) == group(order[b])) ++e;
     tel.emplace_back(order.begin() + b, order.begin() + e);
     std::sort(tel.back().begin(), tel.back().end());
     T.group_tile_begin[group(order[b]) + 1] = static_cast<int>(tel.size());

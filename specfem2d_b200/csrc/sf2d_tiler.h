@@ -69,9 +69,11 @@ struct Tiling {
 // curve so tiles are compact; without it elements keep their input order.
 // `elem_group` (nspec values in [0, ngroups), may be null) keeps elements of
 // different groups in different tiles, group 0 first: the elements of a CPML
-// layer get tiles (and a kernel variant) of their own.
+// layer get tiles (and a kernel variant) of their own.  `group_tile_elems`
+// (ngroups values, may be null) sets a tile size per group.
 // Returns an empty string on success, else an error message.
 std::string build_tiling(int nspec, int nglob, const int *ibool, const double *centroid_xz,
-                         int tile_elems, Tiling &out, const int *elem_group = nullptr, int ngroups = 1);
+                         int tile_elems, Tiling &out, const int *elem_group = nullptr, int ngroups = 1,
+                         const int *group_tile_elems = nullptr);
 
 }  // namespace sf2d
