@@ -389,6 +389,8 @@ def main():
     ap.add_argument("--threads", type=int, default=256)
     ap.add_argument("--fluid-tile-elems", type=int, default=0, help="fluid tiles (coupled runs); 0 = --tile-elems")
     ap.add_argument("--fluid-threads", type=int, default=0, help="fluid CTA threads; 0 = --threads")
+    ap.add_argument("--pml-tile-elems", type=int, default=0, help="solid CPML tiles; 0 = --tile-elems")
+    ap.add_argument("--pml-threads", type=int, default=0, help="solid CPML CTA threads; 0 = --threads")
     ap.add_argument("--autotune", action="store_true", help="pick tile size and threads per CTA first")
     ap.add_argument("--ref-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -438,8 +440,10 @@ def main():
     def make_solver():
         if coupled:
             return CoupledSolver(db, tile_elems=args.tile_elems, threads_per_block=args.threads,
-                                 fluid_tile_elems=args.fluid_tile_elems, fluid_threads_per_block=args.fluid_threads)
-        return ElasticSolver(db, tile_elems=args.tile_elems, threads_per_block=args.threads)
+                                 fluid_tile_elems=args.fluid_tile_elems, fluid_threads_per_block=args.fluid_threads,
+                                 pml_tile_elems=args.pml_tile_elems, pml_threads_per_block=args.pml_threads)
+        return ElasticSolver(db, tile_elems=args.tile_elems, threads_per_block=args.threads,
+                             pml_tile_elems=args.pml_tile_elems, pml_threads_per_block=args.pml_threads)
 
     solver = make_solver()
     el_db = solver.sub_db if coupled else db   # the solid part the element-kernel roofline refers to
@@ -549,6 +553,8 @@ def main():
                    "nspec": db.nspec, "nglob": db.nglob, "tile_elems": args.tile_elems,
                    "fluid_tile_elems": args.fluid_tile_elems or args.tile_elems,
                    "fluid_threads_per_cta": args.fluid_threads or args.threads,
+                   "cpml_tile_elems": args.pml_tile_elems or args.tile_elems,
+                   "cpml_threads_per_cta": args.pml_threads or args.threads,
                    "threads_per_cta": args.threads, "autotuned": bool(tune),
                    "ntiles": st["ntiles"], "shared_points": nsh,
                    "nspec_fluid": solver.nspec_fluid if coupled else 0,

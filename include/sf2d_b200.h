@@ -107,14 +107,29 @@ typedef struct {
    * the layer); rho and the Jacobian per element GLL point (nspec*25) for the layer's
    * acceleration terms; the points of the layer's outer edge, zeroed every step
    * (pml_boundary_elastic, pml_compute.f90:545-574); DT in double for the
-   * convolution coefficients.  Isotropic, non-attenuating forward runs only, and
-   * not together with Stacey conditions (read_parameter_file.F90:1495). */
+   * convolution coefficients.  Isotropic forward runs only, not together with
+   * Stacey conditions (read_parameter_file.F90:1495); with attenuation, Newmark only
+   * (pml_compute_memory_variables.f90:736-741). */
   const int *pml_region;
   const double *pml_K_x, *pml_K_z, *pml_d_x, *pml_d_z, *pml_alpha_x, *pml_alpha_z;
   const float *rhostore, *jacobian;
   int npml_edge;
   const int *pml_edge_iglob;
   double pml_dt;
+  /* CPML in attenuating solids (pml_compute_memory_variables_viscoelastic,
+   * pml_compute_memory_variables.f90:546-894): pml_visco[e] = 1 for a layer element
+   * whose largest Qkappa and Qmu are both below 9998.999 (those elements take the
+   * viscoelastic update, compute_forces_viscoelastic.F90:249-267; NULL = none).  They
+   * need att_itau1/2 and att_phi1/2 above (also under Newmark), the strain relaxation
+   * times tau_epsilon_nu1/2 (nspec*25*3) and Mu_nu1/2 (nspec*25) of
+   * attenuation_model.f90:147-160. */
+  const int *pml_visco;
+  const float *att_teps1, *att_teps2;
+  const float *att_mu1, *att_mu2;
+  /* tiles of the CPML layer: elements per tile and threads per CTA (128, 250, 256
+   * or 512) of their kernel; 0 = tile_elems and threads_per_block */
+  int pml_tile_elems;
+  int pml_threads_per_block;
 } sf2d_elastic_desc;
 
 /* Builds the tiled device layout and uploads everything (fields start at 0). */

@@ -53,6 +53,7 @@ class OracleDb(ctypes.Structure):
         ("npml_bnd_el", ctypes.c_int), ("npml_bnd_ac", ctypes.c_int), ("pml_bnd_el", _ip), ("pml_bnd_ac", _ip),
         ("cpl_ac_elpt", _ip), ("cpl_el_acpt", _ip),
         ("DT", ctypes.c_double),
+        ("pml_visco", _ip), ("att_teps1", _dp), ("att_teps2", _dp), ("att_mu1", _dp), ("att_mu2", _dp),
     ]
 
 
@@ -200,6 +201,10 @@ class Oracle:
             s.pml_alpha_x, s.pml_alpha_z = d(pm["alpha_x"]), d(pm["alpha_z"])
             s.npml_bnd_el, s.pml_bnd_el = len(pm["bnd_el"]), i(pm["bnd_el"])
             s.npml_bnd_ac, s.pml_bnd_ac = len(pm["bnd_ac"]), i(pm["bnd_ac"])
+            if "visco" in pm and at is not None and np.any(pm["visco"]):
+                s.pml_visco = i(pm["visco"])
+                s.att_teps1, s.att_teps2 = d(at["teps1"]), d(at["teps2"])
+                s.att_mu1, s.att_mu2 = d(at["mu1"]), d(at["mu2"])
         if adj_src is not None:
             s.adj_src = d(adj_src)
             s.nstep_total = int(np.asarray(adj_src).shape[1])

@@ -142,6 +142,44 @@ PmlCoef l_parameters(double DT, double kx, double bx, double ax, double kz, doub
   return L;
 }
 
+// lik_parameter_computation_viscoelastic (pml_compute.f90:173-280) with the
+// two-pole split of decompose_rational_fraction_PML (pml_compute.f90:578-610):
+// A0, A1, A2 and the Zener term of one strain component and one relaxation
+// time; index_ik 13 or 31 swaps the X-only and Z-only regions.
+struct ViscoLik {
+  double A0, A1, A2, Az;
+};
+ViscoLik lik_viscoelastic(double kx, double bx, double ax, double kz, double bz, double az, int region,
+                          int index_ik, double itau, double teps) {
+  const int xo = index_ik == 13 ? CPML_X_ONLY : CPML_Z_ONLY;
+  const int zo = index_ik == 13 ? CPML_Z_ONLY : CPML_X_ONLY;
+  const auto gamma = [&](double b, double a) {
+    return (b * (itau - a * teps * itau) + a * a * (teps * itau - 1.0)) / (itau - a);
+  };
+  const auto eta = [&](double b, double a) { return itau * (b - a) / (itau - a); };
+  ViscoLik L{};
+  if (region == CPML_XZ) {
+    L.A0 = kx / kz;
+    const double a1 = ax, a2 = bz;
+    const double b1 = (a1 * a2 + a1 * a1 + 2.0 * bx * az - 2.0 * a1 * (bx + az)) / (a2 - a1);
+    const double b2 = (a1 * a2 + a2 * a2 + 2.0 * bx * az - 2.0 * a2 * (bx + az)) / (a1 - a2);
+    L.A1 = L.A0 / 2.0 * (gamma(b1, a1) - a1);
+    L.A2 = L.A0 / 2.0 * (gamma(b2, a2) - a2);
+    L.Az = L.A0 * (teps * itau - 1.0) * ((eta(b1, a1) + eta(b2, a2)) / 2.0 - itau);
+  } else if (region == xo) {
+    L.A0 = kx;
+    L.A1 = L.A0 * (gamma(bx, ax) - ax);
+    L.A2 = 0.0;
+    L.Az = L.A0 * (teps * itau - 1.0) * (eta(bx, ax) - itau);
+  } else if (region == zo) {
+    L.A0 = 1.0 / kz;
+    L.A1 = 0.0;
+    L.A2 = L.A0 * (gamma(az, bz) - bz);
+    L.Az = L.A0 * (teps * itau - 1.0) * (eta(az, bz) - itau);
+  }
+  return L;
+}
+
 struct StateBase {
   virtual ~StateBase() = default;
   virtual int run(int nstep, double *seis, int nthreads) = 0;
@@ -186,6 +224,10 @@ struct State : StateBase {
   std::vector<real> rm_fsb, rm_fsb_l;     // 2 per fluid-side coupling entry
   std::vector<real> rm_sfb, rm_sfb_l;     // 1 per solid-side coupling entry
   std::vector<real> displ_old, pot_old;
+  // CPML in attenuating solids: memory variables (nspec*25*3*6) and the Zener
+  // parameters, all read as double as the reference declares them
+  std::vector<real> rm_visco;
+  std::vector<double> teps1, teps2, vitau1, vitau2, vphi1, vphi2, mu_nu1, mu_nu2;
   std::vector<real> contrib_pml, contrib_ac_pml;
   int it = 0;  // steps done
 
@@ -320,6 +362,19 @@ struct State : StateBase {
       if (d.time_scheme != 1) {
         rm_el_l.assign(nl * 8, 0);
         rm_displ_l.assign(nl * 4, 0);
+      }
+      if (d.pml_visco) {
+        // kaPML_rmemory_dux_dxl, _duz_dzl, muPML_rmemory_dux_dxl, _duz_dzl, _dux_dzl, _duz_dxl per SLS
+        rm_visco.assign(nl * NSLS * 6, 0);
+        const size_t na = nl * NSLS;
+        teps1.assign(d.att_teps1, d.att_teps1 + na);
+        teps2.assign(d.att_teps2, d.att_teps2 + na);
+        vitau1.assign(d.att_itau1, d.att_itau1 + na);
+        vitau2.assign(d.att_itau2, d.att_itau2 + na);
+        vphi1.assign(d.att_phi1, d.att_phi1 + na);
+        vphi2.assign(d.att_phi2, d.att_phi2 + na);
+        mu_nu1.assign(d.att_mu1, d.att_mu1 + nl);
+        mu_nu2.assign(d.att_mu2, d.att_mu2 + nl);
       }
       if (acoustic) {
         rm_ac.assign(nl * 4, 0);
@@ -593,6 +648,10 @@ struct State : StateBase {
         // unmodified strains, kept for the PML stress (compute_forces_viscoelastic.F90:600-610)
         const real p_dux_dxl = dux_dxl, p_dux_dzl = dux_dzl, p_duz_dxl = duz_dxl, p_duz_dzl = duz_dzl;
         const int region = pml_region(ispec);
+        const bool visco = region > 0 && d.pml_visco && d.pml_visco[ispec];
+        // modified strains of a viscoelastic layer element (kappa and mu parts)
+        real vk_pml_xx = 0, vk_pml_zz = 0, vm_pml_xx = 0, vm_pml_zz = 0, vm_pml_xz = 0, vm_pml_zx = 0;
+        real vk_xx = 0, vk_zz = 0, vm_xx = 0, vm_zz = 0, vm_xz = 0, vm_zx = 0;
         if (region > 0) {
           // pml_compute_memory_variables_elastic (pml_compute_memory_variables.f90:230-540)
           real dxi_ox = 0, dxi_oz = 0, dg_ox = 0, dg_oz = 0;
@@ -621,10 +680,75 @@ struct State : StateBase {
           rm_update(r[5], rl[5], xz.c0_2, xz.c1_2, xz.c2_2, xz.bb2, p_dux_dzl, o_dux_dzl, stage);
           rm_update(r[6], rl[6], xz.c0_1, xz.c1_1, xz.c2_1, xz.bb1, p_duz_dzl, o_duz_dzl, stage);
           rm_update(r[7], rl[7], xz.c0_2, xz.c1_2, xz.c2_2, xz.bb2, p_duz_dzl, o_duz_dzl, stage);
-          dux_dxl = static_cast<real>(zx.A0 * p_dux_dxl + zx.A1 * r[0] + zx.A2 * r[1]);
-          duz_dxl = static_cast<real>(zx.A0 * p_duz_dxl + zx.A1 * r[2] + zx.A2 * r[3]);
-          dux_dzl = static_cast<real>(xz.A0 * p_dux_dzl + xz.A1 * r[4] + xz.A2 * r[5]);
-          duz_dzl = static_cast<real>(xz.A0 * p_duz_dzl + xz.A1 * r[6] + xz.A2 * r[7]);
+          if (visco) {
+            // pml_compute_memory_variables_viscoelastic (pml_compute_memory_variables.f90:686-892):
+            // per SLS, convolutions of the strains with 1/tau_sigma, their Zener and
+            // phi-weighted sums, then the modified strains of the kappa and mu parts
+            double A01 = 0, A10 = 0, A2k = 0, A2m = 0, A3k = 0, A3m = 0, A4k = 0, A4m = 0, A5k = 0, A5m = 0;
+            double Mk = 0, Mm = 0;
+            real ks_xx = 0, ks_zz = 0, ms_xx = 0, ms_zz = 0, ms_xz = 0, ms_zx = 0;
+            real pk_xx = 0, pk_zz = 0, pm_xx = 0, pm_zz = 0, pm_xz = 0, pm_zx = 0;
+            for (int sl = 0; sl < NSLS; ++sl) {
+              const size_t q = p * NSLS + sl;
+              const double tik = vitau1[q], tim = vitau2[q], tek = teps1[q], tem = teps2[q];
+              Mk = mu_nu1[p] * static_cast<double>(NSLS);
+              Mm = mu_nu2[p] * static_cast<double>(NSLS);
+              const double Ak = vphi1[q], Am = vphi2[q];
+              const ViscoLik k31 = lik_viscoelastic(kz, bz, az, kx, bx, ax, region, 31, tik, tek);
+              const ViscoLik m31 = lik_viscoelastic(kz, bz, az, kx, bx, ax, region, 31, tim, tem);
+              const ViscoLik k13 = lik_viscoelastic(kx, bx, ax, kz, bz, az, region, 13, tik, tek);
+              const ViscoLik m13 = lik_viscoelastic(kx, bx, ax, kz, bz, az, region, 13, tim, tem);
+              A01 = m31.A0;
+              A10 = m13.A0;
+              double ck0, ck1, ck2, cm0, cm1, cm2;
+              coef_convolution(tik, d.DT, ck0, ck1, ck2);
+              coef_convolution(tim, d.DT, cm0, cm1, cm2);
+              real *v = &rm_visco[q * 6];
+              v[0] = static_cast<real>(ck0 * v[0] + ck1 * p_dux_dxl + ck2 * o_dux_dxl);
+              v[1] = static_cast<real>(ck0 * v[1] + ck1 * p_duz_dzl + ck2 * o_duz_dzl);
+              v[2] = static_cast<real>(cm0 * v[2] + cm1 * p_dux_dxl + cm2 * o_dux_dxl);
+              v[3] = static_cast<real>(cm0 * v[3] + cm1 * p_duz_dzl + cm2 * o_duz_dzl);
+              v[4] = static_cast<real>(cm0 * v[4] + cm1 * p_dux_dzl + cm2 * o_dux_dzl);
+              v[5] = static_cast<real>(cm0 * v[5] + cm1 * p_duz_dxl + cm2 * o_duz_dxl);
+              A2k = A2k + k31.A1;
+              A2m = A2m + m31.A1;
+              A3k = A3k + k31.A2;
+              A3m = A3m + m31.A2;
+              A4k = A4k + k13.A1;
+              A4m = A4m + m13.A1;
+              A5k = A5k + k13.A2;
+              A5m = A5m + m13.A2;
+              ks_xx = static_cast<real>(ks_xx + k31.Az * v[0] / Mk);
+              ks_zz = static_cast<real>(ks_zz + k13.Az * v[1] / Mk);
+              ms_xx = static_cast<real>(ms_xx + m31.Az * v[2] / Mm);
+              ms_zz = static_cast<real>(ms_zz + m13.Az * v[3] / Mm);
+              ms_xz = static_cast<real>(ms_xz + m13.Az * v[4] / Mm);
+              ms_zx = static_cast<real>(ms_zx + m31.Az * v[5] / Mm);
+              pk_xx = static_cast<real>(pk_xx + Ak * v[0]);
+              pk_zz = static_cast<real>(pk_zz + Ak * v[1]);
+              pm_xx = static_cast<real>(pm_xx + Am * v[2]);
+              pm_zz = static_cast<real>(pm_zz + Am * v[3]);
+              pm_xz = static_cast<real>(pm_xz + Am * v[4]);
+              pm_zx = static_cast<real>(pm_zx + Am * v[5]);
+            }
+            vk_pml_xx = static_cast<real>(A01 * p_dux_dxl + ks_xx + A2k * r[0] / Mk + A3k * r[1] / Mk);
+            vk_pml_zz = static_cast<real>(A10 * p_duz_dzl + ks_zz + A4k * r[6] / Mk + A5k * r[7] / Mk);
+            vm_pml_xx = static_cast<real>(A01 * p_dux_dxl + ms_xx + A2m * r[0] / Mm + A3m * r[1] / Mm);
+            vm_pml_zz = static_cast<real>(A10 * p_duz_dzl + ms_zz + A4m * r[6] / Mm + A5m * r[7] / Mm);
+            vm_pml_xz = static_cast<real>(A10 * p_dux_dzl + ms_xz + A4m * r[4] / Mm + A5m * r[5] / Mm);
+            vm_pml_zx = static_cast<real>(A01 * p_duz_dxl + ms_zx + A2m * r[2] / Mm + A3m * r[3] / Mm);
+            vk_xx = p_dux_dxl + pk_xx;
+            vk_zz = p_duz_dzl + pk_zz;
+            vm_xx = p_dux_dxl + pm_xx;
+            vm_zz = p_duz_dzl + pm_zz;
+            vm_xz = p_dux_dzl + pm_xz;
+            vm_zx = p_duz_dxl + pm_zx;
+          } else {
+            dux_dxl = static_cast<real>(zx.A0 * p_dux_dxl + zx.A1 * r[0] + zx.A2 * r[1]);
+            duz_dxl = static_cast<real>(zx.A0 * p_duz_dxl + zx.A1 * r[2] + zx.A2 * r[3]);
+            dux_dzl = static_cast<real>(xz.A0 * p_dux_dzl + xz.A1 * r[4] + xz.A2 * r[5]);
+            duz_dzl = static_cast<real>(xz.A0 * p_duz_dzl + xz.A1 * r[6] + xz.A2 * r[7]);
+          }
           // pml_compute_accel_contribution_elastic (pml_compute_accel_contribution.f90:187-333)
           const int g = d.ibool[p];
           const real fac = rho[p] * jacobianl;
@@ -651,7 +775,13 @@ struct State : StateBase {
         const real lambdaplus2mu = lambdal + real(2) * mul;
         const real lambdalplusmul = lambdal + mul;
         real sigma_xx, sigma_zz, sigma_xz, sigma_zx;
-        if (region > 0) {
+        if (visco) {
+          // viscoelastic layer stress with the unrelaxed moduli (compute_forces_viscoelastic.F90:545-555)
+          sigma_xx = (lambdalplusmul * vk_pml_xx + mul * vm_pml_xx) + (lambdalplusmul * vk_zz - mul * vm_zz);
+          sigma_xz = (mul * vm_pml_zx + mul * vm_xz);
+          sigma_zx = (mul * vm_zx + mul * vm_pml_xz);
+          sigma_zz = (lambdalplusmul * vk_xx - mul * vm_xx) + (lambdalplusmul * vk_pml_zz + mul * vm_pml_zz);
+        } else if (region > 0) {
           // PML stress: modified strains on the diagonal pairs, not symmetric
           sigma_xx = lambdaplus2mu * dux_dxl + lambdal * p_duz_dzl;
           sigma_zz = lambdaplus2mu * duz_dzl + lambdal * p_dux_dxl;
@@ -670,7 +800,9 @@ struct State : StateBase {
           sigma_xz = static_cast<real>(C15 * dux_dxl + C35 * duz_dzl + C55 * (duz_dxl + dux_dzl));
           sigma_zx = sigma_xz;
         }
-        if (atten) {
+        // layer elements keep no attenuation memory variables
+        // (compute_attenuation_viscoelastic.f90:85)
+        if (atten && region == 0) {
           real e1s, e11s, e13s;
           attenuation(p, dux_dxl, dux_dzl, duz_dxl, duz_dzl, stage, e1s, e11s, e13s);
           sigma_xx = sigma_xx + lambdalplusmul * e1s + real(2) * mul * e11s;
@@ -1029,14 +1161,18 @@ extern "C" void *sf2d_oracle_create(const sf2d_oracle_db *db, int precision) {
   if (db->time_scheme == 2 && (!db->alpha_lddrk || !db->beta_lddrk)) return nullptr;
   if (db->ispec_is_acoustic && (!db->kappastore || !db->rmass_inverse_acoustic || db->adj_src)) return nullptr;
   if (db->pml_region) {
-    // CPML is restated for isotropic, non-attenuating elements of a forward run
+    // CPML is restated for isotropic elements of a forward run
     if (!db->pml_K_x || !db->pml_K_z || !db->pml_d_x || !db->pml_d_z || !db->pml_alpha_x || !db->pml_alpha_z ||
         db->adj_src || db->DT <= 0.0)
+      return nullptr;
+    // CPML in attenuating solids: Newmark only, as the reference
+    // (pml_compute_memory_variables.f90:736-741)
+    if (db->pml_visco && (db->time_scheme != 1 || !db->att_itau1 || !db->att_itau2 || !db->att_phi1 ||
+                          !db->att_phi2 || !db->att_teps1 || !db->att_teps2 || !db->att_mu1 || !db->att_mu2))
       return nullptr;
     for (int e = 0; e < db->nspec; ++e) {
       if (db->pml_region[e] <= 0) continue;
       if (db->ispec_is_anisotropic && db->ispec_is_anisotropic[e]) return nullptr;
-      if ((db->att_a1 || db->att_itau1) && !(db->ispec_is_acoustic && db->ispec_is_acoustic[e])) return nullptr;
     }
     if (db->ispec_is_acoustic && (!db->cpl_ac_elpt || !db->cpl_el_acpt)) return nullptr;
   }

@@ -93,6 +93,14 @@ typedef struct {
   const int *pml_bnd_el, *pml_bnd_ac;
   const int *cpl_ac_elpt, *cpl_el_acpt;                   /* other-domain element point per coupling entry */
   double DT;                                              /* time step in double (PML coefficients) */
+  /* CPML in attenuating solids, Newmark only (pml_compute_memory_variables.f90:546-894):
+   * pml_visco[e] = 1 for a layer element whose largest Qkappa and Qmu are both below
+   * 9998.999 (compute_forces_viscoelastic.F90:249-267), NULL = none; for them the Zener
+   * strain relaxation times tau_epsilon_nu1/2 (nspec*25*3) and Mu_nu1/2 (nspec*25) of
+   * attenuation_model.f90:147-160, with att_itau and att_phi above */
+  const int *pml_visco;
+  const double *att_teps1, *att_teps2;
+  const double *att_mu1, *att_mu2;
 } sf2d_oracle_db;
 
 /* Fields addressed by sf2d_oracle_get/set. */

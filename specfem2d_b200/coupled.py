@@ -186,13 +186,14 @@ class CoupledSolver:
     """Device-resident coupled fluid-solid solver for one Database."""
 
     def __init__(self, db, tile_elems: int = 32, threads_per_block: int = 256, fluid_tile_elems: int = 0,
-                 fluid_threads_per_block: int = 0):
+                 fluid_threads_per_block: int = 0, pml_tile_elems: int = 0, pml_threads_per_block: int = 0):
         """Tile sizes and threads per CTA of the solid; the fluid's default to the same."""
         lib = _lib()
         sub, fl, cp, maps = split(db)
         seismotype = int(getattr(db, "seismotype", 1))
         if sub is not None:
-            ed, keep = build_desc(sub, tile_elems, 1 if seismotype == 4 else seismotype, threads_per_block)
+            ed, keep = build_desc(sub, tile_elems, 1 if seismotype == 4 else seismotype, threads_per_block,
+                                  pml_tile_elems, pml_threads_per_block)
         else:  # fluid-only mesh
             ed, keep = time_desc(db, tile_elems, threads_per_block)
 

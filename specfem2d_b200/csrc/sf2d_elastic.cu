@@ -65,6 +65,7 @@ int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solv
   if (atten && lddrk && (!d->att_phi1 || !d->att_itau2 || !d->att_phi2))
     return fail(SF2D_ERR_INVALID, "missing LDDRK attenuation coefficients");
   const bool pml = d->pml_region != nullptr;
+  bool pml_visco = false;  // some layer elements attenuate
   std::vector<int> group;
   if (pml) {
     if (!d->pml_K_x || !d->pml_K_z || !d->pml_d_x || !d->pml_d_z || !d->pml_alpha_x || !d->pml_alpha_z ||
@@ -72,7 +73,12 @@ int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solv
       return fail(SF2D_ERR_INVALID, "missing CPML arrays");
     if (kern) return fail(SF2D_ERR_INVALID, "CPML layers are not part of the adjoint sweep");
     if (d->nstacey > 0) return fail(SF2D_ERR_INVALID, "CPML layers and Stacey conditions exclude each other");
-    if (atten) return fail(SF2D_ERR_INVALID, "CPML layers need a non-attenuating medium");
+    if (atten && lddrk)
+      return fail(SF2D_ERR_INVALID, "CPML layers in an attenuating medium need Newmark time stepping");
+    if (d->pml_visco && !atten) return fail(SF2D_ERR_INVALID, "pml_visco needs the attenuation coefficients");
+    if (d->pml_visco && (!d->att_itau1 || !d->att_itau2 || !d->att_phi1 || !d->att_phi2 || !d->att_teps1 ||
+                         !d->att_teps2 || !d->att_mu1 || !d->att_mu2))
+      return fail(SF2D_ERR_INVALID, "missing Zener parameters of the attenuating CPML layer");
     if (d->npml_edge < 0 || (d->npml_edge > 0 && !d->pml_edge_iglob))
       return fail(SF2D_ERR_INVALID, "bad CPML edge list");
     for (int k = 0; k < d->npml_edge; ++k)
@@ -84,14 +90,16 @@ int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solv
       if (r < 0 || r > 3) return fail(SF2D_ERR_INVALID, "CPML region must be 0 to 3");
       if (r > 0 && aniso && d->ispec_is_anisotropic[e]) return fail(SF2D_ERR_INVALID, "anisotropic element in a CPML layer");
       group[e] = r > 0 ? 1 : 0;
+      if (r > 0 && d->pml_visco && d->pml_visco[e]) pml_visco = true;
     }
   }
 
   auto *S = new sf2d_solver();
   std::unique_ptr<sf2d_solver> guard(S);
   const int te = d->tile_elems > 0 ? d->tile_elems : 64;
+  const int group_te[2] = {te, d->pml_tile_elems > 0 ? d->pml_tile_elems : te};
   std::string err = build_tiling(d->nspec, d->nglob, d->ibool, d->centroid_xz, te, S->T,
-                                 pml ? group.data() : nullptr, pml ? 2 : 1);
+                                 pml ? group.data() : nullptr, pml ? 2 : 1, pml ? group_te : nullptr);
   if (!err.empty()) return fail(SF2D_ERR_INVALID, "tiling: " + err);
   const Tiling &T = S->T;
   for (int k = 0; k < d->nsrc; ++k)
@@ -199,12 +207,15 @@ int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solv
   // damping data, the outer edge as per-tile local lists and a shared-point mask
   S->pml_tile0 = pml ? T.group_tile_begin[1] : T.ntiles;
   const int pml_slot0 = S->pml_tile0 < T.ntiles ? T.tiles[S->pml_tile0].elem_base : d->nspec;
-  std::vector<int> pml_set_idx, edge_local;
+  std::vector<int> pml_set_idx, edge_local, pml_vset_idx;
   std::vector<PmlSet> pml_sets;
+  std::vector<PmlVisco> pml_vsets;
   std::vector<float> pml_rhoj;
   std::vector<uint8_t> sh_edge;
   if (pml) {
     pml_build_sets(d, T.elem_order, pml_slot0, d->nspec - pml_slot0, d->pml_dt, pml_sets, pml_set_idx);
+    if (pml_visco)
+      pml_build_visco_sets(d, T.elem_order, pml_slot0, d->nspec - pml_slot0, d->pml_dt, pml_vsets, pml_vset_idx);
     for (int s = pml_slot0; s < d->nspec; ++s)
       for (int q = 0; q < NGLL2; ++q) {
         const size_t p = static_cast<size_t>(T.elem_order[s]) * NGLL2 + q;
@@ -315,6 +326,14 @@ int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solv
       SF2D_CUDA(cudaMemset(rml, 0, sizeof(float4) * std::max<size_t>(1, S->npml_q * 3)));
       P.pml_rm_l = rml;
     }
+    if (pml_visco) {
+      UP(pml_vsets, PmlVisco, pml_vsets);
+      UP(pml_vset_idx, int, pml_vset_idx);
+      float2 *vm = nullptr;
+      if ((rc = S->alloc(&vm, S->npml_q * 9))) return rc;
+      SF2D_CUDA(cudaMemset(vm, 0, sizeof(float2) * std::max<size_t>(1, S->npml_q * 9)));
+      P.pml_vm = vm;
+    }
     P.pml_slot0 = pml_slot0;
     P.DT = d->pml_dt;
     P.h_old = static_cast<double>(d->deltatsquareover2) / 2.0;
@@ -386,14 +405,27 @@ int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solv
   S->nt = d->threads_per_block > 0 ? d->threads_per_block : 256;
   if (S->nt != 128 && S->nt != 250 && S->nt != 256 && S->nt != 512)
     return fail(SF2D_ERR_INVALID, "threads_per_block must be 128, 250, 256 or 512");
+  S->pml_nt = d->pml_threads_per_block > 0 ? d->pml_threads_per_block : S->nt;
+  if (S->pml_nt != 128 && S->pml_nt != 250 && S->pml_nt != 256 && S->pml_nt != 512)
+    return fail(SF2D_ERR_INVALID, "pml_threads_per_block must be 128, 250, 256 or 512");
   if (d->nrec > 0) {
-    for (const TileInfo &t : tiles)
-      if (t.rec_n > S->nt) return fail(SF2D_ERR_INVALID, "more receivers in one tile than threads per CTA");
+    for (int t = 0; t < T.ntiles; ++t)
+      if (tiles[t].rec_n > (t < S->pml_tile0 ? S->nt : S->pml_nt))
+        return fail(SF2D_ERR_INVALID, "more receivers in one tile than threads per CTA");
   }
   S->tile_fn = pick_tile_kernel(S->nt, aniso, atten, lddrk, kern);
   if (pml) {
-    S->pml_fn = pick_pml_kernel(S->nt, lddrk);
-    S->pml_smem = tile_smem_layout(P.max_q, P.max_local, false, true).total;
+    // the layer's tiles may be smaller than the others: their kernel gets its
+    // own shared-memory layout (the largest layer tile's)
+    int pe = 0, pl = 0;
+    for (int t = S->pml_tile0; t < T.ntiles; ++t) {
+      pe = std::max(pe, tiles[t].nelem);
+      pl = std::max(pl, tiles[t].n_int + tiles[t].n_sh);
+    }
+    S->pml_max_q = pe * NGLL2;
+    S->pml_max_local = pl;
+    S->pml_fn = pick_pml_kernel(S->pml_nt, lddrk, pml_visco);
+    S->pml_smem = tile_smem_layout(S->pml_max_q, S->pml_max_local, false, true).total;
     if (S->pml_smem > 220 * 1024) return fail(SF2D_ERR_INVALID, "tile too large for shared memory");
   }
   S->lddrk = lddrk;
@@ -641,6 +673,7 @@ int sf2d_reset_solver(sf2d_solver *S) {
   if (P.rho_kl_glob) SF2D_CUDA(cudaMemsetAsync(P.rho_kl_glob, 0, sizeof(float) * ng, S->stream));
   if (P.pml_rm) SF2D_CUDA(cudaMemsetAsync(P.pml_rm, 0, sizeof(float4) * S->npml_q * 3, S->stream));
   if (P.pml_rm_l) SF2D_CUDA(cudaMemsetAsync(P.pml_rm_l, 0, sizeof(float4) * S->npml_q * 3, S->stream));
+  if (P.pml_vm) SF2D_CUDA(cudaMemsetAsync(P.pml_vm, 0, sizeof(float2) * S->npml_q * 9, S->stream));
   if (S->nrec && S->nstep_total)
     SF2D_CUDA(cudaMemsetAsync(P.seis, 0, sizeof(double) * S->nrec * S->nstep_total * 2, S->stream));
   SF2D_CUDA(cudaMemsetAsync(S->ctr, 0, 3 * sizeof(int), S->stream));

@@ -100,6 +100,12 @@ struct Params {
   // solid-side coupling entries whose fluid element lies in a CPML layer have
   // cpl_src = ~k: their pressure is formed before this kernel (k_cpl_pml_solid)
   const float *cpl_pml_p; // per layer entry k: the pressure to apply
+  // CPML in attenuating solids (Newmark): per PML point its viscoelastic set,
+  // -1 in elastic layer elements; 9 memory variables per PML point, per SLS
+  // (bulk dux_dx, duz_dz), (shear dux_dx, duz_dz), (shear dux_dz, duz_dx)
+  const PmlVisco *pml_vsets;
+  const int *pml_vset_idx;
+  float2 *pml_vm;
   int nstep_stf, nstage, nstep_seis, seismotype, nrec;
   double cosrot, sinrot;
   float dt, dto2, dt2o2;
@@ -579,10 +585,6 @@ __global__ void __launch_bounds__(NT, tile_min_blocks<NT, ANISO, ATTEN, KERN, PM
       pml_update<LDDRK>(r1.y, l1.y, cbz, c.bz, dux_dzl, o_dux_dzl, al, be, dt);
       pml_update<LDDRK>(r1.z, l1.z, cax, c.ax, duz_dzl, o_duz_dzl, al, be, dt);
       pml_update<LDDRK>(r1.w, l1.w, cbz, c.bz, duz_dzl, o_duz_dzl, al, be, dt);
-      const float m_dux_dxl = static_cast<float>(zx.A0 * dux_dxl + zx.A1 * r0.x + zx.A2 * r0.y);
-      const float m_duz_dxl = static_cast<float>(zx.A0 * duz_dxl + zx.A1 * r0.z + zx.A2 * r0.w);
-      const float m_dux_dzl = static_cast<float>(xz.A0 * dux_dzl + xz.A1 * r1.x + xz.A2 * r1.y);
-      const float m_duz_dzl = static_cast<float>(xz.A0 * duz_dzl + xz.A1 * r1.z + xz.A2 * r1.w);
       // the layer's acceleration terms at this point (pml_compute_accel_contribution.f90:187-333)
       const PmlL &Lc = c.l;  // poles alpha_x, alpha_z
       const int lq = le[q];
@@ -604,11 +606,65 @@ __global__ void __launch_bounds__(NT, tile_min_blocks<NT, ANISO, ATTEN, KERN, PM
         P.pml_rm_l[3 * ps + 1] = l1;
         P.pml_rm_l[3 * ps + 2] = ld;
       }
-      // modified strains on the diagonal pairs: the stress is not symmetric
-      const float sxx = lambdaplus2mu * m_dux_dxl + lambdal * duz_dzl;
-      const float szz = lambdaplus2mu * m_duz_dzl + lambdal * dux_dxl;
-      const float szx = mul * (duz_dxl + m_dux_dzl);
-      const float sxz = mul * (dux_dzl + m_duz_dxl);
+      float sxx, szz, szx, sxz;
+      const int vi = (ATTEN && !LDDRK) ? P.pml_vset_idx[ps] : -1;
+      if (ATTEN && !LDDRK && vi >= 0) {
+        // attenuating layer element (pml_compute_memory_variables.f90:686-892): per
+        // SLS the strains convolved with 1/tau_sigma, their Zener and phi-weighted
+        // sums; then the modified bulk (k) and shear (m) strains and the stress with
+        // the unrelaxed moduli (compute_forces_viscoelastic.F90:545-555)
+        const PmlVisco &V = P.pml_vsets[vi];
+        float2 *vm = P.pml_vm + static_cast<size_t>(ps) * 9;
+        float ks_xx = 0.f, ks_zz = 0.f, ms_xx = 0.f, ms_zz = 0.f, ms_xz = 0.f, ms_zx = 0.f;
+        float pk_xx = 0.f, pk_zz = 0.f, pm_xx = 0.f, pm_zz = 0.f, pm_xz = 0.f, pm_zx = 0.f;
+        float unused = 0.f;
+#pragma unroll
+        for (int sl = 0; sl < PML_NSLS; ++sl) {
+          float2 a = vm[3 * sl], b = vm[3 * sl + 1], c = vm[3 * sl + 2];
+          pml_update<false>(a.x, unused, V.ck[sl], 0.0, dux_dxl, o_dux_dxl, 0.f, 0.f, 0.f);
+          pml_update<false>(a.y, unused, V.ck[sl], 0.0, duz_dzl, o_duz_dzl, 0.f, 0.f, 0.f);
+          pml_update<false>(b.x, unused, V.cm[sl], 0.0, dux_dxl, o_dux_dxl, 0.f, 0.f, 0.f);
+          pml_update<false>(b.y, unused, V.cm[sl], 0.0, duz_dzl, o_duz_dzl, 0.f, 0.f, 0.f);
+          pml_update<false>(c.x, unused, V.cm[sl], 0.0, dux_dzl, o_dux_dzl, 0.f, 0.f, 0.f);
+          pml_update<false>(c.y, unused, V.cm[sl], 0.0, duz_dxl, o_duz_dxl, 0.f, 0.f, 0.f);
+          vm[3 * sl] = a;
+          vm[3 * sl + 1] = b;
+          vm[3 * sl + 2] = c;
+          ks_xx = static_cast<float>(ks_xx + V.k31[sl] * a.x);
+          ks_zz = static_cast<float>(ks_zz + V.k13[sl] * a.y);
+          ms_xx = static_cast<float>(ms_xx + V.m31[sl] * b.x);
+          ms_zz = static_cast<float>(ms_zz + V.m13[sl] * b.y);
+          ms_xz = static_cast<float>(ms_xz + V.m13[sl] * c.x);
+          ms_zx = static_cast<float>(ms_zx + V.m31[sl] * c.y);
+          pk_xx = static_cast<float>(pk_xx + V.phik[sl] * a.x);
+          pk_zz = static_cast<float>(pk_zz + V.phik[sl] * a.y);
+          pm_xx = static_cast<float>(pm_xx + V.phim[sl] * b.x);
+          pm_zz = static_cast<float>(pm_zz + V.phim[sl] * b.y);
+          pm_xz = static_cast<float>(pm_xz + V.phim[sl] * c.x);
+          pm_zx = static_cast<float>(pm_zx + V.phim[sl] * c.y);
+        }
+        const float kp_xx = static_cast<float>(V.A01 * dux_dxl + ks_xx + V.k2 * r0.x + V.k3 * r0.y);
+        const float kp_zz = static_cast<float>(V.A10 * duz_dzl + ks_zz + V.k4 * r1.z + V.k5 * r1.w);
+        const float mp_xx = static_cast<float>(V.A01 * dux_dxl + ms_xx + V.m2 * r0.x + V.m3 * r0.y);
+        const float mp_zz = static_cast<float>(V.A10 * duz_dzl + ms_zz + V.m4 * r1.z + V.m5 * r1.w);
+        const float mp_xz = static_cast<float>(V.A10 * dux_dzl + ms_xz + V.m4 * r1.x + V.m5 * r1.y);
+        const float mp_zx = static_cast<float>(V.A01 * duz_dxl + ms_zx + V.m2 * r0.z + V.m3 * r0.w);
+        const float lpm = lambdal + mul;
+        sxx = (lpm * kp_xx + mul * mp_xx) + (lpm * (duz_dzl + pk_zz) - mul * (duz_dzl + pm_zz));
+        sxz = mul * mp_zx + mul * (dux_dzl + pm_xz);
+        szx = mul * (duz_dxl + pm_zx) + mul * mp_xz;
+        szz = (lpm * (dux_dxl + pk_xx) - mul * (dux_dxl + pm_xx)) + (lpm * kp_zz + mul * mp_zz);
+      } else {
+        // modified strains on the diagonal pairs: the stress is not symmetric
+        const float m_dux_dxl = static_cast<float>(zx.A0 * dux_dxl + zx.A1 * r0.x + zx.A2 * r0.y);
+        const float m_duz_dxl = static_cast<float>(zx.A0 * duz_dxl + zx.A1 * r0.z + zx.A2 * r0.w);
+        const float m_dux_dzl = static_cast<float>(xz.A0 * dux_dzl + xz.A1 * r1.x + xz.A2 * r1.y);
+        const float m_duz_dzl = static_cast<float>(xz.A0 * duz_dzl + xz.A1 * r1.z + xz.A2 * r1.w);
+        sxx = lambdaplus2mu * m_dux_dxl + lambdal * duz_dzl;
+        szz = lambdaplus2mu * m_duz_dzl + lambdal * dux_dxl;
+        szx = mul * (duz_dxl + m_dux_dzl);
+        sxz = mul * (dux_dzl + m_duz_dxl);
+      }
       s_d1[f] = make_float2(jacobianl * (sxx * xixl + szx * xizl), jacobianl * (sxz * xixl + szz * xizl));
       s_d2[f] = make_float2(jacobianl * (sxx * gammaxl + szx * gammazl), jacobianl * (sxz * gammaxl + szz * gammazl));
       continue;

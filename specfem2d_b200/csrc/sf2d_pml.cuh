@@ -181,4 +181,148 @@ void pml_build_sets(const Desc *d, const std::vector<int> &elem_order, int slot0
   }
 }
 
+// CPML in an attenuating solid (Newmark; pml_compute_memory_variables.f90:546-894).
+// lik_parameter_computation_viscoelastic (pml_compute.f90:173-280), with the
+// two-pole split of decompose_rational_fraction_PML (:578-610) in the XZ
+// region: A0, A1, A2 and the Zener term Az of one strain component for one
+// relaxation time 1/tau_sigma and strain relaxation time tau_epsilon.
+struct PmlViscoLik {
+  double A0, A1, A2, Az;
+};
+inline PmlViscoLik pml_visco_lik(double kx, double bx, double ax, double kz, double bz, double az, int region,
+                                 bool ik13, double itau, double teps) {
+  const int xo = ik13 ? CPML_X_ONLY : CPML_Z_ONLY;
+  const int zo = ik13 ? CPML_Z_ONLY : CPML_X_ONLY;
+  const auto gamma = [&](double b, double a) {
+    return (b * (itau - a * teps * itau) + a * a * (teps * itau - 1.0)) / (itau - a);
+  };
+  const auto eta = [&](double b, double a) { return itau * (b - a) / (itau - a); };
+  PmlViscoLik L{0.0, 0.0, 0.0, 0.0};
+  if (region == CPML_XZ) {
+    L.A0 = kx / kz;
+    const double a1 = ax, a2 = bz;  // poles of the two fractions, split into (a_k, b_k)
+    const double b1 = (a1 * a2 + a1 * a1 + 2.0 * bx * az - 2.0 * a1 * (bx + az)) / (a2 - a1);
+    const double b2 = (a1 * a2 + a2 * a2 + 2.0 * bx * az - 2.0 * a2 * (bx + az)) / (a1 - a2);
+    L.A1 = L.A0 / 2.0 * (gamma(b1, a1) - a1);
+    L.A2 = L.A0 / 2.0 * (gamma(b2, a2) - a2);
+    L.Az = L.A0 * (teps * itau - 1.0) * ((eta(b1, a1) + eta(b2, a2)) / 2.0 - itau);
+  } else if (region == xo) {
+    L.A0 = kx;
+    L.A1 = L.A0 * (gamma(bx, ax) - ax);
+    L.Az = L.A0 * (teps * itau - 1.0) * (eta(bx, ax) - itau);
+  } else if (region == zo) {
+    L.A0 = 1.0 / kz;
+    L.A2 = L.A0 * (gamma(az, bz) - bz);
+    L.Az = L.A0 * (teps * itau - 1.0) * (eta(az, bz) - itau);
+  }
+  return L;
+}
+
+constexpr int PML_NSLS = 3;
+
+// Per-point coefficients of the viscoelastic layer update: for each SLS the
+// convolution weights of 1/tau_sigma for the bulk (k) and shear (m) parts,
+// the Zener terms divided by Mu = N_SLS Mu_nu (for the 31 and 13 strain
+// components) and phi; then A0 of both forms and the SLS sums of A1, A2
+// divided by Mu that weight the layer's strain memory variables.
+struct alignas(16) PmlVisco {
+  PmlConv ck[PML_NSLS], cm[PML_NSLS];
+  double k31[PML_NSLS], k13[PML_NSLS], m31[PML_NSLS], m13[PML_NSLS];  // Az / Mu
+  double phik[PML_NSLS], phim[PML_NSLS];
+  double A01, A10;
+  double k2, k3, k4, k5, m2, m3, m4, m5;  // sum over SLS of A1 (31), A2 (31), A1 (13), A2 (13), over Mu
+};
+inline PmlVisco pml_visco_set(double kx, double kz, double ax, double az, double bx, double bz, int region, double DT,
+                              const double *itau1, const double *itau2, const double *teps1, const double *teps2,
+                              const double *phi1, const double *phi2, double mu1, double mu2) {
+  PmlVisco v{};
+  const double Mk = mu1 * PML_NSLS, Mm = mu2 * PML_NSLS;
+  double s2k = 0, s2m = 0, s3k = 0, s3m = 0, s4k = 0, s4m = 0, s5k = 0, s5m = 0;
+  for (int s = 0; s < PML_NSLS; ++s) {
+    const PmlViscoLik k31 = pml_visco_lik(kz, bz, az, kx, bx, ax, region, false, itau1[s], teps1[s]);
+    const PmlViscoLik m31 = pml_visco_lik(kz, bz, az, kx, bx, ax, region, false, itau2[s], teps2[s]);
+    const PmlViscoLik k13 = pml_visco_lik(kx, bx, ax, kz, bz, az, region, true, itau1[s], teps1[s]);
+    const PmlViscoLik m13 = pml_visco_lik(kx, bx, ax, kz, bz, az, region, true, itau2[s], teps2[s]);
+    v.A01 = m31.A0;
+    v.A10 = m13.A0;
+    v.ck[s] = pml_conv(itau1[s], DT);
+    v.cm[s] = pml_conv(itau2[s], DT);
+    v.k31[s] = k31.Az / Mk;
+    v.k13[s] = k13.Az / Mk;
+    v.m31[s] = m31.Az / Mm;
+    v.m13[s] = m13.Az / Mm;
+    v.phik[s] = phi1[s];
+    v.phim[s] = phi2[s];
+    s2k += k31.A1;
+    s2m += m31.A1;
+    s3k += k31.A2;
+    s3m += m31.A2;
+    s4k += k13.A1;
+    s4m += m13.A1;
+    s5k += k13.A2;
+    s5m += m13.A2;
+  }
+  v.k2 = s2k / Mk;
+  v.k3 = s3k / Mk;
+  v.k4 = s4k / Mk;
+  v.k5 = s5k / Mk;
+  v.m2 = s2m / Mm;
+  v.m3 = s3m / Mm;
+  v.m4 = s4m / Mm;
+  v.m5 = s5m / Mm;
+  return v;
+}
+
+// Viscoelastic coefficient sets of the layer elements in slots [slot0,
+// slot0 + nslots) whose pml_visco flag is set, deduplicated on the bits of the
+// damping data and the Zener parameters; idx gets one entry per GLL point in
+// slot order, -1 for points of elastic layer elements.  Desc carries
+// pml_visco per element and att_itau1/2, att_phi1/2, att_teps1/2
+// (float, [ispec][j][i][sls]) and att_mu1/2 (float, [ispec][j][i]).
+template <typename Desc>
+void pml_build_visco_sets(const Desc *d, const std::vector<int> &elem_order, int slot0, int nslots, double DT,
+                          std::vector<PmlVisco> &sets, std::vector<int> &idx) {
+  std::map<std::vector<uint64_t>, int> seen;
+  auto bits = [](double x) {
+    uint64_t b;
+    std::memcpy(&b, &x, sizeof(b));
+    return b;
+  };
+  sets.clear();
+  idx.clear();
+  for (int s = slot0; s < slot0 + nslots; ++s) {
+    const int e = elem_order[s];
+    const int region = d->pml_region[e];
+    for (int q = 0; q < 25; ++q) {
+      if (!d->pml_visco || !d->pml_visco[e]) {
+        idx.push_back(-1);
+        continue;
+      }
+      const size_t p = static_cast<size_t>(e) * 25 + q;
+      const double kx = d->pml_K_x[p], kz = d->pml_K_z[p], dx = d->pml_d_x[p], dz = d->pml_d_z[p];
+      const double ax = d->pml_alpha_x[p], az = d->pml_alpha_z[p];
+      double it1[PML_NSLS], it2[PML_NSLS], te1[PML_NSLS], te2[PML_NSLS], ph1[PML_NSLS], ph2[PML_NSLS];
+      std::vector<uint64_t> key{static_cast<uint64_t>(region), bits(kx), bits(kz), bits(dx), bits(dz), bits(ax),
+                                bits(az), bits(d->att_mu1[p]), bits(d->att_mu2[p])};
+      for (int l = 0; l < PML_NSLS; ++l) {
+        const size_t a = p * PML_NSLS + l;
+        it1[l] = d->att_itau1[a];
+        it2[l] = d->att_itau2[a];
+        te1[l] = d->att_teps1[a];
+        te2[l] = d->att_teps2[a];
+        ph1[l] = d->att_phi1[a];
+        ph2[l] = d->att_phi2[a];
+        for (double x : {it1[l], it2[l], te1[l], te2[l], ph1[l], ph2[l]}) key.push_back(bits(x));
+      }
+      auto it = seen.find(key);
+      if (it == seen.end()) {
+        sets.push_back(pml_visco_set(kx, kz, ax, az, ax + dx / kx, az + dz / kz, region, DT, it1, it2, te1, te2, ph1,
+                                     ph2, d->att_mu1[p], d->att_mu2[p]));
+        it = seen.emplace(key, static_cast<int>(sets.size()) - 1).first;
+      }
+      idx.push_back(it->second);
+    }
+  }
+}
+
 }  // namespace sf2d

@@ -41,13 +41,19 @@ TileKernel pick_tile_kernel(bool aniso, bool atten, bool lddrk) {
   return lddrk ? k_elastic_tile<NT, false, false, true, KERN> : k_elastic_tile<NT, false, false, false, KERN>;
 }
 
-// the kernel of a CPML layer's tiles (isotropic, no attenuation, forward)
-inline TileKernel pick_pml_kernel(int nt, bool lddrk) {
+// the kernel of a CPML layer's tiles (isotropic, forward); visco: some layer
+// elements attenuate (Newmark only)
+template <int NT>
+inline TileKernel pick_pml_kernel(bool lddrk, bool visco) {
+  if (visco) return k_elastic_tile<NT, false, true, false, false, true>;
+  return lddrk ? k_elastic_tile<NT, false, false, true, false, true> : k_elastic_tile<NT, false, false, false, false, true>;
+}
+inline TileKernel pick_pml_kernel(int nt, bool lddrk, bool visco = false) {
   switch (nt) {
-    case 128: return lddrk ? k_elastic_tile<128, false, false, true, false, true> : k_elastic_tile<128, false, false, false, false, true>;
-    case 250: return lddrk ? k_elastic_tile<250, false, false, true, false, true> : k_elastic_tile<250, false, false, false, false, true>;
-    case 512: return lddrk ? k_elastic_tile<512, false, false, true, false, true> : k_elastic_tile<512, false, false, false, false, true>;
-    default: return lddrk ? k_elastic_tile<256, false, false, true, false, true> : k_elastic_tile<256, false, false, false, false, true>;
+    case 128: return pick_pml_kernel<128>(lddrk, visco);
+    case 250: return pick_pml_kernel<250>(lddrk, visco);
+    case 512: return pick_pml_kernel<512>(lddrk, visco);
+    default: return pick_pml_kernel<256>(lddrk, visco);
   }
 }
 
@@ -124,6 +130,7 @@ struct sf2d_solver {
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
   int nt = 256;  // threads per CTA of the tile kernel
+  int pml_nt = 256, pml_max_q = 0, pml_max_local = 0;  // the CPML tiles' kernel
 
   template <typename T_>
   int alloc(T_ **p, size_t count) {
@@ -173,21 +180,32 @@ struct sf2d_solver {
     SF2D_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
     return SF2D_OK;
   }
+  // parameters of the CPML tiles' kernel: its shared-memory layout is sized
+  // by the layer's largest tile
+  sf2d::Params pml_params() const {
+    sf2d::Params Q = P;
+    Q.max_q = pml_max_q;
+    Q.max_local = pml_max_local;
+    return Q;
+  }
   void launch_tile(bool record_prev, int stage) {
     const int rp = record_prev ? 1 : 0;
     if (side) {
       cudaEventRecord(ev_fork, stream);
       cudaStreamWaitEvent(side, ev_fork, 0);
-      pml_fn<<<T.ntiles - pml_tile0, nt, pml_smem, side>>>(P, rp, stage, pml_tile0);
+      pml_fn<<<T.ntiles - pml_tile0, pml_nt, pml_smem, side>>>(pml_params(), rp, stage, pml_tile0);
       cudaEventRecord(ev_join, side);
       tile_fn<<<pml_tile0, nt, smem, stream>>>(P, rp, stage, 0);
       cudaStreamWaitEvent(stream, ev_join, 0);
       return;
     }
     if (pml_tile0 > 0) tile_fn<<<pml_tile0, nt, smem, stream>>>(P, rp, stage, 0);
-    if (pml_tile0 < T.ntiles)
-      (pml_fn ? pml_fn : tile_fn)<<<T.ntiles - pml_tile0, nt, pml_fn ? pml_smem : smem, stream>>>(P, rp, stage,
-                                                                                                   pml_tile0);
+    if (pml_tile0 < T.ntiles) {
+      if (pml_fn)
+        pml_fn<<<T.ntiles - pml_tile0, pml_nt, pml_smem, stream>>>(pml_params(), rp, stage, pml_tile0);
+      else
+        tile_fn<<<T.ntiles - pml_tile0, nt, smem, stream>>>(P, rp, stage, pml_tile0);
+    }
   }
   void launch_shared(int stage) {
     const int nb = std::max(1, (P.nshared + sf2d::SHARED_NT - 1) / sf2d::SHARED_NT);

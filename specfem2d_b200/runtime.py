@@ -62,6 +62,8 @@ class ElasticDesc(ctypes.Structure):
         ("rhostore", _f), ("jacobian", _f),
         ("npml_edge", ctypes.c_int), ("pml_edge_iglob", _i),
         ("pml_dt", ctypes.c_double),
+        ("pml_visco", _i), ("att_teps1", _f), ("att_teps2", _f), ("att_mu1", _f), ("att_mu2", _f),
+        ("pml_tile_elems", ctypes.c_int), ("pml_threads_per_block", ctypes.c_int),
     ]
 
 
@@ -165,7 +167,8 @@ def member_norms_noalloc(field_ptr: int, offsets, stream: int = 0) -> np.ndarray
     return out
 
 
-def build_desc(db, tile_elems: int = 32, seismotype: int = 1, threads_per_block: int = 256):
+def build_desc(db, tile_elems: int = 32, seismotype: int = 1, threads_per_block: int = 256,
+               pml_tile_elems: int = 0, pml_threads_per_block: int = 0):
     """sf2d_elastic_desc for a setup Database; returns (desc, arrays kept alive)."""
     keep = []
 
@@ -212,6 +215,7 @@ def build_desc(db, tile_elems: int = 32, seismotype: int = 1, threads_per_block:
                                                     float(db.deltatsquareover2))
     d.tile_elems = tile_elems
     d.threads_per_block = threads_per_block
+    d.pml_tile_elems, d.pml_threads_per_block = pml_tile_elems, pml_threads_per_block
     from .setup.solver_setup import ALPHA_LDDRK, BETA_LDDRK
 
     d.time_scheme = int(db.time_scheme)
@@ -237,6 +241,13 @@ def build_desc(db, tile_elems: int = 32, seismotype: int = 1, threads_per_block:
         d.rhostore, d.jacobian = f(db.rhostore), f(db.jacobian)
         d.npml_edge, d.pml_edge_iglob = len(pm["bnd_el"]), i(pm["bnd_el"])
         d.pml_dt = float(pm["dt"])
+        if at is not None and "visco" in pm and np.any(pm["visco"]):
+            # attenuating layer elements: the Zener parameters of the viscoelastic CPML update
+            d.pml_visco = i(pm["visco"])
+            d.att_itau1, d.att_phi1 = f(at["itau1"]), f(at["phi1"])
+            d.att_itau2, d.att_phi2 = f(at["itau2"]), f(at["phi2"])
+            d.att_teps1, d.att_teps2 = f(at["teps1"]), f(at["teps2"])
+            d.att_mu1, d.att_mu2 = f(at["mu1"]), f(at["mu2"])
     return d, keep
 
 
@@ -269,9 +280,10 @@ def time_desc(db, tile_elems: int = 32, threads_per_block: int = 256):
 class ElasticSolver:
     """Device-resident elastic solver (Newmark or LDDRK) for one Database."""
 
-    def __init__(self, db, tile_elems: int = 32, seismotype: int = 1, threads_per_block: int = 256):
+    def __init__(self, db, tile_elems: int = 32, seismotype: int = 1, threads_per_block: int = 256,
+                 pml_tile_elems: int = 0, pml_threads_per_block: int = 0):
         lib = load_library()
-        d, keep = build_desc(db, tile_elems, seismotype, threads_per_block)
+        d, keep = build_desc(db, tile_elems, seismotype, threads_per_block, pml_tile_elems, pml_threads_per_block)
         h = ctypes.c_void_p()
         _check(lib.sf2d_elastic_create(ctypes.byref(d), ctypes.byref(h)))
         self._h = h

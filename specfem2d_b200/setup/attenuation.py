@@ -156,8 +156,9 @@ def compute_attenuation_coeffs(n, qref, f0, fmin, fmax):
 
 
 @lru_cache(maxsize=4096)
-def attenuation_model(qkappa: float, qmu: float, f0_ref: float, n: int = N_SLS):
-    """FP32 (inv_tau_sigma_nu1, phi_nu1, inv_tau_sigma_nu2, phi_nu2) for one (Qkappa, Qmu)."""
+def zener_parameters(qkappa: float, qmu: float, f0_ref: float, n: int = N_SLS):
+    """FP32 (inv_tau_sigma, phi, tau_epsilon, Mu) for Qkappa (nu1) and for Qmu (nu2):
+    attenuation_model.f90:147-160 (Mu = sum(tau_epsilon / tau_sigma) / N_SLS)."""
     fmin = f0_ref / 10.0
     fmax = f0_ref * 10.0
     te1, ts1 = compute_attenuation_coeffs(n, qkappa, f0_ref, fmin, fmax)
@@ -169,10 +170,14 @@ def attenuation_model(qkappa: float, qmu: float, f0_ref: float, n: int = N_SLS):
             s = s + a / b
         itau = np.array([1.0 / t for t in ts]).astype(f32)
         phi = np.array([(1.0 - a / b) / b / s for a, b in zip(te, ts)]).astype(f32)
-        return itau, phi
+        return itau, phi, np.array(te).astype(f32), f32(s / n)
 
-    it1, ph1 = parts(te1, ts1)
-    it2, ph2 = parts(te2, ts2)
+    return parts(te1, ts1), parts(te2, ts2)
+
+
+def attenuation_model(qkappa: float, qmu: float, f0_ref: float, n: int = N_SLS):
+    """FP32 (inv_tau_sigma_nu1, phi_nu1, inv_tau_sigma_nu2, phi_nu2) for one (Qkappa, Qmu)."""
+    (it1, ph1, _, _), (it2, ph2, _, _) = zener_parameters(qkappa, qmu, f0_ref, n)
     return it1, ph1, it2, ph2
 
 
@@ -195,17 +200,21 @@ def attenuation_arrays(qkappa, qmu, f0_ref: float, dt: float, no_atten_mask=None
     qk = np.asarray(qkappa, dtype=np.float64)
     qm = np.asarray(qmu, dtype=np.float64)
     shape = qk.shape + (N_SLS,)
-    out = {k: np.zeros(shape, dtype=f32) for k in ("a1", "b1", "a2", "b2", "itau1", "phi1", "itau2", "phi2")}
+    out = {k: np.zeros(shape, dtype=f32) for k in ("a1", "b1", "a2", "b2", "itau1", "phi1", "itau2", "phi2",
+                                                   "teps1", "teps2")}
+    # Mu_nu1, Mu_nu2 per point (used by CPML layers in attenuating solids)
+    out["mu1"] = np.zeros(qk.shape, dtype=f32)
+    out["mu2"] = np.zeros(qk.shape, dtype=f32)
     active = ~((qk > 9998.999) & (qm > 9998.999))
     if no_atten_mask is not None:
         active &= ~no_atten_mask
     pairs = np.unique(np.stack([qk[active], qm[active]], axis=1), axis=0) if active.any() else []
     for qkv, qmv in pairs:
         sel = active & (qk == qkv) & (qm == qmv)
-        it1, ph1, it2, ph2 = attenuation_model(float(qkv), float(qmv), float(f0_ref))
+        (it1, ph1, te1, m1), (it2, ph2, te2, m2) = zener_parameters(float(qkv), float(qmv), float(f0_ref))
         a1, b1 = newmark_coefficients(it1, ph1, dt)
         a2, b2 = newmark_coefficients(it2, ph2, dt)
         for k, v in (("a1", a1), ("b1", b1), ("a2", a2), ("b2", b2), ("itau1", it1), ("phi1", ph1),
-                     ("itau2", it2), ("phi2", ph2)):
+                     ("itau2", it2), ("phi2", ph2), ("teps1", te1), ("teps2", te2), ("mu1", m1), ("mu2", m2)):
             out[k][sel] = v
     return out

@@ -544,8 +544,16 @@ def build_database(mesh: Mesh, rho, vp, vs, sources, receivers_xz, nstep: int, d
         f0_ref = attenuation_f0
         if sources and sources[0].time_function_type not in (4, 5):
             f0_ref = sources[0].f0  # prepare_attenuation.f90:319-321
-        atten = attenuation_arrays(np.broadcast_to(np.asarray(qkappa, dtype=np.float64), shp),
-                                   np.broadcast_to(np.asarray(qmu, dtype=np.float64), shp), f0_ref, dt)
+        qk_all = np.broadcast_to(np.asarray(qkappa, dtype=np.float64), shp)
+        qm_all = np.broadcast_to(np.asarray(qmu, dtype=np.float64), shp)
+        atten = attenuation_arrays(qk_all, qm_all, f0_ref, dt)
+        if pml_db is not None:
+            # layer elements whose largest Qkappa and Qmu are both below 9998.999 take the
+            # viscoelastic CPML update, the others the elastic one
+            # (compute_forces_viscoelastic.F90:178-181, 249-267)
+            low = (qk_all.reshape(mesh.nspec, -1).max(axis=1) < 9998.999) & \
+                  (qm_all.reshape(mesh.nspec, -1).max(axis=1) < 9998.999)
+            pml_db["visco"] = ((np.asarray(pml_db["region"]) > 0) & low & ~is_ac).astype(np.int32)
     return Database(
         nspec=mesh.nspec, nglob=nglob, ibool=ibool.astype(np.int32),
         xix=geo["xix"], xiz=geo["xiz"], gammax=geo["gammax"], gammaz=geo["gammaz"],

@@ -97,6 +97,20 @@ def test_viscoelastic_example_matches_ref_seis_before_boundary_reflections():
     assert rel_l2(out[0, w, 1], seis["S0001_BXZ"][w]) < 1e-5
 
 
+def test_viscoelastic_cpml_example_matches_ref_seis_full_trace():
+    """The same example with its own CPML layers (3 elements, attenuating):
+    pml_compute_memory_variables_viscoelastic restated in the oracle; the whole
+    1400-step trace matches REF_SEIS."""
+    import oracle
+
+    cfg, seis = load_golden("attenuation_viscoelastic")
+    db = database_from_config(cfg)
+    assert db.pml is not None and int(np.sum(db.pml["visco"])) > 0
+    out = oracle.Oracle(db, 4).run(db.nstep)
+    assert rel_l2(out[0, :, 0], seis["S0001_BXX"]) < 1e-5
+    assert rel_l2(out[0, :, 1], seis["S0001_BXZ"]) < 1e-5
+
+
 def test_oracle_lddrk_close_to_newmark():
     """The LDDRK restatement (6 stages, update_displacement_LDDRK.F90) and the
     Newmark one solve the same problem: traces agree to time-discretisation error."""

@@ -54,6 +54,40 @@ def test_semi_infinite_cpml_fields_and_layer_absorbs():
     assert _close(u_gpu, o32.displ, o64.displ, 2.0)
 
 
+@pytest.mark.parametrize("tile_elems,threads", [(32, 256), (16, 250)])
+def test_attenuating_cpml_matches_oracle_and_ref_seis(tile_elems, threads):
+    """EXAMPLES/attenuation/viscoelastic with its own 3-element CPML layers in an
+    attenuating solid (Qkappa 22.3, Qmu 20, 3 SLS; 492 layer elements take the
+    viscoelastic layer update), the whole 1400-step trace against REF_SEIS, and
+    the final displacement field against the oracle."""
+    import oracle
+    from specfem2d_b200.runtime import ElasticSolver
+
+    cfg, seis = load_golden("attenuation_viscoelastic")
+    db = database_from_config(cfg)
+    assert int(np.sum(db.pml["visco"])) == 492
+    s = ElasticSolver(db, tile_elems=tile_elems, threads_per_block=threads)
+    gpu = s.run(db.nstep)
+    u_gpu = s.get_fields()[0]
+    o32, o64 = oracle.Oracle(db, 4), oracle.Oracle(db, 8)
+    r32, r64 = o32.run(db.nstep), o64.run(db.nstep)
+    assert _close(gpu, r32, r64, 2.0)
+    assert _close(u_gpu, o32.displ, o64.displ, 2.0)
+    assert rel_l2(gpu[0, :, 0], seis["S0001_BXX"]) < 1e-5
+    assert rel_l2(gpu[0, :, 1], seis["S0001_BXZ"]) < 1e-5
+
+
+def test_attenuating_cpml_with_lddrk_is_rejected():
+    """The reference stops for LDDRK in an attenuating CPML layer
+    (pml_compute_memory_variables.f90:736-741); so does the solver."""
+    from specfem2d_b200.runtime import ElasticSolver, SF2DError
+
+    cfg, _ = load_golden("attenuation_viscoelastic")
+    db = database_from_config(cfg, time_scheme=2)
+    with pytest.raises(SF2DError, match="Newmark"):
+        ElasticSolver(db)
+
+
 def test_fluid_only_cpml_pressure_matches_oracle_and_ref_seis():
     """EXAMPLES/check_absolute_amplitude_of_pressure_source_seismograms_acoustic:
     a fluid-only mesh (no solid sub-solver) with CPML on all sides (492 layer
