@@ -117,6 +117,18 @@ int sf2d_coupled_get_fields(sf2d_coupled *c, float *displ, float *veloc, float *
                             float *chi_dot, float *chi_dot_dot);
 int sf2d_coupled_set_fields(sf2d_coupled *c, const float *displ, const float *veloc, const float *accel,
                             const float *chi, const float *chi_dot, const float *chi_dot_dot);
+/* Whole-mesh numbering of the two sub-meshes: solid_points[k] (fluid_points[k])
+ * is the mesh point of the solid's (fluid's) point k, nglob_total points in
+ * all (solid_points may be NULL for a fluid-only mesh).  Set once; afterwards
+ * the _global transfers take whole-mesh arrays (displ/veloc/accel nglob_total*2,
+ * chi/chi_dot/chi_dot_dot nglob_total) and permute on the device, so the host
+ * touches no point twice.  get: points outside a field's domain read zero. */
+int sf2d_coupled_set_global_numbering(sf2d_coupled *c, int nglob_total, const int *solid_points,
+                                      const int *fluid_points);
+int sf2d_coupled_set_fields_global(sf2d_coupled *c, const float *displ, const float *veloc, const float *accel,
+                                   const float *chi, const float *chi_dot, const float *chi_dot_dot);
+int sf2d_coupled_get_fields_global(sf2d_coupled *c, float *displ, float *veloc, float *accel, float *chi,
+                                   float *chi_dot, float *chi_dot_dot);
 /* Average ms per launch of the fluid tile, fluid shared-point, solid tile and
  * solid shared-point kernels (ms[0..3]) and per step (ms[4]); advances nstep steps. */
 int sf2d_coupled_time_kernels(sf2d_coupled *c, int nstep, float *ms);

@@ -15,7 +15,7 @@ import ctypes
 
 import numpy as np
 
-from .runtime import _check, _d, _f, _i, build_desc, load_library, time_desc
+from .runtime import _check, _d, _f, _i, _seis_buffer, build_desc, load_library, time_desc
 
 _vp = ctypes.c_void_p
 
@@ -73,6 +73,9 @@ def _lib():
         lib.sf2d_coupled_get_stream.argtypes = [_vp, ctypes.POINTER(_vp)]
         lib.sf2d_coupled_solid_layout_info.argtypes = [_vp, ctypes.POINTER(ctypes.c_longlong)]
         lib.sf2d_coupled_launch_count.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]
+        lib.sf2d_coupled_set_global_numbering.argtypes = [_vp, ctypes.c_int, _i, _i]
+        lib.sf2d_coupled_set_fields_global.argtypes = [_vp, _f, _f, _f, _f, _f, _f]
+        lib.sf2d_coupled_get_fields_global.argtypes = [_vp, _f, _f, _f, _f, _f, _f]
         for n in ("create", "run", "get_fields", "set_fields", "time_kernels", "layout_info", "destroy",
                   "enqueue", "synchronize", "get_stream", "solid_layout_info", "launch_count", "prepare"):
             getattr(lib, "sf2d_coupled_" + n).restype = ctypes.c_int
@@ -254,6 +257,11 @@ class CoupledSolver:
         self._h, self._lib = h, lib
         self.nglob, self.nrec, self.nstep_total = db.nglob, len(db.rec_ispec), db.nstep
         self.solid_points, self.fluid_points = maps["solid_points"], maps["fluid_points"]
+        # whole-mesh numbering on the device: field transfers permute there
+        sp = None if sub is None else np.ascontiguousarray(self.solid_points, dtype=np.int32)
+        fp = np.ascontiguousarray(self.fluid_points, dtype=np.int32)
+        _check(lib.sf2d_coupled_set_global_numbering(h, int(db.nglob), None if sp is None else sp.ctypes.data_as(_i),
+                                                     fp.ctypes.data_as(_i)))
         self.sub_db = sub
         self.nspec_fluid, self.nglob_fluid = fl["nspec"], fl["nglob"]
         del keep
@@ -269,9 +277,10 @@ class CoupledSolver:
         except Exception:
             pass
 
-    def run(self, nstep: int, seismograms: bool = True):
-        """Advance nstep steps; returns seismograms (nrec, nstep, 2) float64 or None."""
-        seis = np.zeros((self.nrec, nstep, 2), dtype=np.float64) if seismograms else None
+    def run(self, nstep: int, seismograms: bool = True, out=None):
+        """Advance nstep steps; returns seismograms (nrec, nstep, 2) float64 (in `out` when
+        given: a C-contiguous float64 array of that shape) or None."""
+        seis = _seis_buffer(self.nrec, nstep, out) if seismograms else None
         _check(self._lib.sf2d_coupled_run(self._h, nstep, None if seis is None else seis.ctypes.data_as(_d)))
         return seis
 
@@ -290,34 +299,40 @@ class CoupledSolver:
         _check(self._lib.sf2d_coupled_get_stream(self._h, ctypes.byref(v)))
         return int(v.value or 0)
 
-    def get_fields(self):
-        """displ, veloc, accel (nglob, 2) and pot, pot_dot, pot_dot_dot (nglob,) in global numbering."""
-        ns, nf = len(self.solid_points), len(self.fluid_points)
-        sv = [np.empty((ns, 2), dtype=np.float32) for _ in range(3)]
-        fv = [np.empty(nf, dtype=np.float32) for _ in range(3)]
-        _check(self._lib.sf2d_coupled_get_fields(self._h, *[x.ctypes.data_as(_f) for x in sv + fv]))
-        out = {}
-        for k, x in zip(("displ", "veloc", "accel"), sv):
-            g = np.zeros((self.nglob, 2), dtype=np.float32)
-            g[self.solid_points] = x
-            out[k] = g
-        for k, x in zip(("pot", "pot_dot", "pot_dot_dot"), fv):
-            g = np.zeros(self.nglob, dtype=np.float32)
-            g[self.fluid_points] = x
-            out[k] = g
-        return out
+    def get_fields(self, out=None):
+        """displ, veloc, accel (nglob, 2) and pot, pot_dot, pot_dot_dot (nglob,) in global numbering
+        (points outside a field's domain read zero).  `out`: a dict of preallocated float32
+        C-contiguous arrays to fill (pinned host memory copies fastest)."""
+        shapes = {"displ": (self.nglob, 2), "veloc": (self.nglob, 2), "accel": (self.nglob, 2),
+                  "pot": (self.nglob,), "pot_dot": (self.nglob,), "pot_dot_dot": (self.nglob,)}
+        res = {}
+        for k, shp in shapes.items():
+            a = None if out is None else out.get(k)
+            if a is None:
+                a = np.empty(shp, dtype=np.float32)
+            elif a.shape != shp or a.dtype != np.float32 or not a.flags.c_contiguous:
+                raise ValueError(f"{k}: need a C-contiguous float32 array of shape {shp}")
+            res[k] = a
+        _check(self._lib.sf2d_coupled_get_fields_global(
+            self._h, *[res[k].ctypes.data_as(_f) for k in shapes]))
+        return res
 
     def set_fields(self, **fields):
         """Set displ/veloc/accel (nglob, 2) and pot/pot_dot/pot_dot_dot (nglob,) (global numbering);
-        missing fields are zeroed."""
-        arrs = []
-        for k in ("displ", "veloc", "accel"):
+        missing fields are zeroed.  Arrays are used in place when they are C-contiguous float32."""
+        ptrs, keep = [], []
+        for k, shp in (("displ", (self.nglob, 2)), ("veloc", (self.nglob, 2)), ("accel", (self.nglob, 2)),
+                       ("pot", (self.nglob,)), ("pot_dot", (self.nglob,)), ("pot_dot_dot", (self.nglob,))):
             v = fields.get(k)
-            arrs.append(None if v is None else np.ascontiguousarray(np.asarray(v, np.float32)[self.solid_points]))
-        for k in ("pot", "pot_dot", "pot_dot_dot"):
-            v = fields.get(k)
-            arrs.append(None if v is None else np.ascontiguousarray(np.asarray(v, np.float32)[self.fluid_points]))
-        _check(self._lib.sf2d_coupled_set_fields(self._h, *[None if x is None else x.ctypes.data_as(_f) for x in arrs]))
+            if v is None:
+                ptrs.append(None)
+                continue
+            a = np.ascontiguousarray(v, dtype=np.float32)
+            if a.shape != shp:
+                raise ValueError(f"{k}: expected shape {shp}, got {a.shape}")
+            keep.append(a)
+            ptrs.append(a.ctypes.data_as(_f))
+        _check(self._lib.sf2d_coupled_set_fields_global(self._h, *ptrs))
 
     def time_kernels(self, nstep: int):
         """Average ms per launch: fluid tile, fluid shared, solid tile, solid shared; and per step."""

@@ -32,6 +32,15 @@ __global__ void k_scatter_f(const float *src, const int *dev2glob, float *dst, i
   const int d = blockIdx.x * blockDim.x + threadIdx.x;
   if (d < n) dst[dev2glob[d]] = src[d];
 }
+// whole-mesh <-> solid device order (map: device point -> whole-mesh point)
+__global__ void k_gather_f2(const float2 *src, const int *map, float2 *dst, int n) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d < n) dst[d] = src[map[d]];
+}
+__global__ void k_scatter_f2(const float2 *src, const int *map, float2 *dst, int n) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d < n) dst[map[d]] = src[d];
+}
 
 using AcTileFn = void (*)(AcParams, int, int, int);
 
@@ -72,6 +81,11 @@ struct sf2d_coupled {
   std::vector<void *> allocs;
   int *d_dev2glob = nullptr;
   float *d_stage = nullptr;
+  // whole-mesh numbering (sf2d_coupled_set_global_numbering): device point ->
+  // whole-mesh point of each domain, and a whole-mesh staging buffer
+  int nglob_total = 0;
+  int *d_gmap_solid = nullptr, *d_gmap_fluid = nullptr;
+  float2 *d_gstage = nullptr;
   int *ctr = nullptr;
   double *seis = nullptr;
   sf2d::CplPml cpl_fluid{}, cpl_solid{};  // coupling entries next to a CPML layer
@@ -779,6 +793,106 @@ extern "C" int sf2d_coupled_set_fields(sf2d_coupled *C, const float *displ, cons
     SF2D_CUDA(cudaMemcpyAsync(C->d_stage, src[k], sizeof(float) * n, cudaMemcpyHostToDevice, s));
     k_gather_f<<<(n + 255) / 256, 256, 0, s>>>(C->d_stage, C->d_dev2glob, dst[k], n);
     SF2D_CUDA(cudaGetLastError());
+  }
+  SF2D_CUDA(cudaStreamSynchronize(s));
+  return SF2D_OK;
+}
+
+extern "C" int sf2d_coupled_set_global_numbering(sf2d_coupled *C, int nglob_total, const int *solid_points,
+                                                  const int *fluid_points) {
+  using namespace sf2d;
+  if (!C || nglob_total <= 0 || !fluid_points || (C->el && !solid_points))
+    return fail(SF2D_ERR_INVALID, "bad arguments");
+  if (C->d_gstage) return fail(SF2D_ERR_INVALID, "global numbering already set");
+  std::vector<int> gf(C->nglob), gs;
+  for (int d = 0; d < C->nglob; ++d) {
+    const int g = fluid_points[C->T.dev2glob[d]];
+    if (g < 0 || g >= nglob_total) return fail(SF2D_ERR_INVALID, "fluid point outside the mesh numbering");
+    gf[d] = g;
+  }
+  if (C->el) {
+    const sf2d_solver *S = C->el;
+    gs.resize(S->nglob);
+    for (int d = 0; d < S->nglob; ++d) {
+      const int g = solid_points[S->T.dev2glob[d]];
+      if (g < 0 || g >= nglob_total) return fail(SF2D_ERR_INVALID, "solid point outside the mesh numbering");
+      gs[d] = g;
+    }
+  }
+  int rc;
+  if ((rc = C->upload(&C->d_gmap_fluid, gf.data(), gf.size()))) return rc;
+  if (C->el && (rc = C->upload(&C->d_gmap_solid, gs.data(), gs.size()))) return rc;
+  if ((rc = C->alloc(&C->d_gstage, static_cast<size_t>(nglob_total)))) return rc;
+  C->nglob_total = nglob_total;
+  return SF2D_OK;
+}
+
+extern "C" int sf2d_coupled_set_fields_global(sf2d_coupled *C, const float *displ, const float *veloc,
+                                              const float *accel, const float *pot, const float *pot_dot,
+                                              const float *pot_dot_dot) {
+  using namespace sf2d;
+  if (!C) return fail(SF2D_ERR_INVALID, "null solver");
+  if (!C->d_gstage) return fail(SF2D_ERR_INVALID, "no whole-mesh numbering (sf2d_coupled_set_global_numbering)");
+  const size_t nt = static_cast<size_t>(C->nglob_total);
+  cudaStream_t s = C->stream();
+  if (C->el) {
+    sf2d_solver *S = C->el;
+    float2 *dst[3] = {S->P.u, S->P.v, S->P.a};
+    const float *src[3] = {displ, veloc, accel};
+    const int n = S->nglob;
+    for (int k = 0; k < 3; ++k) {
+      if (!src[k]) {
+        SF2D_CUDA(cudaMemsetAsync(dst[k], 0, sizeof(float2) * n, s));
+        continue;
+      }
+      SF2D_CUDA(cudaMemcpyAsync(C->d_gstage, src[k], sizeof(float2) * nt, cudaMemcpyHostToDevice, s));
+      k_gather_f2<<<(n + 255) / 256, 256, 0, s>>>(C->d_gstage, C->d_gmap_solid, dst[k], n);
+      SF2D_CUDA(cudaGetLastError());
+    }
+  }
+  float *dst[3] = {C->A.p, C->A.pd, C->A.pdd};
+  const float *src[3] = {pot, pot_dot, pot_dot_dot};
+  const int n = C->nglob;
+  float *stage = reinterpret_cast<float *>(C->d_gstage);
+  for (int k = 0; k < 3; ++k) {
+    if (!src[k]) {
+      SF2D_CUDA(cudaMemsetAsync(dst[k], 0, sizeof(float) * n, s));
+      continue;
+    }
+    SF2D_CUDA(cudaMemcpyAsync(stage, src[k], sizeof(float) * nt, cudaMemcpyHostToDevice, s));
+    k_gather_f<<<(n + 255) / 256, 256, 0, s>>>(stage, C->d_gmap_fluid, dst[k], n);
+    SF2D_CUDA(cudaGetLastError());
+  }
+  SF2D_CUDA(cudaStreamSynchronize(s));
+  return SF2D_OK;
+}
+
+extern "C" int sf2d_coupled_get_fields_global(sf2d_coupled *C, float *displ, float *veloc, float *accel, float *pot,
+                                              float *pot_dot, float *pot_dot_dot) {
+  using namespace sf2d;
+  if (!C) return fail(SF2D_ERR_INVALID, "null solver");
+  if (!C->d_gstage) return fail(SF2D_ERR_INVALID, "no whole-mesh numbering (sf2d_coupled_set_global_numbering)");
+  const size_t nt = static_cast<size_t>(C->nglob_total);
+  cudaStream_t s = C->stream();
+  float *hdst[6] = {displ, veloc, accel, pot, pot_dot, pot_dot_dot};
+  for (int k = 0; k < 6; ++k) {
+    if (!hdst[k]) continue;
+    const bool solid = k < 3;
+    // points outside the domain read zero
+    SF2D_CUDA(cudaMemsetAsync(C->d_gstage, 0, (solid ? sizeof(float2) : sizeof(float)) * nt, s));
+    if (solid && C->el) {
+      const float2 *src[3] = {C->el->P.u, C->el->P.v, C->el->P.a};
+      const int n = C->el->nglob;
+      k_scatter_f2<<<(n + 255) / 256, 256, 0, s>>>(src[k], C->d_gmap_solid, C->d_gstage, n);
+    } else if (!solid) {
+      const float *src[3] = {C->A.p, C->A.pd, C->A.pdd};
+      const int n = C->nglob;
+      k_scatter_f<<<(n + 255) / 256, 256, 0, s>>>(src[k - 3], C->d_gmap_fluid, reinterpret_cast<float *>(C->d_gstage),
+                                                   n);
+    }
+    SF2D_CUDA(cudaGetLastError());
+    SF2D_CUDA(cudaMemcpyAsync(hdst[k], C->d_gstage, (solid ? sizeof(float2) : sizeof(float)) * nt,
+                              cudaMemcpyDeviceToHost, s));
   }
   SF2D_CUDA(cudaStreamSynchronize(s));
   return SF2D_OK;

@@ -114,6 +114,14 @@ def load_library(path: str = LIB):
     return lib
 
 
+def _seis_buffer(nrec: int, nstep: int, out=None):
+    if out is None:
+        return np.zeros((nrec, nstep, 2), dtype=np.float64)
+    if out.shape != (nrec, nstep, 2) or out.dtype != np.float64 or not out.flags.c_contiguous:
+        raise ValueError(f"seismogram buffer must be C-contiguous float64 of shape {(nrec, nstep, 2)}")
+    return out
+
+
 def _check(rc):
     if rc == SF2D_OK:
         return
@@ -309,14 +317,21 @@ class ElasticSolver:
         ptrs = [None if x is None else x.ctypes.data_as(_f) for x in arrs]
         _check(self._lib.sf2d_set_fields(self._h, *ptrs))
 
-    def get_fields(self):
-        out = [np.empty((self.nglob, 2), dtype=np.float32) for _ in range(3)]
+    def get_fields(self, out=None):
+        """displ, veloc, accel (nglob, 2); `out`: three preallocated C-contiguous float32
+        arrays to fill (pinned host memory copies fastest)."""
+        if out is None:
+            out = [np.empty((self.nglob, 2), dtype=np.float32) for _ in range(3)]
+        for a in out:
+            if a.shape != (self.nglob, 2) or a.dtype != np.float32 or not a.flags.c_contiguous:
+                raise ValueError(f"need C-contiguous float32 arrays of shape {(self.nglob, 2)}")
         _check(self._lib.sf2d_get_fields(self._h, *[x.ctypes.data_as(_f) for x in out]))
         return out
 
-    def run(self, nstep: int, seismograms: bool = True):
-        """Advance nstep steps; returns seismograms (nrec, nstep, 2) float64 or None."""
-        seis = np.zeros((self.nrec, nstep, 2), dtype=np.float64) if seismograms else None
+    def run(self, nstep: int, seismograms: bool = True, out=None):
+        """Advance nstep steps; returns seismograms (nrec, nstep, 2) float64 (in `out` when
+        given: a C-contiguous float64 array of that shape) or None."""
+        seis = _seis_buffer(self.nrec, nstep, out) if seismograms else None
         _check(self._lib.sf2d_run(self._h, nstep, None if seis is None else seis.ctypes.data_as(_d)))
         return seis
 
