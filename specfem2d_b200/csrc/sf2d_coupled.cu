@@ -193,6 +193,9 @@ struct sf2d_coupled {
   // one (they only read fluid fields, which the solid kernels do not touch),
   // joined before the next fluid tile kernel
   cudaEvent_t ev_rec = nullptr, ev_rec_done = nullptr;
+  // the solid's early tiles (no coupling point) beside the fluid step
+  cudaStream_t early = nullptr;
+  cudaEvent_t ev_early_fork = nullptr, ev_early_join = nullptr;
   bool rec_pending = false;
   void launch_ac_receivers() {
     if (A.nrec <= 0) return;
@@ -213,6 +216,13 @@ struct sf2d_coupled {
   }
   void launch_step(bool record_prev) {
     for (int st = 0; st < nstage; ++st) {
+      const bool split = el && early && el->late_tile0 > 0;
+      if (split) {
+        cudaEventRecord(ev_early_fork, stream());
+        cudaStreamWaitEvent(early, ev_early_fork, 0);
+        el->launch_early(early, record_prev && st == 0, st);
+        cudaEventRecord(ev_early_join, early);
+      }
       launch_cpl_fluid(st);
       join_ac_receivers();
       launch_ac_tile(record_prev && st == 0, st);
@@ -220,7 +230,8 @@ struct sf2d_coupled {
       if (st == nstage - 1) launch_ac_receivers();
       launch_cpl_solid(st);
       if (el) {
-        el->launch_tile(record_prev && st == 0, st);
+        el->launch_tile(record_prev && st == 0, st, split ? el->late_tile0 : 0);
+        if (split) cudaStreamWaitEvent(stream(), ev_early_join, 0);
         el->launch_shared(st);
       }
     }
@@ -240,6 +251,9 @@ struct sf2d_coupled {
     if (ev_join) cudaEventDestroy(ev_join);
     if (ev_rec) cudaEventDestroy(ev_rec);
     if (ev_rec_done) cudaEventDestroy(ev_rec_done);
+    if (ev_early_fork) cudaEventDestroy(ev_early_fork);
+    if (ev_early_join) cudaEventDestroy(ev_early_join);
+    if (early) cudaStreamDestroy(early);
     if (side) cudaStreamDestroy(side);
     if (own_stream) cudaStreamDestroy(own_stream);
   }
@@ -336,7 +350,29 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
   } else {
     sf2d_elastic_desc e2 = *eld;
     if (e2.seismotype == 4 || e2.seismotype == 0) e2.seismotype = 1;
-    if (int rc = sf2d_create_solver_internal(&e2, false, &C->el)) return rc;
+    // solid elements touching a coupling point get tiles of their own (late
+    // tiles, after the fluid step); the others never touch a point the fluid
+    // reads or a fluid value, so they run beside the fluid step
+    if (eld->nglob <= 0 || !eld->ibool || (cp->ncpl_el > 0 && !cp->cpl_el_point) ||
+        (cp->ncpl_ac > 0 && !cp->cpl_ac_el_point))
+      return fail(SF2D_ERR_INVALID, "missing solid mesh or coupling points");
+    std::vector<uint8_t> cpl_pt(eld->nglob, 0), late(eld->nspec, 0);
+    for (int k = 0; k < cp->ncpl_el; ++k) {
+      const int g = cp->cpl_el_point[k];
+      if (g < 0 || g >= eld->nglob) return fail(SF2D_ERR_INVALID, "solid coupling point out of range");
+      cpl_pt[g] = 1;
+    }
+    for (int k = 0; k < cp->ncpl_ac; ++k) {
+      const int g = cp->cpl_ac_el_point[k];
+      if (g < 0 || g >= eld->nglob) return fail(SF2D_ERR_INVALID, "solid coupling point out of range");
+      cpl_pt[g] = 1;
+    }
+    for (int e = 0; e < eld->nspec; ++e)
+      for (int q = 0; q < NGLL2; ++q) {
+        const int g = eld->ibool[static_cast<size_t>(e) * NGLL2 + q];
+        if (g >= 0 && g < eld->nglob && cpl_pt[g]) late[e] = 1;
+      }
+    if (int rc = sf2d_create_solver_internal(&e2, false, &C->el, late.data())) return rc;
     S = C->el;
     C->lddrk = S->lddrk;
     C->nstage = S->nstage;
@@ -596,12 +632,19 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
     C->pml_smem = ac_smem_layout(A.max_q, A.max_local, true).total;
     if (C->pml_smem > 220 * 1024) return fail(SF2D_ERR_INVALID, "fluid tile too large for shared memory");
     if (C->pml_tile0 > 0 && C->pml_tile0 < T.ntiles) {
-      SF2D_CUDA(cudaStreamCreateWithFlags(&C->side, cudaStreamNonBlocking));
+      SF2D_CUDA(cudaStreamCreateWithPriority(&C->side, cudaStreamNonBlocking, C->el ? C->el->priority : 0));
       SF2D_CUDA(cudaEventCreateWithFlags(&C->ev_fork, cudaEventDisableTiming));
       SF2D_CUDA(cudaEventCreateWithFlags(&C->ev_join, cudaEventDisableTiming));
       SF2D_CUDA(cudaEventCreateWithFlags(&C->ev_rec, cudaEventDisableTiming));
       SF2D_CUDA(cudaEventCreateWithFlags(&C->ev_rec_done, cudaEventDisableTiming));
     }
+  }
+  if (C->el && C->el->late_tile0 > 0) {
+    int least = 0, greatest = 0;
+    SF2D_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    SF2D_CUDA(cudaStreamCreateWithPriority(&C->early, cudaStreamNonBlocking, least));
+    SF2D_CUDA(cudaEventCreateWithFlags(&C->ev_early_fork, cudaEventDisableTiming));
+    SF2D_CUDA(cudaEventCreateWithFlags(&C->ev_early_join, cudaEventDisableTiming));
   }
   {
     // the limit belongs to the kernel: only ever raise it (see the solid solver)
@@ -641,7 +684,11 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
         if (eg_tile[g] < 0) eg_tile[g] = S->T.elem_tile[e];
       }
     std::vector<std::vector<int>> by_t(S->T.ntiles);
-    for (int k = 0; k < cp->ncpl_el; ++k) by_t[eg_tile[cp->cpl_el_point[k]]].push_back(k);
+    for (int k = 0; k < cp->ncpl_el; ++k) {
+      const int t = eg_tile[cp->cpl_el_point[k]];
+      if (t < S->late_tile0) return fail(SF2D_ERR_INVALID, "coupling entry in an early tile");
+      by_t[t].push_back(k);
+    }
     std::vector<int> e_local, e_src, e_pt;
     std::vector<float4> e_nw;
     std::vector<double> e_coef;
@@ -701,7 +748,8 @@ extern "C" int sf2d_coupled_prepare(sf2d_coupled *C) {
   SF2D_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
   C->launch_chunk(K);
   SF2D_CUDA(cudaStreamEndCapture(st, &g));
-  cudaError_t e = cudaGraphInstantiate(&C->graph, g, 0);
+  // the captured kernels keep their streams' priorities
+  cudaError_t e = cudaGraphInstantiate(&C->graph, g, cudaGraphInstantiateFlagUseNodePriority);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return fail(SF2D_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
   SF2D_CUDA(cudaGraphUpload(C->graph, st));
@@ -966,7 +1014,7 @@ extern "C" int sf2d_coupled_launch_count(sf2d_coupled *C, int nstep, long long *
   const sf2d_solver *S = C->el;
   long long per_stage = (C->cpl_fluid.n > 0) + (C->pml_tile0 > 0) + (C->pml_tile0 < C->T.ntiles) + 1 +
                         (C->cpl_solid.n > 0);
-  if (S) per_stage += (S->pml_tile0 > 0) + (S->pml_tile0 < S->T.ntiles) + 1;
+  if (S) per_stage += (C->early ? S->tile_launches(S->late_tile0) + (S->late_tile0 > 0) : S->tile_launches(0)) + 1;
   const long long chunks = nstep / C->chunk + (nstep % C->chunk ? 1 : 0);
   *launches = per_stage * C->nstage * nstep + (C->A.nrec > 0 ? nstep : 0) + (S && S->nrec > 0 ? chunks : 0);
   return SF2D_OK;

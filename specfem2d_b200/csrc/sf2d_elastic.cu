@@ -32,7 +32,7 @@ const char *last_error() { return g_err.c_str(); }
 
 extern "C" const char *sf2d_last_error(void) { return sf2d::last_error(); }
 
-int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solver **out) {
+int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solver **out, const uint8_t *late_elem) {
   using namespace sf2d;
   if (!d || !out) return fail(SF2D_ERR_INVALID, "null argument");
   *out = nullptr;
@@ -89,19 +89,29 @@ int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solv
       const int r = d->pml_region[e];
       if (r < 0 || r > 3) return fail(SF2D_ERR_INVALID, "CPML region must be 0 to 3");
       if (r > 0 && aniso && d->ispec_is_anisotropic[e]) return fail(SF2D_ERR_INVALID, "anisotropic element in a CPML layer");
-      group[e] = r > 0 ? 1 : 0;
+      group[e] = r > 0 ? 2 : 0;
       if (r > 0 && d->pml_visco && d->pml_visco[e]) pml_visco = true;
     }
   }
+  // tile groups: 0 early (no point another domain reads or writes), 1 late
+  // (elements in late_elem: fluid-solid coupling), 2 CPML layer; the early
+  // tiles of a coupled step may run beside the fluid step
+  if (late_elem) {
+    if (group.empty()) group.assign(d->nspec, 0);
+    for (int e = 0; e < d->nspec; ++e)
+      if (group[e] == 0 && late_elem[e]) group[e] = 1;
+  }
+  const bool grouped = !group.empty();
 
   auto *S = new sf2d_solver();
   std::unique_ptr<sf2d_solver> guard(S);
   const int te = d->tile_elems > 0 ? d->tile_elems : 64;
-  const int group_te[2] = {te, d->pml_tile_elems > 0 ? d->pml_tile_elems : te};
+  const int group_te[3] = {te, te, d->pml_tile_elems > 0 ? d->pml_tile_elems : te};
   std::string err = build_tiling(d->nspec, d->nglob, d->ibool, d->centroid_xz, te, S->T,
-                                 pml ? group.data() : nullptr, pml ? 2 : 1, pml ? group_te : nullptr);
+                                 grouped ? group.data() : nullptr, grouped ? 3 : 1, grouped ? group_te : nullptr);
   if (!err.empty()) return fail(SF2D_ERR_INVALID, "tiling: " + err);
   const Tiling &T = S->T;
+  S->late_tile0 = late_elem ? T.group_tile_begin[1] : 0;
   for (int k = 0; k < d->nsrc; ++k)
     if (d->src_ispec[k] < 0 || d->src_ispec[k] >= d->nspec) return fail(SF2D_ERR_INVALID, "source element out of range");
   for (int k = 0; k < d->nrec; ++k)
@@ -205,7 +215,7 @@ int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solv
   }
   // CPML layer: element slots [pml_slot0, nspec) (the last tiles), per-point
   // damping data, the outer edge as per-tile local lists and a shared-point mask
-  S->pml_tile0 = pml ? T.group_tile_begin[1] : T.ntiles;
+  S->pml_tile0 = grouped ? T.group_tile_begin[2] : T.ntiles;
   const int pml_slot0 = S->pml_tile0 < T.ntiles ? T.tiles[S->pml_tile0].elem_base : d->nspec;
   std::vector<int> pml_set_idx, edge_local, pml_vset_idx;
   std::vector<PmlSet> pml_sets;
@@ -240,7 +250,15 @@ int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solv
   S->h_st_local = st_local;
   S->h_src_local = src_local;
 
-  SF2D_CUDA(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
+  // a solver split for a coupled step runs its streams at the highest
+  // priority: the other domain's step, on the critical path, shares them, and
+  // the early tiles beside it take the lowest
+  if (late_elem) {
+    int least = 0, greatest = 0;
+    SF2D_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    S->priority = greatest;
+  }
+  SF2D_CUDA(cudaStreamCreateWithPriority(&S->stream, cudaStreamNonBlocking, S->priority));
   Params &P = S->P;
   int rc = 0;
   float2 *u, *v, *a;
@@ -456,7 +474,7 @@ int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solv
 }
 
 extern "C" int sf2d_elastic_create(const sf2d_elastic_desc *d, sf2d_solver **out) {
-  return sf2d_create_solver_internal(d, false, out);
+  return sf2d_create_solver_internal(d, false, out, nullptr);
 }
 
 extern "C" int sf2d_set_fields(sf2d_solver *S, const float *displ, const float *veloc, const float *accel) {
@@ -646,7 +664,7 @@ extern "C" int sf2d_layout_info(sf2d_solver *S, long long *info) {
 
 extern "C" int sf2d_launch_count(sf2d_solver *S, int nstep, long long *launches) {
   if (!S || !launches || nstep < 0) return fail(SF2D_ERR_INVALID, "bad arguments");
-  const long long per_stage = (S->pml_tile0 > 0) + (S->pml_tile0 < S->T.ntiles) + 1;
+  const long long per_stage = S->tile_launches(0) + 1;
   const long long chunks = nstep / S->chunk + (nstep % S->chunk ? 1 : 0);
   *launches = per_stage * S->nstage * nstep + (S->nrec > 0 ? chunks : 0);
   return SF2D_OK;

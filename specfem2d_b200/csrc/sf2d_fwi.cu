@@ -53,7 +53,7 @@ extern "C" int sf2d_fwi_create(const sf2d_elastic_desc *d, const float *rhostore
   if (d->time_scheme == 2) return fail(SF2D_ERR_INVALID, "the gradient is implemented for Newmark");
   if (d->nrec < 1 || d->nstep < 1) return fail(SF2D_ERR_INVALID, "the gradient needs receivers and steps");
   auto F = std::make_unique<sf2d_fwi>();
-  int rc = sf2d_create_solver_internal(d, false, &F->fwd);
+  int rc = sf2d_create_solver_internal(d, false, &F->fwd, nullptr);
   if (rc) return rc;
   // adjoint problem: the same medium, one pseudo-source per receiver component
   // whose weights are the receiver's Lagrange products (formed in FP32)
@@ -76,7 +76,7 @@ extern "C" int sf2d_fwi_create(const sf2d_elastic_desc *d, const float *rhostore
   ad.stf = a_stf.data();
   ad.nstage = 1;
   ad.nrec = 0;
-  rc = sf2d_create_solver_internal(&ad, true, &F->adj);
+  rc = sf2d_create_solver_internal(&ad, true, &F->adj, nullptr);
   if (rc) return rc;
   F->nstep = nstep;
   F->K = checkpoint_every;

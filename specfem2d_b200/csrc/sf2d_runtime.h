@@ -131,6 +131,8 @@ struct sf2d_solver {
   int graph_steps = 0;
   int nt = 256;  // threads per CTA of the tile kernel
   int pml_nt = 256, pml_max_q = 0, pml_max_local = 0;  // the CPML tiles' kernel
+  int late_tile0 = 0;  // tiles [late_tile0, pml_tile0) touch points another domain uses
+  int priority = 0;    // of the solver's streams (0: the default, lowest)
 
   template <typename T_>
   int alloc(T_ **p, size_t count) {
@@ -175,7 +177,7 @@ struct sf2d_solver {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int make_side_stream() {
     if (side || !(pml_tile0 > 0 && pml_tile0 < T.ntiles)) return SF2D_OK;
-    SF2D_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    SF2D_CUDA(cudaStreamCreateWithPriority(&side, cudaStreamNonBlocking, priority));
     SF2D_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
     SF2D_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
     return SF2D_OK;
@@ -188,24 +190,36 @@ struct sf2d_solver {
     Q.max_local = pml_max_local;
     return Q;
   }
-  void launch_tile(bool record_prev, int stage) {
+  // Tiles [first, ntiles): the plain ones on the solver stream, the CPML ones
+  // beside them on the side stream when there is one.  first = late_tile0
+  // leaves the early tiles to launch_early.
+  void launch_tile(bool record_prev, int stage, int first = 0) {
     const int rp = record_prev ? 1 : 0;
+    const int nplain = pml_tile0 - first;
     if (side) {
       cudaEventRecord(ev_fork, stream);
       cudaStreamWaitEvent(side, ev_fork, 0);
       pml_fn<<<T.ntiles - pml_tile0, pml_nt, pml_smem, side>>>(pml_params(), rp, stage, pml_tile0);
       cudaEventRecord(ev_join, side);
-      tile_fn<<<pml_tile0, nt, smem, stream>>>(P, rp, stage, 0);
+      if (nplain > 0) tile_fn<<<nplain, nt, smem, stream>>>(P, rp, stage, first);
       cudaStreamWaitEvent(stream, ev_join, 0);
       return;
     }
-    if (pml_tile0 > 0) tile_fn<<<pml_tile0, nt, smem, stream>>>(P, rp, stage, 0);
+    if (nplain > 0) tile_fn<<<nplain, nt, smem, stream>>>(P, rp, stage, first);
     if (pml_tile0 < T.ntiles) {
       if (pml_fn)
         pml_fn<<<T.ntiles - pml_tile0, pml_nt, pml_smem, stream>>>(pml_params(), rp, stage, pml_tile0);
       else
         tile_fn<<<T.ntiles - pml_tile0, nt, smem, stream>>>(P, rp, stage, pml_tile0);
     }
+  }
+  // the early tiles [0, late_tile0) on stream s
+  void launch_early(cudaStream_t s, bool record_prev, int stage) {
+    if (late_tile0 > 0) tile_fn<<<late_tile0, nt, smem, s>>>(P, record_prev ? 1 : 0, stage, 0);
+  }
+  // tile-kernel launches of one stage of launch_tile(first)
+  int tile_launches(int first) const {
+    return (pml_tile0 - first > 0) + (pml_tile0 < T.ntiles);
   }
   void launch_shared(int stage) {
     const int nb = std::max(1, (P.nshared + sf2d::SHARED_NT - 1) / sf2d::SHARED_NT);
@@ -247,7 +261,10 @@ struct sf2d_solver {
 
 // Builds a solver; `kern` selects the adjoint variant that accumulates
 // sensitivity kernels against forward displacement frames.
-int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solver **out);
+// late_elem (may be NULL): per element 1 when another domain reads or writes
+// one of its points (fluid-solid coupling); those elements get tiles of their
+// own, launched after the other domain's step, and the rest may run beside it
+int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solver **out, const uint8_t *late_elem);
 
 // Zeroes every wavefield, memory variable, kernel sum and counter of a solver.
 int sf2d_reset_solver(sf2d_solver *S);
