@@ -387,10 +387,10 @@ def main():
     ap.add_argument("--batch", type=int, default=0, help="members per packed mesh in the FWI workloads (0 = all)")
     ap.add_argument("--tile-elems", type=int, default=32)
     ap.add_argument("--threads", type=int, default=256)
-    ap.add_argument("--fluid-tile-elems", type=int, default=0, help="fluid tiles (coupled runs); 0 = --tile-elems")
+    ap.add_argument("--fluid-tile-elems", type=int, default=64, help="fluid tiles (coupled runs); 0 = --tile-elems")
     ap.add_argument("--fluid-threads", type=int, default=0, help="fluid CTA threads; 0 = --threads")
-    ap.add_argument("--pml-tile-elems", type=int, default=0, help="solid CPML tiles; 0 = --tile-elems")
-    ap.add_argument("--pml-threads", type=int, default=0, help="solid CPML CTA threads; 0 = --threads")
+    ap.add_argument("--pml-tile-elems", type=int, default=16, help="solid CPML tiles; 0 = --tile-elems")
+    ap.add_argument("--pml-threads", type=int, default=128, help="solid CPML CTA threads; 0 = --threads")
     ap.add_argument("--autotune", action="store_true", help="pick tile size and threads per CTA first")
     ap.add_argument("--ref-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -146,6 +146,37 @@ def test_coupled_cpml_250_threads(c2_pml):
     assert _close(gpu, r32, r64)
 
 
+def test_coupled_cpml_small_layer_tiles(c2_pml):
+    """The benchmark's tile options: 64-element fluid tiles, and the solid
+    layer in 16-element tiles of its own 128-thread kernel (its shared-memory
+    layout sized by the layer's tiles)."""
+    import oracle
+    from specfem2d_b200.coupled import CoupledSolver
+
+    db = c2_pml
+    s = CoupledSolver(db, fluid_tile_elems=64, pml_tile_elems=16, pml_threads_per_block=128)
+    gpu = s.run(600)
+    f = s.get_fields()
+    o32, o64 = oracle.Oracle(db, 4), oracle.Oracle(db, 8)
+    r32, r64 = o32.run(600), o64.run(600)
+    assert _close(gpu, r32, r64)
+    assert _close(f["displ"], o32.displ, o64.displ, 2.0)
+
+
+def test_semi_infinite_cpml_small_layer_tiles():
+    """Elastic layer in 8-element tiles with 128 threads beside 32-element tiles."""
+    import oracle
+    from specfem2d_b200.runtime import ElasticSolver
+
+    cfg, seis = load_golden("semi_infinite_homogeneous")
+    db = database_from_config(cfg)
+    gpu = ElasticSolver(db, tile_elems=32, pml_tile_elems=8, pml_threads_per_block=128).run(db.nstep)
+    o32 = oracle.Oracle(db, 4).run(db.nstep)
+    o64 = oracle.Oracle(db, 8).run(db.nstep)
+    assert _close(gpu, o32, o64, 2.0)
+    assert rel_l2(gpu[0, :, 0], seis["S0001_BXX"]) < 1e-5
+
+
 def test_coupled_cpml_lddrk(c2_pml):
     """The same model with LDDRK: six stages of every memory variable."""
     import oracle
