@@ -289,6 +289,9 @@ def run_fwi(args, rank, world):
     from specfem2d_b200.distributed import max_over_ranks, shard, sum_over_ranks
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    from specfem2d_b200.runtime import initialize_device
+
+    initialize_device(int(os.environ.get("LOCAL_RANK", "0")))  # the library's own runtime, same device
     if world > 1:
         import datetime
 
@@ -414,6 +417,9 @@ def main():
     import torch
 
     torch.cuda.set_device(local_rank)
+    from specfem2d_b200.runtime import initialize_device
+
+    initialize_device(local_rank)  # the library's own CUDA runtime on the same device
     dist = None
     if world > 1:
         import datetime

@@ -33,6 +33,7 @@
  *                            fused into one tile-staged kernel per step
  *   sf2d_get_norm         <- get_norm_elastic_from_device
  *                            (src/gpu/check_fields_cuda.cu:358)
+ *   sf2d_initialize_device <- initialize_cuda_device (src/gpu/initialize_cuda.cu:50)
  *   sf2d_destroy          <- prepare_cleanup_device
  *                            (src/gpu/prepare_mesh_constants_cuda.cu:1139)
  */
@@ -131,6 +132,15 @@ typedef struct {
   int pml_tile_elems;
   int pml_threads_per_block;
 } sf2d_elastic_desc;
+
+/* Makes device rank % (visible devices) current for the calling thread, as
+ * initialize_cuda_device (src/gpu/initialize_cuda.cu:50-125) does for each MPI
+ * rank; *ndevices (may be NULL) gets the number of visible devices.  Every
+ * later call of this library on the thread uses that device.  The library
+ * links its own CUDA runtime, so a host that selected a device through another
+ * runtime (torch.cuda.set_device, say) calls this with the same rank.
+ * SF2D_ERR_CUDA when no device is visible. */
+int sf2d_initialize_device(int rank, int *ndevices);
 
 /* Builds the tiled device layout and uploads everything (fields start at 0). */
 int sf2d_elastic_create(const sf2d_elastic_desc *desc, sf2d_solver **out);

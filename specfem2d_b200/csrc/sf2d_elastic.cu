@@ -473,6 +473,21 @@ int sf2d_create_solver_internal(const sf2d_elastic_desc *d, bool kern, sf2d_solv
   return SF2D_OK;
 }
 
+extern "C" int sf2d_initialize_device(int rank, int *ndevices) {
+  if (rank < 0) return fail(SF2D_ERR_INVALID, "rank must be >= 0");
+  int n = 0;
+  const cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess) return fail(SF2D_ERR_CUDA, std::string("cudaGetDeviceCount: ") + cudaGetErrorString(e));
+  if (n == 0) return fail(SF2D_ERR_CUDA, "there is no CUDA device");
+  const int dev = rank % n;
+  SF2D_CUDA(cudaSetDevice(dev));
+  int got = -1;
+  SF2D_CUDA(cudaGetDevice(&got));
+  if (got != dev) return fail(SF2D_ERR_CUDA, "device id conflict after cudaSetDevice");
+  if (ndevices) *ndevices = n;
+  return SF2D_OK;
+}
+
 extern "C" int sf2d_elastic_create(const sf2d_elastic_desc *d, sf2d_solver **out) {
   return sf2d_create_solver_internal(d, false, out, nullptr);
 }

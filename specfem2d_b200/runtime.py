@@ -80,6 +80,7 @@ def load_library(path: str = LIB):
     lib = ctypes.CDLL(path)
     vp = ctypes.c_void_p
     sigs = {
+        "sf2d_initialize_device": [ctypes.c_int, ctypes.POINTER(ctypes.c_int)],
         "sf2d_elastic_create": [ctypes.POINTER(ElasticDesc), ctypes.POINTER(vp)],
         "sf2d_set_fields": [vp, _f, _f, _f],
         "sf2d_get_fields": [vp, _f, _f, _f],
@@ -120,6 +121,16 @@ def _seis_buffer(nrec: int, nstep: int, out=None):
     if out.shape != (nrec, nstep, 2) or out.dtype != np.float64 or not out.flags.c_contiguous:
         raise ValueError(f"seismogram buffer must be C-contiguous float64 of shape {(nrec, nstep, 2)}")
     return out
+
+
+def initialize_device(rank: int) -> int:
+    """Make device rank % (visible devices) current for this thread in the
+    library's own CUDA runtime (the reference's initialize_cuda_device); call it
+    with the same number given to torch.cuda.set_device.  Returns the number of
+    visible devices."""
+    n = ctypes.c_int(0)
+    _check(load_library().sf2d_initialize_device(int(rank), ctypes.byref(n)))
+    return int(n.value)
 
 
 def _check(rc):

@@ -143,3 +143,21 @@ def test_solvers_with_different_tile_sizes_coexist(tromp):
     assert rel_l2(a, b) < TOL
     big.close()
     small.close()
+
+
+def test_initialize_device_selects_rank_modulo_devices(tromp):
+    """sf2d_initialize_device (initialize_cuda_device): rank % visible devices
+    becomes current in the library's runtime, and a solver created afterwards
+    runs on it; a negative rank is an error."""
+    import torch
+
+    from specfem2d_b200.runtime import ElasticSolver, SF2DError, initialize_device
+
+    n = initialize_device(0)
+    assert n == torch.cuda.device_count() and n >= 1
+    assert initialize_device(n) == n  # rank n wraps to device 0
+    db, _ = tromp
+    s = ElasticSolver(db)
+    assert np.isfinite(s.run(10)).all()
+    with pytest.raises(SF2DError):
+        initialize_device(-1)
