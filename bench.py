@@ -64,6 +64,14 @@ def build_workload(name: str, nstep: int):
     return db
 
 
+# DRAM bytes one step's solid tile launches move (read + write), measured with
+# ncu on one B200 for the workload and tile configuration of the key
+# (workload, tile elements, threads, fluid tile elements, CPML tile elements,
+# CPML threads); the roofline's "traffic" reports it beside the algorithmic bytes
+TILE_TRAFFIC = {
+    ("c2_coupled", 32, 256, 64, 16, 128): 233.0e6 + 43.45e6 + 71.07e6 + 0.40e6 + 1.25e6,
+}
+
 WORKLOAD_DESC = {
     "c2_coupled": ("800x320-element (20 km x 8 km, 4,100,481 GLL points) coupled fluid-solid model: 1 km "
                    "water layer (vp 1500, rho 1020, 32,000 acoustic elements) over rock with vp 2000->4500 "
@@ -510,6 +518,8 @@ def main():
     if coupled:
         step_bytes = algorithmic_bytes_coupled(el_db.nspec, el_db.nglob, solver.nspec_fluid, solver.nglob_fluid,
                                                npml_el, npml_ac)
+    traffic_key = (args.workload, args.tile_elems, args.threads, args.fluid_tile_elems, args.pml_tile_elems,
+                   args.pml_threads)
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -586,7 +596,10 @@ def main():
                    "parallelism": f"replicas x{world}"},
         "hbm_gbs_step": step_bytes / (ms / K * 1e-3) / 1e9,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak, "traffic": TILE_TRAFFIC.get(traffic_key),
+                     "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one step's solid "
+                                        "tile launches (early, late and CPML tiles), one capture"
+                                        if traffic_key in TILE_TRAFFIC else None),
                      "kernel": "k_elastic_tile", "kernel_ms": tile_ms, "shared_kernel_ms": shared_ms,
                      "fluid_kernels_ms": k_ms[:2] if coupled else None, "step_kernels_ms": k_ms[-1],
                      "algorithmic_bytes_per_launch": tile_bytes,
