@@ -2,7 +2,7 @@
 
 Run from the repository root, in a container where the reference is mounted:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py /root/reference [example name ...]
 
 For each pinned example it writes ``<name>.json`` (the parsed Par_file
 subset, SOURCE and interfaces needed to rebuild the run, plus the source and
@@ -50,6 +50,16 @@ EXAMPLES["pressure_source_acoustic"] = (
     # fluid only, CPML on all sides, Gaussian pressure source with USE_TRICK_FOR_BETTER_PRESSURE
     "EXAMPLES/check_absolute_amplitude_of_pressure_source_seismograms_acoustic", [("S0001", "PRE")],
     "../REF_SEIS/Par_file", "../REF_SEIS/SOURCE")
+
+EXAMPLES["force_source_elastic"] = (
+    # elastic medium with 3-element CPML, vertical force at a corner shared by four elements
+    "EXAMPLES/check_absolute_amplitude_of_force_source_seismograms_elastic", [("S0001", "BXX"), ("S0001", "BXZ")],
+    "../REF_SEIS/Par_file", "../REF_SEIS/SOURCE")
+
+EXAMPLES["moment_tensor_dip_slip"] = (
+    # moment-tensor source (vertical dip slip) in an elastic medium with 3-element CPML
+    "EXAMPLES/infinite_homogeneous_moment_tensor_vertical_dip_slip", [("S0001", "BXX"), ("S0001", "BXZ")],
+    "Par_file", "SOURCE")
 
 # examples whose TOMOGRAPHY_FILE is written by a script of the reference
 TOMO_SCRIPTS = {"tomographic_ocean_model": "utils/createTomographyFile.py"}
@@ -103,8 +113,11 @@ def log_locations(path):
     return out
 
 
-def main(ref_root):
+def main(ref_root, names=None):
+    """Write the fixtures of `names` (all examples when None)."""
     for name, (rel, traces, par_file, source_file) in EXAMPLES.items():
+        if names and name not in names:
+            continue
         ex = os.path.join(ref_root, rel)
         cfg = config_from_data_dir(os.path.join(ex, "DATA"), par_file, source_file)
         cfg["log_locations"] = log_locations(os.path.join(ex, "REF_SEIS", "output.log"))
@@ -125,4 +138,5 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    # python tests/golden/make_golden.py <reference root> [example name ...]
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference", sys.argv[2:] or None)

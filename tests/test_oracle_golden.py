@@ -206,6 +206,26 @@ def test_cpml_elastic_example_matches_ref_seis():
     assert rel_l2(out[0, :, 1], seis["S0001_BXZ"]) < 1e-5
 
 
+@pytest.mark.parametrize("name,npml", [("force_source_elastic", 492), ("moment_tensor_dip_slip", 564)])
+def test_cpml_force_and_moment_tensor_examples_match_ref_seis(name, npml):
+    """EXAMPLES/check_absolute_amplitude_of_force_source_seismograms_elastic
+    (vertical force at a point shared by four elements) and
+    EXAMPLES/infinite_homogeneous_moment_tensor_vertical_dip_slip (moment-tensor
+    source, Mxz = 1, factor 1e8), both with 3-element CPML layers: source and
+    receiver elements as the reference's output.log reports them, and both
+    traces over the whole run."""
+    import oracle
+
+    cfg, seis = load_golden(name)
+    db = database_from_config(cfg)
+    assert int((db.pml["region"] > 0).sum()) == npml
+    (se, _, _), (re_, _, _) = cfg["log_locations"]
+    assert db.source_ispec[0] + 1 == se and db.rec_ispec[0] + 1 == re_
+    out = oracle.Oracle(db, 4).run(db.nstep)
+    assert rel_l2(out[0, :, 0], seis["S0001_BXX"]) < 1e-5
+    assert rel_l2(out[0, :, 1], seis["S0001_BXZ"]) < 1e-5
+
+
 def test_cpml_acoustic_pressure_example_matches_ref_seis():
     """EXAMPLES/check_absolute_amplitude_of_pressure_source_seismograms_acoustic:
     fluid only, CPML on all sides (492 PML elements), Gaussian pressure source

@@ -38,6 +38,24 @@ def test_semi_infinite_cpml_matches_oracle_and_ref_seis():
     assert rel_l2(gpu[0, :, 1], seis["S0001_BXZ"]) < 1e-5
 
 
+@pytest.mark.parametrize("name", ["force_source_elastic", "moment_tensor_dip_slip"])
+def test_force_and_moment_tensor_cpml_examples(name):
+    """EXAMPLES/check_absolute_amplitude_of_force_source_seismograms_elastic and
+    EXAMPLES/infinite_homogeneous_moment_tensor_vertical_dip_slip (3-element
+    CPML): traces against the oracle and the reference's REF_SEIS."""
+    import oracle
+    from specfem2d_b200.runtime import ElasticSolver
+
+    cfg, seis = load_golden(name)
+    db = database_from_config(cfg)
+    gpu = ElasticSolver(db).run(db.nstep)
+    o32 = oracle.Oracle(db, 4).run(db.nstep)
+    o64 = oracle.Oracle(db, 8).run(db.nstep)
+    assert _close(gpu, o32, o64, 2.0)
+    assert rel_l2(gpu[0, :, 0], seis["S0001_BXX"]) < 1e-5
+    assert rel_l2(gpu[0, :, 1], seis["S0001_BXZ"]) < 1e-5
+
+
 def test_semi_infinite_cpml_fields_and_layer_absorbs():
     """Displacement field after the run (16-element tiles) against the oracle."""
     import oracle
