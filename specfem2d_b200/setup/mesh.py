@@ -127,8 +127,14 @@ def internal_mesh(xmin, xmax, nx, interfaces, nz_layer, absorb=(True, True, Fals
     analytic top surface x -> z used instead of a spline of the top
     interface (for synthetic sinusoidal topography).
     """
-    if ngnod != 4:
-        raise NotImplementedError("internal mesher restated for NGNOD = 4")
+    if ngnod not in (4, 9):
+        raise ValueError("NGNOD must be either 4 or 9")
+    # 9-node elements: the same grid at twice the resolution, every layer's
+    # element count doubled (read_parameter_file.F90:103-108)
+    mult = 1 if ngnod == 4 else 2
+    nx_el, nz_el = nx, int(sum(nz_layer))
+    nx = nx * mult
+    nz_layer = [int(n) * mult for n in nz_layer]
     nzt = int(sum(nz_layer))
     gx = np.zeros((nx + 1, nzt + 1))
     gz = np.zeros((nx + 1, nzt + 1))
@@ -158,22 +164,44 @@ def internal_mesh(xmin, xmax, nx, interfaces, nz_layer, absorb=(True, True, Fals
                 gz[ix, iz + ioffset] = a00 * bot0 + a01 * top0
         ioffset += nzl
         xb, zb = xt, zt
-    # node numbering num_4(i,j) = j*(nx+1) + i  (get_node_number.f90)
     coorg = np.zeros(((nx + 1) * (nzt + 1), 2))
     jj, ii = np.meshgrid(np.arange(nzt + 1), np.arange(nx + 1), indexing="ij")
-    num = (jj * (nx + 1) + ii).ravel()
-    coorg[num, 0] = gx[ii.ravel(), jj.ravel()]
-    coorg[num, 1] = gz[ii.ravel(), jj.ravel()]
-    # elements in raster order, j (z) outer, i (x) inner; nodes counter-clockwise
-    ej, ei = np.meshgrid(np.arange(nzt), np.arange(nx), indexing="ij")
+    ii, jj = ii.ravel(), jj.ravel()
+    num = _num_9(ii, jj, nx_el, nz_el) if ngnod == 9 else jj * (nx + 1) + ii
+    coorg[num, 0] = gx[ii, jj]
+    coorg[num, 1] = gz[ii, jj]
+    # elements in raster order, j (z) outer, i (x) inner; corners counter-clockwise
+    # from bottom left, then (9 nodes) the bottom, right, top, left edge middles
+    # and the centre (meshfem2D.F90:132-156)
+    ej, ei = np.meshgrid(np.arange(nz_el), np.arange(nx_el), indexing="ij")
     ej, ei = ej.ravel(), ei.ravel()
-    knods = np.stack([ej * (nx + 1) + ei, ej * (nx + 1) + ei + 1,
-                      (ej + 1) * (nx + 1) + ei + 1, (ej + 1) * (nx + 1) + ei], axis=1)
-    mesh = Mesh(nspec=nx * nzt, ngnod=4, knods=knods.astype(np.int64), coorg=coorg, nx=nx, nz=nzt)
+    if ngnod == 4:
+        knods = np.stack([ej * (nx + 1) + ei, ej * (nx + 1) + ei + 1,
+                          (ej + 1) * (nx + 1) + ei + 1, (ej + 1) * (nx + 1) + ei], axis=1)
+    else:
+        gi, gj = 2 * ei, 2 * ej
+        knods = np.stack([_num_9(gi + a, gj + b, nx_el, nz_el)
+                          for a, b in ((0, 0), (2, 0), (2, 2), (0, 2), (1, 0), (2, 1), (1, 2), (0, 1), (1, 1))],
+                         axis=1)
+    mesh = Mesh(nspec=nx_el * nz_el, ngnod=ngnod, knods=knods.astype(np.int64), coorg=coorg, nx=nx_el, nz=nz_el)
     _absorbing_edges(mesh, absorb)
     mesh.free_top = not absorb[2]
     mesh.absorb = tuple(bool(a) for a in absorb)
     return mesh
+
+
+def _num_9(i, j, nx, nz):
+    """0-based control-node id of the point (i, j) of the double-resolution grid
+    of a 9-node mesh with nx x nz elements (num_9, get_node_number.f90:65-83):
+    corners first, then the horizontal edge middles, then the rows of vertical
+    edge middles and centres."""
+    i, j = np.asarray(i), np.asarray(j)
+    corner = (i % 2 == 0) & (j % 2 == 0)
+    even_row = (j % 2 == 0)
+    n_corner = (nx + 1) * (nz + 1)
+    return np.where(corner, j // 2 * (nx + 1) + i // 2,
+                    np.where(even_row, n_corner + j // 2 * nx + (i + 1) // 2 - 1,
+                             n_corner + nx * (nz + 1) + j // 2 * (2 * nx + 1) + i))
 
 
 def _absorbing_edges(mesh: Mesh, absorb) -> None:

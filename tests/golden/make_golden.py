@@ -61,6 +61,12 @@ EXAMPLES["moment_tensor_dip_slip"] = (
     "EXAMPLES/infinite_homogeneous_moment_tensor_vertical_dip_slip", [("S0001", "BXX"), ("S0001", "BXZ")],
     "Par_file", "SOURCE")
 
+EXAMPLES["topography_fluid_layer"] = (
+    # 9-node elements (curved topography), fluid layer, 3-element CPML; the reference
+    # stored the traces of the first of its two receiver lines (11 stations)
+    "EXAMPLES/simple_topography_and_also_a_simple_fluid_layer",
+    [(f"S{k:04d}", c) for k in range(1, 12) for c in ("BXX", "BXZ")], "Par_file", "SOURCE")
+
 # examples whose TOMOGRAPHY_FILE is written by a script of the reference
 TOMO_SCRIPTS = {"tomographic_ocean_model": "utils/createTomographyFile.py"}
 

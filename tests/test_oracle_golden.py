@@ -226,6 +226,21 @@ def test_cpml_force_and_moment_tensor_examples_match_ref_seis(name, npml):
     assert rel_l2(out[0, :, 1], seis["S0001_BXZ"]) < 1e-5
 
 
+def test_nine_node_topography_fluid_example_matches_ref_seis():
+    """EXAMPLES/simple_topography_and_also_a_simple_fluid_layer: 9-node
+    (NGNOD = 9) elements under a curved surface, a fluid layer, 3-element CPML;
+    the 11 stored stations over the whole run."""
+    import oracle
+
+    cfg, seis = load_golden("topography_fluid_layer")
+    db = database_from_config(cfg)
+    assert db.mesh.ngnod == 9 and db.acoustic is not None and db.pml is not None
+    out = oracle.Oracle(db, 4).run(db.nstep)
+    for k in range(11):
+        for c, comp in enumerate(("BXX", "BXZ")):
+            assert rel_l2(out[k, :, c], seis[f"S{k + 1:04d}_{comp}"]) < 1e-5
+
+
 def test_cpml_acoustic_pressure_example_matches_ref_seis():
     """EXAMPLES/check_absolute_amplitude_of_pressure_source_seismograms_acoustic:
     fluid only, CPML on all sides (492 PML elements), Gaussian pressure source

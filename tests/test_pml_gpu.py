@@ -56,6 +56,23 @@ def test_force_and_moment_tensor_cpml_examples(name):
     assert rel_l2(gpu[0, :, 1], seis["S0001_BXZ"]) < 1e-5
 
 
+def test_nine_node_topography_fluid_example():
+    """EXAMPLES/simple_topography_and_also_a_simple_fluid_layer (9-node elements,
+    fluid layer, CPML): the coupled solver against the oracle and REF_SEIS."""
+    import oracle
+    from specfem2d_b200.coupled import CoupledSolver
+
+    cfg, seis = load_golden("topography_fluid_layer")
+    db = database_from_config(cfg)
+    gpu = CoupledSolver(db).run(db.nstep)
+    o32 = oracle.Oracle(db, 4).run(db.nstep)
+    o64 = oracle.Oracle(db, 8).run(db.nstep)
+    assert _close(gpu, o32, o64, 2.0)
+    for k in range(11):
+        assert rel_l2(gpu[k, :, 0], seis[f"S{k + 1:04d}_BXX"]) < 1e-5
+        assert rel_l2(gpu[k, :, 1], seis[f"S{k + 1:04d}_BXZ"]) < 1e-5
+
+
 def test_semi_infinite_cpml_fields_and_layer_absorbs():
     """Displacement field after the run (16-element tiles) against the oracle."""
     import oracle
