@@ -11,12 +11,17 @@
 // src/specfem2D/compute_forces_viscoelastic_calling_routine.F90:58-100, all
 // elements are "inner" with one process), then element contributions in
 // ascending element order.  Element work is spread over host threads into
-// a per-element buffer and assembled serially, so results do not depend on
-// the thread count.
+// a per-element buffer; assembly gathers, per global point, the contributions
+// of its elements in ascending element order (the serial loop's order at every
+// point), so results do not depend on the thread count.
 #include "sf2d_oracle.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <condition_variable>
+#include <functional>
+#include <mutex>
 #include <cstdlib>
 #include <cstring>
 #include <thread>
@@ -35,23 +40,94 @@ int default_threads() {
   return n ? static_cast<int>(n) : 1;
 }
 
-// Static block partition of [0, n) over `nt` threads.
+// Persistent worker threads.  run(n, nt, f) splits [0, n) into nt static
+// blocks, runs block 0 on the calling thread and the others on the workers,
+// and returns when every block is done.  Workers spin briefly on a generation
+// counter before sleeping, so one call costs microseconds, not a thread
+// start per block.  Callers are serialised: a second State waits its turn.
+class Pool {
+ public:
+  static Pool &get() {
+    static Pool p;
+    return p;
+  }
+  template <typename F>
+  void run(int n, int nt, F &&f) {
+    nt = std::max(1, std::min(nt, n));
+    if (nt == 1) {
+      f(0, n);
+      return;
+    }
+    std::lock_guard<std::mutex> call(call_m_);
+    while (static_cast<int>(workers_.size()) < nt - 1) {
+      // a new worker starts from the current generation, so it takes the
+      // job published below even if it first runs after the publication
+      const int k = static_cast<int>(workers_.size()) + 1;
+      const unsigned g0 = gen_.load(std::memory_order_acquire);
+      workers_.emplace_back([this, k, g0] { worker(k, g0); });
+    }
+    job_ = [&f, n, nt](int k) {
+      const int b = static_cast<int>(static_cast<long long>(n) * k / nt);
+      const int e = static_cast<int>(static_cast<long long>(n) * (k + 1) / nt);
+      if (b < e) f(b, e);
+    };
+    nblocks_ = nt;
+    pending_.store(static_cast<int>(workers_.size()), std::memory_order_relaxed);
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      gen_.fetch_add(1, std::memory_order_release);
+    }
+    cv_.notify_all();
+    job_(0);
+    while (pending_.load(std::memory_order_acquire) != 0) relax();
+  }
+  ~Pool() {
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      stop_.store(true, std::memory_order_release);
+      gen_.fetch_add(1, std::memory_order_release);
+    }
+    cv_.notify_all();
+    for (auto &t : workers_) t.join();
+  }
+
+ private:
+  static void relax() {
+#if defined(__x86_64__)
+    __builtin_ia32_pause();
+#endif
+  }
+  void worker(int k, unsigned seen) {
+    for (;;) {
+      for (int spin = 0; spin < 20000 && gen_.load(std::memory_order_acquire) == seen; ++spin) relax();
+      if (gen_.load(std::memory_order_acquire) == seen) {
+        std::unique_lock<std::mutex> lk(m_);
+        cv_.wait(lk, [&] { return gen_.load(std::memory_order_acquire) != seen; });
+      }
+      seen = gen_.load(std::memory_order_acquire);
+      if (stop_.load(std::memory_order_acquire)) return;
+      if (k < nblocks_) job_(k);
+      pending_.fetch_sub(1, std::memory_order_release);
+    }
+  }
+  std::vector<std::thread> workers_;
+  std::mutex call_m_, m_;
+  std::condition_variable cv_;
+  std::atomic<unsigned> gen_{0};
+  std::atomic<int> pending_{0};
+  std::atomic<bool> stop_{false};
+  std::function<void(int)> job_;
+  int nblocks_ = 0;
+};
+
 template <typename F>
 void parallel_for(int n, int nt, F &&f) {
-  nt = std::max(1, std::min(nt, n));
-  if (nt == 1) {
-    f(0, n);
-    return;
-  }
-  std::vector<std::thread> pool;
-  pool.reserve(nt);
-  for (int t = 0; t < nt; ++t) {
-    const int b = static_cast<int>(static_cast<long long>(n) * t / nt);
-    const int e = static_cast<int>(static_cast<long long>(n) * (t + 1) / nt);
-    pool.emplace_back([&f, b, e] { f(b, e); });
-  }
-  for (auto &th : pool) th.join();
+  Pool::get().run(n, nt, std::forward<F>(f));
 }
+
+// Point loops go parallel from this many global points on (smaller meshes
+// finish a loop in microseconds).
+constexpr int POINT_PARALLEL_MIN = 16384;
 
 template <typename real>
 std::vector<real> cvt(const double *p, size_t n) {
@@ -229,6 +305,9 @@ struct State : StateBase {
   std::vector<real> rm_visco;
   std::vector<double> teps1, teps2, vitau1, vitau2, vphi1, vphi2, mu_nu1, mu_nu2;
   std::vector<real> contrib_pml, contrib_ac_pml;
+  // per global point, the (element * 25 + GLL point) entries of its solid and
+  // of its fluid elements in ascending element order (gather assembly)
+  std::vector<int> gat_el_off, gat_el, gat_ac_off, gat_ac;
   int it = 0;  // steps done
 
   bool is_acoustic(int e) const { return acoustic && d.ispec_is_acoustic[e] != 0; }
@@ -391,6 +470,30 @@ struct State : StateBase {
         }
       }
     }
+    build_gather(false, gat_el_off, gat_el);
+    if (acoustic) build_gather(true, gat_ac_off, gat_ac);
+  }
+
+  void build_gather(bool fluid, std::vector<int> &off, std::vector<int> &idx) const {
+    off.assign(static_cast<size_t>(nglob) + 1, 0);
+    for (int e = 0; e < nspec; ++e)
+      if (is_acoustic(e) == fluid)
+        for (int q = 0; q < NGLL2; ++q) ++off[d.ibool[static_cast<size_t>(e) * NGLL2 + q] + 1];
+    for (int g = 0; g < nglob; ++g) off[g + 1] += off[g];
+    idx.assign(off[nglob], 0);
+    std::vector<int> fill(off.begin(), off.end() - 1);
+    for (int e = 0; e < nspec; ++e)
+      if (is_acoustic(e) == fluid)
+        for (int q = 0; q < NGLL2; ++q) {
+          const int g = d.ibool[static_cast<size_t>(e) * NGLL2 + q];
+          idx[fill[g]++] = e * NGLL2 + q;
+        }
+  }
+
+  // Runs f(b, e) over blocks of [0, nglob) on the pool when the mesh is large.
+  template <typename F>
+  void points_for(int nt, F &&f) const {
+    parallel_for(nglob, nglob >= POINT_PARALLEL_MIN ? nt : 1, std::forward<F>(f));
   }
 
   // Zeroes the outer PML edge points (pml_boundary_elastic/_acoustic, pml_compute.f90:502-574)
@@ -551,16 +654,16 @@ struct State : StateBase {
           acoustic_element_force(e, stage, &contrib_ac[static_cast<size_t>(e) * NGLL2],
                                  pml ? &contrib_ac_pml[static_cast<size_t>(e) * NGLL2] : nullptr);
     });
-    for (int e = 0; e < nspec; ++e) {
-      if (!is_acoustic(e)) continue;
-      const real *c = &contrib_ac[static_cast<size_t>(e) * NGLL2];
-      const int *ib = &d.ibool[static_cast<size_t>(e) * NGLL2];
-      for (int q = 0; q < NGLL2; ++q) pot_dd[ib[q]] = pot_dd[ib[q]] - c[q];
-      if (pml_region(e) > 0) {
-        const real *cp = &contrib_ac_pml[static_cast<size_t>(e) * NGLL2];
-        for (int q = 0; q < NGLL2; ++q) pot_dd[ib[q]] = pot_dd[ib[q]] - cp[q];
-      }
-    }
+    // each point takes its elements' contributions in ascending element order,
+    // an element's layer term right after its weak-form term
+    points_for(nt, [&](int b, int e1_) {
+      for (int g = b; g < e1_; ++g)
+        for (int k = gat_ac_off[g]; k < gat_ac_off[g + 1]; ++k) {
+          const int eq = gat_ac[k];
+          pot_dd[g] = pot_dd[g] - contrib_ac[eq];
+          if (pml_region(eq / NGLL2) > 0) pot_dd[g] = pot_dd[g] - contrib_ac_pml[eq];
+        }
+    });
     pml_boundary_acoustic();
   }
 
@@ -897,25 +1000,20 @@ struct State : StateBase {
           element_force(e, stage, &contrib[static_cast<size_t>(e) * NGLL2 * 2],
                         pml ? &contrib_pml[static_cast<size_t>(e) * NGLL2 * 2] : nullptr);
     });
-    for (int e = 0; e < nspec; ++e) {
-      if (is_acoustic(e)) continue;
-      const real *c = &contrib[static_cast<size_t>(e) * NGLL2 * 2];
-      const int *ib = &d.ibool[static_cast<size_t>(e) * NGLL2];
-      for (int q = 0; q < NGLL2; ++q) {
-        const int g = ib[q];
-        accel[2 * g] = accel[2 * g] - c[2 * q];
-        accel[2 * g + 1] = accel[2 * g + 1] - c[2 * q + 1];
-      }
-      if (pml_region(e) > 0) {
-        // the element's PML contribution after its weak-form terms (compute_forces_viscoelastic.F90:785-797)
-        const real *cp = &contrib_pml[static_cast<size_t>(e) * NGLL2 * 2];
-        for (int q = 0; q < NGLL2; ++q) {
-          const int g = ib[q];
-          accel[2 * g] = accel[2 * g] - cp[2 * q];
-          accel[2 * g + 1] = accel[2 * g + 1] - cp[2 * q + 1];
+    // gather in ascending element order per point; the element's PML
+    // contribution right after its weak-form terms (compute_forces_viscoelastic.F90:785-797)
+    points_for(nt, [&](int b, int e1_) {
+      for (int g = b; g < e1_; ++g)
+        for (int k = gat_el_off[g]; k < gat_el_off[g + 1]; ++k) {
+          const int eq = gat_el[k];
+          accel[2 * g] = accel[2 * g] - contrib[2 * eq];
+          accel[2 * g + 1] = accel[2 * g + 1] - contrib[2 * eq + 1];
+          if (pml_region(eq / NGLL2) > 0) {
+            accel[2 * g] = accel[2 * g] - contrib_pml[2 * eq];
+            accel[2 * g + 1] = accel[2 * g + 1] - contrib_pml[2 * eq + 1];
+          }
         }
-      }
-    }
+    });
   }
 
   // Receiver in an acoustic element (write_seismograms.F90:75-150):
@@ -989,47 +1087,56 @@ struct State : StateBase {
 
   int run(int nstep, double *seis, int nthreads) override {
     const int nt = nthreads > 0 ? nthreads : default_threads();
-    const size_t ng = static_cast<size_t>(nglob) * 2;
     for (int s = 0; s < nstep; ++s, ++it) {
       if (d.time_scheme == 1) {
         if (pml) {
           // mid-step fields of the CPML convolutions (update_displacement_Newmark.F90:374-380, 429-433)
           const double h = static_cast<double>(deltatsquareover2) / 2.0;
-          for (size_t g = 0; g < ng; ++g)
-            displ_old[g] = static_cast<real>(static_cast<double>(displ[g]) + h * static_cast<double>(accel[g]));
-          if (acoustic)
-            for (int g = 0; g < nglob; ++g)
-              pot_old[g] = static_cast<real>(static_cast<double>(pot[g]) + h * static_cast<double>(pot_dd[g]));
+          points_for(nt, [&](int b, int e) {
+            for (size_t g = 2 * static_cast<size_t>(b); g < 2 * static_cast<size_t>(e); ++g)
+              displ_old[g] = static_cast<real>(static_cast<double>(displ[g]) + h * static_cast<double>(accel[g]));
+            if (acoustic)
+              for (int g = b; g < e; ++g)
+                pot_old[g] = static_cast<real>(static_cast<double>(pot[g]) + h * static_cast<double>(pot_dd[g]));
+          });
         }
         // predictor (update_displacement_Newmark.F90:408-454)
-        for (size_t g = 0; g < ng; ++g) {
-          displ[g] = displ[g] + deltat * veloc[g] + deltatsquareover2 * accel[g];
-          veloc[g] = veloc[g] + deltatover2 * accel[g];
-          accel[g] = 0;
-        }
+        points_for(nt, [&](int b, int e) {
+          for (size_t g = 2 * static_cast<size_t>(b); g < 2 * static_cast<size_t>(e); ++g) {
+            displ[g] = displ[g] + deltat * veloc[g] + deltatsquareover2 * accel[g];
+            veloc[g] = veloc[g] + deltatover2 * accel[g];
+            accel[g] = 0;
+          }
+        });
         if (acoustic) {
           // acoustic predictor (update_displacement_Newmark.F90:353-402), then the
           // whole acoustic step before the elastic one (iterate_time.F90:183-196)
-          for (int g = 0; g < nglob; ++g) {
-            pot[g] = pot[g] + deltat * pot_d[g] + deltatsquareover2 * pot_dd[g];
-            pot_d[g] = pot_d[g] + deltatover2 * pot_dd[g];
-            pot_dd[g] = 0;
-          }
+          points_for(nt, [&](int b, int e) {
+            for (int g = b; g < e; ++g) {
+              pot[g] = pot[g] + deltat * pot_d[g] + deltatsquareover2 * pot_dd[g];
+              pot_d[g] = pot_d[g] + deltatover2 * pot_dd[g];
+              pot_dd[g] = 0;
+            }
+          });
           enforce_free_surface();
           acoustic_forces(0, nt);
-          for (int g = 0; g < nglob; ++g) {
-            pot_dd[g] = pot_dd[g] * rmass_ac[g];
-            pot_d[g] = pot_d[g] + deltatover2 * pot_dd[g];  // update_veloc_acoustic_Newmark
-          }
+          points_for(nt, [&](int b, int e) {
+            for (int g = b; g < e; ++g) {
+              pot_dd[g] = pot_dd[g] * rmass_ac[g];
+              pot_d[g] = pot_d[g] + deltatover2 * pot_dd[g];  // update_veloc_acoustic_Newmark
+            }
+          });
           enforce_free_surface();
         }
         forces(0, nt);
         // mass matrix and corrector (compute_forces_viscoelastic_calling_routine.F90:181,
         // update_displacement_Newmark.F90:564-589)
-        for (size_t g = 0; g < ng; ++g) {
-          accel[g] = accel[g] * rmass[g];
-          veloc[g] = veloc[g] + deltatover2 * accel[g];
-        }
+        points_for(nt, [&](int b, int e) {
+          for (size_t g = 2 * static_cast<size_t>(b); g < 2 * static_cast<size_t>(e); ++g) {
+            accel[g] = accel[g] * rmass[g];
+            veloc[g] = veloc[g] + deltatover2 * accel[g];
+          }
+        });
       } else {
         for (int stage = 0; stage < 6; ++stage) {
           // iterate_time.F90:167-181 clears accel, then forces and the LDDRK update
@@ -1041,23 +1148,27 @@ struct State : StateBase {
             enforce_free_surface();
             acoustic_forces(stage, nt);
             // update_veloc_acoustic_LDDRK (update_displacement_LDDRK.F90:88-115)
-            for (int g = 0; g < nglob; ++g) {
-              pot_dd[g] = pot_dd[g] * rmass_ac[g];
-              pot_d_l[g] = al * pot_d_l[g] + deltat * pot_dd[g];
-              pot_l[g] = al * pot_l[g] + deltat * pot_d[g];
-              pot_d[g] = pot_d[g] + be * pot_d_l[g];
-              pot[g] = pot[g] + be * pot_l[g];
-            }
+            points_for(nt, [&](int b, int e) {
+              for (int g = b; g < e; ++g) {
+                pot_dd[g] = pot_dd[g] * rmass_ac[g];
+                pot_d_l[g] = al * pot_d_l[g] + deltat * pot_dd[g];
+                pot_l[g] = al * pot_l[g] + deltat * pot_d[g];
+                pot_d[g] = pot_d[g] + be * pot_d_l[g];
+                pot[g] = pot[g] + be * pot_l[g];
+              }
+            });
             enforce_free_surface();
           }
           forces(stage, nt);
-          for (size_t g = 0; g < ng; ++g) {
-            accel[g] = accel[g] * rmass[g];
-            veloc_l[g] = al * veloc_l[g] + deltat * accel[g];
-            displ_l[g] = al * displ_l[g] + deltat * veloc[g];
-            veloc[g] = veloc[g] + be * veloc_l[g];
-            displ[g] = displ[g] + be * displ_l[g];
-          }
+          points_for(nt, [&](int b, int e) {
+            for (size_t g = 2 * static_cast<size_t>(b); g < 2 * static_cast<size_t>(e); ++g) {
+              accel[g] = accel[g] * rmass[g];
+              veloc_l[g] = al * veloc_l[g] + deltat * accel[g];
+              displ_l[g] = al * displ_l[g] + deltat * veloc[g];
+              veloc[g] = veloc[g] + be * veloc_l[g];
+              displ[g] = displ[g] + be * displ_l[g];
+            }
+          });
         }
       }
       // receivers (write_seismograms.F90:150-190, compute_interpolated_dva.f90:34-97)

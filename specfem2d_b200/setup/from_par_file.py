@@ -1,10 +1,10 @@
 """Build a setup Database from a reference-style DATA/ directory.
 
 Supports the internal-mesher subset used by the hot path: interfaces file,
-isotropic material table with regions, Stacey or free edges, force or
-moment-tensor sources, a receiver line (src/meshfem2D/save_stations_file.f90:
-receivers evenly spaced between (xdeb,zdeb) and (xfin,zfin), written with
-7 decimals), Newmark or LDDRK time scheme.
+isotropic material table with regions, Stacey, CPML or free edges, force or
+moment-tensor sources or an analytical initial field, a receiver line
+(src/meshfem2D/save_stations_file.f90: receivers evenly spaced between
+(xdeb,zdeb) and (xfin,zfin), written with 7 decimals), Newmark or LDDRK.
 """
 from __future__ import annotations
 
@@ -48,7 +48,8 @@ PAR_KEYS = ("NSTEP", "DT", "time_stepping_scheme", "NGNOD", "xmin", "xmax", "nx"
             "seismotype", "materials", "regions", "ATTENUATION_VISCOELASTIC", "PML_BOUNDARY_CONDITIONS",
             "ATTENUATION_f0_REFERENCE", "NELEM_PML_THICKNESS", "receiver_sets", "USE_TRICK_FOR_BETTER_PRESSURE",
             "TOMOGRAPHY_FILE", "MODEL", "K_MIN_PML", "K_MAX_PML", "damping_change_factor_acoustic",
-            "damping_change_factor_elastic", "ROTATE_PML_ACTIVATE", "PML_PARAMETER_ADJUSTMENT")
+            "damping_change_factor_elastic", "ROTATE_PML_ACTIVATE", "PML_PARAMETER_ADJUSTMENT",
+            "initialfield")
 
 
 def config_from_data_dir(data_dir: str, par_file: str = "Par_file", source_file: str = "SOURCE") -> dict:
@@ -88,6 +89,10 @@ def database_from_config(cfg: dict, nstep: int | None = None, absorbing_as_stace
     nz_layer = list(cfg["nz_layer"])
     absorb = (bool(par["absorbbottom"]), bool(par["absorbright"]), bool(par["absorbtop"]),
               bool(par["absorbleft"]))
+    if not (bool(par["STACEY_ABSORBING_CONDITIONS"]) or bool(par.get("PML_BOUNDARY_CONDITIONS", False))):
+        # without Stacey or CPML no edge absorbs: every edge is a free surface
+        # (read_parameter_file.F90:1678-1687, read_parameter_file_derive_flags)
+        absorb = (False, False, False, False)
     mesh = internal_mesh(float(par["xmin"]), float(par["xmax"]), int(par["nx"]), interfaces, nz_layer,
                          absorb=absorb, ngnod=int(par["NGNOD"]))
     mats = {m["index"]: m for m in (material_from_row(r) for r in par["materials"])}
@@ -172,7 +177,8 @@ def database_from_config(cfg: dict, nstep: int | None = None, absorbing_as_stace
                         time_scheme=int(time_scheme or par["time_stepping_scheme"]), user_t0=float(par["USER_T0"]),
                         anglerec_deg=float(par["anglerec"]),
                         qkappa=qk if atten else None, qmu=qm if atten else None,
-                        attenuation_f0=float(par.get("ATTENUATION_f0_REFERENCE", 1.0)))
+                        attenuation_f0=float(par.get("ATTENUATION_f0_REFERENCE", 1.0)),
+                        initialfield=bool(par.get("initialfield", False)))
     if is_aniso.any():
         db.aniso = {"ispec": is_aniso, **{k: v.astype(np.float32) for k, v in cstore.items()}}
     return db

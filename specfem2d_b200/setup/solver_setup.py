@@ -124,6 +124,9 @@ class Database:
     # CPML layers (None = none): keys region (nspec,) int (0 outside, 1 X, 2 Z, 3 XZ),
     # K_x K_z d_x d_z alpha_x alpha_z (nspec,5,5) float64, bnd_ac/bnd_el outer-edge points, dt
     pml: dict = None
+    # analytical initial wavefield (None = start from rest): pot, pot_dot, pot_dot_dot (nglob,) f32
+    # for a fluid, or displ, veloc, accel (nglob, 2) f32 for a solid
+    initial_field: dict = None
 
     @property
     def deltat(self):
@@ -426,7 +429,7 @@ def build_database(mesh: Mesh, rho, vp, vs, sources, receivers_xz, nstep: int, d
                    stacey: bool = True, external_model: bool = True, time_scheme: int = 1,
                    user_t0: float = 0.0, anglerec_deg: float = 0.0, qkappa=None, qmu=None,
                    attenuation_f0: float | None = None, use_trick: bool = False,
-                   seismotype: int = 1, pml: dict | None = None) -> Database:
+                   seismotype: int = 1, pml: dict | None = None, initialfield: bool = False) -> Database:
     """Run the host setup chain and return a Database.
 
     ``rho, vp, vs`` are per-GLL-point arrays (nspec,5,5) (external model) or
@@ -437,7 +440,10 @@ def build_database(mesh: Mesh, rho, vp, vs, sources, receivers_xz, nstep: int, d
     records pressure (receivers in acoustic elements).  ``pml`` (keys
     nelem_thickness, and optionally k_min, k_max, damping_acoustic,
     damping_elastic) puts CPML layers on the absorbing sides instead of
-    Stacey conditions; the profiles go into ``Database.pml``.
+    Stacey conditions; the profiles go into ``Database.pml``.  With
+    ``initialfield`` the sources set t0 only: none is injected, and the
+    analytical initial wavefield of the first source's type goes into
+    ``Database.initial_field`` (prepare_initial_field.F90).
     """
     from . import acoustic as ac_setup
 
@@ -490,7 +496,15 @@ def build_database(mesh: Mesh, rho, vp, vs, sources, receivers_xz, nstep: int, d
     nstage = 1 if time_scheme == 1 else 6
     src_ispec, src_arr, src_stf, sxi, sgam = [], [], [], [], []
     locator = _PointLocator(ibool, coord)
-    for s in sources:
+    init = None
+    if initialfield:
+        # setup_sources_receivers.F90:958-961: no source arrays with an initial field
+        from .initial_field import initial_mode_field
+
+        if not sources or sources[0].source_type != 6:
+            raise NotImplementedError("initial fields: only the membrane mode (source_type 6) is restated")
+        init = initial_mode_field(coord, mat["rho_vpstore"], mat["rhostore"], t0, acoustic=bool(is_ac.any()))
+    for s in ([] if initialfield else sources):
         e, xi, gamma, _, _ = _locate(mesh, ibool, coord, gll, s.x, s.z, iterate=True, locator=locator)
         hx, hpx = lagrange_any(xi, gll.xigll)
         hg, hpg = lagrange_any(gamma, gll.zigll)
@@ -562,12 +576,12 @@ def build_database(mesh: Mesh, rho, vp, vs, sources, receivers_xz, nstep: int, d
         stacey_iglob=spts[0], stacey_nx=spts[1], stacey_nz=spts[2], stacey_weight=spts[3],
         stacey_rho_vp=spts[4], stacey_rho_vs=spts[5],
         source_ispec=np.array(src_ispec, dtype=np.int32),
-        sourcearrays=np.array(src_arr, dtype=f32).reshape(len(sources), NGLL, NGLL, 2),
-        stf=np.array(src_stf, dtype=f32).reshape(len(sources), nstep, nstage),
+        sourcearrays=np.array(src_arr, dtype=f32).reshape(len(src_ispec), NGLL, NGLL, 2),
+        stf=np.array(src_stf, dtype=f32).reshape(len(src_ispec), nstep, nstage),
         rec_ispec=np.array(rec_ispec, dtype=np.int32), rec_xi=np.array(rxi), rec_gamma=np.array(rgam),
         hxir=np.array(hxr).reshape(-1, NGLL), hgammar=np.array(hgr).reshape(-1, NGLL),
         rec_x=np.array(rxx), rec_z=np.array(rzz),
         cosrot=math.cos(ang), sinrot=math.sin(ang),
         nstep=nstep, dt=dt, t0=t0, time_scheme=time_scheme, gll=gll, mesh=mesh,
         src_xi=np.array(sxi), src_gamma=np.array(sgam), atten=atten, acoustic=acoustic,
-        seismotype=int(seismotype), pml=pml_db)
+        seismotype=int(seismotype), pml=pml_db, initial_field=init)

@@ -67,6 +67,11 @@ EXAMPLES["topography_fluid_layer"] = (
     "EXAMPLES/simple_topography_and_also_a_simple_fluid_layer",
     [(f"S{k:04d}", c) for k in range(1, 12) for c in ("BXX", "BXZ")], "Par_file", "SOURCE")
 
+EXAMPLES["initial_mode_lddrk"] = (
+    # fluid-only 2 km x 2 km square (50 x 50 elements, no absorbing terms), LDDRK, initial
+    # potential = the (2, 3) membrane mode of prepare_initial_field.F90, one receiver
+    "EXAMPLES/initial_mode_LDDRK", [("S0001", "BXX"), ("S0001", "BXZ")], "Par_file", "SOURCE")
+
 # examples whose TOMOGRAPHY_FILE is written by a script of the reference
 TOMO_SCRIPTS = {"tomographic_ocean_model": "utils/createTomographyFile.py"}
 
@@ -144,5 +149,6 @@ def main(ref_root, names=None):
 
 
 if __name__ == "__main__":
-    # python tests/golden/make_golden.py <reference root> [example name ...]
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference", sys.argv[2:] or None)
+    if len(sys.argv) < 2:
+        sys.exit("usage: python tests/golden/make_golden.py <reference root> [example name ...]")
+    main(sys.argv[1], sys.argv[2:] or None)

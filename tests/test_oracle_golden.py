@@ -10,7 +10,7 @@ import os
 import numpy as np
 import pytest
 
-from helpers import load_golden, rel_l2
+from helpers import initial_mode_run, load_golden, rel_l2, within_fp32_band
 from specfem2d_b200.setup.from_par_file import database_from_config
 
 
@@ -269,3 +269,47 @@ def test_cpml_coupled_absorbs_like_stacey_before_reflections():
     b = oracle.Oracle(pm, 4).run(pm.nstep)
     w = slice(0, 500)  # direct and sea-floor waves only
     assert rel_l2(b[:, w], a[:, w]) < 5e-3
+
+
+@pytest.fixture(scope="module")
+def lddrk_mode():
+    cfg, seis = load_golden("initial_mode_lddrk")
+    db = database_from_config(cfg)
+    ref = np.stack([seis["S0001_BXX"], seis["S0001_BXZ"]], axis=1)
+    return cfg, db, ref, initial_mode_run(db, 4), initial_mode_run(db, 8)
+
+
+def test_lddrk_initial_mode_example_matches_ref_seis(lddrk_mode):
+    """EXAMPLES/initial_mode_LDDRK pins the 6-stage LDDRK scheme: a 2 km square of
+    fluid (50 x 50 elements; neither Stacey nor CPML, so every edge is a free
+    surface), the (2, 3) membrane mode of prepare_initial_field.F90 as initial
+    potential, 5500 steps, one displacement receiver (grad chi / rho).
+
+    REF_SEIS is an FP32 run.  Over 5500 steps its FP32 rounding moves it away
+    from the FP64 solution by as much as the FP32 oracle moves from the FP64
+    oracle (1.2e-3 on the small x component, 1.9e-4 on z), so the pin is that
+    the reference's traces lie within that FP32 band around the FP64 oracle,
+    on early and late windows; the FP32 oracle is within 2.5x that band of them."""
+    cfg, db, ref, o32, o64 = lddrk_mode
+    assert db.nspec == 2500 and db.nglob == 201 * 201 and db.time_scheme == 2
+    assert db.acoustic["free_iglob"].size == 800 and db.source_ispec.size == 0
+    assert db.rec_ispec[0] + 1 == cfg["log_locations"][0][0]
+    assert db.initial_field["omega"] == pytest.approx(16.990760098708467, rel=1e-15)
+    # the first recorded sample (after one step) agrees to FP32 rounding of the field
+    assert rel_l2(o64[0], ref[0]) < 2e-5
+    assert within_fp32_band(ref, o64, o32, o64)
+    for c in (0, 1):
+        assert rel_l2(o32[:, c], ref[:, c]) < 2.5 * rel_l2(o32[:, c], o64[:, c])
+
+
+def test_lddrk_pin_detects_a_coefficient_slip(lddrk_mode, monkeypatch):
+    """A planted mistake in the oracle (BETA_LDDRK[1] off by 1e-4 relative) moves the
+    FP64 traces out of the band the reference's traces sit in."""
+    import specfem2d_b200.setup.solver_setup as ss
+
+    cfg, db, ref, o32, o64 = lddrk_mode
+    beta = ss.BETA_LDDRK.copy()
+    beta[1] = np.float32(beta[1] * (1.0 + 1e-4))
+    monkeypatch.setattr(ss, "BETA_LDDRK", beta)
+    bad = initial_mode_run(db, 8)
+    assert not within_fp32_band(ref, bad, o32, o64)

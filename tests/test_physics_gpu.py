@@ -78,3 +78,25 @@ def test_lddrk_and_newmark_agree_to_time_discretisation_error():
     a = ElasticSolver(nm).run(nm.nstep)
     b = ElasticSolver(lk).run(lk.nstep)
     assert rel_l2(b, a) < 2e-2
+
+
+def test_lddrk_initial_mode_gpu_matches_oracle_and_ref_seis():
+    """EXAMPLES/initial_mode_LDDRK on the fluid tile kernels (LDDRK variant, free
+    surfaces on all four edges, no source): started from the analytical membrane
+    mode, the GPU traces over 5500 steps lie within the FP32 band around the FP64
+    oracle (as the reference's own FP32 traces do) and within 2.5x that band of
+    the reference's traces.  See test_oracle_golden for the band."""
+    from helpers import initial_mode_run, within_fp32_band
+    from specfem2d_b200.coupled import CoupledSolver
+
+    cfg, seis = load_golden("initial_mode_lddrk")
+    db = database_from_config(cfg)
+    ref = np.stack([seis["S0001_BXX"], seis["S0001_BXZ"]], axis=1)
+    o32, o64 = initial_mode_run(db, 4), initial_mode_run(db, 8)
+    s = CoupledSolver(db)
+    f = db.initial_field
+    s.set_fields(pot=f["pot"], pot_dot=f["pot_dot"], pot_dot_dot=f["pot_dot_dot"])
+    gpu = s.run(db.nstep)[0]
+    assert within_fp32_band(gpu, o64, o32, o64)
+    for c in (0, 1):
+        assert rel_l2(gpu[:, c], ref[:, c]) < 2.5 * rel_l2(o32[:, c], o64[:, c])
