@@ -217,6 +217,11 @@ int sf2d_fwi_forward(sf2d_fwi *f, double *seismograms);
  * rho_kl = -rho dt sum(a_adj . u), kappa_kl = -kappa dt sum(div div),
  * mu_kl = -2 mu dt sum(eps:eps - 1/3 div div). */
 int sf2d_fwi_backward(sf2d_fwi *f, const float *adj_src, float *rho_kl, float *kappa_kl, float *mu_kl);
+/* Receiver traces of the adjoint wavefield of the last sf2d_fwi_backward, in
+ * the adjoint run's own time order (nrec*nstep*2 doubles, [irec][it][comp]):
+ * the seismograms a kernel run writes (write_seismograms.F90:36-150 records
+ * the adjoint field when SIMULATION_TYPE = 3). */
+int sf2d_fwi_adjoint_seismograms(sf2d_fwi *f, double *seismograms);
 int sf2d_fwi_destroy(sf2d_fwi *f);
 
 /* Host-only diagnostic, no GPU needed: builds the tiling of a mesh and checks

@@ -277,18 +277,15 @@ def checkpoint_fields(o):
     return {k: o.get(k) for k in names}
 
 
-def gradient(db, observed, checkpoint_every=200, precision=4, nthreads=0):
-    """Misfit, synthetics and sensitivity kernels of the L2 waveform misfit
-    chi = 1/2 sum_r sum_it |s - d|^2 dt, with the adjoint source s - d.
-
-    Forward run with a state checkpoint every `checkpoint_every` steps, then,
-    segment by segment in reverse, the forward segment is recomputed from its
-    checkpoint (frames of the displacement kept) and the adjoint field is
-    advanced over it; adjoint step it is paired with forward step
+def adjoint_kernels(db, adj_src, checkpoint_every=200, precision=4, nthreads=0):
+    """Forward run from rest with a state checkpoint every `checkpoint_every`
+    steps, then, segment by segment in reverse, the forward segment is
+    recomputed from its checkpoint (frames of the displacement kept) and the
+    adjoint field, driven by `adj_src` (nrec, nstep, 2) in time order, or by
+    `adj_src(synthetics)` when it is a function, is advanced over it; adjoint step it is paired with forward step
     NSTEP - it + 1 (src/specfem2D/iterate_time_undoatt.F90:193-601).  Returns
-    (chi, synthetics, rho_kl, kappa_kl, mu_kl) with the kernels scaled as
-    save_adjoint_kernels.f90:134-141 does.
-    """
+    (synthetics, adjoint traces, rho_kl, kappa_kl, mu_kl) with the kernels
+    scaled as save_adjoint_kernels.f90:134-141 does."""
     nstep = db.nstep
     fwd = Oracle(db, precision)
     ckpts = {}
@@ -297,10 +294,11 @@ def gradient(db, observed, checkpoint_every=200, precision=4, nthreads=0):
         ckpts[s0] = checkpoint_fields(fwd)
         n = min(checkpoint_every, nstep - s0)
         seis[:, s0:s0 + n] = fwd.run(n, nthreads)
-    resid = seis - observed
-    dt = float(db.dt)
-    chi = 0.5 * float(np.sum(resid ** 2)) * dt
-    adj = Oracle(db, precision, adj_src=resid)
+    if callable(adj_src):
+        adj_src = adj_src(seis)
+    adj = Oracle(db, precision, adj_src=adj_src)
+    adj_seis = np.zeros_like(seis)
+    done = 0
     for s0 in sorted(ckpts, reverse=True):
         n = min(checkpoint_every, nstep - s0)
         rec = Oracle(db, precision)
@@ -313,14 +311,31 @@ def gradient(db, observed, checkpoint_every=200, precision=4, nthreads=0):
             rec.run(1, nthreads)
             frames.append(rec.displ)
         for k in range(n - 1, -1, -1):
-            adj.run(1, nthreads)
+            adj_seis[:, done:done + 1] = adj.run(1, nthreads)
+            done += 1
             adj.accumulate_kernels(frames[k])
     f = np.float32 if precision == 4 else np.float64
-    dtf = f(db.deltat) if precision == 4 else dt
+    dtf = f(db.deltat) if precision == 4 else float(db.dt)
     rho_kl = (-db.rhostore.astype(f) * dtf) * adj.get(RHO_KL)
     mu_kl = (-f(2.0) * db.mustore.astype(f) * dtf) * adj.get(MU_KL)
     kappa_kl = (-db.kappastore.astype(f) * dtf) * adj.get(KAPPA_KL)
-    return chi, seis, rho_kl, kappa_kl, mu_kl
+    return seis, adj_seis, rho_kl, kappa_kl, mu_kl
+
+
+def gradient(db, observed, checkpoint_every=200, precision=4, nthreads=0):
+    """Misfit, synthetics and sensitivity kernels of the L2 waveform misfit
+    chi = 1/2 sum_r sum_it |s - d|^2 dt, with the adjoint source s - d
+    (the run of adjoint_kernels).  Returns (chi, synthetics, rho_kl,
+    kappa_kl, mu_kl)."""
+    misfit = {}
+
+    def residual(syn):
+        resid = syn - observed
+        misfit["chi"] = 0.5 * float(np.sum(resid ** 2)) * float(db.dt)
+        return resid
+
+    seis, _, rho_kl, kappa_kl, mu_kl = adjoint_kernels(db, residual, checkpoint_every, precision, nthreads)
+    return misfit["chi"], seis, rho_kl, kappa_kl, mu_kl
 
 
 def _set_step(o, it):

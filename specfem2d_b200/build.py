@@ -16,11 +16,13 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIBDIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(LIBDIR, "libsf2d_b200.so")
-SOURCES = ["sf2d_elastic.cu", "sf2d_fwi.cu", "sf2d_noalloc.cu", "sf2d_coupled.cu", "sf2d_tiler.cpp"]
+SOURCES = ["sf2d_elastic.cu", "sf2d_fwi.cu", "sf2d_noalloc.cu", "sf2d_coupled.cu", "sf2d_tiler.cpp",
+           "sf2d_fortran.cpp"]
 HEADERS = ["sf2d_tiler.h", "sf2d_kernels.cuh", "sf2d_runtime.h", "sf2d_acoustic.cuh", "sf2d_pml.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+OBJDIR = os.path.join(PKG, "_build")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
-         "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall", "-shared", "-cudart", "static",
+         "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
          "-I", os.path.join(ROOT, "include"), "-I", CSRC]
 
 
@@ -29,18 +31,36 @@ def needs_build() -> bool:
         return True
     t = os.path.getmtime(LIB)
     deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [
-        os.path.join(ROOT, "include", h) for h in ("sf2d_b200.h", "sf2d_coupled.h")]
+        os.path.join(ROOT, "include", h) for h in ("sf2d_b200.h", "sf2d_coupled.h", "sf2d_fortran.h")]
     return any(os.path.getmtime(p) > t for p in deps)
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compiles every source to an object in parallel, then links the shared
+    library against the static CUDA runtime."""
+    from concurrent.futures import ThreadPoolExecutor
+
     if not force and not needs_build():
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
-    cmd = [NVCC, *FLAGS, *[os.path.join(CSRC, s) for s in SOURCES], "-o", LIB + ".tmp"]
+    os.makedirs(OBJDIR, exist_ok=True)
+    objs = [os.path.join(OBJDIR, os.path.splitext(s)[0] + ".o") for s in SOURCES]
+    cmds = [[NVCC, *FLAGS, "-c", os.path.join(CSRC, s), "-o", o] for s, o in zip(SOURCES, objs)]
+
+    def compile_one(cmd):
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        return subprocess.run(cmd).returncode
+
+    with ThreadPoolExecutor(max_workers=len(cmds)) as ex:
+        codes = list(ex.map(compile_one, cmds))
+    if any(codes):
+        raise subprocess.CalledProcessError(max(codes), "nvcc")
+    link = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-cudart", "static", *objs,
+            "-o", LIB + ".tmp"]
     if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+        print(" ".join(link), flush=True)
+    subprocess.run(link, check=True)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

@@ -1,0 +1,704 @@
+// The reference's Fortran-to-GPU entry points (include/sf2d_fortran.h) over
+// this library's fused solver.  The SPECFEM2D Fortran host (prepare_gpu.f90,
+// compute_gpu_elastic.f90, update_displacement_Newmark.F90,
+// write_seismograms.F90, check_stability.F90) calls them with its own arrays;
+// they gather what sf2d_elastic_create needs, build the solver when the time
+// step is first known (update_displacement_cuda) and advance one fused step
+// per kernel_3_a_cuda.  Errors print and exit, as the reference's
+// exit_on_error (src/gpu/helper_functions.cu) does.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "sf2d_b200.h"
+#include "sf2d_fortran.h"
+
+namespace {
+
+constexpr int NGLL = 5, NGLL2 = 25;
+
+[[noreturn]] void stop(const char *routine, const std::string &msg) {
+  std::fprintf(stderr, "Error in %s: %s\n", routine, msg.c_str());
+  std::fflush(stderr);
+  std::exit(EXIT_FAILURE);
+}
+
+void check(const char *routine, int rc) {
+  if (rc != SF2D_OK) stop(routine, sf2d_last_error());
+}
+
+enum Why { FLUID, KERNEL_RUN, MPI, DEBUG, OTHER };
+
+[[noreturn]] void unsupported(const char *routine, Why why) {
+  static const char *const text[] = {
+      "fluid domains and CPML run through sf2d_coupled_create / sf2d_coupled_run (include/sf2d_coupled.h)",
+      "kernel runs use sf2d_fwi_create / sf2d_fwi_forward / sf2d_fwi_backward (include/sf2d_b200.h), which "
+      "replay the forward field from checkpoints instead of reconstructing it backwards",
+      "this library runs one mesh per process: there is no MPI halo exchange",
+      "debug helper not provided by libsf2d_b200",
+      "not provided by libsf2d_b200"};
+  stop(routine, text[why]);
+}
+
+// Everything one Mesh_pointer holds: the host copies the descriptor points
+// into, the solver once built, and the step bookkeeping.
+struct FortranMesh {
+  sf2d_elastic_desc d{};
+  int nspec = 0, nglob = 0, nstep = 0, nlength = 0, nrec = 0, nsrc = 0;
+  bool stacey = false, save_forward = false, have_rmass = false, have_stacey = false;
+  std::vector<int> ibool, src_ispec, rec_ispec, st_iglob, aniso_flag;
+  std::vector<float> xix, xiz, gammax, gammaz, lambda, mu, hprime, hprimewgll, wxgll, srcarr, stf, rmass;
+  std::vector<float> st_nx, st_nz, st_w, st_rvp, st_rvs;
+  std::vector<float> c11, c13, c15, c33, c35, c55, a1, b1, a2, b2;
+  std::vector<double> hxir, hgammar, centroid;
+  sf2d_solver *S = nullptr;
+  float dt = 0.f, dtover2 = 0.f, dtsq2 = 0.f;
+  int steps = 0;  // steps advanced (the Fortran `it` of the last finished step)
+  int stage = 0;  // 0 between steps, 1 after update_displacement_cuda, 2 after the outer forces phase
+  std::vector<float> staged_u, staged_v, staged_a;  // fields given before the solver exists
+  std::vector<int> sample_step;                     // step of each sample in the host's trace buffer
+};
+
+FortranMesh *mesh_of(const char *routine, const long *p) {
+  if (!p || *p == 0) stop(routine, "Mesh_pointer was not prepared by prepare_constants_device");
+  return reinterpret_cast<FortranMesh *>(*p);
+}
+
+// Column-major (n1, n2) -> row-major [i1][i2]: the transpose of the memory order.
+template <typename T, typename U>
+std::vector<T> transpose(const U *a, int n1, int n2) {
+  std::vector<T> out(static_cast<size_t>(n1) * n2);
+  for (int i2 = 0; i2 < n2; ++i2)
+    for (int i1 = 0; i1 < n1; ++i1) out[static_cast<size_t>(i1) * n2 + i2] = static_cast<T>(a[static_cast<size_t>(i2) * n1 + i1]);
+  return out;
+}
+
+// Element centres for the tiler's Morton order.  The reference hands the GPU
+// no coordinates, so they are rebuilt from the mapping derivatives: x_xi =
+// gammaz J, z_xi = -gammax J, x_gamma = -xiz J, z_gamma = xix J with J =
+// 1/(xix gammaz - xiz gammax), integrated along GLL lines through the
+// Lagrange interpolant of the derivative (exact for the 4- and 9-node
+// mappings), and elements placed next to their already placed neighbours
+// through shared points.  Only tile shapes depend on them.
+void rebuild_centroids(FortranMesh &m) {
+  const double s37 = std::sqrt(3.0 / 7.0);
+  const double xi[NGLL] = {-1.0, -s37, 0.0, s37, 1.0};
+  // W[i][k] = integral from -1 to xi_i of the k-th Lagrange polynomial
+  double W[NGLL][NGLL];
+  for (int k = 0; k < NGLL; ++k) {
+    // coefficients of l_k by expanding the product, lowest degree first
+    double c[NGLL] = {1.0, 0, 0, 0, 0};
+    double den = 1.0;
+    int deg = 0;
+    for (int q = 0; q < NGLL; ++q) {
+      if (q == k) continue;
+      for (int p = deg + 1; p > 0; --p) c[p] = c[p - 1] - xi[q] * c[p];
+      c[0] = -xi[q] * c[0];
+      ++deg;
+      den *= xi[k] - xi[q];
+    }
+    for (int i = 0; i < NGLL; ++i) {
+      double a = 0.0, b = 0.0;
+      for (int p = 0; p < NGLL; ++p) {
+        a += c[p] / (p + 1) * std::pow(xi[i], p + 1);
+        b += c[p] / (p + 1) * std::pow(-1.0, p + 1);
+      }
+      W[i][k] = (a - b) / den;
+    }
+  }
+  const int ne = m.nspec;
+  std::vector<double> lx(static_cast<size_t>(ne) * NGLL2), lz(lx.size());
+  for (int e = 0; e < ne; ++e) {
+    double xx[NGLL2], zx[NGLL2], xg[NGLL2], zg[NGLL2];
+    for (int q = 0; q < NGLL2; ++q) {
+      const size_t p = static_cast<size_t>(e) * NGLL2 + q;
+      const double det = static_cast<double>(m.xix[p]) * m.gammaz[p] - static_cast<double>(m.xiz[p]) * m.gammax[p];
+      const double J = det != 0.0 ? 1.0 / det : 0.0;
+      xx[q] = m.gammaz[p] * J;
+      zx[q] = -m.gammax[p] * J;
+      xg[q] = -m.xiz[p] * J;
+      zg[q] = m.xix[p] * J;
+    }
+    // along gamma on the first column, then along xi on every row
+    double cx[NGLL], cz[NGLL];
+    for (int j = 0; j < NGLL; ++j) {
+      cx[j] = cz[j] = 0.0;
+      for (int k = 0; k < NGLL; ++k) {
+        cx[j] += W[j][k] * xg[k * NGLL];
+        cz[j] += W[j][k] * zg[k * NGLL];
+      }
+    }
+    for (int j = 0; j < NGLL; ++j)
+      for (int i = 0; i < NGLL; ++i) {
+        double x = cx[j], z = cz[j];
+        for (int k = 0; k < NGLL; ++k) {
+          x += W[i][k] * xx[j * NGLL + k];
+          z += W[i][k] * zx[j * NGLL + k];
+        }
+        lx[static_cast<size_t>(e) * NGLL2 + j * NGLL + i] = x;
+        lz[static_cast<size_t>(e) * NGLL2 + j * NGLL + i] = z;
+      }
+  }
+  // place elements breadth first through shared points
+  std::vector<std::vector<int>> elems_of(m.nglob);
+  for (int e = 0; e < ne; ++e)
+    for (int q = 0; q < NGLL2; ++q) elems_of[m.ibool[static_cast<size_t>(e) * NGLL2 + q]].push_back(e);
+  std::vector<double> gx(m.nglob, 0.0), gz(m.nglob, 0.0);
+  std::vector<char> known(m.nglob, 0), placed(ne, 0);
+  std::vector<int> queue;
+  double shift = 0.0;
+  for (int seed = 0; seed < ne; ++seed) {
+    if (placed[seed]) continue;
+    // a new connected part: put it to the right of the previous ones
+    queue.assign(1, seed);
+    placed[seed] = 1;
+    for (size_t h = 0; h < queue.size(); ++h) {
+      const int e = queue[h];
+      const size_t o = static_cast<size_t>(e) * NGLL2;
+      double ox = shift, oz = 0.0;
+      for (int q = 0; q < NGLL2; ++q) {
+        const int g = m.ibool[o + q];
+        if (known[g]) {
+          ox = gx[g] - lx[o + q];
+          oz = gz[g] - lz[o + q];
+          break;
+        }
+      }
+      double cxs = 0.0, czs = 0.0;
+      for (int q = 0; q < NGLL2; ++q) {
+        const int g = m.ibool[o + q];
+        if (!known[g]) {
+          gx[g] = lx[o + q] + ox;
+          gz[g] = lz[o + q] + oz;
+          known[g] = 1;
+        }
+        cxs += lx[o + q] + ox;
+        czs += lz[o + q] + oz;
+        for (int nb : elems_of[g])
+          if (!placed[nb]) {
+            placed[nb] = 1;
+            queue.push_back(nb);
+          }
+      }
+      m.centroid[2 * e] = cxs / NGLL2;
+      m.centroid[2 * e + 1] = czs / NGLL2;
+    }
+    double xmax = shift;
+    for (int e : queue) xmax = std::max(xmax, m.centroid[2 * e]);
+    shift = xmax + 1.0e6;
+  }
+}
+
+void build_solver(const char *routine, FortranMesh &m) {
+  if (m.S) return;
+  if (!m.have_rmass) stop(routine, "prepare_fields_elastic_device has not been called");
+  if (m.stacey && !m.have_stacey) stop(routine, "prepare_stacey_device has not been called");
+  sf2d_elastic_desc &d = m.d;
+  d.nspec = m.nspec;
+  d.nglob = m.nglob;
+  d.ibool = m.ibool.data();
+  d.xix = m.xix.data();
+  d.xiz = m.xiz.data();
+  d.gammax = m.gammax.data();
+  d.gammaz = m.gammaz.data();
+  d.lambdastore = m.lambda.data();
+  d.mustore = m.mu.data();
+  d.rmass_inverse = m.rmass.data();
+  d.hprime = m.hprime.data();
+  d.hprimewgll = m.hprimewgll.data();
+  d.wxgll = d.wzgll = m.wxgll.data();
+  d.centroid_xz = m.centroid.data();
+  d.nstacey = static_cast<int>(m.st_iglob.size());
+  d.st_iglob = m.st_iglob.data();
+  d.st_nx = m.st_nx.data();
+  d.st_nz = m.st_nz.data();
+  d.st_w = m.st_w.data();
+  d.st_rho_vp = m.st_rvp.data();
+  d.st_rho_vs = m.st_rvs.data();
+  d.nsrc = m.nsrc;
+  d.src_ispec = m.src_ispec.data();
+  d.sourcearrays = m.srcarr.data();
+  d.stf = m.stf.data();
+  d.nrec = m.nrec;
+  d.rec_ispec = m.rec_ispec.data();
+  d.hxir = m.hxir.data();
+  d.hgammar = m.hgammar.data();
+  d.nstep = m.nstep;
+  d.deltat = m.dt;
+  d.deltatover2 = m.dtover2;
+  d.deltatsquareover2 = m.dtsq2;
+  d.tile_elems = 32;
+  d.threads_per_block = 256;
+  d.time_scheme = 1;
+  d.nstage = 1;
+  if (!m.aniso_flag.empty()) {
+    d.ispec_is_anisotropic = m.aniso_flag.data();
+    d.c11 = m.c11.data();
+    d.c13 = m.c13.data();
+    d.c15 = m.c15.data();
+    d.c33 = m.c33.data();
+    d.c35 = m.c35.data();
+    d.c55 = m.c55.data();
+  }
+  if (!m.a1.empty()) {
+    d.att_a1 = m.a1.data();
+    d.att_b1 = m.b1.data();
+    d.att_a2 = m.a2.data();
+    d.att_b2 = m.b2.data();
+  }
+  check(routine, sf2d_elastic_create(&d, &m.S));
+  if (!m.staged_u.empty()) {
+    check(routine, sf2d_set_fields(m.S, m.staged_u.data(), m.staged_v.data(), m.staged_a.data()));
+    m.staged_u.clear();
+    m.staged_v.clear();
+    m.staged_a.clear();
+  }
+}
+
+void need_size(const char *routine, const FortranMesh &m, const int *size) {
+  if (!size || *size != 2 * m.nglob) stop(routine, "size must be NDIM*NGLOB_AB = " + std::to_string(2 * m.nglob));
+}
+
+void fields_from(const char *R, FortranMesh *m, const int *size, realw *displ, realw *veloc, realw *accel) {
+  need_size(R, *m, size);
+  if (m->S) {
+    check(R, sf2d_get_fields(m->S, displ, veloc, accel));
+    return;
+  }
+  const size_t n = static_cast<size_t>(*size);
+  const bool staged = !m->staged_u.empty();
+  for (auto pr : {std::make_pair(displ, &m->staged_u), std::make_pair(veloc, &m->staged_v),
+                  std::make_pair(accel, &m->staged_a)})
+    if (pr.first) {
+      if (staged)
+        std::memcpy(pr.first, pr.second->data(), n * sizeof(realw));
+      else
+        std::memset(pr.first, 0, n * sizeof(realw));
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+// ---- device and memory ----
+
+// initialize_cuda_device (src/gpu/initialize_cuda.cu:50): device myrank % count
+void initialize_cuda_device_(int *myrank_f, int *ncuda_devices) {
+  int n = 0;
+  check("initialize_cuda_device", sf2d_initialize_device(myrank_f ? *myrank_f : 0, &n));
+  if (ncuda_devices) *ncuda_devices = n;
+}
+
+void initialize_cuda_aware_mpi_() {}
+
+void pause_for_debug_() {}
+
+// output_free_device_memory / get_free_device_memory (src/gpu/check_fields_cuda.cu)
+void get_free_device_memory_(realw *free_mb, realw *used_mb, realw *total_mb) {
+  size_t fr = 0, tot = 0;
+  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) stop("get_free_device_memory", "cudaMemGetInfo failed");
+  if (free_mb) *free_mb = static_cast<realw>(fr / 1048576.0);
+  if (used_mb) *used_mb = static_cast<realw>((tot - fr) / 1048576.0);
+  if (total_mb) *total_mb = static_cast<realw>(tot / 1048576.0);
+}
+
+void output_free_device_memory_(int *myrank_f) {
+  realw fr = 0, used = 0, tot = 0;
+  get_free_device_memory_(&fr, &used, &tot);
+  std::printf("rank %d: GPU memory usage: used = %f MB, free = %f MB, total = %f MB\n", myrank_f ? *myrank_f : 0,
+              used, fr, tot);
+  std::fflush(stdout);
+}
+
+// ---- set-up and clean-up ----
+
+// prepare_constants_device (src/gpu/prepare_mesh_constants_cuda.cu:83)
+void prepare_constants_device_(long *Mesh_pointer, int *h_NGLLX, int *NSPEC_AB, int *NGLOB_AB, realw *h_xix,
+                               realw *h_xiz, realw *h_gammax, realw *h_gammaz, realw *h_kappav, realw *h_muv,
+                               int *h_ibool, int *num_interfaces_ext_mesh, int *, int *, int *,
+                               realw *h_hprime_xx, realw *h_hprimewgll_xx, realw *h_wxgll,
+                               int *STACEY_BOUNDARY_CONDITIONS, int *PML_BOUNDARY_CONDITIONS, int *,
+                               int *nsources_local_f, realw *h_sourcearrays, realw *h_source_time_function,
+                               int *NSTEP, int *h_ispec_selected_source, int *h_ispec_selected_rec_loc,
+                               int *nrec_local, realw *h_cosrot, realw *h_sinrot, int *SIMULATION_TYPE, int *P_SV,
+                               int *nspec_acoustic, int *, int *, int *, int *, int *SAVE_FORWARD,
+                               realw *h_xir_store, realw *h_gammar_store, int *h_NSIGTYPE, int *h_seismotypeVec,
+                               int *nlength_seismogram) {
+  const char *R = "prepare_constants_device";
+  if (!Mesh_pointer) stop(R, "null Mesh_pointer");
+  if (*h_NGLLX != NGLL) stop(R, "NGLLX must be 5");
+  if (!*P_SV) stop(R, "SH (membrane) waves are not provided: P_SV only");
+  if (*SIMULATION_TYPE != 1) unsupported(R, KERNEL_RUN);
+  if (*SAVE_FORWARD)
+    stop(R, "SAVE_FORWARD: the boundary values of a backward reconstruction are not produced; kernel runs use "
+            "sf2d_fwi_* (include/sf2d_b200.h)");
+  if (*nspec_acoustic > 0 || *PML_BOUNDARY_CONDITIONS) unsupported(R, FLUID);
+  if (*num_interfaces_ext_mesh > 0) unsupported(R, MPI);
+  if (*h_NSIGTYPE != 1) stop(R, "one seismogram type per run (NSIGTYPE = 1)");
+  if (h_seismotypeVec[0] < 1 || h_seismotypeVec[0] > 3)
+    stop(R, "elastic runs record displacement, velocity or acceleration (seismotype 1-3)");
+  auto m = new FortranMesh();
+  const int ns = *NSPEC_AB, ng = *NGLOB_AB;
+  const size_t nl = static_cast<size_t>(ns) * NGLL2;
+  m->nspec = ns;
+  m->nglob = ng;
+  m->nstep = *NSTEP;
+  m->nlength = *nlength_seismogram;
+  m->stacey = *STACEY_BOUNDARY_CONDITIONS != 0;
+  m->ibool.resize(nl);
+  for (size_t p = 0; p < nl; ++p) {
+    m->ibool[p] = h_ibool[p] - 1;
+    if (m->ibool[p] < 0 || m->ibool[p] >= ng) stop(R, "ibool out of range");
+  }
+  m->xix.assign(h_xix, h_xix + nl);
+  m->xiz.assign(h_xiz, h_xiz + nl);
+  m->gammax.assign(h_gammax, h_gammax + nl);
+  m->gammaz.assign(h_gammaz, h_gammaz + nl);
+  m->mu.assign(h_muv, h_muv + nl);
+  // the reference's GPU kernel forms lambda = kappa - mu in CUSTOM_REAL
+  // (Kernel_2_viscoelastic_impl.cu:501)
+  m->lambda.resize(nl);
+  for (size_t p = 0; p < nl; ++p) m->lambda[p] = h_kappav[p] - h_muv[p];
+  // hprime_xx(i2, i1) = l'_i1(xi_i2) in Fortran order: the descriptor's [i2][i1]
+  m->hprime = transpose<float>(h_hprime_xx, NGLL, NGLL);
+  m->hprimewgll = transpose<float>(h_hprimewgll_xx, NGLL, NGLL);
+  m->wxgll.assign(h_wxgll, h_wxgll + NGLL);
+  // sources: sourcearray_loc(NDIM, NGLLX, NGLLZ, nsrc) is already [isrc][j][i][comp];
+  // source_time_function_loc(nsrc, NSTEP) is transposed to [isrc][it]
+  m->nsrc = *nsources_local_f;
+  m->src_ispec.resize(m->nsrc);
+  for (int s = 0; s < m->nsrc; ++s) m->src_ispec[s] = h_ispec_selected_source[s] - 1;
+  m->srcarr.assign(h_sourcearrays, h_sourcearrays + static_cast<size_t>(m->nsrc) * NGLL2 * 2);
+  m->stf = transpose<float>(h_source_time_function, m->nsrc, m->nstep);
+  // receivers: xir_store_loc(nrec, NGLLX) -> [irec][i]; one rotation for all receivers
+  m->nrec = *nrec_local;
+  m->rec_ispec.resize(m->nrec);
+  for (int r = 0; r < m->nrec; ++r) m->rec_ispec[r] = h_ispec_selected_rec_loc[r] - 1;
+  m->hxir = transpose<double>(h_xir_store, m->nrec, NGLL);
+  m->hgammar = transpose<double>(h_gammar_store, m->nrec, NGLL);
+  for (int r = 1; r < m->nrec; ++r)
+    if (h_cosrot[r] != h_cosrot[0] || h_sinrot[r] != h_sinrot[0])
+      stop(R, "receivers with different rotation angles are not provided");
+  m->d.cosrot = m->nrec ? static_cast<double>(h_cosrot[0]) : 1.0;
+  m->d.sinrot = m->nrec ? static_cast<double>(h_sinrot[0]) : 0.0;
+  m->d.seismotype = h_seismotypeVec[0];
+  m->centroid.assign(2 * static_cast<size_t>(ns), 0.0);
+  rebuild_centroids(*m);
+  *Mesh_pointer = reinterpret_cast<long>(m);
+}
+
+// prepare_fields_elastic_device (src/gpu/prepare_mesh_constants_cuda.cu:527)
+void prepare_fields_elastic_device_(long *Mesh_pointer, realw *rmassx, realw *rmassz, int *, int *,
+                                    int *ispec_is_anisotropic, int *ANISOTROPY, realw *c11store, realw *,
+                                    realw *c13store, realw *c15store, realw *, realw *, realw *c33store,
+                                    realw *c35store, realw *c55store, int *h_ninterface_elastic, int *,
+                                    int *ATTENUATION_VISCOELASTIC, realw *h_A_newmark_mu, realw *h_B_newmark_mu,
+                                    realw *h_A_newmark_kappa, realw *h_B_newmark_kappa) {
+  const char *R = "prepare_fields_elastic_device";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (m->S) stop(R, "called after the time loop started");
+  if (*h_ninterface_elastic > 0) unsupported(R, MPI);
+  m->rmass.resize(2 * static_cast<size_t>(m->nglob));
+  for (int g = 0; g < m->nglob; ++g) {
+    m->rmass[2 * g] = rmassx[g];
+    m->rmass[2 * g + 1] = rmassz[g];
+  }
+  m->have_rmass = true;
+  const size_t nl = static_cast<size_t>(m->nspec) * NGLL2;
+  if (*ANISOTROPY) {
+    m->aniso_flag.resize(m->nspec);
+    for (int e = 0; e < m->nspec; ++e) m->aniso_flag[e] = ispec_is_anisotropic[e] != 0;
+    m->c11.assign(c11store, c11store + nl);
+    m->c13.assign(c13store, c13store + nl);
+    m->c15.assign(c15store, c15store + nl);
+    m->c33.assign(c33store, c33store + nl);
+    m->c35.assign(c35store, c35store + nl);
+    m->c55.assign(c55store, c55store + nl);
+  }
+  if (*ATTENUATION_VISCOELASTIC) {
+    // A/B_newmark_nu1 (bulk, "kappa") and _nu2 (shear, "mu"), (N_SLS, NGLLX, NGLLZ, nspec)
+    const size_t na = nl * 3;
+    m->a1.assign(h_A_newmark_kappa, h_A_newmark_kappa + na);
+    m->b1.assign(h_B_newmark_kappa, h_B_newmark_kappa + na);
+    m->a2.assign(h_A_newmark_mu, h_A_newmark_mu + na);
+    m->b2.assign(h_B_newmark_mu, h_B_newmark_mu + na);
+  }
+}
+
+// prepare_stacey_device (src/gpu/prepare_mesh_constants_cuda.cu:926): faces to
+// one entry per absorbing GLL point, in face order; a point whose i or j is
+// NGLLX + 1 (a corner a neighbouring face already covers) is left out, as
+// compute_stacey_elastic_kernel skips it
+void prepare_stacey_device_(long *Mesh_pointer, int *, int *ELASTIC_SIMULATION, realw *rho_vp, realw *rho_vs, int *,
+                            int *, int *, int *, int *h_abs_boundary_ispec, int *h_abs_boundary_ij,
+                            realw *h_abs_boundary_normal, realw *h_abs_boundary_jacobian1Dw,
+                            int *h_num_abs_boundary_faces, int *, int *, int *, int *, int *) {
+  const char *R = "prepare_stacey_device";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (m->S) stop(R, "called after the time loop started");
+  m->st_iglob.clear();
+  m->st_nx.clear();
+  m->st_nz.clear();
+  m->st_w.clear();
+  m->st_rvp.clear();
+  m->st_rvs.clear();
+  const int nf = *h_num_abs_boundary_faces;
+  for (int f = 0; f < (*ELASTIC_SIMULATION ? nf : 0); ++f) {
+    const int e = h_abs_boundary_ispec[f] - 1;
+    if (e < 0 || e >= m->nspec) stop(R, "abs_boundary_ispec out of range");
+    for (int k = 0; k < NGLL; ++k) {
+      const int i = h_abs_boundary_ij[(f * NGLL + k) * 2] - 1;
+      const int j = h_abs_boundary_ij[(f * NGLL + k) * 2 + 1] - 1;
+      if (i == NGLL || j == NGLL) continue;
+      if (i < 0 || i >= NGLL || j < 0 || j >= NGLL) stop(R, "abs_boundary_ij out of range");
+      const size_t p = static_cast<size_t>(e) * NGLL2 + j * NGLL + i;
+      m->st_iglob.push_back(m->ibool[p]);
+      m->st_nx.push_back(h_abs_boundary_normal[(f * NGLL + k) * 2]);
+      m->st_nz.push_back(h_abs_boundary_normal[(f * NGLL + k) * 2 + 1]);
+      m->st_w.push_back(h_abs_boundary_jacobian1Dw[f * NGLL + k]);
+      m->st_rvp.push_back(rho_vp[p]);
+      m->st_rvs.push_back(rho_vs[p]);
+    }
+  }
+  m->have_stacey = true;
+}
+
+// prepare_cleanup_device (src/gpu/prepare_mesh_constants_cuda.cu:1139)
+void prepare_cleanup_device_(long *Mesh_pointer, int *, int *, int *, int *, int *, int *, int *, realw *) {
+  FortranMesh *m = mesh_of("prepare_cleanup_device", Mesh_pointer);
+  if (m->S) sf2d_destroy(m->S);
+  delete m;
+  *Mesh_pointer = 0;
+}
+
+// ---- one elastic time step ----
+
+// update_displacement_cuda (src/gpu/update_displacement_cuda.cu:52): the first
+// call of a step; the first one of the run also builds the solver, since this
+// is where the host first passes the time step
+void update_displacement_cuda_(long *Mesh_pointer, realw *deltat_F, realw *deltatsqover2_F, realw *deltatover2_F,
+                               realw *, realw *, realw *) {
+  const char *R = "update_displacement_cuda";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (m->stage != 0) stop(R, "the previous time step did not reach kernel_3_a_cuda");
+  if (!m->S) {
+    m->dt = *deltat_F;
+    m->dtsq2 = *deltatsqover2_F;
+    m->dtover2 = *deltatover2_F;
+    build_solver(R, *m);
+  } else if (*deltat_F != m->dt || *deltatsqover2_F != m->dtsq2 || *deltatover2_F != m->dtover2) {
+    stop(R, "the time step changed during the run");
+  }
+  if (m->steps >= m->nstep) stop(R, "more time steps than NSTEP");
+  m->stage = 1;
+}
+
+// compute_forces_viscoelastic_cuda (src/gpu/compute_forces_viscoelastic_cuda.cu:327):
+// outer (iphase 1) then inner (iphase 2) elements; with one process every
+// element is inner and the fused step covers both
+void compute_forces_viscoelastic_cuda_(long *Mesh_pointer, int *iphase, realw *, int *, int *, int *, int *,
+                                       int *, int *compute_wavefield_2) {
+  const char *R = "compute_forces_viscoelastic_cuda";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (*compute_wavefield_2) unsupported(R, KERNEL_RUN);
+  if (*iphase == 1 && m->stage == 1)
+    m->stage = 2;
+  else if (!(*iphase == 2 && m->stage == 2))
+    stop(R, "called out of the order update_displacement_cuda, iphase 1, iphase 2, kernel_3_a_cuda");
+}
+
+// compute_stacey_viscoelastic_cuda (src/gpu/compute_stacey_viscoelastic_cuda.cu:40):
+// the absorbing terms are part of the fused step
+void compute_stacey_viscoelastic_cuda_(long *Mesh_pointer, int *, realw *, realw *, realw *, realw *, int *,
+                                       int *compute_wavefield_2, int *) {
+  const char *R = "compute_stacey_viscoelastic_cuda";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (*compute_wavefield_2) unsupported(R, KERNEL_RUN);
+  if (m->stage != 2) stop(R, "called outside a time step");
+}
+
+// compute_add_sources_el_cuda (src/gpu/compute_add_sources_viscoelastic_cuda.cu:46):
+// the fused step adds source_time_function(:, it) of the step it advances
+void compute_add_sources_el_cuda_(long *Mesh_pointer, int *, int *itf) {
+  const char *R = "compute_add_sources_el_cuda";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (m->stage != 2) stop(R, "called outside a time step");
+  if (*itf != m->steps + 1) stop(R, "time step " + std::to_string(*itf) + " out of sequence");
+}
+
+// kernel_3_a_cuda (src/gpu/update_displacement_cuda.cu:221): the last call of
+// the step; the whole fused step is queued here
+void kernel_3_a_cuda_(long *Mesh_pointer, realw *, realw *, int *, int *compute_wavefield_2) {
+  const char *R = "kernel_3_a_cuda";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (*compute_wavefield_2) unsupported(R, KERNEL_RUN);
+  if (m->stage != 2) stop(R, "called before compute_forces_viscoelastic_cuda");
+  check(R, sf2d_enqueue(m->S, 1));
+  ++m->steps;
+  m->stage = 0;
+}
+
+// compute_seismograms_cuda (src/gpu/write_seismograms_cuda.cu:41): sample
+// seismo_current of the host's buffer is the state after step `it`; the
+// buffer sisux/sisuz(nlength_seismogram, nrec_local) is filled when it is
+// full or at the last step
+void compute_seismograms_cuda_(long *Mesh_pointer_f, int *i_sigf, double *sisux, double *sisuz,
+                               int *seismo_currentf, int *nlength_seismogramf, int *, int *, int *, int *, int *itf,
+                               int *it_endf) {
+  const char *R = "compute_seismograms_cuda";
+  FortranMesh *m = mesh_of(R, Mesh_pointer_f);
+  if (*i_sigf != 1) stop(R, "one seismogram type per run");
+  if (m->nrec == 0) return;
+  const int j = *seismo_currentf - 1, nlen = *nlength_seismogramf;
+  if (j < 0 || j >= nlen) stop(R, "seismo_current out of range");
+  if (*itf != m->steps) stop(R, "called for a step that has not been advanced");
+  if (static_cast<int>(m->sample_step.size()) != j) m->sample_step.resize(j);
+  m->sample_step.push_back(*itf - 1);
+  if (j != nlen - 1 && *itf != *it_endf) return;
+  const int s0 = m->sample_step.front(), s1 = m->sample_step.back();
+  const int n = s1 - s0 + 1;
+  std::vector<double> tr(static_cast<size_t>(m->nrec) * n * 2);
+  check(R, sf2d_copy_seismograms(m->S, s0, n, tr.data()));
+  for (int r = 0; r < m->nrec; ++r)
+    for (size_t k = 0; k < m->sample_step.size(); ++k) {
+      const size_t src = (static_cast<size_t>(r) * n + (m->sample_step[k] - s0)) * 2;
+      sisux[k + static_cast<size_t>(nlen) * r] = tr[src];
+      sisuz[k + static_cast<size_t>(nlen) * r] = tr[src + 1];
+    }
+  m->sample_step.clear();
+}
+
+// get_norm_elastic_from_device (src/gpu/check_fields_cuda.cu:358)
+void get_norm_elastic_from_device_(realw *norm, long *Mesh_pointer, const int *FORWARD_OR_ADJOINT) {
+  const char *R = "get_norm_elastic_from_device";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (FORWARD_OR_ADJOINT && *FORWARD_OR_ADJOINT == 3) unsupported(R, KERNEL_RUN);
+  if (!m->S) {
+    float mx = 0.f;
+    for (size_t g = 0; g < m->staged_u.size() / 2; ++g)
+      mx = std::max(mx, std::sqrt(m->staged_u[2 * g] * m->staged_u[2 * g] + m->staged_u[2 * g + 1] * m->staged_u[2 * g + 1]));
+    *norm = mx;
+    return;
+  }
+  check(R, sf2d_get_norm(m->S, norm));
+}
+
+// ---- wavefield transfers (src/gpu/transfer_fields_cuda.cu:53-140) ----
+
+void transfer_fields_el_to_device_(int *size, realw *displ, realw *veloc, realw *accel, long *Mesh_pointer) {
+  const char *R = "transfer_fields_el_to_device";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  need_size(R, *m, size);
+  if (m->S) {
+    check(R, sf2d_set_fields(m->S, displ, veloc, accel));
+    return;
+  }
+  m->staged_u.assign(displ, displ + *size);
+  m->staged_v.assign(veloc, veloc + *size);
+  m->staged_a.assign(accel, accel + *size);
+}
+
+void transfer_fields_el_from_device_(int *size, realw *displ, realw *veloc, realw *accel, long *Mesh_pointer) {
+  fields_from("transfer_fields_el_from_device", mesh_of("transfer_fields_el_from_device", Mesh_pointer), size,
+              displ, veloc, accel);
+}
+
+void transfer_displ_from_device_(int *size, realw *displ, long *Mesh_pointer) {
+  fields_from("transfer_displ_from_device", mesh_of("transfer_displ_from_device", Mesh_pointer), size, displ,
+              nullptr, nullptr);
+}
+
+void transfer_accel_from_device_(int *size, realw *accel, long *Mesh_pointer) {
+  fields_from("transfer_accel_from_device", mesh_of("transfer_accel_from_device", Mesh_pointer), size, nullptr,
+              nullptr, accel);
+}
+
+void transfer_accel_to_device_(int *size, realw *accel, long *Mesh_pointer) {
+  const char *R = "transfer_accel_to_device";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  need_size(R, *m, size);
+  std::vector<realw> u(*size), v(*size);
+  fields_from(R, m, size, u.data(), v.data(), nullptr);
+  transfer_fields_el_to_device_(size, u.data(), v.data(), accel, Mesh_pointer);
+}
+
+// ---- not provided ----
+void transfer_boun_pot_from_device_(long*, realw*, const int*) { unsupported("transfer_boun_pot_from_device", MPI); }
+void transfer_asmbl_pot_to_device_(long*, realw*, const int*) { unsupported("transfer_asmbl_pot_to_device", MPI); }
+void transfer_boun_accel_from_device_(long*, realw*, const int*) { unsupported("transfer_boun_accel_from_device", MPI); }
+void transfer_boundary_from_device_a_(long*) { unsupported("transfer_boundary_from_device_a", MPI); }
+void prepare_boundary_on_device_(long*) { unsupported("prepare_boundary_on_device", MPI); }
+void transfer_boundary_to_device_a_(long*, realw*, const int*) { unsupported("transfer_boundary_to_device_a", MPI); }
+void transfer_asmbl_accel_to_device_(long*, realw*, const int*, const int*, const int*, const int*) { unsupported("transfer_asmbl_accel_to_device", MPI); }
+void sync_copy_from_device_(long*, int*, realw*) { unsupported("sync_copy_from_device", MPI); }
+void get_norm_acoustic_from_device_(realw*, long*, const int*) { unsupported("get_norm_acoustic_from_device", FLUID); }
+void get_max_accel_(int*, int*, long*) { unsupported("get_max_accel", DEBUG); }
+void check_max_norm_displ_gpu_(int*, realw*, long*, int*) { unsupported("check_max_norm_displ_gpu", DEBUG); }
+void check_max_norm_vector_(int*, realw*, int*) { unsupported("check_max_norm_vector", DEBUG); }
+void check_max_norm_displ_(int*, realw*, int*) { unsupported("check_max_norm_displ", DEBUG); }
+void check_max_norm_b_displ_gpu_(int*, realw*, long*, int*) { unsupported("check_max_norm_b_displ_gpu", DEBUG); }
+void check_max_norm_b_accel_gpu_(int*, realw*, long*, int*) { unsupported("check_max_norm_b_accel_gpu", DEBUG); }
+void check_max_norm_b_veloc_gpu_(int*, realw*, long*, int*) { unsupported("check_max_norm_b_veloc_gpu", DEBUG); }
+void check_max_norm_b_displ_(int*, realw*, int*) { unsupported("check_max_norm_b_displ", DEBUG); }
+void check_max_norm_b_accel_(int*, realw*, int*) { unsupported("check_max_norm_b_accel", DEBUG); }
+void check_error_vectors_(int*, realw*, realw*) { unsupported("check_error_vectors", DEBUG); }
+void compute_add_sources_ac_cuda_(long*, int*, int*) { unsupported("compute_add_sources_ac_cuda", FLUID); }
+void compute_add_sources_ac_s3_cuda_(long*, int*, int*) { unsupported("compute_add_sources_ac_s3_cuda", KERNEL_RUN); }
+void compute_add_moving_sources_ac_cuda_(long*, int*, int*, int*, int*, int*) { unsupported("compute_add_moving_sources_ac_cuda", OTHER); }
+void add_sources_ac_sim_2_or_3_cuda_(long*, int*, int*, int*, int*) { unsupported("add_sources_ac_sim_2_or_3_cuda", KERNEL_RUN); }
+void compute_add_sources_el_s3_cuda_(long*, int*, int*) { unsupported("compute_add_sources_el_s3_cuda", KERNEL_RUN); }
+void add_sources_el_sim_type_2_or_3_(long*, int*, int*, int*, int*) { unsupported("add_sources_el_sim_type_2_or_3", KERNEL_RUN); }
+void compute_coupling_ac_el_cuda_(long*, int*, int*, int*) { unsupported("compute_coupling_ac_el_cuda", FLUID); }
+void compute_coupling_el_ac_cuda_(long*, int*, int*, int*) { unsupported("compute_coupling_el_ac_cuda", FLUID); }
+void compute_forces_acoustic_cuda_(long*, int*, int*, int*, int*, int*, int*) { unsupported("compute_forces_acoustic_cuda", FLUID); }
+void compute_kernels_elastic_cuda_(long*, realw*) { unsupported("compute_kernels_elastic_cuda", KERNEL_RUN); }
+void compute_kernels_acoustic_cuda_(long*, realw*) { unsupported("compute_kernels_acoustic_cuda", KERNEL_RUN); }
+void compute_kernels_hess_cuda_(long*, int*, int*) { unsupported("compute_kernels_hess_cuda", OTHER); }
+void compute_stacey_acoustic_cuda_(long*, int*, realw*, realw*, realw*, realw*, int*, int*, int*) { unsupported("compute_stacey_acoustic_cuda", FLUID); }
+void acoustic_enforce_free_surf_cuda_(long*, int*, int*) { unsupported("acoustic_enforce_free_surf_cuda", FLUID); }
+void pml_boundary_acoustic_cuda_(long*, int*, int*) { unsupported("pml_boundary_acoustic_cuda", FLUID); }
+void prepare_fields_acoustic_device_(long*, realw*, realw*, realw*, int*, int*, int*, int*, int*, int*, int*, int*, int*, realw*, realw*, int*, int*, int*, realw*, realw*, int*, realw*) { unsupported("prepare_fields_acoustic_device", FLUID); }
+void prepare_fields_acoustic_adj_dev_(long*, int*, int*, int*) { unsupported("prepare_fields_acoustic_adj_dev", KERNEL_RUN); }
+void prepare_fields_elastic_adj_dev_(long*, int*, int*, int*, int*) { unsupported("prepare_fields_elastic_adj_dev", KERNEL_RUN); }
+void prepare_sim2_or_3_const_device_(long*, int*, realw*, int*) { unsupported("prepare_sim2_or_3_const_device", KERNEL_RUN); }
+void prepare_pml_device_(long*, int*, int*, int*, int*, int*, realw*, realw*, realw*, realw*, realw*, realw*, realw*, realw*, int*, int*) { unsupported("prepare_pml_device", FLUID); }
+void prepare_moving_sources_cuda_(long*, int*, int*, realw*, int*, int*, realw*) { unsupported("prepare_moving_sources_cuda", OTHER); }
+void prepare_arrays_gpu_(long*, realw*, realw*, realw*, realw*, realw*, realw*, int*, int*, realw*) { unsupported("prepare_arrays_gpu", OTHER); }
+void compute_smooth_(long*, realw*, realw*, realw*, realw*, const int*) { unsupported("compute_smooth", OTHER); }
+void get_smooth_(long*, realw*) { unsupported("get_smooth", OTHER); }
+void transfer_b_fields_to_device_(int*, realw*, realw*, realw*, long*) { unsupported("transfer_b_fields_to_device", KERNEL_RUN); }
+void transfer_b_fields_from_device_(int*, realw*, realw*, realw*, long*) { unsupported("transfer_b_fields_from_device", KERNEL_RUN); }
+void transfer_b_accel_from_device_(int*, realw*, long*) { unsupported("transfer_b_accel_from_device", KERNEL_RUN); }
+void transfer_b_displ_from_device_(int*, realw*, long*) { unsupported("transfer_b_displ_from_device", KERNEL_RUN); }
+void transfer_kernels_el_to_host_(long*, realw*, realw*, realw*, int*) { unsupported("transfer_kernels_el_to_host", KERNEL_RUN); }
+void transfer_fields_ac_to_device_(int*, realw*, realw*, realw*, long*) { unsupported("transfer_fields_ac_to_device", FLUID); }
+void transfer_b_fields_ac_to_device_(int*, realw*, realw*, realw*, long*) { unsupported("transfer_b_fields_ac_to_device", KERNEL_RUN); }
+void transfer_fields_ac_from_device_(int*, realw*, realw*, realw*, long*) { unsupported("transfer_fields_ac_from_device", FLUID); }
+void transfer_b_fields_ac_from_device_(int*, realw*, realw*, realw*, long*) { unsupported("transfer_b_fields_ac_from_device", KERNEL_RUN); }
+void transfer_b_potential_ac_from_device_(int*, realw*, long*) { unsupported("transfer_b_potential_ac_from_device", KERNEL_RUN); }
+void transfer_b_potential_ac_to_device_(int*, realw*, long*) { unsupported("transfer_b_potential_ac_to_device", KERNEL_RUN); }
+void transfer_dot_dot_from_device_(int*, realw*, long*) { unsupported("transfer_dot_dot_from_device", FLUID); }
+void transfer_b_dot_dot_from_device_(int*, realw*, long*) { unsupported("transfer_b_dot_dot_from_device", KERNEL_RUN); }
+void transfer_kernels_ac_to_host_(long*, realw*, realw*, int*) { unsupported("transfer_kernels_ac_to_host", KERNEL_RUN); }
+void transfer_kernels_hess_el_tohost_(long*, realw*, int*) { unsupported("transfer_kernels_hess_el_tohost", OTHER); }
+void transfer_kernels_hess_ac_tohost_(long*, realw*, int*) { unsupported("transfer_kernels_hess_ac_tohost", OTHER); }
+void transfer_viscoacoustic_b_var_to_device_(int*, realw*, realw*, long*) { unsupported("transfer_viscoacoustic_b_var_to_device", KERNEL_RUN); }
+void transfer_viscoacoustic_var_from_device_(int*, realw*, realw*, long*) { unsupported("transfer_viscoacoustic_var_from_device", KERNEL_RUN); }
+void transfer_viscoelastic_b_var_to_device_(int*, realw*, realw*, realw*, realw*, realw*, realw*, long*) { unsupported("transfer_viscoelastic_b_var_to_device", KERNEL_RUN); }
+void transfer_viscoelastic_var_from_device_(int*, realw*, realw*, realw*, realw*, realw*, realw*, long*) { unsupported("transfer_viscoelastic_var_from_device", KERNEL_RUN); }
+void transfer_async_pot_ac_from_device_(realw*, long*) { unsupported("transfer_async_pot_ac_from_device", MPI); }
+void transfer_async_pot_ac_to_device_(realw*, long*) { unsupported("transfer_async_pot_ac_to_device", MPI); }
+void transfer_compute_kernel_answers_from_device_(long*, realw*, int*, realw*, int*, realw*, int*) { unsupported("transfer_compute_kernel_answers_from_device", KERNEL_RUN); }
+void transfer_compute_kernel_fields_from_device_(long*, realw*, int*, realw*, int*, realw*, realw*, realw*, realw*, realw*, int*, realw*, realw*, realw*, realw*, realw*, int*, realw*, int*, realw*, int*, realw*, int*, realw*, realw*, int*) { unsupported("transfer_compute_kernel_fields_from_device", KERNEL_RUN); }
+void update_displacement_ac_cuda_(long*, realw*, realw*, realw*, realw*, realw*, realw*, int*, int*) { unsupported("update_displacement_ac_cuda", FLUID); }
+void kernel_3_b_cuda_(long*, realw*, realw*) { unsupported("kernel_3_b_cuda", KERNEL_RUN); }
+void kernel_3_acoustic_cuda_(long*, realw*, realw*, int*, int*) { unsupported("kernel_3_acoustic_cuda", FLUID); }
+
+}  // extern "C"

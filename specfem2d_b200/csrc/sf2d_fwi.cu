@@ -75,7 +75,8 @@ extern "C" int sf2d_fwi_create(const sf2d_elastic_desc *d, const float *rhostore
   ad.sourcearrays = a_arr.data();
   ad.stf = a_stf.data();
   ad.nstage = 1;
-  ad.nrec = 0;
+  // the adjoint field is recorded at the receivers too (write_seismograms.F90
+  // records the adjoint wavefield in a kernel run)
   rc = sf2d_create_solver_internal(&ad, true, &F->adj, nullptr);
   if (rc) return rc;
   F->nstep = nstep;
@@ -202,6 +203,11 @@ extern "C" int sf2d_fwi_backward(sf2d_fwi *F, const float *adj_src, float *rho_k
     }
   }
   return st;
+}
+
+extern "C" int sf2d_fwi_adjoint_seismograms(sf2d_fwi *F, double *seismograms) {
+  if (!F || !seismograms) return fail(SF2D_ERR_INVALID, "null argument");
+  return sf2d_copy_seismograms(F->adj, 0, F->nstep, seismograms);
 }
 
 extern "C" int sf2d_fwi_destroy(sf2d_fwi *F) {

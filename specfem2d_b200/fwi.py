@@ -61,6 +61,12 @@ class FWIGradient:
         _check(self._lib.sf2d_fwi_backward(self._h, adj.ctypes.data_as(_f), *[o.ctypes.data_as(_f) for o in out]))
         return tuple(out)
 
+    def adjoint_seismograms(self) -> np.ndarray:
+        """Receiver traces (nrec, nstep, 2) of the adjoint field of the last backward()."""
+        seis = np.zeros((self.nrec, self.nstep, 2), dtype=np.float64)
+        _check(self._lib.sf2d_fwi_adjoint_seismograms(self._h, seis.ctypes.data_as(_d)))
+        return seis
+
 
 def l2_misfit_gradient(db, observed, checkpoint_every: int = 200, **kw):
     """(chi, synthetics, rho_kl, kappa_kl, mu_kl) for chi = 1/2 sum_r sum_it |s - d|^2 dt."""

@@ -99,6 +99,7 @@ def load_library(path: str = LIB):
         "sf2d_fwi_create": [ctypes.POINTER(ElasticDesc), _f, _f, ctypes.c_int, ctypes.POINTER(vp)],
         "sf2d_fwi_forward": [vp, _d],
         "sf2d_fwi_backward": [vp, _f, _f, _f, _f],
+        "sf2d_fwi_adjoint_seismograms": [vp, _d],
         "sf2d_fwi_destroy": [vp],
         "sf2d_member_norms_noalloc": [vp, ctypes.POINTER(ctypes.c_int64), ctypes.c_int, _f, vp],
     }

@@ -209,6 +209,30 @@ def _edge_points(mesh: Mesh, abs_corner_skip=True):
         yield k, t, pts
 
 
+def edge_normal(geo: dict, gll: GLL, e: int, i: int, j: int, t: int):
+    """Outward normal (nx, nz) and weight jacobian1D * w of GLL point (i, j) of
+    element e on an edge of type t, in FP32 arithmetic
+    (compute_stacey_elastic.f90:118-980, prepare_timerun.F90:1315-1430)."""
+    jac = geo["jacobian"][e, j, i]
+    if t in (ILEFT, IRIGHT):
+        xgamma = f32(-geo["xiz"][e, j, i] * jac)
+        zgamma = f32(geo["xix"][e, j, i] * jac)
+        j1d = f32(np.sqrt(f32(f32(xgamma * xgamma) + f32(zgamma * zgamma))))
+        if t == ILEFT:
+            nx, nz = f32(-zgamma / j1d), f32(xgamma / j1d)
+        else:
+            nx, nz = f32(zgamma / j1d), f32(-xgamma / j1d)
+        return nx, nz, f32(j1d * gll.wzgll[j])
+    xxi = f32(geo["gammaz"][e, j, i] * jac)
+    zxi = f32(-geo["gammax"][e, j, i] * jac)
+    j1d = f32(np.sqrt(f32(f32(xxi * xxi) + f32(zxi * zxi))))
+    if t == IBOTTOM:
+        nx, nz = f32(zxi / j1d), f32(-xxi / j1d)
+    else:
+        nx, nz = f32(-zxi / j1d), f32(xxi / j1d)
+    return nx, nz, f32(j1d * gll.wxgll[i])
+
+
 def stacey_points(mesh: Mesh, geo: dict, mat: dict, ibool, gll: GLL, stacey: bool, elastic=None):
     """Per absorbing GLL point of an elastic element (all elements when
     ``elastic`` is None): iglob, normal, weight, rho*vp, rho*vs in FP32 arithmetic."""
@@ -219,25 +243,7 @@ def stacey_points(mesh: Mesh, geo: dict, mat: dict, ibool, gll: GLL, stacey: boo
             if elastic is not None and not elastic[e]:
                 continue
             for (i, j) in pts:
-                jac = geo["jacobian"][e, j, i]
-                if t in (ILEFT, IRIGHT):
-                    xgamma = f32(-geo["xiz"][e, j, i] * jac)
-                    zgamma = f32(geo["xix"][e, j, i] * jac)
-                    j1d = f32(np.sqrt(f32(f32(xgamma * xgamma) + f32(zgamma * zgamma))))
-                    if t == ILEFT:
-                        nx, nz = f32(-zgamma / j1d), f32(xgamma / j1d)
-                    else:
-                        nx, nz = f32(zgamma / j1d), f32(-xgamma / j1d)
-                    w = f32(j1d * gll.wzgll[j])
-                else:
-                    xxi = f32(geo["gammaz"][e, j, i] * jac)
-                    zxi = f32(-geo["gammax"][e, j, i] * jac)
-                    j1d = f32(np.sqrt(f32(f32(xxi * xxi) + f32(zxi * zxi))))
-                    if t == IBOTTOM:
-                        nx, nz = f32(zxi / j1d), f32(-xxi / j1d)
-                    else:
-                        nx, nz = f32(-zxi / j1d), f32(xxi / j1d)
-                    w = f32(j1d * gll.wxgll[i])
+                nx, nz, w = edge_normal(geo, gll, e, i, j, t)
                 out["iglob"].append(int(ibool[e, j, i]))
                 out["nx"].append(nx)
                 out["nz"].append(nz)

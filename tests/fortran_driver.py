@@ -1,0 +1,148 @@
+"""Drives libsf2d_b200.so through the reference's Fortran-to-GPU entry points
+(include/sf2d_fortran.h) in the order the SPECFEM2D Fortran host calls them,
+with arguments passed by reference as gfortran passes them:
+
+* prepare_GPU (src/specfem2D/prepare_gpu.f90:34-320): initialize_cuda_device,
+  prepare_constants_device, prepare_fields_elastic_device, prepare_Stacey_device,
+  transfer_fields_el_to_device;
+* each time step it = 1..NSTEP (iterate_time.F90:146-260):
+  update_displacement_cuda (update_displacement_Newmark.F90:530-549), then
+  compute_forces_viscoelastic_GPU (compute_gpu_elastic.f90:36-215): forces for
+  iphase 1 with Stacey and sources, forces for iphase 2, kernel_3_a_cuda; then
+  write_seismograms (write_seismograms.F90:199-205) and, every `check_every`
+  steps, check_stability's get_norm_elastic_from_device;
+* prepare_cleanup_device.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from specfem2d_b200.setup.fortran_host import gpu_arrays
+
+
+def _lib():
+    from specfem2d_b200.runtime import load_library
+
+    return load_library()
+
+
+class _Refs:
+    """Keeps the by-reference scalars and arrays of the calls alive."""
+
+    def __init__(self):
+        self.keep = []
+
+    def i(self, v):
+        x = ctypes.c_int(int(v))
+        self.keep.append(x)
+        return ctypes.byref(x)
+
+    def f(self, v):
+        x = ctypes.c_float(float(v))
+        self.keep.append(x)
+        return ctypes.byref(x)
+
+    def a(self, arr):
+        self.keep.append(arr)
+        return arr.ctypes.data_as(ctypes.c_void_p)
+
+
+def run_forward(db, nstep=None, check_every=1000, nlength_seismogram=None):
+    """Returns (seismograms (nrec, nstep, 2) float64, final displacement (nglob, 2), norms)."""
+    lib = _lib()
+    A = gpu_arrays(db, nlength_seismogram)
+    nstep = int(nstep or A["nstep"])
+    nlen = A["nlength_seismogram"]
+    r = _Refs()
+    mesh = ctypes.c_long(0)
+    M = ctypes.byref(mesh)
+    ndev = ctypes.c_int(0)
+    lib.initialize_cuda_device_(r.i(0), ctypes.byref(ndev))
+    dummy_i = np.zeros(1, np.int32)
+    dummy_f = np.zeros(1, np.float32)
+    lib.prepare_constants_device_(
+        M, r.i(5), r.i(A["nspec"]), r.i(A["nglob"]),
+        r.a(A["xix"]), r.a(A["xiz"]), r.a(A["gammax"]), r.a(A["gammaz"]),
+        r.a(A["kappastore"]), r.a(A["mustore"]), r.a(A["ibool"]),
+        r.i(0), r.i(0), r.a(dummy_i), r.a(dummy_i),
+        r.a(A["hprime_xx"]), r.a(A["hprimewgll_xx"]), r.a(A["wxgll"]),
+        r.i(1 if A["stacey"] else 0), r.i(0), r.a(np.ones(A["nspec"], np.int32)),
+        r.i(A["nsrc"]), r.a(A["sourcearrays"]), r.a(A["source_time_function"]),
+        r.i(A["nstep"]), r.a(A["ispec_selected_source"]), r.a(A["ispec_selected_rec_loc"]),
+        r.i(A["nrec"]), r.a(A["cosrot"]), r.a(A["sinrot"]),
+        r.i(1), r.i(1), r.i(0), r.i(A["nspec"]),
+        r.a(np.zeros(A["nspec"], np.int32)), r.a(np.ones(A["nspec"], np.int32)),
+        r.i(0), r.i(0),
+        r.a(A["xir_store"]), r.a(A["gammar_store"]),
+        r.i(1), r.a(np.array([A["seismotype"]], np.int32)), r.i(nlen))
+    aniso = "ispec_is_anisotropic" in A
+    atten = "att_a1" in A
+    c = {k: (A[k + "store"] if aniso else dummy_f) for k in ("c11", "c13", "c15", "c33", "c35", "c55")}
+    att = {k: (A["att_" + k] if atten else dummy_f) for k in ("a1", "b1", "a2", "b2")}
+    lib.prepare_fields_elastic_device_(
+        M, r.a(A["rmassx"]), r.a(A["rmassz"]), r.i(A["nspec"]), r.a(np.arange(1, A["nspec"] + 1, dtype=np.int32)),
+        r.a(A["ispec_is_anisotropic"] if aniso else dummy_i), r.i(1 if aniso else 0),
+        r.a(c["c11"]), r.a(dummy_f), r.a(c["c13"]), r.a(c["c15"]), r.a(dummy_f), r.a(dummy_f),
+        r.a(c["c33"]), r.a(c["c35"]), r.a(c["c55"]),
+        r.i(0), r.a(dummy_i), r.i(1 if atten else 0),
+        r.a(att["a2"]), r.a(att["b2"]), r.a(att["a1"]), r.a(att["b1"]))
+    if A["stacey"]:
+        ab = A["abs"]
+        lib.prepare_stacey_device_(
+            M, r.i(0), r.i(1), r.a(A["rho_vpstore"]), r.a(A["rho_vsstore"]),
+            r.i(ab["counts"]["bottom"]), r.i(ab["counts"]["left"]), r.i(ab["counts"]["right"]),
+            r.i(ab["counts"]["top"]), r.a(ab["abs_boundary_ispec"]), r.a(ab["abs_boundary_ij"]),
+            r.a(ab["abs_boundary_normal"]), r.a(ab["abs_boundary_jacobian1Dw"]), r.i(ab["nface"]),
+            r.a(ab["edge_abs"]), r.a(dummy_i), r.a(dummy_i), r.a(dummy_i), r.a(dummy_i))
+    ng2 = 2 * A["nglob"]
+    zeros = np.zeros(ng2, np.float32)
+    lib.transfer_fields_el_to_device_(r.i(ng2), r.a(zeros), r.a(zeros.copy()), r.a(zeros.copy()), M)
+    sisux = np.zeros((A["nrec"], nlen), np.float64)
+    sisuz = np.zeros_like(sisux)
+    seis = np.zeros((A["nrec"], nstep, 2))
+    dt, dt2, dtsq2 = ctypes.c_float(A["deltat"]), ctypes.c_float(A["deltatover2"]), ctypes.c_float(A["deltatsquareover2"])
+    one, two, zero = ctypes.c_int(1), ctypes.c_int(2), ctypes.c_int(0)
+    nspec_c, aniso_c, atten_c = ctypes.c_int(A["nspec"]), ctypes.c_int(int(aniso)), ctypes.c_int(int(atten))
+    it_c, cur_c, nlen_c, end_c = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(nlen), ctypes.c_int(nstep)
+    stype = ctypes.c_int(A["seismotype"])
+    norm = ctypes.c_float(0.0)
+    norms = []
+    dummy_b = dummy_f.ctypes.data_as(ctypes.c_void_p)
+    seismo_current = 0
+    for it in range(1, nstep + 1):
+        it_c.value = it
+        lib.update_displacement_cuda_(M, ctypes.byref(dt), ctypes.byref(dtsq2), ctypes.byref(dt2),
+                                      ctypes.byref(dt), ctypes.byref(dtsq2), ctypes.byref(dt2))
+        for iphase in (one, two):
+            lib.compute_forces_viscoelastic_cuda_(M, ctypes.byref(iphase), ctypes.byref(dt), ctypes.byref(zero),
+                                                  ctypes.byref(nspec_c), ctypes.byref(aniso_c), ctypes.byref(atten_c),
+                                                  ctypes.byref(one), ctypes.byref(zero))
+            if iphase is one:
+                if A["stacey"]:
+                    lib.compute_stacey_viscoelastic_cuda_(M, ctypes.byref(one), dummy_b, dummy_b, dummy_b, dummy_b,
+                                                          ctypes.byref(one), ctypes.byref(zero), ctypes.byref(zero))
+                lib.compute_add_sources_el_cuda_(M, ctypes.byref(one), ctypes.byref(it_c))
+        lib.kernel_3_a_cuda_(M, ctypes.byref(dt2), ctypes.byref(dt2), ctypes.byref(one), ctypes.byref(zero))
+        seismo_current += 1
+        cur_c.value = seismo_current
+        lib.compute_seismograms_cuda_(M, ctypes.byref(one), sisux.ctypes.data_as(ctypes.c_void_p),
+                                      sisuz.ctypes.data_as(ctypes.c_void_p), ctypes.byref(cur_c),
+                                      ctypes.byref(nlen_c), ctypes.byref(one), ctypes.byref(zero),
+                                      ctypes.byref(zero), ctypes.byref(atten_c), ctypes.byref(it_c),
+                                      ctypes.byref(end_c))
+        if seismo_current == nlen or it == nstep:
+            # write_seismograms saves the buffer and starts it again
+            n = seismo_current
+            seis[:, it - n:it, 0] = sisux[:, :n]
+            seis[:, it - n:it, 1] = sisuz[:, :n]
+            seismo_current = 0
+        if it % check_every == 0 or it == nstep:
+            lib.get_norm_elastic_from_device_(ctypes.byref(norm), M, ctypes.byref(one))
+            norms.append(float(norm.value))
+    displ = np.zeros(ng2, np.float32)
+    lib.transfer_displ_from_device_(r.i(ng2), r.a(displ), M)
+    lib.prepare_cleanup_device_(M, r.i(0), r.i(1), r.i(int(aniso)), r.i(0), r.i(0), r.i(int(atten)), r.i(0),
+                                r.a(dummy_f))
+    return seis, displ.reshape(-1, 2), norms

@@ -124,6 +124,34 @@ def log_locations(path):
     return out
 
 
+def kernel_log_values(path):
+    """Numbers printed by the adjoint-source tool and the kernel run in
+    REF_KERNEL/output.log: the cross-correlation norm per component, the
+    adjoint sources' min/max as read by the solver, and the elastic kernels'
+    maxima (save_adjoint_kernels.f90:202-216)."""
+    out = {"norm": [], "kernel_max": {}}
+    keys = {"rho  kernel": "rho", "kappa kernel": "kappa", "mu kernel": "mu", "rho prime kernel": "rhop",
+            "alpha kernel": "alpha", "beta kernel": "beta"}
+    with open(path) as f:
+        for ln in f:
+            m = re.match(r"\s*Norm =\s+(\S+)", ln)
+            if m:
+                out["norm"].append(float(m.group(1)))
+            m = re.search(r"adjoint sources min/max\s*=\s*(\S+)\s+(\S+)", ln)
+            if m:
+                out["adj_min_max"] = [float(m.group(1)), float(m.group(2))]
+            for k, v in keys.items():
+                m = re.search(r"maximum value of " + k + r"\s*=\s*(\S+)", ln)
+                if m:
+                    out["kernel_max"][v] = float(m.group(1))
+    return out
+
+
+# adjoint (SIMULATION_TYPE = 3) run of an example: its REF_KERNEL traces (the
+# adjoint wavefield at the adjoint station) and the numbers of its log
+KERNEL_RUNS = {"tromp2005_kernel": ("EXAMPLES/Tromp2005_kernel", [("S0001", "BXX"), ("S0001", "BXZ")])}
+
+
 def main(ref_root, names=None):
     """Write the fixtures of `names` (all examples when None)."""
     for name, (rel, traces, par_file, source_file) in EXAMPLES.items():
@@ -142,6 +170,17 @@ def main(ref_root, names=None):
             arrs["t_first"] = np.array(d[0, 0])
             arrs["t_step"] = np.array(d[1, 0] - d[0, 0])
         np.savez_compressed(os.path.join(HERE, name + "_seis.npz"), **arrs)
+        if name in KERNEL_RUNS:
+            rel_k, ktraces = KERNEL_RUNS[name]
+            kdir = os.path.join(ref_root, rel_k, "REF_KERNEL")
+            # sample times of the forward traces as the adjoint-source tool reads them
+            karr = {"t_forward": np.loadtxt(os.path.join(ex, "REF_SEIS", f"AA.{ktraces[0][0]}.{ktraces[0][1]}.semd"))[:, 0]}
+            for st, comp in ktraces:
+                d = np.loadtxt(os.path.join(kdir, f"AA.{st}.{comp}.semd"))
+                karr[f"{st}_{comp}"] = d[:, 1]
+            np.savez_compressed(os.path.join(HERE, name + "_adjoint.npz"), **karr)
+            with open(os.path.join(HERE, name + "_adjoint.json"), "w") as f:
+                json.dump(kernel_log_values(os.path.join(kdir, "output.log")), f, indent=1)
         if name in TOMO_SCRIPTS:
             x, z, vp, vs, rho = tomography_grid(ref_root, TOMO_SCRIPTS[name])
             np.savez_compressed(os.path.join(HERE, name + "_tomo.npz"), x=x, z=z, vp=vp, vs=vs, rho=rho)

@@ -55,3 +55,71 @@ def test_coupled_split_keeps_every_interface_point():
     assert (maps["fluid_points"][cp["ac_point"]] == g).all() and (maps["solid_points"][cp["ac_el_point"]] == g).all()
     assert len(fl["rec_global"]) + len(cp["el_rec_global"]) == len(db.rec_ispec)
     assert sub.ibool.max() == sub.nglob - 1 and fl["ibool"].max() == fl["nglob"] - 1
+
+
+def fortran_symbols():
+    txt = open(os.path.join(ROOT, "include", "sf2d_fortran.h")).read()
+    return sorted(set(re.findall(r"^void (\w+_)\(", txt, re.M)))
+
+
+def test_library_exports_the_reference_fortran_interface():
+    """All 91 entry points of the reference's src/gpu Fortran interface
+    (specfem2D_gpu_cuda_method_stubs.c) with gfortran's trailing underscore."""
+    lib = runtime.load_library()
+    names = fortran_symbols()
+    assert len(names) == 91
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+@pytest.mark.parametrize("call,needle", [
+    ("compute_forces_acoustic_cuda_", "sf2d_coupled_create"),
+    ("kernel_3_b_cuda_", "sf2d_fwi_create"),
+    ("transfer_boun_accel_from_device_", "MPI"),
+    ("update_displacement_cuda_", "Mesh_pointer was not prepared"),
+])
+def test_fortran_interface_errors_exit_like_the_reference(call, needle):
+    """A call the library does not provide, or one on an unprepared handle, prints
+    the reason and exits with EXIT_FAILURE, as the reference's exit_on_error does
+    (no GPU is touched)."""
+    import subprocess
+    import sys
+
+    code = ("import ctypes, sys; sys.path.insert(0, %r); from specfem2d_b200.runtime import load_library; "
+            "lib = load_library(); h = ctypes.c_long(0); z = ctypes.c_int(0); "
+            "getattr(lib, %r)(ctypes.byref(h), ctypes.byref(z), ctypes.byref(z), ctypes.byref(z), "
+            "ctypes.byref(z), ctypes.byref(z), ctypes.byref(z)); print('returned')") % (ROOT, call)
+    p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120)
+    assert p.returncode == 1, (p.returncode, p.stdout, p.stderr)
+    assert needle in p.stderr and "returned" not in p.stdout
+
+
+def test_fortran_host_absorbing_faces_give_the_solver_stacey_points():
+    """The face arrays of prepare_timerun.F90 (fortran_host), unrolled the way
+    prepare_stacey_device unrolls them (points marked NGLLX + 1 left out), are
+    the per-point Stacey entries of the solver setup, value for value."""
+    import numpy as np
+
+    from specfem2d_b200.setup.fortran_host import gpu_arrays
+
+    cfg, _ = load_golden("tromp2005_kernel")
+    db = database_from_config(cfg, nstep=4)
+    A = gpu_arrays(db)
+    ab = A["abs"]
+    ig, nx, nz, w, rvp = [], [], [], [], []
+    for f in range(ab["nface"]):
+        e = ab["abs_boundary_ispec"][f] - 1
+        for k in range(5):
+            i, j = ab["abs_boundary_ij"][f, k] - 1
+            if i == 5 or j == 5:
+                continue
+            ig.append(db.ibool[e, j, i])
+            nx.append(ab["abs_boundary_normal"][f, k, 0])
+            nz.append(ab["abs_boundary_normal"][f, k, 1])
+            w.append(ab["abs_boundary_jacobian1Dw"][f, k])
+            rvp.append(A["rho_vpstore"][e, j, i])
+    assert np.array_equal(np.array(ig), db.stacey_iglob)
+    for got, want in ((nx, db.stacey_nx), (nz, db.stacey_nz), (w, db.stacey_weight), (rvp, db.stacey_rho_vp)):
+        assert np.array_equal(np.array(got, np.float32), want)
+    # hprime_xx(i2, i1) = l'_i1(xi_i2) in Fortran order
+    assert A["hprime_xx"].ravel()[1 * 5 + 3] == db.gll.hprime[3, 1]
