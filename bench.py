@@ -36,32 +36,49 @@ sys.path.insert(0, ROOT)
 CACHE = os.path.join("/tmp", "sf2d_bench_cache")
 
 
-def build_workload(name: str, nstep: int):
+def _make_workload(name: str, nstep: int, scale: int = 1):
     from specfem2d_b200 import configs
 
-    os.makedirs(CACHE, exist_ok=True)
-    path = os.path.join(CACHE, f"{name}_{nstep}.pkl")
-    if os.path.exists(path):
-        with open(path, "rb") as f:
-            return pickle.load(f)
+    if scale != 1 and name not in ("c2_coupled", "c2_coupled_stacey", "c2_geometry", "c3_viscoelastic",
+                                   "c3_viscoelastic_lddrk"):
+        raise SystemExit(f"--scale applies to the c2 and c3 workloads, not {name}")
     if name == "c2_coupled":
-        db = configs.c2_coupled(nstep=nstep, pml_thickness=20)
-    elif name == "c2_coupled_stacey":
-        db = configs.c2_coupled(nstep=nstep)
-    elif name == "c2_geometry":
-        db = configs.c2_geometry(nstep=nstep)
-    elif name == "c1":
-        db = configs.c1_homogeneous(nstep=nstep)
-    elif name == "c3_viscoelastic":
-        db = configs.c3_viscoelastic(nstep=nstep, time_scheme=1)
-    elif name == "c3_viscoelastic_lddrk":
-        db = configs.c3_viscoelastic(nstep=nstep, time_scheme=2)
-    else:
-        raise SystemExit(f"unknown workload {name}")
-    with open(path + ".tmp", "wb") as f:
-        pickle.dump(db, f, protocol=4)
-    os.replace(path + ".tmp", path)
+        return configs.c2_coupled(nstep=nstep, pml_thickness=20 // scale, scale=scale)
+    if name == "c2_coupled_stacey":
+        return configs.c2_coupled(nstep=nstep, scale=scale)
+    if name == "c2_geometry":
+        return configs.c2_geometry(nstep=nstep, scale=scale)
+    if name == "c1":
+        return configs.c1_homogeneous(nstep=nstep)
+    if name == "c3_viscoelastic":
+        return configs.c3_viscoelastic(nstep=nstep, time_scheme=1, scale=scale)
+    if name == "c3_viscoelastic_lddrk":
+        return configs.c3_viscoelastic(nstep=nstep, time_scheme=2, scale=scale)
+    raise SystemExit(f"unknown workload {name}")
+
+
+def build_workload(name: str, nstep: int, rank: int = 0, dist=None, scale: int = 1):
+    """The workload's Database (``scale`` divides the element counts: profiling
+    cases).  With several ranks, rank 0 builds it and the others load its
+    pickle (one set-up's memory instead of one per rank)."""
+    if dist is None:
+        return _make_workload(name, nstep, scale)
+    os.makedirs(CACHE, exist_ok=True)
+    path = os.path.join(CACHE, f"{name}_{nstep}_{scale}.pkl")
+    if rank == 0:
+        db = _make_workload(name, nstep, scale)
+        with open(path + ".tmp", "wb") as f:
+            pickle.dump(db, f, protocol=5)
+        os.replace(path + ".tmp", path)
+    dist.barrier()
+    if rank != 0:
+        with open(path, "rb") as f:
+            db = pickle.load(f)
     return db
+
+
+# steps of the configuration's whole run (the end-to-end leg over the full run)
+WORKLOAD_NSTEP = {"c1": 2000, "c2_coupled": 6000, "c3_viscoelastic": 8000}
 
 
 # DRAM bytes one step's solid tile launches move (read + write), measured with
@@ -71,6 +88,8 @@ def build_workload(name: str, nstep: int):
 TILE_TRAFFIC = {
     ("c2_coupled", 32, 256, 64, 16, 128): 233.0e6 + 43.45e6 + 71.07e6 + 0.40e6 + 1.25e6,
 }
+TRAFFIC_SOURCE = {k: "ncu dram__bytes_read.sum + dram__bytes_write.sum of one step's solid tile launches "
+                     "(early, late and CPML tiles), one capture" for k in TILE_TRAFFIC}
 
 WORKLOAD_DESC = {
     "c2_coupled": ("800x320-element (20 km x 8 km, 4,100,481 GLL points) coupled fluid-solid model: 1 km "
@@ -213,7 +232,7 @@ def run_reference_fwi(args, rank):
 def run_reference(args, rank):
     if rank != 0:
         return
-    db = build_workload(args.workload, max(args.steps, 8) + args.warmup + 8)
+    db = build_workload(args.workload, max(args.steps, 8) + args.warmup + 8, scale=args.scale)
     n, dt, threads = time_oracle(db, max_steps=max(args.steps, 2), target_s=args.ref_seconds)
     value = db.nglob * n / dt
     line = {
@@ -285,37 +304,21 @@ def fwi_members(n_models: int, nstep: int, which: str = "first"):
     return models
 
 
-def run_fwi(args, rank, world):
+def measure_fwi(args, all_models, nstep, world, rank):
     """Seconds per misfit gradient per model: plain (one model per run) and
-    batched (all models in one packed mesh), both through sf2d_fwi_* with the
-    traces and kernels copied to the host."""
+    batched (the models packed into meshes of --batch members, one launch per
+    step for all of them), both through sf2d_fwi_* with the traces and
+    kernels copied to the host; models are sharded over the ranks."""
     import torch
 
     from specfem2d_b200 import batch
+    from specfem2d_b200.distributed import max_over_ranks, shard, sum_over_ranks
     from specfem2d_b200.fwi import FWIGradient
 
-    from specfem2d_b200.distributed import max_over_ranks, shard, sum_over_ranks
-
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    from specfem2d_b200.runtime import initialize_device
-
-    initialize_device(int(os.environ.get("LOCAL_RANK", "0")))  # the library's own runtime, same device
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    if args.workload == "c4_fwi_shots":
-        all_models = c4_shots(args.models, args.fwi_steps)
-    else:
-        all_models = fwi_members(args.models, args.fwi_steps, args.fwi_set)
-    # shots and models are independent: each rank takes a share of nearly equal size
     mine = shard([m.nspec for m in all_models], rank, world)
     models = [all_models[k] for k in mine]
-    observed = [np.zeros((len(m.rec_ispec), args.fwi_steps, 2)) for m in models]
+    observed = [np.zeros((len(m.rec_ispec), nstep, 2)) for m in models]
     every = 100
-    nq = sum(m.nspec for m in all_models)
 
     def one(db, obs):
         g = FWIGradient(db, every, tile_elems=args.tile_elems, threads_per_block=args.threads)
@@ -338,8 +341,6 @@ def run_fwi(args, rank, world):
             t, k = one(m, obs)
             plain_s += t
             plain_k.append(k)
-        # batched: the members packed into meshes of at most --batch members
-        # (device memory: checkpoint frames grow with the packed mesh)
         bsize = args.batch if args.batch > 0 else len(models)
         bk = [[], [], []]
         for b0 in range(0, len(models), bsize):
@@ -356,25 +357,51 @@ def run_fwi(args, rank, world):
                 ref = plain_k[m][c].astype(np.float64)
                 num += float(np.sum((part.astype(np.float64) - ref) ** 2))
                 den += float(np.sum(ref ** 2))
-    # the job takes as long as its slowest rank
     plain_s = max_over_ranks(plain_s, device="cuda")
     batched_s = max_over_ranks(batched_s, device="cuda")
     num, den = (float(x) for x in sum_over_ranks(np.array([num, den]), device="cuda"))
     n = len(all_models)
     packed_nglob = int(sum_over_ranks(np.array([float(local_nglob)]), device="cuda")[0])
+    return {"metric": "s per FWI gradient per shot", "unit": "s", "models": n, "steps": nstep,
+            "sizes": [[int(m.nspec), int(m.nglob)] for m in all_models], "checkpoint_every": every,
+            "plain_s_per_shot": plain_s / n, "batched_s_per_shot": batched_s / n,
+            "speedup_batched_vs_plain": plain_s / batched_s,
+            "gradient_rel_l2_batched_vs_plain": (num / den) ** 0.5 if den > 0 else 0.0,
+            "point_updates_per_s_batched": 3.0 * packed_nglob * nstep / batched_s,
+            "nglob_total": packed_nglob}
+
+
+def run_fwi(args, rank, world):
+    """The FWI workloads as their own bench line (s per gradient per shot, batched)."""
+    import torch
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    from specfem2d_b200.runtime import initialize_device
+
+    initialize_device(int(os.environ.get("LOCAL_RANK", "0")))  # the library's own runtime, same device
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    if args.workload == "c4_fwi_shots":
+        all_models = c4_shots(args.models, args.fwi_steps)
+    else:
+        all_models = fwi_members(args.models, args.fwi_steps, args.fwi_set)
+    r = measure_fwi(args, all_models, args.fwi_steps, world, rank)
     line = {
-        "metric": "s per FWI gradient per shot", "value": batched_s / n, "unit": "s", "n_gpus": world,
+        "metric": "s per FWI gradient per shot", "value": r["batched_s_per_shot"], "unit": "s", "n_gpus": world,
         "steps": args.fwi_steps, "warmup": 1, "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": {"workload": args.workload, "description": FWI_WORKLOADS[args.workload], "models": n,
-                   "model_set": args.fwi_set, "sizes": [[int(m.nspec), int(m.nglob)] for m in all_models],
-                   "nspec_total": nq, "nglob_total": packed_nglob, "checkpoint_every": every,
+        "config": {"workload": args.workload, "description": FWI_WORKLOADS[args.workload], "models": r["models"],
+                   "model_set": args.fwi_set, "sizes": r["sizes"],
+                   "nspec_total": sum(m.nspec for m in all_models), "nglob_total": r["nglob_total"],
+                   "checkpoint_every": r["checkpoint_every"],
                    "parallelism": f"models sharded over {world} GPU(s)",
                    "tile_elems": args.tile_elems, "threads_per_cta": args.threads},
-        "plain_s_per_shot": plain_s / n, "batched_s_per_shot": batched_s / n,
-        "speedup_batched_vs_plain": plain_s / batched_s,
-        "gradient_rel_l2_batched_vs_plain": (num / den) ** 0.5 if den > 0 else 0.0,
-        "point_updates_per_s_batched": 3.0 * packed_nglob * args.fwi_steps / batched_s,
+        **{k: r[k] for k in ("plain_s_per_shot", "batched_s_per_shot", "speedup_batched_vs_plain",
+                             "gradient_rel_l2_batched_vs_plain", "point_updates_per_s_batched")},
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -384,66 +411,20 @@ def run_fwi(args, rank, world):
         dist.destroy_process_group()
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=6000)
-    ap.add_argument("--warmup", type=int, default=100)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2_coupled", choices=sorted(WORKLOAD_DESC) + sorted(FWI_WORKLOADS))
-    ap.add_argument("--models", type=int, default=12, help="models of the FWI workload")
-    ap.add_argument("--fwi-steps", type=int, default=1000, help="time steps of each FWI model")
-    ap.add_argument("--fwi-set", default="first", choices=["first", "smallest"],
-                    help="the first --models of the 48 seeded sizes, or the smallest")
-    ap.add_argument("--batch", type=int, default=0, help="members per packed mesh in the FWI workloads (0 = all)")
-    ap.add_argument("--tile-elems", type=int, default=32)
-    ap.add_argument("--threads", type=int, default=256)
-    ap.add_argument("--fluid-tile-elems", type=int, default=64, help="fluid tiles (coupled runs); 0 = --tile-elems")
-    ap.add_argument("--fluid-threads", type=int, default=0, help="fluid CTA threads; 0 = --threads")
-    ap.add_argument("--pml-tile-elems", type=int, default=16, help="solid CPML tiles; 0 = --tile-elems")
-    ap.add_argument("--pml-threads", type=int, default=128, help="solid CPML CTA threads; 0 = --threads")
-    ap.add_argument("--autotune", action="store_true", help="pick tile size and threads per CTA first")
-    ap.add_argument("--ref-seconds", type=float, default=15.0)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
-    args = ap.parse_args()
-    args.warmup = max(args.warmup, 3)
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-
-    if args.workload in FWI_WORKLOADS:
-        if args.impl == "reference":
-            run_reference_fwi(args, rank)
-        else:
-            run_fwi(args, rank, world)
-        return
-    if args.impl == "reference":
-        run_reference(args, rank)
-        return
-
+def measure_forward(db, args, workload, K, W, world, dist, nstep_full=0):
+    """One forward workload: K graph-queued steps timed with CUDA events on the
+    solver stream (max over ranks), per-kernel times for the roofline, and the
+    end-to-end leg through the public API with pinned host buffers (K steps,
+    and, with nstep_full, the configuration's whole run).  Returns the JSON
+    fields of the workload."""
     import torch
 
-    torch.cuda.set_device(local_rank)
-    from specfem2d_b200.runtime import initialize_device
-
-    initialize_device(local_rank)  # the library's own CUDA runtime on the same device
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist_mod
-
-        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-        dist = dist_mod
     from specfem2d_b200.configs import (algorithmic_bytes_coupled, algorithmic_bytes_elastic,
                                         algorithmic_bytes_viscoelastic)
     from specfem2d_b200.coupled import CoupledSolver
     from specfem2d_b200.distributed import job_throughput, max_over_ranks
     from specfem2d_b200.runtime import ElasticSolver
 
-    K, W = args.steps, args.warmup
-    db = build_workload(args.workload, K + W + 8)
     coupled = db.acoustic is not None
     tune = None
     if args.autotune and not coupled:
@@ -464,7 +445,8 @@ def main():
     stream = torch.cuda.ExternalStream(solver.stream_handle())
 
     # graph built and uploaded outside the timed region, warm-up, then the timed
-    # region: K steps queued as CUDA graphs on the solver stream
+    # region: K steps queued as CUDA graphs on the solver stream.  Fields and
+    # element data exceed the 126 MB L2, so no flush is needed between steps.
     solver.prepare()
     solver.enqueue(W)
     solver.synchronize(600)
@@ -485,8 +467,6 @@ def main():
     ms = max_over_ranks(ev0.elapsed_time(ev1), device="cuda")  # the job lasts as long as its slowest rank
     if dist:
         dist.barrier()
-    # per step (stage): a tile launch per tile group (with and without CPML) and a shared-point
-    # kernel per domain, and the CPML coupling-entry kernels; receiver kernels per chunk
     launches = solver.launch_count(K)
 
     # kernel-level timing for the roofline (events around each launch, same stream)
@@ -518,7 +498,7 @@ def main():
     if coupled:
         step_bytes = algorithmic_bytes_coupled(el_db.nspec, el_db.nglob, solver.nspec_fluid, solver.nglob_fluid,
                                                npml_el, npml_ac)
-    traffic_key = (args.workload, args.tile_elems, args.threads, args.fluid_tile_elems, args.pml_tile_elems,
+    traffic_key = (workload, args.tile_elems, args.threads, args.fluid_tile_elems, args.pml_tile_elems,
                    args.pml_threads)
     peaks = {}
     try:
@@ -528,96 +508,176 @@ def main():
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = tile_bytes / (tile_ms * 1e-3) / 1e9
-
-    # end to end through the public API with host buffers
-    # end to end: solver creation and its step-graph build are setup (outside the
-    # timed region, like the reference's prepare_*_device calls); the timed region
-    # uploads the initial fields, runs the K steps, and reads back the traces and
-    # the final fields, all through pinned host buffers
-    if args.no_e2e:
-        e2e_solver = None
-    else:
-        e2e_solver = make_solver()
-        e2e_solver.prepare()
+    solver.close()
 
     def pinned(shape, dtype):
         return torch.zeros(shape, dtype=dtype).pin_memory().numpy()
 
-    e2e_s, h2d, d2h = float("nan"), 0, 0
-    if e2e_solver is not None:
+    def e2e_run(nsteps):
+        """Seconds (max over ranks) and bytes of one run through the public API:
+        upload the initial fields, advance nsteps, read back the traces and the
+        final fields, all through pinned host buffers.  The solver and its step
+        graph are set up before the timed region, as the reference's
+        prepare_*_device calls are."""
+        sol = make_solver()
+        sol.prepare()
         zeros = pinned((db.nglob, 2), torch.float32)
-        seis_buf = pinned((e2e_solver.nrec, K, 2), torch.float64)
+        seis_buf = pinned((sol.nrec, nsteps, 2), torch.float64)
         if coupled:
             z1 = pinned((db.nglob,), torch.float32)
             outs = {k: pinned((db.nglob, 2), torch.float32) for k in ("displ", "veloc", "accel")}
             outs.update({k: pinned((db.nglob,), torch.float32) for k in ("pot", "pot_dot", "pot_dot_dot")})
         else:
             outs = [pinned((db.nglob, 2), torch.float32) for _ in range(3)]
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    if e2e_solver is not None:
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
         t0 = time.perf_counter()
         if coupled:
-            e2e_solver.set_fields(displ=zeros, veloc=zeros, accel=zeros, pot=z1, pot_dot=z1, pot_dot_dot=z1)
-            seis = e2e_solver.run(K, seismograms=True, out=seis_buf)
-            e2e_solver.get_fields(out=outs)
+            sol.set_fields(displ=zeros, veloc=zeros, accel=zeros, pot=z1, pot_dot=z1, pot_dot_dot=z1)
+            seis = sol.run(nsteps, seismograms=True, out=seis_buf)
+            sol.get_fields(out=outs)
             h2d = 3 * db.nglob * 8 + 3 * db.nglob * 4
-            d2h = seis.nbytes + h2d       # get_fields reads back the same six fields
         else:
-            e2e_solver.set_fields(zeros, zeros, zeros)
-            seis = e2e_solver.run(K, seismograms=True, out=seis_buf)
-            e2e_solver.get_fields(out=outs)
+            sol.set_fields(zeros, zeros, zeros)
+            seis = sol.run(nsteps, seismograms=True, out=seis_buf)
+            sol.get_fields(out=outs)
             h2d = 3 * db.nglob * 8
-            d2h = seis.nbytes + h2d
         t1 = time.perf_counter()
-        e2e_s = t1 - t0
-        e2e_solver.close()
-    e2e_s = max_over_ranks(e2e_s, device="cuda")
+        d2h = seis.nbytes + h2d  # the traces and the same fields read back
+        sol.close()
+        return max_over_ranks(t1 - t0, device="cuda"), h2d, d2h
+
+    e2e = None
+    if not args.no_e2e:
+        e2e_s, h2d, d2h = e2e_run(K)
+        e2e = {"value": db.nglob * K * world / e2e_s, "unit": "point-updates/s",
+               "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K}
+    e2e_full = None
+    if nstep_full and not args.no_e2e:
+        e2e_s, h2d, d2h = e2e_run(nstep_full)
+        e2e_full = {"value": db.nglob * nstep_full * world / e2e_s, "unit": "point-updates/s", "steps": nstep_full,
+                    "seconds": e2e_s, "h2d_bytes_per_step": h2d / nstep_full, "d2h_bytes_per_step": d2h / nstep_full}
 
     value = job_throughput(db.nglob * K, ms * 1e-3, world, device="cuda")
-    line = {
-        "metric": "GLL point-updates/s", "value": value, "unit": "point-updates/s",
-        "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": args.workload, "description": WORKLOAD_DESC[args.workload],
+    return {
+        "value": value, "ms_per_step": ms / K,
+        "config": {"workload": workload, "description": WORKLOAD_DESC[workload], "scale": args.scale,
                    "nspec": db.nspec, "nglob": db.nglob, "tile_elems": args.tile_elems,
-                   "fluid_tile_elems": args.fluid_tile_elems or args.tile_elems,
-                   "fluid_threads_per_cta": args.fluid_threads or args.threads,
+                   "fluid_tile_elems": (args.fluid_tile_elems or args.tile_elems) if coupled else None,
+                   "fluid_threads_per_cta": (args.fluid_threads or args.threads) if coupled else None,
                    "cpml_tile_elems": args.pml_tile_elems or args.tile_elems,
                    "cpml_threads_per_cta": args.pml_threads or args.threads,
                    "threads_per_cta": args.threads, "autotuned": bool(tune),
                    "ntiles": st["ntiles"], "shared_points": nsh,
                    "nspec_fluid": solver.nspec_fluid if coupled else 0,
                    "cpml_elements": {"solid": npml_el, "fluid": npml_ac},
-                   "l2": "inputs larger than L2 (fields + element data > 126 MB)",
+                   "l2": "inputs larger than L2 (fields + element data > 126 MB), no flush needed",
                    "e2e_setup": "solver created and step graph built before the timed region; "
                                 "fields and traces through pinned host buffers",
                    "parallelism": f"replicas x{world}"},
         "hbm_gbs_step": step_bytes / (ms / K * 1e-3) / 1e9,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": TILE_TRAFFIC.get(traffic_key),
-                     "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one step's solid "
-                                        "tile launches (early, late and CPML tiles), one capture"
-                                        if traffic_key in TILE_TRAFFIC else None),
+                     "traffic_source": TRAFFIC_SOURCE.get(traffic_key),
                      "kernel": "k_elastic_tile", "kernel_ms": tile_ms, "shared_kernel_ms": shared_ms,
                      "fluid_kernels_ms": k_ms[:2] if coupled else None, "step_kernels_ms": k_ms[-1],
                      "algorithmic_bytes_per_launch": tile_bytes,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
-        "e2e": {"value": db.nglob * K * world / e2e_s, "unit": "point-updates/s",
-                "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K},
+        "e2e": e2e, "e2e_full_run": e2e_full,
         "gpu_launches": launches,
         "clocks": clk,
     }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c3_viscoelastic", choices=sorted(WORKLOAD_DESC) + sorted(FWI_WORKLOADS))
+    ap.add_argument("--models", type=int, default=12, help="models of the FWI workload")
+    ap.add_argument("--fwi-steps", type=int, default=1000, help="time steps of each FWI model")
+    ap.add_argument("--fwi-set", default="first", choices=["first", "smallest"],
+                    help="the first --models of the 48 seeded sizes, or the smallest")
+    ap.add_argument("--batch", type=int, default=0, help="members per packed mesh in the FWI workloads (0 = all)")
+    ap.add_argument("--tile-elems", type=int, default=32)
+    ap.add_argument("--threads", type=int, default=256)
+    ap.add_argument("--fluid-tile-elems", type=int, default=64, help="fluid tiles (coupled runs); 0 = --tile-elems")
+    ap.add_argument("--fluid-threads", type=int, default=0, help="fluid CTA threads; 0 = --threads")
+    ap.add_argument("--pml-tile-elems", type=int, default=16, help="solid CPML tiles; 0 = --tile-elems")
+    ap.add_argument("--pml-threads", type=int, default=128, help="solid CPML CTA threads; 0 = --threads")
+    ap.add_argument("--autotune", action="store_true", help="pick tile size and threads per CTA first")
+    ap.add_argument("--ref-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end legs (profiling runs)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="headline workload only (no C2 coupled and batched-gradient keys)")
+    ap.add_argument("--scale", type=int, default=1,
+                    help="divide the element counts of the c2/c3 workloads (small profiling cases only)")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.workload in FWI_WORKLOADS:
+        if args.impl == "reference":
+            run_reference_fwi(args, rank)
+        else:
+            run_fwi(args, rank, world)
+        return
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    from specfem2d_b200.runtime import initialize_device
+
+    initialize_device(local_rank)  # the library's own CUDA runtime on the same device
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist_mod
+
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+        dist = dist_mod
+
+    K, W = args.steps, args.warmup
+    full = WORKLOAD_NSTEP.get(args.workload, 0) if args.scale == 1 else 0
+    db = build_workload(args.workload, max(K + W + 8, full), rank=rank, dist=dist, scale=args.scale)
+    res = measure_forward(db, args, args.workload, K, W, world, dist, nstep_full=full if world == 1 else 0)
+    line = {"metric": "GLL point-updates/s", "value": res["value"], "unit": "point-updates/s",
+            "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": res["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", **{k: res[k] for k in ("config", "hbm_gbs_step", "roofline", "e2e",
+                                                          "e2e_full_run", "gpu_launches", "clocks")}}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         n, dt, threads = time_oracle(db, max_steps=K, target_s=args.ref_seconds)
         line["cpu_baseline"] = {"value": db.nglob * n / dt, "unit": "point-updates/s", "cores": threads,
                                 "kind": "port",
                                 "sample": f"{n} time steps of the full mesh, C++ restatement of the "
                                           "reference CPU solver (FP32), all host threads"}
+    del db
+    if world == 1 and not args.no_extras and args.scale == 1:
+        # the other configurations of the metric, as extra keys of the same line
+        c2 = build_workload("c2_coupled", K + W + 8)
+        r2 = measure_forward(c2, args, "c2_coupled", K, W, world, dist)
+        line["c2_coupled"] = {"value": r2["value"], "unit": "point-updates/s", "ms_per_step": r2["ms_per_step"],
+                              "nglob": c2.nglob, "roofline_frac": r2["roofline"]["frac"],
+                              "tile_kernel_ms": r2["roofline"]["kernel_ms"], "e2e": r2["e2e"],
+                              "clocks": r2["clocks"]}
+        del c2
+        fwi = measure_fwi(args, fwi_members(24, 400, "smallest"), 400, world, rank)
+        fwi["description"] = ("the c5_fwi_models workload on its 24 smallest models (5,450-149,151 elements), "
+                              "400 steps: " + FWI_WORKLOADS["c5_fwi_models"])
+        line["fwi_gradient"] = fwi
     if rank == 0:
         print(json.dumps(line), flush=True)
-    solver.close()
     if dist:
         dist.destroy_process_group()
 

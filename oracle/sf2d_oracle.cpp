@@ -22,6 +22,8 @@
 #include <condition_variable>
 #include <functional>
 #include <mutex>
+#include <new>
+#include <pthread.h>
 #include <cstdlib>
 #include <cstring>
 #include <thread>
@@ -81,6 +83,10 @@ class Pool {
     job_(0);
     while (pending_.load(std::memory_order_acquire) != 0) relax();
   }
+  Pool() {
+    // a forked child has none of the parent's workers: it starts with none
+    pthread_atfork(nullptr, nullptr, [] { Pool::get().forget_workers(); });
+  }
   ~Pool() {
     {
       std::lock_guard<std::mutex> lk(m_);
@@ -92,6 +98,17 @@ class Pool {
   }
 
  private:
+  // In a child of fork(): the workers' std::thread objects name threads of the
+  // parent; they are abandoned (never joined or destroyed) and the locks made
+  // anew, so the child's first parallel call starts its own workers.
+  void forget_workers() {
+    new (&workers_) std::vector<std::thread>();
+    new (&call_m_) std::mutex();
+    new (&m_) std::mutex();
+    new (&cv_) std::condition_variable();
+    pending_.store(0, std::memory_order_relaxed);
+    nblocks_ = 0;
+  }
   static void relax() {
 #if defined(__x86_64__)
     __builtin_ia32_pause();

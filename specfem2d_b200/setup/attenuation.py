@@ -200,21 +200,35 @@ def attenuation_arrays(qkappa, qmu, f0_ref: float, dt: float, no_atten_mask=None
     qk = np.asarray(qkappa, dtype=np.float64)
     qm = np.asarray(qmu, dtype=np.float64)
     shape = qk.shape + (N_SLS,)
-    out = {k: np.zeros(shape, dtype=f32) for k in ("a1", "b1", "a2", "b2", "itau1", "phi1", "itau2", "phi2",
-                                                   "teps1", "teps2")}
+    keys = ("a1", "b1", "a2", "b2", "itau1", "phi1", "itau2", "phi2", "teps1", "teps2")
     # Mu_nu1, Mu_nu2 per point (used by CPML layers in attenuating solids)
+    out = {k: np.zeros(shape, dtype=f32) for k in keys}
     out["mu1"] = np.zeros(qk.shape, dtype=f32)
     out["mu2"] = np.zeros(qk.shape, dtype=f32)
     active = ~((qk > 9998.999) & (qm > 9998.999))
     if no_atten_mask is not None:
         active &= ~no_atten_mask
-    pairs = np.unique(np.stack([qk[active], qm[active]], axis=1), axis=0) if active.any() else []
-    for qkv, qmv in pairs:
-        sel = active & (qk == qkv) & (qm == qmv)
-        (it1, ph1, te1, m1), (it2, ph2, te2, m2) = zener_parameters(float(qkv), float(qmv), float(f0_ref))
+    if not active.any():
+        return out
+    import pandas as pd
+
+    # distinct (Qkappa, Qmu) pairs by hashing (models hold a few of them); row 0 of
+    # every table is the zero row of points without attenuation
+    codes, uniq = pd.factorize((qk + 1j * qm).ravel())
+    codes += 1
+    codes[~active.ravel()] = 0
+    tables = {k: np.zeros((len(uniq) + 1, N_SLS), dtype=f32) for k in keys}
+    tables["mu1"] = np.zeros(len(uniq) + 1, dtype=f32)
+    tables["mu2"] = np.zeros(len(uniq) + 1, dtype=f32)
+    used = np.unique(codes)
+    for c in used[used > 0]:
+        qkv, qmv = float(uniq[c - 1].real), float(uniq[c - 1].imag)
+        (it1, ph1, te1, m1), (it2, ph2, te2, m2) = zener_parameters(qkv, qmv, float(f0_ref))
         a1, b1 = newmark_coefficients(it1, ph1, dt)
         a2, b2 = newmark_coefficients(it2, ph2, dt)
         for k, v in (("a1", a1), ("b1", b1), ("a2", a2), ("b2", b2), ("itau1", it1), ("phi1", ph1),
                      ("itau2", it2), ("phi2", ph2), ("teps1", te1), ("teps2", te2), ("mu1", m1), ("mu2", m2)):
-            out[k][sel] = v
+            tables[k][c] = v
+    for k in out:
+        out[k] = tables[k][codes].reshape(out[k].shape)
     return out

@@ -118,6 +118,12 @@ class Mesh:
     free_top: bool = True
     absorb: tuple = (True, True, False, True)  # (bottom, right, top, left) outer edges absorbing
 
+    def __getstate__(self):
+        # the node-interpolation cache is derived data: rebuilt on demand, never pickled
+        state = dict(self.__dict__)
+        state.pop("_interp_cache", None)
+        return state
+
 
 def internal_mesh(xmin, xmax, nx, interfaces, nz_layer, absorb=(True, True, False, True),
                   ngnod=4, topography_fn=None):
@@ -253,14 +259,22 @@ def _shape_tables(gll: GLL, ngnod: int):
 
 
 def _interp_nodes(mesh: Mesh, tab):
-    """Sum_in tab[j,i,in] * coorg[knods[e,in]] accumulated in node order, for x and z."""
+    """Sum_in tab[j,i,in] * coorg[knods[e,in]] accumulated in node order, for x and z.
+    The result is kept on the mesh for later calls with the same table."""
+    cache = mesh.__dict__.setdefault("_interp_cache", {})
+    key = (tab.shape, tab.tobytes())
+    if key in cache:
+        return cache[key]
     xe = mesh.coorg[mesh.knods, 0]  # (nspec, ngnod)
     ze = mesh.coorg[mesh.knods, 1]
     x = np.zeros((mesh.nspec, NGLL, NGLL))
     z = np.zeros((mesh.nspec, NGLL, NGLL))
     for ia in range(mesh.ngnod):
-        x = x + tab[None, :, :, ia] * xe[:, ia, None, None]
-        z = z + tab[None, :, :, ia] * ze[:, ia, None, None]
+        x += tab[None, :, :, ia] * xe[:, ia, None, None]
+        z += tab[None, :, :, ia] * ze[:, ia, None, None]
+    x.flags.writeable = False
+    z.flags.writeable = False
+    cache[key] = (x, z)
     return x, z
 
 

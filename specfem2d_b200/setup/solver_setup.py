@@ -313,7 +313,9 @@ class _PointLocator:
         self.tree = cKDTree(coord)
         flat = ibool.ravel()
         first = np.full(coord.shape[0], flat.size, dtype=np.int64)
-        np.minimum.at(first, flat, np.arange(flat.size))
+        # first occurrence of every point in scan order: with a repeated index the
+        # last assignment wins, so the occurrences are written in reverse order
+        first[flat[::-1]] = np.arange(flat.size - 1, -1, -1, dtype=np.int64)
         self.first = first
         # corner point -> elements having it as a corner (CSR), for the candidate search
         corners = ibool[:, [0, 0, NGLL - 1, NGLL - 1], [0, NGLL - 1, 0, NGLL - 1]].ravel()
