@@ -87,9 +87,16 @@ WORKLOAD_NSTEP = {"c1": 2000, "c2_coupled": 6000, "c3_viscoelastic": 8000}
 # CPML threads); the roofline's "traffic" reports it beside the algorithmic bytes
 TILE_TRAFFIC = {
     ("c2_coupled", 32, 256, 64, 16, 128): 233.0e6 + 43.45e6 + 71.07e6 + 0.40e6 + 1.25e6,
+    # 376.16 MB per launch on the quarter-scale model (80,000 elements), x16 elements
+    ("c3_viscoelastic", 32, 256, 64, 16, 128): 376.16e6 * 16,
 }
-TRAFFIC_SOURCE = {k: "ncu dram__bytes_read.sum + dram__bytes_write.sum of one step's solid tile launches "
-                     "(early, late and CPML tiles), one capture" for k in TILE_TRAFFIC}
+TRAFFIC_SOURCE = {
+    ("c2_coupled", 32, 256, 64, 16, 128): "ncu dram__bytes_read.sum + dram__bytes_write.sum of one step's solid "
+                                          "tile launches (early, late and CPML tiles), one capture",
+    ("c3_viscoelastic", 32, 256, 64, 16, 128): "ncu dram__bytes_read.sum + dram__bytes_write.sum of one tile "
+                                               "launch on the quarter-scale model (--scale 4), scaled by the "
+                                               "element count (x16)",
+}
 
 WORKLOAD_DESC = {
     "c2_coupled": ("800x320-element (20 km x 8 km, 4,100,481 GLL points) coupled fluid-solid model: 1 km "

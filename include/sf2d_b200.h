@@ -52,6 +52,7 @@ extern "C" {
 #define SF2D_ERR_CUDA (-2)
 #define SF2D_ERR_OOM (-3)
 #define SF2D_ERR_UNSTABLE (-4)
+#define SF2D_ERR_TIMEOUT (-5)
 
 typedef struct sf2d_solver sf2d_solver;
 
@@ -161,10 +162,25 @@ int sf2d_run(sf2d_solver *s, int nstep, double *seismograms);
  * stream (CUDA graphs of fixed step chunks).  sf2d_synchronize waits (with a
  * timeout in seconds, <= 0 meaning none) and returns the stability status. */
 int sf2d_enqueue(sf2d_solver *s, int nstep);
+/* (sf2d_synchronize returns SF2D_ERR_TIMEOUT when the steps have not finished
+ * within timeout_s; they keep running and a later call waits for them.) */
 /* Builds and uploads the CUDA graph of one step chunk now (capture runs
  * nothing), so that a later sf2d_enqueue starts without that host work. */
 int sf2d_prepare(sf2d_solver *s);
 int sf2d_synchronize(sf2d_solver *s, double timeout_s);
+
+/* Packed batches (several independent meshes in one solver, the GPU form of
+ * NUMBER_OF_SIMULTANEOUS_RUNS, src/shared/parallel.F90:40-50): elem_member
+ * (nspec values in [0, nmembers)) names the member of every element.  From
+ * then on a member whose displacement becomes NaN or exceeds 1e25 is masked:
+ * its tiles and points keep their last values and stop advancing, the other
+ * members run on, and the run does not return SF2D_ERR_UNSTABLE for it.  The
+ * reference instead aborts all runs and leaves a runXXXX_failed marker
+ * (parallel.F90:190-214).  A tile or point may not mix members
+ * (SF2D_ERR_INVALID).  Clears every member's status. */
+int sf2d_set_members(sf2d_solver *s, const int *elem_member, int nmembers);
+/* status (nmembers ints): 0 running, 1 masked because its field blew up. */
+int sf2d_member_status(sf2d_solver *s, int *status);
 
 /* Copies receiver traces [it0, it0+nstep) already recorded on the device. */
 int sf2d_copy_seismograms(sf2d_solver *s, int it0, int nstep, double *out);

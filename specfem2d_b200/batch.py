@@ -88,6 +88,12 @@ def split_seismograms(seis, index: BatchIndex):
     return [seis[index.rec_off[m]:index.rec_off[m + 1]] for m in range(len(index.rec_off) - 1)]
 
 
+def element_members(index: BatchIndex) -> np.ndarray:
+    """Member id of every element of a packed Database (for ElasticSolver.set_members)."""
+    off = np.asarray(index.elem_off)
+    return np.repeat(np.arange(len(off) - 1, dtype=np.int32), np.diff(off))
+
+
 def split_elements(arr, index: BatchIndex):
     """Per-member views of a per-element array (nspec_total, ...)."""
     return [arr[index.elem_off[m]:index.elem_off[m + 1]] for m in range(len(index.elem_off) - 1)]

@@ -570,12 +570,66 @@ extern "C" int sf2d_synchronize(sf2d_solver *S, double timeout_s) {
     if (e != cudaErrorNotReady) return fail(SF2D_ERR_CUDA, std::string("stream: ") + cudaGetErrorString(e));
     if (timeout_s > 0 &&
         std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > timeout_s)
-      return fail(SF2D_ERR_CUDA, "timeout waiting for the time loop");
+      return fail(SF2D_ERR_TIMEOUT, "the time loop did not finish within the timeout (the steps keep running)");
     std::this_thread::sleep_for(std::chrono::microseconds(50));
   }
   int status = 0;
   SF2D_CUDA(cudaMemcpy(&status, S->P.d_status, sizeof(int), cudaMemcpyDeviceToHost));
   if (status) return fail(SF2D_ERR_UNSTABLE, "wavefield blew up (NaN or |u| > 1e25)");
+  return SF2D_OK;
+}
+
+extern "C" int sf2d_set_members(sf2d_solver *S, const int *elem_member, int nmembers) {
+  if (!S || !elem_member || nmembers < 1) return fail(SF2D_ERR_INVALID, "bad arguments");
+  const sf2d::Tiling &T = S->T;
+  std::vector<int> tm(T.ntiles), sm(T.nshared, -1);
+  for (int t = 0; t < T.ntiles; ++t) {
+    const sf2d::TileInfo &ti = T.tiles[t];
+    int m = -1;
+    for (int k = 0; k < ti.nelem; ++k) {
+      const int e = T.elem_order[ti.elem_base + k];
+      const int me = elem_member[e];
+      if (me < 0 || me >= nmembers) return fail(SF2D_ERR_INVALID, "member id out of range");
+      if (m >= 0 && me != m) return fail(SF2D_ERR_INVALID, "a tile holds elements of two members");
+      m = me;
+    }
+    tm[t] = m;
+    for (int k = 0; k < ti.n_sh; ++k) {
+      const int s = T.sh_ids[ti.sh_off + k] - T.shared_begin;
+      if (sm[s] >= 0 && sm[s] != m) return fail(SF2D_ERR_INVALID, "two members share a point");
+      sm[s] = m;
+    }
+  }
+  if (!S->P.member_status) {
+    int *d_tm = nullptr, *d_sm = nullptr, *d_st = nullptr;
+    if (int rc = S->alloc(&d_tm, tm.size())) return rc;
+    if (int rc = S->alloc(&d_sm, sm.size())) return rc;
+    if (int rc = S->alloc(&d_st, static_cast<size_t>(nmembers))) return rc;
+    S->P.tile_member = d_tm;
+    S->P.shared_member = d_sm;
+    S->P.member_status = d_st;
+    S->nmembers = nmembers;
+  } else if (nmembers != S->nmembers) {
+    return fail(SF2D_ERR_INVALID, "the member count is fixed by the first sf2d_set_members");
+  }
+  SF2D_CUDA(cudaMemcpy(const_cast<int *>(S->P.tile_member), tm.data(), sizeof(int) * tm.size(), cudaMemcpyHostToDevice));
+  if (!sm.empty())
+    SF2D_CUDA(cudaMemcpy(const_cast<int *>(S->P.shared_member), sm.data(), sizeof(int) * sm.size(),
+                         cudaMemcpyHostToDevice));
+  SF2D_CUDA(cudaMemset(S->P.member_status, 0, sizeof(int) * nmembers));
+  // graphs captured before hold the old parameters
+  if (S->graph) {
+    cudaGraphExecDestroy(S->graph);
+    S->graph = nullptr;
+  }
+  return SF2D_OK;
+}
+
+extern "C" int sf2d_member_status(sf2d_solver *S, int *status) {
+  if (!S || !status) return fail(SF2D_ERR_INVALID, "bad arguments");
+  if (!S->P.member_status) return fail(SF2D_ERR_INVALID, "no members: call sf2d_set_members first");
+  SF2D_CUDA(cudaMemcpyAsync(status, S->P.member_status, sizeof(int) * S->nmembers, cudaMemcpyDeviceToHost, S->stream));
+  SF2D_CUDA(cudaStreamSynchronize(S->stream));
   return SF2D_OK;
 }
 

@@ -71,6 +71,10 @@ struct Params {
   const double *rec_h;    // 10 per receiver: hxir[5], hgammar[5]
   double *seis;           // [irec][it][2]
   int *d_step, *d_status;
+  // packed batches: the member (independent sub-mesh) of every tile and shared
+  // point, and one status word per member (1 = its field blew up, masked)
+  const int *tile_member, *shared_member;
+  int *member_status;
   int *d_step_b;          // copy of *d_step written by the tile kernel, read by the shared-point kernel
   // segment recomputation: displacement frames written after every step, frame = step - *frame_base
   float2 *frames;
@@ -377,6 +381,8 @@ __global__ void __launch_bounds__(NT, tile_min_blocks<NT, ANISO, ATTEN, KERN, PM
   if (blockIdx.x == 0 && tid == 0) *P.d_step_b = step;
   // receivers of the previous step read the old fields before any write
   if (record_prev && tid < ti.rec_n) record_receiver(P, ti.rec_off + tid, step - 1);
+  // a masked member neither reads nor writes its points from here on (uniform over the CTA)
+  if (P.tile_member && P.member_status[P.tile_member[tile0 + blockIdx.x]]) return;
   const float2 *kframe = nullptr;
   if (KERN) kframe = P.kframes + static_cast<size_t>(*P.kern_base - step) * P.nglob;
 
@@ -797,14 +803,19 @@ __global__ void __launch_bounds__(NT, tile_min_blocks<NT, ANISO, ATTEN, KERN, PM
       P.partial[sp] = acc;
     }
   }
-  if (bad) *P.d_status = 1;
+  if (bad) {
+    if (P.tile_member)
+      P.member_status[P.tile_member[tile0 + blockIdx.x]] = 1;
+    else
+      *P.d_status = 1;
+  }
 }
 
 template <bool LDDRK, bool KERN>
 __global__ void __launch_bounds__(SHARED_NT) k_elastic_shared(const Params P, int stage, int last_stage) {
   const int s = blockIdx.x * SHARED_NT + threadIdx.x;
   const int step = *P.d_step_b;
-  if (s < P.nshared) {
+  if (s < P.nshared && !(P.shared_member && P.member_status[P.shared_member[s]])) {
     const int g = P.shared_begin + s;
     float2 u = P.u[g], v = P.v[g];
     if (!LDDRK) {
@@ -854,7 +865,12 @@ __global__ void __launch_bounds__(SHARED_NT) k_elastic_shared(const Params P, in
       const float2 b = P.kframes[static_cast<size_t>(*P.kern_base - step) * P.nglob + g];
       P.rho_kl_glob[g] = P.rho_kl_glob[g] + (a.x * b.x + a.y * b.y);
     }
-    if (!(fabsf(u.x) < 1e25f && fabsf(u.y) < 1e25f)) *P.d_status = 1;
+    if (!(fabsf(u.x) < 1e25f && fabsf(u.y) < 1e25f)) {
+      if (P.shared_member)
+        P.member_status[P.shared_member[s]] = 1;
+      else
+        *P.d_status = 1;
+    }
   }
   if (last_stage && blockIdx.x == 0 && threadIdx.x == 0) *P.d_step = step + 1;
 }

@@ -132,6 +132,7 @@ struct sf2d_solver {
   int nt = 256;  // threads per CTA of the tile kernel
   int pml_nt = 256, pml_max_q = 0, pml_max_local = 0;  // the CPML tiles' kernel
   int late_tile0 = 0;  // tiles [late_tile0, pml_tile0) touch points another domain uses
+  int nmembers = 0;    // members of a packed batch (sf2d_set_members), 0 = none
   int priority = 0;    // of the solver's streams (0: the default, lowest)
 
   template <typename T_>

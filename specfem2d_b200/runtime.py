@@ -22,6 +22,7 @@ SF2D_ERR_INVALID = -1
 SF2D_ERR_CUDA = -2
 SF2D_ERR_OOM = -3
 SF2D_ERR_UNSTABLE = -4
+SF2D_ERR_TIMEOUT = -5
 
 
 class SF2DError(RuntimeError):
@@ -32,6 +33,10 @@ class SF2DError(RuntimeError):
 
 class UnstableError(SF2DError):
     pass
+
+
+class SolverTimeout(SF2DError):
+    """synchronize() gave up waiting; the queued steps keep running."""
 
 
 class ElasticDesc(ctypes.Structure):
@@ -100,6 +105,8 @@ def load_library(path: str = LIB):
         "sf2d_fwi_forward": [vp, _d],
         "sf2d_fwi_backward": [vp, _f, _f, _f, _f],
         "sf2d_fwi_adjoint_seismograms": [vp, _d],
+        "sf2d_set_members": [vp, _i, ctypes.c_int],
+        "sf2d_member_status": [vp, _i],
         "sf2d_fwi_destroy": [vp],
         "sf2d_member_norms_noalloc": [vp, ctypes.POINTER(ctypes.c_int64), ctypes.c_int, _f, vp],
     }
@@ -140,6 +147,8 @@ def _check(rc):
     msg = load_library().sf2d_last_error().decode(errors="replace")
     if rc == SF2D_ERR_UNSTABLE:
         raise UnstableError(rc, msg)
+    if rc == SF2D_ERR_TIMEOUT:
+        raise SolverTimeout(rc, msg)
     raise SF2DError(rc, msg)
 
 
@@ -356,6 +365,19 @@ class ElasticSolver:
 
     def synchronize(self, timeout_s: float = 0.0):
         _check(self._lib.sf2d_synchronize(self._h, float(timeout_s)))
+
+    def set_members(self, elem_member):
+        """Name the member (independent sub-mesh) of every element of a packed
+        batch: a member whose field blows up is then masked and the others run on."""
+        m = np.ascontiguousarray(np.asarray(elem_member, dtype=np.int32))
+        self.nmembers = int(m.max()) + 1
+        _check(self._lib.sf2d_set_members(self._h, m.ctypes.data_as(_i), self.nmembers))
+
+    def member_status(self) -> np.ndarray:
+        """Per member: 0 running, 1 masked (its field blew up)."""
+        st = np.zeros(self.nmembers, dtype=np.int32)
+        _check(self._lib.sf2d_member_status(self._h, st.ctypes.data_as(_i)))
+        return st
 
     def copy_seismograms(self, it0: int, nstep: int, out=None):
         if out is None:

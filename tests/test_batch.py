@@ -71,3 +71,57 @@ def test_batched_gradient_matches_members():
         s32 = sum(r[k].astype(np.float64) for r in ref32)
         assert rel_l2(gsum, s64) < 1.5 * rel_l2(s32, s64)
     assert abs(chi - sum(r[0] for r in ref32)) / chi < 1e-4
+
+
+@pytest.mark.gpu
+def test_a_failed_member_is_masked_and_the_others_run_on():
+    """Failure injected on the host: after 200 steps one member's displacement is
+    set to NaN.  With members declared, that member is masked (status 1), the run
+    does not fail, and the other members' traces are bit-identical to a run
+    without the fault.  Without members the same fault fails the whole run, as
+    the reference's check_stability does (check_stability.F90:95-98)."""
+    from specfem2d_b200.runtime import ElasticSolver, UnstableError
+
+    c, db, shots = _members()
+    packed, idx = batch.pack(shots)
+    members = batch.element_members(idx)
+    go, ro = idx.glob_off, idx.rec_off
+
+    def run(declare, inject):
+        sol = ElasticSolver(packed)
+        if declare:
+            sol.set_members(members)
+        s1 = sol.run(200)
+        if inject:
+            u, v, a = sol.get_fields()
+            u[go[1]:go[2]] = np.nan
+            sol.set_fields(u, v, a)
+        s2 = sol.run(packed.nstep - 200)
+        st = sol.member_status() if declare else None
+        sol.close()
+        return np.concatenate([s1, s2], axis=1), st
+
+    ref, st0 = run(True, False)
+    assert list(st0) == [0, 0, 0]
+    got, st = run(True, True)
+    assert list(st) == [0, 1, 0]
+    for m in (0, 2):
+        assert np.array_equal(got[ro[m]:ro[m + 1]], ref[ro[m]:ro[m + 1]])
+    with pytest.raises(UnstableError):
+        run(False, True)
+
+
+@pytest.mark.gpu
+def test_synchronize_gives_up_with_a_timeout_status():
+    """A wait shorter than the queued work returns SF2D_ERR_TIMEOUT; the steps
+    keep running and a later wait without a limit finishes them."""
+    from specfem2d_b200.runtime import ElasticSolver, SolverTimeout
+
+    c, db, shots = _members()
+    sol = ElasticSolver(db)
+    sol.enqueue(db.nstep)
+    with pytest.raises(SolverTimeout):
+        sol.synchronize(1e-5)
+    sol.synchronize(0.0)
+    assert sol.step_index() == db.nstep
+    sol.close()
