@@ -311,7 +311,7 @@ def fwi_members(n_models: int, nstep: int, which: str = "first"):
     return models
 
 
-def measure_fwi(args, all_models, nstep, world, rank):
+def measure_fwi(args, all_models, nstep, world, rank, sum_shots=False):
     """Seconds per misfit gradient per model: plain (one model per run) and
     batched (the models packed into meshes of --batch members, one launch per
     step for all of them), both through sf2d_fwi_* with the traces and
@@ -364,6 +364,20 @@ def measure_fwi(args, all_models, nstep, world, rank):
                 ref = plain_k[m][c].astype(np.float64)
                 num += float(np.sum((part.astype(np.float64) - ref) ** 2))
                 den += float(np.sum(ref ** 2))
+    summed = None
+    if sum_shots:
+        # shots of one model: the gradient of the summed misfit is the sum of the
+        # shots' kernels, added on each rank and then over the ranks (NCCL)
+        local = np.zeros((3,) + tuple(all_models[0].rhostore.shape), dtype=np.float64)
+        for c in range(3):
+            for part in (bk[c] if models else []):
+                local[c] += part
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        total = sum_over_ranks(local, device="cuda")
+        t_ar = max_over_ranks(time.perf_counter() - t0, device="cuda")
+        summed = {"all_reduce_s": t_ar, "bytes": int(local.nbytes),
+                  "max_abs": [float(np.abs(total[c]).max()) for c in range(3)]}
     plain_s = max_over_ranks(plain_s, device="cuda")
     batched_s = max_over_ranks(batched_s, device="cuda")
     num, den = (float(x) for x in sum_over_ranks(np.array([num, den]), device="cuda"))
@@ -375,7 +389,7 @@ def measure_fwi(args, all_models, nstep, world, rank):
             "speedup_batched_vs_plain": plain_s / batched_s,
             "gradient_rel_l2_batched_vs_plain": (num / den) ** 0.5 if den > 0 else 0.0,
             "point_updates_per_s_batched": 3.0 * packed_nglob * nstep / batched_s,
-            "nglob_total": packed_nglob}
+            "nglob_total": packed_nglob, "summed_gradient": summed}
 
 
 def run_fwi(args, rank, world):
@@ -396,7 +410,7 @@ def run_fwi(args, rank, world):
         all_models = c4_shots(args.models, args.fwi_steps)
     else:
         all_models = fwi_members(args.models, args.fwi_steps, args.fwi_set)
-    r = measure_fwi(args, all_models, args.fwi_steps, world, rank)
+    r = measure_fwi(args, all_models, args.fwi_steps, world, rank, sum_shots=args.workload == "c4_fwi_shots")
     line = {
         "metric": "s per FWI gradient per shot", "value": r["batched_s_per_shot"], "unit": "s", "n_gpus": world,
         "steps": args.fwi_steps, "warmup": 1, "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
@@ -408,7 +422,8 @@ def run_fwi(args, rank, world):
                    "parallelism": f"models sharded over {world} GPU(s)",
                    "tile_elems": args.tile_elems, "threads_per_cta": args.threads},
         **{k: r[k] for k in ("plain_s_per_shot", "batched_s_per_shot", "speedup_batched_vs_plain",
-                             "gradient_rel_l2_batched_vs_plain", "point_updates_per_s_batched")},
+                             "gradient_rel_l2_batched_vs_plain", "point_updates_per_s_batched",
+                             "summed_gradient")},
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -434,10 +449,15 @@ def measure_forward(db, args, workload, K, W, world, dist, nstep_full=0):
 
     coupled = db.acoustic is not None
     tune = None
-    if args.autotune and not coupled:
-        from specfem2d_b200.autotune import autotune_elastic
+    if args.autotune:
+        from specfem2d_b200.autotune import autotune_coupled, autotune_elastic
 
-        (args.tile_elems, args.threads), tune = autotune_elastic(db, tiles=(48, 64, 96), threads=(256, 512))
+        if coupled:
+            (args.fluid_tile_elems, args.pml_tile_elems, args.pml_threads), tune = autotune_coupled(
+                db, args.tile_elems, args.threads)
+        else:
+            (args.tile_elems, args.threads), tune = autotune_elastic(db, tiles=(32, 48, 64), threads=(256, 512),
+                                                                     steps=10, warmup=3)
 
     def make_solver():
         if coupled:
@@ -576,6 +596,7 @@ def measure_forward(db, args, workload, K, W, world, dist, nstep_full=0):
                    "cpml_tile_elems": args.pml_tile_elems or args.tile_elems,
                    "cpml_threads_per_cta": args.pml_threads or args.threads,
                    "threads_per_cta": args.threads, "autotuned": bool(tune),
+                   "autotune_candidates": tune,
                    "ntiles": st["ntiles"], "shared_points": nsh,
                    "nspec_fluid": solver.nspec_fluid if coupled else 0,
                    "cpml_elements": {"solid": npml_el, "fluid": npml_ac},
@@ -615,7 +636,8 @@ def main():
     ap.add_argument("--fluid-threads", type=int, default=0, help="fluid CTA threads; 0 = --threads")
     ap.add_argument("--pml-tile-elems", type=int, default=16, help="solid CPML tiles; 0 = --tile-elems")
     ap.add_argument("--pml-threads", type=int, default=128, help="solid CPML CTA threads; 0 = --threads")
-    ap.add_argument("--autotune", action="store_true", help="pick tile size and threads per CTA first")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="keep the given tile options instead of tuning them first")
     ap.add_argument("--ref-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end legs (profiling runs)")
@@ -679,7 +701,16 @@ def main():
                               "tile_kernel_ms": r2["roofline"]["kernel_ms"], "e2e": r2["e2e"],
                               "clocks": r2["clocks"]}
         del c2
-        fwi = measure_fwi(args, fwi_members(24, 400, "smallest"), 400, world, rank)
+        members = fwi_members(24, 400, "smallest")
+        btune = None
+        if args.autotune:
+            from specfem2d_b200.autotune import autotune_batch
+
+            obs = [np.zeros((len(m.rec_ispec), 400, 2)) for m in members]
+            args.batch, btune = autotune_batch(members, obs, sizes=(1, 4, 8, 24), sample=24)
+        fwi = measure_fwi(args, members, 400, world, rank)
+        fwi["members_per_batch"] = args.batch or len(members)
+        fwi["autotune_candidates"] = btune
         fwi["description"] = ("the c5_fwi_models workload on its 24 smallest models (5,450-149,151 elements), "
                               "400 steps: " + FWI_WORKLOADS["c5_fwi_models"])
         line["fwi_gradient"] = fwi

@@ -118,3 +118,44 @@ def SeismogramOperator():
             return out[0], out[1], out[2], None, None, None
 
     return _Op
+
+
+def summed_shot_gradient(shots, observed, checkpoint_every: int = 200, batch_size: int = 0, gradient_fn=None):
+    """Misfit and kernels summed over the shots of one model: the gradient of
+    sum_s chi_s, as a survey inversion needs it.
+
+    `shots` are Databases of the same mesh and model that differ in their
+    sources (batch.shots_on_model); `observed` the data of each shot.  The
+    shots are split over the ranks of the process group (one GPU each), each
+    rank runs its share packed `batch_size` at a time (0 = all in one packed
+    mesh) and sums its kernels, and one all-reduce adds the ranks' sums (NCCL
+    on GPUs, gloo on CPU).  `gradient_fn(db, observed) -> (chi, synthetics,
+    rho_kl, kappa_kl, mu_kl)` defaults to l2_misfit_gradient.  Returns
+    (chi, rho_kl, kappa_kl, mu_kl), the kernels as float64 (nspec, 5, 5)."""
+    from . import batch
+    from .distributed import rank_world, shard, sum_over_ranks
+
+    if gradient_fn is None:
+        def gradient_fn(db, obs):
+            return l2_misfit_gradient(db, obs, checkpoint_every=checkpoint_every)
+    rank, world = rank_world()
+    mine = shard([s.nspec for s in shots], rank, world)
+    nspec = shots[0].nspec
+    acc = np.zeros((4, nspec, 5, 5), dtype=np.float64)  # chi in acc[0, 0, 0, 0]
+    size = batch_size if batch_size > 0 else max(1, len(mine))
+    for b0 in range(0, len(mine), size):
+        grp = [shots[k] for k in mine[b0:b0 + size]]
+        obs = [observed[k] for k in mine[b0:b0 + size]]
+        if len(grp) == 1:
+            chi, _, *kern = gradient_fn(grp[0], obs[0])
+            parts = [[k] for k in kern]
+        else:
+            packed, idx = batch.pack(grp)
+            chi, _, *kern = gradient_fn(packed, np.concatenate(obs, axis=0))
+            parts = [batch.split_elements(k, idx) for k in kern]
+        acc[0, 0, 0, 0] += chi
+        for c in range(3):
+            for p in parts[c]:
+                acc[1 + c] += p
+    total = sum_over_ranks(acc)
+    return float(total[0, 0, 0, 0]), total[1], total[2], total[3]

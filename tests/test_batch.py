@@ -125,3 +125,26 @@ def test_synchronize_gives_up_with_a_timeout_status():
     sol.synchronize(0.0)
     assert sol.step_index() == db.nstep
     sol.close()
+
+
+@pytest.mark.gpu
+def test_summed_shot_gradient_batched_equals_per_shot_sum():
+    """The survey gradient (kernels summed over the shots of one model) from one
+    packed batch equals the sum of the shots' gradients run one at a time."""
+    import oracle
+
+    from specfem2d_b200.fwi import l2_misfit_gradient, summed_shot_gradient
+
+    c, db, shots = _members()
+    truth = batch.shots_on_model(c.true_db(), [(1000.0, 1800.0), (2000.0, 1500.0), (3000.0, 1900.0)], 30.0)
+    observed = [oracle.Oracle(t, 8).run(t.nstep) for t in truth]
+    chi, rk, kk, mk = summed_shot_gradient(shots, observed, checkpoint_every=100)
+    ref = [0.0, 0.0, 0.0, 0.0]
+    for s, o in zip(shots, observed):
+        g = l2_misfit_gradient(s, o, checkpoint_every=100)
+        ref[0] += g[0]
+        for c_ in range(3):
+            ref[1 + c_] = ref[1 + c_] + g[2 + c_].astype(np.float64)
+    assert chi == pytest.approx(ref[0], rel=1e-5)
+    for a, b in zip((rk, kk, mk), ref[1:]):
+        assert rel_l2(a, b) < 1e-5

@@ -72,3 +72,62 @@ def test_single_process_helpers_pass_through():
     assert D.shard([1, 2, 3], 0, 1) == [0, 1, 2]
     with pytest.raises(ValueError):
         D.shard([1], 2, 2)
+
+
+def _grad_worker(rank, world, port, out):
+    import datetime
+    import sys
+
+    import torch.distributed as dist
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    for p in (root, os.path.join(root, "oracle"), os.path.join(root, "tests")):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        out[rank] = _survey_gradient()
+    finally:
+        dist.destroy_process_group()
+
+
+def _survey_gradient():
+    """Summed gradient of three shots on the small inversion case, computed with
+    the FP64 oracle in place of the GPU."""
+    import oracle
+
+    from fwi_case import Case
+    from specfem2d_b200 import batch
+    from specfem2d_b200.fwi import summed_shot_gradient
+
+    c = Case(nstep=300)
+    shots = batch.shots_on_model(c.start_db(), [(1000.0, 1800.0), (2000.0, 1500.0), (3000.0, 1900.0)], 30.0)
+    truth = batch.shots_on_model(c.true_db(), [(1000.0, 1800.0), (2000.0, 1500.0), (3000.0, 1900.0)], 30.0)
+    observed = [oracle.Oracle(t, 8).run(t.nstep) for t in truth]
+
+    def grad(db, obs):
+        return oracle.gradient(db, obs, checkpoint_every=100, precision=8)
+
+    chi, rk, kk, mk = summed_shot_gradient(shots, observed, gradient_fn=grad)
+    return chi, rk, kk, mk
+
+
+def test_summed_shot_gradient_over_two_gloo_ranks():
+    """The shots of one model split over two ranks, each rank's kernels summed,
+    one all-reduce: the same gradient as one process running every shot (up to
+    the order of the sums)."""
+    world = 2
+    port = _free_port()
+    with mp.Manager() as m:
+        out = m.dict()
+        mp.spawn(_grad_worker, args=(world, port, out), nprocs=world, join=True)
+        res = dict(out)
+    single = _survey_gradient()
+    for r in range(world):
+        assert res[r][0] == pytest.approx(single[0], rel=1e-12)
+        for a, b in zip(res[r][1:], single[1:]):
+            assert np.allclose(a, b, rtol=1e-12, atol=1e-12 * np.abs(b).max())
+    # every shot's kernels are in the sum: the three-shot sum is not one shot's
+    assert np.abs(single[1]).max() > 0
