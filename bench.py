@@ -18,6 +18,7 @@ Prints one JSON line on rank 0.
 from __future__ import annotations
 
 import argparse
+import copy
 import json
 import math
 import os
@@ -679,6 +680,7 @@ def main():
     K, W = args.steps, args.warmup
     full = WORKLOAD_NSTEP.get(args.workload, 0) if args.scale == 1 else 0
     db = build_workload(args.workload, max(K + W + 8, full), rank=rank, dist=dist, scale=args.scale)
+    base_args = copy.copy(args)
     res = measure_forward(db, args, args.workload, K, W, world, dist, nstep_full=full if world == 1 else 0)
     line = {"metric": "GLL point-updates/s", "value": res["value"], "unit": "point-updates/s",
             "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": res["ms_per_step"],
@@ -693,23 +695,29 @@ def main():
                                           "reference CPU solver (FP32), all host threads"}
     del db
     if world == 1 and not args.no_extras and args.scale == 1:
-        # the other configurations of the metric, as extra keys of the same line
+        # the other configurations of the metric, as extra keys of the same line,
+        # each tuned from the command line's tile options
         c2 = build_workload("c2_coupled", K + W + 8)
-        r2 = measure_forward(c2, args, "c2_coupled", K, W, world, dist)
+        r2 = measure_forward(c2, copy.copy(base_args), "c2_coupled", K, W, world, dist)
         line["c2_coupled"] = {"value": r2["value"], "unit": "point-updates/s", "ms_per_step": r2["ms_per_step"],
                               "nglob": c2.nglob, "roofline_frac": r2["roofline"]["frac"],
+                              "tiles": {k: r2["config"][k] for k in ("tile_elems", "threads_per_cta",
+                                                                      "fluid_tile_elems", "cpml_tile_elems",
+                                                                      "cpml_threads_per_cta")},
+                              "autotune_candidates": r2["config"]["autotune_candidates"],
                               "tile_kernel_ms": r2["roofline"]["kernel_ms"], "e2e": r2["e2e"],
                               "clocks": r2["clocks"]}
         del c2
         members = fwi_members(24, 400, "smallest")
+        fargs = copy.copy(base_args)
         btune = None
-        if args.autotune:
+        if fargs.autotune:
             from specfem2d_b200.autotune import autotune_batch
 
             obs = [np.zeros((len(m.rec_ispec), 400, 2)) for m in members]
-            args.batch, btune = autotune_batch(members, obs, sizes=(1, 4, 8, 24), sample=24)
-        fwi = measure_fwi(args, members, 400, world, rank)
-        fwi["members_per_batch"] = args.batch or len(members)
+            fargs.batch, btune = autotune_batch(members, obs, sizes=(1, 4, 8, 24), sample=24)
+        fwi = measure_fwi(fargs, members, 400, world, rank)
+        fwi["members_per_batch"] = fargs.batch or len(members)
         fwi["autotune_candidates"] = btune
         fwi["description"] = ("the c5_fwi_models workload on its 24 smallest models (5,450-149,151 elements), "
                               "400 steps: " + FWI_WORKLOADS["c5_fwi_models"])

@@ -233,6 +233,15 @@ int sf2d_fwi_forward(sf2d_fwi *f, double *seismograms);
  * rho_kl = -rho dt sum(a_adj . u), kappa_kl = -kappa dt sum(div div),
  * mu_kl = -2 mu dt sum(eps:eps - 1/3 div div). */
 int sf2d_fwi_backward(sf2d_fwi *f, const float *adj_src, float *rho_kl, float *kappa_kl, float *mu_kl);
+/* The approximate Hessian of the kernel run (APPROXIMATE_HESS_KL,
+ * compute_kernels.f90:749-800, elastic part): the forward sweep also keeps the
+ * forward accelerations of each segment (one more frame buffer) and the adjoint
+ * sweep sums |b_accel|^2 and accel . b_accel at every point.  Call before
+ * sf2d_fwi_forward.  sf2d_fwi_hessian then writes rhorho_el_Hessian_final1 and
+ * _final2 (nspec*25 each, [ispec][j][i]) of the last backward sweep, scaled by
+ * dt as the reference accumulates them. */
+int sf2d_fwi_enable_hessian(sf2d_fwi *f);
+int sf2d_fwi_hessian(sf2d_fwi *f, float *hess1, float *hess2);
 /* Receiver traces of the adjoint wavefield of the last sf2d_fwi_backward, in
  * the adjoint run's own time order (nrec*nstep*2 doubles, [irec][it][comp]):
  * the seismograms a kernel run writes (write_seismograms.F90:36-150 records

@@ -59,6 +59,7 @@ class OracleDb(ctypes.Structure):
 
 DISPL, VELOC, ACCEL, DISPL_LDDRK, VELOC_LDDRK, E1, E11, E13, ATT_OLD, RHO_KL, KAPPA_KL, MU_KL = range(12)
 POT, POT_DOT, POT_DOT_DOT, POT_LDDRK, POT_DOT_LDDRK = range(12, 17)
+HESS1, HESS2 = 17, 18
 
 
 def build() -> str:
@@ -87,6 +88,8 @@ def lib():
             fn.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
         _lib.sf2d_oracle_accumulate_kernels.restype = ctypes.c_int
         _lib.sf2d_oracle_accumulate_kernels.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        _lib.sf2d_oracle_accumulate_hessian.restype = ctypes.c_int
+        _lib.sf2d_oracle_accumulate_hessian.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         _lib.sf2d_oracle_set_step.restype = ctypes.c_int
         _lib.sf2d_oracle_set_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
         _lib.sf2d_oracle_destroy.restype = None
@@ -223,6 +226,8 @@ class Oracle:
             self.h = None
 
     def _size(self, which):
+        if which in (HESS1, HESS2):
+            return (self.s.nspec, 5, 5)
         if which >= POT:
             return (self.s.nglob,)
         if which <= VELOC_LDDRK:
@@ -235,6 +240,11 @@ class Oracle:
         b = np.ascontiguousarray(b_displ, dtype=self.dtype).reshape(self.s.nglob, 2)
         if lib().sf2d_oracle_accumulate_kernels(self.h, b.ctypes.data) != 0:
             raise RuntimeError("kernel accumulation failed")
+
+    def accumulate_hessian(self, b_accel):
+        b = np.ascontiguousarray(b_accel, dtype=self.dtype).reshape(self.s.nglob, 2)
+        if lib().sf2d_oracle_accumulate_hessian(self.h, b.ctypes.data) != 0:
+            raise RuntimeError("Hessian accumulation failed")
 
     def get(self, which):
         out = np.empty(self._size(which), dtype=self.dtype)
@@ -277,7 +287,7 @@ def checkpoint_fields(o):
     return {k: o.get(k) for k in names}
 
 
-def adjoint_kernels(db, adj_src, checkpoint_every=200, precision=4, nthreads=0):
+def adjoint_kernels(db, adj_src, checkpoint_every=200, precision=4, nthreads=0, hessian=False):
     """Forward run from rest with a state checkpoint every `checkpoint_every`
     steps, then, segment by segment in reverse, the forward segment is
     recomputed from its checkpoint (frames of the displacement kept) and the
@@ -285,7 +295,8 @@ def adjoint_kernels(db, adj_src, checkpoint_every=200, precision=4, nthreads=0):
     `adj_src(synthetics)` when it is a function, is advanced over it; adjoint step it is paired with forward step
     NSTEP - it + 1 (src/specfem2D/iterate_time_undoatt.F90:193-601).  Returns
     (synthetics, adjoint traces, rho_kl, kappa_kl, mu_kl) with the kernels
-    scaled as save_adjoint_kernels.f90:134-141 does."""
+    scaled as save_adjoint_kernels.f90:134-141 does; with `hessian`, the
+    approximate Hessian (hess1, hess2) of compute_kernels_Hessian follows."""
     nstep = db.nstep
     fwd = Oracle(db, precision)
     ckpts = {}
@@ -306,19 +317,25 @@ def adjoint_kernels(db, adj_src, checkpoint_every=200, precision=4, nthreads=0):
             rec.set(k, v)
         rec.it = s0
         _set_step(rec, s0)
-        frames = []
+        frames, aframes = [], []
         for _ in range(n):
             rec.run(1, nthreads)
             frames.append(rec.displ)
+            if hessian:
+                aframes.append(rec.accel)
         for k in range(n - 1, -1, -1):
             adj_seis[:, done:done + 1] = adj.run(1, nthreads)
             done += 1
             adj.accumulate_kernels(frames[k])
+            if hessian:
+                adj.accumulate_hessian(aframes[k])
     f = np.float32 if precision == 4 else np.float64
     dtf = f(db.deltat) if precision == 4 else float(db.dt)
     rho_kl = (-db.rhostore.astype(f) * dtf) * adj.get(RHO_KL)
     mu_kl = (-f(2.0) * db.mustore.astype(f) * dtf) * adj.get(MU_KL)
     kappa_kl = (-db.kappastore.astype(f) * dtf) * adj.get(KAPPA_KL)
+    if hessian:
+        return seis, adj_seis, rho_kl, kappa_kl, mu_kl, adj.get(HESS1), adj.get(HESS2)
     return seis, adj_seis, rho_kl, kappa_kl, mu_kl
 
 

@@ -279,6 +279,7 @@ struct StateBase {
   virtual int get(int which, void *out) = 0;
   virtual int set(int which, const void *in) = 0;
   virtual int accumulate(const void *b) = 0;
+  virtual int accumulate_hessian(const void *b_accel) = 0;
   virtual void set_step(int it) = 0;
 };
 
@@ -300,6 +301,7 @@ struct State : StateBase {
   std::vector<real> e1, e11, e13, e1_l, e11_l, e13_l;      // nspec*25*3
   std::vector<real> att_old;                                // nspec*25*3: dux_dxl, duz_dzl, dux_dzl+duz_dxl
   std::vector<real> rho_kl, kappa_kl, mu_kl;                // nspec*25
+  std::vector<real> hess1, hess2;                           // nspec*25 (approximate Hessian)
   std::vector<real> adj;                                    // nrec*nstep*2
   std::vector<real> contrib;
   // acoustic domain
@@ -427,6 +429,8 @@ struct State : StateBase {
     rho_kl.assign(nl, 0);
     kappa_kl.assign(nl, 0);
     mu_kl.assign(nl, 0);
+    hess1.assign(nl, 0);
+    hess2.assign(nl, 0);
     if (d.adj_src) adj = cvt<real>(d.adj_src, static_cast<size_t>(d.nrec) * d.nstep_total * 2);
     acoustic = d.ispec_is_acoustic != nullptr;
     if (acoustic) {
@@ -1238,6 +1242,27 @@ struct State : StateBase {
         }
     }
   }
+  // compute_kernels_Hessian (compute_kernels.f90:749-800), elastic part:
+  // per-point temporaries in CUSTOM_REAL, added times deltat at every element point
+  int accumulate_hessian(const void *bp) override {
+    if (!bp) return -1;
+    const real *ba = static_cast<const real *>(bp);
+    std::vector<real> t1(nglob), t2(nglob);
+    for (int g = 0; g < nglob; ++g) {
+      t1[g] = ba[2 * g] * ba[2 * g] + ba[2 * g + 1] * ba[2 * g + 1];
+      t2[g] = accel[2 * g] * ba[2 * g] + accel[2 * g + 1] * ba[2 * g + 1];
+    }
+    for (int e = 0; e < nspec; ++e) {
+      if (is_acoustic(e)) continue;
+      for (int q = 0; q < NGLL2; ++q) {
+        const size_t p = static_cast<size_t>(e) * NGLL2 + q;
+        const int g = d.ibool[p];
+        hess1[p] = hess1[p] + t1[g] * deltat;
+        hess2[p] = hess2[p] + t2[g] * deltat;
+      }
+    }
+    return 0;
+  }
   void set_step(int step) override { it = step; }
   int accumulate(const void *b) override {
     if (!b) return -1;
@@ -1259,6 +1284,8 @@ struct State : StateBase {
       case SF2D_OR_RHO_KL: return &rho_kl;
       case SF2D_OR_KAPPA_KL: return &kappa_kl;
       case SF2D_OR_MU_KL: return &mu_kl;
+      case SF2D_OR_HESS1: return &hess1;
+      case SF2D_OR_HESS2: return &hess2;
       case SF2D_OR_POT: return &pot;
       case SF2D_OR_POT_DOT: return &pot_d;
       case SF2D_OR_POT_DOT_DOT: return &pot_dd;
@@ -1330,6 +1357,10 @@ extern "C" int sf2d_oracle_set(void *h, int which, const void *in) {
 
 extern "C" int sf2d_oracle_accumulate_kernels(void *h, const void *b_displ) {
   return h ? static_cast<StateBase *>(h)->accumulate(b_displ) : -1;
+}
+
+extern "C" int sf2d_oracle_accumulate_hessian(void *h, const void *b_accel) {
+  return h ? static_cast<StateBase *>(h)->accumulate_hessian(b_accel) : -1;
 }
 
 extern "C" int sf2d_oracle_set_step(void *h, int it) {

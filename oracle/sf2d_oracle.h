@@ -111,7 +111,8 @@ enum {
   SF2D_OR_ATT_OLD = 8,                                   /* nspec*25*3: dux_dxl, duz_dzl, dux_dzl+duz_dxl of the last step */
   SF2D_OR_RHO_KL = 9, SF2D_OR_KAPPA_KL = 10, SF2D_OR_MU_KL = 11,  /* nspec*25, unscaled sums */
   SF2D_OR_POT = 12, SF2D_OR_POT_DOT = 13, SF2D_OR_POT_DOT_DOT = 14, /* nglob: chi, chi_dot, chi_dot_dot */
-  SF2D_OR_POT_LDDRK = 15, SF2D_OR_POT_DOT_LDDRK = 16
+  SF2D_OR_POT_LDDRK = 15, SF2D_OR_POT_DOT_LDDRK = 16,
+  SF2D_OR_HESS1 = 17, SF2D_OR_HESS2 = 18                          /* nspec*25: approximate Hessian sums */
 };
 
 /* Creates an oracle state (fields zero).  precision: 4 -> float, 8 -> double.
@@ -132,6 +133,12 @@ int sf2d_oracle_set(void *h, int which, const void *in);
  * state's (adjoint) displacement and acceleration against the forward
  * displacement b_displ (nglob*2, state precision): compute_kernels.f90:75-292. */
 int sf2d_oracle_accumulate_kernels(void *h, const void *b_displ);
+
+/* Adds the approximate-Hessian integrands (compute_kernels.f90:749-800,
+ * elastic): at every point |b_accel|^2 and accel . b_accel of the state's
+ * (adjoint) acceleration against the forward acceleration b_accel, times
+ * deltat, into HESS1 and HESS2 of the element points. */
+int sf2d_oracle_accumulate_hessian(void *h, const void *b_accel);
 
 /* Sets the number of steps done (the source time functions are indexed by it). */
 int sf2d_oracle_set_step(void *h, int it);

@@ -758,6 +758,7 @@ int sf2d_reset_solver(sf2d_solver *S) {
   if (P.att_state_l) SF2D_CUDA(cudaMemsetAsync(P.att_state_l, 0, sizeof(float4) * S->nq * 3, S->stream));
   if (P.kmu_kl) SF2D_CUDA(cudaMemsetAsync(P.kmu_kl, 0, sizeof(float2) * S->nq, S->stream));
   if (P.rho_kl_glob) SF2D_CUDA(cudaMemsetAsync(P.rho_kl_glob, 0, sizeof(float) * ng, S->stream));
+  if (P.hess_glob) SF2D_CUDA(cudaMemsetAsync(P.hess_glob, 0, sizeof(float2) * ng, S->stream));
   if (P.pml_rm) SF2D_CUDA(cudaMemsetAsync(P.pml_rm, 0, sizeof(float4) * S->npml_q * 3, S->stream));
   if (P.pml_rm_l) SF2D_CUDA(cudaMemsetAsync(P.pml_rm_l, 0, sizeof(float4) * S->npml_q * 3, S->stream));
   if (P.pml_vm) SF2D_CUDA(cudaMemsetAsync(P.pml_vm, 0, sizeof(float2) * S->npml_q * 9, S->stream));

@@ -22,6 +22,7 @@ struct sf2d_fwi {
   int nstep = 0, K = 0, nseg = 0, nglob = 0, nspec = 0, nrec = 0;
   float dt = 0.f;
   float2 *frames = nullptr;
+  float2 *aframes = nullptr;  // forward accelerations, with the approximate Hessian
   float2 *ckpt = nullptr;     // nseg * 3 * nglob (u, v, a)
   float4 *ckpt_att = nullptr; // nseg * 3 * nq (memory variables and old strains)
   std::vector<int> ibool;
@@ -203,6 +204,48 @@ extern "C" int sf2d_fwi_backward(sf2d_fwi *F, const float *adj_src, float *rho_k
     }
   }
   return st;
+}
+
+extern "C" int sf2d_fwi_enable_hessian(sf2d_fwi *F) {
+  if (!F) return fail(SF2D_ERR_INVALID, "null handle");
+  if (F->aframes) return SF2D_OK;
+  const size_t ng = static_cast<size_t>(F->nglob);
+  cudaError_t e = cudaMalloc(reinterpret_cast<void **>(&F->aframes), sizeof(float2) * ng * F->K);
+  if (e != cudaSuccess)
+    return fail(e == cudaErrorMemoryAllocation ? SF2D_ERR_OOM : SF2D_ERR_CUDA, "cudaMalloc (acceleration frames)");
+  F->allocs.push_back(F->aframes);
+  float2 *hess = nullptr;
+  e = cudaMalloc(reinterpret_cast<void **>(&hess), sizeof(float2) * std::max<size_t>(ng, 1));
+  if (e != cudaSuccess)
+    return fail(e == cudaErrorMemoryAllocation ? SF2D_ERR_OOM : SF2D_ERR_CUDA, "cudaMalloc (Hessian sums)");
+  F->allocs.push_back(hess);
+  F->fwd->P.aframes = F->aframes;
+  F->adj->P.kaframes = F->aframes;
+  F->adj->P.hess_glob = hess;
+  // step graphs captured before hold the old parameters
+  for (sf2d_solver *S : {F->fwd, F->adj})
+    if (S->graph) {
+      cudaGraphExecDestroy(S->graph);
+      S->graph = nullptr;
+    }
+  return SF2D_OK;
+}
+
+extern "C" int sf2d_fwi_hessian(sf2d_fwi *F, float *hess1, float *hess2) {
+  if (!F || !hess1 || !hess2) return fail(SF2D_ERR_INVALID, "null argument");
+  sf2d_solver *A = F->adj;
+  if (!A->P.hess_glob) return fail(SF2D_ERR_INVALID, "the Hessian was not enabled (sf2d_fwi_enable_hessian)");
+  SF2D_CUDA(cudaStreamSynchronize(A->stream));
+  std::vector<float2> h(F->nglob);
+  SF2D_CUDA(cudaMemcpy(h.data(), A->P.hess_glob, sizeof(float2) * h.size(), cudaMemcpyDeviceToHost));
+  const sf2d::Tiling &T = A->T;
+  const size_t nl = static_cast<size_t>(F->nspec) * 25;
+  for (size_t p = 0; p < nl; ++p) {
+    const float2 v = h[T.glob2dev[F->ibool[p]]];
+    hess1[p] = v.x * F->dt;
+    hess2[p] = v.y * F->dt;
+  }
+  return SF2D_OK;
 }
 
 extern "C" int sf2d_fwi_adjoint_seismograms(sf2d_fwi *F, double *seismograms) {

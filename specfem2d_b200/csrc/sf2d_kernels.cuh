@@ -80,8 +80,12 @@ struct Params {
   float2 *frames;
   const int *frame_base;
   int nframes, nglob;
+  // forward acceleration frames (approximate Hessian), written beside the displacement frames
+  float2 *aframes;
   // adjoint sweep with kernel accumulation: forward frame = *kern_base - step
   const float2 *kframes;
+  const float2 *kaframes;  // forward acceleration frames read by the adjoint sweep (Hessian), or null
+  float2 *hess_glob;       // per device point: sums of |b_a|^2 and a_adj . b_a (Hessian), or null
   const int *kern_base;
   float2 *kmu_kl;         // per element point (slot order): kappa and mu integrand sums
   float *rho_kl_glob;     // per device point: rho integrand sum
@@ -792,11 +796,22 @@ __global__ void __launch_bounds__(NT, tile_min_blocks<NT, ANISO, ATTEN, KERN, PM
       P.a[g] = a;
       if (P.frames) {
         const int fi = step - *P.frame_base;
-        if (fi >= 0 && fi < P.nframes) P.frames[static_cast<size_t>(fi) * P.nglob + g] = u;
+        if (fi >= 0 && fi < P.nframes) {
+          P.frames[static_cast<size_t>(fi) * P.nglob + g] = u;
+          if (P.aframes) P.aframes[static_cast<size_t>(fi) * P.nglob + g] = a;
+        }
       }
       if (KERN) {
         const float2 b = s_b[l];
         P.rho_kl_glob[g] = P.rho_kl_glob[g] + (a.x * b.x + a.y * b.y);
+        if (P.hess_glob) {
+          // compute_kernels_Hessian: |b_accel|^2 and accel . b_accel at the point
+          const float2 ba = P.kaframes[static_cast<size_t>(*P.kern_base - step) * P.nglob + g];
+          float2 h = P.hess_glob[g];
+          h.x = h.x + (ba.x * ba.x + ba.y * ba.y);
+          h.y = h.y + (a.x * ba.x + a.y * ba.y);
+          P.hess_glob[g] = h;
+        }
       }
       bad |= !(fabsf(u.x) < 1e25f && fabsf(u.y) < 1e25f);
     } else {
@@ -859,11 +874,21 @@ __global__ void __launch_bounds__(SHARED_NT) k_elastic_shared(const Params P, in
     P.a[g] = a;
     if (P.frames) {
       const int fi = step - *P.frame_base;
-      if (fi >= 0 && fi < P.nframes) P.frames[static_cast<size_t>(fi) * P.nglob + g] = u;
+      if (fi >= 0 && fi < P.nframes) {
+        P.frames[static_cast<size_t>(fi) * P.nglob + g] = u;
+        if (P.aframes) P.aframes[static_cast<size_t>(fi) * P.nglob + g] = a;
+      }
     }
     if (KERN) {
       const float2 b = P.kframes[static_cast<size_t>(*P.kern_base - step) * P.nglob + g];
       P.rho_kl_glob[g] = P.rho_kl_glob[g] + (a.x * b.x + a.y * b.y);
+      if (P.hess_glob) {
+        const float2 ba = P.kaframes[static_cast<size_t>(*P.kern_base - step) * P.nglob + g];
+        float2 h = P.hess_glob[g];
+        h.x = h.x + (ba.x * ba.x + ba.y * ba.y);
+        h.y = h.y + (a.x * ba.x + a.y * ba.y);
+        P.hess_glob[g] = h;
+      }
     }
     if (!(fabsf(u.x) < 1e25f && fabsf(u.y) < 1e25f)) {
       if (P.shared_member)

@@ -24,7 +24,9 @@ from .runtime import _check, _d, _f, build_desc, load_library
 
 
 class FWIGradient:
-    def __init__(self, db, checkpoint_every: int = 200, tile_elems: int = 32, threads_per_block: int = 256):
+    def __init__(self, db, checkpoint_every: int = 200, tile_elems: int = 32, threads_per_block: int = 256,
+                 hessian: bool = False):
+        """`hessian` also accumulates the approximate Hessian (see hessian())."""
         if int(db.time_scheme) != 1:
             raise ValueError("the gradient is implemented for the Newmark scheme")
         lib = load_library()
@@ -35,6 +37,8 @@ class FWIGradient:
         _check(lib.sf2d_fwi_create(ctypes.byref(d), rho.ctypes.data_as(_f), kap.ctypes.data_as(_f),
                                    int(checkpoint_every), ctypes.byref(h)))
         self._h, self._lib = h, lib
+        if hessian:
+            _check(lib.sf2d_fwi_enable_hessian(h))
         self.nrec, self.nstep, self.nspec = len(db.rec_ispec), db.nstep, db.nspec
         self.dt = float(db.dt)
         del keep
@@ -59,6 +63,14 @@ class FWIGradient:
         adj = np.ascontiguousarray(np.asarray(adj_src, dtype=np.float32).reshape(self.nrec, self.nstep, 2))
         out = [np.zeros((self.nspec, 5, 5), dtype=np.float32) for _ in range(3)]
         _check(self._lib.sf2d_fwi_backward(self._h, adj.ctypes.data_as(_f), *[o.ctypes.data_as(_f) for o in out]))
+        return tuple(out)
+
+    def hessian(self):
+        """rhorho_el_Hessian_final1 and _final2 (nspec, 5, 5) of the last backward():
+        the time integrals of |b_accel|^2 and of accel_adj . b_accel
+        (compute_kernels.f90:749-800)."""
+        out = [np.zeros((self.nspec, 5, 5), dtype=np.float32) for _ in range(2)]
+        _check(self._lib.sf2d_fwi_hessian(self._h, out[0].ctypes.data_as(_f), out[1].ctypes.data_as(_f)))
         return tuple(out)
 
     def adjoint_seismograms(self) -> np.ndarray:

@@ -105,6 +105,8 @@ def load_library(path: str = LIB):
         "sf2d_fwi_forward": [vp, _d],
         "sf2d_fwi_backward": [vp, _f, _f, _f, _f],
         "sf2d_fwi_adjoint_seismograms": [vp, _d],
+        "sf2d_fwi_enable_hessian": [vp],
+        "sf2d_fwi_hessian": [vp, _f, _f],
         "sf2d_set_members": [vp, _i, ctypes.c_int],
         "sf2d_member_status": [vp, _i],
         "sf2d_fwi_destroy": [vp],

@@ -128,23 +128,24 @@ def test_synchronize_gives_up_with_a_timeout_status():
 
 
 @pytest.mark.gpu
-def test_summed_shot_gradient_batched_equals_per_shot_sum():
-    """The survey gradient (kernels summed over the shots of one model) from one
-    packed batch equals the sum of the shots' gradients run one at a time."""
+def test_summed_shot_gradient_matches_the_oracle_sum():
+    """The survey gradient of summed_shot_gradient (kernels summed over the shots
+    of one model, one packed batch on the GPU) against the sum of the oracle's
+    per-shot gradients: as close to the FP64 sum as the FP32 oracle's sum is
+    (this case's residual is 0.14 % of the synthetics, so FP32 rounding of the
+    synthetics sets the agreement; see test_gradient_gpu)."""
     import oracle
 
-    from specfem2d_b200.fwi import l2_misfit_gradient, summed_shot_gradient
+    from specfem2d_b200.fwi import summed_shot_gradient
 
     c, db, shots = _members()
     truth = batch.shots_on_model(c.true_db(), [(1000.0, 1800.0), (2000.0, 1500.0), (3000.0, 1900.0)], 30.0)
     observed = [oracle.Oracle(t, 8).run(t.nstep) for t in truth]
     chi, rk, kk, mk = summed_shot_gradient(shots, observed, checkpoint_every=100)
-    ref = [0.0, 0.0, 0.0, 0.0]
-    for s, o in zip(shots, observed):
-        g = l2_misfit_gradient(s, o, checkpoint_every=100)
-        ref[0] += g[0]
-        for c_ in range(3):
-            ref[1 + c_] = ref[1 + c_] + g[2 + c_].astype(np.float64)
-    assert chi == pytest.approx(ref[0], rel=1e-5)
-    for a, b in zip((rk, kk, mk), ref[1:]):
-        assert rel_l2(a, b) < 1e-5
+    ref64 = [oracle.gradient(s, o, checkpoint_every=100, precision=8) for s, o in zip(shots, observed)]
+    ref32 = [oracle.gradient(s, o, checkpoint_every=100, precision=4) for s, o in zip(shots, observed)]
+    assert chi == pytest.approx(sum(r[0] for r in ref32), rel=1e-4)
+    for k, got in ((2, rk), (3, kk), (4, mk)):
+        s64 = sum(r[k].astype(np.float64) for r in ref64)
+        s32 = sum(r[k].astype(np.float64) for r in ref32)
+        assert rel_l2(got, s64) < 1.5 * rel_l2(s32, s64)

@@ -159,3 +159,24 @@ def test_adjoint_run_matches_ref_kernel():
                beta=d["beta"].max())
     for k, v in log["kernel_max"].items():
         assert float(got[k]) == pytest.approx(v, rel=5e-6), k
+
+
+def test_approximate_hessian_matches_oracle(case):
+    """compute_kernels_Hessian (elastic): H1 = int |b_accel|^2 dt depends on the
+    forward field only and agrees with the FP32 oracle to 1e-5; H2 = int
+    accel_adj . b_accel dt carries the adjoint field and sits in the FP32 band
+    of the FP64 oracle, like the kernels."""
+    import oracle
+
+    from specfem2d_b200.fwi import FWIGradient
+
+    c, obs, db0, _, _ = case
+    o32 = oracle.adjoint_kernels(db0, lambda s: s - obs, checkpoint_every=150, precision=4, hessian=True)
+    o64 = oracle.adjoint_kernels(db0, lambda s: s - obs, checkpoint_every=150, precision=8, hessian=True)
+    g = FWIGradient(db0, checkpoint_every=150, hessian=True)
+    syn = g.forward()
+    g.backward(syn - obs)
+    h1, h2 = g.hessian()
+    g.close()
+    assert rel_l2(h1, o32[5]) < 1e-5
+    assert rel_l2(h2, o64[6]) < 1.5 * rel_l2(o32[6], o64[6])
