@@ -249,6 +249,25 @@ int sf2d_fwi_hessian(sf2d_fwi *f, float *hess1, float *hess2);
 int sf2d_fwi_adjoint_seismograms(sf2d_fwi *f, double *seismograms);
 int sf2d_fwi_destroy(sf2d_fwi *f);
 
+/* ---- kernel smoothing (post-gradient step) ----
+ * Gaussian smoothing of per-element-point fields, as
+ * src/tomography/postprocess_sensitivity_kernels/smooth_sem.F90:63-467 does to
+ * sensitivity kernels (its GPU path: src/gpu/smooth_cuda.cu, kernels/process_smooth.cu):
+ * out_k(i) = sum_j G J_j w_j f_k(j) / sum_j G J_j w_j with
+ * G = exp(-dx^2 / (2 sigma_h^2) - dz^2 / (2 sigma_v^2)) over every element GLL
+ * point j.  x, z, jacobian, fields and out are host arrays of nspec*25 values
+ * per field ([ispec][j][i]; fields and out [field][ispec][j][i]); wgll_sq the
+ * 25 products wxgll(i) wzgll(j) [j][i].  Points farther than `cutoff` standard
+ * deviations (the ellipse (dx/sigma_h)^2 + (dz/sigma_v)^2 <= cutoff^2) are
+ * left out: their weights are below exp(-cutoff^2/2) of the largest (6: 1.5e-8).
+ * The reference's CPU program sums over every pair; its GPU kernel leaves out
+ * element pairs whose first points are farther than 3 sigma + max(sigma)/2.
+ * Sums in double.  Returns after the results are in `out`. */
+#define SF2D_SMOOTH_MAX_FIELDS 4
+int sf2d_smooth(int nspec, const float *x, const float *z, const float *jacobian, const float *wgll_sq,
+                int nfields, const float *fields, float sigma_h, float sigma_v, float cutoff, float *out,
+                void *stream);
+
 /* Host-only diagnostic, no GPU needed: builds the tiling of a mesh and checks
  * its invariants (one device id per point, local ibool consistent with
  * ibool, colours conflict-free, shared-point slots complete and in tile

@@ -360,5 +360,27 @@ def _set_step(o, it):
     lib().sf2d_oracle_set_step(o.h, it)
 
 
+def smooth(db, fields, sigma_h: float, sigma_v: float) -> np.ndarray:
+    """smooth_sem's CPU smoothing of per-element-point fields (nfields, nspec, 5, 5)
+    on the Database's mesh, float32 (all pairs: small meshes only)."""
+    fl = np.ascontiguousarray(np.asarray(fields, dtype=np.float32).reshape(-1, db.nspec, 5, 5))
+    x = np.ascontiguousarray(db.coord[db.ibool, 0], dtype=np.float32)
+    z = np.ascontiguousarray(db.coord[db.ibool, 1], dtype=np.float32)
+    jac = np.ascontiguousarray(db.jacobian, dtype=np.float32)
+    w = db.gll.wgll_dble
+    wsq = np.ascontiguousarray((w[None, :] * w[:, None]).astype(np.float32))  # [j][i] = w_i w_j
+    ib = np.ascontiguousarray(db.ibool, dtype=np.int32)
+    out = np.zeros_like(fl)
+    f = lib().sf2d_oracle_smooth
+    f.restype = ctypes.c_int
+    rc = f(db.nspec, db.nglob, ib.ctypes.data_as(_ip), x.ctypes.data_as(ctypes.c_void_p),
+           z.ctypes.data_as(ctypes.c_void_p), jac.ctypes.data_as(ctypes.c_void_p), wsq.ctypes.data_as(ctypes.c_void_p),
+           fl.shape[0], fl.ctypes.data_as(ctypes.c_void_p), ctypes.c_float(sigma_h), ctypes.c_float(sigma_v),
+           out.ctypes.data_as(ctypes.c_void_p))
+    if rc != 0:
+        raise RuntimeError("oracle smoothing failed")
+    return out
+
+
 def max_threads() -> int:
     return int(lib().sf2d_oracle_max_threads())

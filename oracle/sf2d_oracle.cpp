@@ -1359,6 +1359,62 @@ extern "C" int sf2d_oracle_accumulate_kernels(void *h, const void *b_displ) {
   return h ? static_cast<StateBase *>(h)->accumulate(b_displ) : -1;
 }
 
+// smooth_sem.F90:63-467, the CPU branch: for every global point (done once,
+// by the first element holding it, as imask does), over every element ispec2
+// in order: exp_val = exp(-sigma_h2_inv dist_h - sigma_v2_inv dist_v) (CUSTOM_REAL),
+// times jacobian * wgll_sq, summed over the 25 points with i fastest (Fortran's
+// sum) and added to tk and bk; finally tk / bk at every element point.  Target
+// elements run in parallel: a point belongs to exactly one of them.
+extern "C" int sf2d_oracle_smooth(int nspec, int nglob, const int *ibool, const float *x, const float *z,
+                                  const float *jacobian, const float *wgll_sq, int nfields, const float *fields,
+                                  float sigma_h, float sigma_v, float *out) {
+  if (nspec < 1 || nglob < 1 || !ibool || !x || !z || !jacobian || !wgll_sq || nfields < 1 || !fields || !out)
+    return -1;
+  const float sigma_h2_inv = 1.0f / (2.0f * (sigma_h * sigma_h));
+  const float sigma_v2_inv = 1.0f / (2.0f * (sigma_v * sigma_v));
+  const size_t n = static_cast<size_t>(nspec) * NGLL2;
+  std::vector<int> first(nglob, -1);
+  for (int e = 0; e < nspec; ++e)
+    for (int q = 0; q < NGLL2; ++q) {
+      const int g = ibool[static_cast<size_t>(e) * NGLL2 + q];
+      if (first[g] < 0) first[g] = e;
+    }
+  std::vector<float> tk(static_cast<size_t>(nglob) * nfields, 0.f), bk(nglob, 0.f);
+  parallel_for(nspec, default_threads(), [&](int b, int e1) {
+    float exp_val[NGLL2];
+    for (int ispec = b; ispec < e1; ++ispec)
+      for (int ispec2 = 0; ispec2 < nspec; ++ispec2) {
+        const size_t o2 = static_cast<size_t>(ispec2) * NGLL2;
+        for (int j = 0; j < NGLL; ++j)
+          for (int i = 0; i < NGLL; ++i) {
+            const size_t p = static_cast<size_t>(ispec) * NGLL2 + j * NGLL + i;
+            const int g = ibool[p];
+            if (first[g] != ispec) continue;
+            const float x0 = x[p], z0 = z[p];
+            for (int q = 0; q < NGLL2; ++q) {
+              const float dh = (x0 - x[o2 + q]) * (x0 - x[o2 + q]);
+              const float dv = (z0 - z[o2 + q]) * (z0 - z[o2 + q]);
+              exp_val[q] = std::exp(-sigma_h2_inv * dh - sigma_v2_inv * dv);
+              exp_val[q] = exp_val[q] * (jacobian[o2 + q] * wgll_sq[q]);
+            }
+            for (int k = 0; k < nfields; ++k) {
+              float sum = 0.f;
+              for (int q = 0; q < NGLL2; ++q) sum = sum + exp_val[q] * fields[static_cast<size_t>(k) * n + o2 + q];
+              tk[static_cast<size_t>(g) * nfields + k] = tk[static_cast<size_t>(g) * nfields + k] + sum;
+            }
+            float sum = 0.f;
+            for (int q = 0; q < NGLL2; ++q) sum = sum + exp_val[q];
+            bk[g] = bk[g] + sum;
+          }
+      }
+  });
+  for (size_t p = 0; p < n; ++p) {
+    const int g = ibool[p];
+    for (int k = 0; k < nfields; ++k) out[static_cast<size_t>(k) * n + p] = tk[static_cast<size_t>(g) * nfields + k] / bk[g];
+  }
+  return 0;
+}
+
 extern "C" int sf2d_oracle_accumulate_hessian(void *h, const void *b_accel) {
   return h ? static_cast<StateBase *>(h)->accumulate_hessian(b_accel) : -1;
 }

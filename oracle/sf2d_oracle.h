@@ -140,6 +140,13 @@ int sf2d_oracle_accumulate_kernels(void *h, const void *b_displ);
  * deltat, into HESS1 and HESS2 of the element points. */
 int sf2d_oracle_accumulate_hessian(void *h, const void *b_accel);
 
+/* Gaussian smoothing of per-element-point fields, the CPU loop of
+ * smooth_sem.F90:63-467 (every pair of points, no cutoff, CUSTOM_REAL = float).
+ * x, z, jacobian: nspec*25; wgll_sq: 25; fields, out: nfields*nspec*25. */
+int sf2d_oracle_smooth(int nspec, int nglob, const int *ibool, const float *x, const float *z,
+                       const float *jacobian, const float *wgll_sq, int nfields, const float *fields,
+                       float sigma_h, float sigma_v, float *out);
+
 /* Sets the number of steps done (the source time functions are indexed by it). */
 int sf2d_oracle_set_step(void *h, int it);
 

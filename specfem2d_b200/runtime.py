@@ -105,6 +105,8 @@ def load_library(path: str = LIB):
         "sf2d_fwi_forward": [vp, _d],
         "sf2d_fwi_backward": [vp, _f, _f, _f, _f],
         "sf2d_fwi_adjoint_seismograms": [vp, _d],
+        "sf2d_smooth": [ctypes.c_int, _f, _f, _f, _f, ctypes.c_int, _f, ctypes.c_float, ctypes.c_float,
+                        ctypes.c_float, _f, vp],
         "sf2d_fwi_enable_hessian": [vp],
         "sf2d_fwi_hessian": [vp, _f, _f],
         "sf2d_set_members": [vp, _i, ctypes.c_int],
@@ -182,6 +184,25 @@ def tiling_stats(db, tile_elems: int = 64):
         raise SF2DError(rc, "tiling invariant violated")
     keys = ["ntiles", "nshared", "max_local", "max_elems", "max_colours", "n_interior", "n_slots", "reserved"]
     return dict(zip(keys, [int(x) for x in out]))
+
+
+def smooth(db, fields, sigma_h: float, sigma_v: float, cutoff: float = 6.0) -> np.ndarray:
+    """Gaussian smoothing of per-element-point fields (nfields <= 4, each
+    (nspec, 5, 5)) on the GPU, as smooth_sem.F90 smooths sensitivity kernels:
+    horizontal and vertical standard deviations sigma_h, sigma_v in metres,
+    points within `cutoff` standard deviations."""
+    lib = load_library()
+    fl = np.ascontiguousarray(np.asarray(fields, dtype=np.float32).reshape(-1, db.nspec, 5, 5))
+    x = np.ascontiguousarray(db.coord[db.ibool, 0], dtype=np.float32)
+    z = np.ascontiguousarray(db.coord[db.ibool, 1], dtype=np.float32)
+    jac = np.ascontiguousarray(db.jacobian, dtype=np.float32)
+    w = db.gll.wgll_dble
+    wsq = np.ascontiguousarray((w[None, :] * w[:, None]).astype(np.float32))
+    out = np.zeros_like(fl)
+    _check(lib.sf2d_smooth(int(db.nspec), x.ctypes.data_as(_f), z.ctypes.data_as(_f), jac.ctypes.data_as(_f),
+                           wsq.ctypes.data_as(_f), fl.shape[0], fl.ctypes.data_as(_f), float(sigma_h),
+                           float(sigma_v), float(cutoff), out.ctypes.data_as(_f), None))
+    return out
 
 
 def member_norms_noalloc(field_ptr: int, offsets, stream: int = 0) -> np.ndarray:
