@@ -60,6 +60,7 @@ class OracleDb(ctypes.Structure):
 DISPL, VELOC, ACCEL, DISPL_LDDRK, VELOC_LDDRK, E1, E11, E13, ATT_OLD, RHO_KL, KAPPA_KL, MU_KL = range(12)
 POT, POT_DOT, POT_DOT_DOT, POT_LDDRK, POT_DOT_LDDRK = range(12, 17)
 HESS1, HESS2 = 17, 18
+RHO_AC_KL, KAPPA_AC_KL = 19, 20
 
 
 def build() -> str:
@@ -88,6 +89,8 @@ def lib():
             fn.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
         _lib.sf2d_oracle_accumulate_kernels.restype = ctypes.c_int
         _lib.sf2d_oracle_accumulate_kernels.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        _lib.sf2d_oracle_accumulate_kernels_acoustic.restype = ctypes.c_int
+        _lib.sf2d_oracle_accumulate_kernels_acoustic.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         _lib.sf2d_oracle_accumulate_hessian.restype = ctypes.c_int
         _lib.sf2d_oracle_accumulate_hessian.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         _lib.sf2d_oracle_set_step.restype = ctypes.c_int
@@ -226,7 +229,7 @@ class Oracle:
             self.h = None
 
     def _size(self, which):
-        if which in (HESS1, HESS2):
+        if which in (HESS1, HESS2, RHO_AC_KL, KAPPA_AC_KL):
             return (self.s.nspec, 5, 5)
         if which >= POT:
             return (self.s.nglob,)
@@ -240,6 +243,11 @@ class Oracle:
         b = np.ascontiguousarray(b_displ, dtype=self.dtype).reshape(self.s.nglob, 2)
         if lib().sf2d_oracle_accumulate_kernels(self.h, b.ctypes.data) != 0:
             raise RuntimeError("kernel accumulation failed")
+
+    def accumulate_kernels_acoustic(self, b_pot):
+        b = np.ascontiguousarray(b_pot, dtype=self.dtype).reshape(self.s.nglob)
+        if lib().sf2d_oracle_accumulate_kernels_acoustic(self.h, b.ctypes.data) != 0:
+            raise RuntimeError("fluid kernel accumulation failed")
 
     def accumulate_hessian(self, b_accel):
         b = np.ascontiguousarray(b_accel, dtype=self.dtype).reshape(self.s.nglob, 2)
@@ -284,20 +292,27 @@ def checkpoint_fields(o):
     names = [DISPL, VELOC, ACCEL]
     if o.db.atten is not None:
         names += [E1, E11, E13, ATT_OLD]
+    if getattr(o.db, "acoustic", None) is not None:
+        names += [POT, POT_DOT, POT_DOT_DOT]
     return {k: o.get(k) for k in names}
 
 
-def adjoint_kernels(db, adj_src, checkpoint_every=200, precision=4, nthreads=0, hessian=False):
+def kernels(db, adj_src, checkpoint_every=200, precision=4, nthreads=0, hessian=False):
     """Forward run from rest with a state checkpoint every `checkpoint_every`
     steps, then, segment by segment in reverse, the forward segment is
-    recomputed from its checkpoint (frames of the displacement kept) and the
-    adjoint field, driven by `adj_src` (nrec, nstep, 2) in time order, or by
-    `adj_src(synthetics)` when it is a function, is advanced over it; adjoint step it is paired with forward step
-    NSTEP - it + 1 (src/specfem2D/iterate_time_undoatt.F90:193-601).  Returns
-    (synthetics, adjoint traces, rho_kl, kappa_kl, mu_kl) with the kernels
-    scaled as save_adjoint_kernels.f90:134-141 does; with `hessian`, the
-    approximate Hessian (hess1, hess2) of compute_kernels_Hessian follows."""
+    recomputed from its checkpoint (frames of the displacement and, with fluid
+    elements, of the potential kept) and the adjoint field, driven by
+    `adj_src` (nrec, nstep, 2) in time order, or by `adj_src(synthetics)` when
+    it is a function, is advanced over it; adjoint step it is paired with
+    forward step NSTEP - it + 1 (src/specfem2D/iterate_time_undoatt.F90:193-601).
+
+    Returns a dict: ``seis`` and ``adj_seis`` (nrec, nstep, 2); the solid
+    kernels ``rho``, ``kappa``, ``mu`` scaled as save_adjoint_kernels.f90:134-141
+    does (zero in fluid elements); with fluid elements ``rho_ac`` and
+    ``kappa_ac`` (compute_kernels.f90:420-436, deltat included, zero in solid
+    elements); with `hessian` the approximate Hessian ``hess1``, ``hess2``."""
     nstep = db.nstep
+    fluid = getattr(db, "acoustic", None) is not None
     fwd = Oracle(db, precision)
     ckpts = {}
     seis = np.zeros((db.rec_ispec.size, nstep, 2))
@@ -317,26 +332,42 @@ def adjoint_kernels(db, adj_src, checkpoint_every=200, precision=4, nthreads=0, 
             rec.set(k, v)
         rec.it = s0
         _set_step(rec, s0)
-        frames, aframes = [], []
+        frames, pframes, aframes = [], [], []
         for _ in range(n):
             rec.run(1, nthreads)
             frames.append(rec.displ)
+            if fluid:
+                pframes.append(rec.get(POT))
             if hessian:
                 aframes.append(rec.accel)
         for k in range(n - 1, -1, -1):
             adj_seis[:, done:done + 1] = adj.run(1, nthreads)
             done += 1
             adj.accumulate_kernels(frames[k])
+            if fluid:
+                adj.accumulate_kernels_acoustic(pframes[k])
             if hessian:
                 adj.accumulate_hessian(aframes[k])
     f = np.float32 if precision == 4 else np.float64
     dtf = f(db.deltat) if precision == 4 else float(db.dt)
-    rho_kl = (-db.rhostore.astype(f) * dtf) * adj.get(RHO_KL)
-    mu_kl = (-f(2.0) * db.mustore.astype(f) * dtf) * adj.get(MU_KL)
-    kappa_kl = (-db.kappastore.astype(f) * dtf) * adj.get(KAPPA_KL)
+    out = {"seis": seis, "adj_seis": adj_seis,
+           "rho": (-db.rhostore.astype(f) * dtf) * adj.get(RHO_KL),
+           "mu": (-f(2.0) * db.mustore.astype(f) * dtf) * adj.get(MU_KL),
+           "kappa": (-db.kappastore.astype(f) * dtf) * adj.get(KAPPA_KL)}
+    if fluid:
+        out["rho_ac"] = adj.get(RHO_AC_KL)
+        out["kappa_ac"] = adj.get(KAPPA_AC_KL)
     if hessian:
-        return seis, adj_seis, rho_kl, kappa_kl, mu_kl, adj.get(HESS1), adj.get(HESS2)
-    return seis, adj_seis, rho_kl, kappa_kl, mu_kl
+        out["hess1"], out["hess2"] = adj.get(HESS1), adj.get(HESS2)
+    return out
+
+
+def adjoint_kernels(db, adj_src, checkpoint_every=200, precision=4, nthreads=0, hessian=False):
+    """The solid part of `kernels` as a tuple: (synthetics, adjoint traces,
+    rho_kl, kappa_kl, mu_kl), then hess1, hess2 with `hessian`."""
+    k = kernels(db, adj_src, checkpoint_every, precision, nthreads, hessian)
+    t = (k["seis"], k["adj_seis"], k["rho"], k["kappa"], k["mu"])
+    return t + (k["hess1"], k["hess2"]) if hessian else t
 
 
 def gradient(db, observed, checkpoint_every=200, precision=4, nthreads=0):

@@ -280,6 +280,7 @@ struct StateBase {
   virtual int set(int which, const void *in) = 0;
   virtual int accumulate(const void *b) = 0;
   virtual int accumulate_hessian(const void *b_accel) = 0;
+  virtual int accumulate_acoustic(const void *b_pot) = 0;
   virtual void set_step(int it) = 0;
 };
 
@@ -301,6 +302,7 @@ struct State : StateBase {
   std::vector<real> e1, e11, e13, e1_l, e11_l, e13_l;      // nspec*25*3
   std::vector<real> att_old;                                // nspec*25*3: dux_dxl, duz_dzl, dux_dzl+duz_dxl
   std::vector<real> rho_kl, kappa_kl, mu_kl;                // nspec*25
+  std::vector<real> rho_ac_kl, kappa_ac_kl;                 // nspec*25 (fluid elements)
   std::vector<real> hess1, hess2;                           // nspec*25 (approximate Hessian)
   std::vector<real> adj;                                    // nrec*nstep*2
   std::vector<real> contrib;
@@ -431,6 +433,8 @@ struct State : StateBase {
     mu_kl.assign(nl, 0);
     hess1.assign(nl, 0);
     hess2.assign(nl, 0);
+    rho_ac_kl.assign(nl, 0);
+    kappa_ac_kl.assign(nl, 0);
     if (d.adj_src) adj = cvt<real>(d.adj_src, static_cast<size_t>(d.nrec) * d.nstep_total * 2);
     acoustic = d.ispec_is_acoustic != nullptr;
     if (acoustic) {
@@ -632,7 +636,10 @@ struct State : StateBase {
     }
     for (int p = 0; p < d.ncpl_ac; ++p) {
       const int g = d.cpl_ac_iglob[p];
-      real ux = displ[2 * g], uz = displ[2 * g + 1];
+      // the adjoint field takes minus the solid's acceleration of this step
+      // (compute_coupling_acoustic_el.f90:89-95, SIMULATION_TYPE 3)
+      real ux = d.adj_src ? -accel[2 * g] : displ[2 * g];
+      real uz = d.adj_src ? -accel[2 * g + 1] : displ[2 * g + 1];
       if (pml && d.pml_region[d.cpl_ac_elpt[p] / NGLL2] > 0) {
         // solid element in a PML layer (compute_coupling_acoustic_el.f90:78-140)
         const size_t q = d.cpl_ac_elpt[p];
@@ -654,7 +661,23 @@ struct State : StateBase {
       const real displ_n = ux * cpl_ac_nx[p] + uz * cpl_ac_nz[p];
       pot_dd[g] = pot_dd[g] + cpl_ac_w[p] * displ_n;
     }
-    for (int isrc = 0; isrc < d.nsrc; ++isrc) {
+    if (d.adj_src) {
+      // adjoint sources of receivers in fluid elements, time-reversed
+      // (compute_add_sources_acoustic.f90:247-290): (xir * gammar) * s, in CUSTOM_REAL
+      const int it_tmp = d.nstep_total - 1 - it;
+      for (int r = 0; r < d.nrec && it_tmp >= 0; ++r) {
+        const int e = d.rec_ispec[r];
+        if (!is_acoustic(e)) continue;
+        const real a = adj[(static_cast<size_t>(r) * d.nstep_total + it_tmp) * 2];
+        for (int j = 0; j < NGLL; ++j)
+          for (int i = 0; i < NGLL; ++i) {
+            const int g = d.ibool[static_cast<size_t>(e) * NGLL2 + j * NGLL + i];
+            const real h = static_cast<real>(d.hxir[r * NGLL + i]) * static_cast<real>(d.hgammar[r * NGLL + j]);
+            pot_dd[g] = pot_dd[g] + h * a;
+          }
+      }
+    }
+    for (int isrc = 0; isrc < d.nsrc && !d.adj_src; ++isrc) {
       const int e = d.src_ispec[isrc];
       if (!is_acoustic(e)) continue;
       real stf = 0;
@@ -969,7 +992,9 @@ struct State : StateBase {
     // fluid pressure on the solid (compute_coupling_viscoelastic_ac.f90:80-250)
     for (int p = 0; p < (acoustic ? d.ncpl_el : 0); ++p) {
       const int g = d.cpl_el_iglob[p];
-      real pressure = -pot_dd[g];
+      // the adjoint field takes the fluid's potential of this step
+      // (compute_coupling_viscoelastic_ac.f90:89-93, SIMULATION_TYPE 3)
+      real pressure = d.adj_src ? pot[g] : -pot_dd[g];
       if (pml && d.pml_region[d.cpl_el_acpt[p] / NGLL2] > 0) {
         // fluid element in a PML layer (:100-150)
         const size_t q = d.cpl_el_acpt[p];
@@ -990,6 +1015,7 @@ struct State : StateBase {
       const int it_tmp = d.nstep_total - 1 - it;
       for (int r = 0; r < d.nrec && it_tmp >= 0; ++r) {
         const int e = d.rec_ispec[r];
+        if (is_acoustic(e)) continue;
         const real ax = adj[(static_cast<size_t>(r) * d.nstep_total + it_tmp) * 2];
         const real az = adj[(static_cast<size_t>(r) * d.nstep_total + it_tmp) * 2 + 1];
         for (int j = 0; j < NGLL; ++j)
@@ -1041,11 +1067,23 @@ struct State : StateBase {
   // seismotype 1-3 interpolate grad(chi)/rho of chi, chi_dot or chi_dot_dot
   // formed in double (compute_vector_field.f90:143-207) and stored in
   // CUSTOM_REAL; seismotype 4 interpolates the pressure -chi_dot_dot (or -chi
-  // with USE_TRICK_FOR_BETTER_PRESSURE, compute_pressure.f90:542-572).
+  // with USE_TRICK_FOR_BETTER_PRESSURE, compute_pressure.f90:542-572),
+  // seismotype 6 the potential chi itself (write_seismograms.F90:149-170).
   void record_acoustic(int r, double *out) {
     const int e = d.rec_ispec[r];
     const size_t off = static_cast<size_t>(e) * NGLL2;
     double vx = 0.0, vz = 0.0;
+    if (d.seismotype == 6) {
+      for (int j = 0; j < NGLL; ++j)
+        for (int i = 0; i < NGLL; ++i) {
+          const double h = static_cast<double>(static_cast<real>(d.hxir[r * NGLL + i]) *
+                                               static_cast<real>(d.hgammar[r * NGLL + j]));
+          vx = vx + static_cast<double>(pot[d.ibool[off + j * NGLL + i]]) * h;
+        }
+      out[0] = vx;
+      out[1] = 0.0;
+      return;
+    }
     if (d.seismotype == 4) {
       const std::vector<real> &f = d.use_trick ? pot : pot_dd;
       for (int j = 0; j < NGLL; ++j)
@@ -1090,6 +1128,12 @@ struct State : StateBase {
         record_acoustic(r, &seis[(static_cast<size_t>(r) * nstep + s) * 2]);
         continue;
       }
+      if (d.seismotype == 6) {
+        // a potential receiver in a solid records nothing
+        seis[(static_cast<size_t>(r) * nstep + s) * 2] = 0.0;
+        seis[(static_cast<size_t>(r) * nstep + s) * 2 + 1] = 0.0;
+        continue;
+      }
       double vx = 0.0, vz = 0.0;
       for (int j = 0; j < NGLL; ++j)
         for (int i = 0; i < NGLL; ++i) {
@@ -1130,8 +1174,7 @@ struct State : StateBase {
           }
         });
         if (acoustic) {
-          // acoustic predictor (update_displacement_Newmark.F90:353-402), then the
-          // whole acoustic step before the elastic one (iterate_time.F90:183-196)
+          // acoustic predictor (update_displacement_Newmark.F90:353-402)
           points_for(nt, [&](int b, int e) {
             for (int g = b; g < e; ++g) {
               pot[g] = pot[g] + deltat * pot_d[g] + deltatsquareover2 * pot_dd[g];
@@ -1139,6 +1182,8 @@ struct State : StateBase {
               pot_dd[g] = 0;
             }
           });
+        }
+        auto fluid_step = [&]() {
           enforce_free_surface();
           acoustic_forces(0, nt);
           points_for(nt, [&](int b, int e) {
@@ -1148,16 +1193,23 @@ struct State : StateBase {
             }
           });
           enforce_free_surface();
-        }
-        forces(0, nt);
-        // mass matrix and corrector (compute_forces_viscoelastic_calling_routine.F90:181,
-        // update_displacement_Newmark.F90:564-589)
-        points_for(nt, [&](int b, int e) {
-          for (size_t g = 2 * static_cast<size_t>(b); g < 2 * static_cast<size_t>(e); ++g) {
-            accel[g] = accel[g] * rmass[g];
-            veloc[g] = veloc[g] + deltatover2 * accel[g];
-          }
-        });
+        };
+        auto solid_step = [&]() {
+          forces(0, nt);
+          // mass matrix and corrector (compute_forces_viscoelastic_calling_routine.F90:181,
+          // update_displacement_Newmark.F90:564-589)
+          points_for(nt, [&](int b, int e) {
+            for (size_t g = 2 * static_cast<size_t>(b); g < 2 * static_cast<size_t>(e); ++g) {
+              accel[g] = accel[g] * rmass[g];
+              veloc[g] = veloc[g] + deltatover2 * accel[g];
+            }
+          });
+        };
+        // the whole fluid step before the solid one (iterate_time.F90:270-290); an
+        // adjoint run switches the order (iterate_time.F90:300-327)
+        if (acoustic && !d.adj_src) fluid_step();
+        solid_step();
+        if (acoustic && d.adj_src) fluid_step();
       } else {
         for (int stage = 0; stage < 6; ++stage) {
           // iterate_time.F90:167-181 clears accel, then forces and the LDDRK update
@@ -1200,8 +1252,11 @@ struct State : StateBase {
 
   // compute_kernels.f90:75-292 (P-SV): strains of both fields with the mapping
   // derivatives read as double, kernel integrands accumulated in CUSTOM_REAL
+  // (elements in parallel: each writes only its own points)
   void accumulate_kernels(const real *b) {
-    for (int e = 0; e < nspec; ++e) {
+    parallel_for(nspec, nspec > 256 ? default_threads() : 1, [&](int eb, int ee) {
+    for (int e = eb; e < ee; ++e) {
+      if (is_acoustic(e)) continue;  // compute_kernels_el runs over solid elements
       const size_t off = static_cast<size_t>(e) * NGLL2;
       for (int j = 0; j < NGLL; ++j)
         for (int i = 0; i < NGLL; ++i) {
@@ -1241,6 +1296,7 @@ struct State : StateBase {
           kappa_kl[p] = kappa_kl[p] + kappa_k;
         }
     }
+    });
   }
   // compute_kernels_Hessian (compute_kernels.f90:749-800), elastic part:
   // per-point temporaries in CUSTOM_REAL, added times deltat at every element point
@@ -1261,6 +1317,43 @@ struct State : StateBase {
         hess2[p] = hess2[p] + t2[g] * deltat;
       }
     }
+    return 0;
+  }
+  // compute_kernels_ac (compute_kernels.f90:293-449), fluid elements: gradients
+  // of the adjoint and forward potentials summed in CUSTOM_REAL, mapped with the
+  // derivatives read as double and stored in CUSTOM_REAL;
+  //   rho_ac_kl += 1/rho (grad chi_adj . grad chi) deltat,
+  //   kappa_ac_kl += 1/kappa chi_adj_dot_dot chi deltat
+  int accumulate_acoustic(const void *bp) override {
+    if (!bp || !acoustic) return -1;
+    const real *b = static_cast<const real *>(bp);
+    parallel_for(nspec, nspec > 256 ? default_threads() : 1, [&](int eb, int ee) {
+    for (int e = eb; e < ee; ++e) {
+      if (!is_acoustic(e)) continue;
+      const size_t off = static_cast<size_t>(e) * NGLL2;
+      for (int j = 0; j < NGLL; ++j)
+        for (int i = 0; i < NGLL; ++i) {
+          real t1 = 0, t2 = 0, bt1 = 0, bt2 = 0;
+          for (int k = 0; k < NGLL; ++k) {
+            const int gr = d.ibool[off + j * NGLL + k], gc = d.ibool[off + k * NGLL + i];
+            t1 = t1 + pot[gr] * hprime[i][k];
+            bt1 = bt1 + b[gr] * hprime[i][k];
+            t2 = t2 + pot[gc] * hprime[j][k];
+            bt2 = bt2 + b[gc] * hprime[j][k];
+          }
+          const size_t p = off + j * NGLL + i;
+          const double xixl = xix[p], xizl = xiz[p], gammaxl = gammax[p], gammazl = gammaz[p];
+          const real ax = static_cast<real>(t1 * xixl + t2 * gammaxl);
+          const real az = static_cast<real>(t1 * xizl + t2 * gammazl);
+          const real bx = static_cast<real>(bt1 * xixl + bt2 * gammaxl);
+          const real bz = static_cast<real>(bt1 * xizl + bt2 * gammazl);
+          const int g = d.ibool[p];
+          const real dotp = ax * bx + az * bz;
+          rho_ac_kl[p] = rho_ac_kl[p] + real(1) / rho[p] * dotp * deltat;
+          kappa_ac_kl[p] = kappa_ac_kl[p] + real(1) / kappa[p] * pot_dd[g] * b[g] * deltat;
+        }
+    }
+    });
     return 0;
   }
   void set_step(int step) override { it = step; }
@@ -1286,6 +1379,8 @@ struct State : StateBase {
       case SF2D_OR_MU_KL: return &mu_kl;
       case SF2D_OR_HESS1: return &hess1;
       case SF2D_OR_HESS2: return &hess2;
+      case SF2D_OR_RHO_AC_KL: return &rho_ac_kl;
+      case SF2D_OR_KAPPA_AC_KL: return &kappa_ac_kl;
       case SF2D_OR_POT: return &pot;
       case SF2D_OR_POT_DOT: return &pot_d;
       case SF2D_OR_POT_DOT_DOT: return &pot_dd;
@@ -1314,7 +1409,9 @@ extern "C" void *sf2d_oracle_create(const sf2d_oracle_db *db, int precision) {
   if (!db || db->nspec <= 0 || db->nglob <= 0 || !db->ibool) return nullptr;
   if (db->time_scheme != 1 && db->time_scheme != 2) return nullptr;
   if (db->time_scheme == 2 && (!db->alpha_lddrk || !db->beta_lddrk)) return nullptr;
-  if (db->ispec_is_acoustic && (!db->kappastore || !db->rmass_inverse_acoustic || db->adj_src)) return nullptr;
+  if (db->ispec_is_acoustic && (!db->kappastore || !db->rmass_inverse_acoustic)) return nullptr;
+  // adjoint runs with fluid elements are restated for Newmark
+  if (db->ispec_is_acoustic && db->adj_src && db->time_scheme != 1) return nullptr;
   if (db->pml_region) {
     // CPML is restated for isotropic elements of a forward run
     if (!db->pml_K_x || !db->pml_K_z || !db->pml_d_x || !db->pml_d_z || !db->pml_alpha_x || !db->pml_alpha_z ||
@@ -1331,6 +1428,7 @@ extern "C" void *sf2d_oracle_create(const sf2d_oracle_db *db, int precision) {
     }
     if (db->ispec_is_acoustic && (!db->cpl_ac_elpt || !db->cpl_el_acpt)) return nullptr;
   }
+  if (db->seismotype < 1 || db->seismotype > 6 || db->seismotype == 5) return nullptr;
   if (db->seismotype == 4 && db->nrec > 0) {
     // pressure is recorded in acoustic elements only
     if (!db->ispec_is_acoustic) return nullptr;
@@ -1413,6 +1511,10 @@ extern "C" int sf2d_oracle_smooth(int nspec, int nglob, const int *ibool, const 
     for (int k = 0; k < nfields; ++k) out[static_cast<size_t>(k) * n + p] = tk[static_cast<size_t>(g) * nfields + k] / bk[g];
   }
   return 0;
+}
+
+extern "C" int sf2d_oracle_accumulate_kernels_acoustic(void *h, const void *b_pot) {
+  return h ? static_cast<StateBase *>(h)->accumulate_acoustic(b_pot) : -1;
 }
 
 extern "C" int sf2d_oracle_accumulate_hessian(void *h, const void *b_accel) {

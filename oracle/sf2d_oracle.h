@@ -46,7 +46,7 @@ typedef struct {
   const int *rec_ispec;
   const double *hxir, *hgammar;                           /* nrec*5 */
   double cosrot, sinrot;
-  int seismotype;                                         /* 1 displ, 2 veloc, 3 accel */
+  int seismotype;                                         /* 1 displ, 2 veloc, 3 accel, 4 pressure, 6 potential */
   double deltat, deltatover2, deltatsquareover2;
   /* anisotropy (may be NULL): per-element flag and c11,c13,c15,c33,c35,c55 */
   const int *ispec_is_anisotropic;
@@ -63,7 +63,11 @@ typedef struct {
   /* adjoint simulation (SIMULATION_TYPE = 3): when adj_src is not NULL the
    * force sources are replaced by the adjoint sources at the receivers,
    * adj_src[irec][it][comp] in time order, injected time-reversed
-   * (compute_add_sources_viscoelastic.f90:351-405) */
+   * (compute_add_sources_viscoelastic.f90:351-405; in a fluid element comp 0
+   * into chi_dot_dot, compute_add_sources_acoustic.f90:247-290).  With fluid
+   * elements (Newmark only) the solid step runs first, the solid takes the
+   * fluid potential and the fluid minus the solid acceleration as coupling
+   * terms (iterate_time.F90:298-327, compute_coupling_*.f90 SIMULATION_TYPE 3) */
   const double *adj_src;
   /* acoustic (fluid) domain, potential formulation u = grad(chi)/rho (may be
    * NULL = no acoustic element): compute_forces_viscoacoustic.f90:34-417,
@@ -112,7 +116,8 @@ enum {
   SF2D_OR_RHO_KL = 9, SF2D_OR_KAPPA_KL = 10, SF2D_OR_MU_KL = 11,  /* nspec*25, unscaled sums */
   SF2D_OR_POT = 12, SF2D_OR_POT_DOT = 13, SF2D_OR_POT_DOT_DOT = 14, /* nglob: chi, chi_dot, chi_dot_dot */
   SF2D_OR_POT_LDDRK = 15, SF2D_OR_POT_DOT_LDDRK = 16,
-  SF2D_OR_HESS1 = 17, SF2D_OR_HESS2 = 18                          /* nspec*25: approximate Hessian sums */
+  SF2D_OR_HESS1 = 17, SF2D_OR_HESS2 = 18,                         /* nspec*25: approximate Hessian sums */
+  SF2D_OR_RHO_AC_KL = 19, SF2D_OR_KAPPA_AC_KL = 20                /* nspec*25: fluid kernels, deltat included */
 };
 
 /* Creates an oracle state (fields zero).  precision: 4 -> float, 8 -> double.
@@ -133,6 +138,12 @@ int sf2d_oracle_set(void *h, int which, const void *in);
  * state's (adjoint) displacement and acceleration against the forward
  * displacement b_displ (nglob*2, state precision): compute_kernels.f90:75-292. */
 int sf2d_oracle_accumulate_kernels(void *h, const void *b_displ);
+
+/* Adds the fluid-element kernel integrands of the state's (adjoint) potential
+ * against the forward potential b_pot (nglob, state precision):
+ * compute_kernels.f90:293-449.  Solid elements are left to
+ * sf2d_oracle_accumulate_kernels. */
+int sf2d_oracle_accumulate_kernels_acoustic(void *h, const void *b_pot);
 
 /* Adds the approximate-Hessian integrands (compute_kernels.f90:749-800,
  * elastic): at every point |b_accel|^2 and accel . b_accel of the state's

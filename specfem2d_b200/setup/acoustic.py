@@ -219,7 +219,13 @@ def mass_matrix_acoustic(ibool, nglob, geo, mat, gll, is_acoustic, st_ac, newmar
 def free_surface_points(mesh, ibool, is_acoustic):
     """Global points zeroed by enforce_acoustic_free_surface: every GLL point of
     the outer edges of acoustic elements on the non-absorbing sides of the
-    structured mesh (determine_acoustic_surface.f90:50-140)."""
+    structured mesh (determine_acoustic_surface.f90:50-140), or the GLL ranges
+    of the listed edges of an external mesh (enforce_acoustic_free_surface.f90
+    over acoustic_surface)."""
+    if mesh.free_edges is not None:
+        pts = [int(ibool[e, j, i]) for (e, i0, i1, j0, j1) in mesh.free_edges if is_acoustic[e]
+               for j in range(j0, j1 + 1) for i in range(i0, i1 + 1)]
+        return np.unique(np.array(pts, dtype=np.int32)) if pts else np.zeros(0, np.int32)
     nx, nz = mesh.nx, mesh.nz
     ab, ar, at, al = mesh.absorb
     pts = []

@@ -20,11 +20,15 @@ from .solver_setup import Source, build_database
 
 def _receivers_from_par(par, top_interface):
     """Receiver lines of all receiver sets, in set order."""
+    sets = par.get("receiver_sets") or [par]
+    if top_interface is None:
+        if any(rs.get("record_at_surface_same_vertical", False) for rs in sets):
+            raise NotImplementedError("receivers moved to the surface of an external mesh")
+        top_interface = ([0.0, 1.0], [0.0, 0.0])
     xs_t, zs_t = top_interface
     t1 = (zs_t[1] - zs_t[0]) / (xs_t[1] - xs_t[0])
     tn = (zs_t[-1] - zs_t[-2]) / (xs_t[-1] - xs_t[-2])
     coefs = spline_construction(xs_t, zs_t, t1, tn)
-    sets = par.get("receiver_sets") or [par]
     out = []
     for rs in sets:
         nrec = int(rs["nrec"])
@@ -49,19 +53,42 @@ PAR_KEYS = ("NSTEP", "DT", "time_stepping_scheme", "NGNOD", "xmin", "xmax", "nx"
             "ATTENUATION_f0_REFERENCE", "NELEM_PML_THICKNESS", "receiver_sets", "USE_TRICK_FOR_BETTER_PRESSURE",
             "TOMOGRAPHY_FILE", "MODEL", "K_MIN_PML", "K_MAX_PML", "damping_change_factor_acoustic",
             "damping_change_factor_elastic", "ROTATE_PML_ACTIVATE", "PML_PARAMETER_ADJUSTMENT",
-            "initialfield")
+            "initialfield", "read_external_mesh")
+
+# Par_file keys of the external-mesh text files and the tables they fill
+EXTERNAL_MESH_FILES = (("mesh_file", "elements"), ("nodes_coords_file", "nodes"), ("materials_file", "materials"),
+                       ("free_surface_file", "free_surface"), ("absorbing_surface_file", "absorbing"))
 
 
 def config_from_data_dir(data_dir: str, par_file: str = "Par_file", source_file: str = "SOURCE") -> dict:
     """Parse Par_file, SOURCE and the interfaces file of a DATA/ directory into a plain dict."""
     par = read_par_file(os.path.join(data_dir, par_file))
     srcs = read_source_file(os.path.join(data_dir, source_file))
+    cfg = {k: par[k] for k in PAR_KEYS if k in par}
+    cfg["sources"] = srcs
+    if par.get("read_external_mesh", False):
+        from .external_mesh import read_external_mesh_files
+
+        # the file names are relative to the directory the programs run in, DATA/'s parent
+        run_dir = os.path.dirname(os.path.abspath(data_dir))
+
+        def path(key):
+            v = str(par.get(key, "dummy")).strip()
+            if not v or v == "dummy":
+                return None
+            return os.path.join(run_dir, v)
+
+        stacey = bool(par["STACEY_ABSORBING_CONDITIONS"])
+        pml = bool(par.get("PML_BOUNDARY_CONDITIONS", False))
+        cfg["external_mesh"] = read_external_mesh_files(
+            path("mesh_file"), path("nodes_coords_file"), path("materials_file"), int(par["NGNOD"]),
+            free_surface_file=path("free_surface_file"),
+            absorbing_file=path("absorbing_surface_file") if (stacey or pml) else None)
+        return cfg
     ifile = str(par["interfacesfile"]).strip()
     cand = [os.path.join(data_dir, ifile), os.path.join(data_dir, os.path.basename(ifile))]
     ipath = next(p for p in cand if os.path.exists(p))
     interfaces, nz_layer = read_interfaces_file(ipath)
-    cfg = {k: par[k] for k in PAR_KEYS if k in par}
-    cfg["sources"] = srcs
     cfg["interfaces"] = [[list(x), list(z)] for (x, z) in interfaces]
     cfg["nz_layer"] = list(nz_layer)
     return cfg
@@ -85,17 +112,37 @@ def database_from_config(cfg: dict, nstep: int | None = None, absorbing_as_stace
     route (define_external_model_from_tomo_file.f90:386-470)."""
     par = cfg
     srcs = cfg["sources"]
-    interfaces = [(list(x), list(z)) for (x, z) in cfg["interfaces"]]
-    nz_layer = list(cfg["nz_layer"])
+    interfaces = [(list(x), list(z)) for (x, z) in cfg.get("interfaces", [])]
+    nz_layer = list(cfg.get("nz_layer", []))
     absorb = (bool(par["absorbbottom"]), bool(par["absorbright"]), bool(par["absorbtop"]),
               bool(par["absorbleft"]))
     if not (bool(par["STACEY_ABSORBING_CONDITIONS"]) or bool(par.get("PML_BOUNDARY_CONDITIONS", False))):
         # without Stacey or CPML no edge absorbs: every edge is a free surface
         # (read_parameter_file.F90:1678-1687, read_parameter_file_derive_flags)
         absorb = (False, False, False, False)
-    mesh = internal_mesh(float(par["xmin"]), float(par["xmax"]), int(par["nx"]), interfaces, nz_layer,
-                         absorb=absorb, ngnod=int(par["NGNOD"]))
     mats = {m["index"]: m for m in (material_from_row(r) for r in par["materials"])}
+    if par.get("read_external_mesh", False):
+        from .external_mesh import external_mesh
+
+        if bool(par.get("PML_BOUNDARY_CONDITIONS", False)) and not absorbing_as_stacey:
+            raise NotImplementedError("CPML layers of an external mesh (absorbing_cpml_file)")
+
+        # free-surface lines are kept on isotropic fluid materials, |vs| <= TINYVAL
+        # (read_material_table.f90:179-183, read_external_mesh_files.F90:398-420)
+        fluid = [k for k, m in mats.items() if m["kind"] == 1 and abs(float(m["vs"])) <= 1e-9]
+        mesh = external_mesh(cfg["external_mesh"], int(par["NGNOD"]), fluid)
+        mat_of = np.asarray(cfg["external_mesh"]["materials"], dtype=np.int64).copy()
+    else:
+        mesh = internal_mesh(float(par["xmin"]), float(par["xmax"]), int(par["nx"]), interfaces, nz_layer,
+                             absorb=absorb, ngnod=int(par["NGNOD"]))
+        # later regions overwrite earlier ones, in the order of the table
+        mat_of = np.zeros(mesh.nspec, dtype=np.int64)
+        for (ix0, ix1, iz0, iz1, imat) in par["regions"]:
+            for iz in range(iz0, iz1 + 1):
+                mat_of[(iz - 1) * mesh.nx + ix0 - 1:(iz - 1) * mesh.nx + ix1] = imat
+    missing = sorted(set(int(k) for k in np.unique(mat_of)) - set(mats))
+    if missing:
+        raise ValueError(f"elements use materials {missing} that the material table does not define")
     rho = np.zeros((mesh.nspec, NGLL, NGLL))
     vp = np.zeros_like(rho)
     vs = np.zeros_like(rho)
@@ -104,17 +151,16 @@ def database_from_config(cfg: dict, nstep: int | None = None, absorbing_as_stace
     ckeys = ("c11", "c13", "c15", "c33", "c35", "c55")
     cstore = {k: np.zeros_like(rho) for k in ckeys}
     is_aniso = np.zeros(mesh.nspec, dtype=bool)
-    for (ix0, ix1, iz0, iz1, imat) in par["regions"]:
-        m = mats[imat]
-        for iz in range(iz0, iz1 + 1):
-            for ix in range(ix0, ix1 + 1):
-                e = (iz - 1) * mesh.nx + (ix - 1)
-                rho[e], vp[e], vs[e] = m["rho"], m["vp"], m["vs"]
-                qk[e], qm[e] = m["qkappa"], m["qmu"]
-                if m["kind"] == 2:
-                    is_aniso[e] = True
-                    for k in ckeys:
-                        cstore[k][e] = m[k]
+    for imat, m in mats.items():
+        sel = mat_of == imat
+        if not sel.any():
+            continue
+        rho[sel], vp[sel], vs[sel] = m["rho"], m["vp"], m["vs"]
+        qk[sel], qm[sel] = m["qkappa"], m["qmu"]
+        if m["kind"] == 2:
+            is_aniso[sel] = True
+            for k in ckeys:
+                cstore[k][sel] = m[k]
     tomo_mats = [k for k, m in mats.items() if m["kind"] == -1]
     external = False
     if tomo_mats:
@@ -129,13 +175,9 @@ def database_from_config(cfg: dict, nstep: int | None = None, absorbing_as_stace
             lp2m = m["rho"] * m["vp"] * m["vp"]
             mu = m["rho"] * m["vs"] * m["vs"]
             m["vp"], m["vs"] = float(np.sqrt(lp2m / m["rho"])), float(np.sqrt(mu / m["rho"]))
-        mat_of = np.zeros(mesh.nspec, dtype=np.int64)
-        for (ix0, ix1, iz0, iz1, imat) in par["regions"]:
-            for iz in range(iz0, iz1 + 1):
-                for ix in range(ix0, ix1 + 1):
-                    e = (iz - 1) * mesh.nx + (ix - 1)
-                    mat_of[e] = imat
-                    vp[e], vs[e] = mats[imat]["vp"], mats[imat]["vs"]
+        for imat, m in mats.items():
+            sel = mat_of == imat
+            vp[sel], vs[sel] = m["vp"], m["vs"]
         external = True
     atten = bool(par.get("ATTENUATION_VISCOELASTIC", False))
     sources = []
@@ -145,7 +187,7 @@ def database_from_config(cfg: dict, nstep: int | None = None, absorbing_as_stace
                               tshift=float(s["tshift"]), anglesource_deg=float(s["anglesource"]),
                               Mxx=float(s["Mxx"]), Mzz=float(s["Mzz"]), Mxz=float(s["Mxz"]),
                               factor=float(s["factor"])))
-    recs = _receivers_from_par(par, interfaces[-1])
+    recs = _receivers_from_par(par, interfaces[-1] if interfaces else None)
     n = int(par["NSTEP"]) if nstep is None else nstep
     stacey = bool(par["STACEY_ABSORBING_CONDITIONS"]) or (
         absorbing_as_stacey and bool(par.get("PML_BOUNDARY_CONDITIONS", False)))

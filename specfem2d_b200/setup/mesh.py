@@ -117,6 +117,9 @@ class Mesh:
     abs_corner: np.ndarray = None  # (nabs, 4) bool codeabs_corner
     free_top: bool = True
     absorb: tuple = (True, True, False, True)  # (bottom, right, top, left) outer edges absorbing
+    # listed acoustic free-surface edges of an external mesh: (nfree, 5) int,
+    # rows (element, imin, imax, jmin, jmax) 0-based; None on the structured mesh
+    free_edges: np.ndarray = None
 
     def __getstate__(self):
         # the node-interpolation cache is derived data: rebuilt on demand, never pickled
@@ -228,8 +231,16 @@ def _absorbing_edges(mesh: Mesh, absorb) -> None:
                 isp.append(e); typ.append(ILEFT)
     isp = np.array(isp, dtype=np.int64)
     typ = np.array(typ, dtype=np.int64)
+    corner = absorbing_corners(isp, typ)
+    mesh.abs_ispec, mesh.abs_type, mesh.abs_corner = isp, typ, corner
+
+
+def absorbing_corners(isp, typ):
+    """codeabs_corner of each absorbing entry: a bottom (top) edge of an element
+    that also lists a left or right absorbing edge skips that corner point
+    (read_mesh_databases.F90:985-1030).  Returns (nabs, 4) bool: bottom-left,
+    bottom-right, top-left, top-right."""
     corner = np.zeros((len(isp), 4), dtype=bool)
-    # read_mesh_databases.F90:985-1030
     by_elem = {}
     for k, (e, t) in enumerate(zip(isp, typ)):
         by_elem.setdefault(int(e), []).append((k, int(t)))
@@ -241,7 +252,7 @@ def _absorbing_edges(mesh: Mesh, absorb) -> None:
         if t == ITOP:
             corner[k, 2] = ILEFT in others
             corner[k, 3] = IRIGHT in others
-    mesh.abs_ispec, mesh.abs_type, mesh.abs_corner = isp, typ, corner
+    return corner
 
 
 def _shape_tables(gll: GLL, ngnod: int):

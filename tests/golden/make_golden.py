@@ -9,7 +9,8 @@ subset, SOURCE and interfaces needed to rebuild the run, plus the source and
 receiver locations the reference printed in REF_SEIS/output.log),
 ``<name>_seis.npz`` (the REF_SEIS seismogram values as float64, with the
 first time sample and the time step of the trace) and, for a tomographic
-model, ``<name>_tomo.npz`` (the gridded model the example's script writes).
+model, ``<name>_tomo.npz`` (the gridded model the example's script writes) and,
+for an external mesh, ``<name>_mesh.npz`` (the tables of its MESH/ text files).
 """
 from __future__ import annotations
 
@@ -72,6 +73,12 @@ EXAMPLES["initial_mode_lddrk"] = (
     # potential = the (2, 3) membrane mode of prepare_initial_field.F90, one receiver
     "EXAMPLES/initial_mode_LDDRK", [("S0001", "BXX"), ("S0001", "BXZ")], "Par_file", "SOURCE")
 
+EXAMPLES["gmsh_stacey_external"] = (
+    # external (Gmsh) mesh of 2942 9-node fluid elements with a circular inclusion, Stacey on
+    # three sides, a listed free surface; 11 pressure stations.  The reference ran it on 4 MPI
+    # slices (its output.log numbers elements per slice); Par_file.serial is the same run on one
+    "EXAMPLES/Gmsh_example_Stacey_MPI", [(f"S{k:04d}", "PRE") for k in range(1, 12)], "Par_file.serial", "SOURCE")
+
 # examples whose TOMOGRAPHY_FILE is written by a script of the reference
 TOMO_SCRIPTS = {"tomographic_ocean_model": "utils/createTomographyFile.py"}
 
@@ -127,13 +134,26 @@ def log_locations(path):
 def kernel_log_values(path):
     """Numbers printed by the adjoint-source tool and the kernel run in
     REF_KERNEL/output.log: the cross-correlation norm per component, the
-    adjoint sources' min/max as read by the solver, and the elastic kernels'
-    maxima (save_adjoint_kernels.f90:202-216)."""
+    adjoint sources' min/max as read by the solver, the elastic kernels'
+    maxima (save_adjoint_kernels.f90:202-216) and, after "Acoustic kernels:",
+    the fluid kernels' maxima (save_adjoint_kernels.f90:453-460)."""
     out = {"norm": [], "kernel_max": {}}
     keys = {"rho  kernel": "rho", "kappa kernel": "kappa", "mu kernel": "mu", "rho prime kernel": "rhop",
             "alpha kernel": "alpha", "beta kernel": "beta"}
+    ac_keys = {"rho kernel": "rho", "kappa kernel": "kappa", "rho prime kernel": "rhop", "alpha kernel": "alpha"}
     with open(path) as f:
+        section = "elastic"
         for ln in f:
+            if "Acoustic kernels:" in ln:
+                section = "acoustic"
+            elif "Elastic kernels:" in ln:
+                section = "elastic"
+            if section == "acoustic":
+                for k, v in ac_keys.items():
+                    m = re.search(r"maximum value of " + k + r"\s*=\s*(\S+)", ln)
+                    if m:
+                        out.setdefault("acoustic_kernel_max", {})[v] = float(m.group(1))
+                continue
             m = re.match(r"\s*Norm =\s+(\S+)", ln)
             if m:
                 out["norm"].append(float(m.group(1)))
@@ -152,14 +172,46 @@ def kernel_log_values(path):
 KERNEL_RUNS = {"tromp2005_kernel": ("EXAMPLES/Tromp2005_kernel", [("S0001", "BXX"), ("S0001", "BXZ")])}
 
 
+# kernel examples without REF_SEIS: (example dir, Par_file, station, component).  Their
+# REF_KERNEL holds the adjoint source the example's tool made from the forward trace
+# (the forward trace, zeroed after its window), the adjoint run's trace at the
+# station and the log of both runs
+KERNEL_ONLY = {"luoyang_fluid_solid_kernel": ("EXAMPLES/LuoYang_fluid_solid_kernel", "Par_file", "S0001", "POT")}
+
+
+def kernel_only(ref_root, name):
+    rel, par_file, st, comp = KERNEL_ONLY[name]
+    ex = os.path.join(ref_root, rel)
+    kdir = os.path.join(ex, "REF_KERNEL")
+    cfg = config_from_data_dir(os.path.join(ex, "DATA"), par_file, "SOURCE")
+    cfg["log_locations"] = log_locations(os.path.join(kdir, "output.log"))
+    with open(os.path.join(HERE, name + ".json"), "w") as f:
+        json.dump(cfg, f, indent=1, default=str)
+    ext = "semx" if comp == "POT" else ("semp" if comp == "PRE" else "semd")
+    adj = np.loadtxt(os.path.join(kdir, f"AA.{st}.{comp}.adj"))
+    trace = np.loadtxt(os.path.join(kdir, f"AA.{st}.{comp}.{ext}"))
+    np.savez_compressed(os.path.join(HERE, name + "_adjoint.npz"), t=adj[:, 0], adj_source=adj[:, 1],
+                        t_adjoint=trace[:, 0], adjoint_trace=trace[:, 1])
+    with open(os.path.join(HERE, name + "_adjoint.json"), "w") as f:
+        json.dump(kernel_log_values(os.path.join(kdir, "output.log")), f, indent=1)
+
+
 def main(ref_root, names=None):
     """Write the fixtures of `names` (all examples when None)."""
+    for name in KERNEL_ONLY:
+        if not names or name in names:
+            kernel_only(ref_root, name)
+            print("wrote", name)
     for name, (rel, traces, par_file, source_file) in EXAMPLES.items():
         if names and name not in names:
             continue
         ex = os.path.join(ref_root, rel)
         cfg = config_from_data_dir(os.path.join(ex, "DATA"), par_file, source_file)
         cfg["log_locations"] = log_locations(os.path.join(ex, "REF_SEIS", "output.log"))
+        ext = cfg.pop("external_mesh", None)
+        if ext is not None:
+            # the mesh files' tables, ids as in the files
+            np.savez_compressed(os.path.join(HERE, name + "_mesh.npz"), **ext)
         with open(os.path.join(HERE, name + ".json"), "w") as f:
             json.dump(cfg, f, indent=1, default=str)
         arrs = {}

@@ -13,6 +13,9 @@ def load_golden(name):
     with open(os.path.join(GOLDEN, name + ".json")) as f:
         cfg = json.load(f)
     seis = dict(np.load(os.path.join(GOLDEN, name + "_seis.npz")))
+    mesh = os.path.join(GOLDEN, name + "_mesh.npz")
+    if os.path.exists(mesh):
+        cfg["external_mesh"] = dict(np.load(mesh))
     return cfg, seis
 
 
