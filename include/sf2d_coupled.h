@@ -75,7 +75,8 @@ typedef struct {
 typedef struct {
   int nrec_total;                            /* receivers of the run (solid + fluid) */
   const int *el_rec_global;                  /* index of each solid receiver in that list */
-  int seismotype;                            /* 1-3 displacement/velocity/acceleration, 4 pressure (fluid only) */
+  int seismotype;                            /* 1-3 displacement/velocity/acceleration, 4 pressure (fluid only),
+                                                6 potential (fluid; zero in the solid) */
   int use_trick;                             /* USE_TRICK_FOR_BETTER_PRESSURE: pressure = -chi */
   double cosrot, sinrot;
   /* fluid side (compute_coupling_acoustic_el.f90): chi_dd[ac] += w * (u_pred[el] . n) */
@@ -92,6 +93,14 @@ typedef struct {
    * memory terms (compute_coupling_acoustic_el.f90:78-140,
    * compute_coupling_viscoelastic_ac.f90:105-150) */
   const int *cpl_ac_el_elpt, *cpl_el_ac_elpt;
+  /* 1: an adjoint run (SIMULATION_TYPE = 3, Newmark, no CPML): the solid step
+   * runs first and accumulates the solid kernels, the solid takes the fluid's
+   * predicted chi as its pressure term and the fluid minus the solid's new
+   * acceleration as its displacement term (iterate_time.F90:298-327,
+   * compute_coupling_viscoelastic_ac.f90:89-93, compute_coupling_acoustic_el.f90:89-95);
+   * fluid sources add (hlagrange) stf to chi_dot_dot without 1/kappa
+   * (compute_add_sources_acoustic.f90:247-290).  Used by sf2d_coupled_fwi_*. */
+  int adjoint;
 } sf2d_coupling_desc;
 
 /* A solid description with nspec = 0 makes a fluid-only run (no coupling entries,
@@ -140,6 +149,39 @@ int sf2d_coupled_solid_layout_info(sf2d_coupled *c, long long *info8);
 /* Kernel launches that sf2d_coupled_enqueue(c, nstep) issues. */
 int sf2d_coupled_launch_count(sf2d_coupled *c, int nstep, long long *launches);
 int sf2d_coupled_destroy(sf2d_coupled *c);
+
+/* Sensitivity kernels of a coupled fluid-solid mesh (the kernel run of
+ * SIMULATION_TYPE = 3 with fluid and solid elements), as sf2d_fwi_* for a
+ * solid mesh: a forward run with a state checkpoint (solid u, v, a and fluid
+ * chi, chi_dot, chi_dot_dot) every checkpoint_every steps, then an adjoint
+ * sweep that recomputes each forward segment from its checkpoint (solid
+ * displacement and fluid chi frames) while the adjoint field, driven by the
+ * time-reversed adjoint sources at the receivers, accumulates
+ *   solid: rho_kl, kappa_kl, mu_kl as sf2d_fwi_backward (compute_kernels.f90:75-292,
+ *          save_adjoint_kernels.f90:134-141), over the solid sub-mesh's elements;
+ *   fluid: rho_ac_kl = sum 1/rho grad(chi_adj) . grad(chi) dt and
+ *          kappa_ac_kl = sum 1/kappa chi_adj_dd chi dt (compute_kernels.f90:293-449),
+ *          over the fluid sub-mesh's elements.
+ * Adjoint step it is paired with forward step NSTEP - it + 1 (iterate_time_undoatt.F90).
+ * Newmark only, no CPML.  Replaces the GPU kernel run of
+ * compute_kernels_acoustic_cuda / compute_kernels_elastic_cuda
+ * (src/gpu/compute_kernels_cuda.cu) driven by iterate_time.F90. */
+typedef struct sf2d_coupled_fwi sf2d_coupled_fwi;
+/* solid_rhostore, solid_kappastore: nspec*25 of the solid sub-mesh (may be
+ * NULL for a fluid-only mesh) */
+int sf2d_coupled_fwi_create(const sf2d_elastic_desc *solid, const sf2d_acoustic_desc *fluid,
+                            const sf2d_coupling_desc *coupling, const float *solid_rhostore,
+                            const float *solid_kappastore, int checkpoint_every, sf2d_coupled_fwi **out);
+/* forward run from rest; seismograms (may be NULL): nrec_total*nstep*2 [irec][it][comp] */
+int sf2d_coupled_fwi_forward(sf2d_coupled_fwi *f, double *seismograms);
+/* adj_src: nrec_total*nstep*2 in time order ([irec][it][comp]; a fluid receiver
+ * uses comp 0).  Kernels in each sub-mesh's element order; solid arrays may be
+ * NULL for a fluid-only mesh. */
+int sf2d_coupled_fwi_backward(sf2d_coupled_fwi *f, const float *adj_src, float *rho_kl, float *kappa_kl,
+                              float *mu_kl, float *rho_ac_kl, float *kappa_ac_kl);
+/* receiver traces of the adjoint field of the last backward (nrec_total*nstep*2) */
+int sf2d_coupled_fwi_adjoint_seismograms(sf2d_coupled_fwi *f, double *seismograms);
+int sf2d_coupled_fwi_destroy(sf2d_coupled_fwi *f);
 
 #ifdef __cplusplus
 }

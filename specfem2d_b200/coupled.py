@@ -51,6 +51,7 @@ class CouplingDesc(ctypes.Structure):
         ("ncpl_el", ctypes.c_int), ("cpl_el_point", _i), ("cpl_el_ac_point", _i),
         ("cpl_el_nx", _f), ("cpl_el_nz", _f), ("cpl_el_w", _f),
         ("cpl_ac_el_elpt", _i), ("cpl_el_ac_elpt", _i),
+        ("adjoint", ctypes.c_int),
     ]
 
 
@@ -185,6 +186,74 @@ def split(db):
     return sub, fluid, cpl, dict(solid_points=gl, fluid_points=ga)
 
 
+def coupled_descs(db, tile_elems: int = 32, threads_per_block: int = 256, fluid_tile_elems: int = 0,
+                  fluid_threads_per_block: int = 0, pml_tile_elems: int = 0, pml_threads_per_block: int = 0):
+    """The C descriptions of a coupled Database: (solid desc, fluid desc,
+    coupling desc, arrays to keep alive, solid sub-Database or None, fluid
+    arrays, coupling arrays, point maps)."""
+    sub, fl, cp, maps = split(db)
+    seismotype = int(getattr(db, "seismotype", 1))
+    if sub is not None:
+        ed, keep = build_desc(sub, tile_elems, 1 if seismotype in (4, 6) else seismotype, threads_per_block,
+                              pml_tile_elems, pml_threads_per_block)
+    else:  # fluid-only mesh
+        ed, keep = time_desc(db, tile_elems, threads_per_block)
+
+    def f(a):
+        arr = np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+        keep.append(arr)
+        return arr.ctypes.data_as(_f)
+
+    def dd(a):
+        arr = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+        keep.append(arr)
+        return arr.ctypes.data_as(_d)
+
+    def i(a):
+        arr = np.ascontiguousarray(np.asarray(a, dtype=np.int32))
+        keep.append(arr)
+        return arr.ctypes.data_as(_i)
+
+    a = AcousticDesc()
+    a.nspec, a.nglob = fl["nspec"], fl["nglob"]
+    a.ibool = i(fl["ibool"])
+    a.xix, a.xiz, a.gammax, a.gammaz = f(fl["xix"]), f(fl["xiz"]), f(fl["gammax"]), f(fl["gammaz"])
+    a.jacobian, a.rhostore, a.kappastore = f(fl["jacobian"]), f(fl["rhostore"]), f(fl["kappastore"])
+    a.rmass_inverse = f(fl["rmass"])
+    a.centroid_xz = dd(fl["centroid"])
+    a.nfree, a.free_iglob = len(fl["free"]), i(fl["free"])
+    a.nstacey, a.st_iglob = len(fl["st_iglob"]), i(fl["st_iglob"])
+    a.st_w, a.st_rho_vp = f(fl["st_w"]), f(fl["st_rvp"])
+    a.nsrc, a.src_ispec = len(fl["src_ispec"]), i(fl["src_ispec"])
+    a.sourcearrays, a.stf = f(fl["sourcearrays"]), f(fl["stf"])
+    a.nrec, a.rec_ispec = len(fl["rec_ispec"]), i(fl["rec_ispec"])
+    a.hxir, a.hgammar, a.rec_global = dd(fl["hxir"]), dd(fl["hgammar"]), i(fl["rec_global"])
+    a.tile_elems = fluid_tile_elems or tile_elems
+    a.threads_per_block = fluid_threads_per_block
+    fp = fl["pml"]
+    if fp is not None:
+        a.pml_region = i(fp["region"])
+        a.pml_K_x, a.pml_K_z = dd(fp["K_x"]), dd(fp["K_z"])
+        a.pml_d_x, a.pml_d_z = dd(fp["d_x"]), dd(fp["d_z"])
+        a.pml_alpha_x, a.pml_alpha_z = dd(fp["alpha_x"]), dd(fp["alpha_z"])
+        a.npml_edge, a.pml_edge_iglob = len(fp["bnd"]), i(fp["bnd"])
+        a.pml_dt = float(fp["dt"])
+    c = CouplingDesc()
+    c.nrec_total = len(db.rec_ispec)
+    c.el_rec_global = i(cp["el_rec_global"])
+    c.seismotype, c.use_trick = seismotype, int(cp["use_trick"])
+    c.cosrot, c.sinrot = float(db.cosrot), float(db.sinrot)
+    c.ncpl_ac = len(cp["ac_point"])
+    c.cpl_ac_point, c.cpl_ac_el_point = i(cp["ac_point"]), i(cp["ac_el_point"])
+    c.cpl_ac_nx, c.cpl_ac_nz, c.cpl_ac_w = f(cp["ac_nx"]), f(cp["ac_nz"]), f(cp["ac_w"])
+    c.ncpl_el = len(cp["el_point"])
+    c.cpl_el_point, c.cpl_el_ac_point = i(cp["el_point"]), i(cp["el_ac_point"])
+    c.cpl_el_nx, c.cpl_el_nz, c.cpl_el_w = f(cp["el_nx"]), f(cp["el_nz"]), f(cp["el_w"])
+    if cp["ac_el_elpt"] is not None:
+        c.cpl_ac_el_elpt, c.cpl_el_ac_elpt = i(cp["ac_el_elpt"]), i(cp["el_ac_elpt"])
+    return ed, a, c, keep, sub, fl, cp, maps
+
+
 class CoupledSolver:
     """Device-resident coupled fluid-solid solver for one Database."""
 
@@ -192,66 +261,9 @@ class CoupledSolver:
                  fluid_threads_per_block: int = 0, pml_tile_elems: int = 0, pml_threads_per_block: int = 0):
         """Tile sizes and threads per CTA of the solid; the fluid's default to the same."""
         lib = _lib()
-        sub, fl, cp, maps = split(db)
-        seismotype = int(getattr(db, "seismotype", 1))
-        if sub is not None:
-            ed, keep = build_desc(sub, tile_elems, 1 if seismotype == 4 else seismotype, threads_per_block,
-                                  pml_tile_elems, pml_threads_per_block)
-        else:  # fluid-only mesh
-            ed, keep = time_desc(db, tile_elems, threads_per_block)
-
-        def f(a):
-            arr = np.ascontiguousarray(np.asarray(a, dtype=np.float32))
-            keep.append(arr)
-            return arr.ctypes.data_as(_f)
-
-        def dd(a):
-            arr = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
-            keep.append(arr)
-            return arr.ctypes.data_as(_d)
-
-        def i(a):
-            arr = np.ascontiguousarray(np.asarray(a, dtype=np.int32))
-            keep.append(arr)
-            return arr.ctypes.data_as(_i)
-
-        a = AcousticDesc()
-        a.nspec, a.nglob = fl["nspec"], fl["nglob"]
-        a.ibool = i(fl["ibool"])
-        a.xix, a.xiz, a.gammax, a.gammaz = f(fl["xix"]), f(fl["xiz"]), f(fl["gammax"]), f(fl["gammaz"])
-        a.jacobian, a.rhostore, a.kappastore = f(fl["jacobian"]), f(fl["rhostore"]), f(fl["kappastore"])
-        a.rmass_inverse = f(fl["rmass"])
-        a.centroid_xz = dd(fl["centroid"])
-        a.nfree, a.free_iglob = len(fl["free"]), i(fl["free"])
-        a.nstacey, a.st_iglob = len(fl["st_iglob"]), i(fl["st_iglob"])
-        a.st_w, a.st_rho_vp = f(fl["st_w"]), f(fl["st_rvp"])
-        a.nsrc, a.src_ispec = len(fl["src_ispec"]), i(fl["src_ispec"])
-        a.sourcearrays, a.stf = f(fl["sourcearrays"]), f(fl["stf"])
-        a.nrec, a.rec_ispec = len(fl["rec_ispec"]), i(fl["rec_ispec"])
-        a.hxir, a.hgammar, a.rec_global = dd(fl["hxir"]), dd(fl["hgammar"]), i(fl["rec_global"])
-        a.tile_elems = fluid_tile_elems or tile_elems
-        a.threads_per_block = fluid_threads_per_block
-        fp = fl["pml"]
-        if fp is not None:
-            a.pml_region = i(fp["region"])
-            a.pml_K_x, a.pml_K_z = dd(fp["K_x"]), dd(fp["K_z"])
-            a.pml_d_x, a.pml_d_z = dd(fp["d_x"]), dd(fp["d_z"])
-            a.pml_alpha_x, a.pml_alpha_z = dd(fp["alpha_x"]), dd(fp["alpha_z"])
-            a.npml_edge, a.pml_edge_iglob = len(fp["bnd"]), i(fp["bnd"])
-            a.pml_dt = float(fp["dt"])
-        c = CouplingDesc()
-        c.nrec_total = len(db.rec_ispec)
-        c.el_rec_global = i(cp["el_rec_global"])
-        c.seismotype, c.use_trick = seismotype, int(cp["use_trick"])
-        c.cosrot, c.sinrot = float(db.cosrot), float(db.sinrot)
-        c.ncpl_ac = len(cp["ac_point"])
-        c.cpl_ac_point, c.cpl_ac_el_point = i(cp["ac_point"]), i(cp["ac_el_point"])
-        c.cpl_ac_nx, c.cpl_ac_nz, c.cpl_ac_w = f(cp["ac_nx"]), f(cp["ac_nz"]), f(cp["ac_w"])
-        c.ncpl_el = len(cp["el_point"])
-        c.cpl_el_point, c.cpl_el_ac_point = i(cp["el_point"]), i(cp["el_ac_point"])
-        c.cpl_el_nx, c.cpl_el_nz, c.cpl_el_w = f(cp["el_nx"]), f(cp["el_nz"]), f(cp["el_w"])
-        if cp["ac_el_elpt"] is not None:
-            c.cpl_ac_el_elpt, c.cpl_el_ac_elpt = i(cp["ac_el_elpt"]), i(cp["el_ac_elpt"])
+        ed, a, c, keep, sub, fl, cp, maps = coupled_descs(db, tile_elems, threads_per_block, fluid_tile_elems,
+                                                          fluid_threads_per_block, pml_tile_elems,
+                                                          pml_threads_per_block)
         h = _vp()
         _check(lib.sf2d_coupled_create(ctypes.byref(ed), ctypes.byref(a), ctypes.byref(c), ctypes.byref(h)))
         self._h, self._lib = h, lib
@@ -360,3 +372,115 @@ class CoupledSolver:
         n = ctypes.c_longlong()
         _check(self._lib.sf2d_coupled_launch_count(self._h, nstep, ctypes.byref(n)))
         return int(n.value)
+
+
+def _fwi_lib():
+    from .runtime import ElasticDesc
+
+    lib = _lib()
+    if not getattr(lib, "_coupled_fwi_sigs", False):
+        lib.sf2d_coupled_fwi_create.argtypes = [ctypes.POINTER(ElasticDesc), ctypes.POINTER(AcousticDesc),
+                                                ctypes.POINTER(CouplingDesc), _f, _f, ctypes.c_int,
+                                                ctypes.POINTER(_vp)]
+        lib.sf2d_coupled_fwi_forward.argtypes = [_vp, _d]
+        lib.sf2d_coupled_fwi_backward.argtypes = [_vp, _f, _f, _f, _f, _f, _f]
+        lib.sf2d_coupled_fwi_adjoint_seismograms.argtypes = [_vp, _d]
+        lib.sf2d_coupled_fwi_destroy.argtypes = [_vp]
+        for n in ("create", "forward", "backward", "adjoint_seismograms", "destroy"):
+            getattr(lib, "sf2d_coupled_fwi_" + n).restype = ctypes.c_int
+        lib._coupled_fwi_sigs = True
+    return lib
+
+
+class CoupledKernels:
+    """Kernel run (SIMULATION_TYPE = 3) of a Database with fluid elements on the
+    GPU (sf2d_coupled_fwi_* of the C ABI): `forward()` runs from rest with a
+    state checkpoint every `checkpoint_every` steps and returns the receiver
+    traces; `backward(adj_src)` runs the adjoint sweep driven by the adjoint
+    sources (nrec, nstep, 2) in time order (a fluid receiver uses component 0)
+    and returns the kernels in the Database's element layout:
+
+    * ``rho``, ``kappa``, ``mu``: solid kernels scaled as save_adjoint_kernels.f90:134-141
+      (zero in fluid elements);
+    * ``rho_ac``, ``kappa_ac``: fluid kernels of compute_kernels.f90:420-436, deltat
+      included (zero in solid elements).
+
+    Newmark, Stacey or free edges (no CPML)."""
+
+    def __init__(self, db, checkpoint_every: int = 200, tile_elems: int = 32, threads_per_block: int = 256):
+        if int(db.time_scheme) != 1:
+            raise ValueError("the kernel run is implemented for the Newmark scheme")
+        if getattr(db, "pml", None) is not None:
+            raise ValueError("the kernel run is implemented without CPML layers")
+        lib = _fwi_lib()
+        ed, a, c, keep, sub, fl, cp, maps = coupled_descs(db, tile_elems, threads_per_block)
+        is_ac = np.asarray(db.acoustic["ispec"], dtype=bool)
+        self.el_e, self.ac_e = np.flatnonzero(~is_ac), np.flatnonzero(is_ac)
+        rho = kap = None
+        if sub is not None:
+            rho = np.ascontiguousarray(sub.rhostore, dtype=np.float32)
+            kap = np.ascontiguousarray(sub.kappastore, dtype=np.float32)
+            keep += [rho, kap]
+        h = _vp()
+        _check(lib.sf2d_coupled_fwi_create(ctypes.byref(ed), ctypes.byref(a), ctypes.byref(c),
+                                           None if rho is None else rho.ctypes.data_as(_f),
+                                           None if kap is None else kap.ctypes.data_as(_f),
+                                           int(checkpoint_every), ctypes.byref(h)))
+        self._h, self._lib = h, lib
+        self.nrec, self.nstep, self.nspec = len(db.rec_ispec), db.nstep, db.nspec
+        del keep
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.sf2d_coupled_fwi_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def forward(self) -> np.ndarray:
+        seis = np.zeros((self.nrec, self.nstep, 2), dtype=np.float64)
+        _check(self._lib.sf2d_coupled_fwi_forward(self._h, seis.ctypes.data_as(_d)))
+        return seis
+
+    def backward(self, adj_src) -> dict:
+        adj = np.ascontiguousarray(np.asarray(adj_src, dtype=np.float32).reshape(self.nrec, self.nstep, 2))
+        ns, nf = len(self.el_e), len(self.ac_e)
+        sol = [np.zeros((ns, 5, 5), dtype=np.float32) for _ in range(3)]
+        flu = [np.zeros((nf, 5, 5), dtype=np.float32) for _ in range(2)]
+        ptr = [None if ns == 0 else x.ctypes.data_as(_f) for x in sol] + [x.ctypes.data_as(_f) for x in flu]
+        _check(self._lib.sf2d_coupled_fwi_backward(self._h, adj.ctypes.data_as(_f), *ptr))
+        out = {}
+        for k, v in zip(("rho", "kappa", "mu"), sol):
+            full = np.zeros((self.nspec, 5, 5), dtype=np.float32)
+            full[self.el_e] = v
+            out[k] = full
+        for k, v in zip(("rho_ac", "kappa_ac"), flu):
+            full = np.zeros((self.nspec, 5, 5), dtype=np.float32)
+            full[self.ac_e] = v
+            out[k] = full
+        return out
+
+    def adjoint_seismograms(self) -> np.ndarray:
+        """Receiver traces (nrec, nstep, 2) of the adjoint field of the last backward()."""
+        seis = np.zeros((self.nrec, self.nstep, 2), dtype=np.float64)
+        _check(self._lib.sf2d_coupled_fwi_adjoint_seismograms(self._h, seis.ctypes.data_as(_d)))
+        return seis
+
+
+def coupled_kernels(db, adj_src, checkpoint_every: int = 200, **kw) -> dict:
+    """Forward traces, adjoint traces and kernels of one kernel run: a dict with
+    ``seis``, ``adj_seis`` and the kernels of CoupledKernels.backward.  `adj_src`
+    is an array (nrec, nstep, 2) or a function of the forward traces."""
+    k = CoupledKernels(db, checkpoint_every, **kw)
+    try:
+        seis = k.forward()
+        src = adj_src(seis) if callable(adj_src) else adj_src
+        out = k.backward(src)
+        out["seis"], out["adj_seis"] = seis, k.adjoint_seismograms()
+    finally:
+        k.close()
+    return out

@@ -90,6 +90,24 @@ struct AcParams {
   // fluid-side coupling entries whose solid element lies in a CPML layer have
   // cpl_src = ~k: the displacement they see is formed before this kernel (k_cpl_pml_fluid)
   const float2 *cpl_pml_u;    // per layer entry k: the displacement to apply
+  // adjoint run (SIMULATION_TYPE 3): the solid step runs first and the fluid
+  // takes minus the solid's acceleration of this step as its coupling
+  // displacement (compute_coupling_acoustic_el.f90:89-95)
+  int adjoint;
+  // segment recomputation: chi frames written after every step, frame = step - *pframe_base;
+  // npframes frames (written by a forward run, read by an adjoint run)
+  float *pframes;
+  const int *pframe_base;
+  int npframes;
+  // adjoint sweep with kernel accumulation: forward chi frame = *kp_base - step;
+  // per element point (slot order) its fluid point, rho and kappa, and the
+  // sums of 1/rho grad(chi_adj) . grad(chi) dt and 1/kappa chi_adj_dd chi dt
+  const float *kpframes;
+  const int *kp_base;
+  const int *slot_ibool;
+  const float2 *slot_rk;
+  float2 *kl_ac;
+  int nslot_q, nglob_ac;
 };
 
 // Scalar line helpers of the fluid kernel (as line_derivs / line_weighted of
@@ -177,6 +195,17 @@ __device__ __forceinline__ void record_receiver_ac(const AcParams &A, int r, int
   const double *h = A.rec_h + 10 * r;
   double vx = 0.0, vz = 0.0;
   double *out = A.seis + (static_cast<size_t>(A.rec_id[r]) * A.nstep_seis + step) * 2;
+  if (A.seismotype == 6) {
+    // the potential itself (write_seismograms.F90:149-170)
+    for (int j = 0; j < 5; ++j)
+      for (int i = 0; i < 5; ++i) {
+        const double hl = static_cast<double>(static_cast<float>(h[i]) * static_cast<float>(h[5 + j]));
+        vx += static_cast<double>(A.p[dev[j * 5 + i]]) * hl;
+      }
+    out[0] = vx;
+    out[1] = 0.0;
+    return;
+  }
   if (A.seismotype == 4) {
     const float *f = A.use_trick ? A.p : A.pdd;
     for (int j = 0; j < 5; ++j)
@@ -318,7 +347,10 @@ __global__ void __launch_bounds__(NT, PML ? 768 / NT : 1536 / NT)
       const int ge = A.cpl_src[q];
       const float4 nw = A.cpl_nw[q];
       float2 u;
-      if (ge >= 0) {
+      if (ge >= 0 && A.adjoint) {
+        const float2 a = A.a_el[ge];
+        u = make_float2(-a.x, -a.y);
+      } else if (ge >= 0) {
         u = A.u_el[ge];
         if (!LDDRK) {
           const float2 v = A.v_el[ge], a = A.a_el[ge];
@@ -637,6 +669,50 @@ __global__ void k_cpl_pml_solid(const CplPml C, const float *p, const float *pd,
 static __global__ void k_acoustic_receivers(const AcParams A) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r < A.nrec) record_receiver_ac(A, r, *A.d_step - 1);
+}
+
+// After a finished step (*d_step already advanced): chi into its frame when the
+// frame lies in [0, npframes).
+static __global__ void k_fluid_frame(const AcParams A) {
+  const int fi = (*A.d_step - 1) - *A.pframe_base;
+  if (fi < 0 || fi >= A.npframes) return;
+  float *dst = A.pframes + static_cast<size_t>(fi) * A.nglob_ac;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < A.nglob_ac; g += gridDim.x * blockDim.x) dst[g] = A.p[g];
+}
+
+// compute_kernels_ac (compute_kernels.f90:293-449; the GPU form,
+// compute_kernels_acoustic_cuda in src/gpu/compute_kernels_cuda.cu), after a
+// finished adjoint step: at every fluid element point the gradients of the
+// adjoint chi and of the forward chi of the paired frame (derivative lines in
+// FP32, the mapping applied in double and stored in FP32), and
+//   sum.x += 1/rho (grad chi_adj . grad chi) dt,  sum.y += 1/kappa chi_adj_dd chi dt.
+static __global__ void k_fluid_kernels(const AcParams A) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= A.nslot_q) return;
+  const int fi = *A.kp_base - (*A.d_step - 1);
+  if (fi < 0 || fi >= A.npframes) return;  // no paired frame: nothing accumulates
+  const float *b = A.kpframes + static_cast<size_t>(fi) * A.nglob_ac;
+  const int e0 = q - q % 25, i = q % 5, j = (q % 25) / 5;
+  float t1 = 0.f, t2 = 0.f, b1 = 0.f, b2 = 0.f;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    const int gr = A.slot_ibool[e0 + j * 5 + k], gc = A.slot_ibool[e0 + k * 5 + i];
+    t1 = t1 + A.p[gr] * A.hconst[5 * i + k];
+    b1 = b1 + b[gr] * A.hconst[5 * i + k];
+    t2 = t2 + A.p[gc] * A.hconst[5 * j + k];
+    b2 = b2 + b[gc] * A.hconst[5 * j + k];
+  }
+  const float4 gm = A.geo[q];
+  const float ax = static_cast<float>(static_cast<double>(t1) * gm.x + static_cast<double>(t2) * gm.z);
+  const float az = static_cast<float>(static_cast<double>(t1) * gm.y + static_cast<double>(t2) * gm.w);
+  const float bx = static_cast<float>(static_cast<double>(b1) * gm.x + static_cast<double>(b2) * gm.z);
+  const float bz = static_cast<float>(static_cast<double>(b1) * gm.y + static_cast<double>(b2) * gm.w);
+  const int g = A.slot_ibool[q];
+  const float2 rk = A.slot_rk[q];
+  float2 s = A.kl_ac[q];
+  s.x = s.x + 1.f / rk.x * (ax * bx + az * bz) * A.dt;
+  s.y = s.y + 1.f / rk.y * A.pdd[g] * b[g] * A.dt;
+  A.kl_ac[q] = s;
 }
 
 }  // namespace sf2d

@@ -97,6 +97,7 @@ struct sf2d_coupled {
   int nt = 256, nstage = 1, nglob = 0, nrec_total = 0, nstep = 0, steps_done = 0;
   size_t npml_q = 0;  // GLL points of the fluid CPML elements
   bool lddrk = false;
+  bool adjoint = false;  // an adjoint run: the solid step first (sf2d_coupling_desc.adjoint)
   int chunk = 32;
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
@@ -214,7 +215,26 @@ struct sf2d_coupled {
     if (rec_pending) cudaStreamWaitEvent(stream(), ev_rec_done, 0);
     rec_pending = false;
   }
+  // after a finished fluid step: its chi frame (segment recomputation) and the
+  // fluid kernel sums (adjoint sweep), when the run keeps them
+  void launch_fluid_post() {
+    if (A.pframes) sf2d::k_fluid_frame<<<std::min(1184, (nglob + 255) / 256), 256, 0, stream()>>>(A);
+    if (A.kl_ac) sf2d::k_fluid_kernels<<<(A.nslot_q + 127) / 128, 128, 0, stream()>>>(A);
+  }
   void launch_step(bool record_prev) {
+    if (adjoint) {
+      // kernel runs switch the order: the whole solid step, then the fluid step
+      // (iterate_time.F90:298-327); Newmark, no CPML, no side streams
+      if (el) {
+        el->launch_tile(record_prev, 0, 0);
+        el->launch_shared(0);
+      }
+      launch_ac_tile(record_prev, 0);
+      launch_ac_shared(0);
+      launch_ac_receivers();
+      launch_fluid_post();
+      return;
+    }
     for (int st = 0; st < nstage; ++st) {
       const bool split = el && early && el->late_tile0 > 0;
       if (split) {
@@ -227,7 +247,10 @@ struct sf2d_coupled {
       join_ac_receivers();
       launch_ac_tile(record_prev && st == 0, st);
       launch_ac_shared(st);
-      if (st == nstage - 1) launch_ac_receivers();
+      if (st == nstage - 1) {
+        launch_ac_receivers();
+        launch_fluid_post();
+      }
       launch_cpl_solid(st);
       if (el) {
         el->launch_tile(record_prev && st == 0, st, split ? el->late_tile0 : 0);
@@ -270,7 +293,8 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
   if (ad->nfree < 0 || ad->nstacey < 0 || ad->nsrc < 0 || ad->nrec < 0 || cp->ncpl_ac < 0 || cp->ncpl_el < 0)
     return fail(SF2D_ERR_INVALID, "negative count");
   if (cp->nrec_total != eld->nrec + ad->nrec) return fail(SF2D_ERR_INVALID, "receiver counts do not add up");
-  if (cp->seismotype < 1 || cp->seismotype > 4) return fail(SF2D_ERR_INVALID, "seismotype must be 1 to 4");
+  if (cp->seismotype < 1 || cp->seismotype > 6 || cp->seismotype == 5)
+    return fail(SF2D_ERR_INVALID, "seismotype must be 1 to 4 or 6");
   if (cp->seismotype == 4 && eld->nrec > 0)
     return fail(SF2D_ERR_INVALID, "pressure receivers must lie in fluid elements");
   for (int k = 0; k < ad->nrec; ++k)
@@ -298,6 +322,9 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
   for (int k = 0; k < ad->nrec; ++k)
     if (ad->rec_ispec[k] < 0 || ad->rec_ispec[k] >= ad->nspec) return fail(SF2D_ERR_INVALID, "fluid receiver element out of range");
   const bool pml_ac = ad->pml_region != nullptr, pml_el = eld->pml_region != nullptr;
+  const bool adjoint = cp->adjoint != 0;
+  if (adjoint && (pml_ac || pml_el)) return fail(SF2D_ERR_INVALID, "adjoint runs are implemented without CPML layers");
+  if (adjoint && eld->time_scheme == 2) return fail(SF2D_ERR_INVALID, "adjoint runs are implemented for Newmark");
   std::vector<int> group;
   if (pml_ac) {
     if (!ad->pml_K_x || !ad->pml_K_z || !ad->pml_d_x || !ad->pml_d_z || !ad->pml_alpha_x || !ad->pml_alpha_z ||
@@ -328,6 +355,7 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
 
   auto *C = new sf2d_coupled();
   std::unique_ptr<sf2d_coupled> guard(C);
+  C->adjoint = adjoint;
   // the solid sub-solver; its receivers are renumbered into the run's list below.
   // A solid description with nspec = 0 makes a fluid-only run: only its time
   // stepping members (nstep, deltat..., time_scheme, nstage, alpha/beta_lddrk,
@@ -349,7 +377,7 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
     SF2D_CUDA(cudaStreamCreateWithFlags(&C->own_stream, cudaStreamNonBlocking));
   } else {
     sf2d_elastic_desc e2 = *eld;
-    if (e2.seismotype == 4 || e2.seismotype == 0) e2.seismotype = 1;
+    if (e2.seismotype == 4 || e2.seismotype == 6 || e2.seismotype == 0) e2.seismotype = 1;
     // solid elements touching a coupling point get tiles of their own (late
     // tiles, after the fluid step); the others never touch a point the fluid
     // reads or a fluid value, so they run beside the fluid step
@@ -372,8 +400,10 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
         const int g = eld->ibool[static_cast<size_t>(e) * NGLL2 + q];
         if (g >= 0 && g < eld->nglob && cpl_pt[g]) late[e] = 1;
       }
-    if (int rc = sf2d_create_solver_internal(&e2, false, &C->el, late.data())) return rc;
+    // an adjoint run's solid accumulates the sensitivity kernels
+    if (int rc = sf2d_create_solver_internal(&e2, adjoint, &C->el, late.data())) return rc;
     S = C->el;
+    if (cp->seismotype == 6) S->P.seismotype = 6;  // potential receivers in the solid record zero
     C->lddrk = S->lddrk;
     C->nstage = S->nstage;
     C->nt = S->nt;
@@ -481,7 +511,10 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
         const size_t p = static_cast<size_t>(ad->src_ispec[k]) * NGLL2 + q;
         src_local.push_back(T.local_id(t, ad->ibool[p]));
         src_id.push_back(k);
-        src_sk.push_back(make_float2(ad->sourcearrays[static_cast<size_t>(k) * NGLL2 + q], ad->kappastore[p]));
+        // an adjoint source adds (xir gammar) s to chi_dot_dot, without 1/kappa
+        // (compute_add_sources_acoustic.f90:247-290): divided by 1 here
+        src_sk.push_back(make_float2(ad->sourcearrays[static_cast<size_t>(k) * NGLL2 + q],
+                                     adjoint ? 1.f : ad->kappastore[p]));
       }
     tiles[t].src_n = static_cast<int>(src_local.size()) - tiles[t].src_off;
     tiles[t].rec_off = static_cast<int>(rec_id.size());
@@ -589,11 +622,16 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
   if ((rc = C->alloc(&C->seis, nseis))) return rc;
   SF2D_CUDA(cudaMemset(C->seis, 0, sizeof(double) * std::max<size_t>(1, nseis)));
   A.seis = C->seis;
-  if ((rc = C->alloc(&C->ctr, 4))) return rc;
-  SF2D_CUDA(cudaMemset(C->ctr, 0, 4 * sizeof(int)));
+  // step, step shadow, status, -, chi frame base, kernel frame base
+  if ((rc = C->alloc(&C->ctr, 8))) return rc;
+  SF2D_CUDA(cudaMemset(C->ctr, 0, 8 * sizeof(int)));
   A.d_step = C->ctr;
   A.d_step_b = C->ctr + 1;
   A.d_status = C->ctr + 2;
+  A.pframe_base = C->ctr + 4;
+  A.kp_base = C->ctr + 5;
+  A.adjoint = adjoint ? 1 : 0;
+  A.nglob_ac = ad->nglob;
   if (S) {
     A.u_el = S->P.u;
     A.v_el = S->P.v;
@@ -639,7 +677,7 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
       SF2D_CUDA(cudaEventCreateWithFlags(&C->ev_rec_done, cudaEventDisableTiming));
     }
   }
-  if (C->el && C->el->late_tile0 > 0) {
+  if (C->el && C->el->late_tile0 > 0 && !adjoint) {
     int least = 0, greatest = 0;
     SF2D_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
     SF2D_CUDA(cudaStreamCreateWithPriority(&C->early, cudaStreamNonBlocking, least));
@@ -730,6 +768,9 @@ extern "C" int sf2d_coupled_create(const sf2d_elastic_desc *eld, const sf2d_acou
         (rc = C->upload_const(&S->P.cpl_nw, e_nw)))
       return rc;
     S->P.pdd_ac = A.pdd;
+    S->P.p_ac = A.p;
+    S->P.pd_ac = A.pd;
+    S->P.cpl_adjoint = adjoint ? 1 : 0;
   }
   SF2D_CUDA(cudaDeviceSynchronize());
   *out = guard.release();
@@ -1016,7 +1057,8 @@ extern "C" int sf2d_coupled_launch_count(sf2d_coupled *C, int nstep, long long *
                         (C->cpl_solid.n > 0);
   if (S) per_stage += (C->early ? S->tile_launches(S->late_tile0) + (S->late_tile0 > 0) : S->tile_launches(0)) + 1;
   const long long chunks = nstep / C->chunk + (nstep % C->chunk ? 1 : 0);
-  *launches = per_stage * C->nstage * nstep + (C->A.nrec > 0 ? nstep : 0) + (S && S->nrec > 0 ? chunks : 0);
+  *launches = per_stage * C->nstage * nstep + (C->A.nrec > 0 ? nstep : 0) + (S && S->nrec > 0 ? chunks : 0) +
+              ((C->A.pframes != nullptr) + (C->A.kl_ac != nullptr)) * static_cast<long long>(nstep);
   return SF2D_OK;
 }
 
@@ -1029,5 +1071,340 @@ extern "C" int sf2d_coupled_get_stream(sf2d_coupled *C, void **stream) {
 
 extern "C" int sf2d_coupled_destroy(sf2d_coupled *C) {
   delete C;
+  return SF2D_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Kernel run of a coupled mesh (sf2d_coupled_fwi_*): the solid path's scheme
+// (sf2d_fwi.cu) over both domains.  The forward solver writes solid
+// displacement frames (its tile kernels) and fluid chi frames (k_fluid_frame)
+// while a segment is recomputed; the adjoint solver (adjoint = 1) reads them
+// in its solid tile kernels and in k_fluid_kernels.
+
+namespace {
+
+// Zeroes the fields, kernel sums, seismograms and step counters of a coupled
+// solver (frame bases are left to the caller).
+int coupled_reset(sf2d_coupled *C) {
+  cudaStream_t s = C->stream();
+  if (C->el)
+    if (int rc = sf2d_reset_solver(C->el)) return rc;
+  const size_t n = static_cast<size_t>(C->nglob);
+  SF2D_CUDA(cudaMemsetAsync(C->A.p, 0, sizeof(float) * n, s));
+  SF2D_CUDA(cudaMemsetAsync(C->A.pd, 0, sizeof(float) * n, s));
+  SF2D_CUDA(cudaMemsetAsync(C->A.pdd, 0, sizeof(float) * n, s));
+  if (C->A.kl_ac) SF2D_CUDA(cudaMemsetAsync(C->A.kl_ac, 0, sizeof(float2) * C->A.nslot_q, s));
+  const size_t nseis = static_cast<size_t>(C->nrec_total) * C->nstep * 2;
+  if (nseis) SF2D_CUDA(cudaMemsetAsync(C->seis, 0, sizeof(double) * nseis, s));
+  SF2D_CUDA(cudaMemsetAsync(C->ctr, 0, 3 * sizeof(int), s));
+  C->steps_done = 0;
+  return SF2D_OK;
+}
+
+int put_ctr(int *ctr, int idx, int value, cudaStream_t s) {
+  // pageable source: staged at call time, ordered on the stream
+  SF2D_CUDA(cudaMemcpyAsync(ctr + idx, &value, sizeof(int), cudaMemcpyHostToDevice, s));
+  return SF2D_OK;
+}
+
+constexpr int NO_FRAMES = 1 << 30;  // a frame base no step reaches
+
+}  // namespace
+
+struct sf2d_coupled_fwi {
+  sf2d_coupled *fwd = nullptr, *adj = nullptr;
+  int nstep = 0, K = 0, nseg = 0, nrec_total = 0, ng_s = 0, ng_f = 0, nspec_s = 0, nspec_f = 0;
+  float dt = 0.f;
+  float2 *sframes = nullptr, *ckpt_s = nullptr;  // solid: K frames; nseg * 3 * ng_s (u, v, a)
+  float *pframes = nullptr, *ckpt_f = nullptr;   // fluid: K frames; nseg * 3 * ng_f (chi, chi_dot, chi_dot_dot)
+  std::vector<int> ibool_s, el_rec, ac_rec;      // solid ibool; run receiver index of each solid / fluid receiver
+  std::vector<float> rho_s, kappa_s, mu_s;
+  std::vector<void *> allocs;
+  cudaEvent_t ev_fwd = nullptr, ev_adj = nullptr;
+  ~sf2d_coupled_fwi() {
+    if (fwd) cudaStreamSynchronize(fwd->stream());
+    if (adj) cudaStreamSynchronize(adj->stream());
+    if (ev_fwd) cudaEventDestroy(ev_fwd);
+    if (ev_adj) cudaEventDestroy(ev_adj);
+    for (void *p : allocs) cudaFree(p);
+    delete adj;
+    delete fwd;
+  }
+  template <typename T_>
+  int alloc(T_ **p, size_t count) {
+    cudaError_t e = cudaMalloc(reinterpret_cast<void **>(p), std::max<size_t>(count, 1) * sizeof(T_));
+    if (e != cudaSuccess)
+      return fail(e == cudaErrorMemoryAllocation ? SF2D_ERR_OOM : SF2D_ERR_CUDA,
+                  std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    allocs.push_back(*p);
+    return SF2D_OK;
+  }
+};
+
+extern "C" int sf2d_coupled_fwi_create(const sf2d_elastic_desc *eld, const sf2d_acoustic_desc *ad,
+                                       const sf2d_coupling_desc *cp, const float *solid_rhostore,
+                                       const float *solid_kappastore, int checkpoint_every, sf2d_coupled_fwi **out) {
+  using namespace sf2d;
+  if (!eld || !ad || !cp || !out) return fail(SF2D_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (checkpoint_every < 1) return fail(SF2D_ERR_INVALID, "checkpoint_every must be >= 1");
+  if (eld->time_scheme == 2) return fail(SF2D_ERR_INVALID, "the kernel run is implemented for Newmark");
+  if (cp->adjoint) return fail(SF2D_ERR_INVALID, "pass the forward coupling description");
+  if (cp->nrec_total < 1 || eld->nstep < 1) return fail(SF2D_ERR_INVALID, "the kernel run needs receivers and steps");
+  const bool solid = eld->nspec > 0;
+  if (solid && (!solid_rhostore || !solid_kappastore || !eld->mustore))
+    return fail(SF2D_ERR_INVALID, "missing solid rho / kappa / mu");
+  auto F = std::make_unique<sf2d_coupled_fwi>();
+  sf2d_coupled *fw = nullptr;
+  if (int rc = sf2d_coupled_create(eld, ad, cp, &fw)) return rc;
+  F->fwd = fw;
+  const int nstep = eld->nstep;
+  // adjoint problem: one pseudo-source per solid receiver component and per
+  // fluid receiver, weighted by the receiver's Lagrange products (FP32)
+  sf2d_elastic_desc ed = *eld;
+  std::vector<int> s_ispec;
+  std::vector<float> s_arr, s_stf;
+  if (solid) {
+    const int nr = eld->nrec;
+    s_ispec.resize(2 * nr);
+    s_arr.assign(static_cast<size_t>(2 * nr) * 50, 0.f);
+    s_stf.assign(static_cast<size_t>(std::max(1, 2 * nr)) * nstep, 0.f);
+    for (int r = 0; r < nr; ++r)
+      for (int c = 0; c < 2; ++c) {
+        s_ispec[2 * r + c] = eld->rec_ispec[r];
+        for (int j = 0; j < 5; ++j)
+          for (int i = 0; i < 5; ++i)
+            s_arr[(static_cast<size_t>(2 * r + c) * 25 + j * 5 + i) * 2 + c] =
+                static_cast<float>(eld->hxir[r * 5 + i]) * static_cast<float>(eld->hgammar[r * 5 + j]);
+      }
+    ed.nsrc = 2 * nr;
+    ed.src_ispec = s_ispec.data();
+    ed.sourcearrays = s_arr.data();
+    ed.stf = s_stf.data();
+    ed.nstage = 1;
+  }
+  sf2d_acoustic_desc a2 = *ad;
+  const int nrf = ad->nrec;
+  std::vector<float> f_arr(static_cast<size_t>(nrf) * 25), f_stf(static_cast<size_t>(std::max(1, nrf)) * nstep, 0.f);
+  for (int r = 0; r < nrf; ++r)
+    for (int j = 0; j < 5; ++j)
+      for (int i = 0; i < 5; ++i)
+        f_arr[static_cast<size_t>(r) * 25 + j * 5 + i] =
+            static_cast<float>(ad->hxir[r * 5 + i]) * static_cast<float>(ad->hgammar[r * 5 + j]);
+  a2.nsrc = nrf;
+  a2.src_ispec = ad->rec_ispec;
+  a2.sourcearrays = f_arr.data();
+  a2.stf = f_stf.data();
+  sf2d_coupling_desc c2 = *cp;
+  c2.adjoint = 1;
+  sf2d_coupled *aj = nullptr;
+  if (int rc = sf2d_coupled_create(&ed, &a2, &c2, &aj)) return rc;
+  F->adj = aj;
+  F->nstep = nstep;
+  F->K = checkpoint_every;
+  F->nseg = (nstep + checkpoint_every - 1) / checkpoint_every;
+  F->nrec_total = cp->nrec_total;
+  F->ng_f = ad->nglob;
+  F->nspec_f = ad->nspec;
+  F->dt = eld->deltat;
+  F->ac_rec.assign(ad->rec_global, ad->rec_global + nrf);
+  if (solid) {
+    F->ng_s = eld->nglob;
+    F->nspec_s = eld->nspec;
+    const size_t nl = static_cast<size_t>(eld->nspec) * 25;
+    F->ibool_s.assign(eld->ibool, eld->ibool + nl);
+    F->rho_s.assign(solid_rhostore, solid_rhostore + nl);
+    F->kappa_s.assign(solid_kappastore, solid_kappastore + nl);
+    F->mu_s.assign(eld->mustore, eld->mustore + nl);
+    F->el_rec.assign(cp->el_rec_global, cp->el_rec_global + eld->nrec);
+  }
+  int rc = 0;
+  const size_t K = static_cast<size_t>(F->K);
+  if ((rc = F->alloc(&F->pframes, K * F->ng_f)) || (rc = F->alloc(&F->ckpt_f, static_cast<size_t>(F->nseg) * 3 * F->ng_f)))
+    return rc;
+  if (solid && ((rc = F->alloc(&F->sframes, K * F->ng_s)) ||
+                (rc = F->alloc(&F->ckpt_s, static_cast<size_t>(F->nseg) * 3 * F->ng_s))))
+    return rc;
+  // fluid kernel accumulation: per element point (slot order) its point, rho, kappa
+  {
+    const Tiling &T = aj->T;
+    const size_t nq = static_cast<size_t>(ad->nspec) * 25;
+    std::vector<int> sib(nq);
+    std::vector<float2> rk(nq);
+    for (int sl = 0; sl < ad->nspec; ++sl)
+      for (int q = 0; q < 25; ++q) {
+        const size_t p = static_cast<size_t>(T.elem_order[sl]) * 25 + q;
+        sib[static_cast<size_t>(sl) * 25 + q] = T.glob2dev[ad->ibool[p]];
+        rk[static_cast<size_t>(sl) * 25 + q] = make_float2(ad->rhostore[p], ad->kappastore[p]);
+      }
+    AcParams &A = aj->A;
+    if ((rc = aj->upload_const(&A.slot_ibool, sib)) || (rc = aj->upload_const(&A.slot_rk, rk)) ||
+        (rc = aj->alloc(&A.kl_ac, nq)))
+      return rc;
+    SF2D_CUDA(cudaMemset(A.kl_ac, 0, sizeof(float2) * std::max<size_t>(nq, 1)));
+    A.nslot_q = static_cast<int>(nq);
+    A.kpframes = F->pframes;
+    A.npframes = F->K;
+    // the forward solver's fluid tiling is the adjoint one's (same mesh, same options)
+    fw->A.pframes = F->pframes;
+    fw->A.npframes = F->K;
+  }
+  if (solid) {
+    fw->el->P.frames = F->sframes;
+    fw->el->P.nframes = F->K;
+    aj->el->P.kframes = F->sframes;
+  }
+  SF2D_CUDA(cudaEventCreateWithFlags(&F->ev_fwd, cudaEventDisableTiming));
+  SF2D_CUDA(cudaEventCreateWithFlags(&F->ev_adj, cudaEventDisableTiming));
+  if ((rc = put_ctr(fw->ctr, 4, NO_FRAMES, fw->stream()))) return rc;
+  if (solid && (rc = put_ctr(fw->el->ctr, 3, NO_FRAMES, fw->stream()))) return rc;
+  SF2D_CUDA(cudaStreamSynchronize(fw->stream()));
+  *out = F.release();
+  return SF2D_OK;
+}
+
+extern "C" int sf2d_coupled_fwi_forward(sf2d_coupled_fwi *F, double *seismograms) {
+  using namespace sf2d;
+  if (!F) return fail(SF2D_ERR_INVALID, "null handle");
+  sf2d_coupled *C = F->fwd;
+  cudaStream_t s = C->stream();
+  int rc = coupled_reset(C);
+  if (rc) return rc;
+  if ((rc = put_ctr(C->ctr, 4, NO_FRAMES, s))) return rc;
+  if (C->el && (rc = put_ctr(C->el->ctr, 3, NO_FRAMES, s))) return rc;
+  const size_t ns = static_cast<size_t>(F->ng_s), nf = static_cast<size_t>(F->ng_f);
+  for (int seg = 0; seg < F->nseg; ++seg) {
+    if (C->el) {
+      float2 *ck = F->ckpt_s + static_cast<size_t>(seg) * 3 * ns;
+      const sf2d::Params &P = C->el->P;
+      SF2D_CUDA(cudaMemcpyAsync(ck, P.u, sizeof(float2) * ns, cudaMemcpyDeviceToDevice, s));
+      SF2D_CUDA(cudaMemcpyAsync(ck + ns, P.v, sizeof(float2) * ns, cudaMemcpyDeviceToDevice, s));
+      SF2D_CUDA(cudaMemcpyAsync(ck + 2 * ns, P.a, sizeof(float2) * ns, cudaMemcpyDeviceToDevice, s));
+    }
+    float *cf = F->ckpt_f + static_cast<size_t>(seg) * 3 * nf;
+    SF2D_CUDA(cudaMemcpyAsync(cf, C->A.p, sizeof(float) * nf, cudaMemcpyDeviceToDevice, s));
+    SF2D_CUDA(cudaMemcpyAsync(cf + nf, C->A.pd, sizeof(float) * nf, cudaMemcpyDeviceToDevice, s));
+    SF2D_CUDA(cudaMemcpyAsync(cf + 2 * nf, C->A.pdd, sizeof(float) * nf, cudaMemcpyDeviceToDevice, s));
+    if ((rc = sf2d_coupled_enqueue(C, std::min(F->K, F->nstep - seg * F->K)))) return rc;
+  }
+  const int st = sf2d_coupled_synchronize(C);
+  if (st && st != SF2D_ERR_UNSTABLE) return st;
+  if (seismograms)
+    SF2D_CUDA(cudaMemcpy(seismograms, C->seis, sizeof(double) * F->nrec_total * F->nstep * 2, cudaMemcpyDeviceToHost));
+  return st;
+}
+
+extern "C" int sf2d_coupled_fwi_backward(sf2d_coupled_fwi *F, const float *adj_src, float *rho_kl, float *kappa_kl,
+                                         float *mu_kl, float *rho_ac_kl, float *kappa_ac_kl) {
+  using namespace sf2d;
+  if (!F || !adj_src || !rho_ac_kl || !kappa_ac_kl) return fail(SF2D_ERR_INVALID, "null argument");
+  sf2d_coupled *A = F->adj, *C = F->fwd;
+  const bool solid = A->el != nullptr;
+  if (solid && (!rho_kl || !kappa_kl || !mu_kl)) return fail(SF2D_ERR_INVALID, "null solid kernel array");
+  const int nstep = F->nstep;
+  cudaStream_t sa = A->stream(), sf = C->stream();
+  // time-reversed adjoint sources of the pseudo-sources
+  if (solid) {
+    const int nr = static_cast<int>(F->el_rec.size());
+    std::vector<float> stf(static_cast<size_t>(2 * nr) * nstep);
+    for (int r = 0; r < nr; ++r)
+      for (int c = 0; c < 2; ++c)
+        for (int it = 0; it < nstep; ++it)
+          stf[static_cast<size_t>(2 * r + c) * nstep + it] =
+              adj_src[(static_cast<size_t>(F->el_rec[r]) * nstep + (nstep - 1 - it)) * 2 + c];
+    if (nr) SF2D_CUDA(cudaMemcpy(A->el->d_stf, stf.data(), sizeof(float) * stf.size(), cudaMemcpyHostToDevice));
+  }
+  {
+    const int nr = static_cast<int>(F->ac_rec.size());
+    std::vector<float> stf(static_cast<size_t>(nr) * nstep);
+    for (int r = 0; r < nr; ++r)
+      for (int it = 0; it < nstep; ++it)
+        stf[static_cast<size_t>(r) * nstep + it] = adj_src[(static_cast<size_t>(F->ac_rec[r]) * nstep + (nstep - 1 - it)) * 2];
+    if (nr)
+      SF2D_CUDA(cudaMemcpy(const_cast<float *>(A->A.stf), stf.data(), sizeof(float) * stf.size(), cudaMemcpyHostToDevice));
+  }
+  int rc = coupled_reset(A);
+  if (rc) return rc;
+  const size_t ns = static_cast<size_t>(F->ng_s), nf = static_cast<size_t>(F->ng_f);
+  for (int seg = F->nseg - 1; seg >= 0; --seg) {
+    const int s0 = seg * F->K;
+    const int n = std::min(F->K, nstep - s0);
+    // recompute the forward segment once the adjoint sweep no longer reads the frames
+    SF2D_CUDA(cudaStreamWaitEvent(sf, F->ev_adj, 0));
+    if (solid) {
+      const float2 *ck = F->ckpt_s + static_cast<size_t>(seg) * 3 * ns;
+      const sf2d::Params &P = C->el->P;
+      SF2D_CUDA(cudaMemcpyAsync(P.u, ck, sizeof(float2) * ns, cudaMemcpyDeviceToDevice, sf));
+      SF2D_CUDA(cudaMemcpyAsync(P.v, ck + ns, sizeof(float2) * ns, cudaMemcpyDeviceToDevice, sf));
+      SF2D_CUDA(cudaMemcpyAsync(P.a, ck + 2 * ns, sizeof(float2) * ns, cudaMemcpyDeviceToDevice, sf));
+      if ((rc = put_ctr(C->el->ctr, 0, s0, sf)) || (rc = put_ctr(C->el->ctr, 3, s0, sf))) return rc;
+    }
+    const float *cf = F->ckpt_f + static_cast<size_t>(seg) * 3 * nf;
+    SF2D_CUDA(cudaMemcpyAsync(C->A.p, cf, sizeof(float) * nf, cudaMemcpyDeviceToDevice, sf));
+    SF2D_CUDA(cudaMemcpyAsync(C->A.pd, cf + nf, sizeof(float) * nf, cudaMemcpyDeviceToDevice, sf));
+    SF2D_CUDA(cudaMemcpyAsync(C->A.pdd, cf + 2 * nf, sizeof(float) * nf, cudaMemcpyDeviceToDevice, sf));
+    if ((rc = put_ctr(C->ctr, 0, s0, sf)) || (rc = put_ctr(C->ctr, 4, s0, sf))) return rc;
+    if ((rc = sf2d_coupled_enqueue(C, n))) return rc;
+    SF2D_CUDA(cudaEventRecord(F->ev_fwd, sf));
+    // adjoint steps nstep-s0-n .. nstep-s0-1 pair with frames n-1 .. 0
+    SF2D_CUDA(cudaStreamWaitEvent(sa, F->ev_fwd, 0));
+    if (solid && (rc = put_ctr(A->el->ctr, 4, nstep - 1 - s0, sa))) return rc;
+    if ((rc = put_ctr(A->ctr, 5, nstep - 1 - s0, sa))) return rc;
+    if ((rc = sf2d_coupled_enqueue(A, n))) return rc;
+    SF2D_CUDA(cudaEventRecord(F->ev_adj, sa));
+  }
+  SF2D_CUDA(cudaStreamSynchronize(sf));
+  const int st = sf2d_coupled_synchronize(A);
+  if (st && st != SF2D_ERR_UNSTABLE) return st;
+  if ((rc = put_ctr(C->ctr, 4, NO_FRAMES, sf))) return rc;
+  if (solid && (rc = put_ctr(C->el->ctr, 3, NO_FRAMES, sf))) return rc;
+  // solid kernel sums back to the sub-mesh layout with save_kernels_elastic's scaling
+  if (solid) {
+    const sf2d_solver *S = A->el;
+    std::vector<float2> kmu(S->nq);
+    std::vector<float> rg(ns);
+    SF2D_CUDA(cudaMemcpy(kmu.data(), S->P.kmu_kl, sizeof(float2) * S->nq, cudaMemcpyDeviceToHost));
+    SF2D_CUDA(cudaMemcpy(rg.data(), S->P.rho_kl_glob, sizeof(float) * ns, cudaMemcpyDeviceToHost));
+    const sf2d::Tiling &T = S->T;
+    const float dt = F->dt;
+    for (int sl = 0; sl < F->nspec_s; ++sl) {
+      const int e = T.elem_order[sl];
+      for (int q = 0; q < 25; ++q) {
+        const size_t p = static_cast<size_t>(e) * 25 + q;
+        const float rsum = rg[T.glob2dev[F->ibool_s[p]]];
+        const float2 km = kmu[static_cast<size_t>(sl) * 25 + q];
+        rho_kl[p] = -F->rho_s[p] * dt * rsum;
+        mu_kl[p] = -2.f * F->mu_s[p] * dt * km.y;
+        kappa_kl[p] = -F->kappa_s[p] * dt * km.x;
+      }
+    }
+  }
+  // fluid sums (deltat and 1/rho, 1/kappa already in) back to element order
+  {
+    std::vector<float2> kl(A->A.nslot_q);
+    SF2D_CUDA(cudaMemcpy(kl.data(), A->A.kl_ac, sizeof(float2) * kl.size(), cudaMemcpyDeviceToHost));
+    const sf2d::Tiling &T = A->T;
+    for (int sl = 0; sl < F->nspec_f; ++sl) {
+      const size_t e = static_cast<size_t>(T.elem_order[sl]);
+      for (int q = 0; q < 25; ++q) {
+        rho_ac_kl[e * 25 + q] = kl[static_cast<size_t>(sl) * 25 + q].x;
+        kappa_ac_kl[e * 25 + q] = kl[static_cast<size_t>(sl) * 25 + q].y;
+      }
+    }
+  }
+  return st;
+}
+
+extern "C" int sf2d_coupled_fwi_adjoint_seismograms(sf2d_coupled_fwi *F, double *seismograms) {
+  using namespace sf2d;
+  if (!F || !seismograms) return fail(SF2D_ERR_INVALID, "null argument");
+  SF2D_CUDA(cudaStreamSynchronize(F->adj->stream()));
+  SF2D_CUDA(cudaMemcpy(seismograms, F->adj->seis, sizeof(double) * F->nrec_total * F->nstep * 2,
+                       cudaMemcpyDeviceToHost));
+  return SF2D_OK;
+}
+
+extern "C" int sf2d_coupled_fwi_destroy(sf2d_coupled_fwi *F) {
+  delete F;
   return SF2D_OK;
 }

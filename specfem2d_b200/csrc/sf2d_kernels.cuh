@@ -93,6 +93,11 @@ struct Params {
   const int *cpl_local, *cpl_src;
   const float4 *cpl_nw;
   const float *pdd_ac;    // chi_dot_dot of the fluid, fluid device order
+  // adjoint run (SIMULATION_TYPE 3, solid step first): the pressure term is the
+  // fluid's predicted chi of this step, formed from chi, chi_dot, chi_dot_dot
+  // (compute_coupling_viscoelastic_ac.f90:89-93)
+  const float *p_ac, *pd_ac;
+  int cpl_adjoint;
   // CPML: elements of slots >= pml_slot0 lie in the layer, "PML points" are
   // their GLL points in slot order (index (slot - pml_slot0) * 25 + q)
   int pml_slot0;
@@ -138,6 +143,13 @@ __device__ __forceinline__ float newmark_veloc(float v, float a, float dto2) { r
 
 __device__ __forceinline__ void record_receiver(const Params &P, int r, int step) {
   if (step < 0 || step >= P.nstep_seis) return;
+  if (P.seismotype == 6) {
+    // a potential receiver in a solid records nothing (write_seismograms.F90:149-170)
+    double *out = P.seis + (static_cast<size_t>(P.rec_id[r]) * P.nstep_seis + step) * 2;
+    out[0] = 0.0;
+    out[1] = 0.0;
+    return;
+  }
   const float2 *field = P.seismotype == 2 ? P.v : (P.seismotype == 3 ? P.a : P.u);
   const int *dev = P.rec_dev + 25 * r;
   const double *h = P.rec_h + 10 * r;
@@ -477,7 +489,13 @@ __global__ void __launch_bounds__(NT, tile_min_blocks<NT, ANISO, ATTEN, KERN, PM
       const int p = ix[k];
       const float4 nw = P.cpl_nw[p];
       const int ga = P.cpl_src[p];
-      const float pressure = ga >= 0 ? -P.pdd_ac[ga] : P.cpl_pml_p[~ga];
+      float pressure;
+      if (ga < 0)
+        pressure = P.cpl_pml_p[~ga];
+      else if (P.cpl_adjoint)
+        pressure = newmark_displ(P.p_ac[ga], P.pd_ac[ga], P.pdd_ac[ga], P.dt, P.dt2o2);
+      else
+        pressure = -P.pdd_ac[ga];
       acc.x += nw.z * nw.x * pressure;
       acc.y += nw.z * nw.y * pressure;
     }

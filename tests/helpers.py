@@ -19,6 +19,17 @@ def load_golden(name):
     return cfg, seis
 
 
+def load_kernel_golden(name):
+    """(config, adjoint arrays, kernel-run log values) of a kernel example
+    without REF_SEIS (tests/golden/make_golden.py KERNEL_ONLY)."""
+    with open(os.path.join(GOLDEN, name + ".json")) as f:
+        cfg = json.load(f)
+    ref = dict(np.load(os.path.join(GOLDEN, name + "_adjoint.npz")))
+    with open(os.path.join(GOLDEN, name + "_adjoint.json")) as f:
+        log = json.load(f)
+    return cfg, ref, log
+
+
 def rel_l2(a, b):
     a = np.asarray(a, dtype=np.float64).ravel()
     b = np.asarray(b, dtype=np.float64).ravel()

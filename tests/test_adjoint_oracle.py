@@ -20,7 +20,7 @@ import os
 import numpy as np
 import pytest
 
-from helpers import GOLDEN, load_golden, rel_l2
+from helpers import GOLDEN, load_golden, load_kernel_golden, rel_l2
 from specfem2d_b200.setup.adjoint import cross_correlation_adjoint_source, derived_kernels
 from specfem2d_b200.setup.from_par_file import database_from_config
 
@@ -85,17 +85,8 @@ def test_oracle_adjoint_traces_and_kernel_maxima_match_ref_kernel(kernel_run):
 
 @pytest.fixture(scope="module")
 def fluid_solid():
-    cfg, _ = _load_kernel_only("luoyang_fluid_solid_kernel")
-    db = database_from_config(cfg)
-    ref = dict(np.load(os.path.join(GOLDEN, "luoyang_fluid_solid_kernel_adjoint.npz")))
-    with open(os.path.join(GOLDEN, "luoyang_fluid_solid_kernel_adjoint.json")) as f:
-        log = json.load(f)
-    return db, cfg, ref, log
-
-
-def _load_kernel_only(name):
-    with open(os.path.join(GOLDEN, name + ".json")) as f:
-        return json.load(f), None
+    cfg, ref, log = load_kernel_golden("luoyang_fluid_solid_kernel")
+    return database_from_config(cfg), cfg, ref, log
 
 
 def test_fluid_solid_forward_potential_matches_the_adjoint_source(fluid_solid):
