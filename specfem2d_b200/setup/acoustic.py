@@ -216,26 +216,18 @@ def mass_matrix_acoustic(ibool, nglob, geo, mat, gll, is_acoustic, st_ac, newmar
     return (f32(1.0) / m).astype(f32)
 
 
-def free_surface_points(mesh, ibool, is_acoustic):
-    """Global points zeroed by enforce_acoustic_free_surface: every GLL point of
-    the outer edges of acoustic elements on the non-absorbing sides of the
-    structured mesh (determine_acoustic_surface.f90:50-140), or the GLL ranges
-    of the listed edges of an external mesh (enforce_acoustic_free_surface.f90
-    over acoustic_surface)."""
-    if mesh.free_edges is not None:
-        pts = [int(ibool[e, j, i]) for (e, i0, i1, j0, j1) in mesh.free_edges if is_acoustic[e]
-               for j in range(j0, j1 + 1) for i in range(i0, i1 + 1)]
-        return np.unique(np.array(pts, dtype=np.int32)) if pts else np.zeros(0, np.int32)
+def structured_free_edges(mesh, is_acoustic):
+    """(nfree, 5) rows (element, imin, imax, jmin, jmax): the outer edges of
+    fluid elements on the non-absorbing sides of the structured mesh, top,
+    bottom, left, right (determine_acoustic_surface.f90:50-140)."""
     nx, nz = mesh.nx, mesh.nz
     ab, ar, at, al = mesh.absorb
-    pts = []
+    rows = []
+    span = {ITOP: (0, L, L, L), IBOTTOM: (0, L, 0, 0), ILEFT: (0, 0, 0, L), IRIGHT: (L, L, 0, L)}
 
     def add(e, edge):
-        if not is_acoustic[e]:
-            return
-        for p in range(NGLL):
-            i, j = _ivalue(p, edge)
-            pts.append(int(ibool[e, j, i]))
+        if is_acoustic[e]:
+            rows.append((e,) + span[edge])
 
     if not at:
         for ix in range(nx):
@@ -249,4 +241,16 @@ def free_surface_points(mesh, ibool, is_acoustic):
     if not ar:
         for iz in range(nz):
             add(iz * nx + nx - 1, IRIGHT)
+    return np.array(rows, dtype=np.int64).reshape(-1, 5)
+
+
+def free_surface_points(mesh, ibool, is_acoustic):
+    """Global points zeroed by enforce_acoustic_free_surface
+    (enforce_acoustic_free_surface.f90:35-96): every GLL point of the listed
+    free-surface edges of fluid elements, those of an external mesh
+    (mesh.free_edges) or the structured mesh's outer edges
+    (structured_free_edges)."""
+    rows = mesh.free_edges if mesh.free_edges is not None else structured_free_edges(mesh, is_acoustic)
+    pts = [int(ibool[e, j, i]) for (e, i0, i1, j0, j1) in rows if is_acoustic[e]
+           for j in range(j0, j1 + 1) for i in range(i0, i1 + 1)]
     return np.unique(np.array(pts, dtype=np.int32)) if pts else np.zeros(0, np.int32)

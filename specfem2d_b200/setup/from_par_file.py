@@ -94,6 +94,20 @@ def config_from_data_dir(data_dir: str, par_file: str = "Par_file", source_file:
     return cfg
 
 
+def config_from_mesh_database(data_dir: str, database: str, par_file: str = "Par_file",
+                              source_file: str = "SOURCE") -> dict:
+    """The run's parameters from DATA/ (Par_file, SOURCE: the solver reads them
+    itself) and its mesh and materials from the mesher's database file
+    (OUTPUT_FILES/Database00000.bin), as xspecfem2D takes them."""
+    from .database_file import read_database
+
+    par = read_par_file(os.path.join(data_dir, par_file))
+    cfg = {k: par[k] for k in PAR_KEYS if k in par}
+    cfg["sources"] = read_source_file(os.path.join(data_dir, source_file))
+    cfg["mesh_database"] = read_database(database)
+    return cfg
+
+
 def database_from_data_dir(data_dir: str, nstep: int | None = None):
     """Return (Database, config dict) for the example whose DATA/ is ``data_dir``."""
     cfg = config_from_data_dir(data_dir)
@@ -121,7 +135,18 @@ def database_from_config(cfg: dict, nstep: int | None = None, absorbing_as_stace
         # (read_parameter_file.F90:1678-1687, read_parameter_file_derive_flags)
         absorb = (False, False, False, False)
     mats = {m["index"]: m for m in (material_from_row(r) for r in par["materials"])}
-    if par.get("read_external_mesh", False):
+    if cfg.get("mesh_database") is not None:
+        from .database_file import material_rows, mesh_from_database
+
+        # the mesher's database holds the mesh and the material table (read_mesh_databases.F90)
+        dbf = cfg["mesh_database"]
+        if np.any(dbf["pml"]):
+            raise NotImplementedError("CPML flags of a mesh database")
+        mats = {m["index"]: m for m in (material_from_row(r) for r in material_rows(dbf))}
+        fluid = [k for k, m in mats.items() if m["kind"] == 1 and abs(float(m["vs"])) <= 1e-9]
+        mesh = mesh_from_database(dbf, fluid)
+        mat_of = np.asarray(dbf["kmato"], dtype=np.int64).copy()
+    elif par.get("read_external_mesh", False):
         from .external_mesh import external_mesh
 
         if bool(par.get("PML_BOUNDARY_CONDITIONS", False)) and not absorbing_as_stacey:
