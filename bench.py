@@ -51,6 +51,8 @@ def _make_workload(name: str, nstep: int, scale: int = 1):
         return configs.c2_geometry(nstep=nstep, scale=scale)
     if name == "c1":
         return configs.c1_homogeneous(nstep=nstep)
+    if name == "c4_elastic":
+        return configs.c4_gradient(nstep=nstep)
     if name == "c3_viscoelastic":
         return configs.c3_viscoelastic(nstep=nstep, time_scheme=1, scale=scale)
     if name == "c3_viscoelastic_lddrk":
@@ -113,6 +115,9 @@ WORKLOAD_DESC = {
                     "vs=vp/1.73, Gardner rho, 5% Gaussian random field (corr. 200 m, seed 2), "
                     "Ricker 8 Hz force, dt 5e-4, 400 receivers"),
     "c1": "80x60 homogeneous elastic, Stacey L/R/B, free top, Ricker 10 Hz, 20 receivers",
+    "c4_elastic": ("forward run of the 1000x400-element (25 km x 10 km, 6,405,601 GLL points) isotropic "
+                   "starting model of the gradient configuration: linear-gradient background, Stacey "
+                   "sides and bottom, Ricker 8 Hz, 200 receivers, dt 4e-4"),
     "c3_viscoelastic": ("1600x800-element (40 km x 20 km, 20,489,601 GLL points) viscoelastic model under "
                         "sinusoidal topography (200 m, 5 km), 3 SLS Qkappa 200 Qmu 60, vp 2500-6000, "
                         "seeded moment tensor, Ricker 5 Hz, dt 3e-4, Newmark"),
@@ -310,6 +315,34 @@ def fwi_members(n_models: int, nstep: int, which: str = "first"):
     with open(path, "wb") as f:
         pickle.dump(models, f)
     return models
+
+
+def measure_coupled_gradient(db, checkpoint_every: int = 100):
+    """Kernel run of a fluid-solid model through sf2d_coupled_fwi_* (forward
+    with checkpoints, then the adjoint sweep with the forward segments
+    recomputed; solid and fluid kernels): one untimed run, then one timed by
+    the host clock around the C-ABI calls (traces in, kernels out included).
+    The adjoint source is the synthetics themselves (zero observed data): the
+    time does not depend on the data."""
+    from specfem2d_b200.coupled import CoupledKernels
+
+    k = CoupledKernels(db, checkpoint_every)
+    try:
+        k.backward(k.forward())
+        t0 = time.perf_counter()
+        seis = k.forward()
+        t1 = time.perf_counter()
+        kern = k.backward(seis)
+        t2 = time.perf_counter()
+    finally:
+        k.close()
+    ok = all(np.isfinite(v).all() for v in kern.values())
+    return {"value": t2 - t0, "unit": "s per gradient", "forward_s": t1 - t0, "backward_s": t2 - t1,
+            "nstep": db.nstep, "nglob": db.nglob, "checkpoint_every": checkpoint_every,
+            "point_updates_per_s": 3.0 * db.nstep * db.nglob / (t2 - t0), "finite": bool(ok),
+            "description": ("kernel run (forward, recomputed forward, adjoint; rho/kappa/mu in the solid, "
+                            "rho/kappa in the water) of the c2 coupled model with Stacey sides and bottom, "
+                            "host clock around sf2d_coupled_fwi_forward and _backward")}
 
 
 def measure_fwi(args, all_models, nstep, world, rank, sum_shots=False):
@@ -722,6 +755,9 @@ def main():
         fwi["description"] = ("the c5_fwi_models workload on its 24 smallest models (5,450-149,151 elements), "
                               "400 steps: " + FWI_WORKLOADS["c5_fwi_models"])
         line["fwi_gradient"] = fwi
+        c2s = build_workload("c2_coupled_stacey", 400)
+        line["fluid_solid_gradient"] = measure_coupled_gradient(c2s, 100)
+        del c2s
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
