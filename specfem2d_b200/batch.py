@@ -44,6 +44,10 @@ def pack(members) -> tuple[Database, BatchIndex]:
             raise ValueError("batch members must share dt, nstep and the time scheme")
         if (d.atten is None) != (d0.atten is None) or (d.aniso is None) != (d0.aniso is None):
             raise ValueError("batch members must share the physics (attenuation, anisotropy)")
+    for d in members:
+        # the packed mesh concatenates the solid arrays only
+        if getattr(d, "acoustic", None) is not None or getattr(d, "pml", None) is not None:
+            raise ValueError("batch members with fluid elements or CPML layers cannot be packed")
     eo = np.cumsum([0] + [d.nspec for d in members])
     go = np.cumsum([0] + [d.nglob for d in members])
     ro = np.cumsum([0] + [len(d.rec_ispec) for d in members])

@@ -166,12 +166,22 @@ extern "C" int sf2d_member_norms_noalloc(const float *d_field, const int64_t *of
     CUdeviceptr base = 0;
     size_t size = 0;
     if (g_address_range(&base, &size, reinterpret_cast<CUdeviceptr>(d_field)) != CUDA_SUCCESS)
+      return fail(SF2D_ERR_INVALID, "field pointer is not device memory");
+    // the allocation must live on the current device (a peer's memory passes the range query)
+    cudaPointerAttributes attr{};
+    int dev = -1;
+    if (cudaPointerGetAttributes(&attr, d_field) != cudaSuccess || cudaGetDevice(&dev) != cudaSuccess ||
+        attr.type != cudaMemoryTypeDevice || attr.device != dev) {
+      cudaGetLastError();
       return fail(SF2D_ERR_INVALID, "field pointer is not device memory of the current device");
-    const unsigned long long lo =
-        reinterpret_cast<uintptr_t>(d_field) + 8ull * static_cast<unsigned long long>(offsets[0]);
-    const unsigned long long hi =
-        reinterpret_cast<uintptr_t>(d_field) + 8ull * static_cast<unsigned long long>(offsets[nmembers]);
-    if (hi > static_cast<unsigned long long>(base) + size || lo < static_cast<unsigned long long>(base))
+    }
+    // bounds in float2 units before any address is formed: offsets (>= 0, increasing) must stay
+    // within the entries between d_field and the end of its allocation
+    const unsigned long long f = reinterpret_cast<uintptr_t>(d_field);
+    const unsigned long long b = static_cast<unsigned long long>(base);
+    if (f < b || f >= b + size) return fail(SF2D_ERR_INVALID, "field pointer outside its allocation");
+    const unsigned long long room = (b + size - f) / 8;
+    if (static_cast<unsigned long long>(offsets[nmembers]) > room)
       return fail(SF2D_ERR_INVALID, "member offsets reach past the field's allocation");
   }
 

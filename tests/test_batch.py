@@ -37,6 +37,16 @@ def test_pack_rejects_mismatched_members():
         batch.pack([shots[0], other])
 
 
+def test_pack_rejects_fluid_or_cpml_members():
+    """A packed mesh concatenates the solid arrays only: members with fluid
+    elements or CPML layers are refused instead of being modelled wrong."""
+    cfg, _ = load_golden("pressure_source_acoustic")
+    db = database_from_config(cfg)
+    assert db.acoustic is not None and db.pml is not None
+    with pytest.raises(ValueError):
+        batch.pack([db, db])
+
+
 @pytest.mark.gpu
 def test_batched_forward_matches_members():
     import oracle

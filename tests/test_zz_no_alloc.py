@@ -76,6 +76,7 @@ def test_member_norms_edge_cases_and_rejections():
     assert member_norms_noalloc(u.data_ptr(), [0, 600])[0] == 5.0
     # beyond the static scratch, decreasing offsets, no member, beyond the allocation
     big = np.zeros(4097 + 1, dtype=np.int64)
-    for bad in (big, [0, 10, 5], [0], [0, 1 << 40]):
+    # the last offset near INT64_MAX / 8 wraps 8 * offset past 2^64: it must still be rejected
+    for bad in (big, [0, 10, 5], [0], [0, 1 << 40], [0, (1 << 63) // 8 - 1], [0, (1 << 63) - 1]):
         with pytest.raises(SF2DError):
             member_norms_noalloc(u.data_ptr(), bad)
