@@ -117,6 +117,9 @@ int sf2d_coupled_run(sf2d_coupled *c, int nstep, double *seismograms);
  * chunks on the solver's stream); sf2d_coupled_synchronize waits for them and
  * returns the stability status; sf2d_coupled_get_stream gives the stream. */
 int sf2d_coupled_enqueue(sf2d_coupled *c, int nstep);
+/* Traces of steps it0 .. it0+n-1 (0-based) of the run's receivers:
+ * out nrec_total*n*2 [irec][k][comp]; waits for the queued steps. */
+int sf2d_coupled_copy_seismograms(sf2d_coupled *c, int it0, int n, double *out);
 int sf2d_coupled_prepare(sf2d_coupled *c);  /* as sf2d_prepare */
 int sf2d_coupled_synchronize(sf2d_coupled *c);
 int sf2d_coupled_get_stream(sf2d_coupled *c, void **stream);

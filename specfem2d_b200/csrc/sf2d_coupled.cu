@@ -844,6 +844,17 @@ extern "C" int sf2d_coupled_run(sf2d_coupled *C, int nstep, double *seismograms)
   return SF2D_OK;
 }
 
+extern "C" int sf2d_coupled_copy_seismograms(sf2d_coupled *C, int it0, int n, double *out) {
+  using namespace sf2d;
+  if (!C || !out || it0 < 0 || n < 0 || it0 + n > C->nstep) return fail(SF2D_ERR_INVALID, "bad arguments");
+  SF2D_CUDA(cudaStreamSynchronize(C->stream()));
+  if (C->nrec_total && n)
+    SF2D_CUDA(cudaMemcpy2D(out, sizeof(double) * 2 * n, C->seis + static_cast<size_t>(it0) * 2,
+                           sizeof(double) * 2 * C->nstep, sizeof(double) * 2 * n, C->nrec_total,
+                           cudaMemcpyDeviceToHost));
+  return SF2D_OK;
+}
+
 extern "C" int sf2d_coupled_get_fields(sf2d_coupled *C, float *displ, float *veloc, float *accel, float *pot,
                                        float *pot_dot, float *pot_dot_dot) {
   using namespace sf2d;

@@ -1,11 +1,14 @@
 // The reference's Fortran-to-GPU entry points (include/sf2d_fortran.h) over
-// this library's fused solver.  The SPECFEM2D Fortran host (prepare_gpu.f90,
-// compute_gpu_elastic.f90, update_displacement_Newmark.F90,
-// write_seismograms.F90, check_stability.F90) calls them with its own arrays;
-// they gather what sf2d_elastic_create needs, build the solver when the time
-// step is first known (update_displacement_cuda) and advance one fused step
-// per kernel_3_a_cuda.  Errors print and exit, as the reference's
-// exit_on_error (src/gpu/helper_functions.cu) does.
+// this library's fused solvers.  The SPECFEM2D Fortran host (prepare_gpu.f90,
+// compute_gpu_acoustic.f90, compute_gpu_elastic.f90,
+// update_displacement_Newmark.F90, write_seismograms.F90, check_stability.F90)
+// calls them with its own arrays; they gather what sf2d_elastic_create (a
+// solid mesh) or sf2d_coupled_create (a mesh with fluid elements: solid and
+// fluid sub-meshes with their own point numberings) needs, build the solver
+// when the time step is first known (the first update_displacement_*_cuda)
+// and advance one fused step per kernel_3_a_cuda (kernel_3_acoustic_cuda on a
+// fluid-only mesh).  Errors print and exit, as the reference's exit_on_error
+// (src/gpu/helper_functions.cu) does.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -17,6 +20,7 @@
 #include <vector>
 
 #include "sf2d_b200.h"
+#include "sf2d_coupled.h"
 #include "sf2d_fortran.h"
 
 namespace {
@@ -33,11 +37,12 @@ void check(const char *routine, int rc) {
   if (rc != SF2D_OK) stop(routine, sf2d_last_error());
 }
 
-enum Why { FLUID, KERNEL_RUN, MPI, DEBUG, OTHER };
+enum Why { PML, KERNEL_RUN, MPI, DEBUG, OTHER };
 
 [[noreturn]] void unsupported(const char *routine, Why why) {
   static const char *const text[] = {
-      "fluid domains and CPML run through sf2d_coupled_create / sf2d_coupled_run (include/sf2d_coupled.h)",
+      "CPML layers run through sf2d_elastic_create / sf2d_coupled_create with the descriptors' pml_* members "
+      "(include/sf2d_b200.h, include/sf2d_coupled.h)",
       "kernel runs use sf2d_fwi_create / sf2d_fwi_forward / sf2d_fwi_backward (include/sf2d_b200.h), which "
       "replay the forward field from checkpoints instead of reconstructing it backwards",
       "this library runs one mesh per process: there is no MPI halo exchange",
@@ -63,6 +68,21 @@ struct FortranMesh {
   int stage = 0;  // 0 between steps, 1 after update_displacement_cuda, 2 after the outer forces phase
   std::vector<float> staged_u, staged_v, staged_a;  // fields given before the solver exists
   std::vector<int> sample_step;                     // step of each sample in the host's trace buffer
+  // fluid elements (prepare_fields_acoustic_device): the run goes through the coupled solver
+  bool fluid = false, have_fluid = false;
+  int nspec_acoustic = 0;
+  std::vector<unsigned char> is_ac;                 // per element: mustore zero (ispec_is_acoustic)
+  std::vector<float> rmass_ac, rho, kappa;          // nglob; nspec*25; nspec*25
+  std::vector<int> free_iglob;                      // points of the free-surface faces
+  std::vector<int> cpl_iglob;                       // one entry per coupling-face point
+  std::vector<float> cpl_nx, cpl_nz, cpl_w;
+  std::vector<int> st_ac_iglob;                     // fluid absorbing points
+  std::vector<float> st_ac_w, st_ac_rvp;
+  sf2d_coupled *C = nullptr;
+  std::vector<float> staged_p, staged_pd, staged_pdd;
+  // step bookkeeping of a coupled mesh: 0 between steps, 1 fluid predicted,
+  // 2 solid predicted, 3 fluid forces, 4 fluid step done, 5 solid forces
+  int ac_phase = 0;
 };
 
 FortranMesh *mesh_of(const char *routine, const long *p) {
@@ -195,8 +215,14 @@ void rebuild_centroids(FortranMesh &m) {
   }
 }
 
+void build_coupled(const char *routine, FortranMesh &m);
+
 void build_solver(const char *routine, FortranMesh &m) {
-  if (m.S) return;
+  if (m.S || m.C) return;
+  if (m.fluid) {
+    build_coupled(routine, m);
+    return;
+  }
   if (!m.have_rmass) stop(routine, "prepare_fields_elastic_device has not been called");
   if (m.stacey && !m.have_stacey) stop(routine, "prepare_stacey_device has not been called");
   sf2d_elastic_desc &d = m.d;
@@ -261,12 +287,326 @@ void build_solver(const char *routine, FortranMesh &m) {
   }
 }
 
+// The elements of one domain with a compact numbering of their points
+// (ascending global id), as the coupled solver takes each sub-mesh.
+struct SubMesh {
+  std::vector<int> elems, pts, gmap, ibool;  // gmap: global point -> local, -1 outside
+};
+
+SubMesh submesh(const FortranMesh &m, bool fluid) {
+  SubMesh s;
+  s.gmap.assign(m.nglob, -1);
+  for (int e = 0; e < m.nspec; ++e)
+    if ((m.is_ac[e] != 0) == fluid) s.elems.push_back(e);
+  std::vector<char> used(m.nglob, 0);
+  for (int e : s.elems)
+    for (int q = 0; q < NGLL2; ++q) used[m.ibool[static_cast<size_t>(e) * NGLL2 + q]] = 1;
+  for (int g = 0; g < m.nglob; ++g)
+    if (used[g]) {
+      s.gmap[g] = static_cast<int>(s.pts.size());
+      s.pts.push_back(g);
+    }
+  s.ibool.resize(s.elems.size() * NGLL2);
+  for (size_t k = 0; k < s.elems.size(); ++k)
+    for (int q = 0; q < NGLL2; ++q)
+      s.ibool[k * NGLL2 + q] = s.gmap[m.ibool[static_cast<size_t>(s.elems[k]) * NGLL2 + q]];
+  return s;
+}
+
+template <typename T>
+std::vector<T> elem_rows(const std::vector<T> &a, const std::vector<int> &elems, size_t per) {
+  std::vector<T> out(elems.size() * per);
+  for (size_t k = 0; k < elems.size(); ++k)
+    std::copy(a.begin() + static_cast<size_t>(elems[k]) * per, a.begin() + static_cast<size_t>(elems[k] + 1) * per,
+              out.begin() + k * per);
+  return out;
+}
+
+// The coupled solver of a mesh with fluid elements: the solid and fluid
+// sub-meshes, the coupling faces of prepare_fields_acoustic_device for both
+// directions (the reference's GPU kernels use the fluid element's normals and
+// weights for both, compute_coupling_*_kernel.cu), sources and receivers split
+// by the domain of their element.
+void build_coupled(const char *routine, FortranMesh &m) {
+  if (!m.have_fluid) stop(routine, "prepare_fields_acoustic_device has not been called");
+  if (m.stacey && !m.have_stacey) stop(routine, "prepare_stacey_device has not been called");
+  const SubMesh S = submesh(m, false), F = submesh(m, true);
+  const bool solid = !S.elems.empty();
+  if (solid && !m.have_rmass) stop(routine, "prepare_fields_elastic_device has not been called");
+  // --- solid description (time stepping and GLL arrays only on a fluid-only mesh)
+  sf2d_elastic_desc d{};
+  d.hprime = m.hprime.data();
+  d.hprimewgll = m.hprimewgll.data();
+  d.wxgll = d.wzgll = m.wxgll.data();
+  d.nstep = m.nstep;
+  d.deltat = m.dt;
+  d.deltatover2 = m.dtover2;
+  d.deltatsquareover2 = m.dtsq2;
+  d.tile_elems = 32;
+  d.threads_per_block = 256;
+  d.time_scheme = 1;
+  d.nstage = 1;
+  d.seismotype = m.d.seismotype;
+  std::vector<float> s_xix, s_xiz, s_gx, s_gz, s_lambda, s_mu, s_rmass, s_srcarr, s_stf, s_st_nx, s_st_nz, s_st_w,
+      s_st_rvp, s_st_rvs, s_c[6], s_a[4];
+  std::vector<int> s_st_iglob, s_src, s_rec, s_rec_global, s_aniso;
+  std::vector<double> s_hxir, s_hgammar, s_cent;
+  std::vector<int> s_elem_of(m.nspec, -1), f_elem_of(m.nspec, -1);
+  for (size_t k = 0; k < S.elems.size(); ++k) s_elem_of[S.elems[k]] = static_cast<int>(k);
+  for (size_t k = 0; k < F.elems.size(); ++k) f_elem_of[F.elems[k]] = static_cast<int>(k);
+  if (solid) {
+    s_xix = elem_rows(m.xix, S.elems, NGLL2);
+    s_xiz = elem_rows(m.xiz, S.elems, NGLL2);
+    s_gx = elem_rows(m.gammax, S.elems, NGLL2);
+    s_gz = elem_rows(m.gammaz, S.elems, NGLL2);
+    s_lambda = elem_rows(m.lambda, S.elems, NGLL2);
+    s_mu = elem_rows(m.mu, S.elems, NGLL2);
+    s_cent = elem_rows(m.centroid, S.elems, 2);
+    s_rmass.resize(2 * S.pts.size());
+    for (size_t k = 0; k < S.pts.size(); ++k) {
+      s_rmass[2 * k] = m.rmass[2 * static_cast<size_t>(S.pts[k])];
+      s_rmass[2 * k + 1] = m.rmass[2 * static_cast<size_t>(S.pts[k]) + 1];
+    }
+    for (size_t k = 0; k < m.st_iglob.size(); ++k) {
+      const int l = S.gmap[m.st_iglob[k]];
+      if (l < 0) stop(routine, "a solid absorbing point outside the solid elements");
+      s_st_iglob.push_back(l);
+      s_st_nx.push_back(m.st_nx[k]);
+      s_st_nz.push_back(m.st_nz[k]);
+      s_st_w.push_back(m.st_w[k]);
+      s_st_rvp.push_back(m.st_rvp[k]);
+      s_st_rvs.push_back(m.st_rvs[k]);
+    }
+    for (int k = 0; k < m.nsrc; ++k) {
+      if (m.is_ac[m.src_ispec[k]]) continue;
+      s_src.push_back(s_elem_of[m.src_ispec[k]]);
+      s_srcarr.insert(s_srcarr.end(), m.srcarr.begin() + static_cast<size_t>(k) * NGLL2 * 2,
+                      m.srcarr.begin() + static_cast<size_t>(k + 1) * NGLL2 * 2);
+      s_stf.insert(s_stf.end(), m.stf.begin() + static_cast<size_t>(k) * m.nstep,
+                   m.stf.begin() + static_cast<size_t>(k + 1) * m.nstep);
+    }
+    for (int r = 0; r < m.nrec; ++r) {
+      if (m.is_ac[m.rec_ispec[r]]) continue;
+      s_rec.push_back(s_elem_of[m.rec_ispec[r]]);
+      s_rec_global.push_back(r);
+      s_hxir.insert(s_hxir.end(), m.hxir.begin() + r * NGLL, m.hxir.begin() + (r + 1) * NGLL);
+      s_hgammar.insert(s_hgammar.end(), m.hgammar.begin() + r * NGLL, m.hgammar.begin() + (r + 1) * NGLL);
+    }
+    d.nspec = static_cast<int>(S.elems.size());
+    d.nglob = static_cast<int>(S.pts.size());
+    d.ibool = S.ibool.data();
+    d.xix = s_xix.data();
+    d.xiz = s_xiz.data();
+    d.gammax = s_gx.data();
+    d.gammaz = s_gz.data();
+    d.lambdastore = s_lambda.data();
+    d.mustore = s_mu.data();
+    d.rmass_inverse = s_rmass.data();
+    d.centroid_xz = s_cent.data();
+    d.nstacey = static_cast<int>(s_st_iglob.size());
+    d.st_iglob = s_st_iglob.data();
+    d.st_nx = s_st_nx.data();
+    d.st_nz = s_st_nz.data();
+    d.st_w = s_st_w.data();
+    d.st_rho_vp = s_st_rvp.data();
+    d.st_rho_vs = s_st_rvs.data();
+    d.nsrc = static_cast<int>(s_src.size());
+    d.src_ispec = s_src.data();
+    d.sourcearrays = s_srcarr.data();
+    d.stf = s_stf.data();
+    d.nrec = static_cast<int>(s_rec.size());
+    d.rec_ispec = s_rec.data();
+    d.hxir = s_hxir.data();
+    d.hgammar = s_hgammar.data();
+    d.cosrot = m.d.cosrot;
+    d.sinrot = m.d.sinrot;
+    if (!m.aniso_flag.empty()) {
+      s_aniso = elem_rows(m.aniso_flag, S.elems, 1);
+      const std::vector<float> *c[6] = {&m.c11, &m.c13, &m.c15, &m.c33, &m.c35, &m.c55};
+      for (int k = 0; k < 6; ++k) s_c[k] = elem_rows(*c[k], S.elems, NGLL2);
+      d.ispec_is_anisotropic = s_aniso.data();
+      d.c11 = s_c[0].data();
+      d.c13 = s_c[1].data();
+      d.c15 = s_c[2].data();
+      d.c33 = s_c[3].data();
+      d.c35 = s_c[4].data();
+      d.c55 = s_c[5].data();
+    }
+    if (!m.a1.empty()) {
+      const std::vector<float> *a[4] = {&m.a1, &m.b1, &m.a2, &m.b2};
+      for (int k = 0; k < 4; ++k) s_a[k] = elem_rows(*a[k], S.elems, NGLL2 * 3);
+      d.att_a1 = s_a[0].data();
+      d.att_b1 = s_a[1].data();
+      d.att_a2 = s_a[2].data();
+      d.att_b2 = s_a[3].data();
+    }
+  }
+  // --- fluid description
+  sf2d_acoustic_desc a{};
+  const std::vector<float> f_xix = elem_rows(m.xix, F.elems, NGLL2), f_xiz = elem_rows(m.xiz, F.elems, NGLL2),
+                           f_gx = elem_rows(m.gammax, F.elems, NGLL2), f_gz = elem_rows(m.gammaz, F.elems, NGLL2),
+                           f_rho = elem_rows(m.rho, F.elems, NGLL2), f_kappa = elem_rows(m.kappa, F.elems, NGLL2);
+  std::vector<float> f_jac(f_xix.size());
+  // the reference's GPU kernels form the Jacobian from the inverse mapping in FP32
+  // (Kernel_2_acoustic_impl.cu)
+  for (size_t p = 0; p < f_jac.size(); ++p) f_jac[p] = 1.f / (f_xix[p] * f_gz[p] - f_gx[p] * f_xiz[p]);
+  const std::vector<double> f_cent = elem_rows(m.centroid, F.elems, 2);
+  std::vector<float> f_rmass(F.pts.size()), f_st_w, f_st_rvp, f_srcarr, f_stf;
+  for (size_t k = 0; k < F.pts.size(); ++k) f_rmass[k] = m.rmass_ac[F.pts[k]];
+  std::vector<int> f_free, f_st, f_src, f_rec, f_rec_global;
+  std::vector<double> f_hxir, f_hgammar;
+  for (int g : m.free_iglob) {
+    const int l = F.gmap[g];
+    if (l < 0) stop(routine, "a free-surface point outside the fluid elements");
+    f_free.push_back(l);
+  }
+  for (size_t k = 0; k < m.st_ac_iglob.size(); ++k) {
+    const int l = F.gmap[m.st_ac_iglob[k]];
+    if (l < 0) stop(routine, "a fluid absorbing point outside the fluid elements");
+    f_st.push_back(l);
+    f_st_w.push_back(m.st_ac_w[k]);
+    f_st_rvp.push_back(m.st_ac_rvp[k]);
+  }
+  for (int k = 0; k < m.nsrc; ++k) {
+    if (!m.is_ac[m.src_ispec[k]]) continue;
+    f_src.push_back(f_elem_of[m.src_ispec[k]]);
+    // sourcearray(1, i, j): the first component drives the potential
+    for (int q = 0; q < NGLL2; ++q) f_srcarr.push_back(m.srcarr[(static_cast<size_t>(k) * NGLL2 + q) * 2]);
+    f_stf.insert(f_stf.end(), m.stf.begin() + static_cast<size_t>(k) * m.nstep,
+                 m.stf.begin() + static_cast<size_t>(k + 1) * m.nstep);
+  }
+  for (int r = 0; r < m.nrec; ++r) {
+    if (!m.is_ac[m.rec_ispec[r]]) continue;
+    f_rec.push_back(f_elem_of[m.rec_ispec[r]]);
+    f_rec_global.push_back(r);
+    f_hxir.insert(f_hxir.end(), m.hxir.begin() + r * NGLL, m.hxir.begin() + (r + 1) * NGLL);
+    f_hgammar.insert(f_hgammar.end(), m.hgammar.begin() + r * NGLL, m.hgammar.begin() + (r + 1) * NGLL);
+  }
+  a.nspec = static_cast<int>(F.elems.size());
+  a.nglob = static_cast<int>(F.pts.size());
+  a.ibool = F.ibool.data();
+  a.xix = f_xix.data();
+  a.xiz = f_xiz.data();
+  a.gammax = f_gx.data();
+  a.gammaz = f_gz.data();
+  a.jacobian = f_jac.data();
+  a.rhostore = f_rho.data();
+  a.kappastore = f_kappa.data();
+  a.rmass_inverse = f_rmass.data();
+  a.centroid_xz = f_cent.data();
+  a.nfree = static_cast<int>(f_free.size());
+  a.free_iglob = f_free.data();
+  a.nstacey = static_cast<int>(f_st.size());
+  a.st_iglob = f_st.data();
+  a.st_w = f_st_w.data();
+  a.st_rho_vp = f_st_rvp.data();
+  a.nsrc = static_cast<int>(f_src.size());
+  a.src_ispec = f_src.data();
+  a.sourcearrays = f_srcarr.data();
+  a.stf = f_stf.data();
+  a.nrec = static_cast<int>(f_rec.size());
+  a.rec_ispec = f_rec.data();
+  a.hxir = f_hxir.data();
+  a.hgammar = f_hgammar.data();
+  a.rec_global = f_rec_global.data();
+  a.tile_elems = 32;
+  // --- coupling entries, the same faces for both directions
+  sf2d_coupling_desc c{};
+  std::vector<int> c_f, c_s;
+  for (int g : m.cpl_iglob) {
+    if (F.gmap[g] < 0 || S.gmap[g] < 0) stop(routine, "a coupling point not shared by a fluid and a solid element");
+    c_f.push_back(F.gmap[g]);
+    c_s.push_back(S.gmap[g]);
+  }
+  c.nrec_total = m.nrec;
+  c.el_rec_global = s_rec_global.data();
+  c.seismotype = m.d.seismotype;
+  c.use_trick = 0;
+  c.cosrot = m.d.cosrot;
+  c.sinrot = m.d.sinrot;
+  c.ncpl_ac = c.ncpl_el = static_cast<int>(c_f.size());
+  c.cpl_ac_point = c_f.data();
+  c.cpl_ac_el_point = c_s.data();
+  c.cpl_ac_nx = c.cpl_el_nx = m.cpl_nx.data();
+  c.cpl_ac_nz = c.cpl_el_nz = m.cpl_nz.data();
+  c.cpl_ac_w = c.cpl_el_w = m.cpl_w.data();
+  c.cpl_el_point = c_s.data();
+  c.cpl_el_ac_point = c_f.data();
+  check(routine, sf2d_coupled_create(&d, &a, &c, &m.C));
+  check(routine, sf2d_coupled_set_global_numbering(m.C, m.nglob, solid ? S.pts.data() : nullptr, F.pts.data()));
+  if (!m.staged_u.empty() || !m.staged_p.empty()) {
+    auto ptr = [](std::vector<float> &v) -> const float * { return v.empty() ? nullptr : v.data(); };
+    check(routine, sf2d_coupled_set_fields_global(m.C, ptr(m.staged_u), ptr(m.staged_v), ptr(m.staged_a),
+                                                  ptr(m.staged_p), ptr(m.staged_pd), ptr(m.staged_pdd)));
+  }
+  m.staged_u.clear();
+  m.staged_v.clear();
+  m.staged_a.clear();
+  m.staged_p.clear();
+  m.staged_pd.clear();
+  m.staged_pdd.clear();
+}
+
+// Whole-mesh fields of a coupled run (points outside a field's domain read zero);
+// before the solver exists, the staged copies (or zeros).
+void coupled_fields(const char *R, FortranMesh *m, realw *u, realw *v, realw *a, realw *p, realw *pd, realw *pdd) {
+  if (m->C) {
+    check(R, sf2d_coupled_get_fields_global(m->C, u, v, a, p, pd, pdd));
+    return;
+  }
+  const size_t n2 = 2 * static_cast<size_t>(m->nglob), n1 = m->nglob;
+  const std::pair<realw *, std::vector<float> *> f[6] = {{u, &m->staged_u}, {v, &m->staged_v}, {a, &m->staged_a},
+                                                           {p, &m->staged_p}, {pd, &m->staged_pd},
+                                                           {pdd, &m->staged_pdd}};
+  for (int k = 0; k < 6; ++k) {
+    if (!f[k].first) continue;
+    const size_t n = k < 3 ? n2 : n1;
+    if (f[k].second->empty())
+      std::memset(f[k].first, 0, n * sizeof(realw));
+    else
+      std::memcpy(f[k].first, f[k].second->data(), n * sizeof(realw));
+  }
+}
+
+// Sets some fields of a coupled run, keeping the others.
+void coupled_set(const char *R, FortranMesh *m, const realw *u, const realw *v, const realw *a, const realw *p,
+                 const realw *pd, const realw *pdd) {
+  const size_t n2 = 2 * static_cast<size_t>(m->nglob), n1 = m->nglob;
+  std::vector<float> cur[6] = {std::vector<float>(n2), std::vector<float>(n2), std::vector<float>(n2),
+                               std::vector<float>(n1), std::vector<float>(n1), std::vector<float>(n1)};
+  coupled_fields(R, m, cur[0].data(), cur[1].data(), cur[2].data(), cur[3].data(), cur[4].data(), cur[5].data());
+  const realw *in[6] = {u, v, a, p, pd, pdd};
+  for (int k = 0; k < 6; ++k)
+    if (in[k]) std::memcpy(cur[k].data(), in[k], cur[k].size() * sizeof(float));
+  if (m->C) {
+    check(R, sf2d_coupled_set_fields_global(m->C, cur[0].data(), cur[1].data(), cur[2].data(), cur[3].data(),
+                                            cur[4].data(), cur[5].data()));
+    return;
+  }
+  std::vector<float> *st[6] = {&m->staged_u, &m->staged_v, &m->staged_a, &m->staged_p, &m->staged_pd, &m->staged_pdd};
+  for (int k = 0; k < 6; ++k) *st[k] = std::move(cur[k]);
+}
+
+void fluid_phase_call(const char *R, FortranMesh *m, const int *compute_wavefield_2) {
+  if (compute_wavefield_2 && *compute_wavefield_2) unsupported(R, KERNEL_RUN);
+  if (m->ac_phase != 3) stop(R, "called outside the fluid forces of a time step");
+}
+
+void need_ac_size(const char *R, const FortranMesh *m, const int *size) {
+  if (!m->fluid) stop(R, "the mesh has no fluid element");
+  if (!size || *size != m->nglob) stop(R, "size must be NGLOB_AB = " + std::to_string(m->nglob));
+}
+
 void need_size(const char *routine, const FortranMesh &m, const int *size) {
   if (!size || *size != 2 * m.nglob) stop(routine, "size must be NDIM*NGLOB_AB = " + std::to_string(2 * m.nglob));
 }
 
 void fields_from(const char *R, FortranMesh *m, const int *size, realw *displ, realw *veloc, realw *accel) {
   need_size(R, *m, size);
+  if (m->fluid) {
+    coupled_fields(R, m, displ, veloc, accel, nullptr, nullptr, nullptr);
+    return;
+  }
   if (m->S) {
     check(R, sf2d_get_fields(m->S, displ, veloc, accel));
     return;
@@ -328,7 +668,7 @@ void prepare_constants_device_(long *Mesh_pointer, int *h_NGLLX, int *NSPEC_AB, 
                                int *nsources_local_f, realw *h_sourcearrays, realw *h_source_time_function,
                                int *NSTEP, int *h_ispec_selected_source, int *h_ispec_selected_rec_loc,
                                int *nrec_local, realw *h_cosrot, realw *h_sinrot, int *SIMULATION_TYPE, int *P_SV,
-                               int *nspec_acoustic, int *, int *, int *, int *, int *SAVE_FORWARD,
+                               int *nspec_acoustic, int *, int *ispec_is_acoustic, int *, int *, int *SAVE_FORWARD,
                                realw *h_xir_store, realw *h_gammar_store, int *h_NSIGTYPE, int *h_seismotypeVec,
                                int *nlength_seismogram) {
   const char *R = "prepare_constants_device";
@@ -339,14 +679,26 @@ void prepare_constants_device_(long *Mesh_pointer, int *h_NGLLX, int *NSPEC_AB, 
   if (*SAVE_FORWARD)
     stop(R, "SAVE_FORWARD: the boundary values of a backward reconstruction are not produced; kernel runs use "
             "sf2d_fwi_* (include/sf2d_b200.h)");
-  if (*nspec_acoustic > 0 || *PML_BOUNDARY_CONDITIONS) unsupported(R, FLUID);
+  if (*PML_BOUNDARY_CONDITIONS) unsupported(R, PML);
   if (*num_interfaces_ext_mesh > 0) unsupported(R, MPI);
   if (*h_NSIGTYPE != 1) stop(R, "one seismogram type per run (NSIGTYPE = 1)");
-  if (h_seismotypeVec[0] < 1 || h_seismotypeVec[0] > 3)
-    stop(R, "elastic runs record displacement, velocity or acceleration (seismotype 1-3)");
+  const int st = h_seismotypeVec[0];
+  if (*nspec_acoustic > 0 ? (st < 1 || st > 6 || st == 5) : (st < 1 || st > 3))
+    stop(R, "seismotype 1-3 (displacement, velocity, acceleration), with fluid elements also 4 (pressure) "
+            "and 6 (potential)");
   auto m = new FortranMesh();
   const int ns = *NSPEC_AB, ng = *NGLOB_AB;
   const size_t nl = static_cast<size_t>(ns) * NGLL2;
+  // ispec_is_acoustic is a Fortran logical array: nonzero is true
+  m->is_ac.assign(ns, 0);
+  if (*nspec_acoustic > 0) {
+    if (!ispec_is_acoustic) stop(R, "missing ispec_is_acoustic");
+    for (int e = 0; e < ns; ++e) m->is_ac[e] = ispec_is_acoustic[e] != 0;
+    if (std::count(m->is_ac.begin(), m->is_ac.end(), 1) != *nspec_acoustic)
+      stop(R, "ispec_is_acoustic disagrees with nspec_acoustic");
+    m->fluid = true;
+    m->nspec_acoustic = *nspec_acoustic;
+  }
   m->nspec = ns;
   m->nglob = ng;
   m->nstep = *NSTEP;
@@ -436,7 +788,8 @@ void prepare_fields_elastic_device_(long *Mesh_pointer, realw *rmassx, realw *rm
 // one entry per absorbing GLL point, in face order; a point whose i or j is
 // NGLLX + 1 (a corner a neighbouring face already covers) is left out, as
 // compute_stacey_elastic_kernel skips it
-void prepare_stacey_device_(long *Mesh_pointer, int *, int *ELASTIC_SIMULATION, realw *rho_vp, realw *rho_vs, int *,
+void prepare_stacey_device_(long *Mesh_pointer, int *ACOUSTIC_SIMULATION, int *ELASTIC_SIMULATION, realw *rho_vp,
+                            realw *rho_vs, int *,
                             int *, int *, int *, int *h_abs_boundary_ispec, int *h_abs_boundary_ij,
                             realw *h_abs_boundary_normal, realw *h_abs_boundary_jacobian1Dw,
                             int *h_num_abs_boundary_faces, int *, int *, int *, int *, int *) {
@@ -449,16 +802,28 @@ void prepare_stacey_device_(long *Mesh_pointer, int *, int *ELASTIC_SIMULATION, 
   m->st_w.clear();
   m->st_rvp.clear();
   m->st_rvs.clear();
+  m->st_ac_iglob.clear();
+  m->st_ac_w.clear();
+  m->st_ac_rvp.clear();
   const int nf = *h_num_abs_boundary_faces;
-  for (int f = 0; f < (*ELASTIC_SIMULATION ? nf : 0); ++f) {
+  for (int f = 0; f < nf; ++f) {
     const int e = h_abs_boundary_ispec[f] - 1;
     if (e < 0 || e >= m->nspec) stop(R, "abs_boundary_ispec out of range");
+    const bool fluid_face = m->is_ac[e] != 0;
+    if (fluid_face ? !*ACOUSTIC_SIMULATION : !*ELASTIC_SIMULATION) continue;
     for (int k = 0; k < NGLL; ++k) {
       const int i = h_abs_boundary_ij[(f * NGLL + k) * 2] - 1;
       const int j = h_abs_boundary_ij[(f * NGLL + k) * 2 + 1] - 1;
       if (i == NGLL || j == NGLL) continue;
       if (i < 0 || i >= NGLL || j < 0 || j >= NGLL) stop(R, "abs_boundary_ij out of range");
       const size_t p = static_cast<size_t>(e) * NGLL2 + j * NGLL + i;
+      if (fluid_face) {
+        // compute_stacey_acoustic_kernel: chi_dd -= chi_d w / (rho vp)
+        m->st_ac_iglob.push_back(m->ibool[p]);
+        m->st_ac_w.push_back(h_abs_boundary_jacobian1Dw[f * NGLL + k]);
+        m->st_ac_rvp.push_back(rho_vp[p]);
+        continue;
+      }
       m->st_iglob.push_back(m->ibool[p]);
       m->st_nx.push_back(h_abs_boundary_normal[(f * NGLL + k) * 2]);
       m->st_nz.push_back(h_abs_boundary_normal[(f * NGLL + k) * 2 + 1]);
@@ -474,6 +839,7 @@ void prepare_stacey_device_(long *Mesh_pointer, int *, int *ELASTIC_SIMULATION, 
 void prepare_cleanup_device_(long *Mesh_pointer, int *, int *, int *, int *, int *, int *, int *, realw *) {
   FortranMesh *m = mesh_of("prepare_cleanup_device", Mesh_pointer);
   if (m->S) sf2d_destroy(m->S);
+  if (m->C) sf2d_coupled_destroy(m->C);
   delete m;
   *Mesh_pointer = 0;
 }
@@ -487,6 +853,12 @@ void update_displacement_cuda_(long *Mesh_pointer, realw *deltat_F, realw *delta
                                realw *, realw *, realw *) {
   const char *R = "update_displacement_cuda";
   FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (m->fluid) {
+    // coupled mesh: the solid predictor follows the fluid's (update_displacement_Newmark.F90:150-240)
+    if (m->ac_phase != 1) stop(R, "update_displacement_ac_cuda must start the step");
+    m->ac_phase = 2;
+    return;
+  }
   if (m->stage != 0) stop(R, "the previous time step did not reach kernel_3_a_cuda");
   if (!m->S) {
     m->dt = *deltat_F;
@@ -508,6 +880,13 @@ void compute_forces_viscoelastic_cuda_(long *Mesh_pointer, int *iphase, realw *,
   const char *R = "compute_forces_viscoelastic_cuda";
   FortranMesh *m = mesh_of(R, Mesh_pointer);
   if (*compute_wavefield_2) unsupported(R, KERNEL_RUN);
+  if (m->fluid) {
+    if (*iphase == 1 && m->ac_phase == 4)
+      m->ac_phase = 5;
+    else if (!(*iphase == 2 && m->ac_phase == 5))
+      stop(R, "called out of the order kernel_3_acoustic_cuda, iphase 1, iphase 2, kernel_3_a_cuda");
+    return;
+  }
   if (*iphase == 1 && m->stage == 1)
     m->stage = 2;
   else if (!(*iphase == 2 && m->stage == 2))
@@ -521,7 +900,7 @@ void compute_stacey_viscoelastic_cuda_(long *Mesh_pointer, int *, realw *, realw
   const char *R = "compute_stacey_viscoelastic_cuda";
   FortranMesh *m = mesh_of(R, Mesh_pointer);
   if (*compute_wavefield_2) unsupported(R, KERNEL_RUN);
-  if (m->stage != 2) stop(R, "called outside a time step");
+  if (m->fluid ? m->ac_phase != 5 : m->stage != 2) stop(R, "called outside a time step");
 }
 
 // compute_add_sources_el_cuda (src/gpu/compute_add_sources_viscoelastic_cuda.cu:46):
@@ -529,7 +908,7 @@ void compute_stacey_viscoelastic_cuda_(long *Mesh_pointer, int *, realw *, realw
 void compute_add_sources_el_cuda_(long *Mesh_pointer, int *, int *itf) {
   const char *R = "compute_add_sources_el_cuda";
   FortranMesh *m = mesh_of(R, Mesh_pointer);
-  if (m->stage != 2) stop(R, "called outside a time step");
+  if (m->fluid ? m->ac_phase != 5 : m->stage != 2) stop(R, "called outside a time step");
   if (*itf != m->steps + 1) stop(R, "time step " + std::to_string(*itf) + " out of sequence");
 }
 
@@ -539,6 +918,14 @@ void kernel_3_a_cuda_(long *Mesh_pointer, realw *, realw *, int *, int *compute_
   const char *R = "kernel_3_a_cuda";
   FortranMesh *m = mesh_of(R, Mesh_pointer);
   if (*compute_wavefield_2) unsupported(R, KERNEL_RUN);
+  if (m->fluid) {
+    // the last call of a coupled step: both domains advance in one fused step
+    if (m->ac_phase != 5) stop(R, "called before compute_forces_viscoelastic_cuda");
+    check(R, sf2d_coupled_enqueue(m->C, 1));
+    ++m->steps;
+    m->ac_phase = 0;
+    return;
+  }
   if (m->stage != 2) stop(R, "called before compute_forces_viscoelastic_cuda");
   check(R, sf2d_enqueue(m->S, 1));
   ++m->steps;
@@ -565,7 +952,10 @@ void compute_seismograms_cuda_(long *Mesh_pointer_f, int *i_sigf, double *sisux,
   const int s0 = m->sample_step.front(), s1 = m->sample_step.back();
   const int n = s1 - s0 + 1;
   std::vector<double> tr(static_cast<size_t>(m->nrec) * n * 2);
-  check(R, sf2d_copy_seismograms(m->S, s0, n, tr.data()));
+  if (m->C)
+    check(R, sf2d_coupled_copy_seismograms(m->C, s0, n, tr.data()));
+  else
+    check(R, sf2d_copy_seismograms(m->S, s0, n, tr.data()));
   for (int r = 0; r < m->nrec; ++r)
     for (size_t k = 0; k < m->sample_step.size(); ++k) {
       const size_t src = (static_cast<size_t>(r) * n + (m->sample_step[k] - s0)) * 2;
@@ -580,6 +970,15 @@ void get_norm_elastic_from_device_(realw *norm, long *Mesh_pointer, const int *F
   const char *R = "get_norm_elastic_from_device";
   FortranMesh *m = mesh_of(R, Mesh_pointer);
   if (FORWARD_OR_ADJOINT && *FORWARD_OR_ADJOINT == 3) unsupported(R, KERNEL_RUN);
+  if (m->fluid) {
+    std::vector<float> u(2 * static_cast<size_t>(m->nglob));
+    coupled_fields(R, m, u.data(), nullptr, nullptr, nullptr, nullptr, nullptr);
+    float mx = 0.f;
+    for (int g = 0; g < m->nglob; ++g)
+      mx = std::max(mx, std::sqrt(u[2 * g] * u[2 * g] + u[2 * g + 1] * u[2 * g + 1]));
+    *norm = mx;
+    return;
+  }
   if (!m->S) {
     float mx = 0.f;
     for (size_t g = 0; g < m->staged_u.size() / 2; ++g)
@@ -596,6 +995,10 @@ void transfer_fields_el_to_device_(int *size, realw *displ, realw *veloc, realw 
   const char *R = "transfer_fields_el_to_device";
   FortranMesh *m = mesh_of(R, Mesh_pointer);
   need_size(R, *m, size);
+  if (m->fluid) {
+    coupled_set(R, m, displ, veloc, accel, nullptr, nullptr, nullptr);
+    return;
+  }
   if (m->S) {
     check(R, sf2d_set_fields(m->S, displ, veloc, accel));
     return;
@@ -629,6 +1032,187 @@ void transfer_accel_to_device_(int *size, realw *accel, long *Mesh_pointer) {
   transfer_fields_el_to_device_(size, u.data(), v.data(), accel, Mesh_pointer);
 }
 
+// ---- the fluid domain (compute_gpu_acoustic.f90, update_displacement_Newmark.F90) ----
+
+// prepare_fields_acoustic_device (src/gpu/prepare_mesh_constants_cuda.cu:319):
+// the fluid mass matrix, rho and kappa, the free-surface faces (every point of
+// a face is zeroed) and the fluid-solid faces (one entry per face point)
+void prepare_fields_acoustic_device_(long *Mesh_pointer, realw *rmass_acoustic, realw *rhostore, realw *kappastore,
+                                     int *, int *, int *num_free_surface_faces, int *free_surface_ispec,
+                                     int *free_surface_ijk, int *ELASTIC_SIMULATION, int *num_coupling_ac_el_faces,
+                                     int *coupling_ac_el_ispec, int *coupling_ac_el_ijk, realw *coupling_ac_el_normal,
+                                     realw *coupling_ac_el_jacobian2Dw, int *h_ninterface_acoustic, int *,
+                                     int *ATTENUATION_VISCOACOUSTIC, realw *, realw *, int *NO_BACKWARD_RECONSTRUCTION,
+                                     realw *) {
+  const char *R = "prepare_fields_acoustic_device";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (m->S || m->C) stop(R, "called after the time loop started");
+  if (!m->fluid) stop(R, "prepare_constants_device was given no fluid element (nspec_acoustic = 0)");
+  if (*h_ninterface_acoustic > 0) unsupported(R, MPI);
+  if (*ATTENUATION_VISCOACOUSTIC) stop(R, "viscoacoustic attenuation is not provided");
+  if (*NO_BACKWARD_RECONSTRUCTION) unsupported(R, KERNEL_RUN);
+  const size_t nl = static_cast<size_t>(m->nspec) * NGLL2;
+  m->rmass_ac.assign(rmass_acoustic, rmass_acoustic + m->nglob);
+  m->rho.assign(rhostore, rhostore + nl);
+  m->kappa.assign(kappastore, kappastore + nl);
+  auto point_of = [&](int e, const int *ij, int f, int k, const char *what) {
+    if (e < 0 || e >= m->nspec || !m->is_ac[e]) stop(R, std::string(what) + ": not a fluid element");
+    const int i = ij[(f * NGLL + k) * 2] - 1, j = ij[(f * NGLL + k) * 2 + 1] - 1;
+    if (i < 0 || i >= NGLL || j < 0 || j >= NGLL) stop(R, std::string(what) + ": GLL index out of range");
+    return m->ibool[static_cast<size_t>(e) * NGLL2 + j * NGLL + i];
+  };
+  m->free_iglob.clear();
+  for (int f = 0; f < *num_free_surface_faces; ++f)
+    for (int k = 0; k < NGLL; ++k)
+      m->free_iglob.push_back(point_of(free_surface_ispec[f] - 1, free_surface_ijk, f, k, "free_surface_ispec"));
+  m->cpl_iglob.clear();
+  m->cpl_nx.clear();
+  m->cpl_nz.clear();
+  m->cpl_w.clear();
+  for (int f = 0; f < (*ELASTIC_SIMULATION ? *num_coupling_ac_el_faces : 0); ++f)
+    for (int k = 0; k < NGLL; ++k) {
+      m->cpl_iglob.push_back(point_of(coupling_ac_el_ispec[f] - 1, coupling_ac_el_ijk, f, k, "coupling_ac_el_ispec"));
+      m->cpl_nx.push_back(coupling_ac_el_normal[(f * NGLL + k) * 2]);
+      m->cpl_nz.push_back(coupling_ac_el_normal[(f * NGLL + k) * 2 + 1]);
+      m->cpl_w.push_back(coupling_ac_el_jacobian2Dw[f * NGLL + k]);
+    }
+  m->have_fluid = true;
+}
+
+// update_displacement_ac_cuda (src/gpu/update_displacement_cuda.cu:133): the
+// first call of a step of a mesh with fluid elements; the first one of the
+// run builds the coupled solver
+void update_displacement_ac_cuda_(long *Mesh_pointer, realw *deltat_F, realw *deltatsqover2_F, realw *deltatover2_F,
+                                  realw *, realw *, realw *, int *, int *UNDO_ATTENUATION_AND_OR_PML) {
+  const char *R = "update_displacement_ac_cuda";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (!m->fluid) stop(R, "the mesh has no fluid element");
+  if (UNDO_ATTENUATION_AND_OR_PML && *UNDO_ATTENUATION_AND_OR_PML) unsupported(R, KERNEL_RUN);
+  if (m->ac_phase != 0) stop(R, "the previous time step did not finish");
+  if (!m->C) {
+    m->dt = *deltat_F;
+    m->dtsq2 = *deltatsqover2_F;
+    m->dtover2 = *deltatover2_F;
+    build_solver(R, *m);
+  } else if (*deltat_F != m->dt || *deltatsqover2_F != m->dtsq2 || *deltatover2_F != m->dtover2) {
+    stop(R, "the time step changed during the run");
+  }
+  if (m->steps >= m->nstep) stop(R, "more time steps than NSTEP");
+  // without solid elements no update_displacement_cuda follows
+  m->ac_phase = m->nspec_acoustic == m->nspec ? 2 : 1;
+}
+
+// acoustic_enforce_free_surf_cuda (src/gpu/enforce_acoustic_free_surface_cuda.cu:46):
+// the zeroing before and after the fluid forces is part of the fused step
+void acoustic_enforce_free_surf_cuda_(long *Mesh_pointer, int *, int *compute_wavefield_2) {
+  const char *R = "acoustic_enforce_free_surf_cuda";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (*compute_wavefield_2) unsupported(R, KERNEL_RUN);
+  const bool fluid_only = m->nspec_acoustic == m->nspec;
+  if (!(m->ac_phase == 2 || m->ac_phase == 4 || (fluid_only && m->ac_phase == 0 && m->steps > 0)))
+    stop(R, "called outside a time step");
+}
+
+// compute_forces_acoustic_cuda (src/gpu/compute_forces_acoustic_cuda.cu:248):
+// outer then inner elements; with one process the fused step covers both
+void compute_forces_acoustic_cuda_(long *Mesh_pointer, int *iphase, int *, int *, int *ATTENUATION_VISCOACOUSTIC, int *,
+                                   int *compute_wavefield_2) {
+  const char *R = "compute_forces_acoustic_cuda";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (*compute_wavefield_2) unsupported(R, KERNEL_RUN);
+  if (*ATTENUATION_VISCOACOUSTIC) stop(R, "viscoacoustic attenuation is not provided");
+  if (*iphase == 1 && m->ac_phase == 2)
+    m->ac_phase = 3;
+  else if (!(*iphase == 2 && m->ac_phase == 3))
+    stop(R, "called out of the order update_displacement_*_cuda, iphase 1, iphase 2, kernel_3_acoustic_cuda");
+}
+
+// compute_stacey_acoustic_cuda (src/gpu/compute_stacey_acoustic_cuda.cu:40)
+void compute_stacey_acoustic_cuda_(long *Mesh_pointer, int *, realw *, realw *, realw *, realw *, int *,
+                                   int *compute_wavefield_2, int *) {
+  fluid_phase_call("compute_stacey_acoustic_cuda", mesh_of("compute_stacey_acoustic_cuda", Mesh_pointer),
+                   compute_wavefield_2);
+}
+
+// compute_coupling_ac_el_cuda (src/gpu/compute_coupling_cuda.cu:47): the solid's
+// normal displacement on the fluid, part of the fused step
+void compute_coupling_ac_el_cuda_(long *Mesh_pointer, int *, int *, int *FORWARD_OR_ADJOINT) {
+  const char *R = "compute_coupling_ac_el_cuda";
+  if (*FORWARD_OR_ADJOINT != 1) unsupported(R, KERNEL_RUN);
+  fluid_phase_call(R, mesh_of(R, Mesh_pointer), nullptr);
+}
+
+// compute_add_sources_ac_cuda (src/gpu/compute_add_sources_viscoacoustic_cuda.cu:46)
+void compute_add_sources_ac_cuda_(long *Mesh_pointer, int *, int *itf) {
+  const char *R = "compute_add_sources_ac_cuda";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  fluid_phase_call(R, m, nullptr);
+  if (*itf != m->steps + 1) stop(R, "time step " + std::to_string(*itf) + " out of sequence");
+}
+
+// kernel_3_acoustic_cuda (src/gpu/update_displacement_cuda.cu:322): ends the
+// fluid step; on a fluid-only mesh the fused step is queued here
+void kernel_3_acoustic_cuda_(long *Mesh_pointer, realw *, realw *, int *, int *compute_wavefield_2) {
+  const char *R = "kernel_3_acoustic_cuda";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  fluid_phase_call(R, m, compute_wavefield_2);
+  if (m->nspec_acoustic == m->nspec) {
+    check(R, sf2d_coupled_enqueue(m->C, 1));
+    ++m->steps;
+    m->ac_phase = 0;
+    return;
+  }
+  m->ac_phase = 4;
+}
+
+// compute_coupling_el_ac_cuda (src/gpu/compute_coupling_cuda.cu:125): the fluid
+// pressure on the solid, part of the fused step
+void compute_coupling_el_ac_cuda_(long *Mesh_pointer, int *, int *, int *FORWARD_OR_ADJOINT) {
+  const char *R = "compute_coupling_el_ac_cuda";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (*FORWARD_OR_ADJOINT != 1) unsupported(R, KERNEL_RUN);
+  if (m->ac_phase != 5) stop(R, "called outside the solid forces of a time step");
+}
+
+// get_norm_acoustic_from_device (src/gpu/check_fields_cuda.cu:240): max |chi|
+void get_norm_acoustic_from_device_(realw *norm, long *Mesh_pointer, const int *FORWARD_OR_ADJOINT) {
+  const char *R = "get_norm_acoustic_from_device";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (FORWARD_OR_ADJOINT && *FORWARD_OR_ADJOINT == 3) unsupported(R, KERNEL_RUN);
+  if (!m->fluid) stop(R, "the mesh has no fluid element");
+  std::vector<float> p(m->nglob);
+  coupled_fields(R, m, nullptr, nullptr, nullptr, p.data(), nullptr, nullptr);
+  float mx = 0.f;
+  for (float x : p) mx = std::max(mx, std::fabs(x));
+  *norm = mx;
+}
+
+// transfer_fields_ac_{to,from}_device, transfer_dot_dot_from_device
+// (src/gpu/transfer_fields_cuda.cu:223-300): whole-mesh potentials
+void transfer_fields_ac_to_device_(int *size, realw *potential_acoustic, realw *potential_dot_acoustic,
+                                   realw *potential_dot_dot_acoustic, long *Mesh_pointer) {
+  const char *R = "transfer_fields_ac_to_device";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  need_ac_size(R, m, size);
+  coupled_set(R, m, nullptr, nullptr, nullptr, potential_acoustic, potential_dot_acoustic, potential_dot_dot_acoustic);
+}
+
+void transfer_fields_ac_from_device_(int *size, realw *potential_acoustic, realw *potential_dot_acoustic,
+                                     realw *potential_dot_dot_acoustic, long *Mesh_pointer) {
+  const char *R = "transfer_fields_ac_from_device";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  need_ac_size(R, m, size);
+  coupled_fields(R, m, nullptr, nullptr, nullptr, potential_acoustic, potential_dot_acoustic,
+                 potential_dot_dot_acoustic);
+}
+
+void transfer_dot_dot_from_device_(int *size, realw *potential_dot_dot_acoustic, long *Mesh_pointer) {
+  const char *R = "transfer_dot_dot_from_device";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  need_ac_size(R, m, size);
+  coupled_fields(R, m, nullptr, nullptr, nullptr, nullptr, nullptr, potential_dot_dot_acoustic);
+}
+
 // ---- not provided ----
 void transfer_boun_pot_from_device_(long*, realw*, const int*) { unsupported("transfer_boun_pot_from_device", MPI); }
 void transfer_asmbl_pot_to_device_(long*, realw*, const int*) { unsupported("transfer_asmbl_pot_to_device", MPI); }
@@ -638,7 +1222,6 @@ void prepare_boundary_on_device_(long*) { unsupported("prepare_boundary_on_devic
 void transfer_boundary_to_device_a_(long*, realw*, const int*) { unsupported("transfer_boundary_to_device_a", MPI); }
 void transfer_asmbl_accel_to_device_(long*, realw*, const int*, const int*, const int*, const int*) { unsupported("transfer_asmbl_accel_to_device", MPI); }
 void sync_copy_from_device_(long*, int*, realw*) { unsupported("sync_copy_from_device", MPI); }
-void get_norm_acoustic_from_device_(realw*, long*, const int*) { unsupported("get_norm_acoustic_from_device", FLUID); }
 void get_max_accel_(int*, int*, long*) { unsupported("get_max_accel", DEBUG); }
 void check_max_norm_displ_gpu_(int*, realw*, long*, int*) { unsupported("check_max_norm_displ_gpu", DEBUG); }
 void check_max_norm_vector_(int*, realw*, int*) { unsupported("check_max_norm_vector", DEBUG); }
@@ -649,26 +1232,19 @@ void check_max_norm_b_veloc_gpu_(int*, realw*, long*, int*) { unsupported("check
 void check_max_norm_b_displ_(int*, realw*, int*) { unsupported("check_max_norm_b_displ", DEBUG); }
 void check_max_norm_b_accel_(int*, realw*, int*) { unsupported("check_max_norm_b_accel", DEBUG); }
 void check_error_vectors_(int*, realw*, realw*) { unsupported("check_error_vectors", DEBUG); }
-void compute_add_sources_ac_cuda_(long*, int*, int*) { unsupported("compute_add_sources_ac_cuda", FLUID); }
 void compute_add_sources_ac_s3_cuda_(long*, int*, int*) { unsupported("compute_add_sources_ac_s3_cuda", KERNEL_RUN); }
 void compute_add_moving_sources_ac_cuda_(long*, int*, int*, int*, int*, int*) { unsupported("compute_add_moving_sources_ac_cuda", OTHER); }
 void add_sources_ac_sim_2_or_3_cuda_(long*, int*, int*, int*, int*) { unsupported("add_sources_ac_sim_2_or_3_cuda", KERNEL_RUN); }
 void compute_add_sources_el_s3_cuda_(long*, int*, int*) { unsupported("compute_add_sources_el_s3_cuda", KERNEL_RUN); }
 void add_sources_el_sim_type_2_or_3_(long*, int*, int*, int*, int*) { unsupported("add_sources_el_sim_type_2_or_3", KERNEL_RUN); }
-void compute_coupling_ac_el_cuda_(long*, int*, int*, int*) { unsupported("compute_coupling_ac_el_cuda", FLUID); }
-void compute_coupling_el_ac_cuda_(long*, int*, int*, int*) { unsupported("compute_coupling_el_ac_cuda", FLUID); }
-void compute_forces_acoustic_cuda_(long*, int*, int*, int*, int*, int*, int*) { unsupported("compute_forces_acoustic_cuda", FLUID); }
 void compute_kernels_elastic_cuda_(long*, realw*) { unsupported("compute_kernels_elastic_cuda", KERNEL_RUN); }
 void compute_kernels_acoustic_cuda_(long*, realw*) { unsupported("compute_kernels_acoustic_cuda", KERNEL_RUN); }
 void compute_kernels_hess_cuda_(long*, int*, int*) { unsupported("compute_kernels_hess_cuda", OTHER); }
-void compute_stacey_acoustic_cuda_(long*, int*, realw*, realw*, realw*, realw*, int*, int*, int*) { unsupported("compute_stacey_acoustic_cuda", FLUID); }
-void acoustic_enforce_free_surf_cuda_(long*, int*, int*) { unsupported("acoustic_enforce_free_surf_cuda", FLUID); }
-void pml_boundary_acoustic_cuda_(long*, int*, int*) { unsupported("pml_boundary_acoustic_cuda", FLUID); }
-void prepare_fields_acoustic_device_(long*, realw*, realw*, realw*, int*, int*, int*, int*, int*, int*, int*, int*, int*, realw*, realw*, int*, int*, int*, realw*, realw*, int*, realw*) { unsupported("prepare_fields_acoustic_device", FLUID); }
+void pml_boundary_acoustic_cuda_(long*, int*, int*) { unsupported("pml_boundary_acoustic_cuda", PML); }
 void prepare_fields_acoustic_adj_dev_(long*, int*, int*, int*) { unsupported("prepare_fields_acoustic_adj_dev", KERNEL_RUN); }
 void prepare_fields_elastic_adj_dev_(long*, int*, int*, int*, int*) { unsupported("prepare_fields_elastic_adj_dev", KERNEL_RUN); }
 void prepare_sim2_or_3_const_device_(long*, int*, realw*, int*) { unsupported("prepare_sim2_or_3_const_device", KERNEL_RUN); }
-void prepare_pml_device_(long*, int*, int*, int*, int*, int*, realw*, realw*, realw*, realw*, realw*, realw*, realw*, realw*, int*, int*) { unsupported("prepare_pml_device", FLUID); }
+void prepare_pml_device_(long*, int*, int*, int*, int*, int*, realw*, realw*, realw*, realw*, realw*, realw*, realw*, realw*, int*, int*) { unsupported("prepare_pml_device", PML); }
 void prepare_moving_sources_cuda_(long*, int*, int*, realw*, int*, int*, realw*) { unsupported("prepare_moving_sources_cuda", OTHER); }
 void prepare_arrays_gpu_(long*, realw*, realw*, realw*, realw*, realw*, realw*, int*, int*, realw*) { unsupported("prepare_arrays_gpu", OTHER); }
 void compute_smooth_(long*, realw*, realw*, realw*, realw*, const int*) { unsupported("compute_smooth", OTHER); }
@@ -678,13 +1254,10 @@ void transfer_b_fields_from_device_(int*, realw*, realw*, realw*, long*) { unsup
 void transfer_b_accel_from_device_(int*, realw*, long*) { unsupported("transfer_b_accel_from_device", KERNEL_RUN); }
 void transfer_b_displ_from_device_(int*, realw*, long*) { unsupported("transfer_b_displ_from_device", KERNEL_RUN); }
 void transfer_kernels_el_to_host_(long*, realw*, realw*, realw*, int*) { unsupported("transfer_kernels_el_to_host", KERNEL_RUN); }
-void transfer_fields_ac_to_device_(int*, realw*, realw*, realw*, long*) { unsupported("transfer_fields_ac_to_device", FLUID); }
 void transfer_b_fields_ac_to_device_(int*, realw*, realw*, realw*, long*) { unsupported("transfer_b_fields_ac_to_device", KERNEL_RUN); }
-void transfer_fields_ac_from_device_(int*, realw*, realw*, realw*, long*) { unsupported("transfer_fields_ac_from_device", FLUID); }
 void transfer_b_fields_ac_from_device_(int*, realw*, realw*, realw*, long*) { unsupported("transfer_b_fields_ac_from_device", KERNEL_RUN); }
 void transfer_b_potential_ac_from_device_(int*, realw*, long*) { unsupported("transfer_b_potential_ac_from_device", KERNEL_RUN); }
 void transfer_b_potential_ac_to_device_(int*, realw*, long*) { unsupported("transfer_b_potential_ac_to_device", KERNEL_RUN); }
-void transfer_dot_dot_from_device_(int*, realw*, long*) { unsupported("transfer_dot_dot_from_device", FLUID); }
 void transfer_b_dot_dot_from_device_(int*, realw*, long*) { unsupported("transfer_b_dot_dot_from_device", KERNEL_RUN); }
 void transfer_kernels_ac_to_host_(long*, realw*, realw*, int*) { unsupported("transfer_kernels_ac_to_host", KERNEL_RUN); }
 void transfer_kernels_hess_el_tohost_(long*, realw*, int*) { unsupported("transfer_kernels_hess_el_tohost", OTHER); }
@@ -697,8 +1270,6 @@ void transfer_async_pot_ac_from_device_(realw*, long*) { unsupported("transfer_a
 void transfer_async_pot_ac_to_device_(realw*, long*) { unsupported("transfer_async_pot_ac_to_device", MPI); }
 void transfer_compute_kernel_answers_from_device_(long*, realw*, int*, realw*, int*, realw*, int*) { unsupported("transfer_compute_kernel_answers_from_device", KERNEL_RUN); }
 void transfer_compute_kernel_fields_from_device_(long*, realw*, int*, realw*, int*, realw*, realw*, realw*, realw*, realw*, int*, realw*, realw*, realw*, realw*, realw*, int*, realw*, int*, realw*, int*, realw*, int*, realw*, realw*, int*) { unsupported("transfer_compute_kernel_fields_from_device", KERNEL_RUN); }
-void update_displacement_ac_cuda_(long*, realw*, realw*, realw*, realw*, realw*, realw*, int*, int*) { unsupported("update_displacement_ac_cuda", FLUID); }
 void kernel_3_b_cuda_(long*, realw*, realw*) { unsupported("kernel_3_b_cuda", KERNEL_RUN); }
-void kernel_3_acoustic_cuda_(long*, realw*, realw*, int*, int*) { unsupported("kernel_3_acoustic_cuda", FLUID); }
 
 }  // extern "C"

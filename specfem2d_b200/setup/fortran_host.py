@@ -2,9 +2,11 @@
 memory order, for driving include/sf2d_fortran.h the way SPECFEM2D does.
 
 Restates what src/specfem2D/prepare_gpu.f90 passes to prepare_constants_device,
-prepare_fields_elastic_device and prepare_Stacey_device (init_host_to_dev_variable,
-:346-470: local sources and their time functions, receiver rotations as
-CUSTOM_REAL) and the absorbing-face arrays of prepare_timerun.F90:1270-1440
+prepare_fields_acoustic_device, prepare_fields_elastic_device and
+prepare_Stacey_device (init_host_to_dev_variable, :346-640: local sources and
+their time functions, receiver rotations as CUSTOM_REAL, the free-surface faces
+and the fluid-solid faces with the fluid element's normals and jacobian1D * w)
+and the absorbing-face arrays of prepare_timerun.F90:1270-1440
 (abs_boundary_ij with NGLLX + 1 marking a corner point that the neighbouring
 face covers, outward normals, jacobian1D * w, edge_abs = 1 bottom, 2 right,
 3 top, 4 left).  Every array is a C-contiguous numpy array whose memory
@@ -15,6 +17,7 @@ from __future__ import annotations
 
 import numpy as np
 
+from . import acoustic as ac_setup
 from .gll import NGLL
 from .mesh import IBOTTOM, ILEFT, IRIGHT, ITOP
 from .solver_setup import edge_normal
@@ -29,7 +32,10 @@ def _fortran(a, dtype):
 def abs_boundary_arrays(db):
     """abs_boundary_ispec, abs_boundary_ij (2, NGLLX, nface), abs_boundary_normal
     (2, NGLLX, nface), abs_boundary_jacobian1Dw (NGLLX, nface), edge_abs and the
-    per-side face counts, for the absorbing faces of db.mesh."""
+    per-side face counts, for the absorbing faces of db.mesh.  On a fluid face
+    every point the fluid Stacey loop skips (ibegin/iend_edge: corners and
+    points shared with a fluid-solid edge) is marked NGLLX + 1
+    (prepare_timerun.F90:1330-1420)."""
     mesh = db.mesh
     geo = dict(xix=db.xix, xiz=db.xiz, gammax=db.gammax, gammaz=db.gammaz, jacobian=db.jacobian)
     nf = 0 if mesh.abs_ispec is None else len(mesh.abs_ispec)
@@ -57,6 +63,17 @@ def abs_boundary_arrays(db):
                 ij[k, 0, 0] = NGLL + 1
             if c[3]:
                 ij[k, NGLL - 1, 0] = NGLL + 1
+    if db.acoustic is not None and nf:
+        is_ac = np.asarray(db.acoustic["ispec"], dtype=bool)
+        cpl = ac_setup.coupling_edges(db.ibool, is_ac) if (~is_ac).any() else []
+        for (k, e, t, pts) in ac_setup.absorbing_ranges(mesh, cpl):
+            if not is_ac[e]:
+                continue
+            keep = set(pts)
+            for p in range(NGLL):
+                i, j = ij[k, p] - 1
+                if (int(i), int(j)) not in keep and i < NGLL and j < NGLL:
+                    ij[k, p, 1 if t in (ILEFT, IRIGHT) else 0] = NGLL + 1
     counts = {name: int(np.sum(edge == code)) for name, code in
               (("bottom", IBOTTOM), ("left", ILEFT), ("right", IRIGHT), ("top", ITOP))}
     return dict(abs_boundary_ispec=ispec, abs_boundary_ij=ij, abs_boundary_normal=normal,
@@ -92,9 +109,12 @@ def gpu_arrays(db, nlength_seismogram: int | None = None):
         rmassx=_fortran(db.rmass_inverse_elastic[:, 0], f32),
         rmassz=_fortran(db.rmass_inverse_elastic[:, 1], f32),
         deltat=f32(db.deltat), deltatover2=f32(db.deltatover2), deltatsquareover2=f32(db.deltatsquareover2),
-        stacey=bool(db.stacey_iglob.size > 0),
+        stacey=bool(db.stacey_iglob.size > 0
+                    or (db.acoustic is not None and len(db.acoustic["st_iglob"]) > 0)),
     )
     out["abs"] = abs_boundary_arrays(db)
+    if db.acoustic is not None:
+        out.update(fluid_arrays(db))
     if db.aniso is not None:
         out["ispec_is_anisotropic"] = _fortran(db.aniso["ispec"], np.int32)
         for k in ("c11", "c13", "c15", "c33", "c35", "c55"):
@@ -104,3 +124,40 @@ def gpu_arrays(db, nlength_seismogram: int | None = None):
         for k in ("a1", "b1", "a2", "b2"):
             out["att_" + k] = _fortran(db.atten[k], f32)
     return out
+
+
+def fluid_arrays(db):
+    """prepare_fields_acoustic_device's arrays: ispec_is_acoustic, the fluid
+    mass matrix, rhostore, the free-surface faces (free_ac_ispec and
+    free_surface_ij (2, NGLLX, nface) as prepare_gpu.f90:549-580 spans each
+    listed edge) and the fluid-solid faces (coupling_ac_el_ispec, _ij, _normal
+    and _jacobian1Dw from the fluid element's edge, prepare_gpu.f90:586-640)."""
+    is_ac = np.asarray(db.acoustic["ispec"], dtype=bool)
+    mesh = db.mesh
+    rows = mesh.free_edges if mesh.free_edges is not None else ac_setup.structured_free_edges(mesh, is_ac)
+    rows = [r for r in rows if is_ac[r[0]]]
+    free_ispec = np.array([r[0] + 1 for r in rows], np.int32)
+    free_ij = np.zeros((len(rows), NGLL, 2), np.int32)
+    for k, (e, i0, i1, j0, j1) in enumerate(rows):
+        ii = [i0] * NGLL if i0 == i1 else list(range(i0, i1 + 1))
+        jj = [j0] * NGLL if j0 == j1 else list(range(j0, j1 + 1))
+        free_ij[k, :, 0] = np.array(ii) + 1
+        free_ij[k, :, 1] = np.array(jj) + 1
+    geo = dict(xix=db.xix, xiz=db.xiz, gammax=db.gammax, gammaz=db.gammaz, jacobian=db.jacobian)
+    edges = ac_setup.coupling_edges(db.ibool, is_ac) if (~is_ac).any() else []
+    n = len(edges)
+    c_ispec = np.zeros(n, np.int32)
+    c_ij = np.zeros((n, NGLL, 2), np.int32)
+    c_normal = np.zeros((n, NGLL, 2), f32)
+    c_jw = np.zeros((n, NGLL), f32)
+    for k, (ea, edge_a, _, _) in enumerate(edges):
+        c_ispec[k] = ea + 1
+        for p in range(NGLL):
+            i, j = ac_setup._ivalue(p, edge_a)
+            c_ij[k, p] = (i + 1, j + 1)
+            c_normal[k, p, 0], c_normal[k, p, 1], c_jw[k, p] = ac_setup._edge_normal(geo, ea, i, j, edge_a, db.gll)
+    return dict(ispec_is_acoustic=_fortran(is_ac, np.int32), nspec_acoustic=int(is_ac.sum()),
+                rmass_acoustic=_fortran(db.acoustic["rmass"], f32), rhostore=_fortran(db.rhostore, f32),
+                free_ac_ispec=free_ispec, free_surface_ij=free_ij, nfree=len(rows),
+                coupling_ac_el_ispec=c_ispec, coupling_ac_el_ij=c_ij, coupling_ac_el_normal=c_normal,
+                coupling_ac_el_jacobian1Dw=c_jw, ncoupling=n)

@@ -3,14 +3,19 @@
 with arguments passed by reference as gfortran passes them:
 
 * prepare_GPU (src/specfem2D/prepare_gpu.f90:34-320): initialize_cuda_device,
-  prepare_constants_device, prepare_fields_elastic_device, prepare_Stacey_device,
-  transfer_fields_el_to_device;
+  prepare_constants_device, prepare_fields_acoustic_device (fluid elements),
+  prepare_fields_elastic_device (solid elements), prepare_Stacey_device,
+  transfer_fields_el_to_device / transfer_fields_ac_to_device;
 * each time step it = 1..NSTEP (iterate_time.F90:146-260):
-  update_displacement_cuda (update_displacement_Newmark.F90:530-549), then
-  compute_forces_viscoelastic_GPU (compute_gpu_elastic.f90:36-215): forces for
-  iphase 1 with Stacey and sources, forces for iphase 2, kernel_3_a_cuda; then
-  write_seismograms (write_seismograms.F90:199-205) and, every `check_every`
-  steps, check_stability's get_norm_elastic_from_device;
+  update_displacement_ac_cuda and update_displacement_cuda
+  (update_displacement_Newmark.F90:150-240, 500-549); with fluid elements
+  compute_forces_viscoacoustic_GPU (compute_gpu_acoustic.f90:36-180): the
+  free-surface call, forces for iphase 1 with Stacey, coupling and sources,
+  forces for iphase 2, kernel_3_acoustic_cuda, the free-surface call again;
+  with solid elements compute_forces_viscoelastic_GPU (compute_gpu_elastic.f90:36-215):
+  forces for iphase 1 with Stacey, coupling and sources, forces for iphase 2,
+  kernel_3_a_cuda; then write_seismograms (write_seismograms.F90:199-205) and,
+  every `check_every` steps, check_stability's get_norm_*_from_device;
 * prepare_cleanup_device.
 """
 from __future__ import annotations
@@ -50,7 +55,9 @@ class _Refs:
 
 
 def run_forward(db, nstep=None, check_every=1000, nlength_seismogram=None):
-    """Returns (seismograms (nrec, nstep, 2) float64, final displacement (nglob, 2), norms)."""
+    """Returns (seismograms (nrec, nstep, 2) float64, final displacement (nglob, 2), norms);
+    with fluid elements the norms are (solid, fluid) pairs and the final potential
+    follows as a fourth value."""
     lib = _lib()
     A = gpu_arrays(db, nlength_seismogram)
     nstep = int(nstep or A["nstep"])
@@ -62,6 +69,10 @@ def run_forward(db, nstep=None, check_every=1000, nlength_seismogram=None):
     lib.initialize_cuda_device_(r.i(0), ctypes.byref(ndev))
     dummy_i = np.zeros(1, np.int32)
     dummy_f = np.zeros(1, np.float32)
+    fluid = "ispec_is_acoustic" in A
+    nac = A["nspec_acoustic"] if fluid else 0
+    is_ac = A["ispec_is_acoustic"] if fluid else np.zeros(A["nspec"], np.int32)
+    elastic = nac < A["nspec"]
     lib.prepare_constants_device_(
         M, r.i(5), r.i(A["nspec"]), r.i(A["nglob"]),
         r.a(A["xix"]), r.a(A["xiz"]), r.a(A["gammax"]), r.a(A["gammaz"]),
@@ -72,16 +83,25 @@ def run_forward(db, nstep=None, check_every=1000, nlength_seismogram=None):
         r.i(A["nsrc"]), r.a(A["sourcearrays"]), r.a(A["source_time_function"]),
         r.i(A["nstep"]), r.a(A["ispec_selected_source"]), r.a(A["ispec_selected_rec_loc"]),
         r.i(A["nrec"]), r.a(A["cosrot"]), r.a(A["sinrot"]),
-        r.i(1), r.i(1), r.i(0), r.i(A["nspec"]),
-        r.a(np.zeros(A["nspec"], np.int32)), r.a(np.ones(A["nspec"], np.int32)),
+        r.i(1), r.i(1), r.i(nac), r.i(A["nspec"] - nac),
+        r.a(is_ac), r.a((1 - is_ac).astype(np.int32)),
         r.i(0), r.i(0),
         r.a(A["xir_store"]), r.a(A["gammar_store"]),
         r.i(1), r.a(np.array([A["seismotype"]], np.int32)), r.i(nlen))
+    if fluid:
+        lib.prepare_fields_acoustic_device_(
+            M, r.a(A["rmass_acoustic"]), r.a(A["rhostore"]), r.a(A["kappastore"]),
+            r.i(nac), r.a(np.concatenate([np.zeros(nac, np.int32), np.flatnonzero(is_ac).astype(np.int32) + 1])),
+            r.i(A["nfree"]), r.a(A["free_ac_ispec"]), r.a(A["free_surface_ij"]),
+            r.i(int(elastic)), r.i(A["ncoupling"]), r.a(A["coupling_ac_el_ispec"]), r.a(A["coupling_ac_el_ij"]),
+            r.a(A["coupling_ac_el_normal"]), r.a(A["coupling_ac_el_jacobian1Dw"]),
+            r.i(0), r.a(dummy_i), r.i(0), r.a(dummy_f), r.a(dummy_f), r.i(0), r.a(dummy_f))
     aniso = "ispec_is_anisotropic" in A
     atten = "att_a1" in A
     c = {k: (A[k + "store"] if aniso else dummy_f) for k in ("c11", "c13", "c15", "c33", "c35", "c55")}
     att = {k: (A["att_" + k] if atten else dummy_f) for k in ("a1", "b1", "a2", "b2")}
-    lib.prepare_fields_elastic_device_(
+    prepare_el = lib.prepare_fields_elastic_device_ if elastic else (lambda *a: None)
+    prepare_el(
         M, r.a(A["rmassx"]), r.a(A["rmassz"]), r.i(A["nspec"]), r.a(np.arange(1, A["nspec"] + 1, dtype=np.int32)),
         r.a(A["ispec_is_anisotropic"] if aniso else dummy_i), r.i(1 if aniso else 0),
         r.a(c["c11"]), r.a(dummy_f), r.a(c["c13"]), r.a(c["c15"]), r.a(dummy_f), r.a(dummy_f),
@@ -91,14 +111,18 @@ def run_forward(db, nstep=None, check_every=1000, nlength_seismogram=None):
     if A["stacey"]:
         ab = A["abs"]
         lib.prepare_stacey_device_(
-            M, r.i(0), r.i(1), r.a(A["rho_vpstore"]), r.a(A["rho_vsstore"]),
+            M, r.i(int(fluid)), r.i(int(elastic)), r.a(A["rho_vpstore"]), r.a(A["rho_vsstore"]),
             r.i(ab["counts"]["bottom"]), r.i(ab["counts"]["left"]), r.i(ab["counts"]["right"]),
             r.i(ab["counts"]["top"]), r.a(ab["abs_boundary_ispec"]), r.a(ab["abs_boundary_ij"]),
             r.a(ab["abs_boundary_normal"]), r.a(ab["abs_boundary_jacobian1Dw"]), r.i(ab["nface"]),
             r.a(ab["edge_abs"]), r.a(dummy_i), r.a(dummy_i), r.a(dummy_i), r.a(dummy_i))
     ng2 = 2 * A["nglob"]
     zeros = np.zeros(ng2, np.float32)
-    lib.transfer_fields_el_to_device_(r.i(ng2), r.a(zeros), r.a(zeros.copy()), r.a(zeros.copy()), M)
+    if elastic:
+        lib.transfer_fields_el_to_device_(r.i(ng2), r.a(zeros), r.a(zeros.copy()), r.a(zeros.copy()), M)
+    if fluid:
+        z1 = np.zeros(A["nglob"], np.float32)
+        lib.transfer_fields_ac_to_device_(r.i(A["nglob"]), r.a(z1), r.a(z1.copy()), r.a(z1.copy()), M)
     sisux = np.zeros((A["nrec"], nlen), np.float64)
     sisuz = np.zeros_like(sisux)
     seis = np.zeros((A["nrec"], nstep, 2))
@@ -111,11 +135,32 @@ def run_forward(db, nstep=None, check_every=1000, nlength_seismogram=None):
     norms = []
     dummy_b = dummy_f.ctypes.data_as(ctypes.c_void_p)
     seismo_current = 0
+    ncpl_c = ctypes.c_int(A.get("ncoupling", 0))
     for it in range(1, nstep + 1):
         it_c.value = it
-        lib.update_displacement_cuda_(M, ctypes.byref(dt), ctypes.byref(dtsq2), ctypes.byref(dt2),
-                                      ctypes.byref(dt), ctypes.byref(dtsq2), ctypes.byref(dt2))
-        for iphase in (one, two):
+        if fluid:
+            lib.update_displacement_ac_cuda_(M, ctypes.byref(dt), ctypes.byref(dtsq2), ctypes.byref(dt2),
+                                             ctypes.byref(dt), ctypes.byref(dtsq2), ctypes.byref(dt2),
+                                             ctypes.byref(one), ctypes.byref(zero))
+        if elastic:
+            lib.update_displacement_cuda_(M, ctypes.byref(dt), ctypes.byref(dtsq2), ctypes.byref(dt2),
+                                          ctypes.byref(dt), ctypes.byref(dtsq2), ctypes.byref(dt2))
+        if fluid:
+            if A["nfree"] > 0:
+                lib.acoustic_enforce_free_surf_cuda_(M, ctypes.byref(one), ctypes.byref(zero))
+            for iphase in (one, two):
+                lib.compute_forces_acoustic_cuda_(M, ctypes.byref(iphase), ctypes.byref(zero), ctypes.byref(zero),
+                                                  ctypes.byref(zero), ctypes.byref(one), ctypes.byref(zero))
+                if iphase is one:
+                    if A["stacey"]:
+                        lib.compute_stacey_acoustic_cuda_(M, ctypes.byref(one), dummy_b, dummy_b, dummy_b, dummy_b,
+                                                          ctypes.byref(one), ctypes.byref(zero), ctypes.byref(zero))
+                    if elastic:
+                        lib.compute_coupling_ac_el_cuda_(M, ctypes.byref(one), ctypes.byref(ncpl_c), ctypes.byref(one))
+                    lib.compute_add_sources_ac_cuda_(M, ctypes.byref(one), ctypes.byref(it_c))
+            lib.kernel_3_acoustic_cuda_(M, ctypes.byref(dt2), ctypes.byref(dt2), ctypes.byref(one), ctypes.byref(zero))
+            lib.acoustic_enforce_free_surf_cuda_(M, ctypes.byref(one), ctypes.byref(zero))
+        for iphase in ((one, two) if elastic else ()):
             lib.compute_forces_viscoelastic_cuda_(M, ctypes.byref(iphase), ctypes.byref(dt), ctypes.byref(zero),
                                                   ctypes.byref(nspec_c), ctypes.byref(aniso_c), ctypes.byref(atten_c),
                                                   ctypes.byref(one), ctypes.byref(zero))
@@ -123,8 +168,11 @@ def run_forward(db, nstep=None, check_every=1000, nlength_seismogram=None):
                 if A["stacey"]:
                     lib.compute_stacey_viscoelastic_cuda_(M, ctypes.byref(one), dummy_b, dummy_b, dummy_b, dummy_b,
                                                           ctypes.byref(one), ctypes.byref(zero), ctypes.byref(zero))
+                if fluid:
+                    lib.compute_coupling_el_ac_cuda_(M, ctypes.byref(one), ctypes.byref(ncpl_c), ctypes.byref(one))
                 lib.compute_add_sources_el_cuda_(M, ctypes.byref(one), ctypes.byref(it_c))
-        lib.kernel_3_a_cuda_(M, ctypes.byref(dt2), ctypes.byref(dt2), ctypes.byref(one), ctypes.byref(zero))
+        if elastic:
+            lib.kernel_3_a_cuda_(M, ctypes.byref(dt2), ctypes.byref(dt2), ctypes.byref(one), ctypes.byref(zero))
         seismo_current += 1
         cur_c.value = seismo_current
         lib.compute_seismograms_cuda_(M, ctypes.byref(one), sisux.ctypes.data_as(ctypes.c_void_p),
@@ -140,9 +188,20 @@ def run_forward(db, nstep=None, check_every=1000, nlength_seismogram=None):
             seismo_current = 0
         if it % check_every == 0 or it == nstep:
             lib.get_norm_elastic_from_device_(ctypes.byref(norm), M, ctypes.byref(one))
-            norms.append(float(norm.value))
+            if fluid:
+                n_el = float(norm.value)
+                lib.get_norm_acoustic_from_device_(ctypes.byref(norm), M, ctypes.byref(one))
+                norms.append((n_el, float(norm.value)))
+            else:
+                norms.append(float(norm.value))
     displ = np.zeros(ng2, np.float32)
     lib.transfer_displ_from_device_(r.i(ng2), r.a(displ), M)
+    pot = None
+    if fluid:
+        pot = np.zeros(A["nglob"], np.float32)
+        lib.transfer_fields_ac_from_device_(r.i(A["nglob"]), r.a(pot), r.a(np.zeros_like(pot)), r.a(np.zeros_like(pot)), M)
     lib.prepare_cleanup_device_(M, r.i(0), r.i(1), r.i(int(aniso)), r.i(0), r.i(0), r.i(int(atten)), r.i(0),
                                 r.a(dummy_f))
+    if fluid:
+        return seis, displ.reshape(-1, 2), norms, pot
     return seis, displ.reshape(-1, 2), norms

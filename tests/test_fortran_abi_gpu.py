@@ -59,3 +59,52 @@ def test_anisotropic_and_attenuating_examples_through_the_fortran_interface(name
     ref = o.run(db.nstep)
     assert rel_l2(seis, ref) < 1e-5
     assert rel_l2(displ, o.displ) < 1e-5
+
+
+def _ocean_db():
+    import os
+
+    cfg, seis = load_golden("tomographic_ocean_model")
+    t = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "tomographic_ocean_model_tomo.npz"))
+    return database_from_config(cfg, tomo=(t["x"], t["z"], t["vp"], t["vs"], t["rho"])), seis
+
+
+def test_coupled_ocean_through_the_fortran_interface():
+    """EXAMPLES/tomographic_ocean_model (fluid over rock: coupling both ways,
+    Stacey in both domains, a free sea surface, displacement receivers in both)
+    through prepare_fields_acoustic_device and compute_gpu_acoustic.f90's call
+    order: within the FP32 band of the FP64 oracle, and the reference's traces
+    as close as the coupled GPU solver gets them."""
+    import oracle
+
+    db, seis = _ocean_db()
+    out, displ, norms, pot = run_forward(db, check_every=400)
+    o32 = oracle.Oracle(db, 4)
+    ref32 = o32.run(db.nstep)
+    ref64 = oracle.Oracle(db, 8).run(db.nstep)
+    assert rel_l2(out, ref64) < 2.0 * rel_l2(ref32, ref64)
+    g, r = [], []
+    for k in (1, 3, 6, 9, 12, 14, 16, 18, 20, 22):
+        for c, ci in (("BXX", 0), ("BXZ", 1)):
+            g.append(out[k - 1, :, ci])
+            r.append(seis[f"S{k:04d}_{c}"])
+    assert rel_l2(np.concatenate(g), np.concatenate(r)) < 3e-5
+    assert rel_l2(pot, o32.get(oracle.POT)) < 1e-4
+    assert len(norms) == 4 and all(a > 0 and b > 0 for a, b in norms)
+
+
+def test_fluid_only_external_mesh_through_the_fortran_interface():
+    """EXAMPLES/Gmsh_example_Stacey_MPI (fluid only: the fused step is queued by
+    kernel_3_acoustic_cuda), pressure receivers, the listed free surface."""
+    import oracle
+
+    cfg, seis = load_golden("gmsh_stacey_external")
+    db = database_from_config(cfg)
+    out, _, norms, pot = run_forward(db, check_every=600)
+    o32 = oracle.Oracle(db, 4).run(db.nstep)
+    o64 = oracle.Oracle(db, 8).run(db.nstep)
+    for k in range(11):
+        band = rel_l2(o32[k, :, 0], o64[k, :, 0])
+        assert rel_l2(out[k, :, 0], o64[k, :, 0]) < 1.5 * band
+        assert rel_l2(out[k, :, 0], seis[f"S{k + 1:04d}_PRE"]) < 2.0 * band
+    assert np.all(out[:, :, 1] == 0.0) and norms[-1][0] == 0.0 and norms[-1][1] > 0

@@ -73,7 +73,8 @@ def test_library_exports_the_reference_fortran_interface():
 
 
 @pytest.mark.parametrize("call,needle", [
-    ("compute_forces_acoustic_cuda_", "sf2d_coupled_create"),
+    ("pml_boundary_acoustic_cuda_", "CPML layers"),
+    ("compute_forces_acoustic_cuda_", "Mesh_pointer was not prepared"),
     ("kernel_3_b_cuda_", "sf2d_fwi_create"),
     ("transfer_boun_accel_from_device_", "MPI"),
     ("update_displacement_cuda_", "Mesh_pointer was not prepared"),
