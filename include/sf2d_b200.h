@@ -247,6 +247,17 @@ int sf2d_fwi_hessian(sf2d_fwi *f, float *hess1, float *hess2);
  * the seismograms a kernel run writes (write_seismograms.F90:36-150 records
  * the adjoint field when SIMULATION_TYPE = 3). */
 int sf2d_fwi_adjoint_seismograms(sf2d_fwi *f, double *seismograms);
+/* The kernel integrand sums of the last sf2d_fwi_backward before the scaling of
+ * save_adjoint_kernels.f90:134-141 (nspec*25 each, element order): rho_kl =
+ * sum a_adj . b_u, kappa_kl = sum div u_adj div b_u, mu_kl = sum of the
+ * deviatoric strain products (compute_kernels.f90:75-292), as the reference's
+ * transfer_kernels_el_to_host hands them to the host. */
+int sf2d_fwi_kernel_sums(sf2d_fwi *f, float *rho_kl, float *kappa_kl, float *mu_kl);
+/* The adjoint wavefield at the end of the last sf2d_fwi_backward (each
+ * 2*nglob, may be NULL): displ_elastic, veloc_elastic and accel_elastic of a
+ * kernel run, as transfer_fields_el_from_device hands them to the host at its
+ * end (iterate_time.F90:462-504). */
+int sf2d_fwi_adjoint_fields(sf2d_fwi *f, float *displ, float *veloc, float *accel);
 int sf2d_fwi_destroy(sf2d_fwi *f);
 
 /* ---- kernel smoothing (post-gradient step) ----

@@ -43,8 +43,9 @@ enum Why { PML, KERNEL_RUN, MPI, DEBUG, OTHER };
   static const char *const text[] = {
       "CPML layers run through sf2d_elastic_create / sf2d_coupled_create with the descriptors' pml_* members "
       "(include/sf2d_b200.h, include/sf2d_coupled.h)",
-      "kernel runs use sf2d_fwi_create / sf2d_fwi_forward / sf2d_fwi_backward (include/sf2d_b200.h), which "
-      "replay the forward field from checkpoints instead of reconstructing it backwards",
+      "kernel runs replay the forward field from checkpoints instead of reconstructing it backwards: "
+      "SIMULATION_TYPE = 3 of solid meshes runs through this interface, the rest through sf2d_fwi_create / "
+      "sf2d_coupled_fwi_create (include/sf2d_b200.h, include/sf2d_coupled.h)",
       "this library runs one mesh per process: there is no MPI halo exchange",
       "debug helper not provided by libsf2d_b200",
       "not provided by libsf2d_b200"};
@@ -83,6 +84,18 @@ struct FortranMesh {
   // step bookkeeping of a coupled mesh: 0 between steps, 1 fluid predicted,
   // 2 solid predicted, 3 fluid forces, 4 fluid step done, 5 solid forces
   int ac_phase = 0;
+  // kernel run (SIMULATION_TYPE = 3, solid meshes): the checkpointed gradient
+  // (forward replay and adjoint sweep) runs in full when the first step
+  // starts; the calls of each step then follow it and hand out its results
+  int sim_type = 1;
+  bool adj_prepared = false;
+  int nspec_side[4] = {0, 0, 0, 0};  // absorbing faces bottom, left, right, top
+  sf2d_fwi *F = nullptr;
+  std::vector<float> adj_src;        // [irec][it][comp], forward time order
+  std::vector<double> adj_seis;      // adjoint traces [irec][it][comp]
+  std::vector<float> rho_sum, kappa_sum, mu_sum;
+  int kernel_calls = 0;              // compute_kernels_elastic_cuda calls
+  int srcs_added = 0;                // step of the last compute_add_sources_el_s3_cuda
 };
 
 FortranMesh *mesh_of(const char *routine, const long *p) {
@@ -217,8 +230,10 @@ void rebuild_centroids(FortranMesh &m) {
 
 void build_coupled(const char *routine, FortranMesh &m);
 
+void run_kernel_sweep(const char *routine, FortranMesh &m);
+
 void build_solver(const char *routine, FortranMesh &m) {
-  if (m.S || m.C) return;
+  if (m.S || m.C || m.F) return;
   if (m.fluid) {
     build_coupled(routine, m);
     return;
@@ -278,6 +293,10 @@ void build_solver(const char *routine, FortranMesh &m) {
     d.att_a2 = m.a2.data();
     d.att_b2 = m.b2.data();
   }
+  if (m.sim_type == 3) {
+    run_kernel_sweep(routine, m);
+    return;
+  }
   check(routine, sf2d_elastic_create(&d, &m.S));
   if (!m.staged_u.empty()) {
     check(routine, sf2d_set_fields(m.S, m.staged_u.data(), m.staged_v.data(), m.staged_a.data()));
@@ -285,6 +304,43 @@ void build_solver(const char *routine, FortranMesh &m) {
     m.staged_v.clear();
     m.staged_a.clear();
   }
+}
+
+// A kernel run in full (iterate_time.F90:146-400 with SIMULATION_TYPE = 3):
+// the forward field from rest with a checkpoint every min(NSTEP, 200) steps,
+// then the adjoint sweep, which injects source_adjoint(:, NSTEP-it+1) at step
+// it (compute_gpu_elastic.f90:283-311), replays each forward segment from its
+// checkpoint instead of reconstructing it backwards from the last frame and
+// the absorbed-boundary records, and sums the kernel integrands at every step
+// (compute_kernels_cudakernel, NTSTEP_BETWEEN_COMPUTE_KERNELS = 1).
+void run_kernel_sweep(const char *routine, FortranMesh &m) {
+  if (!m.adj_prepared) stop(routine, "prepare_fields_elastic_adj_dev has not been called");
+  if (m.nrec > 0 && m.adj_src.empty()) stop(routine, "prepare_sim2_or_3_const_device has not been called");
+  for (const std::vector<float> *f : {&m.staged_u, &m.staged_v, &m.staged_a})
+    for (float x : *f)
+      if (x != 0.f) stop(routine, "a kernel run starts from rest: the initial fields must be zero");
+  m.staged_u.clear();
+  m.staged_v.clear();
+  m.staged_a.clear();
+  const size_t nl = static_cast<size_t>(m.nspec) * NGLL2;
+  // rhostore/kappastore scale the kernels of sf2d_fwi_backward only; the host
+  // receives the unscaled sums and scales them itself (save_adjoint_kernels.f90)
+  const std::vector<float> ones(nl, 1.f);
+  check(routine, sf2d_fwi_create(&m.d, ones.data(), ones.data(), std::min(m.nstep, 200), &m.F));
+  int rc = sf2d_fwi_forward(m.F, nullptr);
+  if (rc == SF2D_ERR_UNSTABLE) stop(routine, "the forward wavefield of the kernel run became unstable and blew up");
+  check(routine, rc);
+  const float none = 0.f;
+  std::vector<float> rk(nl), kk(nl), mk(nl);
+  rc = sf2d_fwi_backward(m.F, m.adj_src.empty() ? &none : m.adj_src.data(), rk.data(), kk.data(), mk.data());
+  if (rc == SF2D_ERR_UNSTABLE) stop(routine, "the adjoint wavefield became unstable and blew up");
+  check(routine, rc);
+  m.adj_seis.assign(static_cast<size_t>(m.nrec) * m.nstep * 2, 0.0);
+  if (m.nrec) check(routine, sf2d_fwi_adjoint_seismograms(m.F, m.adj_seis.data()));
+  m.rho_sum.resize(nl);
+  m.kappa_sum.resize(nl);
+  m.mu_sum.resize(nl);
+  check(routine, sf2d_fwi_kernel_sums(m.F, m.rho_sum.data(), m.kappa_sum.data(), m.mu_sum.data()));
 }
 
 // The elements of one domain with a compact numbering of their points
@@ -611,6 +667,10 @@ void fields_from(const char *R, FortranMesh *m, const int *size, realw *displ, r
     check(R, sf2d_get_fields(m->S, displ, veloc, accel));
     return;
   }
+  if (m->F) {
+    check(R, sf2d_fwi_adjoint_fields(m->F, displ, veloc, accel));
+    return;
+  }
   const size_t n = static_cast<size_t>(*size);
   const bool staged = !m->staged_u.empty();
   for (auto pr : {std::make_pair(displ, &m->staged_u), std::make_pair(veloc, &m->staged_v),
@@ -675,10 +735,10 @@ void prepare_constants_device_(long *Mesh_pointer, int *h_NGLLX, int *NSPEC_AB, 
   if (!Mesh_pointer) stop(R, "null Mesh_pointer");
   if (*h_NGLLX != NGLL) stop(R, "NGLLX must be 5");
   if (!*P_SV) stop(R, "SH (membrane) waves are not provided: P_SV only");
-  if (*SIMULATION_TYPE != 1) unsupported(R, KERNEL_RUN);
-  if (*SAVE_FORWARD)
-    stop(R, "SAVE_FORWARD: the boundary values of a backward reconstruction are not produced; kernel runs use "
-            "sf2d_fwi_* (include/sf2d_b200.h)");
+  if (*SIMULATION_TYPE != 1 && *SIMULATION_TYPE != 3) unsupported(R, KERNEL_RUN);
+  if (*SIMULATION_TYPE == 3 && *nspec_acoustic > 0)
+    stop(R, "kernel runs with fluid elements go through sf2d_coupled_fwi_* (include/sf2d_coupled.h)");
+  if (*SIMULATION_TYPE == 3 && *nlength_seismogram < 1) stop(R, "nlength_seismogram must be positive");
   if (*PML_BOUNDARY_CONDITIONS) unsupported(R, PML);
   if (*num_interfaces_ext_mesh > 0) unsupported(R, MPI);
   if (*h_NSIGTYPE != 1) stop(R, "one seismogram type per run (NSIGTYPE = 1)");
@@ -687,6 +747,16 @@ void prepare_constants_device_(long *Mesh_pointer, int *h_NGLLX, int *NSPEC_AB, 
     stop(R, "seismotype 1-3 (displacement, velocity, acceleration), with fluid elements also 4 (pressure) "
             "and 6 (potential)");
   auto m = new FortranMesh();
+  m->sim_type = *SIMULATION_TYPE;
+  if (*SAVE_FORWARD && *SIMULATION_TYPE == 1) {
+    // a kernel run through this library replays the forward field from
+    // checkpoints and reads neither the last frame nor the absorbed-boundary
+    // records; the records this run hands back are zeros
+    m->save_forward = true;
+    std::fprintf(stderr,
+                 "prepare_constants_device: SAVE_FORWARD: the absorbing-boundary records (b_absorb_elastic_*) are "
+                 "written as zeros; only a SIMULATION_TYPE = 3 run through this library can follow this run\n");
+  }
   const int ns = *NSPEC_AB, ng = *NGLOB_AB;
   const size_t nl = static_cast<size_t>(ns) * NGLL2;
   // ispec_is_acoustic is a Fortran logical array: nonzero is true
@@ -789,8 +859,8 @@ void prepare_fields_elastic_device_(long *Mesh_pointer, realw *rmassx, realw *rm
 // NGLLX + 1 (a corner a neighbouring face already covers) is left out, as
 // compute_stacey_elastic_kernel skips it
 void prepare_stacey_device_(long *Mesh_pointer, int *ACOUSTIC_SIMULATION, int *ELASTIC_SIMULATION, realw *rho_vp,
-                            realw *rho_vs, int *,
-                            int *, int *, int *, int *h_abs_boundary_ispec, int *h_abs_boundary_ij,
+                            realw *rho_vs, int *h_nspec_bottom, int *h_nspec_left, int *h_nspec_right,
+                            int *h_nspec_top, int *h_abs_boundary_ispec, int *h_abs_boundary_ij,
                             realw *h_abs_boundary_normal, realw *h_abs_boundary_jacobian1Dw,
                             int *h_num_abs_boundary_faces, int *, int *, int *, int *, int *) {
   const char *R = "prepare_stacey_device";
@@ -805,6 +875,10 @@ void prepare_stacey_device_(long *Mesh_pointer, int *ACOUSTIC_SIMULATION, int *E
   m->st_ac_iglob.clear();
   m->st_ac_w.clear();
   m->st_ac_rvp.clear();
+  m->nspec_side[0] = *h_nspec_bottom;
+  m->nspec_side[1] = *h_nspec_left;
+  m->nspec_side[2] = *h_nspec_right;
+  m->nspec_side[3] = *h_nspec_top;
   const int nf = *h_num_abs_boundary_faces;
   for (int f = 0; f < nf; ++f) {
     const int e = h_abs_boundary_ispec[f] - 1;
@@ -839,6 +913,7 @@ void prepare_stacey_device_(long *Mesh_pointer, int *ACOUSTIC_SIMULATION, int *E
 void prepare_cleanup_device_(long *Mesh_pointer, int *, int *, int *, int *, int *, int *, int *, realw *) {
   FortranMesh *m = mesh_of("prepare_cleanup_device", Mesh_pointer);
   if (m->S) sf2d_destroy(m->S);
+  if (m->F) sf2d_fwi_destroy(m->F);
   if (m->C) sf2d_coupled_destroy(m->C);
   delete m;
   *Mesh_pointer = 0;
@@ -860,7 +935,7 @@ void update_displacement_cuda_(long *Mesh_pointer, realw *deltat_F, realw *delta
     return;
   }
   if (m->stage != 0) stop(R, "the previous time step did not reach kernel_3_a_cuda");
-  if (!m->S) {
+  if (!m->S && !m->F) {
     m->dt = *deltat_F;
     m->dtsq2 = *deltatsqover2_F;
     m->dtover2 = *deltatover2_F;
@@ -879,7 +954,7 @@ void compute_forces_viscoelastic_cuda_(long *Mesh_pointer, int *iphase, realw *,
                                        int *, int *compute_wavefield_2) {
   const char *R = "compute_forces_viscoelastic_cuda";
   FortranMesh *m = mesh_of(R, Mesh_pointer);
-  if (*compute_wavefield_2) unsupported(R, KERNEL_RUN);
+  if (*compute_wavefield_2 && m->sim_type != 3) unsupported(R, KERNEL_RUN);
   if (m->fluid) {
     if (*iphase == 1 && m->ac_phase == 4)
       m->ac_phase = 5;
@@ -895,12 +970,21 @@ void compute_forces_viscoelastic_cuda_(long *Mesh_pointer, int *iphase, realw *,
 
 // compute_stacey_viscoelastic_cuda (src/gpu/compute_stacey_viscoelastic_cuda.cu:40):
 // the absorbing terms are part of the fused step
-void compute_stacey_viscoelastic_cuda_(long *Mesh_pointer, int *, realw *, realw *, realw *, realw *, int *,
+void compute_stacey_viscoelastic_cuda_(long *Mesh_pointer, int *iphase, realw *b_absorb_left,
+                                       realw *b_absorb_right, realw *b_absorb_top, realw *b_absorb_bottom, int *,
                                        int *compute_wavefield_2, int *) {
   const char *R = "compute_stacey_viscoelastic_cuda";
   FortranMesh *m = mesh_of(R, Mesh_pointer);
-  if (*compute_wavefield_2) unsupported(R, KERNEL_RUN);
+  if (*compute_wavefield_2 && m->sim_type != 3) unsupported(R, KERNEL_RUN);
   if (m->fluid ? m->ac_phase != 5 : m->stage != 2) stop(R, "called outside a time step");
+  if (m->save_forward && *iphase == 1) {
+    // SIMULATION_TYPE = 1 with SAVE_FORWARD: the host stores these slices as
+    // b_absorb_elastic_*(:,:,:,it); a kernel run here does not read them back
+    realw *side[4] = {b_absorb_bottom, b_absorb_left, b_absorb_right, b_absorb_top};
+    for (int k = 0; k < 4; ++k)
+      if (side[k] && m->nspec_side[k] > 0)
+        std::memset(side[k], 0, sizeof(realw) * 2 * NGLL * static_cast<size_t>(m->nspec_side[k]));
+  }
 }
 
 // compute_add_sources_el_cuda (src/gpu/compute_add_sources_viscoelastic_cuda.cu:46):
@@ -917,7 +1001,7 @@ void compute_add_sources_el_cuda_(long *Mesh_pointer, int *, int *itf) {
 void kernel_3_a_cuda_(long *Mesh_pointer, realw *, realw *, int *, int *compute_wavefield_2) {
   const char *R = "kernel_3_a_cuda";
   FortranMesh *m = mesh_of(R, Mesh_pointer);
-  if (*compute_wavefield_2) unsupported(R, KERNEL_RUN);
+  if (*compute_wavefield_2 && m->sim_type != 3) unsupported(R, KERNEL_RUN);
   if (m->fluid) {
     // the last call of a coupled step: both domains advance in one fused step
     if (m->ac_phase != 5) stop(R, "called before compute_forces_viscoelastic_cuda");
@@ -927,6 +1011,13 @@ void kernel_3_a_cuda_(long *Mesh_pointer, realw *, realw *, int *, int *compute_
     return;
   }
   if (m->stage != 2) stop(R, "called before compute_forces_viscoelastic_cuda");
+  if (m->sim_type == 3) {
+    // the kernel run advanced every step when its first step started
+    if (m->srcs_added != m->steps + 1) stop(R, "compute_add_sources_el_s3_cuda was not called in this step");
+    ++m->steps;
+    m->stage = 0;
+    return;
+  }
   check(R, sf2d_enqueue(m->S, 1));
   ++m->steps;
   m->stage = 0;
@@ -952,7 +1043,11 @@ void compute_seismograms_cuda_(long *Mesh_pointer_f, int *i_sigf, double *sisux,
   const int s0 = m->sample_step.front(), s1 = m->sample_step.back();
   const int n = s1 - s0 + 1;
   std::vector<double> tr(static_cast<size_t>(m->nrec) * n * 2);
-  if (m->C)
+  if (m->F)
+    for (int r = 0; r < m->nrec; ++r)
+      std::memcpy(tr.data() + static_cast<size_t>(r) * n * 2,
+                  m->adj_seis.data() + (static_cast<size_t>(r) * m->nstep + s0) * 2, sizeof(double) * n * 2);
+  else if (m->C)
     check(R, sf2d_coupled_copy_seismograms(m->C, s0, n, tr.data()));
   else
     check(R, sf2d_copy_seismograms(m->S, s0, n, tr.data()));
@@ -969,7 +1064,21 @@ void compute_seismograms_cuda_(long *Mesh_pointer_f, int *i_sigf, double *sisux,
 void get_norm_elastic_from_device_(realw *norm, long *Mesh_pointer, const int *FORWARD_OR_ADJOINT) {
   const char *R = "get_norm_elastic_from_device";
   FortranMesh *m = mesh_of(R, Mesh_pointer);
-  if (FORWARD_OR_ADJOINT && *FORWARD_OR_ADJOINT == 3) unsupported(R, KERNEL_RUN);
+  const bool backward = FORWARD_OR_ADJOINT && *FORWARD_OR_ADJOINT == 3;
+  if (backward && m->sim_type != 3) unsupported(R, KERNEL_RUN);
+  if (m->sim_type == 3) {
+    // the sweep ran when the first step started and stops the run if either
+    // field blew up; reported: the adjoint field at its end, and the replayed
+    // forward field at its end (time zero: at rest)
+    *norm = 0.f;
+    if (!m->F || backward) return;
+    std::vector<float> u(2 * static_cast<size_t>(m->nglob));
+    check(R, sf2d_fwi_adjoint_fields(m->F, u.data(), nullptr, nullptr));
+    float mx = 0.f;
+    for (int g = 0; g < m->nglob; ++g) mx = std::max(mx, std::sqrt(u[2 * g] * u[2 * g] + u[2 * g + 1] * u[2 * g + 1]));
+    *norm = mx;
+    return;
+  }
   if (m->fluid) {
     std::vector<float> u(2 * static_cast<size_t>(m->nglob));
     coupled_fields(R, m, u.data(), nullptr, nullptr, nullptr, nullptr, nullptr);
@@ -1003,6 +1112,7 @@ void transfer_fields_el_to_device_(int *size, realw *displ, realw *veloc, realw 
     check(R, sf2d_set_fields(m->S, displ, veloc, accel));
     return;
   }
+  if (m->F) stop(R, "the fields of a kernel run cannot be replaced after its first step");
   m->staged_u.assign(displ, displ + *size);
   m->staged_v.assign(veloc, veloc + *size);
   m->staged_a.assign(accel, accel + *size);
@@ -1214,6 +1324,101 @@ void transfer_dot_dot_from_device_(int *size, realw *potential_dot_dot_acoustic,
 }
 
 // ---- not provided ----
+// ---- the kernel run (SIMULATION_TYPE = 3) of a solid mesh ----
+
+// prepare_fields_elastic_adj_dev (src/gpu/prepare_mesh_constants_cuda.cu:711):
+// the kernel arrays live in the gradient run this library builds at the first
+// step
+void prepare_fields_elastic_adj_dev_(long *Mesh_pointer, int *size, int *APPROXIMATE_HESS_KL, int *,
+                                     int *NO_BACKWARD_RECONSTRUCTION) {
+  const char *R = "prepare_fields_elastic_adj_dev";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (m->sim_type != 3) stop(R, "called outside a kernel run (SIMULATION_TYPE = 3)");
+  need_size(R, *m, size);
+  // prepare_gpu.f90 stops an approximate Hessian on GPUs as well; the
+  // library's own sf2d_fwi_enable_hessian computes it
+  if (*APPROXIMATE_HESS_KL) stop(R, "APPROXIMATE_HESS_KL: use sf2d_fwi_enable_hessian (include/sf2d_b200.h)");
+  if (*NO_BACKWARD_RECONSTRUCTION)
+    stop(R, "NO_BACKWARD_RECONSTRUCTION: the forward field is replayed from device checkpoints, no frames are read");
+  m->adj_prepared = true;
+}
+
+// prepare_sim2_or_3_const_device (src/gpu/prepare_mesh_constants_cuda.cu:815):
+// source_adjoint(nadj_rec_local, NSTEP, NDIM) in Fortran order, to [irec][it][comp]
+void prepare_sim2_or_3_const_device_(long *Mesh_pointer, int *nadj_rec_local, realw *h_source_adjoint, int *NSTEP) {
+  const char *R = "prepare_sim2_or_3_const_device";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (m->sim_type != 3) stop(R, "called outside a kernel run (SIMULATION_TYPE = 3)");
+  if (m->F) stop(R, "called after the time loop started");
+  if (*NSTEP != m->nstep) stop(R, "NSTEP disagrees with prepare_constants_device");
+  if (*nadj_rec_local != m->nrec) stop(R, "every local receiver must be an adjoint source (nadj_rec_local = nrec_local)");
+  const size_t nr = static_cast<size_t>(m->nrec), nt = static_cast<size_t>(m->nstep);
+  m->adj_src.resize(nr * nt * 2);
+  for (size_t r = 0; r < nr; ++r)
+    for (size_t it = 0; it < nt; ++it)
+      for (size_t c = 0; c < 2; ++c) m->adj_src[(r * nt + it) * 2 + c] = h_source_adjoint[r + nr * (it + nt * c)];
+}
+
+// add_sources_el_sim_type_2_or_3 (src/gpu/compute_add_sources_viscoelastic_cuda.cu:131):
+// the adjoint sources of step it are source_adjoint(:, NSTEP-it+1)
+void add_sources_el_sim_type_2_or_3_(long *Mesh_pointer, int *, int *itf, int *nadj_rec_local, int *NSTEP) {
+  const char *R = "add_sources_el_sim_type_2_or_3";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (m->sim_type != 3) unsupported(R, OTHER);
+  if (m->stage != 2) stop(R, "called outside a time step");
+  if (*nadj_rec_local != m->nrec || *NSTEP != m->nstep) stop(R, "nadj_rec_local or NSTEP changed");
+  if (*itf != m->nstep - m->steps) stop(R, "time step " + std::to_string(*itf) + " out of sequence");
+}
+
+// compute_add_sources_el_s3_cuda (src/gpu/compute_add_sources_viscoelastic_cuda.cu:86):
+// the forward source of the replayed field
+void compute_add_sources_el_s3_cuda_(long *Mesh_pointer, int *, int *itf) {
+  const char *R = "compute_add_sources_el_s3_cuda";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (m->sim_type != 3) stop(R, "called outside a kernel run (SIMULATION_TYPE = 3)");
+  if (m->stage != 2) stop(R, "called outside a time step");
+  if (*itf != m->nstep - m->steps) stop(R, "time step " + std::to_string(*itf) + " out of sequence");
+  m->srcs_added = m->steps + 1;
+}
+
+// compute_kernels_elastic_cuda (src/gpu/compute_kernels_cuda.cu:46): the sums
+// are accumulated inside the sweep at every step
+void compute_kernels_elastic_cuda_(long *Mesh_pointer, realw *) {
+  const char *R = "compute_kernels_elastic_cuda";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (m->sim_type != 3 || !m->F) stop(R, "called outside a kernel run (SIMULATION_TYPE = 3)");
+  if (m->stage != 0) stop(R, "called inside a time step");
+  if (m->kernel_calls >= m->steps) stop(R, "called twice in one time step");
+  ++m->kernel_calls;
+}
+
+// transfer_b_fields_to_device (src/gpu/transfer_fields_cuda.cu:85): the last
+// frame of the forward run (read_forward_arrays.f90); the replayed field
+// starts from rest and needs none
+void transfer_b_fields_to_device_(int *size, realw *, realw *, realw *, long *Mesh_pointer) {
+  const char *R = "transfer_b_fields_to_device";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (m->sim_type != 3) stop(R, "called outside a kernel run (SIMULATION_TYPE = 3)");
+  need_size(R, *m, size);
+}
+
+// transfer_kernels_el_to_host (src/gpu/transfer_fields_cuda.cu:194): rho_kl,
+// mu_kl and kappa_kl before save_adjoint_kernels.f90 scales them
+void transfer_kernels_el_to_host_(long *Mesh_pointer, realw *h_rho_kl, realw *h_mu_kl, realw *h_kappa_kl,
+                                  int *NSPEC_AB) {
+  const char *R = "transfer_kernels_el_to_host";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (m->sim_type != 3 || !m->F) stop(R, "called outside a kernel run (SIMULATION_TYPE = 3)");
+  if (*NSPEC_AB != m->nspec) stop(R, "NSPEC_AB disagrees with prepare_constants_device");
+  if (m->steps != m->nstep) stop(R, "called before the last time step");
+  if (m->kernel_calls != m->nstep)
+    stop(R, "NTSTEP_BETWEEN_COMPUTE_KERNELS must be 1: the sums cover every time step");
+  const size_t nl = static_cast<size_t>(m->nspec) * NGLL2;
+  std::memcpy(h_rho_kl, m->rho_sum.data(), sizeof(realw) * nl);
+  std::memcpy(h_mu_kl, m->mu_sum.data(), sizeof(realw) * nl);
+  std::memcpy(h_kappa_kl, m->kappa_sum.data(), sizeof(realw) * nl);
+}
+
 void transfer_boun_pot_from_device_(long*, realw*, const int*) { unsupported("transfer_boun_pot_from_device", MPI); }
 void transfer_asmbl_pot_to_device_(long*, realw*, const int*) { unsupported("transfer_asmbl_pot_to_device", MPI); }
 void transfer_boun_accel_from_device_(long*, realw*, const int*) { unsupported("transfer_boun_accel_from_device", MPI); }
@@ -1235,25 +1440,18 @@ void check_error_vectors_(int*, realw*, realw*) { unsupported("check_error_vecto
 void compute_add_sources_ac_s3_cuda_(long*, int*, int*) { unsupported("compute_add_sources_ac_s3_cuda", KERNEL_RUN); }
 void compute_add_moving_sources_ac_cuda_(long*, int*, int*, int*, int*, int*) { unsupported("compute_add_moving_sources_ac_cuda", OTHER); }
 void add_sources_ac_sim_2_or_3_cuda_(long*, int*, int*, int*, int*) { unsupported("add_sources_ac_sim_2_or_3_cuda", KERNEL_RUN); }
-void compute_add_sources_el_s3_cuda_(long*, int*, int*) { unsupported("compute_add_sources_el_s3_cuda", KERNEL_RUN); }
-void add_sources_el_sim_type_2_or_3_(long*, int*, int*, int*, int*) { unsupported("add_sources_el_sim_type_2_or_3", KERNEL_RUN); }
-void compute_kernels_elastic_cuda_(long*, realw*) { unsupported("compute_kernels_elastic_cuda", KERNEL_RUN); }
 void compute_kernels_acoustic_cuda_(long*, realw*) { unsupported("compute_kernels_acoustic_cuda", KERNEL_RUN); }
 void compute_kernels_hess_cuda_(long*, int*, int*) { unsupported("compute_kernels_hess_cuda", OTHER); }
 void pml_boundary_acoustic_cuda_(long*, int*, int*) { unsupported("pml_boundary_acoustic_cuda", PML); }
 void prepare_fields_acoustic_adj_dev_(long*, int*, int*, int*) { unsupported("prepare_fields_acoustic_adj_dev", KERNEL_RUN); }
-void prepare_fields_elastic_adj_dev_(long*, int*, int*, int*, int*) { unsupported("prepare_fields_elastic_adj_dev", KERNEL_RUN); }
-void prepare_sim2_or_3_const_device_(long*, int*, realw*, int*) { unsupported("prepare_sim2_or_3_const_device", KERNEL_RUN); }
 void prepare_pml_device_(long*, int*, int*, int*, int*, int*, realw*, realw*, realw*, realw*, realw*, realw*, realw*, realw*, int*, int*) { unsupported("prepare_pml_device", PML); }
 void prepare_moving_sources_cuda_(long*, int*, int*, realw*, int*, int*, realw*) { unsupported("prepare_moving_sources_cuda", OTHER); }
 void prepare_arrays_gpu_(long*, realw*, realw*, realw*, realw*, realw*, realw*, int*, int*, realw*) { unsupported("prepare_arrays_gpu", OTHER); }
 void compute_smooth_(long*, realw*, realw*, realw*, realw*, const int*) { unsupported("compute_smooth", OTHER); }
 void get_smooth_(long*, realw*) { unsupported("get_smooth", OTHER); }
-void transfer_b_fields_to_device_(int*, realw*, realw*, realw*, long*) { unsupported("transfer_b_fields_to_device", KERNEL_RUN); }
 void transfer_b_fields_from_device_(int*, realw*, realw*, realw*, long*) { unsupported("transfer_b_fields_from_device", KERNEL_RUN); }
 void transfer_b_accel_from_device_(int*, realw*, long*) { unsupported("transfer_b_accel_from_device", KERNEL_RUN); }
 void transfer_b_displ_from_device_(int*, realw*, long*) { unsupported("transfer_b_displ_from_device", KERNEL_RUN); }
-void transfer_kernels_el_to_host_(long*, realw*, realw*, realw*, int*) { unsupported("transfer_kernels_el_to_host", KERNEL_RUN); }
 void transfer_b_fields_ac_to_device_(int*, realw*, realw*, realw*, long*) { unsupported("transfer_b_fields_ac_to_device", KERNEL_RUN); }
 void transfer_b_fields_ac_from_device_(int*, realw*, realw*, realw*, long*) { unsupported("transfer_b_fields_ac_from_device", KERNEL_RUN); }
 void transfer_b_potential_ac_from_device_(int*, realw*, long*) { unsupported("transfer_b_potential_ac_from_device", KERNEL_RUN); }

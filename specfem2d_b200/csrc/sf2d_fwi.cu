@@ -253,6 +253,34 @@ extern "C" int sf2d_fwi_adjoint_seismograms(sf2d_fwi *F, double *seismograms) {
   return sf2d_copy_seismograms(F->adj, 0, F->nstep, seismograms);
 }
 
+extern "C" int sf2d_fwi_kernel_sums(sf2d_fwi *F, float *rho_kl, float *kappa_kl, float *mu_kl) {
+  if (!F || !rho_kl || !kappa_kl || !mu_kl) return fail(SF2D_ERR_INVALID, "null argument");
+  const sf2d_solver *A = F->adj;
+  SF2D_CUDA(cudaStreamSynchronize(A->stream));
+  const size_t ng = static_cast<size_t>(F->nglob);
+  std::vector<float2> kmu(A->nq);
+  std::vector<float> rg(ng);
+  SF2D_CUDA(cudaMemcpy(kmu.data(), A->P.kmu_kl, sizeof(float2) * A->nq, cudaMemcpyDeviceToHost));
+  SF2D_CUDA(cudaMemcpy(rg.data(), A->P.rho_kl_glob, sizeof(float) * ng, cudaMemcpyDeviceToHost));
+  const sf2d::Tiling &T = A->T;
+  for (int sl = 0; sl < F->nspec; ++sl) {
+    const int e = T.elem_order[sl];
+    for (int q = 0; q < 25; ++q) {
+      const size_t p = static_cast<size_t>(e) * 25 + q;
+      const float2 km = kmu[static_cast<size_t>(sl) * 25 + q];
+      rho_kl[p] = rg[T.glob2dev[F->ibool[p]]];
+      kappa_kl[p] = km.x;
+      mu_kl[p] = km.y;
+    }
+  }
+  return SF2D_OK;
+}
+
+extern "C" int sf2d_fwi_adjoint_fields(sf2d_fwi *F, float *displ, float *veloc, float *accel) {
+  if (!F) return fail(SF2D_ERR_INVALID, "null handle");
+  return sf2d_get_fields(F->adj, displ, veloc, accel);
+}
+
 extern "C" int sf2d_fwi_destroy(sf2d_fwi *F) {
   delete F;
   return SF2D_OK;

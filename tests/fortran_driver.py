@@ -17,6 +17,15 @@ with arguments passed by reference as gfortran passes them:
   kernel_3_a_cuda; then write_seismograms (write_seismograms.F90:199-205) and,
   every `check_every` steps, check_stability's get_norm_*_from_device;
 * prepare_cleanup_device.
+
+`run_kernel` drives a kernel run (SIMULATION_TYPE = 3) of a solid mesh the
+same way: prepare_fields_elastic_adj_dev and prepare_sim2_or_3_const_device at
+set-up, both wavefields in each step (compute_wavefield_1 and _2), the adjoint
+sources add_sources_el_sim_type_2_or_3 and the replayed source
+compute_add_sources_el_s3_cuda at it_tmp = NSTEP - it + 1
+(compute_gpu_elastic.f90:283-311), transfer_b_fields_to_device after step 1
+(read_forward_arrays.f90), compute_kernels_elastic_cuda every step, and
+transfer_kernels_el_to_host at the end (iterate_time.F90:462-504).
 """
 from __future__ import annotations
 
@@ -54,11 +63,23 @@ class _Refs:
         return arr.ctypes.data_as(ctypes.c_void_p)
 
 
-def run_forward(db, nstep=None, check_every=1000, nlength_seismogram=None):
+def run_forward(db, nstep=None, check_every=1000, nlength_seismogram=None, save_forward=False):
     """Returns (seismograms (nrec, nstep, 2) float64, final displacement (nglob, 2), norms);
     with fluid elements the norms are (solid, fluid) pairs and the final potential
     follows as a fourth value."""
+    return _drive(db, nstep, check_every, nlength_seismogram, None, save_forward)
+
+
+def run_kernel(db, adj_src, check_every=1000, nlength_seismogram=None):
+    """Kernel run with adjoint sources adj_src (nrec, nstep, 2) in forward time
+    order.  Returns (adjoint seismograms, final adjoint displacement, norms as
+    (forward/adjoint, backward) pairs, (rho_kl, mu_kl, kappa_kl) sums (nspec, 5, 5))."""
+    return _drive(db, None, check_every, nlength_seismogram, np.asarray(adj_src, np.float32), False)
+
+
+def _drive(db, nstep, check_every, nlength_seismogram, adj_src, save_forward):
     lib = _lib()
+    kernel = adj_src is not None
     A = gpu_arrays(db, nlength_seismogram)
     nstep = int(nstep or A["nstep"])
     nlen = A["nlength_seismogram"]
@@ -83,9 +104,9 @@ def run_forward(db, nstep=None, check_every=1000, nlength_seismogram=None):
         r.i(A["nsrc"]), r.a(A["sourcearrays"]), r.a(A["source_time_function"]),
         r.i(A["nstep"]), r.a(A["ispec_selected_source"]), r.a(A["ispec_selected_rec_loc"]),
         r.i(A["nrec"]), r.a(A["cosrot"]), r.a(A["sinrot"]),
-        r.i(1), r.i(1), r.i(nac), r.i(A["nspec"] - nac),
+        r.i(3 if kernel else 1), r.i(1), r.i(nac), r.i(A["nspec"] - nac),
         r.a(is_ac), r.a((1 - is_ac).astype(np.int32)),
-        r.i(0), r.i(0),
+        r.i(0), r.i(int(save_forward)),
         r.a(A["xir_store"]), r.a(A["gammar_store"]),
         r.i(1), r.a(np.array([A["seismotype"]], np.int32)), r.i(nlen))
     if fluid:
@@ -108,6 +129,9 @@ def run_forward(db, nstep=None, check_every=1000, nlength_seismogram=None):
         r.a(c["c33"]), r.a(c["c35"]), r.a(c["c55"]),
         r.i(0), r.a(dummy_i), r.i(1 if atten else 0),
         r.a(att["a2"]), r.a(att["b2"]), r.a(att["a1"]), r.a(att["b1"]))
+    ng2 = 2 * A["nglob"]
+    if kernel:
+        lib.prepare_fields_elastic_adj_dev_(M, r.i(ng2), r.i(0), r.i(int(atten)), r.i(0))
     if A["stacey"]:
         ab = A["abs"]
         lib.prepare_stacey_device_(
@@ -116,10 +140,15 @@ def run_forward(db, nstep=None, check_every=1000, nlength_seismogram=None):
             r.i(ab["counts"]["top"]), r.a(ab["abs_boundary_ispec"]), r.a(ab["abs_boundary_ij"]),
             r.a(ab["abs_boundary_normal"]), r.a(ab["abs_boundary_jacobian1Dw"]), r.i(ab["nface"]),
             r.a(ab["edge_abs"]), r.a(dummy_i), r.a(dummy_i), r.a(dummy_i), r.a(dummy_i))
-    ng2 = 2 * A["nglob"]
+    if kernel:
+        # source_adjoint(nadj_rec_local, NSTEP, NDIM) in Fortran order
+        src_adj = np.asfortranarray(adj_src.reshape(A["nrec"], A["nstep"], 2))
+        lib.prepare_sim2_or_3_const_device_(M, r.i(A["nrec"]), r.a(src_adj), r.i(A["nstep"]))
     zeros = np.zeros(ng2, np.float32)
     if elastic:
         lib.transfer_fields_el_to_device_(r.i(ng2), r.a(zeros), r.a(zeros.copy()), r.a(zeros.copy()), M)
+    if kernel:
+        lib.transfer_b_fields_to_device_(r.i(ng2), r.a(zeros), r.a(zeros), r.a(zeros), M)
     if fluid:
         z1 = np.zeros(A["nglob"], np.float32)
         lib.transfer_fields_ac_to_device_(r.i(A["nglob"]), r.a(z1), r.a(z1.copy()), r.a(z1.copy()), M)
@@ -136,8 +165,16 @@ def run_forward(db, nstep=None, check_every=1000, nlength_seismogram=None):
     dummy_b = dummy_f.ctypes.data_as(ctypes.c_void_p)
     seismo_current = 0
     ncpl_c = ctypes.c_int(A.get("ncoupling", 0))
+    # b_absorb_elastic_left/right/top/bottom slices (NDIM, NGLLX, nspec_side)
+    sides = ("left", "right", "top", "bottom")
+    nside = {k: (A["abs"]["counts"][k] if A["stacey"] else 0) for k in sides}
+    b_absorb = [np.full(2 * 5 * max(nside[k], 1), np.nan, np.float32) for k in sides]
+    b_ptr = [b.ctypes.data_as(ctypes.c_void_p) for b in b_absorb]
+    cw2 = one if kernel else zero
+    nrec_c, nstep_c, itmp_c = ctypes.c_int(A["nrec"]), ctypes.c_int(A["nstep"]), ctypes.c_int(0)
     for it in range(1, nstep + 1):
         it_c.value = it
+        itmp_c.value = A["nstep"] - it + 1
         if fluid:
             lib.update_displacement_ac_cuda_(M, ctypes.byref(dt), ctypes.byref(dtsq2), ctypes.byref(dt2),
                                              ctypes.byref(dt), ctypes.byref(dtsq2), ctypes.byref(dt2),
@@ -163,16 +200,28 @@ def run_forward(db, nstep=None, check_every=1000, nlength_seismogram=None):
         for iphase in ((one, two) if elastic else ()):
             lib.compute_forces_viscoelastic_cuda_(M, ctypes.byref(iphase), ctypes.byref(dt), ctypes.byref(zero),
                                                   ctypes.byref(nspec_c), ctypes.byref(aniso_c), ctypes.byref(atten_c),
-                                                  ctypes.byref(one), ctypes.byref(zero))
+                                                  ctypes.byref(one), ctypes.byref(cw2))
             if iphase is one:
                 if A["stacey"]:
-                    lib.compute_stacey_viscoelastic_cuda_(M, ctypes.byref(one), dummy_b, dummy_b, dummy_b, dummy_b,
-                                                          ctypes.byref(one), ctypes.byref(zero), ctypes.byref(zero))
+                    lib.compute_stacey_viscoelastic_cuda_(M, ctypes.byref(one), *b_ptr,
+                                                          ctypes.byref(one), ctypes.byref(cw2), ctypes.byref(zero))
+                    if save_forward:
+                        # the host stores the slices it got back as b_absorb_elastic_*(:,:,:,it)
+                        assert all(np.all(b == 0) for b, k in zip(b_absorb, sides) if nside[k] > 0)
                 if fluid:
                     lib.compute_coupling_el_ac_cuda_(M, ctypes.byref(one), ctypes.byref(ncpl_c), ctypes.byref(one))
-                lib.compute_add_sources_el_cuda_(M, ctypes.byref(one), ctypes.byref(it_c))
+                if kernel:
+                    if A["nrec"] > 0:
+                        lib.add_sources_el_sim_type_2_or_3_(M, ctypes.byref(one), ctypes.byref(itmp_c),
+                                                            ctypes.byref(nrec_c), ctypes.byref(nstep_c))
+                    lib.compute_add_sources_el_s3_cuda_(M, ctypes.byref(one), ctypes.byref(itmp_c))
+                else:
+                    lib.compute_add_sources_el_cuda_(M, ctypes.byref(one), ctypes.byref(it_c))
         if elastic:
-            lib.kernel_3_a_cuda_(M, ctypes.byref(dt2), ctypes.byref(dt2), ctypes.byref(one), ctypes.byref(zero))
+            lib.kernel_3_a_cuda_(M, ctypes.byref(dt2), ctypes.byref(dt2), ctypes.byref(one), ctypes.byref(cw2))
+        if kernel and it == 1:
+            # read_forward_arrays: the last frame of the saved forward run
+            lib.transfer_b_fields_to_device_(r.i(ng2), r.a(zeros), r.a(zeros), r.a(zeros), M)
         seismo_current += 1
         cur_c.value = seismo_current
         lib.compute_seismograms_cuda_(M, ctypes.byref(one), sisux.ctypes.data_as(ctypes.c_void_p),
@@ -186,9 +235,16 @@ def run_forward(db, nstep=None, check_every=1000, nlength_seismogram=None):
             seis[:, it - n:it, 0] = sisux[:, :n]
             seis[:, it - n:it, 1] = sisuz[:, :n]
             seismo_current = 0
+        if kernel:
+            lib.compute_kernels_elastic_cuda_(M, ctypes.byref(dt))
         if it % check_every == 0 or it == nstep:
             lib.get_norm_elastic_from_device_(ctypes.byref(norm), M, ctypes.byref(one))
-            if fluid:
+            if kernel:
+                n_fwd = float(norm.value)
+                three = ctypes.c_int(3)
+                lib.get_norm_elastic_from_device_(ctypes.byref(norm), M, ctypes.byref(three))
+                norms.append((n_fwd, float(norm.value)))
+            elif fluid:
                 n_el = float(norm.value)
                 lib.get_norm_acoustic_from_device_(ctypes.byref(norm), M, ctypes.byref(one))
                 norms.append((n_el, float(norm.value)))
@@ -200,8 +256,14 @@ def run_forward(db, nstep=None, check_every=1000, nlength_seismogram=None):
     if fluid:
         pot = np.zeros(A["nglob"], np.float32)
         lib.transfer_fields_ac_from_device_(r.i(A["nglob"]), r.a(pot), r.a(np.zeros_like(pot)), r.a(np.zeros_like(pot)), M)
+    kl = None
+    if kernel:
+        kl = tuple(np.zeros((A["nspec"], 5, 5), np.float32) for _ in range(3))
+        lib.transfer_kernels_el_to_host_(M, *[r.a(k) for k in kl], r.i(A["nspec"]))
     lib.prepare_cleanup_device_(M, r.i(0), r.i(1), r.i(int(aniso)), r.i(0), r.i(0), r.i(int(atten)), r.i(0),
                                 r.a(dummy_f))
+    if kernel:
+        return seis, displ.reshape(-1, 2), norms, kl
     if fluid:
         return seis, displ.reshape(-1, 2), norms, pot
     return seis, displ.reshape(-1, 2), norms

@@ -108,3 +108,60 @@ def test_fluid_only_external_mesh_through_the_fortran_interface():
         assert rel_l2(out[k, :, 0], o64[k, :, 0]) < 1.5 * band
         assert rel_l2(out[k, :, 0], seis[f"S{k + 1:04d}_PRE"]) < 2.0 * band
     assert np.all(out[:, :, 1] == 0.0) and norms[-1][0] == 0.0 and norms[-1][1] > 0
+
+
+def test_save_forward_run_hands_back_zero_absorbing_records():
+    """SAVE_FORWARD: the traces are those of a plain forward run; the absorbed-
+    boundary slices the host stores come back as zeros (the driver checks every
+    step), since a kernel run here replays the forward field instead."""
+    cfg, _ = load_golden("tromp2005_kernel")
+    db = database_from_config(cfg, nstep=400)
+    a, _, _ = run_forward(db)
+    b, _, _ = run_forward(db, save_forward=True)
+    assert np.array_equal(a, b)
+
+
+def test_tromp2005_kernel_run_through_the_fortran_interface():
+    """EXAMPLES/Tromp2005_kernel as SIMULATION_TYPE = 3 through
+    prepare_fields_elastic_adj_dev, prepare_sim2_or_3_const_device and
+    transfer_kernels_el_to_host: the adjoint traces and the kernel sums equal
+    the library's own gradient run (sf2d_fwi, lambda formed in FP64 there and as
+    kappa - mu in FP32 here), and the kernels scaled as
+    save_adjoint_kernels.f90:134-141 scales them reach the maxima of the
+    reference's kernel run."""
+    import json
+    import os
+
+    from helpers import GOLDEN
+    from fortran_driver import run_kernel
+    from specfem2d_b200.fwi import FWIGradient
+    from specfem2d_b200.setup.adjoint import cross_correlation_adjoint_source, derived_kernels
+
+    cfg, seis = load_golden("tromp2005_kernel")
+    adj_ref = dict(np.load(os.path.join(GOLDEN, "tromp2005_kernel_adjoint.npz")))
+    with open(os.path.join(GOLDEN, "tromp2005_kernel_adjoint.json")) as f:
+        log = json.load(f)
+    traces = np.stack([seis["S0001_BXX"], seis["S0001_BXZ"]], axis=1)
+    adj, _ = cross_correlation_adjoint_source(adj_ref["t_forward"], traces, 27.0, 32.0, 1)
+    db = database_from_config(cfg)
+    adj32 = adj.astype(np.float32).reshape(1, -1, 2)
+    aseis, _, norms, (rs, ms, ks) = run_kernel(db, adj32, check_every=400)
+    g = FWIGradient(db, checkpoint_every=200)
+    g.forward()
+    rk, kk, mk = g.backward(adj32)
+    a = g.adjoint_seismograms()
+    g.close()
+    assert rel_l2(aseis, a) < 1e-5
+    ref = np.stack([adj_ref["S0001_BXX"], adj_ref["S0001_BXZ"]], axis=1)
+    assert rel_l2(aseis[0, :, 0], ref[:, 0]) < 1e-5
+    dt = np.float32(db.deltat)
+    rho, kap, mu = (np.asarray(x, np.float32).reshape(-1, 5, 5) for x in (db.rhostore, db.kappastore, db.mustore))
+    rho_kl, kappa_kl, mu_kl = -rho * dt * rs, -kap * dt * ks, np.float32(-2) * mu * dt * ms
+    for got, want in ((rho_kl, rk), (kappa_kl, kk), (mu_kl, mk)):
+        assert rel_l2(got, want) < 1e-4
+    d = derived_kernels(rho_kl, kappa_kl, mu_kl, db.rhostore, db.kappastore, db.mustore)
+    got = dict(rho=rho_kl.max(), kappa=kappa_kl.max(), mu=mu_kl.max(), rhop=d["rhop"].max(),
+               alpha=d["alpha"].max(), beta=d["beta"].max())
+    for k, v in log["kernel_max"].items():
+        assert float(got[k]) == pytest.approx(v, rel=2e-5), k
+    assert all(f > 0 and b == 0 for f, b in norms) and len(norms) == 8

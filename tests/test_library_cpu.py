@@ -78,6 +78,8 @@ def test_library_exports_the_reference_fortran_interface():
     ("kernel_3_b_cuda_", "sf2d_fwi_create"),
     ("transfer_boun_accel_from_device_", "MPI"),
     ("update_displacement_cuda_", "Mesh_pointer was not prepared"),
+    ("transfer_kernels_el_to_host_", "Mesh_pointer was not prepared"),
+    ("transfer_b_fields_from_device_", "sf2d_fwi_create"),
 ])
 def test_fortran_interface_errors_exit_like_the_reference(call, needle):
     """A call the library does not provide, or one on an unprepared handle, prints
