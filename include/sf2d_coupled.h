@@ -184,6 +184,15 @@ int sf2d_coupled_fwi_backward(sf2d_coupled_fwi *f, const float *adj_src, float *
                               float *mu_kl, float *rho_ac_kl, float *kappa_ac_kl);
 /* receiver traces of the adjoint field of the last backward (nrec_total*nstep*2) */
 int sf2d_coupled_fwi_adjoint_seismograms(sf2d_coupled_fwi *f, double *seismograms);
+/* The solid kernel sums of the last backward before the scaling of
+ * save_adjoint_kernels.f90:134-141 (solid sub-mesh element order): what the
+ * reference's transfer_kernels_el_to_host hands to the host. */
+int sf2d_coupled_fwi_kernel_sums(sf2d_coupled_fwi *f, float *rho_kl, float *kappa_kl, float *mu_kl);
+/* The coupled run of the adjoint field (owned by f, valid until
+ * sf2d_coupled_fwi_destroy) for reading its fields and norms after a backward
+ * sweep (sf2d_coupled_get_fields*, sf2d_coupled_set_global_numbering).  Its
+ * time loop belongs to f: do not enqueue steps on it. */
+int sf2d_coupled_fwi_adjoint_run(sf2d_coupled_fwi *f, sf2d_coupled **adj);
 int sf2d_coupled_fwi_destroy(sf2d_coupled_fwi *f);
 
 #ifdef __cplusplus

@@ -1415,6 +1415,36 @@ extern "C" int sf2d_coupled_fwi_adjoint_seismograms(sf2d_coupled_fwi *F, double 
   return SF2D_OK;
 }
 
+extern "C" int sf2d_coupled_fwi_kernel_sums(sf2d_coupled_fwi *F, float *rho_kl, float *kappa_kl, float *mu_kl) {
+  using namespace sf2d;
+  if (!F || !rho_kl || !kappa_kl || !mu_kl) return fail(SF2D_ERR_INVALID, "null argument");
+  if (!F->adj->el) return fail(SF2D_ERR_INVALID, "the mesh has no solid element");
+  const sf2d_solver *S = F->adj->el;
+  SF2D_CUDA(cudaStreamSynchronize(F->adj->stream()));
+  std::vector<float2> kmu(S->nq);
+  std::vector<float> rg(F->ng_s);
+  SF2D_CUDA(cudaMemcpy(kmu.data(), S->P.kmu_kl, sizeof(float2) * S->nq, cudaMemcpyDeviceToHost));
+  SF2D_CUDA(cudaMemcpy(rg.data(), S->P.rho_kl_glob, sizeof(float) * F->ng_s, cudaMemcpyDeviceToHost));
+  const sf2d::Tiling &T = S->T;
+  for (int sl = 0; sl < F->nspec_s; ++sl) {
+    const int e = T.elem_order[sl];
+    for (int q = 0; q < 25; ++q) {
+      const size_t p = static_cast<size_t>(e) * 25 + q;
+      const float2 km = kmu[static_cast<size_t>(sl) * 25 + q];
+      rho_kl[p] = rg[T.glob2dev[F->ibool_s[p]]];
+      kappa_kl[p] = km.x;
+      mu_kl[p] = km.y;
+    }
+  }
+  return SF2D_OK;
+}
+
+extern "C" int sf2d_coupled_fwi_adjoint_run(sf2d_coupled_fwi *F, sf2d_coupled **adj) {
+  if (!F || !adj) return sf2d::fail(SF2D_ERR_INVALID, "null argument");
+  *adj = F->adj;
+  return SF2D_OK;
+}
+
 extern "C" int sf2d_coupled_fwi_destroy(sf2d_coupled_fwi *F) {
   delete F;
   return SF2D_OK;

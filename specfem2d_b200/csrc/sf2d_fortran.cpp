@@ -95,7 +95,15 @@ struct FortranMesh {
   std::vector<double> adj_seis;      // adjoint traces [irec][it][comp]
   std::vector<float> rho_sum, kappa_sum, mu_sum;
   int kernel_calls = 0;              // compute_kernels_elastic_cuda calls
-  int srcs_added = 0;                // step of the last compute_add_sources_el_s3_cuda
+  int srcs_added = 0;                // step of the last compute_add_sources_*_s3_cuda
+  // with fluid elements: the coupled gradient run; C then points at its adjoint
+  // run (owned by CF) for the field and norm queries
+  sf2d_coupled_fwi *CF = nullptr;
+  bool kr_open = false;              // a time step of the kernel run is open
+  bool ac_adj_prepared = false;
+  int ac_kernel_calls = 0;           // compute_kernels_acoustic_cuda calls
+  std::vector<int> s_elems, f_elems;  // whole-mesh element of each solid / fluid sub-mesh element
+  std::vector<float> rho_ac_kl, kappa_ac_kl;  // whole-mesh element order, zero in solid elements
 };
 
 FortranMesh *mesh_of(const char *routine, const long *p) {
@@ -233,7 +241,7 @@ void build_coupled(const char *routine, FortranMesh &m);
 void run_kernel_sweep(const char *routine, FortranMesh &m);
 
 void build_solver(const char *routine, FortranMesh &m) {
-  if (m.S || m.C || m.F) return;
+  if (m.S || m.C || m.F || m.CF) return;
   if (m.fluid) {
     build_coupled(routine, m);
     return;
@@ -383,6 +391,67 @@ std::vector<T> elem_rows(const std::vector<T> &a, const std::vector<int> &elems,
 // directions (the reference's GPU kernels use the fluid element's normals and
 // weights for both, compute_coupling_*_kernel.cu), sources and receivers split
 // by the domain of their element.
+// The kernel run of a mesh with fluid elements (iterate_time.F90:146-400 with
+// SIMULATION_TYPE = 3: compute_gpu_elastic.f90 and compute_gpu_acoustic.f90
+// with compute_wavefield_1 and _2): the forward field from rest with
+// checkpoints, then the adjoint sweep that replays it, at the first step.
+// The kernels are summed at every step (NTSTEP_BETWEEN_COMPUTE_KERNELS = 1).
+void run_coupled_kernel_sweep(const char *routine, FortranMesh &m, const sf2d_elastic_desc &d,
+                              const sf2d_acoustic_desc &a, const sf2d_coupling_desc &c) {
+  const bool solid = d.nspec > 0;
+  if (!m.ac_adj_prepared || (solid && !m.adj_prepared))
+    stop(routine, "prepare_fields_acoustic_adj_dev / prepare_fields_elastic_adj_dev has not been called");
+  if (m.nrec > 0 && m.adj_src.empty()) stop(routine, "prepare_sim2_or_3_const_device has not been called");
+  for (const std::vector<float> *f : {&m.staged_u, &m.staged_v, &m.staged_a, &m.staged_p, &m.staged_pd,
+                                      &m.staged_pdd})
+    for (float x : *f)
+      if (x != 0.f) stop(routine, "a kernel run starts from rest: the initial fields must be zero");
+  for (std::vector<float> *f : {&m.staged_u, &m.staged_v, &m.staged_a, &m.staged_p, &m.staged_pd, &m.staged_pdd})
+    f->clear();
+  const size_t nls = static_cast<size_t>(d.nspec) * NGLL2, nlf = static_cast<size_t>(a.nspec) * NGLL2;
+  // solid rhostore/kappastore scale sf2d_coupled_fwi_backward's kernels only; the
+  // host receives the unscaled sums and scales them itself
+  const std::vector<float> ones(std::max<size_t>(nls, 1), 1.f);
+  check(routine, sf2d_coupled_fwi_create(&d, &a, &c, solid ? ones.data() : nullptr, solid ? ones.data() : nullptr,
+                                         std::min(m.nstep, 200), &m.CF));
+  int rc = sf2d_coupled_fwi_forward(m.CF, nullptr);
+  if (rc == SF2D_ERR_UNSTABLE) stop(routine, "the forward wavefield of the kernel run became unstable and blew up");
+  check(routine, rc);
+  const float none = 0.f;
+  std::vector<float> rk(std::max<size_t>(nls, 1)), kk(rk.size()), mk(rk.size()), rac(std::max<size_t>(nlf, 1)),
+      kac(rac.size());
+  rc = sf2d_coupled_fwi_backward(m.CF, m.adj_src.empty() ? &none : m.adj_src.data(), solid ? rk.data() : nullptr,
+                                 solid ? kk.data() : nullptr, solid ? mk.data() : nullptr, rac.data(), kac.data());
+  if (rc == SF2D_ERR_UNSTABLE) stop(routine, "the adjoint wavefield became unstable and blew up");
+  check(routine, rc);
+  m.adj_seis.assign(static_cast<size_t>(m.nrec) * m.nstep * 2, 0.0);
+  if (m.nrec) check(routine, sf2d_coupled_fwi_adjoint_seismograms(m.CF, m.adj_seis.data()));
+  // kernels to the whole mesh's element order, zero in the other domain (the
+  // reference's kernel arrays span NSPEC_AB)
+  const size_t nl = static_cast<size_t>(m.nspec) * NGLL2;
+  m.rho_ac_kl.assign(nl, 0.f);
+  m.kappa_ac_kl.assign(nl, 0.f);
+  for (size_t k = 0; k < m.f_elems.size(); ++k)
+    for (int q = 0; q < NGLL2; ++q) {
+      m.rho_ac_kl[static_cast<size_t>(m.f_elems[k]) * NGLL2 + q] = rac[k * NGLL2 + q];
+      m.kappa_ac_kl[static_cast<size_t>(m.f_elems[k]) * NGLL2 + q] = kac[k * NGLL2 + q];
+    }
+  m.rho_sum.assign(nl, 0.f);
+  m.kappa_sum.assign(nl, 0.f);
+  m.mu_sum.assign(nl, 0.f);
+  if (solid) {
+    check(routine, sf2d_coupled_fwi_kernel_sums(m.CF, rk.data(), kk.data(), mk.data()));
+    for (size_t k = 0; k < m.s_elems.size(); ++k)
+      for (int q = 0; q < NGLL2; ++q) {
+        const size_t p = static_cast<size_t>(m.s_elems[k]) * NGLL2 + q;
+        m.rho_sum[p] = rk[k * NGLL2 + q];
+        m.kappa_sum[p] = kk[k * NGLL2 + q];
+        m.mu_sum[p] = mk[k * NGLL2 + q];
+      }
+  }
+  check(routine, sf2d_coupled_fwi_adjoint_run(m.CF, &m.C));
+}
+
 void build_coupled(const char *routine, FortranMesh &m) {
   if (!m.have_fluid) stop(routine, "prepare_fields_acoustic_device has not been called");
   if (m.stacey && !m.have_stacey) stop(routine, "prepare_stacey_device has not been called");
@@ -588,6 +657,13 @@ void build_coupled(const char *routine, FortranMesh &m) {
   c.cpl_ac_w = c.cpl_el_w = m.cpl_w.data();
   c.cpl_el_point = c_s.data();
   c.cpl_el_ac_point = c_f.data();
+  m.s_elems = S.elems;
+  m.f_elems = F.elems;
+  if (m.sim_type == 3) {
+    run_coupled_kernel_sweep(routine, m, d, a, c);
+    check(routine, sf2d_coupled_set_global_numbering(m.C, m.nglob, solid ? S.pts.data() : nullptr, F.pts.data()));
+    return;
+  }
   check(routine, sf2d_coupled_create(&d, &a, &c, &m.C));
   check(routine, sf2d_coupled_set_global_numbering(m.C, m.nglob, solid ? S.pts.data() : nullptr, F.pts.data()));
   if (!m.staged_u.empty() || !m.staged_p.empty()) {
@@ -627,6 +703,7 @@ void coupled_fields(const char *R, FortranMesh *m, realw *u, realw *v, realw *a,
 // Sets some fields of a coupled run, keeping the others.
 void coupled_set(const char *R, FortranMesh *m, const realw *u, const realw *v, const realw *a, const realw *p,
                  const realw *pd, const realw *pdd) {
+  if (m->CF) stop(R, "the fields of a kernel run cannot be replaced after its first step");
   const size_t n2 = 2 * static_cast<size_t>(m->nglob), n1 = m->nglob;
   std::vector<float> cur[6] = {std::vector<float>(n2), std::vector<float>(n2), std::vector<float>(n2),
                                std::vector<float>(n1), std::vector<float>(n1), std::vector<float>(n1)};
@@ -641,6 +718,19 @@ void coupled_set(const char *R, FortranMesh *m, const realw *u, const realw *v, 
   }
   std::vector<float> *st[6] = {&m->staged_u, &m->staged_v, &m->staged_a, &m->staged_p, &m->staged_pd, &m->staged_pdd};
   for (int k = 0; k < 6; ++k) *st[k] = std::move(cur[k]);
+}
+
+// A per-step call of a kernel run on a mesh with fluid elements: the run went
+// through in full when the first step started, so only the step must be open.
+void kernel_step_call(const char *R, const FortranMesh *m) {
+  if (!m->CF || !m->kr_open) stop(R, "called outside a time step of the kernel run");
+}
+
+// Ends a time step of a kernel run on a mesh with fluid elements.
+void kernel_step_end(const char *R, FortranMesh *m) {
+  if (m->srcs_added != m->steps + 1) stop(R, "no compute_add_sources_*_s3_cuda call in this time step");
+  ++m->steps;
+  m->kr_open = false;
 }
 
 void fluid_phase_call(const char *R, FortranMesh *m, const int *compute_wavefield_2) {
@@ -736,8 +826,6 @@ void prepare_constants_device_(long *Mesh_pointer, int *h_NGLLX, int *NSPEC_AB, 
   if (*h_NGLLX != NGLL) stop(R, "NGLLX must be 5");
   if (!*P_SV) stop(R, "SH (membrane) waves are not provided: P_SV only");
   if (*SIMULATION_TYPE != 1 && *SIMULATION_TYPE != 3) unsupported(R, KERNEL_RUN);
-  if (*SIMULATION_TYPE == 3 && *nspec_acoustic > 0)
-    stop(R, "kernel runs with fluid elements go through sf2d_coupled_fwi_* (include/sf2d_coupled.h)");
   if (*SIMULATION_TYPE == 3 && *nlength_seismogram < 1) stop(R, "nlength_seismogram must be positive");
   if (*PML_BOUNDARY_CONDITIONS) unsupported(R, PML);
   if (*num_interfaces_ext_mesh > 0) unsupported(R, MPI);
@@ -914,7 +1002,10 @@ void prepare_cleanup_device_(long *Mesh_pointer, int *, int *, int *, int *, int
   FortranMesh *m = mesh_of("prepare_cleanup_device", Mesh_pointer);
   if (m->S) sf2d_destroy(m->S);
   if (m->F) sf2d_fwi_destroy(m->F);
-  if (m->C) sf2d_coupled_destroy(m->C);
+  if (m->CF)
+    sf2d_coupled_fwi_destroy(m->CF);  // C is its adjoint run
+  else if (m->C)
+    sf2d_coupled_destroy(m->C);
   delete m;
   *Mesh_pointer = 0;
 }
@@ -929,6 +1020,10 @@ void update_displacement_cuda_(long *Mesh_pointer, realw *deltat_F, realw *delta
   const char *R = "update_displacement_cuda";
   FortranMesh *m = mesh_of(R, Mesh_pointer);
   if (m->fluid) {
+    if (m->sim_type == 3) {
+      kernel_step_call(R, m);
+      return;
+    }
     // coupled mesh: the solid predictor follows the fluid's (update_displacement_Newmark.F90:150-240)
     if (m->ac_phase != 1) stop(R, "update_displacement_ac_cuda must start the step");
     m->ac_phase = 2;
@@ -956,6 +1051,10 @@ void compute_forces_viscoelastic_cuda_(long *Mesh_pointer, int *iphase, realw *,
   FortranMesh *m = mesh_of(R, Mesh_pointer);
   if (*compute_wavefield_2 && m->sim_type != 3) unsupported(R, KERNEL_RUN);
   if (m->fluid) {
+    if (m->sim_type == 3) {
+      kernel_step_call(R, m);
+      return;
+    }
     if (*iphase == 1 && m->ac_phase == 4)
       m->ac_phase = 5;
     else if (!(*iphase == 2 && m->ac_phase == 5))
@@ -976,7 +1075,10 @@ void compute_stacey_viscoelastic_cuda_(long *Mesh_pointer, int *iphase, realw *b
   const char *R = "compute_stacey_viscoelastic_cuda";
   FortranMesh *m = mesh_of(R, Mesh_pointer);
   if (*compute_wavefield_2 && m->sim_type != 3) unsupported(R, KERNEL_RUN);
-  if (m->fluid ? m->ac_phase != 5 : m->stage != 2) stop(R, "called outside a time step");
+  if (m->fluid && m->sim_type == 3)
+    kernel_step_call(R, m);
+  else if (m->fluid ? m->ac_phase != 5 : m->stage != 2)
+    stop(R, "called outside a time step");
   if (m->save_forward && *iphase == 1) {
     // SIMULATION_TYPE = 1 with SAVE_FORWARD: the host stores these slices as
     // b_absorb_elastic_*(:,:,:,it); a kernel run here does not read them back
@@ -1003,6 +1105,13 @@ void kernel_3_a_cuda_(long *Mesh_pointer, realw *, realw *, int *, int *compute_
   FortranMesh *m = mesh_of(R, Mesh_pointer);
   if (*compute_wavefield_2 && m->sim_type != 3) unsupported(R, KERNEL_RUN);
   if (m->fluid) {
+    if (m->sim_type == 3) {
+      // the backward field's corrector ends a kernel-run step (compute_gpu_elastic.f90
+      // with compute_b_wavefield runs last, iterate_time.F90:330-360)
+      kernel_step_call(R, m);
+      if (*compute_wavefield_2) kernel_step_end(R, m);
+      return;
+    }
     // the last call of a coupled step: both domains advance in one fused step
     if (m->ac_phase != 5) stop(R, "called before compute_forces_viscoelastic_cuda");
     check(R, sf2d_coupled_enqueue(m->C, 1));
@@ -1043,7 +1152,7 @@ void compute_seismograms_cuda_(long *Mesh_pointer_f, int *i_sigf, double *sisux,
   const int s0 = m->sample_step.front(), s1 = m->sample_step.back();
   const int n = s1 - s0 + 1;
   std::vector<double> tr(static_cast<size_t>(m->nrec) * n * 2);
-  if (m->F)
+  if (m->F || m->CF)
     for (int r = 0; r < m->nrec; ++r)
       std::memcpy(tr.data() + static_cast<size_t>(r) * n * 2,
                   m->adj_seis.data() + (static_cast<size_t>(r) * m->nstep + s0) * 2, sizeof(double) * n * 2);
@@ -1066,12 +1175,14 @@ void get_norm_elastic_from_device_(realw *norm, long *Mesh_pointer, const int *F
   FortranMesh *m = mesh_of(R, Mesh_pointer);
   const bool backward = FORWARD_OR_ADJOINT && *FORWARD_OR_ADJOINT == 3;
   if (backward && m->sim_type != 3) unsupported(R, KERNEL_RUN);
-  if (m->sim_type == 3) {
-    // the sweep ran when the first step started and stops the run if either
-    // field blew up; reported: the adjoint field at its end, and the replayed
-    // forward field at its end (time zero: at rest)
+  // a kernel run went through when its first step started and stopped the run
+  // if either field blew up; reported: the adjoint field at its end, and the
+  // replayed forward field at its end (time zero: at rest)
+  if (m->sim_type == 3 && (backward || (!m->F && !m->CF))) {
     *norm = 0.f;
-    if (!m->F || backward) return;
+    return;
+  }
+  if (m->sim_type == 3 && m->F) {
     std::vector<float> u(2 * static_cast<size_t>(m->nglob));
     check(R, sf2d_fwi_adjoint_fields(m->F, u.data(), nullptr, nullptr));
     float mx = 0.f;
@@ -1198,6 +1309,22 @@ void update_displacement_ac_cuda_(long *Mesh_pointer, realw *deltat_F, realw *de
   FortranMesh *m = mesh_of(R, Mesh_pointer);
   if (!m->fluid) stop(R, "the mesh has no fluid element");
   if (UNDO_ATTENUATION_AND_OR_PML && *UNDO_ATTENUATION_AND_OR_PML) unsupported(R, KERNEL_RUN);
+  if (m->sim_type == 3) {
+    // the first call of a kernel-run step (update_displacement_Newmark.F90:126-160
+    // advances both fields here); the first step runs the whole gradient
+    if (m->kr_open) stop(R, "the previous time step did not finish");
+    if (!m->CF) {
+      m->dt = *deltat_F;
+      m->dtsq2 = *deltatsqover2_F;
+      m->dtover2 = *deltatover2_F;
+      build_solver(R, *m);
+    } else if (*deltat_F != m->dt || *deltatsqover2_F != m->dtsq2 || *deltatover2_F != m->dtover2) {
+      stop(R, "the time step changed during the run");
+    }
+    if (m->steps >= m->nstep) stop(R, "more time steps than NSTEP");
+    m->kr_open = true;
+    return;
+  }
   if (m->ac_phase != 0) stop(R, "the previous time step did not finish");
   if (!m->C) {
     m->dt = *deltat_F;
@@ -1217,6 +1344,11 @@ void update_displacement_ac_cuda_(long *Mesh_pointer, realw *deltat_F, realw *de
 void acoustic_enforce_free_surf_cuda_(long *Mesh_pointer, int *, int *compute_wavefield_2) {
   const char *R = "acoustic_enforce_free_surf_cuda";
   FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (m->sim_type == 3) {
+    // before and after each field's forces, the last time after the step ended
+    if (!m->CF) stop(R, "called outside a time step of the kernel run");
+    return;
+  }
   if (*compute_wavefield_2) unsupported(R, KERNEL_RUN);
   const bool fluid_only = m->nspec_acoustic == m->nspec;
   if (!(m->ac_phase == 2 || m->ac_phase == 4 || (fluid_only && m->ac_phase == 0 && m->steps > 0)))
@@ -1229,8 +1361,12 @@ void compute_forces_acoustic_cuda_(long *Mesh_pointer, int *iphase, int *, int *
                                    int *compute_wavefield_2) {
   const char *R = "compute_forces_acoustic_cuda";
   FortranMesh *m = mesh_of(R, Mesh_pointer);
-  if (*compute_wavefield_2) unsupported(R, KERNEL_RUN);
   if (*ATTENUATION_VISCOACOUSTIC) stop(R, "viscoacoustic attenuation is not provided");
+  if (m->sim_type == 3) {
+    kernel_step_call(R, m);
+    return;
+  }
+  if (*compute_wavefield_2) unsupported(R, KERNEL_RUN);
   if (*iphase == 1 && m->ac_phase == 2)
     m->ac_phase = 3;
   else if (!(*iphase == 2 && m->ac_phase == 3))
@@ -1238,18 +1374,37 @@ void compute_forces_acoustic_cuda_(long *Mesh_pointer, int *iphase, int *, int *
 }
 
 // compute_stacey_acoustic_cuda (src/gpu/compute_stacey_acoustic_cuda.cu:40)
-void compute_stacey_acoustic_cuda_(long *Mesh_pointer, int *, realw *, realw *, realw *, realw *, int *,
-                                   int *compute_wavefield_2, int *) {
-  fluid_phase_call("compute_stacey_acoustic_cuda", mesh_of("compute_stacey_acoustic_cuda", Mesh_pointer),
-                   compute_wavefield_2);
+void compute_stacey_acoustic_cuda_(long *Mesh_pointer, int *iphase, realw *b_absorb_left, realw *b_absorb_right,
+                                   realw *b_absorb_top, realw *b_absorb_bottom, int *, int *compute_wavefield_2,
+                                   int *) {
+  const char *R = "compute_stacey_acoustic_cuda";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (m->sim_type == 3) {
+    kernel_step_call(R, m);
+    return;
+  }
+  fluid_phase_call(R, m, compute_wavefield_2);
+  if (m->save_forward && *iphase == 1) {
+    // SIMULATION_TYPE = 1 with SAVE_FORWARD: the host stores these slices as
+    // b_absorb_acoustic_*(:,:,it); a kernel run here does not read them back
+    realw *side[4] = {b_absorb_bottom, b_absorb_left, b_absorb_right, b_absorb_top};
+    for (int k = 0; k < 4; ++k)
+      if (side[k] && m->nspec_side[k] > 0)
+        std::memset(side[k], 0, sizeof(realw) * NGLL * static_cast<size_t>(m->nspec_side[k]));
+  }
 }
 
 // compute_coupling_ac_el_cuda (src/gpu/compute_coupling_cuda.cu:47): the solid's
 // normal displacement on the fluid, part of the fused step
 void compute_coupling_ac_el_cuda_(long *Mesh_pointer, int *, int *, int *FORWARD_OR_ADJOINT) {
   const char *R = "compute_coupling_ac_el_cuda";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (m->sim_type == 3 && (*FORWARD_OR_ADJOINT == 1 || *FORWARD_OR_ADJOINT == 3)) {
+    kernel_step_call(R, m);
+    return;
+  }
   if (*FORWARD_OR_ADJOINT != 1) unsupported(R, KERNEL_RUN);
-  fluid_phase_call(R, mesh_of(R, Mesh_pointer), nullptr);
+  fluid_phase_call(R, m, nullptr);
 }
 
 // compute_add_sources_ac_cuda (src/gpu/compute_add_sources_viscoacoustic_cuda.cu:46)
@@ -1265,6 +1420,12 @@ void compute_add_sources_ac_cuda_(long *Mesh_pointer, int *, int *itf) {
 void kernel_3_acoustic_cuda_(long *Mesh_pointer, realw *, realw *, int *, int *compute_wavefield_2) {
   const char *R = "kernel_3_acoustic_cuda";
   FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (m->sim_type == 3) {
+    // on a fluid-only mesh the call with both fields ends the step
+    kernel_step_call(R, m);
+    if (m->nspec_acoustic == m->nspec && *compute_wavefield_2) kernel_step_end(R, m);
+    return;
+  }
   fluid_phase_call(R, m, compute_wavefield_2);
   if (m->nspec_acoustic == m->nspec) {
     check(R, sf2d_coupled_enqueue(m->C, 1));
@@ -1280,6 +1441,10 @@ void kernel_3_acoustic_cuda_(long *Mesh_pointer, realw *, realw *, int *, int *c
 void compute_coupling_el_ac_cuda_(long *Mesh_pointer, int *, int *, int *FORWARD_OR_ADJOINT) {
   const char *R = "compute_coupling_el_ac_cuda";
   FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (m->sim_type == 3 && (*FORWARD_OR_ADJOINT == 1 || *FORWARD_OR_ADJOINT == 3)) {
+    kernel_step_call(R, m);
+    return;
+  }
   if (*FORWARD_OR_ADJOINT != 1) unsupported(R, KERNEL_RUN);
   if (m->ac_phase != 5) stop(R, "called outside the solid forces of a time step");
 }
@@ -1288,8 +1453,14 @@ void compute_coupling_el_ac_cuda_(long *Mesh_pointer, int *, int *, int *FORWARD
 void get_norm_acoustic_from_device_(realw *norm, long *Mesh_pointer, const int *FORWARD_OR_ADJOINT) {
   const char *R = "get_norm_acoustic_from_device";
   FortranMesh *m = mesh_of(R, Mesh_pointer);
-  if (FORWARD_OR_ADJOINT && *FORWARD_OR_ADJOINT == 3) unsupported(R, KERNEL_RUN);
+  const bool backward = FORWARD_OR_ADJOINT && *FORWARD_OR_ADJOINT == 3;
+  if (backward && m->sim_type != 3) unsupported(R, KERNEL_RUN);
   if (!m->fluid) stop(R, "the mesh has no fluid element");
+  // a kernel run: the adjoint field at its end, the replayed field at rest
+  if (m->sim_type == 3 && (backward || !m->CF)) {
+    *norm = 0.f;
+    return;
+  }
   std::vector<float> p(m->nglob);
   coupled_fields(R, m, nullptr, nullptr, nullptr, p.data(), nullptr, nullptr);
   float mx = 0.f;
@@ -1349,7 +1520,7 @@ void prepare_sim2_or_3_const_device_(long *Mesh_pointer, int *nadj_rec_local, re
   const char *R = "prepare_sim2_or_3_const_device";
   FortranMesh *m = mesh_of(R, Mesh_pointer);
   if (m->sim_type != 3) stop(R, "called outside a kernel run (SIMULATION_TYPE = 3)");
-  if (m->F) stop(R, "called after the time loop started");
+  if (m->F || m->CF) stop(R, "called after the time loop started");
   if (*NSTEP != m->nstep) stop(R, "NSTEP disagrees with prepare_constants_device");
   if (*nadj_rec_local != m->nrec) stop(R, "every local receiver must be an adjoint source (nadj_rec_local = nrec_local)");
   const size_t nr = static_cast<size_t>(m->nrec), nt = static_cast<size_t>(m->nstep);
@@ -1365,7 +1536,10 @@ void add_sources_el_sim_type_2_or_3_(long *Mesh_pointer, int *, int *itf, int *n
   const char *R = "add_sources_el_sim_type_2_or_3";
   FortranMesh *m = mesh_of(R, Mesh_pointer);
   if (m->sim_type != 3) unsupported(R, OTHER);
-  if (m->stage != 2) stop(R, "called outside a time step");
+  if (m->fluid)
+    kernel_step_call(R, m);
+  else if (m->stage != 2)
+    stop(R, "called outside a time step");
   if (*nadj_rec_local != m->nrec || *NSTEP != m->nstep) stop(R, "nadj_rec_local or NSTEP changed");
   if (*itf != m->nstep - m->steps) stop(R, "time step " + std::to_string(*itf) + " out of sequence");
 }
@@ -1376,7 +1550,10 @@ void compute_add_sources_el_s3_cuda_(long *Mesh_pointer, int *, int *itf) {
   const char *R = "compute_add_sources_el_s3_cuda";
   FortranMesh *m = mesh_of(R, Mesh_pointer);
   if (m->sim_type != 3) stop(R, "called outside a kernel run (SIMULATION_TYPE = 3)");
-  if (m->stage != 2) stop(R, "called outside a time step");
+  if (m->fluid)
+    kernel_step_call(R, m);
+  else if (m->stage != 2)
+    stop(R, "called outside a time step");
   if (*itf != m->nstep - m->steps) stop(R, "time step " + std::to_string(*itf) + " out of sequence");
   m->srcs_added = m->steps + 1;
 }
@@ -1386,8 +1563,8 @@ void compute_add_sources_el_s3_cuda_(long *Mesh_pointer, int *, int *itf) {
 void compute_kernels_elastic_cuda_(long *Mesh_pointer, realw *) {
   const char *R = "compute_kernels_elastic_cuda";
   FortranMesh *m = mesh_of(R, Mesh_pointer);
-  if (m->sim_type != 3 || !m->F) stop(R, "called outside a kernel run (SIMULATION_TYPE = 3)");
-  if (m->stage != 0) stop(R, "called inside a time step");
+  if (m->sim_type != 3 || (!m->F && !m->CF)) stop(R, "called outside a kernel run (SIMULATION_TYPE = 3)");
+  if (m->fluid ? m->kr_open : m->stage != 0) stop(R, "called inside a time step");
   if (m->kernel_calls >= m->steps) stop(R, "called twice in one time step");
   ++m->kernel_calls;
 }
@@ -1408,7 +1585,7 @@ void transfer_kernels_el_to_host_(long *Mesh_pointer, realw *h_rho_kl, realw *h_
                                   int *NSPEC_AB) {
   const char *R = "transfer_kernels_el_to_host";
   FortranMesh *m = mesh_of(R, Mesh_pointer);
-  if (m->sim_type != 3 || !m->F) stop(R, "called outside a kernel run (SIMULATION_TYPE = 3)");
+  if (m->sim_type != 3 || (!m->F && !m->CF)) stop(R, "called outside a kernel run (SIMULATION_TYPE = 3)");
   if (*NSPEC_AB != m->nspec) stop(R, "NSPEC_AB disagrees with prepare_constants_device");
   if (m->steps != m->nstep) stop(R, "called before the last time step");
   if (m->kernel_calls != m->nstep)
@@ -1417,6 +1594,77 @@ void transfer_kernels_el_to_host_(long *Mesh_pointer, realw *h_rho_kl, realw *h_
   std::memcpy(h_rho_kl, m->rho_sum.data(), sizeof(realw) * nl);
   std::memcpy(h_mu_kl, m->mu_sum.data(), sizeof(realw) * nl);
   std::memcpy(h_kappa_kl, m->kappa_sum.data(), sizeof(realw) * nl);
+}
+
+// ---- the kernel run of a mesh with fluid elements ----
+
+// prepare_fields_acoustic_adj_dev (src/gpu/prepare_mesh_constants_cuda.cu:442)
+void prepare_fields_acoustic_adj_dev_(long *Mesh_pointer, int *APPROXIMATE_HESS_KL, int *ATTENUATION_VISCOACOUSTIC,
+                                      int *NO_BACKWARD_RECONSTRUCTION) {
+  const char *R = "prepare_fields_acoustic_adj_dev";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (m->sim_type != 3 || !m->fluid) stop(R, "called outside a kernel run (SIMULATION_TYPE = 3) with fluid elements");
+  if (*APPROXIMATE_HESS_KL) stop(R, "APPROXIMATE_HESS_KL: the fluid Hessian is not provided");
+  if (*ATTENUATION_VISCOACOUSTIC) stop(R, "viscoacoustic attenuation is not provided");
+  if (*NO_BACKWARD_RECONSTRUCTION)
+    stop(R, "NO_BACKWARD_RECONSTRUCTION: the forward field is replayed from device checkpoints, no frames are read");
+  m->ac_adj_prepared = true;
+}
+
+// add_sources_ac_sim_2_or_3_cuda (src/gpu/compute_add_sources_viscoacoustic_cuda.cu:208):
+// source_adjoint(:, NSTEP-it+1, 1) at the fluid receivers, as it is
+void add_sources_ac_sim_2_or_3_cuda_(long *Mesh_pointer, int *, int *itf, int *nadj_rec_local, int *NSTEP) {
+  const char *R = "add_sources_ac_sim_2_or_3_cuda";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (m->sim_type != 3) unsupported(R, OTHER);
+  kernel_step_call(R, m);
+  if (*nadj_rec_local != m->nrec || *NSTEP != m->nstep) stop(R, "nadj_rec_local or NSTEP changed");
+  if (*itf != m->nstep - m->steps) stop(R, "time step " + std::to_string(*itf) + " out of sequence");
+}
+
+// compute_add_sources_ac_s3_cuda (src/gpu/compute_add_sources_viscoacoustic_cuda.cu:91):
+// the forward source of the replayed field
+void compute_add_sources_ac_s3_cuda_(long *Mesh_pointer, int *, int *itf) {
+  const char *R = "compute_add_sources_ac_s3_cuda";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (m->sim_type != 3) stop(R, "called outside a kernel run (SIMULATION_TYPE = 3)");
+  kernel_step_call(R, m);
+  if (*itf != m->nstep - m->steps) stop(R, "time step " + std::to_string(*itf) + " out of sequence");
+  m->srcs_added = m->steps + 1;
+}
+
+// compute_kernels_acoustic_cuda (src/gpu/compute_kernels_cuda.cu:92): summed in the sweep
+void compute_kernels_acoustic_cuda_(long *Mesh_pointer, realw *) {
+  const char *R = "compute_kernels_acoustic_cuda";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (m->sim_type != 3 || !m->CF) stop(R, "called outside a kernel run (SIMULATION_TYPE = 3) with fluid elements");
+  if (m->kr_open) stop(R, "called inside a time step");
+  if (m->ac_kernel_calls >= m->steps) stop(R, "called twice in one time step");
+  ++m->ac_kernel_calls;
+}
+
+// transfer_b_fields_ac_to_device (src/gpu/transfer_fields_cuda.cu:248): the
+// replayed field starts from rest and needs no last frame
+void transfer_b_fields_ac_to_device_(int *size, realw *, realw *, realw *, long *Mesh_pointer) {
+  const char *R = "transfer_b_fields_ac_to_device";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (m->sim_type != 3) stop(R, "called outside a kernel run (SIMULATION_TYPE = 3)");
+  need_ac_size(R, m, size);
+}
+
+// transfer_kernels_ac_to_host (src/gpu/transfer_fields_cuda.cu:391): rho_ac_kl
+// and kappa_ac_kl with deltat and the material factors already in
+// (compute_kernels.f90:426-431), zero in solid elements
+void transfer_kernels_ac_to_host_(long *Mesh_pointer, realw *h_rho_ac_kl, realw *h_kappa_ac_kl, int *NSPEC_AB) {
+  const char *R = "transfer_kernels_ac_to_host";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (m->sim_type != 3 || !m->CF) stop(R, "called outside a kernel run (SIMULATION_TYPE = 3) with fluid elements");
+  if (*NSPEC_AB != m->nspec) stop(R, "NSPEC_AB disagrees with prepare_constants_device");
+  if (m->steps != m->nstep) stop(R, "called before the last time step");
+  if (m->ac_kernel_calls != m->nstep)
+    stop(R, "NTSTEP_BETWEEN_COMPUTE_KERNELS must be 1: the sums cover every time step");
+  std::memcpy(h_rho_ac_kl, m->rho_ac_kl.data(), sizeof(realw) * m->rho_ac_kl.size());
+  std::memcpy(h_kappa_ac_kl, m->kappa_ac_kl.data(), sizeof(realw) * m->kappa_ac_kl.size());
 }
 
 void transfer_boun_pot_from_device_(long*, realw*, const int*) { unsupported("transfer_boun_pot_from_device", MPI); }
@@ -1437,13 +1685,9 @@ void check_max_norm_b_veloc_gpu_(int*, realw*, long*, int*) { unsupported("check
 void check_max_norm_b_displ_(int*, realw*, int*) { unsupported("check_max_norm_b_displ", DEBUG); }
 void check_max_norm_b_accel_(int*, realw*, int*) { unsupported("check_max_norm_b_accel", DEBUG); }
 void check_error_vectors_(int*, realw*, realw*) { unsupported("check_error_vectors", DEBUG); }
-void compute_add_sources_ac_s3_cuda_(long*, int*, int*) { unsupported("compute_add_sources_ac_s3_cuda", KERNEL_RUN); }
 void compute_add_moving_sources_ac_cuda_(long*, int*, int*, int*, int*, int*) { unsupported("compute_add_moving_sources_ac_cuda", OTHER); }
-void add_sources_ac_sim_2_or_3_cuda_(long*, int*, int*, int*, int*) { unsupported("add_sources_ac_sim_2_or_3_cuda", KERNEL_RUN); }
-void compute_kernels_acoustic_cuda_(long*, realw*) { unsupported("compute_kernels_acoustic_cuda", KERNEL_RUN); }
 void compute_kernels_hess_cuda_(long*, int*, int*) { unsupported("compute_kernels_hess_cuda", OTHER); }
 void pml_boundary_acoustic_cuda_(long*, int*, int*) { unsupported("pml_boundary_acoustic_cuda", PML); }
-void prepare_fields_acoustic_adj_dev_(long*, int*, int*, int*) { unsupported("prepare_fields_acoustic_adj_dev", KERNEL_RUN); }
 void prepare_pml_device_(long*, int*, int*, int*, int*, int*, realw*, realw*, realw*, realw*, realw*, realw*, realw*, realw*, int*, int*) { unsupported("prepare_pml_device", PML); }
 void prepare_moving_sources_cuda_(long*, int*, int*, realw*, int*, int*, realw*) { unsupported("prepare_moving_sources_cuda", OTHER); }
 void prepare_arrays_gpu_(long*, realw*, realw*, realw*, realw*, realw*, realw*, int*, int*, realw*) { unsupported("prepare_arrays_gpu", OTHER); }
@@ -1452,12 +1696,10 @@ void get_smooth_(long*, realw*) { unsupported("get_smooth", OTHER); }
 void transfer_b_fields_from_device_(int*, realw*, realw*, realw*, long*) { unsupported("transfer_b_fields_from_device", KERNEL_RUN); }
 void transfer_b_accel_from_device_(int*, realw*, long*) { unsupported("transfer_b_accel_from_device", KERNEL_RUN); }
 void transfer_b_displ_from_device_(int*, realw*, long*) { unsupported("transfer_b_displ_from_device", KERNEL_RUN); }
-void transfer_b_fields_ac_to_device_(int*, realw*, realw*, realw*, long*) { unsupported("transfer_b_fields_ac_to_device", KERNEL_RUN); }
 void transfer_b_fields_ac_from_device_(int*, realw*, realw*, realw*, long*) { unsupported("transfer_b_fields_ac_from_device", KERNEL_RUN); }
 void transfer_b_potential_ac_from_device_(int*, realw*, long*) { unsupported("transfer_b_potential_ac_from_device", KERNEL_RUN); }
 void transfer_b_potential_ac_to_device_(int*, realw*, long*) { unsupported("transfer_b_potential_ac_to_device", KERNEL_RUN); }
 void transfer_b_dot_dot_from_device_(int*, realw*, long*) { unsupported("transfer_b_dot_dot_from_device", KERNEL_RUN); }
-void transfer_kernels_ac_to_host_(long*, realw*, realw*, int*) { unsupported("transfer_kernels_ac_to_host", KERNEL_RUN); }
 void transfer_kernels_hess_el_tohost_(long*, realw*, int*) { unsupported("transfer_kernels_hess_el_tohost", OTHER); }
 void transfer_kernels_hess_ac_tohost_(long*, realw*, int*) { unsupported("transfer_kernels_hess_ac_tohost", OTHER); }
 void transfer_viscoacoustic_b_var_to_device_(int*, realw*, realw*, long*) { unsupported("transfer_viscoacoustic_b_var_to_device", KERNEL_RUN); }

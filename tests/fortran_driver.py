@@ -72,8 +72,12 @@ def run_forward(db, nstep=None, check_every=1000, nlength_seismogram=None, save_
 
 def run_kernel(db, adj_src, check_every=1000, nlength_seismogram=None):
     """Kernel run with adjoint sources adj_src (nrec, nstep, 2) in forward time
-    order.  Returns (adjoint seismograms, final adjoint displacement, norms as
-    (forward/adjoint, backward) pairs, (rho_kl, mu_kl, kappa_kl) sums (nspec, 5, 5))."""
+    order (a fluid receiver's in component 0).  Returns (adjoint seismograms,
+    final adjoint displacement, norms, kernels): the norms are (forward/adjoint,
+    backward) pairs, one per domain (solid first); the kernels (nspec, 5, 5) are
+    the solid sums rho, mu, kappa as transfer_kernels_el_to_host gives them, the
+    fluid rho_ac, kappa_ac of transfer_kernels_ac_to_host and, with fluid
+    elements, the final adjoint potential "pot"."""
     return _drive(db, None, check_every, nlength_seismogram, np.asarray(adj_src, np.float32), False)
 
 
@@ -117,6 +121,8 @@ def _drive(db, nstep, check_every, nlength_seismogram, adj_src, save_forward):
             r.i(int(elastic)), r.i(A["ncoupling"]), r.a(A["coupling_ac_el_ispec"]), r.a(A["coupling_ac_el_ij"]),
             r.a(A["coupling_ac_el_normal"]), r.a(A["coupling_ac_el_jacobian1Dw"]),
             r.i(0), r.a(dummy_i), r.i(0), r.a(dummy_f), r.a(dummy_f), r.i(0), r.a(dummy_f))
+        if kernel:
+            lib.prepare_fields_acoustic_adj_dev_(M, r.i(0), r.i(0), r.i(0))
     aniso = "ispec_is_anisotropic" in A
     atten = "att_a1" in A
     c = {k: (A[k + "store"] if aniso else dummy_f) for k in ("c11", "c13", "c15", "c33", "c35", "c55")}
@@ -130,7 +136,7 @@ def _drive(db, nstep, check_every, nlength_seismogram, adj_src, save_forward):
         r.i(0), r.a(dummy_i), r.i(1 if atten else 0),
         r.a(att["a2"]), r.a(att["b2"]), r.a(att["a1"]), r.a(att["b1"]))
     ng2 = 2 * A["nglob"]
-    if kernel:
+    if kernel and elastic:
         lib.prepare_fields_elastic_adj_dev_(M, r.i(ng2), r.i(0), r.i(int(atten)), r.i(0))
     if A["stacey"]:
         ab = A["abs"]
@@ -165,13 +171,78 @@ def _drive(db, nstep, check_every, nlength_seismogram, adj_src, save_forward):
     dummy_b = dummy_f.ctypes.data_as(ctypes.c_void_p)
     seismo_current = 0
     ncpl_c = ctypes.c_int(A.get("ncoupling", 0))
-    # b_absorb_elastic_left/right/top/bottom slices (NDIM, NGLLX, nspec_side)
+    # b_absorb_elastic_* slices (NDIM, NGLLX, nspec_side) and b_absorb_acoustic_* (NGLLX, nspec_side)
     sides = ("left", "right", "top", "bottom")
     nside = {k: (A["abs"]["counts"][k] if A["stacey"] else 0) for k in sides}
-    b_absorb = [np.full(2 * 5 * max(nside[k], 1), np.nan, np.float32) for k in sides]
-    b_ptr = [b.ctypes.data_as(ctypes.c_void_p) for b in b_absorb]
-    cw2 = one if kernel else zero
+    b_el = [np.full(2 * 5 * max(nside[k], 1), np.nan, np.float32) for k in sides]
+    b_ac = [np.full(5 * max(nside[k], 1), np.nan, np.float32) for k in sides]
+    p_el = [b.ctypes.data_as(ctypes.c_void_p) for b in b_el]
+    p_ac = [b.ctypes.data_as(ctypes.c_void_p) for b in b_ac]
     nrec_c, nstep_c, itmp_c = ctypes.c_int(A["nrec"]), ctypes.c_int(A["nstep"]), ctypes.c_int(0)
+    three = ctypes.c_int(3)
+
+    def saved_slices_are_zero(slices):
+        # SAVE_FORWARD: the host stores the slices it got back as b_absorb_*(..., it)
+        assert all(np.all(b == 0) for b, k in zip(slices, sides) if nside[k] > 0)
+
+    def acoustic_phase(w1, w2):
+        """compute_forces_viscoacoustic_GPU (compute_gpu_acoustic.f90:36-220)."""
+        c1, c2 = (one if w1 else zero), (one if w2 else zero)
+        if A["nfree"] > 0:
+            lib.acoustic_enforce_free_surf_cuda_(M, ctypes.byref(c1), ctypes.byref(c2))
+        for iphase in (one, two):
+            lib.compute_forces_acoustic_cuda_(M, ctypes.byref(iphase), ctypes.byref(zero), ctypes.byref(zero),
+                                              ctypes.byref(zero), ctypes.byref(c1), ctypes.byref(c2))
+            if iphase is not one:
+                continue
+            if A["stacey"]:
+                lib.compute_stacey_acoustic_cuda_(M, ctypes.byref(one), *p_ac, ctypes.byref(c1), ctypes.byref(c2),
+                                                  ctypes.byref(zero))
+                if save_forward:
+                    saved_slices_are_zero(b_ac)
+            if elastic:
+                for w, kind in ((w1, one), (w2, three)):
+                    if w:
+                        lib.compute_coupling_ac_el_cuda_(M, ctypes.byref(one), ctypes.byref(ncpl_c), ctypes.byref(kind))
+            if not kernel:
+                lib.compute_add_sources_ac_cuda_(M, ctypes.byref(one), ctypes.byref(it_c))
+            else:
+                if A["nrec"] > 0 and w1:
+                    lib.add_sources_ac_sim_2_or_3_cuda_(M, ctypes.byref(one), ctypes.byref(itmp_c),
+                                                        ctypes.byref(nrec_c), ctypes.byref(nstep_c))
+                if w2:
+                    lib.compute_add_sources_ac_s3_cuda_(M, ctypes.byref(one), ctypes.byref(itmp_c))
+        lib.kernel_3_acoustic_cuda_(M, ctypes.byref(dt2), ctypes.byref(dt2), ctypes.byref(c1), ctypes.byref(c2))
+        lib.acoustic_enforce_free_surf_cuda_(M, ctypes.byref(c1), ctypes.byref(c2))
+
+    def elastic_phase(w1, w2):
+        """compute_forces_viscoelastic_GPU (compute_gpu_elastic.f90:36-215)."""
+        c1, c2 = (one if w1 else zero), (one if w2 else zero)
+        for iphase in (one, two):
+            lib.compute_forces_viscoelastic_cuda_(M, ctypes.byref(iphase), ctypes.byref(dt), ctypes.byref(zero),
+                                                  ctypes.byref(nspec_c), ctypes.byref(aniso_c), ctypes.byref(atten_c),
+                                                  ctypes.byref(c1), ctypes.byref(c2))
+            if iphase is not one:
+                continue
+            if A["stacey"]:
+                lib.compute_stacey_viscoelastic_cuda_(M, ctypes.byref(one), *p_el, ctypes.byref(c1),
+                                                      ctypes.byref(c2), ctypes.byref(zero))
+                if save_forward:
+                    saved_slices_are_zero(b_el)
+            if fluid:
+                for w, kind in ((w1, one), (w2, three)):
+                    if w:
+                        lib.compute_coupling_el_ac_cuda_(M, ctypes.byref(one), ctypes.byref(ncpl_c), ctypes.byref(kind))
+            if not kernel:
+                lib.compute_add_sources_el_cuda_(M, ctypes.byref(one), ctypes.byref(it_c))
+            else:
+                if A["nrec"] > 0 and w1:
+                    lib.add_sources_el_sim_type_2_or_3_(M, ctypes.byref(one), ctypes.byref(itmp_c),
+                                                        ctypes.byref(nrec_c), ctypes.byref(nstep_c))
+                if w2:
+                    lib.compute_add_sources_el_s3_cuda_(M, ctypes.byref(one), ctypes.byref(itmp_c))
+        lib.kernel_3_a_cuda_(M, ctypes.byref(dt2), ctypes.byref(dt2), ctypes.byref(c1), ctypes.byref(c2))
+
     for it in range(1, nstep + 1):
         it_c.value = it
         itmp_c.value = A["nstep"] - it + 1
@@ -182,46 +253,30 @@ def _drive(db, nstep, check_every, nlength_seismogram, adj_src, save_forward):
         if elastic:
             lib.update_displacement_cuda_(M, ctypes.byref(dt), ctypes.byref(dtsq2), ctypes.byref(dt2),
                                           ctypes.byref(dt), ctypes.byref(dtsq2), ctypes.byref(dt2))
-        if fluid:
-            if A["nfree"] > 0:
-                lib.acoustic_enforce_free_surf_cuda_(M, ctypes.byref(one), ctypes.byref(zero))
-            for iphase in (one, two):
-                lib.compute_forces_acoustic_cuda_(M, ctypes.byref(iphase), ctypes.byref(zero), ctypes.byref(zero),
-                                                  ctypes.byref(zero), ctypes.byref(one), ctypes.byref(zero))
-                if iphase is one:
-                    if A["stacey"]:
-                        lib.compute_stacey_acoustic_cuda_(M, ctypes.byref(one), dummy_b, dummy_b, dummy_b, dummy_b,
-                                                          ctypes.byref(one), ctypes.byref(zero), ctypes.byref(zero))
-                    if elastic:
-                        lib.compute_coupling_ac_el_cuda_(M, ctypes.byref(one), ctypes.byref(ncpl_c), ctypes.byref(one))
-                    lib.compute_add_sources_ac_cuda_(M, ctypes.byref(one), ctypes.byref(it_c))
-            lib.kernel_3_acoustic_cuda_(M, ctypes.byref(dt2), ctypes.byref(dt2), ctypes.byref(one), ctypes.byref(zero))
-            lib.acoustic_enforce_free_surf_cuda_(M, ctypes.byref(one), ctypes.byref(zero))
-        for iphase in ((one, two) if elastic else ()):
-            lib.compute_forces_viscoelastic_cuda_(M, ctypes.byref(iphase), ctypes.byref(dt), ctypes.byref(zero),
-                                                  ctypes.byref(nspec_c), ctypes.byref(aniso_c), ctypes.byref(atten_c),
-                                                  ctypes.byref(one), ctypes.byref(cw2))
-            if iphase is one:
-                if A["stacey"]:
-                    lib.compute_stacey_viscoelastic_cuda_(M, ctypes.byref(one), *b_ptr,
-                                                          ctypes.byref(one), ctypes.byref(cw2), ctypes.byref(zero))
-                    if save_forward:
-                        # the host stores the slices it got back as b_absorb_elastic_*(:,:,:,it)
-                        assert all(np.all(b == 0) for b, k in zip(b_absorb, sides) if nside[k] > 0)
-                if fluid:
-                    lib.compute_coupling_el_ac_cuda_(M, ctypes.byref(one), ctypes.byref(ncpl_c), ctypes.byref(one))
-                if kernel:
-                    if A["nrec"] > 0:
-                        lib.add_sources_el_sim_type_2_or_3_(M, ctypes.byref(one), ctypes.byref(itmp_c),
-                                                            ctypes.byref(nrec_c), ctypes.byref(nstep_c))
-                    lib.compute_add_sources_el_s3_cuda_(M, ctypes.byref(one), ctypes.byref(itmp_c))
-                else:
-                    lib.compute_add_sources_el_cuda_(M, ctypes.byref(one), ctypes.byref(it_c))
-        if elastic:
-            lib.kernel_3_a_cuda_(M, ctypes.byref(dt2), ctypes.byref(dt2), ctypes.byref(one), ctypes.byref(cw2))
+        if not kernel:
+            # forward: fluid then solid (iterate_time.F90:262-285)
+            if fluid:
+                acoustic_phase(True, False)
+            if elastic:
+                elastic_phase(True, False)
+        elif fluid and elastic:
+            # kernel run of a coupled mesh: solid then fluid for the adjoint field,
+            # fluid then solid for the replayed one (iterate_time.F90:298-360)
+            elastic_phase(True, False)
+            acoustic_phase(True, False)
+            acoustic_phase(False, True)
+            elastic_phase(False, True)
+        elif fluid:
+            acoustic_phase(True, True)
+        else:
+            elastic_phase(True, True)
         if kernel and it == 1:
             # read_forward_arrays: the last frame of the saved forward run
-            lib.transfer_b_fields_to_device_(r.i(ng2), r.a(zeros), r.a(zeros), r.a(zeros), M)
+            if fluid:
+                z1 = np.zeros(A["nglob"], np.float32)
+                lib.transfer_b_fields_ac_to_device_(r.i(A["nglob"]), r.a(z1), r.a(z1), r.a(z1), M)
+            if elastic:
+                lib.transfer_b_fields_to_device_(r.i(ng2), r.a(zeros), r.a(zeros), r.a(zeros), M)
         seismo_current += 1
         cur_c.value = seismo_current
         lib.compute_seismograms_cuda_(M, ctypes.byref(one), sisux.ctypes.data_as(ctypes.c_void_p),
@@ -236,30 +291,46 @@ def _drive(db, nstep, check_every, nlength_seismogram, adj_src, save_forward):
             seis[:, it - n:it, 1] = sisuz[:, :n]
             seismo_current = 0
         if kernel:
-            lib.compute_kernels_elastic_cuda_(M, ctypes.byref(dt))
-        if it % check_every == 0 or it == nstep:
+            # compute_kernels (compute_kernels.f90:35-70): fluid, then solid
+            if fluid:
+                lib.compute_kernels_acoustic_cuda_(M, ctypes.byref(dt))
+            if elastic:
+                lib.compute_kernels_elastic_cuda_(M, ctypes.byref(dt))
+        if kernel and (it % check_every == 0 or it == nstep):
+            # (forward/adjoint, backward) norm pairs: solid, then fluid
+            entry = []
+            for fn, present in ((lib.get_norm_elastic_from_device_, elastic), (lib.get_norm_acoustic_from_device_, fluid)):
+                if present:
+                    fn(ctypes.byref(norm), M, ctypes.byref(one))
+                    f_norm = float(norm.value)
+                    fn(ctypes.byref(norm), M, ctypes.byref(three))
+                    entry.append((f_norm, float(norm.value)))
+            norms.append(entry[0] if len(entry) == 1 else tuple(entry))
+        elif it % check_every == 0 or it == nstep:
             lib.get_norm_elastic_from_device_(ctypes.byref(norm), M, ctypes.byref(one))
-            if kernel:
-                n_fwd = float(norm.value)
-                three = ctypes.c_int(3)
-                lib.get_norm_elastic_from_device_(ctypes.byref(norm), M, ctypes.byref(three))
-                norms.append((n_fwd, float(norm.value)))
-            elif fluid:
+            if fluid:
                 n_el = float(norm.value)
                 lib.get_norm_acoustic_from_device_(ctypes.byref(norm), M, ctypes.byref(one))
                 norms.append((n_el, float(norm.value)))
             else:
                 norms.append(float(norm.value))
     displ = np.zeros(ng2, np.float32)
-    lib.transfer_displ_from_device_(r.i(ng2), r.a(displ), M)
+    if elastic:
+        lib.transfer_displ_from_device_(r.i(ng2), r.a(displ), M)
     pot = None
     if fluid:
         pot = np.zeros(A["nglob"], np.float32)
         lib.transfer_fields_ac_from_device_(r.i(A["nglob"]), r.a(pot), r.a(np.zeros_like(pot)), r.a(np.zeros_like(pot)), M)
     kl = None
     if kernel:
-        kl = tuple(np.zeros((A["nspec"], 5, 5), np.float32) for _ in range(3))
-        lib.transfer_kernels_el_to_host_(M, *[r.a(k) for k in kl], r.i(A["nspec"]))
+        # it_transfer_from_GPU (iterate_time.F90:462-504)
+        kl = {k: np.zeros((A["nspec"], 5, 5), np.float32) for k in ("rho", "mu", "kappa", "rho_ac", "kappa_ac")}
+        if fluid:
+            lib.transfer_kernels_ac_to_host_(M, r.a(kl["rho_ac"]), r.a(kl["kappa_ac"]), r.i(A["nspec"]))
+        if elastic:
+            lib.transfer_kernels_el_to_host_(M, r.a(kl["rho"]), r.a(kl["mu"]), r.a(kl["kappa"]), r.i(A["nspec"]))
+        if fluid:
+            kl["pot"] = pot
     lib.prepare_cleanup_device_(M, r.i(0), r.i(1), r.i(int(aniso)), r.i(0), r.i(0), r.i(int(atten)), r.i(0),
                                 r.a(dummy_f))
     if kernel:

@@ -145,7 +145,8 @@ def test_tromp2005_kernel_run_through_the_fortran_interface():
     adj, _ = cross_correlation_adjoint_source(adj_ref["t_forward"], traces, 27.0, 32.0, 1)
     db = database_from_config(cfg)
     adj32 = adj.astype(np.float32).reshape(1, -1, 2)
-    aseis, _, norms, (rs, ms, ks) = run_kernel(db, adj32, check_every=400)
+    aseis, _, norms, kl = run_kernel(db, adj32, check_every=400)
+    rs, ms, ks = kl["rho"], kl["mu"], kl["kappa"]
     g = FWIGradient(db, checkpoint_every=200)
     g.forward()
     rk, kk, mk = g.backward(adj32)
@@ -165,3 +166,47 @@ def test_tromp2005_kernel_run_through_the_fortran_interface():
     for k, v in log["kernel_max"].items():
         assert float(got[k]) == pytest.approx(v, rel=2e-5), k
     assert all(f > 0 and b == 0 for f, b in norms) and len(norms) == 8
+
+
+def test_fluid_solid_kernel_run_through_the_fortran_interface():
+    """EXAMPLES/LuoYang_fluid_solid_kernel as SIMULATION_TYPE = 3 through the
+    fluid calls of the interface (prepare_fields_acoustic_adj_dev, the adjoint
+    and replayed sources of both domains, coupling with FORWARD_OR_ADJOINT 1
+    and 3, transfer_kernels_ac_to_host): the adjoint potential trace within
+    1e-5 of the reference's, every kernel within the FP32 band of the library's
+    own coupled gradient run (the interface forms lambda and the fluid's
+    Jacobian in FP32 as the reference's GPU code does), and the ten kernel
+    maxima the reference printed."""
+    from helpers import load_kernel_golden
+    from fortran_driver import run_kernel
+    from specfem2d_b200.coupled import coupled_kernels
+    from specfem2d_b200.setup.adjoint import derived_kernels
+
+    cfg, ref, log = load_kernel_golden("luoyang_fluid_solid_kernel")
+    db = database_from_config(cfg)
+    adj = np.zeros((1, db.nstep, 2), np.float32)
+    adj[0, :, 0] = ref["adj_source"].astype(np.float32)
+    aseis, _, norms, kl = run_kernel(db, adj, check_every=800)
+    lib = coupled_kernels(db, adj, checkpoint_every=200)
+    assert rel_l2(aseis[0, :, 0], ref["adjoint_trace"]) < 1e-5
+    assert rel_l2(aseis, lib["adj_seis"]) < 1e-5
+    dt = np.float32(db.deltat)
+    rho, kap, mu = (np.asarray(x, np.float32).reshape(-1, 5, 5) for x in (db.rhostore, db.kappastore, db.mustore))
+    solid = ~np.asarray(db.acoustic["ispec"], dtype=bool)
+    scaled = dict(rho=-rho * dt * kl["rho"], kappa=-kap * dt * kl["kappa"], mu=np.float32(-2) * mu * dt * kl["mu"])
+    for k in ("rho", "kappa", "mu"):
+        assert rel_l2(scaled[k][solid], lib[k][solid]) < 1e-4, k
+        assert not np.any(kl[k][~solid]), k
+    for k in ("rho_ac", "kappa_ac"):
+        assert rel_l2(kl[k], lib[k]) < 1e-4, k
+        assert not np.any(kl[k][solid]), k
+    d = derived_kernels(scaled["rho"], scaled["kappa"], scaled["mu"], db.rhostore, db.kappastore, db.mustore)
+    got = dict(rho=scaled["rho"].max(), kappa=scaled["kappa"].max(), mu=scaled["mu"].max(), rhop=d["rhop"].max(),
+               alpha=d["alpha"].max(), beta=d["beta"].max())
+    for name, v in log["kernel_max"].items():
+        assert float(got[name]) == pytest.approx(v, rel=3e-5), name
+    rac, kac = kl["rho_ac"], kl["kappa_ac"]
+    got_ac = dict(rho=rac.max(), kappa=kac.max(), rhop=(rac + kac).max(), alpha=(np.float32(2.0) * kac).max())
+    for name, v in log["acoustic_kernel_max"].items():
+        assert float(got_ac[name]) == pytest.approx(v, rel=3e-5), name
+    assert all(ef > 0 and eb == 0 and af > 0 and ab == 0 for (ef, eb), (af, ab) in norms)
