@@ -104,6 +104,18 @@ struct FortranMesh {
   int ac_kernel_calls = 0;           // compute_kernels_acoustic_cuda calls
   std::vector<int> s_elems, f_elems;  // whole-mesh element of each solid / fluid sub-mesh element
   std::vector<float> rho_ac_kl, kappa_ac_kl;  // whole-mesh element order, zero in solid elements
+  // CPML layer of a fluid-only mesh (prepare_pml_device): region per element,
+  // K, d, alpha per element point, the layer's outer-edge points
+  bool pml = false, have_pml = false;
+  std::vector<int> pml_region, pml_edge;
+  std::vector<double> pml_K_x, pml_K_z, pml_d_x, pml_d_z, pml_alpha_x, pml_alpha_z;
+  double pml_dt = 0.0;
+  // USE_TRICK_FOR_BETTER_PRESSURE reaches the library only with the first
+  // compute_seismograms_cuda, after the first step; the initial fields are kept
+  // until then so that a pressure run can be rebuilt with it and step 1 repeated
+  int use_trick = 0;
+  bool trick_checked = false;
+  std::vector<float> init_fields[6];
 };
 
 FortranMesh *mesh_of(const char *routine, const long *p) {
@@ -635,6 +647,30 @@ void build_coupled(const char *routine, FortranMesh &m) {
   a.hgammar = f_hgammar.data();
   a.rec_global = f_rec_global.data();
   a.tile_elems = 32;
+  std::vector<int> f_pml_region, f_pml_edge;
+  std::vector<double> f_pml[6];
+  if (m.pml) {
+    if (!m.have_pml) stop(routine, "prepare_pml_device has not been called");
+    f_pml_region = elem_rows(m.pml_region, F.elems, 1);
+    const std::vector<double> *src[6] = {&m.pml_K_x, &m.pml_K_z, &m.pml_d_x, &m.pml_d_z, &m.pml_alpha_x,
+                                         &m.pml_alpha_z};
+    for (int k = 0; k < 6; ++k) f_pml[k] = elem_rows(*src[k], F.elems, NGLL2);
+    for (int g : m.pml_edge) {
+      const int l = F.gmap[g];
+      if (l < 0) stop(routine, "a CPML edge point outside the fluid elements");
+      f_pml_edge.push_back(l);
+    }
+    a.pml_region = f_pml_region.data();
+    a.pml_K_x = f_pml[0].data();
+    a.pml_K_z = f_pml[1].data();
+    a.pml_d_x = f_pml[2].data();
+    a.pml_d_z = f_pml[3].data();
+    a.pml_alpha_x = f_pml[4].data();
+    a.pml_alpha_z = f_pml[5].data();
+    a.npml_edge = static_cast<int>(f_pml_edge.size());
+    a.pml_edge_iglob = f_pml_edge.data();
+    a.pml_dt = m.pml_dt;
+  }
   // --- coupling entries, the same faces for both directions
   sf2d_coupling_desc c{};
   std::vector<int> c_f, c_s;
@@ -646,7 +682,7 @@ void build_coupled(const char *routine, FortranMesh &m) {
   c.nrec_total = m.nrec;
   c.el_rec_global = s_rec_global.data();
   c.seismotype = m.d.seismotype;
-  c.use_trick = 0;
+  c.use_trick = m.use_trick;
   c.cosrot = m.d.cosrot;
   c.sinrot = m.d.sinrot;
   c.ncpl_ac = c.ncpl_el = static_cast<int>(c_f.size());
@@ -670,6 +706,10 @@ void build_coupled(const char *routine, FortranMesh &m) {
     auto ptr = [](std::vector<float> &v) -> const float * { return v.empty() ? nullptr : v.data(); };
     check(routine, sf2d_coupled_set_fields_global(m.C, ptr(m.staged_u), ptr(m.staged_v), ptr(m.staged_a),
                                                   ptr(m.staged_p), ptr(m.staged_pd), ptr(m.staged_pdd)));
+  }
+  if (m.d.seismotype == 4 && !m.trick_checked) {
+    std::vector<float> *st[6] = {&m.staged_u, &m.staged_v, &m.staged_a, &m.staged_p, &m.staged_pd, &m.staged_pdd};
+    for (int k = 0; k < 6; ++k) m.init_fields[k] = *st[k];
   }
   m.staged_u.clear();
   m.staged_v.clear();
@@ -827,7 +867,13 @@ void prepare_constants_device_(long *Mesh_pointer, int *h_NGLLX, int *NSPEC_AB, 
   if (!*P_SV) stop(R, "SH (membrane) waves are not provided: P_SV only");
   if (*SIMULATION_TYPE != 1 && *SIMULATION_TYPE != 3) unsupported(R, KERNEL_RUN);
   if (*SIMULATION_TYPE == 3 && *nlength_seismogram < 1) stop(R, "nlength_seismogram must be positive");
-  if (*PML_BOUNDARY_CONDITIONS) unsupported(R, PML);
+  if (*PML_BOUNDARY_CONDITIONS) {
+    // the reference's GPU path takes CPML layers in fluid-only meshes:
+    // compute_forces_viscoelastic_GPU stops them (compute_gpu_elastic.f90:100-101)
+    if (*nspec_acoustic != *NSPEC_AB) unsupported(R, PML);
+    if (*STACEY_BOUNDARY_CONDITIONS) stop(R, "CPML and Stacey conditions are exclusive");
+    if (*SIMULATION_TYPE != 1) stop(R, "kernel runs with CPML layers are not provided");
+  }
   if (*num_interfaces_ext_mesh > 0) unsupported(R, MPI);
   if (*h_NSIGTYPE != 1) stop(R, "one seismogram type per run (NSIGTYPE = 1)");
   const int st = h_seismotypeVec[0];
@@ -836,6 +882,7 @@ void prepare_constants_device_(long *Mesh_pointer, int *h_NGLLX, int *NSPEC_AB, 
             "and 6 (potential)");
   auto m = new FortranMesh();
   m->sim_type = *SIMULATION_TYPE;
+  m->pml = *PML_BOUNDARY_CONDITIONS != 0;
   if (*SAVE_FORWARD && *SIMULATION_TYPE == 1) {
     // a kernel run through this library replays the forward field from
     // checkpoints and reads neither the last frame nor the absorbed-boundary
@@ -1137,11 +1184,33 @@ void kernel_3_a_cuda_(long *Mesh_pointer, realw *, realw *, int *, int *compute_
 // buffer sisux/sisuz(nlength_seismogram, nrec_local) is filled when it is
 // full or at the last step
 void compute_seismograms_cuda_(long *Mesh_pointer_f, int *i_sigf, double *sisux, double *sisuz,
-                               int *seismo_currentf, int *nlength_seismogramf, int *, int *, int *, int *, int *itf,
-                               int *it_endf) {
+                               int *seismo_currentf, int *nlength_seismogramf, int *, int *,
+                               int *USE_TRICK_FOR_BETTER_PRESSURE, int *, int *itf, int *it_endf) {
   const char *R = "compute_seismograms_cuda";
   FortranMesh *m = mesh_of(R, Mesh_pointer_f);
   if (*i_sigf != 1) stop(R, "one seismogram type per run");
+  if (m->d.seismotype == 4 && m->C) {
+    // pressure from chi instead of chi_dot_dot (write_seismograms_cuda.cu:160-175)
+    const int trick = USE_TRICK_FOR_BETTER_PRESSURE && *USE_TRICK_FOR_BETTER_PRESSURE ? 1 : 0;
+    if (!m->trick_checked) {
+      m->trick_checked = true;
+      if (trick != m->use_trick) {
+        if (m->CF || m->steps != 1) stop(R, "USE_TRICK_FOR_BETTER_PRESSURE must be known before the run starts");
+        // rebuild the run with it from the kept initial fields and repeat step 1
+        m->use_trick = trick;
+        sf2d_coupled_destroy(m->C);
+        m->C = nullptr;
+        std::vector<float> *st[6] = {&m->staged_u, &m->staged_v, &m->staged_a, &m->staged_p, &m->staged_pd,
+                                     &m->staged_pdd};
+        for (int k = 0; k < 6; ++k) *st[k] = std::move(m->init_fields[k]);
+        build_solver(R, *m);
+        check(R, sf2d_coupled_enqueue(m->C, 1));
+      }
+      for (auto &f : m->init_fields) std::vector<float>().swap(f);
+    } else if (trick != m->use_trick) {
+      stop(R, "USE_TRICK_FOR_BETTER_PRESSURE changed during the run");
+    }
+  }
   if (m->nrec == 0) return;
   const int j = *seismo_currentf - 1, nlen = *nlength_seismogramf;
   if (j < 0 || j >= nlen) stop(R, "seismo_current out of range");
@@ -1596,6 +1665,82 @@ void transfer_kernels_el_to_host_(long *Mesh_pointer, realw *h_rho_kl, realw *h_
   std::memcpy(h_kappa_kl, m->kappa_sum.data(), sizeof(realw) * nl);
 }
 
+// ---- CPML layer of a fluid-only mesh ----
+
+// prepare_pml_device (src/gpu/prepare_mesh_constants_cuda.cu:843): the layer's
+// profiles as the reference's GPU kernel forms them
+// (Kernel_2_acoustic_impl.cu:497-505): in CPML_X_ONLY and CPML_Z_ONLY elements
+// alpha = ALPHA_MAX_PML (1 - abs_normalized) and beta = alpha + 2 d0_max
+// abs_normalized^2, in CPML_XZ elements alpha and beta from the stores; the
+// library's CPML (the reference's CPU convolution scheme,
+// pml_compute_memory_variables.f90) takes them as K = 1, d = beta - alpha
+void prepare_pml_device_(long *Mesh_pointer, int *NSPEC_PML, int *NSPEC_PML_X, int *NSPEC_PML_Z, int *NSPEC_PML_XZ,
+                         int *h_spec_to_pml, realw *h_abs_normalized, realw *ALPHA_MAX_PML, realw *d0_max,
+                         realw *deltat, realw *h_alphax_store, realw *h_alphaz_store, realw *h_betax_store,
+                         realw *h_betaz_store, int *PML_nglob_abs_acoustic_f, int *h_PML_abs_points_acoustic) {
+  const char *R = "prepare_pml_device";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (!m->pml) stop(R, "PML_BOUNDARY_CONDITIONS is off in prepare_constants_device");
+  if (m->C) stop(R, "called after the time loop started");
+  const int nx = *NSPEC_PML_X, nz = *NSPEC_PML_Z, nxz = *NSPEC_PML_XZ, np = *NSPEC_PML;
+  if (nx < 0 || nz < 0 || nxz < 0 || nx + nz + nxz != np)
+    stop(R, "NSPEC_PML_X + NSPEC_PML_Z + NSPEC_PML_XZ must equal NSPEC_PML");
+  const size_t nl = static_cast<size_t>(m->nspec) * NGLL2;
+  m->pml_region.assign(m->nspec, 0);
+  m->pml_K_x.assign(nl, 1.0);
+  m->pml_K_z.assign(nl, 1.0);
+  m->pml_d_x.assign(nl, 0.0);
+  m->pml_d_z.assign(nl, 0.0);
+  m->pml_alpha_x.assign(nl, 0.0);
+  m->pml_alpha_z.assign(nl, 0.0);
+  const float amax = *ALPHA_MAX_PML, d0 = *d0_max;
+  for (int e = 0; e < m->nspec; ++e) {
+    const int p = h_spec_to_pml[e];
+    if (p == 0) continue;
+    if (p < 0 || p > np) stop(R, "spec_to_PML out of range");
+    const size_t b = static_cast<size_t>(e) * NGLL2;
+    if (p <= nx + nz) {
+      // one direction: x in CPML_X_ONLY elements, z in CPML_Z_ONLY ones
+      const bool xdir = p <= nx;
+      m->pml_region[e] = xdir ? 1 : 2;
+      std::vector<double> &d = xdir ? m->pml_d_x : m->pml_d_z, &al = xdir ? m->pml_alpha_x : m->pml_alpha_z;
+      for (int q = 0; q < NGLL2; ++q) {
+        const float an = h_abs_normalized[static_cast<size_t>(p - 1) * NGLL2 + q];
+        const float alpha = amax * (1.f - an);
+        const float beta = alpha + 2.f * d0 * an * an;
+        al[b + q] = alpha;
+        d[b + q] = static_cast<double>(beta) - static_cast<double>(alpha);
+      }
+    } else {
+      m->pml_region[e] = 3;
+      const size_t k = static_cast<size_t>(p - nx - nz - 1) * NGLL2;
+      for (int q = 0; q < NGLL2; ++q) {
+        m->pml_alpha_x[b + q] = h_alphax_store[k + q];
+        m->pml_alpha_z[b + q] = h_alphaz_store[k + q];
+        m->pml_d_x[b + q] = static_cast<double>(h_betax_store[k + q]) - static_cast<double>(h_alphax_store[k + q]);
+        m->pml_d_z[b + q] = static_cast<double>(h_betaz_store[k + q]) - static_cast<double>(h_alphaz_store[k + q]);
+      }
+    }
+  }
+  m->pml_edge.clear();
+  for (int k = 0; k < *PML_nglob_abs_acoustic_f; ++k) {
+    const int g = h_PML_abs_points_acoustic[k] - 1;
+    if (g < 0 || g >= m->nglob) stop(R, "PML_abs_points_acoustic out of range");
+    m->pml_edge.push_back(g);
+  }
+  m->pml_dt = *deltat;
+  m->have_pml = true;
+}
+
+// pml_boundary_acoustic_cuda (src/gpu/pml_compute_cuda.cu:47): the
+// zeroing of the layer's outer edge is part of the fused step
+void pml_boundary_acoustic_cuda_(long *Mesh_pointer, int *, int *compute_wavefield_2) {
+  const char *R = "pml_boundary_acoustic_cuda";
+  FortranMesh *m = mesh_of(R, Mesh_pointer);
+  if (!m->pml) stop(R, "the run has no CPML layer");
+  fluid_phase_call(R, m, compute_wavefield_2);
+}
+
 // ---- the kernel run of a mesh with fluid elements ----
 
 // prepare_fields_acoustic_adj_dev (src/gpu/prepare_mesh_constants_cuda.cu:442)
@@ -1687,8 +1832,6 @@ void check_max_norm_b_accel_(int*, realw*, int*) { unsupported("check_max_norm_b
 void check_error_vectors_(int*, realw*, realw*) { unsupported("check_error_vectors", DEBUG); }
 void compute_add_moving_sources_ac_cuda_(long*, int*, int*, int*, int*, int*) { unsupported("compute_add_moving_sources_ac_cuda", OTHER); }
 void compute_kernels_hess_cuda_(long*, int*, int*) { unsupported("compute_kernels_hess_cuda", OTHER); }
-void pml_boundary_acoustic_cuda_(long*, int*, int*) { unsupported("pml_boundary_acoustic_cuda", PML); }
-void prepare_pml_device_(long*, int*, int*, int*, int*, int*, realw*, realw*, realw*, realw*, realw*, realw*, realw*, realw*, int*, int*) { unsupported("prepare_pml_device", PML); }
 void prepare_moving_sources_cuda_(long*, int*, int*, realw*, int*, int*, realw*) { unsupported("prepare_moving_sources_cuda", OTHER); }
 void prepare_arrays_gpu_(long*, realw*, realw*, realw*, realw*, realw*, realw*, int*, int*, realw*) { unsupported("prepare_arrays_gpu", OTHER); }
 void compute_smooth_(long*, realw*, realw*, realw*, realw*, const int*) { unsupported("compute_smooth", OTHER); }

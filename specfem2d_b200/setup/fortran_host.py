@@ -115,6 +115,8 @@ def gpu_arrays(db, nlength_seismogram: int | None = None):
     out["abs"] = abs_boundary_arrays(db)
     if db.acoustic is not None:
         out.update(fluid_arrays(db))
+        # write_seismograms.F90 passes it to compute_seismograms_cuda
+        out["use_trick"] = int(bool(db.acoustic.get("use_trick", False)))
     if db.aniso is not None:
         out["ispec_is_anisotropic"] = _fortran(db.aniso["ispec"], np.int32)
         for k in ("c11", "c13", "c15", "c33", "c35", "c55"):
@@ -123,7 +125,51 @@ def gpu_arrays(db, nlength_seismogram: int | None = None):
         # A/B_newmark_nu1 (bulk) and _nu2 (shear), (N_SLS, NGLLX, NGLLZ, nspec)
         for k in ("a1", "b1", "a2", "b2"):
             out["att_" + k] = _fortran(db.atten[k], f32)
+    if getattr(db, "pml", None) is not None:
+        out["pml"] = pml_arrays(db)
     return out
+
+
+def pml_arrays(db):
+    """prepare_PML_device's arrays (prepare_gpu.f90:213-227, 389-470):
+    spec_to_PML_GPU numbering the CPML_X_ONLY elements first, then CPML_Z_ONLY,
+    then CPML_XZ (each in ascending element order, 0 outside the layer),
+    abs_normalized (NGLLX, NGLLZ, NSPEC_PML) of the X and Z elements,
+    ALPHA_MAX_PML and d0_max (the largest acoustic d0, pml_init.F90:884-887),
+    alpha and beta = alpha + d of the XZ elements (NGLLX, NGLLZ, NSPEC_PML_XZ)
+    and PML_abs_points_acoustic (the fluid points of the layer's outer edge)."""
+    from . import pml as pml_setup
+
+    pm = db.pml
+    region = np.asarray(pm["region"])
+    spec = np.zeros(db.nspec, np.int32)
+    n = 0
+    counts = []
+    for code in (pml_setup.CPML_X_ONLY, pml_setup.CPML_Z_ONLY, pml_setup.CPML_XZ):
+        els = np.flatnonzero(region == code)
+        spec[els] = n + 1 + np.arange(els.size)
+        n += els.size
+        counts.append(int(els.size))
+    nx, nz, nxz = counts
+    absn = np.zeros((max(n, 1), NGLL, NGLL), f32)
+    for e in np.flatnonzero(spec > 0):
+        p = spec[e] - 1
+        if region[e] == pml_setup.CPML_X_ONLY:
+            absn[p] = pm["abs_x"][e]
+        elif region[e] == pml_setup.CPML_Z_ONLY:
+            absn[p] = pm["abs_z"][e]
+    xz = np.flatnonzero(region == pml_setup.CPML_XZ)
+    st = {k: np.zeros((max(nxz, 1), NGLL, NGLL), f32) for k in ("alphax", "alphaz", "betax", "betaz")}
+    for k, e in enumerate(xz):
+        st["alphax"][k] = pm["alpha_x"][e]
+        st["alphaz"][k] = pm["alpha_z"][e]
+        st["betax"][k] = pm["alpha_x"][e] + pm["d_x"][e]
+        st["betaz"][k] = pm["alpha_z"][e] + pm["d_z"][e]
+    return dict(nspec_pml=n, nspec_pml_x=nx, nspec_pml_z=nz, nspec_pml_xz=nxz, spec_to_pml=spec,
+                abs_normalized=_fortran(absn, f32), alpha_max=f32(pm["alpha_max"]), d0_max=f32(pm["d0_max_acoustic"]),
+                alphax=_fortran(st["alphax"], f32), alphaz=_fortran(st["alphaz"], f32),
+                betax=_fortran(st["betax"], f32), betaz=_fortran(st["betaz"], f32),
+                abs_points_acoustic=_fortran(np.asarray(pm["bnd_ac"]) + 1, np.int32))
 
 
 def fluid_arrays(db):

@@ -157,7 +157,10 @@ def pml_coefficients(ibool, coord, is_pml, region, rho_vpstore, rhostore, is_aco
                      k_min: float = 1.0, k_max: float = 1.0, damping_factor_acoustic: float = 0.5,
                      damping_factor_elastic: float = 1.0):
     """K_x, K_z, d_x, d_z, alpha_x, alpha_z per element GLL point (nspec, 5, 5) float64;
-    points outside the PML hold K = 1, d = alpha = 0."""
+    points outside the PML hold K = 1, d = alpha = 0.  Also the normalised
+    abscissae of the x and z profiles (abs_x, abs_z; 0 where none applies),
+    ALPHA_MAX_PML (alpha_max) and the largest acoustic d0 over the four sides
+    (d0_max_acoustic), which the GPU path of pml_init.F90:884-914 keeps."""
     nspec = ibool.shape[0]
     x, z = coord[:, 0], coord[:, 1]
     xmin, xmax, zmin, zmax = x.min(), x.max(), z.min(), z.max()
@@ -199,6 +202,7 @@ def pml_coefficients(ibool, coord, is_pml, region, rho_vpstore, rhostore, is_aco
     Kx = np.ones((nspec, NGLL, NGLL))
     Kz, dx, dz = np.ones_like(Kx), np.zeros_like(Kx), np.zeros_like(Kx)
     ax, az = np.zeros_like(Kx), np.zeros_like(Kx)
+    abs_x, abs_z = np.zeros_like(Kx), np.zeros_like(Kx)
     for e in np.flatnonzero(is_pml):
         r = region[e]
         fac = damping_factor_acoustic if is_acoustic[e] else damping_factor_elastic
@@ -215,6 +219,8 @@ def pml_coefficients(ibool, coord, is_pml, region, rho_vpstore, rhostore, is_aco
                         if cond:
                             d_z, K_z, alpha_z = _side_profile(absc, thick[side], d0s[side][dom], fac,
                                                               alpha_max, k_min, k_max)
+                            if absc >= 0.0:
+                                abs_z[e, j, i] = absc / thick[side]
                             if r == CPML_Z_ONLY:
                                 d_x, K_x, alpha_x = 0.0, 1.0, 0.0
                 if r in (CPML_X_ONLY, CPML_XZ):
@@ -223,6 +229,8 @@ def pml_coefficients(ibool, coord, is_pml, region, rho_vpstore, rhostore, is_aco
                         if cond:
                             d_x, K_x, alpha_x = _side_profile(absc, thick[side], d0s[side][dom], fac,
                                                               alpha_max, k_min, k_max)
+                            if absc >= 0.0:
+                                abs_x[e, j, i] = absc / thick[side]
                             if r == CPML_X_ONLY:
                                 d_z, K_z, alpha_z = 0.0, 1.0, 0.0
                 Kx[e, j, i], Kz[e, j, i], dx[e, j, i], dz[e, j, i] = K_x, K_z, d_x, d_z
@@ -256,4 +264,5 @@ def pml_coefficients(ibool, coord, is_pml, region, rho_vpstore, rhostore, is_aco
                 dx[e, j, i] = (beta_x - alpha_x) * K_x
                 dz[e, j, i] = (beta_z - alpha_z) * K_z
                 ax[e, j, i], az[e, j, i] = alpha_x, alpha_z
-    return dict(K_x=Kx, K_z=Kz, d_x=dx, d_z=dz, alpha_x=ax, alpha_z=az)
+    return dict(K_x=Kx, K_z=Kz, d_x=dx, d_z=dz, alpha_x=ax, alpha_z=az, abs_x=abs_x, abs_z=abs_z,
+                alpha_max=alpha_max, d0_max_acoustic=max(v[0] for v in d0s.values()))

@@ -6,6 +6,8 @@ with arguments passed by reference as gfortran passes them:
   prepare_constants_device, prepare_fields_acoustic_device (fluid elements),
   prepare_fields_elastic_device (solid elements), prepare_Stacey_device,
   transfer_fields_el_to_device / transfer_fields_ac_to_device;
+* with CPML layers (fluid-only meshes) prepare_PML_device, and
+  pml_boundary_acoustic_cuda after each fluid forces call;
 * each time step it = 1..NSTEP (iterate_time.F90:146-260):
   update_displacement_ac_cuda and update_displacement_cuda
   (update_displacement_Newmark.F90:150-240, 500-549); with fluid elements
@@ -104,7 +106,7 @@ def _drive(db, nstep, check_every, nlength_seismogram, adj_src, save_forward):
         r.a(A["kappastore"]), r.a(A["mustore"]), r.a(A["ibool"]),
         r.i(0), r.i(0), r.a(dummy_i), r.a(dummy_i),
         r.a(A["hprime_xx"]), r.a(A["hprimewgll_xx"]), r.a(A["wxgll"]),
-        r.i(1 if A["stacey"] else 0), r.i(0), r.a(np.ones(A["nspec"], np.int32)),
+        r.i(1 if A["stacey"] else 0), r.i(1 if "pml" in A else 0), r.a(np.ones(A["nspec"], np.int32)),
         r.i(A["nsrc"]), r.a(A["sourcearrays"]), r.a(A["source_time_function"]),
         r.i(A["nstep"]), r.a(A["ispec_selected_source"]), r.a(A["ispec_selected_rec_loc"]),
         r.i(A["nrec"]), r.a(A["cosrot"]), r.a(A["sinrot"]),
@@ -135,6 +137,14 @@ def _drive(db, nstep, check_every, nlength_seismogram, adj_src, save_forward):
         r.a(c["c33"]), r.a(c["c35"]), r.a(c["c55"]),
         r.i(0), r.a(dummy_i), r.i(1 if atten else 0),
         r.a(att["a2"]), r.a(att["b2"]), r.a(att["a1"]), r.a(att["b1"]))
+    if "pml" in A:
+        # prepare_PML_device (prepare_gpu.f90:213-227)
+        P = A["pml"]
+        lib.prepare_pml_device_(
+            M, r.i(P["nspec_pml"]), r.i(P["nspec_pml_x"]), r.i(P["nspec_pml_z"]), r.i(P["nspec_pml_xz"]),
+            r.a(P["spec_to_pml"]), r.a(P["abs_normalized"]), r.f(P["alpha_max"]), r.f(P["d0_max"]),
+            r.f(A["deltat"]), r.a(P["alphax"]), r.a(P["alphaz"]), r.a(P["betax"]), r.a(P["betaz"]),
+            r.i(len(P["abs_points_acoustic"])), r.a(P["abs_points_acoustic"]))
     ng2 = 2 * A["nglob"]
     if kernel and elastic:
         lib.prepare_fields_elastic_adj_dev_(M, r.i(ng2), r.i(0), r.i(int(atten)), r.i(0))
@@ -180,6 +190,7 @@ def _drive(db, nstep, check_every, nlength_seismogram, adj_src, save_forward):
     p_ac = [b.ctypes.data_as(ctypes.c_void_p) for b in b_ac]
     nrec_c, nstep_c, itmp_c = ctypes.c_int(A["nrec"]), ctypes.c_int(A["nstep"]), ctypes.c_int(0)
     three = ctypes.c_int(3)
+    trick_c = ctypes.c_int(A.get("use_trick", 0))
 
     def saved_slices_are_zero(slices):
         # SAVE_FORWARD: the host stores the slices it got back as b_absorb_*(..., it)
@@ -193,6 +204,8 @@ def _drive(db, nstep, check_every, nlength_seismogram, adj_src, save_forward):
         for iphase in (one, two):
             lib.compute_forces_acoustic_cuda_(M, ctypes.byref(iphase), ctypes.byref(zero), ctypes.byref(zero),
                                               ctypes.byref(zero), ctypes.byref(c1), ctypes.byref(c2))
+            if "pml" in A:
+                lib.pml_boundary_acoustic_cuda_(M, ctypes.byref(c1), ctypes.byref(c2))
             if iphase is not one:
                 continue
             if A["stacey"]:
@@ -282,7 +295,7 @@ def _drive(db, nstep, check_every, nlength_seismogram, adj_src, save_forward):
         lib.compute_seismograms_cuda_(M, ctypes.byref(one), sisux.ctypes.data_as(ctypes.c_void_p),
                                       sisuz.ctypes.data_as(ctypes.c_void_p), ctypes.byref(cur_c),
                                       ctypes.byref(nlen_c), ctypes.byref(one), ctypes.byref(zero),
-                                      ctypes.byref(zero), ctypes.byref(atten_c), ctypes.byref(it_c),
+                                      ctypes.byref(trick_c), ctypes.byref(atten_c), ctypes.byref(it_c),
                                       ctypes.byref(end_c))
         if seismo_current == nlen or it == nstep:
             # write_seismograms saves the buffer and starts it again

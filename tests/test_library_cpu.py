@@ -3,6 +3,7 @@ function include/sf2d_b200.h declares, and its tiler keeps its invariants."""
 import os
 import re
 
+import numpy as np
 import pytest
 
 from specfem2d_b200 import runtime
@@ -73,7 +74,8 @@ def test_library_exports_the_reference_fortran_interface():
 
 
 @pytest.mark.parametrize("call,needle", [
-    ("pml_boundary_acoustic_cuda_", "CPML layers"),
+    ("pml_boundary_acoustic_cuda_", "Mesh_pointer was not prepared"),
+    ("compute_kernels_hess_cuda_", "not provided by libsf2d_b200"),
     ("compute_forces_acoustic_cuda_", "Mesh_pointer was not prepared"),
     ("kernel_3_b_cuda_", "sf2d_fwi_create"),
     ("transfer_boun_accel_from_device_", "MPI"),
@@ -126,3 +128,39 @@ def test_fortran_host_absorbing_faces_give_the_solver_stacey_points():
         assert np.array_equal(np.array(got, np.float32), want)
     # hprime_xx(i2, i1) = l'_i1(xi_i2) in Fortran order
     assert A["hprime_xx"].ravel()[1 * 5 + 3] == db.gll.hprime[3, 1]
+
+
+def test_fortran_host_pml_arrays_restate_the_layer_profiles():
+    """prepare_PML_device's arrays for the fluid CPML example: elements numbered
+    X, then Z, then XZ; the profiles the GPU path forms from them (alpha =
+    ALPHA_MAX_PML (1 - abs), d = 2 d0_max abs^2 in X and Z elements, the stores
+    in XZ ones, all in FP32) equal the set-up's K = 1 profiles to FP32 rounding."""
+    from specfem2d_b200.setup.fortran_host import pml_arrays
+
+    cfg, _ = load_golden("pressure_source_acoustic")
+    db = database_from_config(cfg)
+    P = pml_arrays(db)
+    pm = db.pml
+    region = np.asarray(pm["region"])
+    assert (P["nspec_pml_x"], P["nspec_pml_z"], P["nspec_pml_xz"]) == (228, 228, 36)
+    spec = P["spec_to_pml"]
+    assert np.array_equal(np.flatnonzero(spec), np.flatnonzero(region))
+    for code, lo, hi in ((1, 1, 228), (2, 229, 456), (3, 457, 492)):
+        els = np.flatnonzero(region == code)
+        assert np.array_equal(spec[els], np.arange(lo, hi + 1))
+    assert np.all(pm["K_x"] == 1.0) and np.all(pm["K_z"] == 1.0)
+    f = np.float32
+    for e in np.flatnonzero(region):
+        p = spec[e] - 1
+        if region[e] < 3:
+            a = P["abs_normalized"][p]
+            alpha = P["alpha_max"] * (f(1) - a)
+            d = (alpha + f(2) * P["d0_max"] * a * a).astype(np.float64) - alpha.astype(np.float64)
+            kd, ka = ("d_x", "alpha_x") if region[e] == 1 else ("d_z", "alpha_z")
+            assert np.allclose(d, pm[kd][e], rtol=1e-6, atol=1e-6 * pm[kd].max()), e
+            assert np.allclose(alpha, pm[ka][e], rtol=1e-6, atol=1e-6 * pm[ka].max()), e
+        else:
+            k = p - 456
+            d = P["betax"][k].astype(np.float64) - P["alphax"][k].astype(np.float64)
+            assert np.allclose(d, pm["d_x"][e], rtol=1e-6, atol=1e-6 * pm["d_x"].max()), e
+    assert np.array_equal(P["abs_points_acoustic"], np.asarray(pm["bnd_ac"]) + 1)
