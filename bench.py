@@ -92,6 +92,8 @@ TILE_TRAFFIC = {
     ("c2_coupled", 32, 256, 64, 16, 128): 233.0e6 + 43.45e6 + 71.07e6 + 0.40e6 + 1.25e6,
     # 376.16 MB per launch on the quarter-scale model (80,000 elements), x16 elements
     ("c3_viscoelastic", 32, 256, 64, 16, 128): 376.16e6 * 16,
+    # 64-element tiles (the autotuner's choice): 371.10 MB per launch at quarter scale, x16
+    ("c3_viscoelastic", 64, 256, 64, 16, 128): 371.10e6 * 16,
 }
 TRAFFIC_SOURCE = {
     ("c2_coupled", 32, 256, 64, 16, 128): "ncu dram__bytes_read.sum + dram__bytes_write.sum of one step's solid "
@@ -99,6 +101,9 @@ TRAFFIC_SOURCE = {
     ("c3_viscoelastic", 32, 256, 64, 16, 128): "ncu dram__bytes_read.sum + dram__bytes_write.sum of one tile "
                                                "launch on the quarter-scale model (--scale 4), scaled by the "
                                                "element count (x16)",
+    ("c3_viscoelastic", 64, 256, 64, 16, 128): "ncu dram__bytes_read.sum + dram__bytes_write.sum of one tile "
+                                               "launch (64-element tiles) on the quarter-scale model (--scale 4), "
+                                               "mean of two launches, scaled by the element count (x16)",
 }
 
 WORKLOAD_DESC = {
