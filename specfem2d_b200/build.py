@@ -8,6 +8,7 @@ CUDA runtime.
 from __future__ import annotations
 
 import os
+import re
 import subprocess
 import sys
 
@@ -24,6 +25,15 @@ OBJDIR = os.path.join(PKG, "_build")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
          "-I", os.path.join(ROOT, "include"), "-I", CSRC]
+
+
+def export_map() -> str:
+    """Linker version script: the library exports its C ABI (sf2d_*) and the
+    reference's Fortran entry points (include/sf2d_fortran.h) and nothing else,
+    so that none of its C++ internals can bind to a host's symbols."""
+    with open(os.path.join(ROOT, "include", "sf2d_fortran.h")) as f:
+        names = sorted(set(re.findall(r"^void (\w+_)\(", f.read(), re.M)))
+    return "{\n  global:\n    sf2d_*;\n" + "".join(f"    {n};\n" for n in names) + "  local:\n    *;\n};\n"
 
 
 def needs_build() -> bool:
@@ -56,8 +66,11 @@ def build(force: bool = False, verbose: bool = False) -> str:
         codes = list(ex.map(compile_one, cmds))
     if any(codes):
         raise subprocess.CalledProcessError(max(codes), "nvcc")
+    mapfile = os.path.join(OBJDIR, "libsf2d_b200.map")
+    with open(mapfile, "w") as f:
+        f.write(export_map())
     link = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-cudart", "static", *objs,
-            "-o", LIB + ".tmp"]
+            "-Xlinker", "--version-script=" + mapfile, "-o", LIB + ".tmp"]
     if verbose:
         print(" ".join(link), flush=True)
     subprocess.run(link, check=True)

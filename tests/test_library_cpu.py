@@ -73,6 +73,21 @@ def test_library_exports_the_reference_fortran_interface():
     assert not missing, missing
 
 
+def test_library_exports_only_its_interfaces():
+    """The shared object exports the C ABI (sf2d_*) and the Fortran entry points
+    and nothing else (a linker version script): no C++ internal of the library
+    can bind to a host program's symbols."""
+    import subprocess
+
+    out = subprocess.run(["nm", "-D", "--defined-only", runtime.LIB], capture_output=True, text=True,
+                         check=True).stdout.split("\n")
+    names = {ln.split()[-1] for ln in out if ln.strip()}
+    allowed = set(fortran_symbols())
+    extra = sorted(n for n in names if not n.startswith("sf2d_") and n not in allowed)
+    assert not extra, extra[:10]
+    assert allowed <= names
+
+
 @pytest.mark.parametrize("call,needle", [
     ("pml_boundary_acoustic_cuda_", "Mesh_pointer was not prepared"),
     ("compute_kernels_hess_cuda_", "not provided by libsf2d_b200"),
