@@ -259,7 +259,9 @@ def run_reference(args, rank):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic", "config": {"workload": args.workload, "description": WORKLOAD_DESC[args.workload],
                                         "nspec": db.nspec, "nglob": db.nglob},
+        "s_per_element_step": dt / n / db.nspec,
         "cpu_baseline": {"value": value, "unit": "point-updates/s", "cores": threads, "kind": "port",
+                         "s_per_element_step": dt / n / db.nspec, "cpu_model": cpu_model(),
                          "sample": f"{n} Newmark steps of the full {db.nspec}-element mesh "
                                    "(C++ restatement of the reference CPU solver, FP32)"},
         "e2e": {"value": value, "unit": "point-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -644,6 +646,10 @@ def measure_forward(db, args, workload, K, W, world, dist, nstep_full=0):
                                 "fields and traces through pinned host buffers",
                    "parallelism": f"replicas x{world}"},
         "hbm_gbs_step": step_bytes / (ms / K * 1e-3) / 1e9,
+        # the reference's logs quote time per spectral element and step; local
+        # point-updates count every element GLL point (25 nspec per step)
+        "local_point_updates_per_s": 25 * db.nspec * K * world / (ms * 1e-3),
+        "s_per_element_step": ms * 1e-3 / K / db.nspec,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": TILE_TRAFFIC.get(traffic_key),
                      "traffic_source": TRAFFIC_SOURCE.get(traffic_key),
@@ -655,6 +661,18 @@ def measure_forward(db, args, workload, K, W, world, dist, nstep_full=0):
         "gpu_launches": launches,
         "clocks": clk,
     }
+
+
+def cpu_model() -> str:
+    """The host CPU's model name (/proc/cpuinfo), recorded beside the CPU baseline."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 def main():
@@ -723,12 +741,14 @@ def main():
     line = {"metric": "GLL point-updates/s", "value": res["value"], "unit": "point-updates/s",
             "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": res["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", **{k: res[k] for k in ("config", "hbm_gbs_step", "roofline", "e2e",
+            "data": "synthetic", **{k: res[k] for k in ("config", "hbm_gbs_step", "local_point_updates_per_s",
+                                                          "s_per_element_step", "roofline", "e2e",
                                                           "e2e_full_run", "gpu_launches", "clocks")}}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         n, dt, threads = time_oracle(db, max_steps=K, target_s=args.ref_seconds)
         line["cpu_baseline"] = {"value": db.nglob * n / dt, "unit": "point-updates/s", "cores": threads,
-                                "kind": "port",
+                                "kind": "port", "s_per_element_step": dt / n / db.nspec,
+                                "cpu_model": cpu_model(),
                                 "sample": f"{n} time steps of the full mesh, C++ restatement of the "
                                           "reference CPU solver (FP32), all host threads"}
     del db
