@@ -260,6 +260,48 @@ int sf2d_fwi_kernel_sums(sf2d_fwi *f, float *rho_kl, float *kappa_kl, float *mu_
 int sf2d_fwi_adjoint_fields(sf2d_fwi *f, float *displ, float *veloc, float *accel);
 int sf2d_fwi_destroy(sf2d_fwi *f);
 
+/* ---- batches of shots and models (one launch per step for all) ----
+ * The GPU counterpart of NUMBER_OF_SIMULTANEOUS_RUNS (src/shared/parallel.F90:
+ * 40-50, 1714), which runs independent simulations as separate MPI groups.
+ * A batch packs its members into one disconnected mesh: a member is a shot on
+ * one of the models, with the model's arrays and the shot's sources; its
+ * elements, points, absorbing points, sources and receivers are appended with
+ * offsets, and its element centres are moved 1e8 m apart along x so that no
+ * tile mixes members.  Models must share nstep, the time step, the time scheme,
+ * the seismogram type and rotation, and their physics (anisotropy and
+ * attenuation present in all or none); CPML layers are not packed.  Receivers,
+ * seismograms and adjoint sources are in member order (each member's
+ * receivers in its model's order). */
+typedef struct {
+  int model;                 /* index into the models array */
+  int nsrc;                  /* the shot's sources, in place of the model's */
+  const int *src_ispec;      /* nsrc elements of the model */
+  const float *sourcearrays; /* nsrc*25*2 [isrc][j][i][comp] */
+  const float *stf;          /* nsrc*nstep*nstage */
+} sf2d_shot;
+typedef struct sf2d_batch sf2d_batch;
+/* nshots = 0: one member per model with its own sources.  checkpoint_every >
+ * 0 makes a gradient batch (Newmark only): rhostore/kappastore then hold one
+ * nspec*25 array per model for the kernel scaling, as in sf2d_fwi_create;
+ * checkpoint_every = 0 makes a forward batch (rhostore/kappastore unused), whose
+ * members are masked one by one if their field blows up (sf2d_set_members). */
+int sf2d_batch_create(const sf2d_elastic_desc *models, int nmodels, const sf2d_shot *shots, int nshots,
+                      const float *const *rhostore, const float *const *kappastore, int checkpoint_every,
+                      sf2d_batch **out);
+/* [members, total elements, total points, total receivers] */
+int sf2d_batch_info(sf2d_batch *b, long long *info4);
+/* Forward run of every member from rest over nstep steps; seismograms (may be
+ * NULL): nrec_total*nstep*2 doubles.  A gradient batch keeps its checkpoints. */
+int sf2d_batch_run_forward(sf2d_batch *b, double *seismograms);
+/* Gradient batch: adjoint sweep with adj_src (nrec_total*nstep*2, time order);
+ * the kernels rho_kl, kappa_kl, mu_kl of each model, summed over its shots
+ * (each array: the models' nspec*25 one after the other, scaled as
+ * sf2d_fwi_backward scales them). */
+int sf2d_batch_run_adjoint(sf2d_batch *b, const float *adj_src, float *rho_kl, float *kappa_kl, float *mu_kl);
+/* Forward batch: per member 0 running, 1 masked (blew up). */
+int sf2d_batch_member_status(sf2d_batch *b, int *status);
+int sf2d_batch_destroy(sf2d_batch *b);
+
 /* ---- kernel smoothing (post-gradient step) ----
  * Gaussian smoothing of per-element-point fields, as
  * src/tomography/postprocess_sensitivity_kernels/smooth_sem.F90:63-467 does to

@@ -138,3 +138,106 @@ def shots_on_model(db, positions, angle_deg: float = 0.0):
         d.src_gamma = np.array([gamma])
         out.append(d)
     return out
+
+
+class NativeBatch:
+    """A batch packed by the library itself (sf2d_batch_*, include/sf2d_b200.h):
+    the models' descriptions and, optionally, shots on them (each a Database
+    of one of the models that differs only in its sources, as shots_on_model
+    makes them).  checkpoint_every > 0 makes a gradient batch whose kernels
+    come back per model, summed over its shots."""
+
+    def __init__(self, models, shots=None, shot_models=None, checkpoint_every: int = 0, tile_elems: int = 32,
+                 threads_per_block: int = 256):
+        import ctypes
+
+        from .runtime import ElasticDesc, _check, build_desc, load_library
+
+        lib = load_library()
+        vp, ip = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)
+        fp = ctypes.POINTER(ctypes.c_float)
+
+        class Shot(ctypes.Structure):
+            _fields_ = [("model", ctypes.c_int), ("nsrc", ctypes.c_int), ("src_ispec", ip),
+                        ("sourcearrays", fp), ("stf", fp)]
+
+        lib.sf2d_batch_create.argtypes = [ctypes.POINTER(ElasticDesc), ctypes.c_int, ctypes.POINTER(Shot),
+                                          ctypes.c_int, ctypes.POINTER(fp), ctypes.POINTER(fp), ctypes.c_int,
+                                          ctypes.POINTER(vp)]
+        for name, args in (("sf2d_batch_info", [vp, ctypes.POINTER(ctypes.c_longlong)]),
+                           ("sf2d_batch_run_forward", [vp, ctypes.POINTER(ctypes.c_double)]),
+                           ("sf2d_batch_run_adjoint", [vp, fp, fp, fp, fp]),
+                           ("sf2d_batch_member_status", [vp, ip]), ("sf2d_batch_destroy", [vp])):
+            getattr(lib, name).argtypes = args
+        self._lib, self._keep = lib, []
+        descs = (ElasticDesc * len(models))()
+        for k, db in enumerate(models):
+            d, keep = build_desc(db, tile_elems, 1, threads_per_block)
+            descs[k] = d
+            self._keep.append(keep)
+        shots = list(shots or [])
+        shot_arr = (Shot * max(len(shots), 1))()
+        for s, db in enumerate(shots):
+            ispec = np.ascontiguousarray(db.source_ispec, dtype=np.int32)
+            arr = np.ascontiguousarray(db.sourcearrays, dtype=np.float32)
+            stf = np.ascontiguousarray(db.stf, dtype=np.float32)
+            self._keep.append((ispec, arr, stf))
+            shot_arr[s] = Shot(int(shot_models[s]) if shot_models is not None else 0, len(ispec),
+                               ispec.ctypes.data_as(ip), arr.ctypes.data_as(fp), stf.ctypes.data_as(fp))
+        rho = (fp * len(models))()
+        kap = (fp * len(models))()
+        if checkpoint_every:
+            for k, db in enumerate(models):
+                r = np.ascontiguousarray(db.rhostore, dtype=np.float32)
+                q = np.ascontiguousarray(db.kappastore, dtype=np.float32)
+                self._keep.append((r, q))
+                rho[k], kap[k] = r.ctypes.data_as(fp), q.ctypes.data_as(fp)
+        h = vp()
+        _check(lib.sf2d_batch_create(descs, len(models), shot_arr, len(shots), rho, kap, int(checkpoint_every),
+                                     ctypes.byref(h)))
+        self._h = h
+        info = (ctypes.c_longlong * 4)()
+        _check(lib.sf2d_batch_info(h, info))
+        self.nmembers, self.nspec, self.nglob, self.nrec = (int(x) for x in info)
+        self.nstep = int(models[0].nstep)
+        self.model_nspec = [int(db.nspec) for db in models]
+
+    def forward(self) -> np.ndarray:
+        """Seismograms of all members (nrec_total, nstep, 2), members in order."""
+        from .runtime import _check, _d
+
+        seis = np.zeros((self.nrec, self.nstep, 2), dtype=np.float64)
+        _check(self._lib.sf2d_batch_run_forward(self._h, seis.ctypes.data_as(_d)))
+        return seis
+
+    def adjoint(self, adj_src):
+        """Kernels (rho, kappa, mu) of each model, (nspec, 5, 5) each, summed over its shots."""
+        from .runtime import _check, _f
+
+        adj = np.ascontiguousarray(np.asarray(adj_src, dtype=np.float32).reshape(self.nrec, self.nstep, 2))
+        n = sum(self.model_nspec)
+        out = [np.zeros((n, 5, 5), dtype=np.float32) for _ in range(3)]
+        _check(self._lib.sf2d_batch_run_adjoint(self._h, adj.ctypes.data_as(_f),
+                                                *[o.ctypes.data_as(_f) for o in out]))
+        off = np.cumsum([0] + self.model_nspec)
+        return [tuple(o[off[k]:off[k + 1]] for o in out) for k in range(len(self.model_nspec))]
+
+    def member_status(self) -> np.ndarray:
+        import ctypes
+
+        from .runtime import _check
+
+        st = np.zeros(self.nmembers, dtype=np.int32)
+        _check(self._lib.sf2d_batch_member_status(self._h, st.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+        return st
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.sf2d_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

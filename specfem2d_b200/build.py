@@ -18,7 +18,7 @@ CSRC = os.path.join(PKG, "csrc")
 LIBDIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(LIBDIR, "libsf2d_b200.so")
 SOURCES = ["sf2d_elastic.cu", "sf2d_fwi.cu", "sf2d_noalloc.cu", "sf2d_coupled.cu", "sf2d_tiler.cpp",
-           "sf2d_fortran.cpp", "sf2d_smooth.cu"]
+           "sf2d_fortran.cpp", "sf2d_smooth.cu", "sf2d_batch.cu"]
 HEADERS = ["sf2d_tiler.h", "sf2d_kernels.cuh", "sf2d_runtime.h", "sf2d_acoustic.cuh", "sf2d_pml.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 OBJDIR = os.path.join(PKG, "_build")

@@ -159,3 +159,69 @@ def test_summed_shot_gradient_matches_the_oracle_sum():
         s64 = sum(r[k].astype(np.float64) for r in ref64)
         s32 = sum(r[k].astype(np.float64) for r in ref32)
         assert rel_l2(got, s64) < 1.5 * rel_l2(s32, s64)
+
+
+@pytest.mark.gpu
+def test_native_batch_forward_matches_the_packed_database():
+    """The batch C ABI (sf2d_batch_*): three shots on one model, packed by the
+    library, give the traces of the same shots packed on the host (the same
+    tiles, so the same arithmetic), and each member matches its own FP32
+    oracle run."""
+    import oracle
+    from specfem2d_b200.runtime import ElasticSolver
+
+    c, db, shots = _members()
+    nb = batch.NativeBatch([db], shots=shots, shot_models=[0, 0, 0])
+    assert (nb.nmembers, nb.nspec, nb.nglob) == (3, 3 * db.nspec, 3 * db.nglob)
+    got = nb.forward()
+    again = nb.forward()
+    assert np.array_equal(got, again) and list(nb.member_status()) == [0, 0, 0]
+    nb.close()
+    packed, idx = batch.pack(shots)
+    ref = ElasticSolver(packed).run(db.nstep)
+    assert rel_l2(got, ref) < 1e-6
+    for m, s in enumerate(shots):
+        assert rel_l2(got[idx.rec_off[m]:idx.rec_off[m + 1]], oracle.Oracle(s, 4).run(db.nstep)) < 1e-5
+
+
+@pytest.mark.gpu
+def test_native_gradient_batch_sums_the_shots_of_each_model():
+    """A gradient batch of two models with shots on each: the kernels come back
+    per model, summed over its shots, equal to the per-shot gradients of the
+    host-packed batch summed on the host."""
+    from specfem2d_b200.fwi import l2_misfit_gradient
+
+    c, db, shots = _members()
+    true_db = c.true_db()
+    pos = [(1000.0, 1800.0), (2000.0, 1500.0), (3000.0, 1900.0)]
+    shots_b = batch.shots_on_model(true_db, pos[:2], angle_deg=30.0)
+    members = shots + shots_b
+    nb = batch.NativeBatch([db, true_db], shots=members, shot_models=[0, 0, 0, 1, 1], checkpoint_every=100)
+    syn = nb.forward()
+    obs = 0.9 * syn
+    per_model = nb.adjoint(syn - obs)
+    nb.close()
+    packed, idx = batch.pack(members)
+    _, syn_ref, rk, kk, mk = l2_misfit_gradient(packed, obs, checkpoint_every=100)
+    assert rel_l2(syn, syn_ref) < 1e-6
+    for model, mem in ((0, [0, 1, 2]), (1, [3, 4])):
+        for k, arr in enumerate((rk, kk, mk)):
+            parts = batch.split_elements(arr, idx)
+            ref = sum(parts[m].astype(np.float64) for m in mem)
+            assert rel_l2(per_model[model][k], ref) < 1e-5, (model, k)
+
+
+def test_native_batch_rejects_mismatched_models_before_any_gpu_work():
+    """sf2d_batch_create checks its models and shots on the host and returns
+    SF2D_ERR_INVALID (no GPU is touched)."""
+    c, db, shots = _members()
+    other = Case(nstep=400).start_db()
+    with pytest.raises(Exception, match="share nstep"):
+        batch.NativeBatch([db, other])
+    with pytest.raises(Exception, match="shot model out of range"):
+        batch.NativeBatch([db], shots=shots[:1], shot_models=[3])
+    cfg, _ = load_golden("pressure_source_acoustic")
+    with pytest.raises(Exception, match="CPML"):
+        fl = database_from_config(cfg)
+        fl.acoustic = None  # the CPML check comes first
+        batch.NativeBatch([fl])
