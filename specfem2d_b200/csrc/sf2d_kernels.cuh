@@ -358,15 +358,18 @@ __device__ __forceinline__ void line_weighted(const Params &P, float2 *buf, int 
 // Resident threads per SM the variants ask for: 1536 for the plain ones (6
 // CTAs of 256, at most 40 registers; with the geometry read from global memory
 // the tile's shared memory allows it, and the extra warps hide the loads'
-// latency), 768 for the anisotropic, attenuating, kernel and CPML ones (at
-// most 80 registers; left unbounded the compiler takes over 130 and one CTA
-// fits an SM).
-template <int NT, bool ANISO, bool ATTEN, bool KERN, bool PML>
+// latency), 1024 for the attenuating Newmark one and the gradient ones without
+// attenuation (at most 64 registers, no spill: more warps keep the memory
+// variables' and frames' loads in flight), 768 for the
+// other anisotropic, attenuating, kernel and CPML ones (at most 80 registers;
+// left unbounded the compiler takes over 130 and one CTA fits an SM).
+template <int NT, bool ANISO, bool ATTEN, bool KERN, bool PML, bool LDDRK>
 constexpr int tile_min_blocks() {
-  return (ANISO || ATTEN || KERN || PML) ? 768 / NT : 1536 / NT;
+  return ((ATTEN && !ANISO && !KERN) || (KERN && !ATTEN)) && !PML && !LDDRK ? 1024 / NT
+                                                       : (ANISO || ATTEN || KERN || PML) ? 768 / NT : 1536 / NT;
 }
 template <int NT, bool ANISO, bool ATTEN, bool LDDRK, bool KERN, bool PML = false>
-__global__ void __launch_bounds__(NT, tile_min_blocks<NT, ANISO, ATTEN, KERN, PML>())
+__global__ void __launch_bounds__(NT, tile_min_blocks<NT, ANISO, ATTEN, KERN, PML, LDDRK>())
     k_elastic_tile(const Params P, int record_prev, int stage, int tile0) {
   extern __shared__ __align__(16) unsigned char smem[];
   const TileInfo &ti = P.tiles[tile0 + blockIdx.x];
