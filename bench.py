@@ -94,6 +94,8 @@ TILE_TRAFFIC = {
     ("c3_viscoelastic", 32, 256, 64, 16, 128): 376.16e6 * 16,
     # 64-element tiles (the autotuner's choice): 371.10 MB per launch at quarter scale, x16
     ("c3_viscoelastic", 64, 256, 64, 16, 128): 371.10e6 * 16,
+    # 48-element tiles (the autotuner's choice with the 64-register bound): 369.33 MB at quarter scale, x16
+    ("c3_viscoelastic", 48, 256, 64, 16, 128): 369.33e6 * 16,
 }
 TRAFFIC_SOURCE = {
     ("c2_coupled", 32, 256, 64, 16, 128): "ncu dram__bytes_read.sum + dram__bytes_write.sum of one step's solid "
@@ -104,6 +106,9 @@ TRAFFIC_SOURCE = {
     ("c3_viscoelastic", 64, 256, 64, 16, 128): "ncu dram__bytes_read.sum + dram__bytes_write.sum of one tile "
                                                "launch (64-element tiles) on the quarter-scale model (--scale 4), "
                                                "mean of two launches, scaled by the element count (x16)",
+    ("c3_viscoelastic", 48, 256, 64, 16, 128): "ncu dram__bytes_read.sum + dram__bytes_write.sum of one tile "
+                                               "launch (48-element tiles, 64 registers) on the quarter-scale model "
+                                               "(--scale 4), mean of two launches, scaled by the element count (x16)",
 }
 
 WORKLOAD_DESC = {
