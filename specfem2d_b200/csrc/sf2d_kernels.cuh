@@ -177,6 +177,16 @@ __device__ __forceinline__ void cp_async16(void *s, const void *g) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(s)), "l"(g) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+// Programmatic dependent launch (sm_90 and later): a step kernel launched with
+// the programmatic-serialization attribute may be scheduled while the kernel
+// before it in the stream still runs; griddepcontrol.wait then blocks until
+// that kernel has completed and its writes are visible, so every read of the
+// previous kernel's results comes after it.  launch_dependents lets the next
+// kernel be scheduled once all of this kernel's CTAs have started (the short
+// shared-point and receiver kernels call it, so the next step's tiles start as
+// they drain).  Both are no-ops for a kernel launched without the attribute.
+__device__ __forceinline__ void wait_previous_kernel() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void allow_next_kernel() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
 
 // Shared-memory layout of one tile (sizes from the largest tile); every region
 // starts on a 16-byte boundary, as 16-byte cp.async destinations require:
@@ -373,6 +383,9 @@ template <int NT, bool ANISO, bool ATTEN, bool LDDRK, bool KERN, bool PML = fals
 __global__ void __launch_bounds__(NT, tile_min_blocks<NT, ANISO, ATTEN, KERN, PML, LDDRK>())
     k_elastic_tile(const Params P, int record_prev, int stage, int tile0) {
   extern __shared__ __align__(16) unsigned char smem[];
+  // the shared-point kernel after it is not released early: its CTAs would sit
+  // on the SMs through this kernel's last wave
+  wait_previous_kernel();
   const TileInfo &ti = P.tiles[tile0 + blockIdx.x];
   const int tid = threadIdx.x;
   const int n_int = ti.n_int;
@@ -850,6 +863,8 @@ __global__ void __launch_bounds__(NT, tile_min_blocks<NT, ANISO, ATTEN, KERN, PM
 
 template <bool LDDRK, bool KERN>
 __global__ void __launch_bounds__(SHARED_NT) k_elastic_shared(const Params P, int stage, int last_stage) {
+  wait_previous_kernel();
+  allow_next_kernel();
   const int s = blockIdx.x * SHARED_NT + threadIdx.x;
   const int step = *P.d_step_b;
   if (s < P.nshared && !(P.shared_member && P.member_status[P.shared_member[s]])) {
@@ -924,6 +939,8 @@ __global__ void __launch_bounds__(SHARED_NT) k_elastic_shared(const Params P, in
 
 // records the step before *d_step for every receiver
 static __global__ void k_receivers(const Params P) {
+  wait_previous_kernel();
+  allow_next_kernel();
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r < P.nrec) record_receiver(P, r, *P.d_step - 1);
 }

@@ -194,6 +194,25 @@ struct sf2d_solver {
   // Tiles [first, ntiles): the plain ones on the solver stream, the CPML ones
   // beside them on the side stream when there is one.  first = late_tile0
   // leaves the early tiles to launch_early.
+  // A step kernel on the solver stream with programmatic dependent launch: its
+  // CTAs may be scheduled while the previous step kernel drains (each kernel
+  // waits for its predecessor's completion before reading, wait_previous_kernel).
+  template <typename F, typename... A>
+  void launch_pdl(F fn, int grid, int block, size_t smem_bytes, A... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(static_cast<unsigned>(grid));
+    cfg.blockDim = dim3(static_cast<unsigned>(block));
+    cfg.dynamicSmemBytes = smem_bytes;
+    cfg.stream = stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, fn, args...);
+    if (e != cudaSuccess && launch_error == cudaSuccess) launch_error = e;
+  }
+  cudaError_t launch_error = cudaSuccess;
   void launch_tile(bool record_prev, int stage, int first = 0) {
     const int rp = record_prev ? 1 : 0;
     const int nplain = pml_tile0 - first;
@@ -206,7 +225,7 @@ struct sf2d_solver {
       cudaStreamWaitEvent(stream, ev_join, 0);
       return;
     }
-    if (nplain > 0) tile_fn<<<nplain, nt, smem, stream>>>(P, rp, stage, first);
+    if (nplain > 0) launch_pdl(tile_fn, nplain, nt, smem, P, rp, stage, first);
     if (pml_tile0 < T.ntiles) {
       if (pml_fn)
         pml_fn<<<T.ntiles - pml_tile0, pml_nt, pml_smem, stream>>>(pml_params(), rp, stage, pml_tile0);
@@ -226,11 +245,11 @@ struct sf2d_solver {
     const int nb = std::max(1, (P.nshared + sf2d::SHARED_NT - 1) / sf2d::SHARED_NT);
     const int last = stage == nstage - 1 ? 1 : 0;
     if (lddrk)
-      sf2d::k_elastic_shared<true, false><<<nb, sf2d::SHARED_NT, 0, stream>>>(P, stage, last);
+      launch_pdl(sf2d::k_elastic_shared<true, false>, nb, sf2d::SHARED_NT, 0, P, stage, last);
     else if (kern)
-      sf2d::k_elastic_shared<false, true><<<nb, sf2d::SHARED_NT, 0, stream>>>(P, stage, last);
+      launch_pdl(sf2d::k_elastic_shared<false, true>, nb, sf2d::SHARED_NT, 0, P, stage, last);
     else
-      sf2d::k_elastic_shared<false, false><<<nb, sf2d::SHARED_NT, 0, stream>>>(P, stage, last);
+      launch_pdl(sf2d::k_elastic_shared<false, false>, nb, sf2d::SHARED_NT, 0, P, stage, last);
   }
   int launch_step(bool record_prev) {
     for (int st = 0; st < nstage; ++st) {
@@ -240,12 +259,17 @@ struct sf2d_solver {
     return SF2D_OK;
   }
   int launch_receivers() {
-    if (nrec > 0) sf2d::k_receivers<<<(nrec + 127) / 128, 128, 0, stream>>>(P);
+    if (nrec > 0) launch_pdl(sf2d::k_receivers, (nrec + 127) / 128, 128, 0, P);
     return SF2D_OK;
   }
   int launch_chunk(int n) {
     for (int k = 0; k < n; ++k) launch_step(k > 0);
     launch_receivers();
+    if (launch_error != cudaSuccess) {
+      const cudaError_t e = launch_error;
+      launch_error = cudaSuccess;
+      return sf2d::fail(SF2D_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+    }
     SF2D_CUDA(cudaGetLastError());
     return SF2D_OK;
   }
