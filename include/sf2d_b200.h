@@ -273,7 +273,7 @@ int sf2d_fwi_destroy(sf2d_fwi *f);
  * seismograms and adjoint sources are in member order (each member's
  * receivers in its model's order). */
 typedef struct {
-  int model;                 /* index into the models array */
+  int model;                 /* 0-based index into the models array */
   int nsrc;                  /* the shot's sources, in place of the model's */
   const int *src_ispec;      /* nsrc elements of the model */
   const float *sourcearrays; /* nsrc*25*2 [isrc][j][i][comp] */
