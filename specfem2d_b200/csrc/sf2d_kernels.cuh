@@ -369,14 +369,15 @@ __device__ __forceinline__ void line_weighted(const Params &P, float2 *buf, int 
 // CTAs of 256, at most 40 registers; with the geometry read from global memory
 // the tile's shared memory allows it, and the extra warps hide the loads'
 // latency), 1024 for the attenuating ones (Newmark: no spill; LDDRK: a
-// 32-byte spill, still 3 % faster than 80 registers) and the gradient ones
-// without attenuation (at most 64 registers: more warps keep the memory
-// variables' and frames' loads in flight), 768 for the
+// 32-byte spill, still 3 % faster than 80 registers) and the Newmark gradient
+// ones (at most 64 registers; with attenuation a 16-byte spill, still 4 %
+// faster: more warps keep the memory variables' and frames' loads in flight),
+// 768 for the
 // other anisotropic, attenuating, kernel and CPML ones (at most 80 registers;
 // left unbounded the compiler takes over 130 and one CTA fits an SM).
 template <int NT, bool ANISO, bool ATTEN, bool KERN, bool PML, bool LDDRK>
 constexpr int tile_min_blocks() {
-  return ((ATTEN && !ANISO && !KERN) || (KERN && !ATTEN && !LDDRK)) && !PML ? 1024 / NT
+  return ((ATTEN && !ANISO && !KERN) || (KERN && !LDDRK)) && !PML ? 1024 / NT
                                                        : (ANISO || ATTEN || KERN || PML) ? 768 / NT : 1536 / NT;
 }
 template <int NT, bool ANISO, bool ATTEN, bool LDDRK, bool KERN, bool PML = false>
